@@ -1,0 +1,351 @@
+"""graphene_b200: B200-native sparse-solver hot path of the Graphene framework.
+
+Python mirror of the reference's matrix / solver surface
+(libgraphene/matrix, esa-tu-darmstadt/graphene) over the C ABI in
+``include/graphene_gpu.h``:
+
+* ``generate3DPoissonMatrix`` / ``loadMatrixFromFile`` / ``HostMatrix.from_coo``
+  -> ``HostMatrix`` (matrix/host/HostMatrix.hpp:31-96)
+* ``HostMatrix.copyToTile()`` -> ``Matrix`` on the current CUDA device
+  (matrix/Matrix.hpp:29-131): ``A * x``, ``A.residual``, ``A.vectorNorm``,
+  ``A.solve(x, b, config)``, ``A.createUninitializedVector``
+* ``Configuration.fromJSON`` + ``Solver.createSolver`` (matrix/solver/)
+
+Device vectors are ``torch`` tensors in tile order (the reference's
+decomposed vector layout without halo cells); ``HostMatrix.decomposeVector``
+and ``composeVector`` convert from / to natural row order. All numerical work
+runs in the CUDA kernels of ``lib/libgraphene_b200.so``; there is no CPU
+fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json as _json
+from dataclasses import dataclass
+from typing import Any, Optional, Union
+
+import numpy as np
+
+from . import _lib
+from ._lib import (FLOAT32, FLOAT64, NORM_L1, NORM_L2, NORM_LINF, NORM_NONE, PART_AUTO, PART_BFS,
+                   PART_CONTIGUOUS, PART_EXPLICIT, PART_RCB, TWOFLOAT32, GrapheneError, check)
+
+__all__ = [
+    "FLOAT32", "FLOAT64", "TWOFLOAT32", "NORM_L1", "NORM_L2", "NORM_LINF",
+    "PART_AUTO", "PART_CONTIGUOUS", "PART_RCB", "PART_BFS", "PART_EXPLICIT",
+    "GrapheneError", "HostMatrix", "Matrix", "Configuration", "Solver", "SolverStats",
+    "generate3DPoissonMatrix", "loadMatrixFromFile", "parseType", "launch_count",
+]
+
+_NP = {FLOAT32: np.float32, FLOAT64: np.float64}
+_NAMES = {"float32": FLOAT32, "float": FLOAT32, "float64": FLOAT64, "double": FLOAT64,
+          "twofloat32": TWOFLOAT32}
+
+
+def parseType(name: Union[str, int]) -> int:
+    """common/Type.cpp parseType: "float32" | "float64" | "twofloat32"."""
+    if isinstance(name, int):
+        return name
+    if name not in _NAMES:
+        raise ValueError(f"Unknown type: {name}")
+    return _NAMES[name]
+
+
+def launch_count() -> int:
+    """Kernel launches issued by the native library so far."""
+    return int(_lib.lib().gr_launch_count())
+
+
+def _torch():
+    import torch  # plumbing for device memory only
+    return torch
+
+
+def _torch_dtype(t: int):
+    torch = _torch()
+    if t == FLOAT32:
+        return torch.float32
+    if t == FLOAT64:
+        return torch.float64
+    raise ValueError("twofloat32 vectors are stored as float32 pairs; use FLOAT32 with 2*n")
+
+
+def _dtype_of(tensor) -> int:
+    torch = _torch()
+    if tensor.dtype == torch.float32:
+        return FLOAT32
+    if tensor.dtype == torch.float64:
+        return FLOAT64
+    raise TypeError(f"unsupported vector dtype {tensor.dtype}")
+
+
+def _ptr(a) -> C.c_void_p:
+    if a is None:
+        return C.c_void_p(None)
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return C.c_void_p(a.ctypes.data)
+    return C.c_void_p(a.data_ptr())
+
+
+@dataclass
+class SolverStats:
+    """matrix/solver/SolverStats.hpp:29-69 (norms accumulated in FP64)."""
+    initialResidual: float
+    finalResidual: float
+    bNorm: float
+    iterations: int
+    converged: bool
+    singular: bool
+    status: int
+    innerIterations: int
+    solveMs: float
+
+    @staticmethod
+    def _from(s: _lib.Stats) -> "SolverStats":
+        return SolverStats(s.initial_residual, s.final_residual, s.b_norm, s.iterations,
+                           bool(s.converged), bool(s.singular), s.status, s.inner_iterations,
+                           s.solve_ms)
+
+
+class HostMatrix:
+    """Host-side matrix with its tile layout (matrix/host/HostMatrix.hpp)."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        info = _lib.MatrixInfo()
+        check(_lib.lib().gr_host_matrix_get_info(self._h, C.byref(info)))
+        self.info = info
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.lib().gr_host_matrix_destroy(h)
+            self._h = None
+
+    # -- constructors ------------------------------------------------------
+    @staticmethod
+    def from_coo(n: int, rows, cols, vals, numTiles: int, partitioner: int = PART_AUTO,
+                 rowToTile=None, coords=None, valueType: int = FLOAT32) -> "HostMatrix":
+        """HostMatrix(MatrixFormat::CRS, TripletMatrix, numTiles)."""
+        r = np.ascontiguousarray(rows, dtype=np.int64)
+        c = np.ascontiguousarray(cols, dtype=np.int64)
+        v = np.ascontiguousarray(vals, dtype=np.float64)
+        rt = None if rowToTile is None else np.ascontiguousarray(rowToTile, dtype=np.int32)
+        cd = None if coords is None else np.ascontiguousarray(coords, dtype=np.float64)
+        if rt is not None:
+            partitioner = PART_EXPLICIT
+        h = C.c_void_p()
+        check(_lib.lib().gr_host_matrix_from_coo(n, len(v), _ptr(r), _ptr(c), _ptr(v), numTiles,
+                                                  partitioner, _ptr(rt), _ptr(cd), valueType,
+                                                  C.byref(h)))
+        return HostMatrix(h)
+
+    # -- layout queries ----------------------------------------------------
+    @property
+    def numRows(self) -> int:
+        return self.info.num_rows
+
+    @property
+    def numTiles(self) -> int:
+        return self.info.num_tiles
+
+    @property
+    def numOffDiag(self) -> int:
+        return self.info.num_off_diag
+
+    def multicolorRecommended(self) -> bool:
+        return bool(self.info.multicolor_recommended)
+
+    def rowToTile(self) -> np.ndarray:
+        out = np.empty(self.numRows, dtype=np.int32)
+        check(_lib.lib().gr_host_matrix_row_to_tile(self._h, _ptr(out)))
+        return out
+
+    def tileSizes(self) -> np.ndarray:
+        out = np.empty((self.numTiles, 3), dtype=np.int64)
+        check(_lib.lib().gr_host_matrix_tile_sizes(self._h, _ptr(out)))
+        return out
+
+    def localToGlobal(self) -> np.ndarray:
+        out = np.empty(self.numRows + self.info.num_halo_total, dtype=np.int64)
+        check(_lib.lib().gr_host_matrix_local_to_global(self._h, _ptr(out)))
+        return out
+
+    def localCrs(self):
+        rp = np.empty(self.numRows + self.numTiles, dtype=np.int64)
+        ci = np.empty(self.numOffDiag, dtype=np.int32)
+        od = np.empty(self.numOffDiag, dtype=np.float64)
+        dg = np.empty(self.numRows, dtype=np.float64)
+        check(_lib.lib().gr_host_matrix_local_crs(self._h, _ptr(rp), _ptr(ci), _ptr(od), _ptr(dg)))
+        return rp, ci, od, dg
+
+    def levels(self):
+        lo = np.empty(self.numRows, dtype=np.int32)
+        up = np.empty(self.numRows, dtype=np.int32)
+        check(_lib.lib().gr_host_matrix_levels(self._h, _ptr(lo), _ptr(up)))
+        return lo, up
+
+    # -- vectors -----------------------------------------------------------
+    def decomposeVector(self, vec, t: int = FLOAT32) -> np.ndarray:
+        """DistributedTileLayout::decomposeVector without halo cells."""
+        a = np.ascontiguousarray(vec, dtype=_NP[t])
+        out = np.empty_like(a)
+        check(_lib.lib().gr_host_matrix_decompose_vector(self._h, _ptr(a), _ptr(out), t))
+        return out
+
+    def composeVector(self, vec, t: int = FLOAT32) -> np.ndarray:
+        a = np.ascontiguousarray(vec, dtype=_NP[t])
+        out = np.empty_like(a)
+        check(_lib.lib().gr_host_matrix_compose_vector(self._h, _ptr(a), _ptr(out), t))
+        return out
+
+    def copyToTile(self) -> "Matrix":
+        """HostMatrix::copyToTile: upload to the current CUDA device."""
+        return Matrix(self)
+
+
+def generate3DPoissonMatrix(valueType: int, nx: int, ny: int, nz: int, numTiles: int,
+                            partitioner: int = PART_AUTO) -> HostMatrix:
+    """matrix/host/HostMatrix.hpp:94-96 (7-point Poisson, Dirichlet)."""
+    h = C.c_void_p()
+    check(_lib.lib().gr_host_matrix_poisson(nx, ny, nz, numTiles, partitioner, parseType(valueType),
+                                            C.byref(h)))
+    return HostMatrix(h)
+
+
+def loadMatrixFromFile(valueType: int, path: str, numTiles: int,
+                       partitioner: int = PART_AUTO) -> HostMatrix:
+    """matrix/host/HostMatrix.hpp:88-91 (MatrixMarket coordinate files)."""
+    h = C.c_void_p()
+    check(_lib.lib().gr_host_matrix_load_mm(str(path).encode(), numTiles, partitioner,
+                                            parseType(valueType), C.byref(h)))
+    return HostMatrix(h)
+
+
+class Configuration:
+    """Solver configuration tree (matrix/solver/Configuration.hpp:40)."""
+
+    def __init__(self, text: str):
+        self.text = text
+
+    @staticmethod
+    def fromJSON(cfg: Union[str, dict]) -> "Configuration":
+        return Configuration(cfg if isinstance(cfg, str) else _json.dumps(cfg))
+
+
+class Solver:
+    """Solver::createSolver(A, config) and Solver::solve(x, b)."""
+
+    def __init__(self, A: "Matrix", config: Union[Configuration, str, dict]):
+        if not isinstance(config, Configuration):
+            config = Configuration.fromJSON(config)
+        self.A = A
+        self._s = C.c_void_p()
+        check(_lib.lib().gr_solver_create(A._m, config.text.encode(), C.byref(self._s)))
+
+    @staticmethod
+    def createSolver(A: "Matrix", config) -> "Solver":
+        return Solver(A, config)
+
+    def __del__(self):
+        s = getattr(self, "_s", None)
+        if s:
+            _lib.lib().gr_solver_destroy(s)
+            self._s = None
+
+    def name(self) -> str:
+        buf = C.create_string_buffer(256)
+        check(_lib.lib().gr_solver_name(self._s, buf, 256))
+        return buf.value.decode()
+
+    def solve(self, x, b) -> SolverStats:
+        """x (in/out) and b: device tensors in tile order."""
+        st = _lib.Stats()
+        check(_lib.lib().gr_solve(self._s, _ptr(x), _dtype_of(x), _ptr(b), _dtype_of(b),
+                                  C.byref(st)))
+        return SolverStats._from(st)
+
+    def solveHost(self, x: np.ndarray, b: np.ndarray) -> SolverStats:
+        """Host arrays in natural order; copies are part of the call."""
+        t = FLOAT32 if x.dtype == np.float32 else FLOAT64
+        st = _lib.Stats()
+        check(_lib.lib().gr_solve_host(self._s, _ptr(x), t, _ptr(b), t, C.byref(st)))
+        return SolverStats._from(st)
+
+    def phi(self, t: int = FLOAT64):
+        """Extended-precision solution of the last IterativeRefinement solve."""
+        torch = _torch()
+        out = torch.empty(self.A.numRows, dtype=_torch_dtype(t), device=self.A.device)
+        check(_lib.lib().gr_solver_phi(self._s, _ptr(out), t))
+        return out
+
+
+class Matrix:
+    """Device matrix (matrix/Matrix.hpp:29-131)."""
+
+    def __init__(self, host: HostMatrix):
+        torch = _torch()
+        self.host = host
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self._m = C.c_void_p()
+        check(_lib.lib().gr_matrix_create(host._h, C.byref(self._m)))
+
+    def __del__(self):
+        m = getattr(self, "_m", None)
+        if m:
+            _lib.lib().gr_matrix_destroy(m)
+            self._m = None
+
+    @property
+    def numRows(self) -> int:
+        return self.host.numRows
+
+    @property
+    def numTiles(self) -> int:
+        return self.host.numTiles
+
+    def createUninitializedVector(self, t: int = FLOAT32):
+        torch = _torch()
+        return torch.empty(self.numRows, dtype=_torch_dtype(parseType(t)), device=self.device)
+
+    def vector(self, natural, t: int = FLOAT32):
+        """Device vector in tile order from a natural-order host array."""
+        torch = _torch()
+        return torch.from_numpy(self.host.decomposeVector(natural, t)).to(self.device)
+
+    def toNatural(self, x) -> np.ndarray:
+        t = _dtype_of(x)
+        return self.host.composeVector(x.detach().cpu().numpy(), t)
+
+    def __mul__(self, x):
+        """Matrix::operator* -> CRSMatrix::spmv."""
+        y = _torch().empty_like(x)
+        check(_lib.lib().gr_spmv(self._m, _ptr(x), _ptr(y), _dtype_of(x)))
+        return y
+
+    def spmv(self, x, y) -> None:
+        check(_lib.lib().gr_spmv(self._m, _ptr(x), _ptr(y), _dtype_of(x)))
+
+    def residual(self, x, b, destType: Optional[int] = None, intermediateType: Optional[int] = None,
+                 xType: Optional[int] = None):
+        """Matrix::residual(x, b, destType, intermediateType)."""
+        torch = _torch()
+        xt = _dtype_of(x) if xType is None else xType
+        if destType is None:
+            destType = xt
+        if intermediateType is None:
+            intermediateType = destType
+        r = torch.empty(self.numRows, dtype=_torch_dtype(destType), device=self.device)
+        check(_lib.lib().gr_residual(self._m, _ptr(x), xt, _ptr(b), _dtype_of(b), _ptr(r),
+                                     destType, intermediateType))
+        return r
+
+    def vectorNorm(self, norm: int, x) -> float:
+        out = C.c_double()
+        check(_lib.lib().gr_vector_norm(self._m, norm, _ptr(x), _dtype_of(x), C.byref(out)))
+        return out.value
+
+    def solve(self, x, b, config) -> SolverStats:
+        """Matrix::solve(x, b, config) (matrix/Matrix.cpp:26-30)."""
+        return Solver(self, config).solve(x, b)

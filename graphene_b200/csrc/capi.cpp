@@ -1,0 +1,335 @@
+// extern "C" boundary of graphene_b200 (include/graphene_gpu.h).
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "device.hpp"
+#include "host_matrix.hpp"
+#include "solvers.hpp"
+
+struct gr_host_matrix {
+  std::shared_ptr<gr::HostMatrix> m;
+};
+
+struct gr_matrix {
+  std::unique_ptr<gr::DeviceMatrix> d;
+};
+
+struct gr_solver {
+  std::unique_ptr<gr::SolverTree> s;
+};
+
+namespace {
+
+thread_local std::string g_lastError;
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    g_lastError.clear();
+    return GR_OK;
+  } catch (const gr::Error& e) {
+    g_lastError = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_lastError = "host allocation failed";
+    return GR_ENOMEM;
+  } catch (const std::exception& e) {
+    g_lastError = e.what();
+    return GR_EINVAL;
+  } catch (...) {
+    g_lastError = "unknown error";
+    return GR_EINVAL;
+  }
+}
+
+void need(const void* p, const char* what) {
+  if (!p) gr::fail(GR_EINVAL, std::string(what) + " must not be NULL");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gr_last_error(void) { return g_lastError.c_str(); }
+
+int gr_version(void) { return 1; }
+
+int64_t gr_launch_count(void) { return gr::launchCount(); }
+
+int gr_host_matrix_from_coo(int64_t num_rows, int64_t nnz, const int64_t* rows, const int64_t* cols,
+                            const double* vals, int64_t num_tiles, gr_partitioner partitioner,
+                            const int32_t* row_to_tile, const double* coords, gr_dtype value_type,
+                            gr_host_matrix** out) {
+  return guarded([&] {
+    need(out, "out");
+    if (nnz < 0) gr::fail(GR_EINVAL, "nnz must be non-negative");
+    if (nnz > 0) { need(rows, "rows"); need(cols, "cols"); need(vals, "vals"); }
+    gr::Coo coo;
+    coo.nrows = coo.ncols = num_rows;
+    coo.row.assign(rows, rows + nnz);
+    coo.col.assign(cols, cols + nnz);
+    coo.val.assign(vals, vals + nnz);
+    auto h = gr::HostMatrix::fromCoo(std::move(coo), num_tiles, partitioner, row_to_tile, coords,
+                                     gr::toDType(value_type));
+    *out = new gr_host_matrix{std::move(h)};
+  });
+}
+
+int gr_host_matrix_poisson(int64_t nx, int64_t ny, int64_t nz, int64_t num_tiles,
+                           gr_partitioner partitioner, gr_dtype value_type, gr_host_matrix** out) {
+  return guarded([&] {
+    need(out, "out");
+    gr::GeneratedCsr g = gr::generatePoisson(nx, ny, nz);
+    auto h = gr::HostMatrix::fromSortedCsr(g.n, std::move(g.rowPtr), std::move(g.col),
+                                           std::move(g.val), num_tiles, partitioner, nullptr,
+                                           std::move(g.coords), gr::toDType(value_type));
+    *out = new gr_host_matrix{std::move(h)};
+  });
+}
+
+int gr_host_matrix_load_mm(const char* path, int64_t num_tiles, gr_partitioner partitioner,
+                           gr_dtype value_type, gr_host_matrix** out) {
+  return guarded([&] {
+    need(path, "path");
+    need(out, "out");
+    gr::Coo coo = gr::readMatrixMarket(path, gr::toDType(value_type));
+    auto h = gr::HostMatrix::fromCoo(std::move(coo), num_tiles, partitioner, nullptr, nullptr,
+                                     gr::toDType(value_type));
+    *out = new gr_host_matrix{std::move(h)};
+  });
+}
+
+void gr_host_matrix_destroy(gr_host_matrix* h) { delete h; }
+
+int gr_host_matrix_get_info(const gr_host_matrix* h, gr_matrix_info* out) {
+  return guarded([&] {
+    need(h, "matrix");
+    need(out, "out");
+    *out = h->m->info();
+  });
+}
+
+int gr_host_matrix_row_to_tile(const gr_host_matrix* h, int32_t* row_to_tile) {
+  return guarded([&] {
+    need(h, "matrix");
+    need(row_to_tile, "row_to_tile");
+    std::memcpy(row_to_tile, h->m->rowToTile.data(), sizeof(int32_t) * h->m->n);
+  });
+}
+
+int gr_host_matrix_tile_sizes(const gr_host_matrix* h, int64_t* out) {
+  return guarded([&] {
+    need(h, "matrix");
+    need(out, "out");
+    for (gr::i32 T = 0; T < h->m->P; ++T) {
+      out[3 * T] = h->m->tiles[T].nInterior;
+      out[3 * T + 1] = h->m->tiles[T].nSeparator;
+      out[3 * T + 2] = h->m->tiles[T].nHalo;
+    }
+  });
+}
+
+int gr_host_matrix_local_to_global(const gr_host_matrix* h, int64_t* out) {
+  return guarded([&] {
+    need(h, "matrix");
+    need(out, "out");
+    const gr::HostMatrix& H = *h->m;
+    int64_t o = 0;
+    for (gr::i32 T = 0; T < H.P; ++T) {
+      for (gr::i64 p = H.tileStart[T]; p < H.tileStart[T + 1]; ++p) out[o++] = H.iperm[p];
+      for (gr::i32 R : H.tiles[T].haloRegions)
+        for (gr::i64 g : H.regions[R].cells) out[o++] = g;
+    }
+  });
+}
+
+int gr_host_matrix_local_crs(const gr_host_matrix* h, int64_t* row_ptr, int32_t* col_ind,
+                             double* off_diag, double* diag) {
+  return guarded([&] {
+    need(h, "matrix");
+    const gr::HostMatrix& H = *h->m;
+    if (row_ptr) {
+      int64_t o = 0;
+      for (gr::i32 T = 0; T < H.P; ++T) {
+        gr::i64 b = H.tileStart[T];
+        for (gr::i64 p = b; p <= H.tileStart[T + 1]; ++p) row_ptr[o++] = H.rowPtr[p] - H.rowPtr[b];
+      }
+    }
+    if (col_ind) std::memcpy(col_ind, H.colLocal.data(), sizeof(int32_t) * H.m);
+    if (off_diag) std::memcpy(off_diag, H.offDiag.data(), sizeof(double) * H.m);
+    if (diag) std::memcpy(diag, H.diag.data(), sizeof(double) * H.n);
+  });
+}
+
+int gr_host_matrix_levels(const gr_host_matrix* h, int32_t* lower_level, int32_t* upper_level) {
+  return guarded([&] {
+    need(h, "matrix");
+    if (lower_level) std::memcpy(lower_level, h->m->lowerLevel.data(), sizeof(int32_t) * h->m->n);
+    if (upper_level) std::memcpy(upper_level, h->m->upperLevel.data(), sizeof(int32_t) * h->m->n);
+  });
+}
+
+int gr_host_matrix_decompose_vector(const gr_host_matrix* h, const void* natural, void* tile_ordered,
+                                    gr_dtype t) {
+  return guarded([&] {
+    need(h, "matrix");
+    need(natural, "natural");
+    need(tile_ordered, "tile_ordered");
+    gr::DType dt = gr::toDType(t);
+    if (dt == gr::DType::F32)
+      h->m->decompose(static_cast<const float*>(natural), static_cast<float*>(tile_ordered));
+    else
+      h->m->decompose(static_cast<const double*>(natural), static_cast<double*>(tile_ordered));
+  });
+}
+
+int gr_host_matrix_compose_vector(const gr_host_matrix* h, const void* tile_ordered, void* natural,
+                                  gr_dtype t) {
+  return guarded([&] {
+    need(h, "matrix");
+    need(natural, "natural");
+    need(tile_ordered, "tile_ordered");
+    gr::DType dt = gr::toDType(t);
+    if (dt == gr::DType::F32)
+      h->m->compose(static_cast<const float*>(tile_ordered), static_cast<float*>(natural));
+    else
+      h->m->compose(static_cast<const double*>(tile_ordered), static_cast<double*>(natural));
+  });
+}
+
+int gr_matrix_create(gr_host_matrix* h, gr_matrix** out) {
+  return guarded([&] {
+    need(h, "host matrix");
+    need(out, "out");
+    auto d = std::make_unique<gr::DeviceMatrix>(h->m);
+    *out = new gr_matrix{std::move(d)};
+  });
+}
+
+void gr_matrix_destroy(gr_matrix* A) { delete A; }
+
+int gr_matrix_set_stream(gr_matrix* A, void* cuda_stream) {
+  return guarded([&] {
+    need(A, "matrix");
+    A->d->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : A->d->ownStream;
+  });
+}
+
+int gr_matrix_get_info(const gr_matrix* A, gr_matrix_info* out) {
+  return guarded([&] {
+    need(A, "matrix");
+    need(out, "out");
+    *out = A->d->host->info();
+  });
+}
+
+int gr_spmv(gr_matrix* A, const void* x, void* y, gr_dtype t) {
+  return guarded([&] {
+    need(A, "matrix");
+    need(x, "x");
+    need(y, "y");
+    gr::launchSpmv(*A->d, x, y, gr::toDType(t), A->d->stream);
+    GR_CUDA(cudaStreamSynchronize(A->d->stream));
+  });
+}
+
+int gr_residual(gr_matrix* A, const void* x, gr_dtype x_t, const void* b, gr_dtype b_t, void* r,
+                gr_dtype r_t, gr_dtype inter_t) {
+  return guarded([&] {
+    need(A, "matrix");
+    need(x, "x");
+    need(b, "b");
+    need(r, "r");
+    gr::launchResidual(*A->d, x, gr::toDType(x_t), b, gr::toDType(b_t), r, gr::toDType(r_t),
+                       gr::toDType(inter_t), -1, nullptr, A->d->stream);
+    GR_CUDA(cudaStreamSynchronize(A->d->stream));
+  });
+}
+
+int gr_vector_norm(gr_matrix* A, gr_norm norm, const void* x, gr_dtype t, double* out) {
+  return guarded([&] {
+    need(A, "matrix");
+    need(x, "x");
+    need(out, "out");
+    if (norm == GR_NORM_NONE || norm < 0 || norm > GR_NORM_NONE) gr::fail(GR_EINVAL, "invalid norm");
+    double* d = A->d->scalarOut.as<double>();
+    gr::launchNorm(*A->d, x, gr::toDType(t), norm, d, A->d->stream);
+    GR_CUDA(cudaMemcpyAsync(out, d, sizeof(double), cudaMemcpyDeviceToHost, A->d->stream));
+    GR_CUDA(cudaStreamSynchronize(A->d->stream));
+  });
+}
+
+int gr_decompose_vector(gr_matrix* A, const void* natural, void* tile_ordered, gr_dtype t) {
+  return guarded([&] {
+    need(A, "matrix");
+    need(natural, "natural");
+    need(tile_ordered, "tile_ordered");
+    gr::launchPermute(*A->d, natural, tile_ordered, gr::toDType(t), true, A->d->stream);
+    GR_CUDA(cudaStreamSynchronize(A->d->stream));
+  });
+}
+
+int gr_compose_vector(gr_matrix* A, const void* tile_ordered, void* natural, gr_dtype t) {
+  return guarded([&] {
+    need(A, "matrix");
+    need(natural, "natural");
+    need(tile_ordered, "tile_ordered");
+    gr::launchPermute(*A->d, tile_ordered, natural, gr::toDType(t), false, A->d->stream);
+    GR_CUDA(cudaStreamSynchronize(A->d->stream));
+  });
+}
+
+int gr_solver_create(gr_matrix* A, const char* json, gr_solver** out) {
+  return guarded([&] {
+    need(A, "matrix");
+    need(json, "json");
+    need(out, "out");
+    auto s = gr::SolverTree::create(*A->d, json);
+    *out = new gr_solver{std::move(s)};
+  });
+}
+
+void gr_solver_destroy(gr_solver* s) { delete s; }
+
+int gr_solve(gr_solver* s, void* x, gr_dtype x_t, const void* b, gr_dtype b_t, gr_stats* stats) {
+  return guarded([&] {
+    need(s, "solver");
+    need(x, "x");
+    need(b, "b");
+    gr_stats st = s->s->solve(x, gr::toDType(x_t), b, gr::toDType(b_t));
+    if (stats) *stats = st;
+  });
+}
+
+int gr_solve_host(gr_solver* s, void* x, gr_dtype x_t, const void* b, gr_dtype b_t, gr_stats* stats) {
+  return guarded([&] {
+    need(s, "solver");
+    need(x, "x");
+    need(b, "b");
+    gr_stats st = s->s->solveHost(x, gr::toDType(x_t), b, gr::toDType(b_t));
+    if (stats) *stats = st;
+  });
+}
+
+int gr_solver_phi(gr_solver* s, void* out, gr_dtype t) {
+  return guarded([&] {
+    need(s, "solver");
+    need(out, "out");
+    s->s->copyPhi(out, gr::toDType(t));
+  });
+}
+
+int gr_solver_name(const gr_solver* s, char* buf, size_t len) {
+  return guarded([&] {
+    need(s, "solver");
+    need(buf, "buf");
+    std::string nm = s->s->name();
+    if (len == 0) gr::fail(GR_EINVAL, "buffer length is 0");
+    std::strncpy(buf, nm.c_str(), len - 1);
+    buf[len - 1] = '\0';
+  });
+}
+
+}  // extern "C"

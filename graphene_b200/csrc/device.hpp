@@ -1,0 +1,149 @@
+// Device-side data structures of graphene_b200 and the host wrappers that
+// launch its CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.hpp"
+#include "host_matrix.hpp"
+
+namespace gr {
+
+void cudaCheck(cudaError_t e, const char* what);
+#define GR_CUDA(call) ::gr::cudaCheck((call), #call)
+
+// Counts every kernel launch made through this library.
+void noteLaunch(int count = 1);
+i64 launchCount();
+
+// Owning device allocation.
+class DBuf {
+ public:
+  DBuf() = default;
+  explicit DBuf(size_t bytes) { alloc(bytes); }
+  ~DBuf() { release(); }
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept : p_(o.p_), bytes_(o.bytes_) { o.p_ = nullptr; o.bytes_ = 0; }
+  DBuf& operator=(DBuf&& o) noexcept {
+    if (this != &o) { release(); p_ = o.p_; bytes_ = o.bytes_; o.p_ = nullptr; o.bytes_ = 0; }
+    return *this;
+  }
+  void alloc(size_t bytes);
+  void release();
+  void* get() const { return p_; }
+  template <class T> T* as() const { return static_cast<T*>(p_); }
+  size_t bytes() const { return bytes_; }
+  template <class T>
+  void upload(const std::vector<T>& v) {
+    alloc(std::max<size_t>(1, v.size()) * sizeof(T));
+    if (!v.empty()) GR_CUDA(cudaMemcpy(p_, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  }
+
+ private:
+  void* p_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+// Values converted to the stored coefficient type (float or double).
+void uploadValues(DBuf& dst, const std::vector<double>& v, DType t);
+
+// Sliced-ELLPACK (chunk height 32) copy of the off-diagonal part in tile
+// order. Row r of chunk c keeps its entries in the reference's tile-local
+// column order at slots base[c] + 32*k + (r % 32); padding slots hold
+// column -1 and value 0. Used by SpMV and residual kernels.
+struct SellMatrix {
+  i32 n = 0, nChunks = 0;
+  i64 slots = 0;
+  DBuf base;  // i32[nChunks + 1]
+  DBuf col;   // i32[slots], tile-order column
+  DBuf val;   // value type [slots]
+};
+
+// Level schedule of one sweep over all tiles: for each tile its levels, for
+// each level its rows, and for each row its entries stored level-major
+// (slot = levelSlotStart + k * levelRows + q), so a level's rows load their
+// k-th entries with one coalesced access.
+struct LevelSchedule {
+  i32 numLevels = 0;
+  i32 maxLevelRows = 0;
+  i64 slots = 0;
+  DBuf tileLvlStart;  // i32[P + 1]
+  DBuf lvlRowStart;   // i32[L + 1]
+  DBuf lvlSlotStart;  // i64[L + 1]
+  DBuf rows;          // i32 tile-order row per level row
+  DBuf col;           // i32 tile-order column per slot, -1 = padding
+  DBuf src;           // i32 index into the local CRS values per slot, -1 = padding
+  DBuf val;           // packed values per slot (value type)
+};
+
+// Kinds of entries a schedule keeps per row.
+enum class SweepEntries {
+  Lower,        // tile-local columns below the row, ascending (ILU forward)
+  UpperDesc,    // tile-local columns above the row (non-halo), descending (ILU backward)
+  All           // every off-diagonal entry in tile-local order (Gauss-Seidel)
+};
+
+struct DeviceMatrix {
+  std::shared_ptr<HostMatrix> host;
+  int device = 0;
+  int numSMs = 148;
+  cudaStream_t ownStream = nullptr;
+  cudaStream_t stream = nullptr;
+  i32 n = 0, P = 0;
+  i64 m = 0;
+  DType vt = DType::F32;
+
+  SellMatrix sell;
+  DBuf diag;       // value type [n]
+  DBuf tileStart;  // i32[P + 1]
+  DBuf iperm;      // i32[n]
+
+  // Tile-local CRS in tile order (for the factorisation), built on demand.
+  bool haveLocalCrs = false;
+  DBuf rowPtr;     // i32[n + 1]
+  DBuf colLocal;   // i32[m]
+  DBuf offDiag;    // value type [m]
+
+  // Schedules, built on demand.
+  std::unique_ptr<LevelSchedule> lowerSched, upperSched, gsSched;
+
+  // Reduction scratch: per-block partials and an arrival counter.
+  DBuf partials;   // double[maxBlocks * 8]
+  DBuf counter;    // unsigned[16]
+  int redBlocks = 0;
+
+  // Small device scratch for norms returned to the host.
+  DBuf scalarOut;  // double[8]
+
+  explicit DeviceMatrix(std::shared_ptr<HostMatrix> h);
+  ~DeviceMatrix();
+
+  void ensureLocalCrs();
+  LevelSchedule& schedule(SweepEntries kind);
+  // Rounded-up kernel grid for a row loop of n rows.
+  int spmvBlocks() const;
+};
+
+// ---- launchers -------------------------------------------------------
+
+// y = A x (reference CRSMatrix::spmv). xt == yt.
+void launchSpmv(DeviceMatrix& A, const void* x, void* y, DType t, cudaStream_t s);
+
+// r = b - A x in inter (reference CRSMatrix::residual); optionally
+// accumulates a norm of r into normOut (device double) when normKind >= 0.
+void launchResidual(DeviceMatrix& A, const void* x, DType xt, const void* b, DType bt, void* r,
+                    DType rt, DType inter, int normKind, double* normOut, cudaStream_t s);
+
+// Norm of a tile-order vector, FP64 accumulation. normKind: gr_norm.
+void launchNorm(DeviceMatrix& A, const void* x, DType t, int normKind, double* out,
+                cudaStream_t s);
+
+void launchPermute(DeviceMatrix& A, const void* src, void* dst, DType t, bool toTileOrder,
+                   cudaStream_t s);
+
+}  // namespace gr

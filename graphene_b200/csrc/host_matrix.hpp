@@ -1,0 +1,135 @@
+// Host-side matrix pipeline: triplets -> CRS with split diagonal -> row
+// partition -> interior/separator/halo tile layout -> tile-local CRS ->
+// level sets. Follows matrix/host/details/crs/CRSHostMatrix.cpp and
+// matrix/host/DistributedTileLayout.cpp of the reference, re-designed for a
+// GPU: tiles are stored contiguously in "tile order" (the reference's
+// decomposed vector layout), so a tile-local column id maps to a global
+// vector index and halo cells need no storage.
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.hpp"
+
+namespace gr {
+
+// A matrix in triplet format (matrix/host/details/CoordinateFormat.hpp:29-38).
+struct Coo {
+  i64 nrows = 0, ncols = 0;
+  std::vector<i64> row, col;
+  std::vector<double> val;
+};
+
+struct HostMatrix {
+  DType valueType = DType::F32;
+  i64 n = 0;  // rows
+  i64 m = 0;  // stored off-diagonal entries
+  i32 P = 0;  // tiles after empty-tile removal
+
+  // Global CRS with the diagonal split off (CRSHostMatrix.cpp:88-137).
+  std::vector<i64> gRowPtr;
+  std::vector<i64> gCol;
+  std::vector<double> gVal;   // rounded to valueType
+  std::vector<double> gDiag;  // rounded to valueType, 0 when absent
+  std::vector<double> coords; // optional, 3 per row (generated grids)
+
+  // Partitioning::rowToTile after empty-tile removal.
+  std::vector<i32> rowToTile;
+
+  // A separator region: the rows of one tile that are needed by exactly the
+  // tiles in dst (DistributedTileLayout.hpp:269-282).
+  struct Region {
+    i32 tile = 0;
+    std::vector<i32> dst;  // ascending
+    std::vector<i64> cells;  // global rows, ascending
+  };
+  std::vector<Region> regions;  // numbered by (owning tile, creation order)
+
+  struct Tile {
+    i64 nInterior = 0, nSeparator = 0, nHalo = 0;
+    std::vector<i64> interior;       // global rows, ascending
+    std::vector<i32> sepRegions;     // region ids in creation order
+    std::vector<i32> haloRegions;    // region ids in canonical order
+    std::vector<std::pair<i32, i64>> haloOffset;  // (region id, local offset), sorted by id
+    i64 rows() const { return nInterior + nSeparator; }
+  };
+  std::vector<Tile> tiles;
+  std::vector<i64> tileStart;  // P + 1 offsets into tile order
+  std::vector<i32> perm;       // global row -> tile-order index
+  std::vector<i32> iperm;      // tile-order index -> global row
+  std::vector<i32> regionOf;   // global row -> region id (-1 for interior rows)
+  std::vector<i32> idxInRegion;
+
+  // Tile-local CRS in tile order: rows are tile-order indices, each row's
+  // entries sorted by tile-local column id (CRSHostMatrix.cpp:379-432).
+  std::vector<i64> rowPtr;     // n + 1
+  std::vector<i32> colPerm;    // column as tile-order index
+  std::vector<i32> colLocal;   // tile-local column id (halo ids >= tile rows)
+  std::vector<double> offDiag; // values in local order
+  std::vector<double> diag;    // tile order
+
+  // Level ("colour") of each row in its tile's lower / upper dependency DAG.
+  std::vector<i32> lowerLevel, upperLevel;  // tile order
+  std::vector<i32> nLowerLevels, nUpperLevels;  // per tile
+  bool multicolorRecommended = false;
+
+  i64 numHaloTotal = 0;
+  i64 maxTileRows = 0;
+
+  // Builds everything from triplets. rowToTileIn is used for
+  // GR_PART_EXPLICIT; coords (3 per row) for GR_PART_RCB.
+  static std::shared_ptr<HostMatrix> fromCoo(Coo coo, i64 numTiles, gr_partitioner part,
+                                             const i32* rowToTileIn, const double* coords,
+                                             DType valueType);
+  // Same, from a CRS whose rows are already sorted by column (fast path of
+  // the generators; identical result to fromCoo on the same entries).
+  static std::shared_ptr<HostMatrix> fromSortedCsr(i64 n, std::vector<i64> rowPtr,
+                                                   std::vector<i64> col, std::vector<double> val,
+                                                   i64 numTiles, gr_partitioner part,
+                                                   const i32* rowToTileIn,
+                                                   std::vector<double> coords, DType valueType);
+
+  gr_matrix_info info() const;
+
+  template <class T>
+  void decompose(const T* natural, T* tileOrdered) const {
+    parallelChunks(n, [&](i64 b, i64 e) {
+      for (i64 p = b; p < e; ++p) tileOrdered[p] = natural[iperm[p]];
+    });
+  }
+  template <class T>
+  void compose(const T* tileOrdered, T* natural) const {
+    parallelChunks(n, [&](i64 b, i64 e) {
+      for (i64 p = b; p < e; ++p) natural[iperm[p]] = tileOrdered[p];
+    });
+  }
+
+ private:
+  void buildFromGlobalCrs(i64 numTiles, gr_partitioner part, const i32* rowToTileIn);
+  void buildTileLayout();
+  void buildLocalCrs();
+  void buildLevels();
+};
+
+// Row partitioners (raw part ids in [0, numParts), before empty-part removal).
+std::vector<i32> partitionContiguous(const HostMatrix& A, i32 numParts);
+std::vector<i32> partitionRcb(const HostMatrix& A, i32 numParts);
+std::vector<i32> partitionBfs(const HostMatrix& A, i32 numParts);
+
+// Generators (rows sorted by column).
+struct GeneratedCsr {
+  i64 n = 0;
+  std::vector<i64> rowPtr, col;
+  std::vector<double> val;
+  std::vector<double> coords;
+};
+GeneratedCsr generatePoisson(i64 nx, i64 ny, i64 nz);
+
+// MatrixMarket reader (public format spec; replaces fast_matrix_market).
+// Values are parsed directly into valueType (strtof for float32) so that
+// they are rounded once, as a reader templated on the value type does.
+Coo readMatrixMarket(const std::string& path, DType valueType);
+
+}  // namespace gr

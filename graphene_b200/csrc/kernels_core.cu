@@ -1,0 +1,433 @@
+// Device matrix set-up and the SpMV / residual / norm kernels.
+//
+// SpMV and residual follow CRSMatrix::spmv / CRSMatrix::residual
+// (matrix/details/crs/CRSMatrix.cpp:42-128): per row, the diagonal product
+// first, then the off-diagonal products added in tile-local column order,
+// each operation rounded in the intermediate type. The reference's halo
+// exchange (MatrixBase.cpp:36-109) becomes a direct read of the neighbour
+// tile's entry of x, which is the value the exchange would have copied.
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+
+#include "device.hpp"
+#include "devmath.cuh"
+
+namespace gr {
+
+namespace {
+std::atomic<i64> g_launches{0};
+}
+
+void noteLaunch(int count) { g_launches.fetch_add(count); }
+i64 launchCount() { return g_launches.load(); }
+
+void cudaCheck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    int code = (e == cudaErrorMemoryAllocation) ? GR_ENOMEM : GR_ECUDA;
+    fail(code, std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+  }
+}
+
+void DBuf::alloc(size_t bytes) {
+  release();
+  if (bytes == 0) bytes = 1;
+  cudaError_t e = cudaMalloc(&p_, bytes);
+  if (e != cudaSuccess) {
+    p_ = nullptr;
+    (void)cudaGetLastError();
+    fail(GR_ENOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " +
+                        cudaGetErrorString(e));
+  }
+  bytes_ = bytes;
+}
+
+void DBuf::release() {
+  if (p_) cudaFree(p_);
+  p_ = nullptr;
+  bytes_ = 0;
+}
+
+void uploadValues(DBuf& dst, const std::vector<double>& v, DType t) {
+  if (t == DType::F64) {
+    dst.upload(v);
+  } else if (t == DType::F32) {
+    std::vector<float> f(v.size());
+    parallelChunks(static_cast<i64>(v.size()), [&](i64 b, i64 e) {
+      for (i64 i = b; i < e; ++i) f[i] = static_cast<float>(v[i]);
+    });
+    dst.upload(f);
+  } else {
+    fail(GR_EUNSUPPORTED, "coefficient type must be float32 or float64");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Device matrix (HostMatrix::copyToTile, CRSHostMatrix.cpp:356-378).
+DeviceMatrix::DeviceMatrix(std::shared_ptr<HostMatrix> h) : host(std::move(h)) {
+  const HostMatrix& H = *host;
+  GR_CUDA(cudaGetDevice(&device));
+  GR_CUDA(cudaDeviceGetAttribute(&numSMs, cudaDevAttrMultiProcessorCount, device));
+  // A blocking stream: work on the legacy default stream (e.g. PyTorch's) and
+  // on this stream stays ordered.
+  GR_CUDA(cudaStreamCreateWithFlags(&ownStream, cudaStreamDefault));
+  stream = ownStream;
+  n = static_cast<i32>(H.n);
+  m = H.m;
+  P = H.P;
+  vt = H.valueType;
+
+  // Sliced ELLPACK, chunk height 32, rows in tile order.
+  sell.n = n;
+  sell.nChunks = (n + 31) / 32;
+  std::vector<i64> chunkLen(sell.nChunks, 0);
+  parallelChunks(sell.nChunks, [&](i64 b, i64 e) {
+    for (i64 c = b; c < e; ++c) {
+      i64 mx = 0;
+      for (i64 r = c * 32; r < std::min<i64>(n, c * 32 + 32); ++r)
+        mx = std::max(mx, H.rowPtr[r + 1] - H.rowPtr[r]);
+      chunkLen[c] = mx;
+    }
+  });
+  std::vector<i32> base(sell.nChunks + 1, 0);
+  i64 acc = 0;
+  for (i64 c = 0; c < sell.nChunks; ++c) {
+    base[c] = static_cast<i32>(acc);
+    acc += 32 * chunkLen[c];
+    if (acc >= (i64(1) << 31)) fail(GR_EUNSUPPORTED, "SELL storage exceeds 2^31 slots");
+  }
+  base[sell.nChunks] = static_cast<i32>(acc);
+  sell.slots = acc;
+  std::vector<i32> col(acc, -1);
+  std::vector<double> val(acc, 0.0);
+  parallelChunks(n, [&](i64 b, i64 e) {
+    for (i64 r = b; r < e; ++r) {
+      i64 c = r / 32, lane = r % 32;
+      for (i64 k = 0; k < H.rowPtr[r + 1] - H.rowPtr[r]; ++k) {
+        i64 s = base[c] + 32 * k + lane;
+        col[s] = H.colPerm[H.rowPtr[r] + k];
+        val[s] = H.offDiag[H.rowPtr[r] + k];
+      }
+    }
+  });
+  sell.base.upload(base);
+  sell.col.upload(col);
+  uploadValues(sell.val, val, vt);
+  uploadValues(diag, H.diag, vt);
+  std::vector<i32> ts(H.tileStart.begin(), H.tileStart.end());
+  tileStart.upload(ts);
+  iperm.upload(H.iperm);
+
+  redBlocks = numSMs * 8;
+  partials.alloc(sizeof(double) * redBlocks * 8);
+  counter.alloc(sizeof(unsigned) * 16);
+  GR_CUDA(cudaMemset(counter.get(), 0, sizeof(unsigned) * 16));
+  scalarOut.alloc(sizeof(double) * 8);
+  GR_CUDA(cudaDeviceSynchronize());
+}
+
+DeviceMatrix::~DeviceMatrix() {
+  if (ownStream) {
+    cudaStreamSynchronize(ownStream);
+    cudaStreamDestroy(ownStream);
+  }
+}
+
+int DeviceMatrix::spmvBlocks() const {
+  int need = (sell.nChunks + 7) / 8;
+  return std::max(1, std::min(need, redBlocks));
+}
+
+void DeviceMatrix::ensureLocalCrs() {
+  if (haveLocalCrs) return;
+  const HostMatrix& H = *host;
+  std::vector<i32> rp(H.rowPtr.begin(), H.rowPtr.end());
+  rowPtr.upload(rp);
+  colLocal.upload(H.colLocal);
+  uploadValues(offDiag, H.offDiag, vt);
+  haveLocalCrs = true;
+}
+
+// ---------------------------------------------------------------------------
+namespace dev {
+
+template <class MV>
+struct SellView {
+  int n, nChunks;
+  const int* __restrict__ base;
+  const int* __restrict__ col;
+  const MV* __restrict__ val;
+  const MV* __restrict__ diag;
+};
+
+// Loads x[i] converted to the accumulation type.
+template <class Acc, class XT>
+__device__ __forceinline__ Acc loadX(const XT* __restrict__ x, int i) {
+  return cvt<Acc>(__ldg(x + i));
+}
+
+// Row loop of one warp-chunk: returns the row's sum in Acc. The products
+// are formed as cvt<Acc>(a) * cvt<Acc>(x), added in stored order.
+template <class Acc, class MV, class XT>
+__device__ __forceinline__ Acc sellRowSum(const SellView<MV>& A, const XT* __restrict__ x, int row,
+                                          int s0, int K, int lane) {
+  Acc acc = mul(cvt<Acc>(__ldg(A.diag + row)), loadX<Acc>(x, row));
+  const int* cp = A.col + s0 + lane;
+  const MV* vp = A.val + s0 + lane;
+#pragma unroll 4
+  for (int k = 0; k < K; ++k) {
+    int c = __ldg(cp + 32 * k);
+    if (c >= 0) acc = add(acc, mul(cvt<Acc>(__ldg(vp + 32 * k)), loadX<Acc>(x, c)));
+  }
+  return acc;
+}
+
+// y = A x.
+template <class MV, class VT>
+__global__ void __launch_bounds__(256) spmvKernel(SellView<MV> A, const VT* __restrict__ x,
+                                                   VT* __restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < A.nChunks; c += nWarps) {
+    const int row = c * 32 + lane;
+    const int s0 = __ldg(A.base + c);
+    const int K = (__ldg(A.base + c + 1) - s0) >> 5;
+    if (row < A.n) y[row] = sellRowSum<VT>(A, x, row, s0, K, lane);
+  }
+}
+
+template <class T> __device__ __forceinline__ double toDouble(T v) { return static_cast<double>(v); }
+
+// Accumulates one stored residual entry into a norm partial.
+__device__ __forceinline__ double normStep(double acc, double r, int kind) {
+  if (kind == GR_NORM_L2) return __dadd_rn(acc, __dmul_rn(r, r));
+  if (kind == GR_NORM_LINF) return fmax(acc, r);
+  return __dadd_rn(acc, r);  // L1: signed sum (dsl/tensor/Tensor.cpp:428-430)
+}
+
+__device__ __forceinline__ int normOp(int kind) { return kind == GR_NORM_LINF ? RED_MAX : RED_SUM; }
+
+__device__ __forceinline__ double normFinish(double total, int kind) {
+  return kind == GR_NORM_L2 ? sqrt(total) : total;
+}
+
+// Residual with an IEEE intermediate type I (float or double):
+// r = (b - (d x + sum a x)) computed in I, stored as RT.
+template <class MV, class XT, class BT, class RT, class I>
+__global__ void __launch_bounds__(256) residualKernel(SellView<MV> A, const XT* __restrict__ x,
+                                                       const BT* __restrict__ b,
+                                                       RT* __restrict__ r, int normKind,
+                                                       double* __restrict__ normOut,
+                                                       double* partials, unsigned* counter) {
+  __shared__ double smem[32];
+  const int lane = threadIdx.x & 31;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  double part = redIdentity(normOp(normKind));
+  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < A.nChunks; c += nWarps) {
+    const int row = c * 32 + lane;
+    const int s0 = __ldg(A.base + c);
+    const int K = (__ldg(A.base + c + 1) - s0) >> 5;
+    if (row < A.n) {
+      I sum = sellRowSum<I>(A, x, row, s0, K, lane);
+      RT res = cvt<RT>(sub(cvt<I>(__ldg(b + row)), sum));
+      r[row] = res;
+      if (normKind >= 0) part = normStep(part, toDouble(res), normKind);
+    }
+  }
+  if (normKind < 0) return;
+  double v[1] = {part};
+  const int ops[1] = {normOp(normKind)};
+  double out[1];
+  blockReduce<1>(v, ops, smem);
+  if (gridReduce<1>(v, ops, partials, counter, smem, out) && threadIdx.x == 0)
+    *normOut = normFinish(out[0], normKind);
+}
+
+// Residual with a double-word intermediate: x is double-word (two floats
+// per entry) or float, the matrix float, b and r float.
+template <bool XDW>
+__global__ void __launch_bounds__(256) residualDwKernel(SellView<float> A, const float* __restrict__ x,
+                                                         const float* __restrict__ b,
+                                                         float* __restrict__ r, int normKind,
+                                                         double* __restrict__ normOut,
+                                                         double* partials, unsigned* counter) {
+  __shared__ double smem[32];
+  const int lane = threadIdx.x & 31;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  double part = redIdentity(normOp(normKind));
+  auto ld = [&](int i) -> dw {
+    if (XDW) {
+      float2 v = __ldg(reinterpret_cast<const float2*>(x) + i);
+      return {v.x, v.y};
+    }
+    return {__ldg(x + i), 0.0f};
+  };
+  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < A.nChunks; c += nWarps) {
+    const int row = c * 32 + lane;
+    const int s0 = __ldg(A.base + c);
+    const int K = (__ldg(A.base + c + 1) - s0) >> 5;
+    if (row < A.n) {
+      dw sum = dwTimesFp(ld(row), __ldg(A.diag + row));
+      const int* cp = A.col + s0 + lane;
+      const float* vp = A.val + s0 + lane;
+      for (int k = 0; k < K; ++k) {
+        int cc = __ldg(cp + 32 * k);
+        if (cc >= 0) sum = dwPlusDw(sum, dwTimesFp(ld(cc), __ldg(vp + 32 * k)));
+      }
+      dw res = dwPlusDw(dw{__ldg(b + row), 0.0f}, dwNeg(sum));
+      float rv = dwToFloat(res);
+      r[row] = rv;
+      if (normKind >= 0) part = normStep(part, static_cast<double>(rv), normKind);
+    }
+  }
+  if (normKind < 0) return;
+  double v[1] = {part};
+  const int ops[1] = {normOp(normKind)};
+  double out[1];
+  blockReduce<1>(v, ops, smem);
+  if (gridReduce<1>(v, ops, partials, counter, smem, out) && threadIdx.x == 0)
+    *normOut = normFinish(out[0], normKind);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) normKernel(const T* __restrict__ x, int n, int kind,
+                                                   double* __restrict__ out, double* partials,
+                                                   unsigned* counter) {
+  __shared__ double smem[32];
+  double part = redIdentity(normOp(kind));
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    part = normStep(part, toDouble(__ldg(x + i)), kind);
+  double v[1] = {part};
+  const int ops[1] = {normOp(kind)};
+  double res[1];
+  blockReduce<1>(v, ops, smem);
+  if (gridReduce<1>(v, ops, partials, counter, smem, res) && threadIdx.x == 0)
+    *out = normFinish(res[0], kind);
+}
+
+template <class T>
+__global__ void permuteKernel(const T* __restrict__ src, T* __restrict__ dst,
+                              const int* __restrict__ iperm, int n, bool toTile) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    int g = __ldg(iperm + p);
+    if (toTile) dst[p] = src[g];
+    else dst[g] = src[p];
+  }
+}
+
+}  // namespace dev
+
+// ---------------------------------------------------------------------------
+namespace {
+
+template <class MV>
+dev::SellView<MV> sellView(const DeviceMatrix& A) {
+  return dev::SellView<MV>{A.n, A.sell.nChunks, A.sell.base.as<int>(), A.sell.col.as<int>(),
+                           A.sell.val.as<MV>(), A.diag.as<MV>()};
+}
+
+void checkLaunch(const char* name) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) fail(GR_ECUDA, std::string("launch of ") + name + " failed: " + cudaGetErrorString(e));
+  noteLaunch();
+}
+
+}  // namespace
+
+void launchSpmv(DeviceMatrix& A, const void* x, void* y, DType t, cudaStream_t s) {
+  const int blocks = A.spmvBlocks();
+  if (A.vt == DType::F32 && t == DType::F32) {
+    dev::spmvKernel<float, float><<<blocks, 256, 0, s>>>(sellView<float>(A), static_cast<const float*>(x),
+                                                         static_cast<float*>(y));
+  } else if (A.vt == DType::F32 && t == DType::F64) {
+    dev::spmvKernel<float, double><<<blocks, 256, 0, s>>>(sellView<float>(A), static_cast<const double*>(x),
+                                                          static_cast<double*>(y));
+  } else if (A.vt == DType::F64 && t == DType::F64) {
+    dev::spmvKernel<double, double><<<blocks, 256, 0, s>>>(sellView<double>(A), static_cast<const double*>(x),
+                                                           static_cast<double*>(y));
+  } else {
+    fail(GR_EUNSUPPORTED, std::string("spmv with ") + dtypeName(A.vt) + " coefficients and " +
+                              dtypeName(t) + " vectors");
+  }
+  checkLaunch("spmv");
+}
+
+void launchResidual(DeviceMatrix& A, const void* x, DType xt, const void* b, DType bt, void* r,
+                    DType rt, DType inter, int normKind, double* normOut, cudaStream_t s) {
+  const int blocks = A.spmvBlocks();
+  double* part = A.partials.as<double>();
+  unsigned* cnt = A.counter.as<unsigned>();
+  auto bad = [&]() {
+    fail(GR_EUNSUPPORTED, std::string("residual with x=") + dtypeName(xt) + " b=" + dtypeName(bt) +
+                              " r=" + dtypeName(rt) + " intermediate=" + dtypeName(inter) +
+                              " coefficients=" + dtypeName(A.vt));
+  };
+  if (inter == DType::DW) {
+    if (A.vt != DType::F32 || bt != DType::F32 || rt != DType::F32) bad();
+    if (xt == DType::DW)
+      dev::residualDwKernel<true><<<blocks, 256, 0, s>>>(sellView<float>(A), static_cast<const float*>(x),
+                                                         static_cast<const float*>(b), static_cast<float*>(r),
+                                                         normKind, normOut, part, cnt);
+    else if (xt == DType::F32)
+      dev::residualDwKernel<false><<<blocks, 256, 0, s>>>(sellView<float>(A), static_cast<const float*>(x),
+                                                          static_cast<const float*>(b), static_cast<float*>(r),
+                                                          normKind, normOut, part, cnt);
+    else bad();
+    checkLaunch("residual_dw");
+    return;
+  }
+  if (xt == DType::DW) bad();
+#define GR_RES(MV, XT, BT, RT, IT)                                                                 \
+  dev::residualKernel<MV, XT, BT, RT, IT><<<blocks, 256, 0, s>>>(                                 \
+      sellView<MV>(A), static_cast<const XT*>(x), static_cast<const BT*>(b), static_cast<RT*>(r), \
+      normKind, normOut, part, cnt)
+  const bool mf = A.vt == DType::F32;
+  const int key = (xt == DType::F64) * 8 + (bt == DType::F64) * 4 + (rt == DType::F64) * 2 +
+                  (inter == DType::F64);
+  if (mf) {
+    switch (key) {
+      case 0: GR_RES(float, float, float, float, float); break;
+      case 1: GR_RES(float, float, float, float, double); break;
+      case 7: GR_RES(float, float, double, double, double); break;
+      case 9: GR_RES(float, double, float, float, double); break;
+      case 11: GR_RES(float, double, float, double, double); break;
+      case 15: GR_RES(float, double, double, double, double); break;
+      default: bad();
+    }
+  } else {
+    switch (key) {
+      case 9: GR_RES(double, double, float, float, double); break;
+      case 11: GR_RES(double, double, float, double, double); break;
+      case 15: GR_RES(double, double, double, double, double); break;
+      default: bad();
+    }
+  }
+#undef GR_RES
+  checkLaunch("residual");
+}
+
+void launchNorm(DeviceMatrix& A, const void* x, DType t, int normKind, double* out, cudaStream_t s) {
+  const int blocks = std::max(1, std::min(A.redBlocks, (A.n + 255) / 256));
+  if (t == DType::F32)
+    dev::normKernel<float><<<blocks, 256, 0, s>>>(static_cast<const float*>(x), A.n, normKind, out,
+                                                  A.partials.as<double>(), A.counter.as<unsigned>());
+  else if (t == DType::F64)
+    dev::normKernel<double><<<blocks, 256, 0, s>>>(static_cast<const double*>(x), A.n, normKind, out,
+                                                   A.partials.as<double>(), A.counter.as<unsigned>());
+  else
+    fail(GR_EUNSUPPORTED, "norm of a twofloat32 vector");
+  checkLaunch("norm");
+}
+
+void launchPermute(DeviceMatrix& A, const void* src, void* dst, DType t, bool toTile, cudaStream_t s) {
+  const int blocks = std::max(1, std::min(A.redBlocks, (A.n + 255) / 256));
+  if (dtypeSize(t) == 4)
+    dev::permuteKernel<float><<<blocks, 256, 0, s>>>(static_cast<const float*>(src), static_cast<float*>(dst),
+                                                     A.iperm.as<int>(), A.n, toTile);
+  else
+    dev::permuteKernel<double><<<blocks, 256, 0, s>>>(static_cast<const double*>(src), static_cast<double*>(dst),
+                                                      A.iperm.as<int>(), A.n, toTile);
+  checkLaunch("permute");
+}
+
+}  // namespace gr

@@ -1,0 +1,25 @@
+// Solver tree: configuration parsing and the solver drivers
+// (matrix/solver/ of the reference).
+#pragma once
+
+#include <memory>
+#include <string>
+
+#include "device.hpp"
+
+namespace gr {
+
+class SolverTree {
+ public:
+  virtual ~SolverTree() = default;
+  // Configuration::fromJSON + Solver::createSolver.
+  static std::unique_ptr<SolverTree> create(DeviceMatrix& A, const std::string& json);
+  // Solver::solve(x, b) with device vectors in tile order.
+  virtual gr_stats solve(void* x, DType xt, const void* b, DType bt) = 0;
+  // Host vectors in natural order, copies included.
+  virtual gr_stats solveHost(void* x, DType xt, const void* b, DType bt) = 0;
+  virtual void copyPhi(void* out, DType t) = 0;
+  virtual std::string name() const = 0;
+};
+
+}  // namespace gr

@@ -1,0 +1,249 @@
+/*
+ * graphene_gpu.h -- C ABI of the B200 sparse-solver hot path.
+ *
+ * This is the drop-in boundary for Graphene's matrix / solver surface
+ * (libgraphene/matrix). Every entry point below names the reference
+ * interface it replaces. The reference is a C++ graph-building API whose
+ * calls record work that runs later on the IPU; here every call executes
+ * immediately on the GPU (or on the host for matrix construction).
+ *
+ * Conventions
+ *  - Every function returns an int status (GR_OK == 0). On failure
+ *    gr_last_error() returns a thread-local message. No C++ exception
+ *    crosses this boundary.
+ *  - Handles are opaque and own their memory; release them with the
+ *    matching *_destroy function. A device matrix keeps its host matrix
+ *    alive (the reference's MatrixBase holds a reference to the host layout,
+ *    matrix/details/MatrixBase.hpp:38).
+ *  - Device vectors are in "tile order": the concatenation over tiles of
+ *    each tile's interior rows followed by its separator rows, i.e. the
+ *    reference's decomposed vector layout without halo cells
+ *    (matrix/host/DistributedTileLayout.cpp:156-183). Halo cells are not
+ *    stored: a kernel reads a neighbour tile's value directly from HBM,
+ *    which is what the reference's halo exchange copies
+ *    (matrix/details/MatrixBase.cpp:36-109).
+ *  - Host vectors passed to gr_vector_decompose / gr_vector_compose are in
+ *    natural (global row) order.
+ *  - All device work of a matrix and of the solvers built on it runs on
+ *    that matrix's CUDA stream (gr_matrix_set_stream, default: a stream
+ *    owned by the matrix).
+ */
+#ifndef GRAPHENE_GPU_H
+#define GRAPHENE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------- */
+#define GR_OK 0
+#define GR_EINVAL 1       /* invalid argument (reference: std::invalid_argument) */
+#define GR_ENOMEM 2       /* host or device allocation failed */
+#define GR_EPARSE 3       /* malformed JSON or MatrixMarket input */
+#define GR_ENOTCONV 4     /* solver stopped without converging */
+#define GR_EBREAKDOWN 5   /* singular rho / omega (SolverStats::singular) */
+#define GR_ETIMEOUT 6     /* a device-side wait ran out of its budget */
+#define GR_ECUDA 7        /* CUDA runtime error */
+#define GR_EUNSUPPORTED 8 /* combination not supported (reference: runtime_error) */
+#define GR_EIO 9          /* file could not be opened */
+#define GR_ENONFINITE 10  /* NaN or Inf detected in a residual norm */
+
+/* ---- enumerations ---------------------------------------------------- */
+/* Element types; names follow common/Type.hpp:125-214 (parseType accepts
+ * "float32", "float64", "twofloat32"). TWOFLOAT32 is a pair {h, l} of
+ * floats stored as two consecutive floats per element. */
+typedef enum { GR_FLOAT32 = 0, GR_FLOAT64 = 1, GR_TWOFLOAT32 = 2 } gr_dtype;
+
+/* matrix/MatrixFormat.hpp:22 */
+typedef enum { GR_FORMAT_CRS = 0, GR_FORMAT_LDU = 1 } gr_format;
+
+/* matrix/Norm.hpp (VectorNorm). L1 is the signed sum and LINF the signed
+ * maximum, as in dsl/tensor/Tensor.cpp:425-439. */
+typedef enum { GR_NORM_L1 = 0, GR_NORM_L2 = 1, GR_NORM_LINF = 2, GR_NORM_NONE = 3 } gr_norm;
+
+/* Row partitioners that produce rowToTile. The reference uses METIS
+ * (matrix/host/details/crs/CRSHostMatrix.cpp:139-271), which is not
+ * available; these are this library's own deterministic partitioners. */
+typedef enum {
+  GR_PART_AUTO = 0,       /* RCB when grid coordinates exist, else BFS bisection */
+  GR_PART_CONTIGUOUS = 1, /* equal-weight blocks in natural row order */
+  GR_PART_RCB = 2,        /* recursive coordinate bisection (generated grids) */
+  GR_PART_BFS = 3,        /* recursive BFS-level-structure graph bisection */
+  GR_PART_EXPLICIT = 4    /* caller-supplied rowToTile */
+} gr_partitioner;
+
+typedef struct gr_host_matrix gr_host_matrix;
+typedef struct gr_matrix gr_matrix;
+typedef struct gr_solver gr_solver;
+
+/* SolverStats (matrix/solver/SolverStats.hpp:29-69). Residual norms are
+ * accumulated in FP64 on the device. */
+typedef struct {
+  double initial_residual;
+  double final_residual;
+  double b_norm;        /* 0 unless relTolerance > 0 */
+  int32_t iterations;
+  int32_t converged;
+  int32_t singular;
+  int32_t status;       /* GR_OK, GR_ETIMEOUT, GR_ENONFINITE, ... */
+  int32_t inner_iterations; /* MPIR / restarter: total iterations of the inner solver */
+  int32_t reserved;
+  double solve_ms;      /* device time of the solve (CUDA events) */
+} gr_stats;
+
+typedef struct {
+  int64_t num_rows;        /* n */
+  int64_t num_off_diag;    /* m: stored off-diagonal entries */
+  int64_t num_tiles;       /* tiles after empty-tile removal */
+  int64_t num_halo_total;  /* sum over tiles of halo cells */
+  int64_t max_tile_rows;   /* largest tile (interior + separator) */
+  int64_t num_lower_levels_total;
+  int64_t num_upper_levels_total;
+  int32_t value_type;      /* gr_dtype of the stored coefficients */
+  int32_t format;          /* gr_format */
+  int32_t multicolor_recommended; /* CRSHostMatrix.cpp:648-669 */
+  int32_t reserved;
+} gr_matrix_info;
+
+/* ---- library ---------------------------------------------------------- */
+const char* gr_last_error(void);
+int gr_version(void);
+/* Number of kernel launches issued by this library since load (all
+ * devices). Used to count launches inside a timed region. */
+int64_t gr_launch_count(void);
+
+/* ---- host matrices (matrix/host/HostMatrix.hpp:31-96) ---------------- */
+
+/* Replaces HostMatrix(MatrixFormat::CRS, TripletMatrix, numTiles)
+ * (matrix/host/HostMatrix.cpp:31-44): sorts the triplets by (row, col),
+ * splits off the diagonal (CRSHostMatrix.cpp:88-137), partitions the rows,
+ * builds the interior/separator/halo tile layout and the tile-local CRS
+ * (CRSHostMatrix.cpp:273-525) and the per-tile level sets
+ * (CRSHostMatrix.cpp:527-675). Values are rounded to value_type.
+ * Duplicate (row, col) entries are rejected with GR_EINVAL.
+ * coords (nullable) gives 3 doubles per row for GR_PART_RCB.
+ * row_to_tile is read for GR_PART_EXPLICIT only. */
+int gr_host_matrix_from_coo(int64_t num_rows, int64_t nnz, const int64_t* rows,
+                            const int64_t* cols, const double* vals,
+                            int64_t num_tiles, gr_partitioner partitioner,
+                            const int32_t* row_to_tile, const double* coords,
+                            gr_dtype value_type, gr_host_matrix** out);
+
+/* Replaces generate3DPoissonMatrix(type, nx, ny, nz, numTiles)
+ * (matrix/host/HostMatrix.hpp:94-96, details/Poisson.cpp:26-69). */
+int gr_host_matrix_poisson(int64_t nx, int64_t ny, int64_t nz, int64_t num_tiles,
+                           gr_partitioner partitioner, gr_dtype value_type,
+                           gr_host_matrix** out);
+
+/* Replaces loadMatrixFromFile(type, path, numTiles)
+ * (matrix/host/HostMatrix.hpp:88-91, details/MatrixMarket.cpp:31-65). */
+int gr_host_matrix_load_mm(const char* path, int64_t num_tiles, gr_partitioner partitioner,
+                           gr_dtype value_type, gr_host_matrix** out);
+
+void gr_host_matrix_destroy(gr_host_matrix* h);
+
+int gr_host_matrix_get_info(const gr_host_matrix* h, gr_matrix_info* out);
+
+/* Partitioning::rowToTile after empty-tile removal (CRSHostMatrix.cpp:235-270). */
+int gr_host_matrix_row_to_tile(const gr_host_matrix* h, int32_t* row_to_tile);
+
+/* Per tile: {numInteriorRows, numSeperatorRows, numHaloRows}
+ * (DistributedTileLayout.hpp:309-328). out has 3*num_tiles entries. */
+int gr_host_matrix_tile_sizes(const gr_host_matrix* h, int64_t* out);
+
+/* TilePartition::localToGlobalRow of every tile, concatenated, halo cells
+ * included (DistributedTileLayout.cpp:91-126). out has n + num_halo_total
+ * entries. */
+int gr_host_matrix_local_to_global(const gr_host_matrix* h, int64_t* out);
+
+/* The tile-local CRS of every tile, concatenated in tile order
+ * (CRSHostMatrix.cpp:379-432, 466-525): row_ptr has n + num_tiles entries
+ * (each tile's local rowPtr, n_t + 1 entries, starting at 0), col_ind has m
+ * entries of tile-local column ids (halo ids >= n_t), off_diag has m values,
+ * diag has n values (tile order). Any output pointer may be NULL. */
+int gr_host_matrix_local_crs(const gr_host_matrix* h, int64_t* row_ptr, int32_t* col_ind,
+                             double* off_diag, double* diag);
+
+/* Per-row level ("colour") of the lower-triangular dependency DAG in tile
+ * order (CRSHostMatrix.cpp:527-614) and the upper-triangular levels used by
+ * the backward sweep. Either pointer may be NULL. */
+int gr_host_matrix_levels(const gr_host_matrix* h, int32_t* lower_level, int32_t* upper_level);
+
+/* Natural order <-> tile order (DistributedTileLayout::decomposeVector,
+ * DistributedTileLayout.cpp:156-183, without halo). Host buffers. */
+int gr_host_matrix_decompose_vector(const gr_host_matrix* h, const void* natural,
+                                    void* tile_ordered, gr_dtype t);
+int gr_host_matrix_compose_vector(const gr_host_matrix* h, const void* tile_ordered,
+                                  void* natural, gr_dtype t);
+
+/* ---- device matrices (matrix/Matrix.hpp:29-131) ---------------------- */
+
+/* Replaces HostMatrix::copyToTile() (matrix/host/HostMatrix.hpp:53,
+ * CRSHostMatrix.cpp:356-378): uploads the coefficients and addressing to the
+ * current CUDA device. The device matrix holds a reference on the host
+ * matrix. */
+int gr_matrix_create(gr_host_matrix* h, gr_matrix** out);
+void gr_matrix_destroy(gr_matrix* A);
+/* Use an external cudaStream_t (NULL restores the matrix's own stream). */
+int gr_matrix_set_stream(gr_matrix* A, void* cuda_stream);
+int gr_matrix_get_info(const gr_matrix* A, gr_matrix_info* out);
+
+/* Replaces Matrix::operator*(Tensor& x) (matrix/Matrix.hpp:95-97,
+ * details/crs/CRSMatrix.cpp:42-83): y = A x. x and y are device pointers in
+ * tile order; xt == yt (FLOAT32 or FLOAT64). */
+int gr_spmv(gr_matrix* A, const void* x, void* y, gr_dtype t);
+
+/* Replaces Matrix::residual(x, b, destType, intermediateType)
+ * (matrix/Matrix.hpp:86-92, CRSMatrix.cpp:85-128): r = b - A x computed in
+ * inter_t and rounded to r_t. x_t may be FLOAT32, FLOAT64 or TWOFLOAT32,
+ * b is FLOAT32 or FLOAT64. */
+int gr_residual(gr_matrix* A, const void* x, gr_dtype x_t, const void* b, gr_dtype b_t,
+                void* r, gr_dtype r_t, gr_dtype inter_t);
+
+/* Replaces Matrix::vectorNorm(norm, x) (matrix/Matrix.hpp:120-122,
+ * details/MatrixBase.cpp:149-152). Accumulates in FP64. */
+int gr_vector_norm(gr_matrix* A, gr_norm norm, const void* x, gr_dtype t, double* out);
+
+/* Natural order <-> tile order on the device. */
+int gr_decompose_vector(gr_matrix* A, const void* natural, void* tile_ordered, gr_dtype t);
+int gr_compose_vector(gr_matrix* A, const void* tile_ordered, void* natural, gr_dtype t);
+
+/* ---- solvers (matrix/solver/) ---------------------------------------- */
+
+/* Replaces Configuration::fromJSON + Solver::createSolver
+ * (matrix/solver/Configuration.cpp:103-136, Solver.cpp:32-56). json is the
+ * reference's solver tree ("type": PBiCGStab | ILU | GaussSeidel |
+ * IterativeRefinement | restarter, nested "preconditioner" /
+ * "innerSolver"); comments are allowed. Construction performs the ILU
+ * factorisation as the reference's ilu::Solver constructor does
+ * (ilu/Solver.cpp:44-51). */
+int gr_solver_create(gr_matrix* A, const char* json, gr_solver** out);
+void gr_solver_destroy(gr_solver* s);
+
+/* Replaces Solver::solve(x, b) (matrix/solver/Solver.hpp:41) and
+ * Matrix::solve (matrix/Matrix.cpp:26-30). x (in/out) and b are device
+ * pointers in tile order of type x_t / b_t (FLOAT32 or FLOAT64; b_t must
+ * equal x_t). Blocks until the solve has finished. */
+int gr_solve(gr_solver* s, void* x, gr_dtype x_t, const void* b, gr_dtype b_t, gr_stats* stats);
+
+/* Same as gr_solve with host buffers in natural order: copies b in, x in
+ * and x out (the end-to-end path). */
+int gr_solve_host(gr_solver* s, void* x, gr_dtype x_t, const void* b, gr_dtype b_t,
+                  gr_stats* stats);
+
+/* After an IterativeRefinement solve: the extended-precision solution phi
+ * (iterative-refinement/Solver.cpp:84,103), copied to a device buffer of
+ * type t in tile order. The reference returns only (float)phi. */
+int gr_solver_phi(gr_solver* s, void* out, gr_dtype t);
+
+/* Name of the solver tree, e.g. "IterativeRefinement(PBiCGStab(ILU(0)))". */
+int gr_solver_name(const gr_solver* s, char* buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRAPHENE_GPU_H */
