@@ -119,8 +119,11 @@ class HostMatrix:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            _lib.lib().gr_host_matrix_destroy(h)
+        if h and _lib is not None:
+            try:
+                _lib.lib().gr_host_matrix_destroy(h)
+            except Exception:
+                pass
             self._h = None
 
     # -- constructors ------------------------------------------------------
@@ -224,10 +227,19 @@ def loadMatrixFromFile(valueType: int, path: str, numTiles: int,
 
 
 class Configuration:
-    """Solver configuration tree (matrix/solver/Configuration.hpp:40)."""
+    """Solver configuration tree (matrix/solver/Configuration.hpp:40).
+
+    Parsed and validated by the native library at construction; the
+    reference's schema is accepted (comments allowed, unknown keys ignored
+    and listed in ``unknownKeys``)."""
 
     def __init__(self, text: str):
         self.text = text
+        name = C.create_string_buffer(512)
+        unk = C.create_string_buffer(1024)
+        check(_lib.lib().gr_config_parse(text.encode(), name, 512, unk, 1024))
+        self.solverName = name.value.decode()
+        self.unknownKeys = [k for k in unk.value.decode().split(",") if k]
 
     @staticmethod
     def fromJSON(cfg: Union[str, dict]) -> "Configuration":
@@ -250,8 +262,11 @@ class Solver:
 
     def __del__(self):
         s = getattr(self, "_s", None)
-        if s:
-            _lib.lib().gr_solver_destroy(s)
+        if s and _lib is not None:
+            try:
+                _lib.lib().gr_solver_destroy(s)
+            except Exception:
+                pass
             self._s = None
 
     def name(self) -> str:
@@ -293,8 +308,11 @@ class Matrix:
 
     def __del__(self):
         m = getattr(self, "_m", None)
-        if m:
-            _lib.lib().gr_matrix_destroy(m)
+        if m and _lib is not None:
+            try:
+                _lib.lib().gr_matrix_destroy(m)
+            except Exception:
+                pass
             self._m = None
 
     @property

@@ -95,6 +95,7 @@ SIGNATURES = {
     "gr_solve_host": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, P(Stats)]),
     "gr_solver_phi": (C.c_int, [vp, vp, C.c_int]),
     "gr_solver_name": (C.c_int, [vp, C.c_char_p, C.c_size_t]),
+    "gr_config_parse": (C.c_int, [C.c_char_p, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t]),
 }
 
 _lib = None

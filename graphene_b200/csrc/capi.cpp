@@ -5,6 +5,7 @@
 
 #include "device.hpp"
 #include "host_matrix.hpp"
+#include "config.hpp"
 #include "solvers.hpp"
 
 struct gr_host_matrix {
@@ -329,6 +330,28 @@ int gr_solver_name(const gr_solver* s, char* buf, size_t len) {
     if (len == 0) gr::fail(GR_EINVAL, "buffer length is 0");
     std::strncpy(buf, nm.c_str(), len - 1);
     buf[len - 1] = '\0';
+  });
+}
+
+int gr_config_parse(const char* json, char* name, size_t name_len, char* unknown_keys, size_t unknown_len) {
+  return guarded([&] {
+    need(json, "json");
+    auto cfg = gr::SolverConfig::fromText(json);
+    auto copy = [](const std::string& v, char* buf, size_t len) {
+      if (!buf || len == 0) return;
+      std::strncpy(buf, v.c_str(), len - 1);
+      buf[len - 1] = '\0';
+    };
+    copy(cfg->solverName(), name, name_len);
+    std::string unk;
+    for (const gr::SolverConfig* c = cfg.get(); c;) {
+      for (auto& k : c->unknownKeys) unk += (unk.empty() ? "" : ",") + k;
+      if (c->preconditioner) {
+        for (auto& k : c->preconditioner->unknownKeys) unk += (unk.empty() ? "" : ",") + k;
+      }
+      c = c->innerSolver.get();
+    }
+    copy(unk, unknown_keys, unknown_len);
   });
 }
 

@@ -1,0 +1,61 @@
+// Solver configuration tree, parsed from the reference's JSON schema
+// (matrix/solver/Configuration.cpp:103-136 and the per-solver
+// Configuration.cpp files). JSON comments are accepted, as
+// nlohmann::json::parse(..., allow_comments=true) does in the reference's
+// benchmark (applications/benchmark/benchmark.cpp:117-118). Unknown keys are
+// ignored like the reference does; they are collected in `unknownKeys` so the
+// caller can report them.
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.hpp"
+
+namespace gr {
+
+// A parsed JSON value. Scalars keep their source text, like a property tree.
+struct Json {
+  enum Kind { Null, Bool, Number, String, Object, Array } kind = Null;
+  std::string text;
+  std::vector<std::pair<std::string, Json>> members;
+  std::vector<Json> items;
+  const Json* find(const std::string& key) const;
+  static Json parse(const std::string& src);
+};
+
+enum class MultiColorMode { Off, On, Auto };  // solver/Configuration.hpp:27
+
+struct SolverConfig {
+  std::string type;  // PBiCGStab | ILU | GaussSeidel | IterativeRefinement | restarter
+  // SolverStats tolerances (pbicgstab/Configuration.hpp:14-23 and siblings).
+  float absTolerance = 0, relTolerance = 0, relResidual = 0;
+  int maxIterations = 2147483647, minIterations = 0;
+  bool printPerformanceAfterSolve = false, printPerformanceEachIteration = false;
+  bool verbose = false;
+  int norm = GR_NORM_L2;
+  int workingType = -1;  // -1: the type of x
+  // ILU (ilu/Configuration.hpp:13-15)
+  MultiColorMode solveMulticolor = MultiColorMode::Auto;
+  MultiColorMode factorizeMulticolor = MultiColorMode::Auto;
+  bool diagonalBased = false;
+  // GaussSeidel (gauss-seidel/Configuration.hpp:19-21)
+  int numSweeps = 1, numFixedIterations = 0;
+  // Extension: "seed": "b" (default, the codelet specification
+  // codelet/ipu/matrix/solvers/gauss-seidel.cpp:44) or "diag" (the CodeDSL
+  // version, gauss-seidel/Solver.cpp:74).
+  bool gsSeedB = true;
+  // IterativeRefinement (iterative-refinement/Configuration.hpp:23-25)
+  int extendedPrecisionType = -1;  // -1: the type of x
+  // restarter (restarter/Configuration.hpp:14)
+  int maxRestarts = 1;
+  std::unique_ptr<SolverConfig> preconditioner, innerSolver;
+  std::vector<std::string> unknownKeys;
+
+  std::string solverName() const;
+  static std::unique_ptr<SolverConfig> fromJson(const Json& j);
+  static std::unique_ptr<SolverConfig> fromText(const std::string& text);
+};
+
+}  // namespace gr

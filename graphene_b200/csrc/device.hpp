@@ -16,9 +16,15 @@ namespace gr {
 void cudaCheck(cudaError_t e, const char* what);
 #define GR_CUDA(call) ::gr::cudaCheck((call), #call)
 
-// Counts every kernel launch made through this library.
+// Counts every kernel launch made through this library. Launches recorded
+// while a CUDA graph is being captured are not counted; graph replays add
+// the graph's kernel count instead.
 void noteLaunch(int count = 1);
 i64 launchCount();
+void setCapturing(bool on);
+bool capturing();
+// Kernels recorded while capturing (per thread).
+i64 capturedCount();
 
 // Owning device allocation.
 class DBuf {
@@ -60,8 +66,9 @@ struct SellMatrix {
   i32 n = 0, nChunks = 0;
   i64 slots = 0;
   DBuf base;  // i32[nChunks + 1]
-  DBuf col;   // i32[slots], tile-order column
-  DBuf val;   // value type [slots]
+  DBuf ent;   // float coefficients: int2 {tile-order column, value bits} [slots]
+  DBuf col;   // double coefficients: i32 tile-order column [slots]
+  DBuf val;   // double coefficients: values [slots]
 };
 
 // Level schedule of one sweep over all tiles: for each tile its levels, for
@@ -78,7 +85,6 @@ struct LevelSchedule {
   DBuf rows;          // i32 tile-order row per level row
   DBuf col;           // i32 tile-order column per slot, -1 = padding
   DBuf src;           // i32 index into the local CRS values per slot, -1 = padding
-  DBuf val;           // packed values per slot (value type)
 };
 
 // Kinds of entries a schedule keeps per row.

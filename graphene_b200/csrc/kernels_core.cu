@@ -12,15 +12,24 @@
 
 #include "device.hpp"
 #include "devmath.cuh"
+#include "sell.cuh"
 
 namespace gr {
 
 namespace {
 std::atomic<i64> g_launches{0};
+thread_local bool g_capturing = false;
+thread_local i64 g_captured = 0;
 }
 
-void noteLaunch(int count) { g_launches.fetch_add(count); }
+void noteLaunch(int count) {
+  if (g_capturing) g_captured += count;
+  else g_launches.fetch_add(count);
+}
+i64 capturedCount() { return g_captured; }
 i64 launchCount() { return g_launches.load(); }
+void setCapturing(bool on) { g_capturing = on; }
+bool capturing() { return g_capturing; }
 
 void cudaCheck(cudaError_t e, const char* what) {
   if (e != cudaSuccess) {
@@ -111,8 +120,21 @@ DeviceMatrix::DeviceMatrix(std::shared_ptr<HostMatrix> h) : host(std::move(h)) {
     }
   });
   sell.base.upload(base);
-  sell.col.upload(col);
-  uploadValues(sell.val, val, vt);
+  if (vt == DType::F32) {
+    std::vector<int2> ent(acc);
+    parallelChunks(acc, [&](i64 b, i64 e) {
+      for (i64 s = b; s < e; ++s) {
+        float f = static_cast<float>(val[s]);
+        int bits;
+        std::memcpy(&bits, &f, sizeof(bits));
+        ent[s] = make_int2(col[s], bits);
+      }
+    });
+    sell.ent.upload(ent);
+  } else {
+    sell.col.upload(col);
+    uploadValues(sell.val, val, vt);
+  }
   uploadValues(diag, H.diag, vt);
   std::vector<i32> ts(H.tileStart.begin(), H.tileStart.end());
   tileStart.upload(ts);
@@ -151,37 +173,6 @@ void DeviceMatrix::ensureLocalCrs() {
 // ---------------------------------------------------------------------------
 namespace dev {
 
-template <class MV>
-struct SellView {
-  int n, nChunks;
-  const int* __restrict__ base;
-  const int* __restrict__ col;
-  const MV* __restrict__ val;
-  const MV* __restrict__ diag;
-};
-
-// Loads x[i] converted to the accumulation type.
-template <class Acc, class XT>
-__device__ __forceinline__ Acc loadX(const XT* __restrict__ x, int i) {
-  return cvt<Acc>(__ldg(x + i));
-}
-
-// Row loop of one warp-chunk: returns the row's sum in Acc. The products
-// are formed as cvt<Acc>(a) * cvt<Acc>(x), added in stored order.
-template <class Acc, class MV, class XT>
-__device__ __forceinline__ Acc sellRowSum(const SellView<MV>& A, const XT* __restrict__ x, int row,
-                                          int s0, int K, int lane) {
-  Acc acc = mul(cvt<Acc>(__ldg(A.diag + row)), loadX<Acc>(x, row));
-  const int* cp = A.col + s0 + lane;
-  const MV* vp = A.val + s0 + lane;
-#pragma unroll 4
-  for (int k = 0; k < K; ++k) {
-    int c = __ldg(cp + 32 * k);
-    if (c >= 0) acc = add(acc, mul(cvt<Acc>(__ldg(vp + 32 * k)), loadX<Acc>(x, c)));
-  }
-  return acc;
-}
-
 // y = A x.
 template <class MV, class VT>
 __global__ void __launch_bounds__(256) spmvKernel(SellView<MV> A, const VT* __restrict__ x,
@@ -194,21 +185,6 @@ __global__ void __launch_bounds__(256) spmvKernel(SellView<MV> A, const VT* __re
     const int K = (__ldg(A.base + c + 1) - s0) >> 5;
     if (row < A.n) y[row] = sellRowSum<VT>(A, x, row, s0, K, lane);
   }
-}
-
-template <class T> __device__ __forceinline__ double toDouble(T v) { return static_cast<double>(v); }
-
-// Accumulates one stored residual entry into a norm partial.
-__device__ __forceinline__ double normStep(double acc, double r, int kind) {
-  if (kind == GR_NORM_L2) return __dadd_rn(acc, __dmul_rn(r, r));
-  if (kind == GR_NORM_LINF) return fmax(acc, r);
-  return __dadd_rn(acc, r);  // L1: signed sum (dsl/tensor/Tensor.cpp:428-430)
-}
-
-__device__ __forceinline__ int normOp(int kind) { return kind == GR_NORM_LINF ? RED_MAX : RED_SUM; }
-
-__device__ __forceinline__ double normFinish(double total, int kind) {
-  return kind == GR_NORM_L2 ? sqrt(total) : total;
 }
 
 // Residual with an IEEE intermediate type I (float or double):
@@ -268,11 +244,10 @@ __global__ void __launch_bounds__(256) residualDwKernel(SellView<float> A, const
     const int K = (__ldg(A.base + c + 1) - s0) >> 5;
     if (row < A.n) {
       dw sum = dwTimesFp(ld(row), __ldg(A.diag + row));
-      const int* cp = A.col + s0 + lane;
-      const float* vp = A.val + s0 + lane;
+      const int2* ep = A.ent + s0 + lane;
       for (int k = 0; k < K; ++k) {
-        int cc = __ldg(cp + 32 * k);
-        if (cc >= 0) sum = dwPlusDw(sum, dwTimesFp(ld(cc), __ldg(vp + 32 * k)));
+        int2 e = __ldcs(ep + 32 * k);
+        if (e.x >= 0) sum = dwPlusDw(sum, dwTimesFp(ld(e.x), __int_as_float(e.y)));
       }
       dw res = dwPlusDw(dw{__ldg(b + row), 0.0f}, dwNeg(sum));
       float rv = dwToFloat(res);
@@ -319,18 +294,6 @@ __global__ void permuteKernel(const T* __restrict__ src, T* __restrict__ dst,
 
 // ---------------------------------------------------------------------------
 namespace {
-
-template <class MV>
-dev::SellView<MV> sellView(const DeviceMatrix& A) {
-  return dev::SellView<MV>{A.n, A.sell.nChunks, A.sell.base.as<int>(), A.sell.col.as<int>(),
-                           A.sell.val.as<MV>(), A.diag.as<MV>()};
-}
-
-void checkLaunch(const char* name) {
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) fail(GR_ECUDA, std::string("launch of ") + name + " failed: " + cudaGetErrorString(e));
-  noteLaunch();
-}
 
 }  // namespace
 

@@ -1,0 +1,314 @@
+// Fused PBiCGStab kernels (pbicgstab/Solver.cpp:48-194) and the
+// mixed-precision vector kernels of iterative refinement
+// (iterative-refinement/Solver.cpp:48-123).
+//
+// Every reduction is a single-pass deterministic FP64 grid reduction whose
+// last block also derives the scalars (alpha, omega, beta, convergence) and
+// writes them into the device-resident KState, so an iteration runs without
+// host round trips. Every kernel returns immediately once KState::done is
+// set, which lets the host enqueue iterations ahead of the convergence test.
+#include <cmath>
+
+#include "devmath.cuh"
+#include "krylov.hpp"
+#include "sell.cuh"
+
+namespace gr {
+
+namespace dev {
+
+constexpr double kVsmall = 1e-37;  // Traits<float>::vsmall (common/Traits.hpp:43)
+
+// SolverStats::checkConvergence (SolverStats.cpp:33-56).
+__device__ __forceinline__ bool converged(const KState* st) {
+  const double f = st->normFinal;
+  bool c = f < st->absTol || f < st->normInit * st->relRes;
+  if (st->relTol > 0) c = c || f < st->bNorm * st->relTol;
+  return c;
+}
+
+// r = b - A x and r0 = r, with the norm of r and r0 . r.
+template <class MV, class W>
+__global__ void __launch_bounds__(256) bicgInitKernel(SellView<MV> A, const W* __restrict__ x,
+                                                       const W* __restrict__ b, W* __restrict__ r,
+                                                       W* __restrict__ r0, KState* st, double* partials,
+                                                       unsigned* counter) {
+  __shared__ double smem[64];
+  const int lane = threadIdx.x & 31;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  const int nk = st->normKind;
+  double v[2] = {redIdentity(normOp(nk)), 0.0};
+  const int ops[2] = {normOp(nk), RED_SUM};
+  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < A.nChunks; c += nWarps) {
+    const int row = c * 32 + lane;
+    const int s0 = __ldg(A.base + c);
+    const int K = (__ldg(A.base + c + 1) - s0) >> 5;
+    if (row < A.n) {
+      W res = sub(__ldg(b + row), sellRowSum<W>(A, x, row, s0, K, lane));
+      r[row] = res;
+      r0[row] = res;
+      v[0] = normStep(v[0], toDouble(res), nk);
+      v[1] = __dadd_rn(v[1], __dmul_rn(toDouble(res), toDouble(res)));
+    }
+  }
+  double out[2];
+  blockReduce<2>(v, ops, smem);
+  if (gridReduce<2>(v, ops, partials, counter, smem, out) && threadIdx.x == 0) {
+    const double nrm = normFinish(out[0], nk);
+    st->normInit = nrm;
+    st->normFinal = nrm;
+    st->rho = out[1];
+    st->iter = 0;
+    st->converged = 0;
+    st->singular = fabs(out[1]) < kVsmall;
+    st->status = isfinite(nrm) ? GR_OK : GR_ENONFINITE;
+    st->done = st->maxIter <= 0 || st->singular || st->status != GR_OK;
+  }
+}
+
+// y = A x with the step's dot products.
+// mode 0: dot0 = r0 . y, alpha = rho / dot0 (pbicgstab/Solver.cpp:119-123)
+// mode 1: dot0 = y . s, dot1 = y . y, omega = dot0 / dot1, singularity
+//         check (pbicgstab/Solver.cpp:149-159)
+template <class MV, class W, int MODE>
+__global__ void __launch_bounds__(256) spmvDotKernel(SellView<MV> A, const W* __restrict__ x,
+                                                      W* __restrict__ y, const W* __restrict__ d1,
+                                                      KState* st, double* partials, unsigned* counter) {
+  __shared__ double smem[64];
+  if (st->done) return;
+  const int lane = threadIdx.x & 31;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  double v[2] = {0.0, 0.0};
+  const int ops[2] = {RED_SUM, RED_SUM};
+  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < A.nChunks; c += nWarps) {
+    const int row = c * 32 + lane;
+    const int s0 = __ldg(A.base + c);
+    const int K = (__ldg(A.base + c + 1) - s0) >> 5;
+    if (row < A.n) {
+      const W yv = sellRowSum<W>(A, x, row, s0, K, lane);
+      y[row] = yv;
+      const double yd = toDouble(yv);
+      v[0] = __dadd_rn(v[0], __dmul_rn(toDouble(__ldg(d1 + row)), yd));
+      if (MODE == 1) v[1] = __dadd_rn(v[1], __dmul_rn(yd, yd));
+    }
+  }
+  double out[2];
+  blockReduce<2>(v, ops, smem);
+  if (gridReduce<2>(v, ops, partials, counter, smem, out) && threadIdx.x == 0) {
+    if (MODE == 0) {
+      st->dot0 = out[0];
+      st->alpha = st->rho / out[0];
+    } else {
+      st->dot0 = out[0];
+      st->dot1 = out[1];
+      st->omega = out[0] / out[1];
+      if (fabs(st->omega) < kVsmall) {
+        st->singular = 1;
+        st->done = 1;
+      }
+    }
+  }
+}
+
+// x = x + alpha y + omega z, r = s - omega t (pbicgstab/Solver.cpp:164-168),
+// then norm, convergence, iteration count and the next rho / beta.
+template <class W>
+__global__ void __launch_bounds__(256) bicgUpdateKernel(W* __restrict__ x, const W* __restrict__ y,
+                                                         const W* __restrict__ z, W* __restrict__ r,
+                                                         const W* __restrict__ s, const W* __restrict__ t,
+                                                         const W* __restrict__ r0, int n, KState* st,
+                                                         double* partials, unsigned* counter) {
+  __shared__ double smem[64];
+  if (st->done) return;
+  const W al = cvt<W>(st->alpha), om = cvt<W>(st->omega);
+  const int nk = st->normKind;
+  double v[2] = {redIdentity(normOp(nk)), 0.0};
+  const int ops[2] = {normOp(nk), RED_SUM};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] = add(add(x[i], mul(al, y[i])), mul(om, z[i]));
+    const W rv = sub(s[i], mul(om, t[i]));
+    r[i] = rv;
+    v[0] = normStep(v[0], toDouble(rv), nk);
+    v[1] = __dadd_rn(v[1], __dmul_rn(toDouble(__ldg(r0 + i)), toDouble(rv)));
+  }
+  double out[2];
+  blockReduce<2>(v, ops, smem);
+  if (gridReduce<2>(v, ops, partials, counter, smem, out) && threadIdx.x == 0) {
+    st->normFinal = normFinish(out[0], nk);
+    st->converged = converged(st);
+    st->rhoOld = st->rho;
+    st->iter += 1;
+    if (!isfinite(st->normFinal)) st->status = GR_ENONFINITE;
+    st->done = (st->converged && st->iter >= st->minIter) || st->iter >= st->maxIter ||
+               st->status != GR_OK;
+    if (!st->done) {
+      // Next iteration's rho = r0 . r and beta (pbicgstab/Solver.cpp:91-99).
+      st->rho = out[1];
+      if (fabs(out[1]) < kVsmall) {
+        st->singular = 1;
+        st->done = 1;
+      } else {
+        st->beta = (st->rho / st->rhoOld) * (st->alpha / st->omega);
+      }
+    }
+  }
+}
+
+__global__ void stateResetKernel(KState* st, KState init) { *st = init; }
+
+// ---- mixed precision ---------------------------------------------------
+__global__ void castUpKernel(const float* __restrict__ x, void* phi, int E, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (E == GR_FLOAT64) static_cast<double*>(phi)[i] = static_cast<double>(x[i]);
+    else if (E == GR_TWOFLOAT32) static_cast<float2*>(phi)[i] = make_float2(x[i], 0.0f);
+    else static_cast<float*>(phi)[i] = x[i];
+  }
+}
+
+// phi = phi + corr.cast(E) (iterative-refinement/Solver.cpp:103).
+__global__ void phiUpdateKernel(void* phi, const float* __restrict__ corr, int E, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (E == GR_FLOAT64) {
+      double* p = static_cast<double*>(phi);
+      p[i] = __dadd_rn(p[i], static_cast<double>(corr[i]));
+    } else if (E == GR_TWOFLOAT32) {
+      float2* p = static_cast<float2*>(phi);
+      const float2 v = p[i];
+      const dw s = dwPlusFp(dw{v.x, v.y}, corr[i]);
+      p[i] = make_float2(s.h, s.l);
+    } else {
+      float* p = static_cast<float*>(phi);
+      p[i] = __fadd_rn(p[i], corr[i]);
+    }
+  }
+}
+
+__global__ void convertKernel(const void* src, int from, void* dst, int to, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double d;
+    float f;
+    if (from == GR_FLOAT64) {
+      d = static_cast<const double*>(src)[i];
+      f = __double2float_rn(d);
+    } else if (from == GR_TWOFLOAT32) {
+      const float2 v = static_cast<const float2*>(src)[i];
+      d = static_cast<double>(v.x) + static_cast<double>(v.y);
+      f = dwToFloat(dw{v.x, v.y});
+    } else {
+      f = static_cast<const float*>(src)[i];
+      d = static_cast<double>(f);
+    }
+    if (to == GR_FLOAT64) static_cast<double*>(dst)[i] = d;
+    else static_cast<float*>(dst)[i] = f;
+  }
+}
+
+}  // namespace dev
+
+// ---------------------------------------------------------------------------
+namespace {
+
+int elemBlocks(const DeviceMatrix& A, i64 n) {
+  return static_cast<int>(std::max<i64>(1, std::min<i64>(A.redBlocks, (n + 255) / 256)));
+}
+
+int elemBlocksN(i64 n) { return static_cast<int>(std::max<i64>(1, std::min<i64>(148 * 8, (n + 255) / 256))); }
+
+}  // namespace
+
+void launchBicgInit(DeviceMatrix& A, const void* x, const void* b, void* r, void* r0, KState* st, DType W,
+                    cudaStream_t s) {
+  const int blocks = A.spmvBlocks();
+  double* part = A.partials.as<double>();
+  unsigned* cnt = A.counter.as<unsigned>();
+  if (A.vt == DType::F32 && W == DType::F32)
+    dev::bicgInitKernel<float, float><<<blocks, 256, 0, s>>>(sellView<float>(A), static_cast<const float*>(x),
+                                                             static_cast<const float*>(b), static_cast<float*>(r),
+                                                             static_cast<float*>(r0), st, part, cnt);
+  else if (A.vt == DType::F32 && W == DType::F64)
+    dev::bicgInitKernel<float, double><<<blocks, 256, 0, s>>>(
+        sellView<float>(A), static_cast<const double*>(x), static_cast<const double*>(b), static_cast<double*>(r),
+        static_cast<double*>(r0), st, part, cnt);
+  else if (A.vt == DType::F64 && W == DType::F64)
+    dev::bicgInitKernel<double, double><<<blocks, 256, 0, s>>>(
+        sellView<double>(A), static_cast<const double*>(x), static_cast<const double*>(b), static_cast<double*>(r),
+        static_cast<double*>(r0), st, part, cnt);
+  else
+    fail(GR_EUNSUPPORTED, "PBiCGStab with float64 coefficients needs float64 vectors");
+  checkLaunch("bicg_init");
+}
+
+namespace {
+template <class MV, class W>
+void spmvDotT(DeviceMatrix& A, const void* x, void* y, const void* d1, int mode, KState* st, cudaStream_t s) {
+  const int blocks = A.spmvBlocks();
+  double* part = A.partials.as<double>();
+  unsigned* cnt = A.counter.as<unsigned>();
+  if (mode == 0)
+    dev::spmvDotKernel<MV, W, 0><<<blocks, 256, 0, s>>>(sellView<MV>(A), static_cast<const W*>(x),
+                                                        static_cast<W*>(y), static_cast<const W*>(d1), st, part,
+                                                        cnt);
+  else
+    dev::spmvDotKernel<MV, W, 1><<<blocks, 256, 0, s>>>(sellView<MV>(A), static_cast<const W*>(x),
+                                                        static_cast<W*>(y), static_cast<const W*>(d1), st, part,
+                                                        cnt);
+}
+}  // namespace
+
+void launchSpmvDot(DeviceMatrix& A, const void* x, void* y, const void* d1, int mode, KState* st, DType W,
+                   cudaStream_t s) {
+  if (A.vt == DType::F32 && W == DType::F32) spmvDotT<float, float>(A, x, y, d1, mode, st, s);
+  else if (A.vt == DType::F32 && W == DType::F64) spmvDotT<float, double>(A, x, y, d1, mode, st, s);
+  else if (A.vt == DType::F64 && W == DType::F64) spmvDotT<double, double>(A, x, y, d1, mode, st, s);
+  else fail(GR_EUNSUPPORTED, "PBiCGStab with float64 coefficients needs float64 vectors");
+  checkLaunch("spmv_dot");
+}
+
+void launchBicgUpdate(DeviceMatrix& A, void* x, const void* y, const void* z, void* r, const void* sv,
+                      const void* t, const void* r0, KState* st, DType W, cudaStream_t s) {
+  const int blocks = elemBlocks(A, A.n);
+  double* part = A.partials.as<double>();
+  unsigned* cnt = A.counter.as<unsigned>();
+  if (W == DType::F32)
+    dev::bicgUpdateKernel<float><<<blocks, 256, 0, s>>>(
+        static_cast<float*>(x), static_cast<const float*>(y), static_cast<const float*>(z), static_cast<float*>(r),
+        static_cast<const float*>(sv), static_cast<const float*>(t), static_cast<const float*>(r0), A.n, st, part,
+        cnt);
+  else
+    dev::bicgUpdateKernel<double><<<blocks, 256, 0, s>>>(
+        static_cast<double*>(x), static_cast<const double*>(y), static_cast<const double*>(z),
+        static_cast<double*>(r), static_cast<const double*>(sv), static_cast<const double*>(t),
+        static_cast<const double*>(r0), A.n, st, part, cnt);
+  checkLaunch("bicg_update");
+}
+
+void launchStateReset(KState* st, const KState& init, cudaStream_t s) {
+  dev::stateResetKernel<<<1, 1, 0, s>>>(st, init);
+  checkLaunch("state_reset");
+}
+
+void launchNormInto(DeviceMatrix& A, const void* x, DType t, int normKind, double* out, cudaStream_t s) {
+  launchNorm(A, x, t, normKind, out, s);
+}
+
+void launchCastUp(const float* x, void* phi, DType E, int n, cudaStream_t s) {
+  dev::castUpKernel<<<elemBlocksN(n), 256, 0, s>>>(x, phi, static_cast<int>(E), n);
+  checkLaunch("cast_up");
+}
+
+void launchPhiUpdate(void* phi, const float* corr, DType E, int n, cudaStream_t s) {
+  dev::phiUpdateKernel<<<elemBlocksN(n), 256, 0, s>>>(phi, corr, static_cast<int>(E), n);
+  checkLaunch("phi_update");
+}
+
+void launchCastDown(const void* phi, float* x, DType E, int n, cudaStream_t s) {
+  dev::convertKernel<<<elemBlocksN(n), 256, 0, s>>>(phi, static_cast<int>(E), x, GR_FLOAT32, n);
+  checkLaunch("cast_down");
+}
+
+void launchConvert(const void* src, DType from, void* dst, DType to, int n, cudaStream_t s) {
+  dev::convertKernel<<<elemBlocksN(n), 256, 0, s>>>(src, static_cast<int>(from), dst, static_cast<int>(to), n);
+  checkLaunch("convert");
+}
+
+}  // namespace gr

@@ -1,0 +1,91 @@
+// Device-resident solver state and the launchers of the preconditioner and
+// Krylov kernels.
+#pragma once
+
+#include "device.hpp"
+
+namespace gr {
+
+// Scalars of one PBiCGStab / Gauss-Seidel solve, kept in device memory so
+// that no iteration needs a host round trip. Written only by the last block
+// of a grid reduction (or a single-thread kernel); read by the kernels that
+// follow in stream order. Reductions accumulate in FP64.
+struct KState {
+  double rho, rhoOld, alpha, omega, beta;
+  double normInit, normFinal, bNorm;
+  double dot0, dot1;
+  // configuration (SolverStats tolerances are floats in the reference)
+  double absTol, relTol, relRes;
+  int maxIter, minIter, normKind;
+  // progress
+  int iter, converged, singular, done, status;
+  int pad[2];
+};
+
+// Prologue of a fused preconditioner application (the vector the
+// preconditioner is applied to).
+enum class Prologue : int {
+  Plain = 0,   // b
+  PUpdate = 1, // p = r (iteration 0) or p = r + beta (p - omega v); writes p
+  SUpdate = 2  // s = r - alpha v; writes s
+};
+
+struct PrologueArgs {
+  Prologue kind = Prologue::Plain;
+  const void* b = nullptr;  // Plain: the right-hand side
+  const void* r = nullptr;
+  void* pOrS = nullptr;     // p (read and written) or s (written)
+  const void* v = nullptr;
+  const KState* st = nullptr;  // scalars; also the early-exit flag (may be null)
+};
+
+// ---- ILU(0) / DILU ----------------------------------------------------
+// F: tile-local CRS values (in / out), D: diagonal (in, factored in place).
+void launchIluFactor(DeviceMatrix& A, void* F, void* D, const void* Aoff, bool dilu, cudaStream_t s);
+// inv = 1 / D
+void launchInvert(DeviceMatrix& A, const void* D, void* inv, cudaStream_t s);
+// Packs the slot values of schedule S (out, S.slots entries) from the
+// tile-local CRS values F.
+void launchPack(DeviceMatrix& A, const LevelSchedule& S, const void* F, void* out, cudaStream_t s);
+// y = M^-1 * prologue; vectors of type W. Lval / Uval: packed values of the
+// Lower / UpperDesc schedules.
+void launchIluApply(DeviceMatrix& A, const void* Lval, const void* Uval, const void* inv, bool dilu,
+                    const PrologueArgs& pro, void* y, DType W, cudaStream_t s);
+
+// ---- Gauss-Seidel -------------------------------------------------------
+// One sweep: xout from xin (xin may alias nothing; must differ from xout).
+// seedB: start each row from b (true) or from the diagonal (false).
+// Gval: packed values of the All schedule.
+void launchGsSweep(DeviceMatrix& A, const void* Gval, const void* b, bool seedB, const void* xin,
+                   bool xinZero, void* xout, DType W, const KState* st, cudaStream_t s);
+
+// ---- Krylov kernels ----------------------------------------------------
+// r = b - A x, r0 = r; state initialised (norm, rho = r0.r, flags).
+void launchBicgInit(DeviceMatrix& A, const void* x, const void* b, void* r, void* r0, KState* st,
+                    DType W, cudaStream_t s);
+// y = A x and the dots of the step: mode 0: alpha = rho / (r0 . y);
+// mode 1: omega = (y . s) / (y . y), singularity check.
+void launchSpmvDot(DeviceMatrix& A, const void* x, void* y, const void* d1, int mode, KState* st,
+                   DType W, cudaStream_t s);
+// x = x + alpha y + omega z; r = s - omega t; convergence; next rho, beta.
+void launchBicgUpdate(DeviceMatrix& A, void* x, const void* y, const void* z, void* r, const void* sv,
+                      const void* t, const void* r0, KState* st, DType W, cudaStream_t s);
+// Elementwise prologue when no fused preconditioner is used; also copies
+// the result into copyTo when non-null.
+void launchPrologue(DeviceMatrix& A, const PrologueArgs& pro, void* copyTo, DType W, cudaStream_t s);
+// Writes the initial state (single thread).
+void launchStateReset(KState* st, const KState& init, cudaStream_t s);
+// Norm of a vector into st->bNorm.
+void launchNormInto(DeviceMatrix& A, const void* x, DType t, int normKind, double* out, cudaStream_t s);
+
+// ---- mixed precision --------------------------------------------------
+// phi (E) = x (float)
+void launchCastUp(const float* x, void* phi, DType E, int n, cudaStream_t s);
+// phi = phi + corr in E arithmetic
+void launchPhiUpdate(void* phi, const float* corr, DType E, int n, cudaStream_t s);
+// x = (float) phi
+void launchCastDown(const void* phi, float* x, DType E, int n, cudaStream_t s);
+// dst (t) = phi (E) converted
+void launchConvert(const void* src, DType from, void* dst, DType to, int n, cudaStream_t s);
+
+}  // namespace gr

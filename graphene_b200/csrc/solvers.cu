@@ -1,10 +1,537 @@
-// Solver drivers (placeholder until the Krylov kernels land).
+// Solver drivers (matrix/solver/ of the reference): the C++ host side that
+// sequences the CUDA kernels. All vectors are device pointers in tile order.
+//
+// Each solver node mirrors one reference solver class:
+//   IluNode          ilu::Solver              (ilu/Solver.cpp:44-574)
+//   GsNode           gaussseidel::Solver      (gauss-seidel/Solver.cpp:39-160)
+//   PbicgstabNode    pbicgstab::Solver        (pbicgstab/Solver.cpp:40-194)
+//   MpirNode         iterativerefinement::Solver (iterative-refinement/Solver.cpp:48-128)
+//   RestarterNode    restarter::Solver        (restarter/Solver.cpp:34-56)
+// and Solver::createSolver's dispatch is makeNode (Solver.cpp:32-56).
+#include <cstdio>
+#include <cstring>
+
+#include "config.hpp"
+#include "krylov.hpp"
 #include "solvers.hpp"
 
 namespace gr {
 
-std::unique_ptr<SolverTree> SolverTree::create(DeviceMatrix&, const std::string&) {
-  fail(GR_EUNSUPPORTED, "solvers are not built yet");
+namespace {
+
+// The working type of a solve: the configured workingType, else x's type.
+DType workingType(const SolverConfig& c, DType xt) {
+  return c.workingType < 0 ? xt : static_cast<DType>(c.workingType);
+}
+
+class Node {
+ public:
+  Node(DeviceMatrix& A, const SolverConfig& c) : A_(A), cfg_(c) {}
+  virtual ~Node() = default;
+  // x: in/out, b: in; both of type W. gate (nullable): the enclosing
+  // solver's state; kernels of this solve return early once it is done.
+  virtual gr_stats solve(void* x, const void* b, DType W, const KState* gate) = 0;
+  virtual bool usesInitialGuess() const = 0;
+  virtual void copyPhi(void*, DType) { fail(GR_EUNSUPPORTED, "only IterativeRefinement keeps phi"); }
+  // Allocates the scratch a solve of type W needs (before graph capture).
+  virtual void prepare(DType) {}
+
+ protected:
+  DeviceMatrix& A_;
+  const SolverConfig& cfg_;
+  cudaStream_t s() const { return A_.stream; }
+};
+
+std::unique_ptr<Node> makeNode(DeviceMatrix& A, const SolverConfig& c);
+
+void printStats(const SolverConfig& c, const DeviceMatrix& A, const gr_stats& st) {
+  static const char* norms[] = {"L1", "L2", "LINF", "None"};
+  std::fprintf(stderr,
+               "%s: Solved on %d tiles, %s norm, Initial residual = %g, Final residual = %g, "
+               "Iterations = %d, Converged = %s, Singular = %s\n",
+               c.solverName().c_str(), A.P, norms[c.norm], st.initial_residual, st.final_residual,
+               st.iterations, st.converged ? "true" : "false", st.singular ? "true" : "false");
+}
+
+// ---------------------------------------------------------------------------
+class IluNode : public Node {
+ public:
+  IluNode(DeviceMatrix& A, const SolverConfig& c) : Node(A, c), dilu_(c.diagonalBased) {
+    A.ensureLocalCrs();
+    LevelSchedule& L = A.schedule(SweepEntries::Lower);
+    LevelSchedule& U = A.schedule(SweepEntries::UpperDesc);
+    const size_t vs = dtypeSize(A.vt);
+    DBuf F, D;
+    if (!dilu_) {
+      F.alloc(std::max<i64>(1, A.m) * vs);
+      GR_CUDA(cudaMemcpyAsync(F.get(), A.offDiag.get(), A.m * vs, cudaMemcpyDeviceToDevice, s()));
+    }
+    D.alloc(A.n * vs);
+    GR_CUDA(cudaMemcpyAsync(D.get(), A.diag.get(), A.n * vs, cudaMemcpyDeviceToDevice, s()));
+    // ilu::Solver::factorize at construction (ilu/Solver.cpp:44-51).
+    launchIluFactor(A, dilu_ ? nullptr : F.get(), D.get(), A.offDiag.get(), dilu_, s());
+    inv_.alloc(A.n * vs);
+    launchInvert(A, D.get(), inv_.get(), s());
+    const void* vals = dilu_ ? A.offDiag.get() : F.get();
+    Lval_.alloc(std::max<i64>(1, L.slots) * vs);
+    Uval_.alloc(std::max<i64>(1, U.slots) * vs);
+    launchPack(A, L, vals, Lval_.get(), s());
+    launchPack(A, U, vals, Uval_.get(), s());
+    GR_CUDA(cudaStreamSynchronize(s()));
+  }
+  gr_stats solve(void* x, const void* b, DType W, const KState* gate) override {
+    PrologueArgs pro;
+    pro.kind = Prologue::Plain;
+    pro.b = b;
+    pro.st = gate;
+    apply(pro, x, W);
+    gr_stats st{};
+    st.iterations = 1;  // ilu/Solver.cpp:571-573
+    return st;
+  }
+  void apply(const PrologueArgs& pro, void* y, DType W) {
+    launchIluApply(A_, Lval_.get(), Uval_.get(), inv_.get(), dilu_, pro, y, W, s());
+  }
+  bool usesInitialGuess() const override { return false; }
+
+ private:
+  bool dilu_;
+  DBuf inv_, Lval_, Uval_;
+};
+
+// ---------------------------------------------------------------------------
+class GsNode : public Node {
+ public:
+  GsNode(DeviceMatrix& A, const SolverConfig& c) : Node(A, c) {
+    A.ensureLocalCrs();
+    LevelSchedule& G = A.schedule(SweepEntries::All);
+    Gval_.alloc(std::max<i64>(1, G.slots) * dtypeSize(A.vt));
+    launchPack(A, G, A.offDiag.get(), Gval_.get(), s());
+    GR_CUDA(cudaStreamSynchronize(s()));
+  }
+
+  // Sweeps ping-pong between x and a scratch vector; the result ends in x.
+  void sweeps(void* x, const void* b, DType W, int count, bool xZero, const KState* gate) {
+    if (count <= 0) return;
+    ensureTmp(W);
+    void* cur = x;
+    void* other = tmp_.get();
+    for (int k = 0; k < count; ++k) {
+      launchGsSweep(A_, Gval_.get(), b, cfg_.gsSeedB, cur, xZero && k == 0, other, W, gate, s());
+      std::swap(cur, other);
+    }
+    if (cur != x) GR_CUDA(cudaMemcpyAsync(x, cur, A_.n * dtypeSize(W), cudaMemcpyDeviceToDevice, s()));
+  }
+
+  gr_stats solve(void* x, const void* b, DType W, const KState* gate) override {
+    return solveImpl(x, b, W, gate, false);
+  }
+  gr_stats solveFromZero(void* x, const void* b, DType W, const KState* gate) {
+    return solveImpl(x, b, W, gate, true);
+  }
+  bool usesInitialGuess() const override { return true; }
+  void prepare(DType W) override { ensureTmp(W); }
+
+ private:
+  gr_stats solveImpl(void* x, const void* b, DType W, const KState* gate, bool xZero) {
+    gr_stats st{};
+    if (workingType(cfg_, W) != W)
+      fail(GR_EUNSUPPORTED, "GaussSeidel workingType different from the vector type");
+    if (cfg_.numFixedIterations > 0) {
+      // gauss-seidel/Solver.cpp:116-126
+      sweeps(x, b, W, cfg_.numFixedIterations, xZero, gate);
+      st.iterations = cfg_.numFixedIterations;
+      return st;
+    }
+    if (gate) fail(GR_EUNSUPPORTED, "a GaussSeidel preconditioner needs numFixedIterations > 0");
+    ensureTmp(W);
+    DBuf r(A_.n * dtypeSize(W));
+    double* d = A_.scalarOut.as<double>();
+    double h = 0;
+    if (cfg_.relTolerance > 0) {
+      launchNorm(A_, b, W, cfg_.norm, d + 1, s());
+      GR_CUDA(cudaMemcpyAsync(&h, d + 1, sizeof(double), cudaMemcpyDeviceToHost, s()));
+      GR_CUDA(cudaStreamSynchronize(s()));
+      st.b_norm = h;
+    }
+    auto residualNorm = [&]() {
+      launchResidual(A_, x, W, b, W, r.get(), W, W, cfg_.norm, d, s());
+      double v = 0;
+      GR_CUDA(cudaMemcpyAsync(&v, d, sizeof(double), cudaMemcpyDeviceToHost, s()));
+      GR_CUDA(cudaStreamSynchronize(s()));
+      return v;
+    };
+    st.initial_residual = st.final_residual = residualNorm();
+    bool conv = false;
+    while (!((conv && st.iterations >= cfg_.minIterations) || st.iterations >= cfg_.maxIterations)) {
+      // gauss-seidel/Solver.cpp:141-155: numSweeps sweeps per convergence check.
+      sweeps(x, b, W, cfg_.numSweeps, xZero && st.iterations == 0, nullptr);
+      st.iterations += cfg_.numSweeps;
+      st.final_residual = residualNorm();
+      conv = st.final_residual < cfg_.absTolerance || st.final_residual < st.initial_residual * cfg_.relResidual ||
+             (cfg_.relTolerance > 0 && st.final_residual < st.b_norm * cfg_.relTolerance);
+      if (!std::isfinite(st.final_residual)) {
+        st.status = GR_ENONFINITE;
+        break;
+      }
+      if (cfg_.printPerformanceEachIteration) {
+        st.converged = conv;
+        printStats(cfg_, A_, st);
+      }
+    }
+    st.converged = conv;
+    if (cfg_.printPerformanceAfterSolve) printStats(cfg_, A_, st);
+    return st;
+  }
+  void ensureTmp(DType W) {
+    const size_t bytes = A_.n * dtypeSize(W);
+    if (tmp_.bytes() < bytes) tmp_.alloc(bytes);
+  }
+  DBuf Gval_, tmp_;
+};
+
+// ---------------------------------------------------------------------------
+// Right-preconditioned BiCGStab. One iteration is five kernels when the
+// preconditioner is ILU (fused vector updates):
+//   ilu_apply(p-update) -> spmv_dot(alpha) -> ilu_apply(s-update) ->
+//   spmv_dot(omega) -> bicg_update(x, r, convergence, next rho/beta)
+// Iterations are captured once into a CUDA graph of `kBatch` iterations
+// that is replayed until the device-side state reports done.
+class PbicgstabNode : public Node {
+ public:
+  static constexpr int kBatch = 8;
+
+  PbicgstabNode(DeviceMatrix& A, const SolverConfig& c) : Node(A, c) {
+    if (c.preconditioner) {
+      pre_ = makeNode(A, *c.preconditioner);
+      ilu_ = dynamic_cast<IluNode*>(pre_.get());
+      gs_ = dynamic_cast<GsNode*>(pre_.get());
+    }
+    st_.alloc(sizeof(KState));
+    GR_CUDA(cudaMallocHost(&host_, sizeof(KState)));
+  }
+  ~PbicgstabNode() override {
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (host_) cudaFreeHost(host_);
+  }
+
+  gr_stats solve(void* x, const void* b, DType Wx, const KState* gate) override {
+    (void)gate;
+    const DType W = workingType(cfg_, Wx);
+    if (W != Wx) fail(GR_EUNSUPPORTED, "PBiCGStab workingType different from the vector type");
+    ensureBuffers(W);
+    const size_t vb = A_.n * dtypeSize(W);
+    KState init{};
+    init.absTol = cfg_.absTolerance;
+    init.relTol = cfg_.relTolerance;
+    init.relRes = cfg_.relResidual;
+    init.maxIter = cfg_.maxIterations;
+    init.minIter = cfg_.minIterations;
+    init.normKind = cfg_.norm;
+    KState* st = st_.as<KState>();
+    launchStateReset(st, init, s());
+    // The reference takes ||x|| here (pbicgstab/Solver.cpp:69-70); the norm
+    // of b is what relTolerance is documented to use (SolverStats.hpp:52-60).
+    if (cfg_.relTolerance > 0) launchNorm(A_, b, W, cfg_.norm, &st->bNorm, s());
+    GR_CUDA(cudaMemcpyAsync(xw(), x, vb, cudaMemcpyDeviceToDevice, s()));
+    launchBicgInit(A_, xw(), b, buf(R), buf(R0), st, W, s());
+    const bool graphable = ilu_ || !pre_ || (gs_ && cfg_.preconditioner->numFixedIterations > 0);
+    const bool perIter = cfg_.printPerformanceEachIteration;
+    int issued = 0;
+    for (;;) {
+      if (graphable && !perIter) {
+        launchBatch(W);
+        issued += kBatch;
+      } else {
+        iteration(W);
+        issued += 1;
+      }
+      GR_CUDA(cudaMemcpyAsync(host_, st, sizeof(KState), cudaMemcpyDeviceToHost, s()));
+      GR_CUDA(cudaStreamSynchronize(s()));
+      if (perIter) printStats(cfg_, A_, stats());
+      if (host_->done) break;
+      if (issued > cfg_.maxIterations && issued > (1 << 30)) break;
+    }
+    GR_CUDA(cudaMemcpyAsync(x, xw(), vb, cudaMemcpyDeviceToDevice, s()));
+    GR_CUDA(cudaStreamSynchronize(s()));
+    gr_stats out = stats();
+    if (cfg_.printPerformanceAfterSolve) printStats(cfg_, A_, out);
+    return out;
+  }
+  bool usesInitialGuess() const override { return true; }
+
+ private:
+  enum { X = 0, R, R0, P, V, Y, S, Z, T, NBUF };
+  std::unique_ptr<Node> pre_;
+  IluNode* ilu_ = nullptr;
+  GsNode* gs_ = nullptr;
+  DBuf st_;
+  KState* host_ = nullptr;
+  DBuf vec_;
+  DType bufType_ = DType::F32;
+  bool haveBufs_ = false;
+  cudaGraphExec_t exec_ = nullptr;
+  DType graphType_ = DType::F32;
+  int graphKernels_ = 0;
+
+  void* buf(int i) { return static_cast<char*>(vec_.get()) + static_cast<size_t>(i) * A_.n * dtypeSize(bufType_); }
+  void* xw() { return buf(X); }
+
+  void ensureBuffers(DType W) {
+    if (haveBufs_ && bufType_ == W) return;
+    vec_.alloc(static_cast<size_t>(NBUF) * A_.n * dtypeSize(W));
+    bufType_ = W;
+    haveBufs_ = true;
+    if (exec_) {
+      cudaGraphExecDestroy(exec_);
+      exec_ = nullptr;
+    }
+  }
+
+  gr_stats stats() const {
+    gr_stats o{};
+    o.initial_residual = host_->normInit;
+    o.final_residual = host_->normFinal;
+    o.b_norm = host_->bNorm;
+    o.iterations = host_->iter;
+    o.converged = host_->converged;
+    o.singular = host_->singular;
+    o.status = host_->status;
+    return o;
+  }
+
+  // Applies the preconditioner to the prologue vector into out.
+  void precondition(const PrologueArgs& pro, void* out, DType W) {
+    KState* st = st_.as<KState>();
+    if (ilu_) {
+      ilu_->apply(pro, out, W);
+      return;
+    }
+    if (!pre_) {
+      launchPrologue(A_, pro, out, W, s());
+      return;
+    }
+    launchPrologue(A_, pro, nullptr, W, s());
+    const void* in = pro.pOrS;
+    if (gs_) {
+      gs_->solveFromZero(out, in, W, st);
+      return;
+    }
+    if (pre_->usesInitialGuess()) GR_CUDA(cudaMemsetAsync(out, 0, A_.n * dtypeSize(W), s()));
+    pre_->solve(out, in, W, st);
+  }
+
+  // One PBiCGStab iteration (pbicgstab/Solver.cpp:90-186).
+  void iteration(DType W) {
+    KState* st = st_.as<KState>();
+    PrologueArgs p;
+    p.kind = Prologue::PUpdate;
+    p.r = buf(R);
+    p.pOrS = buf(P);
+    p.v = buf(V);
+    p.st = st;
+    precondition(p, buf(Y), W);
+    launchSpmvDot(A_, buf(Y), buf(V), buf(R0), 0, st, W, s());
+    PrologueArgs q;
+    q.kind = Prologue::SUpdate;
+    q.r = buf(R);
+    q.pOrS = buf(S);
+    q.v = buf(V);
+    q.st = st;
+    precondition(q, buf(Z), W);
+    launchSpmvDot(A_, buf(Z), buf(T), buf(S), 1, st, W, s());
+    launchBicgUpdate(A_, xw(), buf(Y), buf(Z), buf(R), buf(S), buf(T), buf(R0), st, W, s());
+  }
+
+  void launchBatch(DType W) {
+    if (!exec_ || graphType_ != W) {
+      if (exec_) cudaGraphExecDestroy(exec_);
+      exec_ = nullptr;
+      cudaGraph_t g = nullptr;
+      if (pre_) pre_->prepare(W);
+      GR_CUDA(cudaStreamBeginCapture(s(), cudaStreamCaptureModeThreadLocal));
+      setCapturing(true);
+      int kernels = 0;
+      try {
+        const i64 c0 = capturedCount();
+        for (int k = 0; k < kBatch; ++k) iteration(W);
+        kernels = static_cast<int>(capturedCount() - c0);
+      } catch (...) {
+        setCapturing(false);
+        cudaStreamEndCapture(s(), &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      setCapturing(false);
+      GR_CUDA(cudaStreamEndCapture(s(), &g));
+      GR_CUDA(cudaGraphInstantiate(&exec_, g, 0));
+      cudaGraphDestroy(g);
+      graphType_ = W;
+      graphKernels_ = kernels;
+    }
+    GR_CUDA(cudaGraphLaunch(exec_, s()));
+    noteLaunch(graphKernels_);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Mixed-precision iterative refinement: the residual and the solution phi in
+// the extended type E, the correction solve in the working type (float).
+class MpirNode : public Node {
+ public:
+  MpirNode(DeviceMatrix& A, const SolverConfig& c) : Node(A, c), inner_(makeNode(A, *c.innerSolver)) {
+    scal_.alloc(sizeof(double) * 4);
+  }
+  gr_stats solve(void* x, const void* b, DType W, const KState*) override {
+    if (W != DType::F32)
+      fail(GR_EUNSUPPORTED, "IterativeRefinement expects a float32 working precision (x and b)");
+    E_ = cfg_.extendedPrecisionType < 0 ? W : static_cast<DType>(cfg_.extendedPrecisionType);
+    const int n = A_.n;
+    gr_stats st{};
+    double* d = scal_.as<double>();
+    if (cfg_.relTolerance > 0) {
+      launchNorm(A_, b, DType::F32, cfg_.norm, d + 1, s());
+      GR_CUDA(cudaMemcpyAsync(&st.b_norm, d + 1, sizeof(double), cudaMemcpyDeviceToHost, s()));
+    }
+    if (r_.bytes() < n * sizeof(float)) r_.alloc(n * sizeof(float));
+    if (phi_.bytes() < n * dtypeSize(E_)) phi_.alloc(n * dtypeSize(E_));
+    float* r = r_.as<float>();
+    // Initial residual of x in E, stored as float (iterative-refinement/Solver.cpp:79).
+    launchResidual(A_, x, DType::F32, b, DType::F32, r, DType::F32, E_, cfg_.norm, d, s());
+    st.initial_residual = st.final_residual = readScalar(d);
+    launchCastUp(static_cast<const float*>(x), phi_.get(), E_, n, s());
+    bool conv = false;
+    int innerTotal = 0;
+    while (!((conv && st.iterations >= cfg_.minIterations) || st.iterations >= cfg_.maxIterations)) {
+      st.iterations += 1;
+      if (inner_->usesInitialGuess()) GR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(float), s()));
+      gr_stats is = inner_->solve(x, r, DType::F32, nullptr);
+      innerTotal += is.inner_iterations > 0 ? is.inner_iterations : is.iterations;
+      launchPhiUpdate(phi_.get(), static_cast<const float*>(x), E_, n, s());
+      launchResidual(A_, phi_.get(), E_, b, DType::F32, r, DType::F32, E_, cfg_.norm, d, s());
+      st.final_residual = readScalar(d);
+      conv = st.final_residual < cfg_.absTolerance || st.final_residual < st.initial_residual * cfg_.relResidual ||
+             (cfg_.relTolerance > 0 && st.final_residual < st.b_norm * cfg_.relTolerance);
+      if (!std::isfinite(st.final_residual)) {
+        st.status = GR_ENONFINITE;
+        break;
+      }
+      if (cfg_.printPerformanceEachIteration) {
+        st.converged = conv;
+        printStats(cfg_, A_, st);
+      }
+    }
+    launchCastDown(phi_.get(), static_cast<float*>(x), E_, n, s());
+    GR_CUDA(cudaStreamSynchronize(s()));
+    st.converged = conv;
+    st.inner_iterations = innerTotal;
+    if (cfg_.printPerformanceAfterSolve) printStats(cfg_, A_, st);
+    return st;
+  }
+  bool usesInitialGuess() const override { return true; }
+  void copyPhi(void* out, DType t) override {
+    if (!phi_.get()) fail(GR_EINVAL, "no IterativeRefinement solve has run yet");
+    launchConvert(phi_.get(), E_, out, t, A_.n, s());
+    GR_CUDA(cudaStreamSynchronize(s()));
+  }
+
+ private:
+  std::unique_ptr<Node> inner_;
+  DType E_ = DType::F32;
+  DBuf phi_, r_, scal_;
+  double readScalar(const double* d) {
+    double v = 0;
+    GR_CUDA(cudaMemcpyAsync(&v, d, sizeof(double), cudaMemcpyDeviceToHost, s()));
+    GR_CUDA(cudaStreamSynchronize(s()));
+    return v;
+  }
+};
+
+// ---------------------------------------------------------------------------
+class RestarterNode : public Node {
+ public:
+  RestarterNode(DeviceMatrix& A, const SolverConfig& c) : Node(A, c), inner_(makeNode(A, *c.innerSolver)) {}
+  gr_stats solve(void* x, const void* b, DType W, const KState* gate) override {
+    int restarts = 0;
+    gr_stats st = inner_->solve(x, b, W, gate);
+    int total = st.iterations;
+    while (restarts < cfg_.maxRestarts && !st.converged && st.status == GR_OK) {
+      restarts += 1;
+      st = inner_->solve(x, b, W, gate);
+      total += st.iterations;
+    }
+    st.inner_iterations = total;
+    return st;
+  }
+  bool usesInitialGuess() const override { return inner_->usesInitialGuess(); }
+  void copyPhi(void* out, DType t) override { inner_->copyPhi(out, t); }
+
+ private:
+  std::unique_ptr<Node> inner_;
+};
+
+std::unique_ptr<Node> makeNode(DeviceMatrix& A, const SolverConfig& c) {
+  if (c.type == "GaussSeidel") return std::make_unique<GsNode>(A, c);
+  if (c.type == "IterativeRefinement") return std::make_unique<MpirNode>(A, c);
+  if (c.type == "ILU") return std::make_unique<IluNode>(A, c);
+  if (c.type == "PBiCGStab") return std::make_unique<PbicgstabNode>(A, c);
+  if (c.type == "restarter") return std::make_unique<RestarterNode>(A, c);
+  fail(GR_EPARSE, "Unknown solver: " + c.type);
+}
+
+class Tree : public SolverTree {
+ public:
+  Tree(DeviceMatrix& A, std::unique_ptr<SolverConfig> c) : A_(A), cfg_(std::move(c)) {
+    root_ = makeNode(A, *cfg_);
+    GR_CUDA(cudaEventCreate(&e0_));
+    GR_CUDA(cudaEventCreate(&e1_));
+  }
+  ~Tree() override {
+    cudaEventDestroy(e0_);
+    cudaEventDestroy(e1_);
+  }
+  gr_stats solve(void* x, DType xt, const void* b, DType bt) override {
+    if (xt != bt) fail(GR_EINVAL, "x and b must have the same type");
+    if (xt == DType::DW) fail(GR_EUNSUPPORTED, "twofloat32 x / b");
+    GR_CUDA(cudaEventRecord(e0_, A_.stream));
+    gr_stats st = root_->solve(x, b, xt, nullptr);
+    GR_CUDA(cudaEventRecord(e1_, A_.stream));
+    GR_CUDA(cudaEventSynchronize(e1_));
+    float ms = 0;
+    GR_CUDA(cudaEventElapsedTime(&ms, e0_, e1_));
+    st.solve_ms = ms;
+    return st;
+  }
+  gr_stats solveHost(void* x, DType xt, const void* b, DType bt) override {
+    if (xt != bt) fail(GR_EINVAL, "x and b must have the same type");
+    const size_t bytes = A_.n * dtypeSize(xt);
+    DBuf tmp(bytes), xd(bytes), bd(bytes);
+    cudaStream_t s = A_.stream;
+    GR_CUDA(cudaMemcpyAsync(tmp.get(), b, bytes, cudaMemcpyHostToDevice, s));
+    launchPermute(A_, tmp.get(), bd.get(), xt, true, s);
+    GR_CUDA(cudaMemcpyAsync(tmp.get(), x, bytes, cudaMemcpyHostToDevice, s));
+    launchPermute(A_, tmp.get(), xd.get(), xt, true, s);
+    gr_stats st = solve(xd.get(), xt, bd.get(), bt);
+    launchPermute(A_, xd.get(), tmp.get(), xt, false, s);
+    GR_CUDA(cudaMemcpyAsync(x, tmp.get(), bytes, cudaMemcpyDeviceToHost, s));
+    GR_CUDA(cudaStreamSynchronize(s));
+    return st;
+  }
+  void copyPhi(void* out, DType t) override { root_->copyPhi(out, t); }
+  std::string name() const override { return cfg_->solverName(); }
+
+ private:
+  DeviceMatrix& A_;
+  std::unique_ptr<SolverConfig> cfg_;
+  std::unique_ptr<Node> root_;
+  cudaEvent_t e0_ = nullptr, e1_ = nullptr;
+};
+
+}  // namespace
+
+std::unique_ptr<SolverTree> SolverTree::create(DeviceMatrix& A, const std::string& json) {
+  auto cfg = SolverConfig::fromText(json);
+  return std::make_unique<Tree>(A, std::move(cfg));
 }
 
 }  // namespace gr

@@ -242,6 +242,13 @@ int gr_solver_phi(gr_solver* s, void* out, gr_dtype t);
 /* Name of the solver tree, e.g. "IterativeRefinement(PBiCGStab(ILU(0)))". */
 int gr_solver_name(const gr_solver* s, char* buf, size_t len);
 
+/* Parses a solver configuration without a matrix or a GPU
+ * (Configuration::fromJSON, matrix/solver/Configuration.cpp:103-136) and
+ * writes the solver tree's name; unknown keys, which the reference ignores,
+ * are listed in unknown_keys (comma separated, may be NULL). */
+int gr_config_parse(const char* json, char* name, size_t name_len, char* unknown_keys,
+                    size_t unknown_len);
+
 #ifdef __cplusplus
 }
 #endif
