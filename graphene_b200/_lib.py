@@ -71,6 +71,10 @@ SIGNATURES = {
     "gr_host_matrix_from_coo": (C.c_int, [i64, i64, vp, vp, vp, i64, C.c_int, vp, vp, C.c_int, P(vp)]),
     "gr_host_matrix_poisson": (C.c_int, [i64, i64, i64, i64, C.c_int, C.c_int, P(vp)]),
     "gr_host_matrix_load_mm": (C.c_int, [C.c_char_p, i64, C.c_int, C.c_int, P(vp)]),
+    "gr_host_matrix_generate": (C.c_int, [C.c_int, i64, i64, i64, vp, C.c_uint64, i64, C.c_int,
+                                          C.c_int, P(vp)]),
+    "gr_random_vector": (C.c_int, [C.c_uint64, i64, C.c_int, C.c_double, C.c_double, vp]),
+    "gr_host_matrix_global_crs": (C.c_int, [vp, vp, vp, vp, vp]),
     "gr_host_matrix_destroy": (None, [vp]),
     "gr_host_matrix_get_info": (C.c_int, [vp, P(MatrixInfo)]),
     "gr_host_matrix_row_to_tile": (C.c_int, [vp, vp]),

@@ -90,6 +90,57 @@ int gr_host_matrix_poisson(int64_t nx, int64_t ny, int64_t nz, int64_t num_tiles
   });
 }
 
+int gr_host_matrix_generate(gr_generator kind, int64_t nx, int64_t ny, int64_t nz, const double* params,
+                            uint64_t seed, int64_t num_tiles, gr_partitioner partitioner, gr_dtype value_type,
+                            gr_host_matrix** out) {
+  return guarded([&] {
+    need(out, "out");
+    gr::GeneratedCsr g;
+    switch (kind) {
+      case GR_GEN_POISSON:
+        g = gr::generatePoisson(nx, ny, nz);
+        break;
+      case GR_GEN_VAR_POISSON:
+        need(params, "params");
+        g = gr::generateVarPoisson(nx, ny, nz, params[0], seed);
+        break;
+      case GR_GEN_CONVDIFF:
+        need(params, "params");
+        if (params[0] < 0 || params[1] < 0 || params[2] < 0) gr::fail(GR_EINVAL, "velocity must be >= 0");
+        g = gr::generateConvDiff(nx, ny, nz, params[0], params[1], params[2]);
+        break;
+      default:
+        gr::fail(GR_EINVAL, "unknown generator");
+    }
+    auto h = gr::HostMatrix::fromSortedCsr(g.n, std::move(g.rowPtr), std::move(g.col), std::move(g.val),
+                                           num_tiles, partitioner, nullptr, std::move(g.coords),
+                                           gr::toDType(value_type));
+    *out = new gr_host_matrix{std::move(h)};
+  });
+}
+
+int gr_random_vector(uint64_t seed, int64_t n, int dist, double lo, double hi, double* out) {
+  return guarded([&] {
+    need(out, "out");
+    if (n < 0) gr::fail(GR_EINVAL, "n must be non-negative");
+    if (dist == 0) gr::generateUniform(seed, n, lo, hi, out);
+    else if (dist == 1) gr::generateNormal(seed, n, out);
+    else gr::fail(GR_EINVAL, "dist must be 0 (uniform) or 1 (normal)");
+  });
+}
+
+int gr_host_matrix_global_crs(const gr_host_matrix* h, int64_t* row_ptr, int64_t* col, double* off_diag,
+                              double* diag) {
+  return guarded([&] {
+    need(h, "matrix");
+    const gr::HostMatrix& H = *h->m;
+    if (row_ptr) std::memcpy(row_ptr, H.gRowPtr.data(), sizeof(int64_t) * (H.n + 1));
+    if (col) std::memcpy(col, H.gCol.data(), sizeof(int64_t) * H.m);
+    if (off_diag) std::memcpy(off_diag, H.gVal.data(), sizeof(double) * H.m);
+    if (diag) std::memcpy(diag, H.gDiag.data(), sizeof(double) * H.n);
+  });
+}
+
 int gr_host_matrix_load_mm(const char* path, int64_t num_tiles, gr_partitioner partitioner,
                            gr_dtype value_type, gr_host_matrix** out) {
   return guarded([&] {

@@ -126,6 +126,10 @@ struct GeneratedCsr {
   std::vector<double> coords;
 };
 GeneratedCsr generatePoisson(i64 nx, i64 ny, i64 nz);
+GeneratedCsr generateVarPoisson(i64 nx, i64 ny, i64 nz, double sigma, uint64_t seed);
+GeneratedCsr generateConvDiff(i64 nx, i64 ny, i64 nz, double vx, double vy, double vz);
+void generateUniform(uint64_t seed, i64 n, double lo, double hi, double* out);
+void generateNormal(uint64_t seed, i64 n, double* out);
 
 // MatrixMarket reader (public format spec; replaces fast_matrix_market).
 // Values are parsed directly into valueType (strtof for float32) so that

@@ -138,6 +138,29 @@ int gr_host_matrix_poisson(int64_t nx, int64_t ny, int64_t nz, int64_t num_tiles
                            gr_partitioner partitioner, gr_dtype value_type,
                            gr_host_matrix** out);
 
+/* Synthetic 3-D 7-point matrices (natural row order, neighbours outside the
+ * grid dropped), an extension of generate3DPoissonMatrix:
+ *   GR_GEN_POISSON      params unused: diagonal 6, off-diagonals -1
+ *   GR_GEN_VAR_POISSON  params[0] = sigma: cell coefficient
+ *                       exp(sigma * N(0,1)) from `seed`, harmonic-mean face
+ *                       coefficients, Dirichlet faces add 2 k to the diagonal
+ *   GR_GEN_CONVDIFF     params[0..2] = velocity (>= 0): upwind
+ *                       convection-diffusion, unit diffusion and spacing */
+typedef enum { GR_GEN_POISSON = 0, GR_GEN_VAR_POISSON = 1, GR_GEN_CONVDIFF = 2 } gr_generator;
+int gr_host_matrix_generate(gr_generator kind, int64_t nx, int64_t ny, int64_t nz,
+                            const double* params, uint64_t seed, int64_t num_tiles,
+                            gr_partitioner partitioner, gr_dtype value_type,
+                            gr_host_matrix** out);
+
+/* Seeded vectors from the generators' counter-based stream: dist 0 =
+ * uniform [lo, hi), dist 1 = standard normal. */
+int gr_random_vector(uint64_t seed, int64_t n, int dist, double lo, double hi, double* out);
+
+/* Global CRS with split diagonal in natural order (CRSHostMatrix.cpp:88-137):
+ * row_ptr n + 1, col / off_diag m, diag n. Any pointer may be NULL. */
+int gr_host_matrix_global_crs(const gr_host_matrix* h, int64_t* row_ptr, int64_t* col,
+                              double* off_diag, double* diag);
+
 /* Replaces loadMatrixFromFile(type, path, numTiles)
  * (matrix/host/HostMatrix.hpp:88-91, details/MatrixMarket.cpp:31-65). */
 int gr_host_matrix_load_mm(const char* path, int64_t num_tiles, gr_partitioner partitioner,
