@@ -217,6 +217,62 @@ def generate3DPoissonMatrix(valueType: int, nx: int, ny: int, nz: int, numTiles:
     return HostMatrix(h)
 
 
+GEN_POISSON, GEN_VAR_POISSON, GEN_CONVDIFF = 0, 1, 2
+
+
+def generateMatrix(kind: int, nx: int, ny: int, nz: int, params=(), seed: int = 0,
+                   numTiles: int = 1, partitioner: int = PART_AUTO,
+                   valueType: int = FLOAT32) -> HostMatrix:
+    """Synthetic 7-point matrices (gr_host_matrix_generate): GEN_POISSON,
+    GEN_VAR_POISSON (params = (sigma,)), GEN_CONVDIFF (params = velocity)."""
+    p = (C.c_double * 3)(*(list(params) + [0.0] * (3 - len(params))))
+    h = C.c_void_p()
+    check(_lib.lib().gr_host_matrix_generate(kind, nx, ny, nz, p, seed, numTiles, partitioner,
+                                             parseType(valueType), C.byref(h)))
+    return HostMatrix(h)
+
+
+def randomVector(seed: int, n: int, dist: str = "uniform", lo: float = -1.0,
+                 hi: float = 1.0) -> np.ndarray:
+    """Seeded vector from the generators' counter-based stream (float64)."""
+    out = np.empty(n, dtype=np.float64)
+    check(_lib.lib().gr_random_vector(seed, n, 0 if dist == "uniform" else 1, lo, hi,
+                                      _ptr(out)))
+    return out
+
+
+def _astype(self: HostMatrix, t: int) -> HostMatrix:
+    """Same layout, coefficients stored as type t (gr_host_matrix_astype)."""
+    h = C.c_void_p()
+    check(_lib.lib().gr_host_matrix_astype(self._h, parseType(t), C.byref(h)))
+    return HostMatrix(h)
+
+
+def _global_crs(self: HostMatrix):
+    """Global CRS with split diagonal, natural order."""
+    n, m = self.numRows, self.numOffDiag
+    rp = np.empty(n + 1, np.int64)
+    col = np.empty(m, np.int64)
+    off = np.empty(m, np.float64)
+    dg = np.empty(n, np.float64)
+    check(_lib.lib().gr_host_matrix_global_crs(self._h, _ptr(rp), _ptr(col), _ptr(off), _ptr(dg)))
+    return rp, col, off, dg
+
+
+def _coo(self: HostMatrix):
+    """Global triplets (rows, cols, vals) including the diagonal."""
+    rp, col, off, dg = self.globalCrs()
+    n = self.numRows
+    rows = np.concatenate([np.repeat(np.arange(n, dtype=np.int64), np.diff(rp)),
+                           np.arange(n, dtype=np.int64)])
+    return rows, np.concatenate([col, np.arange(n, dtype=np.int64)]), np.concatenate([off, dg])
+
+
+HostMatrix.astype = _astype
+HostMatrix.globalCrs = _global_crs
+HostMatrix.coo = _coo
+
+
 def loadMatrixFromFile(valueType: int, path: str, numTiles: int,
                        partitioner: int = PART_AUTO) -> HostMatrix:
     """matrix/host/HostMatrix.hpp:88-91 (MatrixMarket coordinate files)."""

@@ -76,6 +76,7 @@ SIGNATURES = {
     "gr_random_vector": (C.c_int, [C.c_uint64, i64, C.c_int, C.c_double, C.c_double, vp]),
     "gr_host_matrix_global_crs": (C.c_int, [vp, vp, vp, vp, vp]),
     "gr_host_matrix_destroy": (None, [vp]),
+    "gr_host_matrix_astype": (C.c_int, [vp, C.c_int, P(vp)]),
     "gr_host_matrix_get_info": (C.c_int, [vp, P(MatrixInfo)]),
     "gr_host_matrix_row_to_tile": (C.c_int, [vp, vp]),
     "gr_host_matrix_tile_sizes": (C.c_int, [vp, vp]),

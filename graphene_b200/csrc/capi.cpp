@@ -155,6 +155,24 @@ int gr_host_matrix_load_mm(const char* path, int64_t num_tiles, gr_partitioner p
 
 void gr_host_matrix_destroy(gr_host_matrix* h) { delete h; }
 
+int gr_host_matrix_astype(const gr_host_matrix* h, gr_dtype value_type, gr_host_matrix** out) {
+  return guarded([&] {
+    need(h, "matrix");
+    need(out, "out");
+    gr::DType t = gr::toDType(value_type);
+    if (t == gr::DType::DW) gr::fail(GR_EUNSUPPORTED, "twofloat32 coefficients are not supported");
+    auto c = std::make_shared<gr::HostMatrix>(*h->m);
+    c->valueType = t;
+    if (t == gr::DType::F32) {
+      auto r = [](std::vector<double>& v) {
+        for (double& x : v) x = static_cast<double>(static_cast<float>(x));
+      };
+      r(c->gVal); r(c->gDiag); r(c->offDiag); r(c->diag);
+    }
+    *out = new gr_host_matrix{std::move(c)};
+  });
+}
+
 int gr_host_matrix_get_info(const gr_host_matrix* h, gr_matrix_info* out) {
   return guarded([&] {
     need(h, "matrix");

@@ -168,6 +168,11 @@ int gr_host_matrix_load_mm(const char* path, int64_t num_tiles, gr_partitioner p
 
 void gr_host_matrix_destroy(gr_host_matrix* h);
 
+/* A copy of h with the same partition and layout and its coefficients
+ * stored as value_type (float64 keeps float32 values exactly; float32
+ * rounds). Used to solve the identical system in another precision. */
+int gr_host_matrix_astype(const gr_host_matrix* h, gr_dtype value_type, gr_host_matrix** out);
+
 int gr_host_matrix_get_info(const gr_host_matrix* h, gr_matrix_info* out);
 
 /* Partitioning::rowToTile after empty-tile removal (CRSHostMatrix.cpp:235-270). */
