@@ -241,6 +241,19 @@ int gr_host_matrix_levels(const gr_host_matrix* h, int32_t* lower_level, int32_t
   });
 }
 
+int gr_host_matrix_check_ilu_stream(const gr_host_matrix* h, int dilu, gr_dtype value_type, int32_t* ring_log2,
+                                    int64_t* stream_bytes) {
+  return guarded([&] {
+    need(h, "matrix");
+    const gr::DType vt = gr::toDType(value_type);
+    gr::HostStream S = gr::buildIluStream(*h->m, dilu != 0, vt);
+    const int lg = gr::ringLog2ForLevel(S.maxLevelBytes);
+    gr::checkIluStream(*h->m, S, dilu != 0, vt, lg);
+    if (ring_log2) *ring_log2 = lg;
+    if (stream_bytes) *stream_bytes = static_cast<int64_t>(S.bytes.size());
+  });
+}
+
 int gr_host_matrix_decompose_vector(const gr_host_matrix* h, const void* natural, void* tile_ordered,
                                     gr_dtype t) {
   return guarded([&] {

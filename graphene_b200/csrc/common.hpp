@@ -44,6 +44,10 @@ inline const char* dtypeName(DType t) {
   return "?";
 }
 
+template <class T> DType dtypeOf();
+template <> inline DType dtypeOf<float>() { return DType::F32; }
+template <> inline DType dtypeOf<double>() { return DType::F64; }
+
 inline DType toDType(int t) {
   if (t < 0 || t > 2) fail(GR_EINVAL, "invalid gr_dtype " + std::to_string(t));
   return static_cast<DType>(t);

@@ -87,6 +87,45 @@ struct LevelSchedule {
   DBuf src;           // i32 index into the local CRS values per slot, -1 = padding
 };
 
+// Byte stream of a tile's whole ILU application, consumed in order by the
+// streamed substitution kernel. Per tile:
+//   tile header  int4 {numLowerLevels, numUpperLevels, 0, 0}
+//   per level    int4 {k rows, E entries per row, hasInv, 0}
+//                rows  k x int32 tile-local row ids            (16-byte padded)
+//                inv   k x value type inverse diagonal (if hasInv)    (padded)
+//                cols  E*k x int32 tile-local columns, -1 pad, entry-major
+//                vals  E*k x value type, entry-major                  (padded)
+// lower levels (forward substitution, ascending columns) first, then upper
+// levels (backward substitution, descending columns). The template holds the
+// structure; a solver copies it and packs its factor values and inverse
+// diagonal in (valPos / valSrc, invPos / invSrc, element indices in units of
+// the value type).
+struct SweepStream {
+  bool dilu = false;
+  i64 bytes = 0;
+  i64 maxLevelBytes = 0;
+  i64 nVal = 0, nInv = 0;
+  DBuf tileOffset;  // i64[P + 1]
+  DBuf templ;       // bytes
+  DBuf valPos, valSrc, invPos, invSrc;  // i32
+};
+
+// Host copy of a SweepStream (built on the host, then uploaded).
+struct HostStream {
+  std::vector<uint8_t> bytes;
+  std::vector<i64> tileOffset;
+  std::vector<i32> valPos, valSrc, invPos, invSrc;
+  i64 maxLevelBytes = 0;
+};
+// Chunks of the streamed kernel's shared-memory ring.
+constexpr int kRingChunksHost = 8;
+HostStream buildIluStream(const HostMatrix& H, bool dilu, DType vt);
+// log2 of the ring size the streamed kernel uses for a given largest level.
+int ringLog2ForLevel(i64 maxLevelBytes);
+// Replays the streamed kernel's reads on the host; throws GR_EINVAL on any
+// out-of-range index, ordering or ring-capacity violation.
+void checkIluStream(const HostMatrix& H, const HostStream& S, bool dilu, DType vt, int ringLog2);
+
 // Kinds of entries a schedule keeps per row.
 enum class SweepEntries {
   Lower,        // tile-local columns below the row, ascending (ILU forward)
@@ -117,6 +156,12 @@ struct DeviceMatrix {
 
   // Schedules, built on demand.
   std::unique_ptr<LevelSchedule> lowerSched, upperSched, gsSched;
+  std::unique_ptr<SweepStream> iluStream[2];  // [dilu]
+  SweepStream& iluSweepStream(bool dilu);
+
+  // Device error word written by kernels whose bounded waits ran out
+  // (GR_ETIMEOUT); 0 when clean.
+  DBuf errFlag;  // int
 
   // Reduction scratch: per-block partials and an arrival counter.
   DBuf partials;   // double[maxBlocks * 8]

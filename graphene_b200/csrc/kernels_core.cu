@@ -145,6 +145,8 @@ DeviceMatrix::DeviceMatrix(std::shared_ptr<HostMatrix> h) : host(std::move(h)) {
   counter.alloc(sizeof(unsigned) * 16);
   GR_CUDA(cudaMemset(counter.get(), 0, sizeof(unsigned) * 16));
   scalarOut.alloc(sizeof(double) * 8);
+  errFlag.alloc(sizeof(int));
+  GR_CUDA(cudaMemset(errFlag.get(), 0, sizeof(int)));
   GR_CUDA(cudaDeviceSynchronize());
 }
 

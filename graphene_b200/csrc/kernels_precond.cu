@@ -267,13 +267,20 @@ __global__ void prologueKernel(Pro<W> pro, W* copyTo, int n) {
 }  // namespace dev
 
 // ---------------------------------------------------------------------------
+int maxDynamicSmem(const DeviceMatrix& A) {
+  static thread_local int cached[64] = {0};
+  const int d = A.device & 63;
+  if (cached[d] == 0) {
+    int v = 0;
+    GR_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, A.device));
+    cached[d] = v;
+  }
+  return cached[d];
+}
+
 namespace {
 
-int maxSmem(const DeviceMatrix& A) {
-  int v = 0;
-  GR_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, A.device));
-  return v;
-}
+int maxSmem(const DeviceMatrix& A) { return maxDynamicSmem(A); }
 
 template <class W>
 dev::Pro<W> makePro(const PrologueArgs& p) {

@@ -1,0 +1,310 @@
+// Streamed block-ILU(0) / DILU substitution.
+//
+// Same arithmetic as iluApplyKernel (ilu/Solver.cpp:367-550, level-scheduled)
+// but every level's data (row ids, inverse diagonal, columns, factor values)
+// comes from a per-tile byte stream (SweepStream) that is copied into a
+// shared-memory ring buffer with bulk asynchronous copies
+// (cp.async.bulk, completion tracked by one mbarrier per ring chunk). One
+// elected thread keeps up to kRingChunks chunks in flight ahead of the level
+// being processed, so a level's work reads only shared memory and the
+// per-level cost is a barrier instead of an HBM round trip. No multicast is
+// used: every CTA copies only its own tile's bytes from this GPU's memory.
+//
+// Every wait on an mbarrier is bounded; a wait that runs out sets the
+// matrix's error word to GR_ETIMEOUT, all threads leave the level loop
+// together at the next barrier, and the elected thread waits (bounded) for
+// its outstanding copies before the block exits.
+#include <algorithm>
+
+#include "devmath.cuh"
+#include "krylov.hpp"
+#include "sell.cuh"
+
+namespace gr {
+namespace dev {
+
+constexpr int kRingChunks = 8;
+constexpr long long kWaitLimit = 1ll << 22;
+
+__device__ __forceinline__ uint32_t smemAddr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbarInit(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fenceBarrierInit() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbarExpectTx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulkLoad(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ bool mbarTryWait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void fenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ long long pad16(long long b) { return (b + 15) & ~15ll; }
+
+// Pro<W> (the fused prologue) is defined in kernels_precond.cu; a local copy
+// of the same functor keeps this translation unit self-contained.
+template <class W>
+struct SPro {
+  int kind;
+  const W* __restrict__ b;
+  const W* __restrict__ r;
+  W* pOrS;
+  const W* __restrict__ v;
+  const KState* st;
+  __device__ __forceinline__ W operator()(int i, W beta, W omega, W alpha, bool first) const {
+    if (kind == static_cast<int>(Prologue::Plain)) return b[i];
+    if (kind == static_cast<int>(Prologue::PUpdate)) {
+      W p = first ? r[i] : add(r[i], mul(beta, sub(pOrS[i], mul(omega, v[i]))));
+      pOrS[i] = p;
+      return p;
+    }
+    W s = sub(r[i], mul(alpha, v[i]));
+    pOrS[i] = s;
+    return s;
+  }
+};
+
+template <class MV, class W>
+__global__ void __launch_bounds__(256) iluStreamKernel(const unsigned char* __restrict__ stream,
+                                                        const long long* __restrict__ tileOffset,
+                                                        const int* __restrict__ tileStart, int ringLog2, bool dilu,
+                                                        SPro<W> pro, W* __restrict__ y, int* errFlag) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ int abortFlag;
+  if (pro.st && pro.st->done) return;
+  const int T = blockIdx.x;
+  const int base = tileStart[T];
+  const int nRows = tileStart[T + 1] - base;
+  const long long g0 = tileOffset[T];
+  const long long len = tileOffset[T + 1] - g0;
+  const unsigned ringBytes = 1u << ringLog2;
+  const unsigned mask = ringBytes - 1;
+  const unsigned C = ringBytes / kRingChunks;
+  const int total = static_cast<int>((len + C - 1) / C);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+  unsigned char* ring = smem + 128;
+  W* xs = reinterpret_cast<W*>(smem + 128 + ringBytes);
+  const unsigned char* g = stream + g0;
+
+  int next = 0;  // next chunk to copy (used by thread 0 only)
+  auto issue = [&](int c) {
+    const unsigned bytes = static_cast<unsigned>(min(static_cast<long long>(C), len - static_cast<long long>(c) * C));
+    const uint32_t bar = smemAddr(bars + (c % kRingChunks));
+    mbarExpectTx(bar, bytes);
+    bulkLoad(smemAddr(ring + (c % kRingChunks) * C), g + static_cast<long long>(c) * C, bytes, bar);
+  };
+  if (threadIdx.x == 0) {
+    abortFlag = 0;
+    for (int r = 0; r < kRingChunks; ++r) mbarInit(smemAddr(bars + r), 1);
+    fenceBarrierInit();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (; next < total && next < kRingChunks; ++next) issue(next);
+
+  // Prologue into the tile's slice of x (overlaps the first copies).
+  {
+    W beta = W(0), omega = W(0), alpha = W(0);
+    bool first = true;
+    if (pro.st) {
+      beta = cvt<W>(pro.st->beta);
+      omega = cvt<W>(pro.st->omega);
+      alpha = cvt<W>(pro.st->alpha);
+      first = pro.st->iter == 0;
+    }
+    for (int i = threadIdx.x; i < nRows; i += blockDim.x) xs[i] = pro(base + i, beta, omega, alpha, first);
+  }
+
+  int waited = 0;
+  bool timedOut = false;
+  auto waitTo = [&](long long endByte) {
+    const int need = static_cast<int>((endByte + C - 1) / C);
+    for (; waited < need && !timedOut; ++waited) {
+      const uint32_t bar = smemAddr(bars + (waited % kRingChunks));
+      const uint32_t parity = (waited / kRingChunks) & 1;
+      long long it = 0;
+      while (!mbarTryWait(bar, parity))
+        if (++it > kWaitLimit) {
+          timedOut = true;
+          break;
+        }
+    }
+  };
+  auto rdInt = [&](long long o) { return *reinterpret_cast<const int*>(ring + (o & mask)); };
+  auto rdVal = [&](long long o) { return *reinterpret_cast<const MV*>(ring + (o & mask)); };
+
+  waitTo(16);
+  if (timedOut) abortFlag = 1;
+  __syncthreads();
+  int nL = 0, nU = 0;
+  if (!abortFlag) {
+    const int4 th = *reinterpret_cast<const int4*>(ring);
+    nL = th.x;
+    nU = th.y;
+  }
+  long long off = 16;
+  for (int lv = 0; lv < nL + nU && !abortFlag; ++lv) {
+    const bool upper = lv >= nL;
+    waitTo(off + 16);
+    int k = 0, E = 0;
+    bool hasInv = false;
+    if (!timedOut) {
+      const int4 h = *reinterpret_cast<const int4*>(ring + (off & mask));
+      k = h.x;
+      E = h.y;
+      hasInv = h.z != 0;
+    }
+    const long long rowsOff = off + 16;
+    const long long invOff = rowsOff + pad16(4ll * k);
+    const long long colsOff = invOff + (hasInv ? pad16(static_cast<long long>(sizeof(MV)) * k) : 0);
+    const long long valsOff = colsOff + pad16(4ll * E * k);
+    const long long end = valsOff + pad16(static_cast<long long>(sizeof(MV)) * E * k);
+    waitTo(end);
+    if (timedOut) {
+      abortFlag = 1;
+    } else if (!upper) {
+      // Forward substitution (ilu/Solver.cpp:380-411).
+      for (int q = threadIdx.x; q < k; q += blockDim.x) {
+        const int il = rdInt(rowsOff + 4ll * q);
+        W temp = xs[il];
+        for (int e = 0; e < E; ++e) {
+          const long long s = static_cast<long long>(e) * k + q;
+          const int c = rdInt(colsOff + 4 * s);
+          if (c < 0) break;
+          temp = sub(temp, mul(cvt<W>(rdVal(valsOff + sizeof(MV) * s)), xs[c]));
+        }
+        xs[il] = dilu ? mul(temp, cvt<W>(rdVal(invOff + sizeof(MV) * q))) : temp;
+      }
+    } else {
+      // Backward substitution (ilu/Solver.cpp:413-442).
+      for (int q = threadIdx.x; q < k; q += blockDim.x) {
+        const int il = rdInt(rowsOff + 4ll * q);
+        W temp = W(0);
+        for (int e = 0; e < E; ++e) {
+          const long long s = static_cast<long long>(e) * k + q;
+          const int c = rdInt(colsOff + 4 * s);
+          if (c < 0) break;
+          temp = sub(temp, mul(cvt<W>(rdVal(valsOff + sizeof(MV) * s)), xs[c]));
+        }
+        const W iv = cvt<W>(rdVal(invOff + sizeof(MV) * q));
+        xs[il] = dilu ? add(xs[il], mul(temp, iv)) : mul(add(xs[il], temp), iv);
+      }
+    }
+    __syncthreads();
+    off = end;
+    if (threadIdx.x == 0 && !abortFlag) {
+      // Chunks below off / C are consumed: refill their ring slots.
+      fenceProxyAsync();
+      const int limit = static_cast<int>(off / C) + kRingChunks;
+      for (; next < total && next < limit; ++next) issue(next);
+    }
+  }
+  if (abortFlag) {
+    if (threadIdx.x == 0) {
+      atomicExch(errFlag, GR_ETIMEOUT);
+      // Let the copies already issued land before the block's shared
+      // memory is released (bounded).
+      for (int c = waited; c < next; ++c) {
+        long long it = 0;
+        while (!mbarTryWait(smemAddr(bars + (c % kRingChunks)), (c / kRingChunks) & 1) && ++it < kWaitLimit) {
+        }
+      }
+    }
+    return;
+  }
+  for (int i = threadIdx.x; i < nRows; i += blockDim.x) y[base + i] = xs[i];
+}
+
+template <class MV>
+__global__ void streamPackKernel(MV* __restrict__ stream, const int* __restrict__ valPos,
+                                 const int* __restrict__ valSrc, long long nVal, const MV* __restrict__ F,
+                                 const int* __restrict__ invPos, const int* __restrict__ invSrc, long long nInv,
+                                 const MV* __restrict__ inv) {
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < nVal; i += stride) {
+    const int s = valSrc[i];
+    stream[valPos[i]] = s >= 0 ? F[s] : MV(0);
+  }
+  for (long long j = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; j < nInv; j += stride)
+    stream[invPos[j]] = inv[invSrc[j]];
+}
+
+}  // namespace dev
+
+// ---------------------------------------------------------------------------
+static_assert(dev::kRingChunks == kRingChunksHost, "ring geometry shared with the host checker");
+
+namespace {
+int ringLog2For(i64 maxLevelBytes) { return ringLog2ForLevel(maxLevelBytes); }
+}  // namespace
+
+size_t iluStreamSmem(const DeviceMatrix& A, const SweepStream& S, DType W) {
+  const int lg = ringLog2For(S.maxLevelBytes);
+  if (lg > 16) return 0;  // rings above 64 KB: use the level-schedule kernel
+  return 128 + (size_t(1) << lg) + static_cast<size_t>(A.host->maxTileRows) * dtypeSize(W);
+}
+
+void launchStreamPack(DeviceMatrix& A, const SweepStream& S, void* stream, const void* F, const void* inv,
+                      cudaStream_t s) {
+  GR_CUDA(cudaMemcpyAsync(stream, S.templ.get(), S.bytes, cudaMemcpyDeviceToDevice, s));
+  const int blocks = static_cast<int>(std::max<i64>(1, std::min<i64>(A.redBlocks, (S.nVal + 255) / 256)));
+  if (A.vt == DType::F32)
+    dev::streamPackKernel<float><<<blocks, 256, 0, s>>>(static_cast<float*>(stream), S.valPos.as<int>(),
+                                                        S.valSrc.as<int>(), S.nVal, static_cast<const float*>(F),
+                                                        S.invPos.as<int>(), S.invSrc.as<int>(), S.nInv,
+                                                        static_cast<const float*>(inv));
+  else
+    dev::streamPackKernel<double><<<blocks, 256, 0, s>>>(
+        static_cast<double*>(stream), S.valPos.as<int>(), S.valSrc.as<int>(), S.nVal, static_cast<const double*>(F),
+        S.invPos.as<int>(), S.invSrc.as<int>(), S.nInv, static_cast<const double*>(inv));
+  checkLaunch("stream_pack");
+}
+
+namespace {
+template <class MV, class W>
+void streamApplyT(DeviceMatrix& A, const SweepStream& S, const void* stream, bool dilu, const PrologueArgs& p,
+                  void* y, cudaStream_t s) {
+  const int lg = ringLog2For(S.maxLevelBytes);
+  const size_t smem = iluStreamSmem(A, S, dtypeOf<W>());
+  auto kernel = dev::iluStreamKernel<MV, W>;
+  static thread_local size_t configured[4] = {0, 0, 0, 0};
+  const int slot = (sizeof(MV) == 8) * 2 + (sizeof(W) == 8);
+  if (smem > configured[slot]) {
+    GR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    configured[slot] = smem;
+  }
+  dev::SPro<W> pro{static_cast<int>(p.kind), static_cast<const W*>(p.b), static_cast<const W*>(p.r),
+                   static_cast<W*>(p.pOrS), static_cast<const W*>(p.v), p.st};
+  kernel<<<A.P, 256, smem, s>>>(static_cast<const unsigned char*>(stream), S.tileOffset.as<long long>(),
+                                A.tileStart.as<int>(), lg, dilu, pro, static_cast<W*>(y), A.errFlag.as<int>());
+  checkLaunch("ilu_stream");
+}
+}  // namespace
+
+void launchIluStream(DeviceMatrix& A, const SweepStream& S, const void* stream, bool dilu,
+                     const PrologueArgs& pro, void* y, DType W, cudaStream_t s) {
+  if (A.vt == DType::F32 && W == DType::F32) streamApplyT<float, float>(A, S, stream, dilu, pro, y, s);
+  else if (A.vt == DType::F32 && W == DType::F64) streamApplyT<float, double>(A, S, stream, dilu, pro, y, s);
+  else if (A.vt == DType::F64 && W == DType::F64) streamApplyT<double, double>(A, S, stream, dilu, pro, y, s);
+  else fail(GR_EUNSUPPORTED, "ILU with float64 coefficients needs float64 vectors");
+}
+
+}  // namespace gr

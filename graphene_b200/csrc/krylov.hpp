@@ -52,6 +52,17 @@ void launchPack(DeviceMatrix& A, const LevelSchedule& S, const void* F, void* ou
 void launchIluApply(DeviceMatrix& A, const void* Lval, const void* Uval, const void* inv, bool dilu,
                     const PrologueArgs& pro, void* y, DType W, cudaStream_t s);
 
+// Streamed substitution (kernels_stream.cu). iluStreamSmem returns the
+// dynamic shared memory a launch with vector type W needs, 0 if the
+// matrix's levels are too large for the ring.
+size_t iluStreamSmem(const DeviceMatrix& A, const SweepStream& S, DType W);
+// stream = template with the factor values F and inverse diagonal inv packed in.
+void launchStreamPack(DeviceMatrix& A, const SweepStream& S, void* stream, const void* F, const void* inv,
+                      cudaStream_t s);
+void launchIluStream(DeviceMatrix& A, const SweepStream& S, const void* stream, bool dilu,
+                     const PrologueArgs& pro, void* y, DType W, cudaStream_t s);
+int maxDynamicSmem(const DeviceMatrix& A);
+
 // ---- Gauss-Seidel -------------------------------------------------------
 // One sweep: xout from xin (xin may alias nothing; must differ from xout).
 // seedB: start each row from b (true) or from the diagonal (false).

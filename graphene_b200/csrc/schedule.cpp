@@ -8,6 +8,7 @@
 // levels, so processing the levels in order with the rows of a level in
 // parallel performs exactly the sequential sweep's operations.
 #include <algorithm>
+#include <cstring>
 
 #include "device.hpp"
 
@@ -119,6 +120,221 @@ LevelSchedule& DeviceMatrix::schedule(SweepEntries kind) {
   S->rows.upload(rows);
   S->col.upload(col);
   S->src.upload(src);
+  slot = std::move(S);
+  return *slot;
+}
+
+// ---------------------------------------------------------------------------
+// ILU application stream (see SweepStream in device.hpp).
+namespace {
+
+inline i64 pad16(i64 b) { return (b + 15) & ~i64(15); }
+
+struct TileBytes {
+  std::vector<uint8_t> bytes;
+  std::vector<std::pair<i64, i32>> vals;  // (byte offset in tile stream, CRS source or -1)
+  std::vector<std::pair<i64, i32>> invs;  // (byte offset, tile-order row)
+  i64 maxLevel = 0;
+};
+
+void putInt4(std::vector<uint8_t>& b, i32 a, i32 c, i32 d, i32 e) {
+  const i32 v[4] = {a, c, d, e};
+  const size_t o = b.size();
+  b.resize(o + 16);
+  std::memcpy(b.data() + o, v, 16);
+}
+
+}  // namespace
+
+HostStream buildIluStream(const HostMatrix& H, bool dilu, DType vt) {
+  const i64 vs = static_cast<i64>(dtypeSize(vt));
+  std::vector<TileBytes> tb(H.P);
+  parallelFor(H.P, [&](i64 T) {
+    TileBytes& t = tb[T];
+    const i64 base = H.tileStart[T];
+    const i64 nRows = H.tileStart[T + 1] - base;
+    putInt4(t.bytes, H.nLowerLevels[T], H.nUpperLevels[T], 0, 0);
+    std::vector<i64> ent;
+    for (int sweep = 0; sweep < 2; ++sweep) {
+      const bool upper = sweep == 1;
+      const SweepEntries kind = upper ? SweepEntries::UpperDesc : SweepEntries::Lower;
+      const i32 nL = upper ? H.nUpperLevels[T] : H.nLowerLevels[T];
+      const std::vector<i32>& lev = upper ? H.upperLevel : H.lowerLevel;
+      std::vector<std::vector<i64>> byLevel(nL);
+      for (i64 i = 0; i < nRows; ++i) byLevel[lev[base + i]].push_back(i);
+      const bool hasInv = upper || dilu;
+      for (i32 l = 0; l < nL; ++l) {
+        const auto& rows = byLevel[l];
+        const i64 k = static_cast<i64>(rows.size());
+        i64 E = 0;
+        for (i64 il : rows) {
+          rowEntries(H, kind, base + il, il, nRows, ent);
+          E = std::max<i64>(E, static_cast<i64>(ent.size()));
+        }
+        const i64 start = static_cast<i64>(t.bytes.size());
+        putInt4(t.bytes, static_cast<i32>(k), static_cast<i32>(E), hasInv ? 1 : 0, 0);
+        const i64 rowsOff = static_cast<i64>(t.bytes.size());
+        const i64 invOff = rowsOff + pad16(4 * k);
+        const i64 colsOff = invOff + (hasInv ? pad16(vs * k) : 0);
+        const i64 valsOff = colsOff + pad16(4 * E * k);
+        const i64 end = valsOff + pad16(vs * E * k);
+        t.bytes.resize(end, 0);
+        std::vector<i32> cols(E * k, -1);
+        for (i64 q = 0; q < k; ++q) {
+          const i64 il = rows[q];
+          const i32 r32 = static_cast<i32>(il);
+          std::memcpy(t.bytes.data() + rowsOff + 4 * q, &r32, 4);
+          if (hasInv) t.invs.emplace_back(invOff + vs * q, static_cast<i32>(base + il));
+          rowEntries(H, kind, base + il, il, nRows, ent);
+          for (i64 e = 0; e < E; ++e) {
+            const bool real = e < static_cast<i64>(ent.size());
+            cols[e * k + q] = real ? H.colLocal[ent[e]] : -1;
+            t.vals.emplace_back(valsOff + vs * (e * k + q), real ? static_cast<i32>(ent[e]) : -1);
+          }
+        }
+        std::memcpy(t.bytes.data() + colsOff, cols.data(), 4 * E * k);
+        t.maxLevel = std::max(t.maxLevel, end - start);
+      }
+    }
+    t.bytes.resize(pad16(static_cast<i64>(t.bytes.size())), 0);
+  });
+  HostStream S;
+  S.tileOffset.assign(H.P + 1, 0);
+  i64 nVal = 0, nInv = 0;
+  for (i32 T = 0; T < H.P; ++T) {
+    S.tileOffset[T + 1] = S.tileOffset[T] + static_cast<i64>(tb[T].bytes.size());
+    S.maxLevelBytes = std::max(S.maxLevelBytes, tb[T].maxLevel);
+    nVal += static_cast<i64>(tb[T].vals.size());
+    nInv += static_cast<i64>(tb[T].invs.size());
+  }
+  const i64 total = S.tileOffset[H.P];
+  if (total / vs >= (i64(1) << 31)) fail(GR_EUNSUPPORTED, "ILU stream exceeds 2^31 elements");
+  S.bytes.resize(total);
+  S.valPos.resize(nVal);
+  S.valSrc.resize(nVal);
+  S.invPos.resize(nInv);
+  S.invSrc.resize(nInv);
+  std::vector<i64> vOff(H.P + 1, 0), iOff(H.P + 1, 0);
+  for (i32 T = 0; T < H.P; ++T) {
+    vOff[T + 1] = vOff[T] + static_cast<i64>(tb[T].vals.size());
+    iOff[T + 1] = iOff[T] + static_cast<i64>(tb[T].invs.size());
+  }
+  parallelFor(H.P, [&](i64 T) {
+    const i64 off = S.tileOffset[T];
+    std::memcpy(S.bytes.data() + off, tb[T].bytes.data(), tb[T].bytes.size());
+    for (size_t i = 0; i < tb[T].vals.size(); ++i) {
+      S.valPos[vOff[T] + i] = static_cast<i32>((off + tb[T].vals[i].first) / vs);
+      S.valSrc[vOff[T] + i] = tb[T].vals[i].second;
+    }
+    for (size_t i = 0; i < tb[T].invs.size(); ++i) {
+      S.invPos[iOff[T] + i] = static_cast<i32>((off + tb[T].invs[i].first) / vs);
+      S.invSrc[iOff[T] + i] = tb[T].invs[i].second;
+    }
+  });
+  return S;
+}
+
+int ringLog2ForLevel(i64 maxLevelBytes) {
+  // The largest level plus one partially consumed chunk must fit in the
+  // ring: ring >= maxLevel * R / (R - 1) + 16.
+  const i64 need = maxLevelBytes * kRingChunksHost / (kRingChunksHost - 1) + 16;
+  int lg = 13;  // 8 KB minimum
+  while ((i64(1) << lg) < need) ++lg;
+  return lg;
+}
+
+// Replays the streamed kernel's consumption of every tile's stream on the
+// host: headers and segment offsets, index ranges, the level order each
+// entry depends on, and that every chunk a level needs has been issued under
+// the producer's refill rule (after a level ending at byte `off`, chunks
+// below off / C + R are in flight). Throws on the first violation.
+void checkIluStream(const HostMatrix& H, const HostStream& S, bool dilu, DType vt, int ringLog2) {
+  const i64 vs = static_cast<i64>(dtypeSize(vt));
+  const i64 ring = i64(1) << ringLog2, C = ring / kRingChunksHost;
+  parallelFor(H.P, [&](i64 T) {
+    const uint8_t* g = S.bytes.data() + S.tileOffset[T];
+    const i64 len = S.tileOffset[T + 1] - S.tileOffset[T];
+    const i64 base = H.tileStart[T];
+    const i64 nRows = H.tileStart[T + 1] - base;
+    auto bad = [&](const std::string& what) {
+      fail(GR_EINVAL, "ILU stream check failed in tile " + std::to_string(T) + ": " + what);
+    };
+    if (len % 16 != 0 || S.tileOffset[T] % 16 != 0) bad("misaligned tile stream");
+    const i64 total = (len + C - 1) / C;
+    i64 issued = std::min<i64>(total, kRingChunksHost);
+    auto needChunks = [&](i64 endByte) {
+      const i64 need = (endByte + C - 1) / C;
+      if (need > issued) bad("level needs chunk " + std::to_string(need - 1) + " before it is issued");
+      if (endByte > len) bad("read past the end of the stream");
+    };
+    auto rd = [&](i64 o) {
+      i32 v;
+      std::memcpy(&v, g + o, 4);
+      return v;
+    };
+    needChunks(16);
+    const i32 nL = rd(0), nU = rd(4);
+    if (nL != H.nLowerLevels[T] || nU != H.nUpperLevels[T]) bad("level counts");
+    std::vector<i32> doneLower(nRows, -1), doneUpper(nRows, -1);
+    i64 off = 16;
+    for (i32 lv = 0; lv < nL + nU; ++lv) {
+      const bool upper = lv >= nL;
+      needChunks(off + 16);
+      const i64 k = rd(off), E = rd(off + 4);
+      const bool hasInv = rd(off + 8) != 0;
+      if (k <= 0 || E < 0) bad("empty level");
+      if (hasInv != (upper || dilu)) bad("inverse-diagonal flag");
+      const i64 rowsOff = off + 16;
+      const i64 invOff = rowsOff + pad16(4 * k);
+      const i64 colsOff = invOff + (hasInv ? pad16(vs * k) : 0);
+      const i64 valsOff = colsOff + pad16(4 * E * k);
+      const i64 end = valsOff + pad16(vs * E * k);
+      needChunks(end);
+      for (i64 q = 0; q < k; ++q) {
+        const i32 il = rd(rowsOff + 4 * q);
+        if (il < 0 || il >= nRows) bad("row id out of range");
+        std::vector<i32>& done = upper ? doneUpper : doneLower;
+        if (done[il] >= 0) bad("row listed twice in one sweep");
+        bool padding = false;
+        for (i64 e = 0; e < E; ++e) {
+          const i32 c = rd(colsOff + 4 * (e * k + q));
+          if (c < 0) {
+            padding = true;
+            continue;
+          }
+          if (padding) bad("column after padding");
+          if (c >= nRows) bad("column out of range");
+          if (!upper && !(c < il)) bad("forward entry not below the diagonal");
+          if (upper && !(c > il)) bad("backward entry not above the diagonal");
+          if (done[c] < 0) bad("entry read before its row is computed");
+        }
+      }
+      for (i64 q = 0; q < k; ++q) (upper ? doneUpper : doneLower)[rd(rowsOff + 4 * q)] = lv;
+      off = end;
+      issued = std::min<i64>(total, off / C + kRingChunksHost);
+    }
+    if (off != len) bad("stream length does not match its levels");
+    for (i64 i = 0; i < nRows; ++i)
+      if (doneLower[i] < 0 || doneUpper[i] < 0) bad("row missing from a sweep");
+  });
+}
+
+SweepStream& DeviceMatrix::iluSweepStream(bool dilu) {
+  std::unique_ptr<SweepStream>& slot = iluStream[dilu ? 1 : 0];
+  if (slot) return *slot;
+  HostStream H = buildIluStream(*host, dilu, vt);
+  auto S = std::make_unique<SweepStream>();
+  S->dilu = dilu;
+  S->bytes = static_cast<i64>(H.bytes.size());
+  S->maxLevelBytes = H.maxLevelBytes;
+  S->nVal = static_cast<i64>(H.valPos.size());
+  S->nInv = static_cast<i64>(H.invPos.size());
+  S->tileOffset.upload(H.tileOffset);
+  S->templ.upload(H.bytes);
+  S->valPos.upload(H.valPos);
+  S->valSrc.upload(H.valSrc);
+  S->invPos.upload(H.invPos);
+  S->invSrc.upload(H.invSrc);
   slot = std::move(S);
   return *slot;
 }

@@ -73,12 +73,23 @@ class IluNode : public Node {
     inv_.alloc(A.n * vs);
     launchInvert(A, D.get(), inv_.get(), s());
     const void* vals = dilu_ ? A.offDiag.get() : F.get();
-    Lval_.alloc(std::max<i64>(1, L.slots) * vs);
-    Uval_.alloc(std::max<i64>(1, U.slots) * vs);
-    launchPack(A, L, vals, Lval_.get(), s());
-    launchPack(A, U, vals, Uval_.get(), s());
+    // Streamed substitution when the ring and the tile slice fit in shared
+    // memory for either vector type; the level-schedule kernel otherwise.
+    SweepStream& S = A.iluSweepStream(dilu_);
+    const size_t need = iluStreamSmem(A, S, DType::F64);
+    if (need > 0 && need <= static_cast<size_t>(maxDynamicSmem(A))) {
+      sweep_ = &S;
+      stream_.alloc(std::max<i64>(16, S.bytes));
+      launchStreamPack(A, S, stream_.get(), vals, inv_.get(), s());
+    } else {
+      Lval_.alloc(std::max<i64>(1, L.slots) * vs);
+      Uval_.alloc(std::max<i64>(1, U.slots) * vs);
+      launchPack(A, L, vals, Lval_.get(), s());
+      launchPack(A, U, vals, Uval_.get(), s());
+    }
     GR_CUDA(cudaStreamSynchronize(s()));
   }
+  bool streamed() const { return sweep_ != nullptr; }
   gr_stats solve(void* x, const void* b, DType W, const KState* gate) override {
     PrologueArgs pro;
     pro.kind = Prologue::Plain;
@@ -90,13 +101,19 @@ class IluNode : public Node {
     return st;
   }
   void apply(const PrologueArgs& pro, void* y, DType W) {
-    launchIluApply(A_, Lval_.get(), Uval_.get(), inv_.get(), dilu_, pro, y, W, s());
+    if (sweep_ && iluStreamSmem(A_, *sweep_, W) <= static_cast<size_t>(maxDynamicSmem(A_)))
+      launchIluStream(A_, *sweep_, stream_.get(), dilu_, pro, y, W, s());
+    else if (sweep_)
+      fail(GR_EUNSUPPORTED, "ILU stream does not fit shared memory for this vector type");
+    else
+      launchIluApply(A_, Lval_.get(), Uval_.get(), inv_.get(), dilu_, pro, y, W, s());
   }
   bool usesInitialGuess() const override { return false; }
 
  private:
   bool dilu_;
-  DBuf inv_, Lval_, Uval_;
+  DBuf inv_, Lval_, Uval_, stream_;
+  const SweepStream* sweep_ = nullptr;
 };
 
 // ---------------------------------------------------------------------------
@@ -500,6 +517,14 @@ class Tree : public SolverTree {
     float ms = 0;
     GR_CUDA(cudaEventElapsedTime(&ms, e0_, e1_));
     st.solve_ms = ms;
+    // A bounded device-side wait that ran out marks the solve as failed.
+    int err = 0;
+    GR_CUDA(cudaMemcpy(&err, A_.errFlag.get(), sizeof(int), cudaMemcpyDeviceToHost));
+    if (err != 0) {
+      GR_CUDA(cudaMemset(A_.errFlag.get(), 0, sizeof(int)));
+      st.status = err;
+      st.converged = 0;
+    }
     return st;
   }
   gr_stats solveHost(void* x, DType xt, const void* b, DType bt) override {

@@ -200,6 +200,15 @@ int gr_host_matrix_local_crs(const gr_host_matrix* h, int64_t* row_ptr, int32_t*
  * the backward sweep. Either pointer may be NULL. */
 int gr_host_matrix_levels(const gr_host_matrix* h, int32_t* lower_level, int32_t* upper_level);
 
+/* Builds the byte stream the streamed ILU(0) substitution kernel consumes
+ * (dilu: DILU variant; value_type: stored coefficient type) and replays the
+ * kernel's reads on the host, checking every index, the dependency order of
+ * the levels and the shared-memory ring capacity. Host only. Writes the
+ * ring size (log2 bytes) and stream length. No counterpart in the reference:
+ * it validates this library's own device layout. */
+int gr_host_matrix_check_ilu_stream(const gr_host_matrix* h, int dilu, gr_dtype value_type,
+                                    int32_t* ring_log2, int64_t* stream_bytes);
+
 /* Natural order <-> tile order (DistributedTileLayout::decomposeVector,
  * DistributedTileLayout.cpp:156-183, without halo). Host buffers. */
 int gr_host_matrix_decompose_vector(const gr_host_matrix* h, const void* natural,

@@ -1,0 +1,51 @@
+"""The streamed ILU substitution's byte stream, replayed on the host (CPU):
+every row / column index in range, entries only reference rows computed in
+earlier levels of the same sweep, and the shared-memory ring always holds the
+chunks a level needs under the kernel's refill rule."""
+import ctypes as C
+
+import pytest
+
+import graphene_b200 as gb
+from tests.util import random_coo
+
+
+def check(h, dilu, vt=gb.FLOAT32):
+    lg = C.c_int32()
+    nbytes = C.c_int64()
+    gb._lib.check(gb._lib.lib().gr_host_matrix_check_ilu_stream(h._h, int(dilu), vt, C.byref(lg),
+                                                                 C.byref(nbytes)))
+    return lg.value, nbytes.value
+
+
+@pytest.mark.parametrize("dims,tiles,part", [
+    ((16, 16, 16), 8, gb.PART_RCB),
+    ((13, 11, 7), 6, gb.PART_BFS),
+    ((12, 10, 8), 1, gb.PART_AUTO),
+    ((20, 20, 20), 200, gb.PART_RCB),
+    ((5, 4, 3), 60, gb.PART_RCB),
+    ((33, 17, 9), 5, gb.PART_CONTIGUOUS),
+])
+@pytest.mark.parametrize("dilu", [False, True])
+@pytest.mark.parametrize("vt", [gb.FLOAT32, gb.FLOAT64])
+def test_stream_replay(dims, tiles, part, dilu, vt):
+    h = gb.generate3DPoissonMatrix(vt, *dims, tiles, part)
+    lg, nbytes = check(h, dilu, vt)
+    assert 13 <= lg <= 20 and nbytes % 16 == 0
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_stream_replay_random(seed):
+    n, r, c, v = random_coo(400, 0.03, seed)
+    h = gb.HostMatrix.from_coo(n, r, c, v, 7, partitioner=gb.PART_BFS)
+    check(h, False)
+    check(h, True)
+    h1 = gb.HostMatrix.from_coo(*random_coo(200, 0.05, seed, symmetric=False), 1)
+    check(h1, False)
+
+
+def test_stream_replay_bench_problem():
+    """The 192^3 variable-coefficient system at the bench's 1024 tiles."""
+    h = gb.generateMatrix(gb.GEN_VAR_POISSON, 192, 192, 192, (1.5,), 2, 1024)
+    lg, nbytes = check(h, False)
+    assert lg <= 16
