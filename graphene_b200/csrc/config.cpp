@@ -244,10 +244,16 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
     if (const Json* v = j.find("workingType")) c->workingType = parseTypeName(v->text);
     if (const Json* v = j.find("preconditioner")) c->preconditioner = fromJson(*v);
   } else if (ty == "ILU") {
-    mark("solveMulticolor"); mark("factorizeMulticolor"); mark("diagonalBased");
+    mark("solveMulticolor"); mark("factorizeMulticolor"); mark("diagonalBased"); mark("kernel");
     readMultiColor(j, "solveMulticolor", c->solveMulticolor);
     readMultiColor(j, "factorizeMulticolor", c->factorizeMulticolor);
     readBool(j, "diagonalBased", c->diagonalBased);
+    if (const Json* v = j.find("kernel")) {
+      if (v->text == "auto") c->iluKernel = 0;
+      else if (v->text == "stream") c->iluKernel = 1;
+      else if (v->text == "levels") c->iluKernel = 2;
+      else fail(GR_EPARSE, "ILU kernel must be \"auto\", \"stream\" or \"levels\"");
+    }
   } else if (ty == "GaussSeidel") {
     mark("numSweeps"); mark("numFixedIterations"); mark("solveMulticolor"); mark("workingType");
     mark("seed");

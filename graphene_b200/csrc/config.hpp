@@ -40,6 +40,9 @@ struct SolverConfig {
   MultiColorMode solveMulticolor = MultiColorMode::Auto;
   MultiColorMode factorizeMulticolor = MultiColorMode::Auto;
   bool diagonalBased = false;
+  // Extension: substitution kernel, "auto" (streamed when it fits shared
+  // memory), "stream" or "levels" (level-schedule kernel).
+  int iluKernel = 0;  // 0 auto, 1 stream, 2 levels
   // GaussSeidel (gauss-seidel/Configuration.hpp:19-21)
   int numSweeps = 1, numFixedIterations = 0;
   // Extension: "seed": "b" (default, the codelet specification

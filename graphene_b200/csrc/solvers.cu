@@ -75,9 +75,16 @@ class IluNode : public Node {
     const void* vals = dilu_ ? A.offDiag.get() : F.get();
     // Streamed substitution when the ring and the tile slice fit in shared
     // memory for either vector type; the level-schedule kernel otherwise.
-    SweepStream& S = A.iluSweepStream(dilu_);
-    const size_t need = iluStreamSmem(A, S, DType::F64);
-    if (need > 0 && need <= static_cast<size_t>(maxDynamicSmem(A))) {
+    bool useStream = false;
+    if (c.iluKernel != 2) {
+      SweepStream& S = A.iluSweepStream(dilu_);
+      const size_t need = iluStreamSmem(A, S, DType::F64);
+      useStream = need > 0 && need <= static_cast<size_t>(maxDynamicSmem(A));
+      if (!useStream && c.iluKernel == 1)
+        fail(GR_EUNSUPPORTED, "the streamed ILU kernel does not fit this matrix's tiles in shared memory");
+    }
+    if (useStream) {
+      SweepStream& S = A.iluSweepStream(dilu_);
       sweep_ = &S;
       stream_.alloc(std::max<i64>(16, S.bytes));
       launchStreamPack(A, S, stream_.get(), vals, inv_.get(), s());

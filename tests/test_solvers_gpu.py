@@ -54,23 +54,25 @@ NAMES = ["poisson16", "poisson_odd_bfs", "poisson_1tile", "random", "many_tiles"
 
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("dilu", [False, True])
-def test_ilu_bit_exact(oracle, name, dilu):
+@pytest.mark.parametrize("kernel", ["stream", "levels"])
+def test_ilu_bit_exact(oracle, name, dilu, kernel):
     h, om = case(name, oracle)
     A = h.copyToTile()
     b = np.random.default_rng(3).uniform(-1, 1, h.numRows).astype(np.float32)
     x = A.createUninitializedVector(gb.FLOAT32)
-    gb.Solver(A, {"type": "ILU", "diagonalBased": dilu}).solve(x, dev(b))
+    gb.Solver(A, {"type": "ILU", "diagonalBased": dilu, "kernel": kernel}).solve(x, dev(b))
     off, inv = om.ilu_factorize(dilu)
     np.testing.assert_array_equal(host(x), om.ilu_solve(off, inv, b, dilu))
 
 
 @pytest.mark.parametrize("name", ["poisson16", "random"])
-def test_ilu_bit_exact_float64(oracle, name):
+@pytest.mark.parametrize("kernel", ["stream", "levels"])
+def test_ilu_bit_exact_float64(oracle, name, kernel):
     h, om = case(name, oracle, gb.FLOAT64)
     A = h.copyToTile()
     b = np.random.default_rng(4).standard_normal(h.numRows)
     x = A.createUninitializedVector(gb.FLOAT64)
-    gb.Solver(A, {"type": "ILU"}).solve(x, dev(b))
+    gb.Solver(A, {"type": "ILU", "kernel": kernel}).solve(x, dev(b))
     off, inv = om.ilu_factorize(False)
     np.testing.assert_array_equal(host(x), om.ilu_solve(off, inv, b, False))
 
@@ -108,6 +110,7 @@ def test_gauss_seidel_converges_with_checks(oracle):
 
 PCFG = {
     "ilu": {"type": "ILU"},
+    "ilu_levels": {"type": "ILU", "kernel": "levels"},
     "dilu": {"type": "ILU", "diagonalBased": True},
     "gs2": {"type": "GaussSeidel", "numFixedIterations": 2},
     "none": None,
