@@ -247,7 +247,7 @@ int gr_host_matrix_check_ilu_stream(const gr_host_matrix* h, int dilu, gr_dtype 
     need(h, "matrix");
     const gr::DType vt = gr::toDType(value_type);
     gr::HostStream S = gr::buildIluStream(*h->m, dilu != 0, vt);
-    const int lg = gr::ringLog2ForLevel(S.maxLevelBytes);
+    const int lg = gr::ringLog2ForLevel(S.maxSpanBytes);
     gr::checkIluStream(*h->m, S, dilu != 0, vt, lg);
     if (ring_log2) *ring_log2 = lg;
     if (stream_bytes) *stream_bytes = static_cast<int64_t>(S.bytes.size());

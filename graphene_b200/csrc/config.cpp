@@ -245,6 +245,10 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
     if (const Json* v = j.find("preconditioner")) c->preconditioner = fromJson(*v);
   } else if (ty == "ILU") {
     mark("solveMulticolor"); mark("factorizeMulticolor"); mark("diagonalBased"); mark("kernel");
+    mark("ringLog2");
+    readInt(j, "ringLog2", c->ringLog2);
+    if (c->ringLog2 != 0 && (c->ringLog2 < 13 || c->ringLog2 > 17))
+      fail(GR_EINVAL, "ringLog2 must be 0 (automatic) or between 13 and 17");
     readMultiColor(j, "solveMulticolor", c->solveMulticolor);
     readMultiColor(j, "factorizeMulticolor", c->factorizeMulticolor);
     readBool(j, "diagonalBased", c->diagonalBased);

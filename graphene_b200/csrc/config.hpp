@@ -43,6 +43,9 @@ struct SolverConfig {
   // Extension: substitution kernel, "auto" (streamed when it fits shared
   // memory), "stream" or "levels" (level-schedule kernel).
   int iluKernel = 0;  // 0 auto, 1 stream, 2 levels
+  // Extension: log2 of the streamed kernel's ring size in bytes (0: the
+  // smallest ring that holds the largest level).
+  int ringLog2 = 0;
   // GaussSeidel (gauss-seidel/Configuration.hpp:19-21)
   int numSweeps = 1, numFixedIterations = 0;
   // Extension: "seed": "b" (default, the codelet specification

@@ -104,6 +104,7 @@ struct SweepStream {
   bool dilu = false;
   i64 bytes = 0;
   i64 maxLevelBytes = 0;
+  i64 maxSpanBytes = 0;  // largest span of two consecutive levels (ring sizing)
   i64 nVal = 0, nInv = 0;
   DBuf tileOffset;  // i64[P + 1]
   DBuf templ;       // bytes
@@ -116,12 +117,17 @@ struct HostStream {
   std::vector<i64> tileOffset;
   std::vector<i32> valPos, valSrc, invPos, invSrc;
   i64 maxLevelBytes = 0;
+  // Largest distance from the start of a level (the tile header for the
+  // first) to the end of the next level: the streamed kernel keeps two
+  // consecutive levels in its ring.
+  i64 maxSpanBytes = 0;
 };
 // Chunks of the streamed kernel's shared-memory ring.
 constexpr int kRingChunksHost = 8;
 HostStream buildIluStream(const HostMatrix& H, bool dilu, DType vt);
-// log2 of the ring size the streamed kernel uses for a given largest level.
-int ringLog2ForLevel(i64 maxLevelBytes);
+// log2 of the ring size the streamed kernel uses for a given largest
+// two-level span.
+int ringLog2ForLevel(i64 maxSpanBytes);
 // Replays the streamed kernel's reads on the host; throws GR_EINVAL on any
 // out-of-range index, ordering or ring-capacity violation.
 void checkIluStream(const HostMatrix& H, const HostStream& S, bool dilu, DType vt, int ringLog2);

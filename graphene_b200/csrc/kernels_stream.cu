@@ -82,11 +82,23 @@ struct SPro {
   }
 };
 
+constexpr int kStreamThreads = 128;
+
+__device__ __forceinline__ uint32_t pad16u(uint32_t b) { return (b + 15u) & ~15u; }
+
+// One thread block per tile. Per level: every thread computes its rows from
+// shared memory; thread 0 refills the ring slots of chunks that lie wholly
+// before the current level (consumed by earlier levels, which every thread
+// finished before the previous barrier); warp 0 waits until the next
+// level's bytes have landed; one barrier ends the level. The ring therefore
+// has to hold two consecutive levels (the host sizes it from the largest
+// two-level span, see ringLog2ForLevel).
 template <class MV, class W>
-__global__ void __launch_bounds__(256) iluStreamKernel(const unsigned char* __restrict__ stream,
-                                                        const long long* __restrict__ tileOffset,
-                                                        const int* __restrict__ tileStart, int ringLog2, bool dilu,
-                                                        SPro<W> pro, W* __restrict__ y, int* errFlag) {
+__global__ void __launch_bounds__(kStreamThreads) iluStreamKernel(const unsigned char* __restrict__ stream,
+                                                                   const long long* __restrict__ tileOffset,
+                                                                   const int* __restrict__ tileStart, int ringLog2,
+                                                                   bool dilu, SPro<W> pro, W* __restrict__ y,
+                                                                   int* errFlag) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int abortFlag;
   if (pro.st && pro.st->done) return;
@@ -94,22 +106,23 @@ __global__ void __launch_bounds__(256) iluStreamKernel(const unsigned char* __re
   const int base = tileStart[T];
   const int nRows = tileStart[T + 1] - base;
   const long long g0 = tileOffset[T];
-  const long long len = tileOffset[T + 1] - g0;
-  const unsigned ringBytes = 1u << ringLog2;
-  const unsigned mask = ringBytes - 1;
-  const unsigned C = ringBytes / kRingChunks;
+  const uint32_t len = static_cast<uint32_t>(tileOffset[T + 1] - g0);
+  const uint32_t ringBytes = 1u << ringLog2;
+  const uint32_t mask = ringBytes - 1;
+  const uint32_t C = ringBytes / kRingChunks;
   const int total = static_cast<int>((len + C - 1) / C);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
   unsigned char* ring = smem + 128;
   W* xs = reinterpret_cast<W*>(smem + 128 + ringBytes);
   const unsigned char* g = stream + g0;
+  const bool waiter = threadIdx.x < 32;
 
-  int next = 0;  // next chunk to copy (used by thread 0 only)
+  int next = 0;  // next chunk to copy (thread 0)
   auto issue = [&](int c) {
-    const unsigned bytes = static_cast<unsigned>(min(static_cast<long long>(C), len - static_cast<long long>(c) * C));
+    const uint32_t bytes = min(C, len - static_cast<uint32_t>(c) * C);
     const uint32_t bar = smemAddr(bars + (c % kRingChunks));
     mbarExpectTx(bar, bytes);
-    bulkLoad(smemAddr(ring + (c % kRingChunks) * C), g + static_cast<long long>(c) * C, bytes, bar);
+    bulkLoad(smemAddr(ring + (c % kRingChunks) * C), g + static_cast<size_t>(c) * C, bytes, bar);
   };
   if (threadIdx.x == 0) {
     abortFlag = 0;
@@ -133,9 +146,9 @@ __global__ void __launch_bounds__(256) iluStreamKernel(const unsigned char* __re
     for (int i = threadIdx.x; i < nRows; i += blockDim.x) xs[i] = pro(base + i, beta, omega, alpha, first);
   }
 
-  int waited = 0;
+  int waited = 0;  // chunks known to have landed (warp 0)
   bool timedOut = false;
-  auto waitTo = [&](long long endByte) {
+  auto waitTo = [&](uint32_t endByte) {
     const int need = static_cast<int>((endByte + C - 1) / C);
     for (; waited < need && !timedOut; ++waited) {
       const uint32_t bar = smemAddr(bars + (waited % kRingChunks));
@@ -148,11 +161,29 @@ __global__ void __launch_bounds__(256) iluStreamKernel(const unsigned char* __re
         }
     }
   };
-  auto rdInt = [&](long long o) { return *reinterpret_cast<const int*>(ring + (o & mask)); };
-  auto rdVal = [&](long long o) { return *reinterpret_cast<const MV*>(ring + (o & mask)); };
+  auto rdInt = [&](uint32_t o) { return *reinterpret_cast<const int*>(ring + (o & mask)); };
+  auto rdVal = [&](uint32_t o) { return *reinterpret_cast<const MV*>(ring + (o & mask)); };
+  auto levelEnd = [&](uint32_t o) {
+    const int4 h = *reinterpret_cast<const int4*>(ring + (o & mask));
+    const uint32_t k = static_cast<uint32_t>(h.x), E = static_cast<uint32_t>(h.y);
+    const uint32_t rowsOff = o + 16;
+    const uint32_t invOff = rowsOff + pad16u(4u * k);
+    const uint32_t colsOff = invOff + (h.z ? pad16u(static_cast<uint32_t>(sizeof(MV)) * k) : 0u);
+    const uint32_t valsOff = colsOff + pad16u(4u * E * k);
+    return valsOff + pad16u(static_cast<uint32_t>(sizeof(MV)) * E * k);
+  };
 
-  waitTo(16);
-  if (timedOut) abortFlag = 1;
+  if (waiter) {
+    waitTo(16);
+    if (!timedOut) {
+      const int4 th = *reinterpret_cast<const int4*>(ring);
+      if (th.x + th.y > 0) {
+        waitTo(32);
+        if (!timedOut) waitTo(levelEnd(16));
+      }
+    }
+    if (timedOut) abortFlag = 1;
+  }
   __syncthreads();
   int nL = 0, nU = 0;
   if (!abortFlag) {
@@ -160,62 +191,57 @@ __global__ void __launch_bounds__(256) iluStreamKernel(const unsigned char* __re
     nL = th.x;
     nU = th.y;
   }
-  long long off = 16;
-  for (int lv = 0; lv < nL + nU && !abortFlag; ++lv) {
-    const bool upper = lv >= nL;
-    waitTo(off + 16);
-    int k = 0, E = 0;
-    bool hasInv = false;
-    if (!timedOut) {
-      const int4 h = *reinterpret_cast<const int4*>(ring + (off & mask));
-      k = h.x;
-      E = h.y;
-      hasInv = h.z != 0;
-    }
-    const long long rowsOff = off + 16;
-    const long long invOff = rowsOff + pad16(4ll * k);
-    const long long colsOff = invOff + (hasInv ? pad16(static_cast<long long>(sizeof(MV)) * k) : 0);
-    const long long valsOff = colsOff + pad16(4ll * E * k);
-    const long long end = valsOff + pad16(static_cast<long long>(sizeof(MV)) * E * k);
-    waitTo(end);
-    if (timedOut) {
-      abortFlag = 1;
-    } else if (!upper) {
+  uint32_t off = 16;
+  for (int lv = 0; lv < nL + nU; ++lv) {
+    const int4 h = *reinterpret_cast<const int4*>(ring + (off & mask));
+    const int k = h.x, E = h.y;
+    const uint32_t rowsOff = off + 16;
+    const uint32_t invOff = rowsOff + pad16u(4u * k);
+    const uint32_t colsOff = invOff + (h.z ? pad16u(static_cast<uint32_t>(sizeof(MV)) * k) : 0u);
+    const uint32_t valsOff = colsOff + pad16u(4u * E * k);
+    const uint32_t end = valsOff + pad16u(static_cast<uint32_t>(sizeof(MV)) * E * k);
+    const uint32_t colStride = 4u * k, valStride = static_cast<uint32_t>(sizeof(MV)) * k;
+    if (lv < nL) {
       // Forward substitution (ilu/Solver.cpp:380-411).
       for (int q = threadIdx.x; q < k; q += blockDim.x) {
-        const int il = rdInt(rowsOff + 4ll * q);
+        const int il = rdInt(rowsOff + 4u * q);
         W temp = xs[il];
-        for (int e = 0; e < E; ++e) {
-          const long long s = static_cast<long long>(e) * k + q;
-          const int c = rdInt(colsOff + 4 * s);
+        uint32_t co = colsOff + 4u * q, vo = valsOff + static_cast<uint32_t>(sizeof(MV)) * q;
+        for (int e = 0; e < E; ++e, co += colStride, vo += valStride) {
+          const int c = rdInt(co);
           if (c < 0) break;
-          temp = sub(temp, mul(cvt<W>(rdVal(valsOff + sizeof(MV) * s)), xs[c]));
+          temp = sub(temp, mul(cvt<W>(rdVal(vo)), xs[c]));
         }
-        xs[il] = dilu ? mul(temp, cvt<W>(rdVal(invOff + sizeof(MV) * q))) : temp;
+        xs[il] = dilu ? mul(temp, cvt<W>(rdVal(invOff + static_cast<uint32_t>(sizeof(MV)) * q))) : temp;
       }
     } else {
       // Backward substitution (ilu/Solver.cpp:413-442).
       for (int q = threadIdx.x; q < k; q += blockDim.x) {
-        const int il = rdInt(rowsOff + 4ll * q);
+        const int il = rdInt(rowsOff + 4u * q);
         W temp = W(0);
-        for (int e = 0; e < E; ++e) {
-          const long long s = static_cast<long long>(e) * k + q;
-          const int c = rdInt(colsOff + 4 * s);
+        uint32_t co = colsOff + 4u * q, vo = valsOff + static_cast<uint32_t>(sizeof(MV)) * q;
+        for (int e = 0; e < E; ++e, co += colStride, vo += valStride) {
+          const int c = rdInt(co);
           if (c < 0) break;
-          temp = sub(temp, mul(cvt<W>(rdVal(valsOff + sizeof(MV) * s)), xs[c]));
+          temp = sub(temp, mul(cvt<W>(rdVal(vo)), xs[c]));
         }
-        const W iv = cvt<W>(rdVal(invOff + sizeof(MV) * q));
+        const W iv = cvt<W>(rdVal(invOff + static_cast<uint32_t>(sizeof(MV)) * q));
         xs[il] = dilu ? add(xs[il], mul(temp, iv)) : mul(add(xs[il], temp), iv);
       }
     }
-    __syncthreads();
-    off = end;
-    if (threadIdx.x == 0 && !abortFlag) {
-      // Chunks below off / C are consumed: refill their ring slots.
+    if (threadIdx.x == 0) {
       fenceProxyAsync();
       const int limit = static_cast<int>(off / C) + kRingChunks;
       for (; next < total && next < limit; ++next) issue(next);
     }
+    if (waiter && lv + 1 < nL + nU) {
+      waitTo(end + 16);
+      if (!timedOut) waitTo(levelEnd(end));
+      if (timedOut) abortFlag = 1;
+    }
+    __syncthreads();
+    if (abortFlag) break;
+    off = end;
   }
   if (abortFlag) {
     if (threadIdx.x == 0) {
@@ -252,13 +278,14 @@ __global__ void streamPackKernel(MV* __restrict__ stream, const int* __restrict_
 // ---------------------------------------------------------------------------
 static_assert(dev::kRingChunks == kRingChunksHost, "ring geometry shared with the host checker");
 
-namespace {
-int ringLog2For(i64 maxLevelBytes) { return ringLog2ForLevel(maxLevelBytes); }
-}  // namespace
+int iluStreamRingLog2(const SweepStream& S, int requested) {
+  const int need = ringLog2ForLevel(S.maxSpanBytes);
+  return requested > need ? requested : need;
+}
 
-size_t iluStreamSmem(const DeviceMatrix& A, const SweepStream& S, DType W) {
-  const int lg = ringLog2For(S.maxLevelBytes);
-  if (lg > 16) return 0;  // rings above 64 KB: use the level-schedule kernel
+size_t iluStreamSmem(const DeviceMatrix& A, const SweepStream& S, DType W, int ringLog2) {
+  const int lg = iluStreamRingLog2(S, ringLog2);
+  if (lg > 17) return 0;    // rings above 128 KB: use the level-schedule kernel
   return 128 + (size_t(1) << lg) + static_cast<size_t>(A.host->maxTileRows) * dtypeSize(W);
 }
 
@@ -281,9 +308,9 @@ void launchStreamPack(DeviceMatrix& A, const SweepStream& S, void* stream, const
 namespace {
 template <class MV, class W>
 void streamApplyT(DeviceMatrix& A, const SweepStream& S, const void* stream, bool dilu, const PrologueArgs& p,
-                  void* y, cudaStream_t s) {
-  const int lg = ringLog2For(S.maxLevelBytes);
-  const size_t smem = iluStreamSmem(A, S, dtypeOf<W>());
+                  void* y, int ringLog2, cudaStream_t s) {
+  const int lg = iluStreamRingLog2(S, ringLog2);
+  const size_t smem = iluStreamSmem(A, S, dtypeOf<W>(), ringLog2);
   auto kernel = dev::iluStreamKernel<MV, W>;
   static thread_local size_t configured[4] = {0, 0, 0, 0};
   const int slot = (sizeof(MV) == 8) * 2 + (sizeof(W) == 8);
@@ -293,17 +320,19 @@ void streamApplyT(DeviceMatrix& A, const SweepStream& S, const void* stream, boo
   }
   dev::SPro<W> pro{static_cast<int>(p.kind), static_cast<const W*>(p.b), static_cast<const W*>(p.r),
                    static_cast<W*>(p.pOrS), static_cast<const W*>(p.v), p.st};
-  kernel<<<A.P, 256, smem, s>>>(static_cast<const unsigned char*>(stream), S.tileOffset.as<long long>(),
+  kernel<<<A.P, dev::kStreamThreads, smem, s>>>(static_cast<const unsigned char*>(stream), S.tileOffset.as<long long>(),
                                 A.tileStart.as<int>(), lg, dilu, pro, static_cast<W*>(y), A.errFlag.as<int>());
   checkLaunch("ilu_stream");
 }
 }  // namespace
 
 void launchIluStream(DeviceMatrix& A, const SweepStream& S, const void* stream, bool dilu,
-                     const PrologueArgs& pro, void* y, DType W, cudaStream_t s) {
-  if (A.vt == DType::F32 && W == DType::F32) streamApplyT<float, float>(A, S, stream, dilu, pro, y, s);
-  else if (A.vt == DType::F32 && W == DType::F64) streamApplyT<float, double>(A, S, stream, dilu, pro, y, s);
-  else if (A.vt == DType::F64 && W == DType::F64) streamApplyT<double, double>(A, S, stream, dilu, pro, y, s);
+                     const PrologueArgs& pro, void* y, DType W, int ringLog2, cudaStream_t s) {
+  if (A.vt == DType::F32 && W == DType::F32) streamApplyT<float, float>(A, S, stream, dilu, pro, y, ringLog2, s);
+  else if (A.vt == DType::F32 && W == DType::F64)
+    streamApplyT<float, double>(A, S, stream, dilu, pro, y, ringLog2, s);
+  else if (A.vt == DType::F64 && W == DType::F64)
+    streamApplyT<double, double>(A, S, stream, dilu, pro, y, ringLog2, s);
   else fail(GR_EUNSUPPORTED, "ILU with float64 coefficients needs float64 vectors");
 }
 

@@ -55,12 +55,14 @@ void launchIluApply(DeviceMatrix& A, const void* Lval, const void* Uval, const v
 // Streamed substitution (kernels_stream.cu). iluStreamSmem returns the
 // dynamic shared memory a launch with vector type W needs, 0 if the
 // matrix's levels are too large for the ring.
-size_t iluStreamSmem(const DeviceMatrix& A, const SweepStream& S, DType W);
+// ringLog2: requested ring size (0 = the smallest that fits).
+size_t iluStreamSmem(const DeviceMatrix& A, const SweepStream& S, DType W, int ringLog2 = 0);
+int iluStreamRingLog2(const SweepStream& S, int requested);
 // stream = template with the factor values F and inverse diagonal inv packed in.
 void launchStreamPack(DeviceMatrix& A, const SweepStream& S, void* stream, const void* F, const void* inv,
                       cudaStream_t s);
 void launchIluStream(DeviceMatrix& A, const SweepStream& S, const void* stream, bool dilu,
-                     const PrologueArgs& pro, void* y, DType W, cudaStream_t s);
+                     const PrologueArgs& pro, void* y, DType W, int ringLog2, cudaStream_t s);
 int maxDynamicSmem(const DeviceMatrix& A);
 
 // ---- Gauss-Seidel -------------------------------------------------------

@@ -135,6 +135,8 @@ struct TileBytes {
   std::vector<std::pair<i64, i32>> vals;  // (byte offset in tile stream, CRS source or -1)
   std::vector<std::pair<i64, i32>> invs;  // (byte offset, tile-order row)
   i64 maxLevel = 0;
+  i64 maxSpan = 0;
+  std::vector<i64> levelStart;  // byte offset of every level header, then the end
 };
 
 void putInt4(std::vector<uint8_t>& b, i32 a, i32 c, i32 d, i32 e) {
@@ -172,6 +174,7 @@ HostStream buildIluStream(const HostMatrix& H, bool dilu, DType vt) {
           E = std::max<i64>(E, static_cast<i64>(ent.size()));
         }
         const i64 start = static_cast<i64>(t.bytes.size());
+        t.levelStart.push_back(start);
         putInt4(t.bytes, static_cast<i32>(k), static_cast<i32>(E), hasInv ? 1 : 0, 0);
         const i64 rowsOff = static_cast<i64>(t.bytes.size());
         const i64 invOff = rowsOff + pad16(4 * k);
@@ -196,6 +199,12 @@ HostStream buildIluStream(const HostMatrix& H, bool dilu, DType vt) {
         t.maxLevel = std::max(t.maxLevel, end - start);
       }
     }
+    t.levelStart.push_back(static_cast<i64>(t.bytes.size()));
+    // Spans: tile header through level 0, then level l through level l + 1.
+    const size_t L = t.levelStart.size() - 1;
+    if (L > 0) t.maxSpan = t.levelStart[1];
+    for (size_t l = 0; l + 1 < L; ++l) t.maxSpan = std::max(t.maxSpan, t.levelStart[l + 2] - t.levelStart[l]);
+    if (L == 1) t.maxSpan = std::max(t.maxSpan, t.levelStart[1] - t.levelStart[0]);
     t.bytes.resize(pad16(static_cast<i64>(t.bytes.size())), 0);
   });
   HostStream S;
@@ -204,6 +213,7 @@ HostStream buildIluStream(const HostMatrix& H, bool dilu, DType vt) {
   for (i32 T = 0; T < H.P; ++T) {
     S.tileOffset[T + 1] = S.tileOffset[T] + static_cast<i64>(tb[T].bytes.size());
     S.maxLevelBytes = std::max(S.maxLevelBytes, tb[T].maxLevel);
+    S.maxSpanBytes = std::max(S.maxSpanBytes, tb[T].maxSpan);
     nVal += static_cast<i64>(tb[T].vals.size());
     nInv += static_cast<i64>(tb[T].invs.size());
   }
@@ -246,8 +256,10 @@ int ringLog2ForLevel(i64 maxLevelBytes) {
 // Replays the streamed kernel's consumption of every tile's stream on the
 // host: headers and segment offsets, index ranges, the level order each
 // entry depends on, and that every chunk a level needs has been issued under
-// the producer's refill rule (after a level ending at byte `off`, chunks
-// below off / C + R are in flight). Throws on the first violation.
+// the producer's refill rule: before waiting for level l + 1, thread 0 has
+// issued every chunk below start(l) / C + R (start(l) = byte offset of level
+// l's header); before the loop, chunks 0 .. R - 1. Throws on the first
+// violation.
 void checkIluStream(const HostMatrix& H, const HostStream& S, bool dilu, DType vt, int ringLog2) {
   const i64 vs = static_cast<i64>(dtypeSize(vt));
   const i64 ring = i64(1) << ringLog2, C = ring / kRingChunksHost;
@@ -276,9 +288,10 @@ void checkIluStream(const HostMatrix& H, const HostStream& S, bool dilu, DType v
     const i32 nL = rd(0), nU = rd(4);
     if (nL != H.nLowerLevels[T] || nU != H.nUpperLevels[T]) bad("level counts");
     std::vector<i32> doneLower(nRows, -1), doneUpper(nRows, -1);
-    i64 off = 16;
+    i64 off = 16, prevStart = -1;
     for (i32 lv = 0; lv < nL + nU; ++lv) {
       const bool upper = lv >= nL;
+      if (lv > 0) issued = std::min<i64>(total, prevStart / C + kRingChunksHost);
       needChunks(off + 16);
       const i64 k = rd(off), E = rd(off + 4);
       const bool hasInv = rd(off + 8) != 0;
@@ -310,8 +323,8 @@ void checkIluStream(const HostMatrix& H, const HostStream& S, bool dilu, DType v
         }
       }
       for (i64 q = 0; q < k; ++q) (upper ? doneUpper : doneLower)[rd(rowsOff + 4 * q)] = lv;
+      prevStart = off;
       off = end;
-      issued = std::min<i64>(total, off / C + kRingChunksHost);
     }
     if (off != len) bad("stream length does not match its levels");
     for (i64 i = 0; i < nRows; ++i)
@@ -327,6 +340,7 @@ SweepStream& DeviceMatrix::iluSweepStream(bool dilu) {
   S->dilu = dilu;
   S->bytes = static_cast<i64>(H.bytes.size());
   S->maxLevelBytes = H.maxLevelBytes;
+  S->maxSpanBytes = H.maxSpanBytes;
   S->nVal = static_cast<i64>(H.valPos.size());
   S->nInv = static_cast<i64>(H.invPos.size());
   S->tileOffset.upload(H.tileOffset);

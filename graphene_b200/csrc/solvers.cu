@@ -78,7 +78,7 @@ class IluNode : public Node {
     bool useStream = false;
     if (c.iluKernel != 2) {
       SweepStream& S = A.iluSweepStream(dilu_);
-      const size_t need = iluStreamSmem(A, S, DType::F64);
+      const size_t need = iluStreamSmem(A, S, DType::F64, c.ringLog2);
       useStream = need > 0 && need <= static_cast<size_t>(maxDynamicSmem(A));
       if (!useStream && c.iluKernel == 1)
         fail(GR_EUNSUPPORTED, "the streamed ILU kernel does not fit this matrix's tiles in shared memory");
@@ -108,8 +108,8 @@ class IluNode : public Node {
     return st;
   }
   void apply(const PrologueArgs& pro, void* y, DType W) {
-    if (sweep_ && iluStreamSmem(A_, *sweep_, W) <= static_cast<size_t>(maxDynamicSmem(A_)))
-      launchIluStream(A_, *sweep_, stream_.get(), dilu_, pro, y, W, s());
+    if (sweep_ && iluStreamSmem(A_, *sweep_, W, cfg_.ringLog2) <= static_cast<size_t>(maxDynamicSmem(A_)))
+      launchIluStream(A_, *sweep_, stream_.get(), dilu_, pro, y, W, cfg_.ringLog2, s());
     else if (sweep_)
       fail(GR_EUNSUPPORTED, "ILU stream does not fit shared memory for this vector type");
     else
