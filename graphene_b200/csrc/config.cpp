@@ -254,9 +254,10 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
     readBool(j, "diagonalBased", c->diagonalBased);
     if (const Json* v = j.find("kernel")) {
       if (v->text == "auto") c->iluKernel = 0;
-      else if (v->text == "stream") c->iluKernel = 1;
+      else if (v->text == "tma") c->iluKernel = 1;
       else if (v->text == "levels") c->iluKernel = 2;
-      else fail(GR_EPARSE, "ILU kernel must be \"auto\", \"stream\" or \"levels\"");
+      else if (v->text == "warp") c->iluKernel = 3;
+      else fail(GR_EPARSE, "ILU kernel must be \"auto\", \"warp\", \"tma\" or \"levels\"");
     }
   } else if (ty == "GaussSeidel") {
     mark("numSweeps"); mark("numFixedIterations"); mark("solveMulticolor"); mark("workingType");

@@ -40,9 +40,10 @@ struct SolverConfig {
   MultiColorMode solveMulticolor = MultiColorMode::Auto;
   MultiColorMode factorizeMulticolor = MultiColorMode::Auto;
   bool diagonalBased = false;
-  // Extension: substitution kernel, "auto" (streamed when it fits shared
-  // memory), "stream" or "levels" (level-schedule kernel).
-  int iluKernel = 0;  // 0 auto, 1 stream, 2 levels
+  // Extension: substitution kernel, "auto" (warp per tile when the tile fits
+  // shared memory, else the level-schedule kernel), "warp", "tma" (bulk-copy
+  // ring) or "levels".
+  int iluKernel = 0;  // 0 auto, 1 tma, 2 levels, 3 warp
   // Extension: log2 of the streamed kernel's ring size in bytes (0: the
   // smallest ring that holds the largest level).
   int ringLog2 = 0;

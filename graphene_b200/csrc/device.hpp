@@ -109,6 +109,14 @@ struct SweepStream {
   DBuf tileOffset;  // i64[P + 1]
   DBuf templ;       // bytes
   DBuf valPos, valSrc, invPos, invSrc;  // i32
+  // Level table: per level int4 {byte offset of its header in the tile's
+  // stream, k, E, hasInv}; tile T's levels are [tileLevel[T], tileLevel[T+1]).
+  DBuf levelTable;  // int4
+  DBuf tileLevel;   // i32[P + 1]
+  i64 numLevels = 0;
+  i32 maxTileLevels = 0;
+  i32 maxLevelRows = 0;
+  i32 maxEntries = 0;
 };
 
 // Host copy of a SweepStream (built on the host, then uploaded).
@@ -121,6 +129,9 @@ struct HostStream {
   // first) to the end of the next level: the streamed kernel keeps two
   // consecutive levels in its ring.
   i64 maxSpanBytes = 0;
+  std::vector<int4> levelTable;  // see SweepStream::levelTable
+  std::vector<i32> tileLevel;
+  i32 maxTileLevels = 0, maxLevelRows = 0, maxEntries = 0;
 };
 // Chunks of the streamed kernel's shared-memory ring.
 constexpr int kRingChunksHost = 8;

@@ -64,6 +64,12 @@ void launchStreamPack(DeviceMatrix& A, const SweepStream& S, void* stream, const
 void launchIluStream(DeviceMatrix& A, const SweepStream& S, const void* stream, bool dilu,
                      const PrologueArgs& pro, void* y, DType W, int ringLog2, cudaStream_t s);
 int maxDynamicSmem(const DeviceMatrix& A);
+// Warp-per-tile substitution (kernels_warp.cu): shared memory per block and
+// the number of rows per lane to prefetch.
+size_t iluWarpSmem(const DeviceMatrix& A, const SweepStream& S, DType W);
+int iluWarpRowsPerLane(const DeviceMatrix& A, const SweepStream& S);
+void launchIluWarp(DeviceMatrix& A, const SweepStream& S, const void* stream, bool dilu, const PrologueArgs& pro,
+                   void* y, DType W, int J, cudaStream_t s);
 
 // ---- Gauss-Seidel -------------------------------------------------------
 // One sweep: xout from xin (xin may alias nothing; must differ from xout).

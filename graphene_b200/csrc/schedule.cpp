@@ -137,6 +137,7 @@ struct TileBytes {
   i64 maxLevel = 0;
   i64 maxSpan = 0;
   std::vector<i64> levelStart;  // byte offset of every level header, then the end
+  std::vector<int4> table;      // {offset, k, E, hasInv} per level
 };
 
 void putInt4(std::vector<uint8_t>& b, i32 a, i32 c, i32 d, i32 e) {
@@ -175,6 +176,7 @@ HostStream buildIluStream(const HostMatrix& H, bool dilu, DType vt) {
         }
         const i64 start = static_cast<i64>(t.bytes.size());
         t.levelStart.push_back(start);
+        t.table.push_back(make_int4(static_cast<int>(start), static_cast<int>(k), static_cast<int>(E), hasInv ? 1 : 0));
         putInt4(t.bytes, static_cast<i32>(k), static_cast<i32>(E), hasInv ? 1 : 0, 0);
         const i64 rowsOff = static_cast<i64>(t.bytes.size());
         const i64 invOff = rowsOff + pad16(4 * k);
@@ -214,8 +216,18 @@ HostStream buildIluStream(const HostMatrix& H, bool dilu, DType vt) {
     S.tileOffset[T + 1] = S.tileOffset[T] + static_cast<i64>(tb[T].bytes.size());
     S.maxLevelBytes = std::max(S.maxLevelBytes, tb[T].maxLevel);
     S.maxSpanBytes = std::max(S.maxSpanBytes, tb[T].maxSpan);
+    S.maxTileLevels = std::max<i32>(S.maxTileLevels, static_cast<i32>(tb[T].table.size()));
+    for (const int4& d : tb[T].table) {
+      S.maxLevelRows = std::max<i32>(S.maxLevelRows, d.y);
+      S.maxEntries = std::max<i32>(S.maxEntries, d.z);
+    }
     nVal += static_cast<i64>(tb[T].vals.size());
     nInv += static_cast<i64>(tb[T].invs.size());
+  }
+  S.tileLevel.assign(H.P + 1, 0);
+  for (i32 T = 0; T < H.P; ++T) {
+    S.tileLevel[T + 1] = S.tileLevel[T] + static_cast<i32>(tb[T].table.size());
+    S.levelTable.insert(S.levelTable.end(), tb[T].table.begin(), tb[T].table.end());
   }
   const i64 total = S.tileOffset[H.P];
   if (total / vs >= (i64(1) << 31)) fail(GR_EUNSUPPORTED, "ILU stream exceeds 2^31 elements");
@@ -297,6 +309,9 @@ void checkIluStream(const HostMatrix& H, const HostStream& S, bool dilu, DType v
       const bool hasInv = rd(off + 8) != 0;
       if (k <= 0 || E < 0) bad("empty level");
       if (hasInv != (upper || dilu)) bad("inverse-diagonal flag");
+      if (S.tileLevel[T + 1] - S.tileLevel[T] != nL + nU) bad("level table size");
+      const int4 d = S.levelTable[S.tileLevel[T] + lv];
+      if (d.x != off || d.y != k || d.z != E || d.w != (hasInv ? 1 : 0)) bad("level table entry");
       const i64 rowsOff = off + 16;
       const i64 invOff = rowsOff + pad16(4 * k);
       const i64 colsOff = invOff + (hasInv ? pad16(vs * k) : 0);
@@ -341,6 +356,12 @@ SweepStream& DeviceMatrix::iluSweepStream(bool dilu) {
   S->bytes = static_cast<i64>(H.bytes.size());
   S->maxLevelBytes = H.maxLevelBytes;
   S->maxSpanBytes = H.maxSpanBytes;
+  S->levelTable.upload(H.levelTable);
+  S->tileLevel.upload(H.tileLevel);
+  S->numLevels = static_cast<i64>(H.levelTable.size());
+  S->maxTileLevels = H.maxTileLevels;
+  S->maxLevelRows = H.maxLevelRows;
+  S->maxEntries = H.maxEntries;
   S->nVal = static_cast<i64>(H.valPos.size());
   S->nInv = static_cast<i64>(H.invPos.size());
   S->tileOffset.upload(H.tileOffset);

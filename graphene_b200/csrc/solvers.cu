@@ -75,17 +75,25 @@ class IluNode : public Node {
     const void* vals = dilu_ ? A.offDiag.get() : F.get();
     // Streamed substitution when the ring and the tile slice fit in shared
     // memory for either vector type; the level-schedule kernel otherwise.
-    bool useStream = false;
+    // Substitution kernel: warp-per-tile over the tile byte stream (auto /
+    // "warp"), the bulk-copy ring kernel ("tma"), or the level-schedule
+    // kernel ("levels", and auto when a tile does not fit shared memory).
+    kernel_ = 2;
     if (c.iluKernel != 2) {
       SweepStream& S = A.iluSweepStream(dilu_);
-      const size_t need = iluStreamSmem(A, S, DType::F64, c.ringLog2);
-      useStream = need > 0 && need <= static_cast<size_t>(maxDynamicSmem(A));
-      if (!useStream && c.iluKernel == 1)
-        fail(GR_EUNSUPPORTED, "the streamed ILU kernel does not fit this matrix's tiles in shared memory");
+      const size_t smemMax = static_cast<size_t>(maxDynamicSmem(A));
+      const bool warpFits = iluWarpSmem(A, S, DType::F64) <= smemMax;
+      const size_t tmaNeed = iluStreamSmem(A, S, DType::F64, c.ringLog2);
+      const bool tmaFits = tmaNeed > 0 && tmaNeed <= smemMax;
+      if (c.iluKernel == 0) kernel_ = warpFits ? 3 : 2;
+      else if (c.iluKernel == 3 && warpFits) kernel_ = 3;
+      else if (c.iluKernel == 1 && tmaFits) kernel_ = 1;
+      else fail(GR_EUNSUPPORTED, "the requested ILU kernel does not fit this matrix's tiles in shared memory");
     }
-    if (useStream) {
+    if (kernel_ != 2) {
       SweepStream& S = A.iluSweepStream(dilu_);
       sweep_ = &S;
+      rowsPerLane_ = iluWarpRowsPerLane(A, S);
       stream_.alloc(std::max<i64>(16, S.bytes));
       launchStreamPack(A, S, stream_.get(), vals, inv_.get(), s());
     } else {
@@ -108,10 +116,10 @@ class IluNode : public Node {
     return st;
   }
   void apply(const PrologueArgs& pro, void* y, DType W) {
-    if (sweep_ && iluStreamSmem(A_, *sweep_, W, cfg_.ringLog2) <= static_cast<size_t>(maxDynamicSmem(A_)))
+    if (kernel_ == 3)
+      launchIluWarp(A_, *sweep_, stream_.get(), dilu_, pro, y, W, rowsPerLane_, s());
+    else if (kernel_ == 1)
       launchIluStream(A_, *sweep_, stream_.get(), dilu_, pro, y, W, cfg_.ringLog2, s());
-    else if (sweep_)
-      fail(GR_EUNSUPPORTED, "ILU stream does not fit shared memory for this vector type");
     else
       launchIluApply(A_, Lval_.get(), Uval_.get(), inv_.get(), dilu_, pro, y, W, s());
   }
@@ -119,6 +127,8 @@ class IluNode : public Node {
 
  private:
   bool dilu_;
+  int kernel_ = 2;  // 1 tma ring, 2 level schedule, 3 warp per tile
+  int rowsPerLane_ = 2;
   DBuf inv_, Lval_, Uval_, stream_;
   const SweepStream* sweep_ = nullptr;
 };

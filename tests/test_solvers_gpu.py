@@ -54,7 +54,7 @@ NAMES = ["poisson16", "poisson_odd_bfs", "poisson_1tile", "random", "many_tiles"
 
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("dilu", [False, True])
-@pytest.mark.parametrize("kernel", ["stream", "levels"])
+@pytest.mark.parametrize("kernel", ["warp", "tma", "levels"])
 def test_ilu_bit_exact(oracle, name, dilu, kernel):
     h, om = case(name, oracle)
     A = h.copyToTile()
@@ -66,7 +66,7 @@ def test_ilu_bit_exact(oracle, name, dilu, kernel):
 
 
 @pytest.mark.parametrize("name", ["poisson16", "random"])
-@pytest.mark.parametrize("kernel", ["stream", "levels"])
+@pytest.mark.parametrize("kernel", ["warp", "tma", "levels"])
 def test_ilu_bit_exact_float64(oracle, name, kernel):
     h, om = case(name, oracle, gb.FLOAT64)
     A = h.copyToTile()
@@ -111,6 +111,7 @@ def test_gauss_seidel_converges_with_checks(oracle):
 PCFG = {
     "ilu": {"type": "ILU"},
     "ilu_levels": {"type": "ILU", "kernel": "levels"},
+    "ilu_tma": {"type": "ILU", "kernel": "tma"},
     "dilu": {"type": "ILU", "diagonalBased": True},
     "gs2": {"type": "GaussSeidel", "numFixedIterations": 2},
     "none": None,
