@@ -40,9 +40,9 @@ struct SolverConfig {
   MultiColorMode solveMulticolor = MultiColorMode::Auto;
   MultiColorMode factorizeMulticolor = MultiColorMode::Auto;
   bool diagonalBased = false;
-  // Extension: substitution kernel, "auto" (warp per tile when the tile fits
-  // shared memory, else the level-schedule kernel), "warp", "tma" (bulk-copy
-  // ring) or "levels".
+  // Extension: substitution kernel, "auto" (the bulk-copy ring kernel when
+  // the tile fits shared memory, else the level-schedule kernel), "tma",
+  // "warp" (warp per tile) or "levels".
   int iluKernel = 0;  // 0 auto, 1 tma, 2 levels, 3 warp
   // Extension: log2 of the streamed kernel's ring size in bytes (0: the
   // smallest ring that holds the largest level).

@@ -82,17 +82,19 @@ struct SPro {
   }
 };
 
-constexpr int kStreamThreads = 128;
+// Four compute warps and one producer warp per tile.
+constexpr int kComputeThreads = 128;
+constexpr int kStreamThreads = kComputeThreads + 32;
 
 __device__ __forceinline__ uint32_t pad16u(uint32_t b) { return (b + 15u) & ~15u; }
 
-// One thread block per tile. Per level: every thread computes its rows from
-// shared memory; thread 0 refills the ring slots of chunks that lie wholly
-// before the current level (consumed by earlier levels, which every thread
-// finished before the previous barrier); warp 0 waits until the next
-// level's bytes have landed; one barrier ends the level. The ring therefore
-// has to hold two consecutive levels (the host sizes it from the largest
-// two-level span, see ringLog2ForLevel).
+// One thread block per tile. Per level: the compute warps compute their rows
+// from shared memory while the producer warp refills the ring slots of
+// chunks that lie wholly before the current level (consumed by earlier
+// levels, which every thread finished before the previous barrier) and waits
+// until the next level's bytes have landed; one barrier ends the level. The
+// ring therefore has to hold two consecutive levels (the host sizes it from
+// the largest two-level span, see ringLog2ForLevel).
 template <class MV, class W>
 __global__ void __launch_bounds__(kStreamThreads) iluStreamKernel(const unsigned char* __restrict__ stream,
                                                                    const long long* __restrict__ tileOffset,
@@ -115,22 +117,24 @@ __global__ void __launch_bounds__(kStreamThreads) iluStreamKernel(const unsigned
   unsigned char* ring = smem + 128;
   W* xs = reinterpret_cast<W*>(smem + 128 + ringBytes);
   const unsigned char* g = stream + g0;
-  const bool waiter = threadIdx.x < 32;
+  const bool waiter = threadIdx.x >= kComputeThreads;      // the producer warp
+  const bool producer = threadIdx.x == kComputeThreads;    // its lane 0 issues copies
+  const bool computer = threadIdx.x < kComputeThreads;
 
-  int next = 0;  // next chunk to copy (thread 0)
+  int next = 0;  // next chunk to copy (producer lane)
   auto issue = [&](int c) {
     const uint32_t bytes = min(C, len - static_cast<uint32_t>(c) * C);
     const uint32_t bar = smemAddr(bars + (c % kRingChunks));
     mbarExpectTx(bar, bytes);
     bulkLoad(smemAddr(ring + (c % kRingChunks) * C), g + static_cast<size_t>(c) * C, bytes, bar);
   };
-  if (threadIdx.x == 0) {
+  if (producer) {
     abortFlag = 0;
     for (int r = 0; r < kRingChunks; ++r) mbarInit(smemAddr(bars + r), 1);
     fenceBarrierInit();
   }
   __syncthreads();
-  if (threadIdx.x == 0)
+  if (producer)
     for (; next < total && next < kRingChunks; ++next) issue(next);
 
   // Prologue into the tile's slice of x (overlaps the first copies).
@@ -201,9 +205,22 @@ __global__ void __launch_bounds__(kStreamThreads) iluStreamKernel(const unsigned
     const uint32_t valsOff = colsOff + pad16u(4u * E * k);
     const uint32_t end = valsOff + pad16u(static_cast<uint32_t>(sizeof(MV)) * E * k);
     const uint32_t colStride = 4u * k, valStride = static_cast<uint32_t>(sizeof(MV)) * k;
-    if (lv < nL) {
+    if (!computer) {
+      // The producer warp: refill consumed ring slots, then wait until the
+      // next level has landed.
+      if (producer) {
+        const int limit = static_cast<int>(off / C) + kRingChunks;
+        if (next < total && next < limit) fenceProxyAsync();
+        for (; next < total && next < limit; ++next) issue(next);
+      }
+      if (lv + 1 < nL + nU) {
+        waitTo(end + 16);
+        if (!timedOut) waitTo(levelEnd(end));
+        if (timedOut) abortFlag = 1;
+      }
+    } else if (lv < nL) {
       // Forward substitution (ilu/Solver.cpp:380-411).
-      for (int q = threadIdx.x; q < k; q += blockDim.x) {
+      for (int q = threadIdx.x; q < k; q += kComputeThreads) {
         const int il = rdInt(rowsOff + 4u * q);
         W temp = xs[il];
         uint32_t co = colsOff + 4u * q, vo = valsOff + static_cast<uint32_t>(sizeof(MV)) * q;
@@ -216,7 +233,7 @@ __global__ void __launch_bounds__(kStreamThreads) iluStreamKernel(const unsigned
       }
     } else {
       // Backward substitution (ilu/Solver.cpp:413-442).
-      for (int q = threadIdx.x; q < k; q += blockDim.x) {
+      for (int q = threadIdx.x; q < k; q += kComputeThreads) {
         const int il = rdInt(rowsOff + 4u * q);
         W temp = W(0);
         uint32_t co = colsOff + 4u * q, vo = valsOff + static_cast<uint32_t>(sizeof(MV)) * q;
@@ -229,22 +246,12 @@ __global__ void __launch_bounds__(kStreamThreads) iluStreamKernel(const unsigned
         xs[il] = dilu ? add(xs[il], mul(temp, iv)) : mul(add(xs[il], temp), iv);
       }
     }
-    if (threadIdx.x == 0) {
-      fenceProxyAsync();
-      const int limit = static_cast<int>(off / C) + kRingChunks;
-      for (; next < total && next < limit; ++next) issue(next);
-    }
-    if (waiter && lv + 1 < nL + nU) {
-      waitTo(end + 16);
-      if (!timedOut) waitTo(levelEnd(end));
-      if (timedOut) abortFlag = 1;
-    }
     __syncthreads();
     if (abortFlag) break;
     off = end;
   }
   if (abortFlag) {
-    if (threadIdx.x == 0) {
+    if (producer) {
       atomicExch(errFlag, GR_ETIMEOUT);
       // Let the copies already issued land before the block's shared
       // memory is released (bounded).

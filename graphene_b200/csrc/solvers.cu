@@ -75,9 +75,10 @@ class IluNode : public Node {
     const void* vals = dilu_ ? A.offDiag.get() : F.get();
     // Streamed substitution when the ring and the tile slice fit in shared
     // memory for either vector type; the level-schedule kernel otherwise.
-    // Substitution kernel: warp-per-tile over the tile byte stream (auto /
-    // "warp"), the bulk-copy ring kernel ("tma"), or the level-schedule
-    // kernel ("levels", and auto when a tile does not fit shared memory).
+    // Substitution kernel: the bulk-copy ring kernel over the tile byte
+    // stream (auto / "tma"), warp-per-tile over the same stream ("warp"), or
+    // the level-schedule kernel ("levels", and auto when a tile does not fit
+    // shared memory).
     kernel_ = 2;
     if (c.iluKernel != 2) {
       SweepStream& S = A.iluSweepStream(dilu_);
@@ -85,7 +86,7 @@ class IluNode : public Node {
       const bool warpFits = iluWarpSmem(A, S, DType::F64) <= smemMax;
       const size_t tmaNeed = iluStreamSmem(A, S, DType::F64, c.ringLog2);
       const bool tmaFits = tmaNeed > 0 && tmaNeed <= smemMax;
-      if (c.iluKernel == 0) kernel_ = warpFits ? 3 : 2;
+      if (c.iluKernel == 0) kernel_ = tmaFits ? 1 : 2;
       else if (c.iluKernel == 3 && warpFits) kernel_ = 3;
       else if (c.iluKernel == 1 && tmaFits) kernel_ = 1;
       else fail(GR_EUNSUPPORTED, "the requested ILU kernel does not fit this matrix's tiles in shared memory");
