@@ -517,14 +517,15 @@ void stripHalo(const or_matrix& A, const std::vector<T>& v, T* tileOrdered) {
 // receives the owner's current values.
 template <class T>
 void exchange(const or_matrix& A, std::vector<T>& v) {
-  for (size_t t = 0; t < A.P; ++t) {
+  // Destination tiles write disjoint halo slots and read owned slots only.
+  forTiles(A.P, [&](size_t t) {
     const Tile& dst = A.tiles[t];
     for (auto& h : dst.halo) {
       const Tile& src = A.tiles[h->src->proc];
       for (size_t g : h->cells)
         v[A.haloStart[t] + dst.g2l.at(g)] = v[A.haloStart[src.id] + src.g2l.at(g)];
     }
-  }
+  });
 }
 
 // Conversion helpers mirroring Value::cast.
@@ -603,11 +604,14 @@ void residualDw(const or_matrix& A, const TileValues<float>& tv, std::vector<X>&
 }
 
 // Matrix::vectorNorm (MatrixBase.cpp:149-152, Tensor.cpp:425-439) on the
-// non-halo cells, FP64 accumulation in tile order.
+// non-halo cells, FP64 accumulation: a partial per tile (tiles in parallel),
+// then the partials in tile order, so the result does not depend on the
+// number of threads.
 template <class T>
 double normT(const or_matrix& A, const std::vector<T>& v, int norm) {
-  double acc = norm == 2 ? -INFINITY : 0.0;
-  for (size_t t = 0; t < A.P; ++t) {
+  std::vector<double> part(A.P);
+  forTiles(A.P, [&](size_t t) {
+    double acc = norm == 2 ? -INFINITY : 0.0;
     size_t nr = A.tileStart[t + 1] - A.tileStart[t];
     for (size_t i = 0; i < nr; ++i) {
       double x = static_cast<double>(v[A.haloStart[t] + i]);
@@ -615,18 +619,25 @@ double normT(const or_matrix& A, const std::vector<T>& v, int norm) {
       else if (norm == 2) acc = std::max(acc, x);
       else acc += x;
     }
-  }
+    part[t] = acc;
+  });
+  double acc = norm == 2 ? -INFINITY : 0.0;
+  for (double p : part) acc = norm == 2 ? std::max(acc, p) : acc + p;
   return norm == 1 ? std::sqrt(acc) : acc;
 }
 
 template <class T>
 double dotT(const or_matrix& A, const std::vector<T>& a, const std::vector<T>& b) {
-  double acc = 0.0;
-  for (size_t t = 0; t < A.P; ++t) {
+  std::vector<double> part(A.P);
+  forTiles(A.P, [&](size_t t) {
+    double acc = 0.0;
     size_t nr = A.tileStart[t + 1] - A.tileStart[t];
     for (size_t i = 0; i < nr; ++i)
       acc += static_cast<double>(a[A.haloStart[t] + i]) * static_cast<double>(b[A.haloStart[t] + i]);
-  }
+    part[t] = acc;
+  });
+  double acc = 0.0;
+  for (double p : part) acc += p;
   return acc;
 }
 
