@@ -42,3 +42,17 @@ def test_error_reporting_without_gpu():
     assert rc == L.GR_EINVAL
     assert b"positive" in lib.gr_last_error()
     assert lib.gr_version() >= 1
+
+
+def test_c_client_of_host_entry_points(tmp_path):
+    """tests/abi_host_example.c, compiled with gcc against the header and
+    linked with the library, runs the host-side entry points from plain C."""
+    import subprocess
+    exe = tmp_path / "abi_host_example"
+    lib_dir = Path(L.LIB_PATH).parent
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-I", str(ROOT / "include"),
+                    str(ROOT / "tests" / "abi_host_example.c"), "-L", str(lib_dir),
+                    "-lgraphene_b200", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.strip() == "ok"
