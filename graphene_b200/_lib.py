@@ -93,6 +93,7 @@ SIGNATURES = {
     "gr_spmv": (C.c_int, [vp, vp, vp, C.c_int]),
     "gr_residual": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, vp, C.c_int, C.c_int]),
     "gr_vector_norm": (C.c_int, [vp, C.c_int, vp, C.c_int, P(C.c_double)]),
+    "gr_vector_norms_noalloc": (C.c_int, [vp, i64, i64, i64, C.c_int, C.c_int, vp, vp]),
     "gr_decompose_vector": (C.c_int, [vp, vp, vp, C.c_int]),
     "gr_compose_vector": (C.c_int, [vp, vp, vp, C.c_int]),
     "gr_solver_create": (C.c_int, [vp, C.c_char_p, P(vp)]),

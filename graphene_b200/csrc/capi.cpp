@@ -344,6 +344,16 @@ int gr_vector_norm(gr_matrix* A, gr_norm norm, const void* x, gr_dtype t, double
   });
 }
 
+int gr_vector_norms_noalloc(const void* x, int64_t n, int64_t count, int64_t ld, gr_dtype t,
+                            gr_norm norm, double* out, void* stream) {
+  return guarded([&] {
+    need(x, "x");
+    need(out, "out");
+    if (norm == GR_NORM_NONE || norm < 0 || norm > GR_NORM_NONE) gr::fail(GR_EINVAL, "invalid norm");
+    gr::launchNormsNoAlloc(x, n, count, ld, gr::toDType(t), norm, out, static_cast<cudaStream_t>(stream));
+  });
+}
+
 int gr_decompose_vector(gr_matrix* A, const void* natural, void* tile_ordered, gr_dtype t) {
   return guarded([&] {
     need(A, "matrix");

@@ -214,4 +214,9 @@ void launchNorm(DeviceMatrix& A, const void* x, DType t, int normKind, double* o
 void launchPermute(DeviceMatrix& A, const void* src, void* dst, DType t, bool toTileOrder,
                    cudaStream_t s);
 
+// Norms of `count` vectors through a static device scratch, allocating
+// nothing (gr_vector_norms_noalloc).
+void launchNormsNoAlloc(const void* x, i64 n, i64 count, i64 ld, DType t, int normKind, double* out,
+                        cudaStream_t s);
+
 }  // namespace gr

@@ -244,6 +244,21 @@ int gr_residual(gr_matrix* A, const void* x, gr_dtype x_t, const void* b, gr_dty
  * details/MatrixBase.cpp:149-152). Accumulates in FP64. */
 int gr_vector_norm(gr_matrix* A, gr_norm norm, const void* x, gr_dtype t, double* out);
 
+/* Norms of `count` device vectors of n elements (vector j starts at element
+ * j * ld of x), FP64 accumulation, written to out[0..count) (device
+ * doubles) on `stream` (NULL: the default stream); returns without waiting.
+ * No counterpart in the reference. Unlike gr_vector_norm it needs no
+ * matrix and allocates no device memory: it reduces through a static
+ * per-device scratch of 75,808 bytes. For callers that must not allocate
+ * device memory at the call (a serving loop held to a fixed HBM footprint,
+ * a caching allocator's own callbacks). Limits: count 1..8, n <= 2^31 - 1;
+ * anything larger returns GR_EINVAL. Calls that overlap on one device
+ * (several streams or threads) share the scratch and race: serialise them.
+ * The first call on each device does the set-up (symbol lookup, scratch
+ * counters cleared); make it before any stream capture. */
+int gr_vector_norms_noalloc(const void* x, int64_t n, int64_t count, int64_t ld, gr_dtype t,
+                            gr_norm norm, double* out, void* stream);
+
 /* Natural order <-> tile order on the device. */
 int gr_decompose_vector(gr_matrix* A, const void* natural, void* tile_ordered, gr_dtype t);
 int gr_compose_vector(gr_matrix* A, const void* tile_ordered, void* natural, gr_dtype t);
