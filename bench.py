@@ -221,6 +221,148 @@ def reference_arm(a):
     return 0
 
 
+def pbicgstab(precond, tol, maxit=1000):
+    pre = {"ILU": {"type": "ILU"},
+           "GS": {"type": "GaussSeidel", "numSweeps": 2, "numFixedIterations": 2}}[precond]
+    return {"type": "PBiCGStab", "maxIterations": maxit, "relResidual": tol, "preconditioner": pre}
+
+
+def timed_solve(gb, A, cfg, b, reps=2):
+    """Best of `reps` (solver creation + solve) by CUDA events, after one
+    warm-up; returns (ms, stats, relative FP64 residual of x)."""
+    import torch
+    n = A.numRows
+
+    def once():
+        x = torch.zeros(n, dtype=b.dtype, device="cuda")
+        st = gb.Solver(A, cfg).solve(x, b)
+        return x, st
+    once()
+    best = None
+    for _ in range(reps):
+        ms, (x, st) = event_ms(once)
+        best = ms if best is None else min(best, ms)
+    r = A.residual(x.double(), b, destType=gb.FLOAT64, intermediateType=gb.FLOAT64)
+    rel = float(torch.linalg.vector_norm(r) / torch.linalg.vector_norm(b.double()))
+    return best, st, rel
+
+
+def other_configs(gb, peak):
+    """The reference's other benchmark configurations on the same GPU."""
+    import numpy as np
+    import torch
+    out = {}
+    # 32^3 Poisson, 64 tiles, PBiCGStab + ILU(0) to 1e-6.
+    h = gb.generate3DPoissonMatrix(gb.FLOAT32, 32, 32, 32, 64)
+    A = h.copyToTile()
+    b = A * A.vector(gb.randomVector(0, h.numRows).astype(np.float32))
+    ms, st, rel = timed_solve(gb, A, pbicgstab("ILU", 1e-6), b, reps=3)
+    out["poisson32_pbicgstab_ilu0"] = {"ms": ms, "iterations": st.iterations, "converged": st.converged,
+                                       "rel_residual_fp64": rel}
+    # 128^3 upwind convection-diffusion (cell Peclet 0.5), 1024 tiles, to 1e-8,
+    # Gauss-Seidel (2 sweeps) and ILU(0), FP32 and FP64.
+    h = gb.generateMatrix(gb.GEN_CONVDIFF, 128, 128, 128, (0.5, 0.25, 0.125), 0, 1024)
+    xt = gb.randomVector(1, h.numRows, "normal")
+    for vt, name in [(gb.FLOAT32, "fp32"), (gb.FLOAT64, "fp64")]:
+        hv = h if vt == gb.FLOAT32 else h.astype(gb.FLOAT64)
+        A = hv.copyToTile()
+        b = A * A.vector(xt.astype(np.float32 if vt == gb.FLOAT32 else np.float64))
+        for pre in ("GS", "ILU"):
+            ms, st, rel = timed_solve(gb, A, pbicgstab(pre, 1e-8, 2000), b)
+            out[f"convdiff128_{pre.lower()}_{name}"] = {"ms": ms, "iterations": st.iterations,
+                                                       "converged": st.converged, "rel_residual_fp64": rel}
+        del A
+    # 100^3 LDU mesh (jittered, permuted), Gauss-Seidel PBiCGStab to 1e-8,
+    # and the LDU SpMV (matrix smaller than L2: L2 flushed before each launch).
+    h = gb.generateLduMesh(100, 100, 100, 4, 5, 6, numTiles=1024)
+    A = h.copyToTile()
+    b = A * A.vector(gb.randomVector(1, h.numRows, "normal").astype(np.float32))
+    ms, st, rel = timed_solve(gb, A, pbicgstab("GS", 1e-8, 4000), b)
+    out["ldu100_pbicgstab_gs"] = {"ms": ms, "iterations": st.iterations, "converged": st.converged,
+                                  "rel_residual_fp64": rel}
+    n, F = h.numRows, h.numOffDiag // 2
+    y = torch.empty_like(b)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    times = []
+    for i in range(23):
+        flush.zero_()
+        t, _ = event_ms(lambda: A.spmv(b, y))
+        if i >= 3:
+            times.append(t)
+    t = statistics.median(times)
+    ldu_bytes = 20 * n + 20 * F       # reference LDU arrays: cells 5 x 4 B, faces 5 x 4 B
+    layout_bytes = 16 * F + 16 * n + 4  # this library's layout: 2F (col, value) pairs, diag, x, y, rowPtr
+    out["ldu100_spmv"] = {"ms": t, "cells": n, "faces": F,
+                          "GBs_ldu_algorithmic": ldu_bytes / (t * 1e-3) / 1e9,
+                          "GBs_device_layout": layout_bytes / (t * 1e-3) / 1e9,
+                          "frac_of_hbm_device_layout": layout_bytes / (t * 1e-3) / 1e9 / peak,
+                          "l2": "flushed before each launch"}
+    return out
+
+
+def serving(gb, requests=300, slots=4, pool=32, seed=7):
+    """Solve server under a Poisson arrival stream: 7-point variable-coefficient
+    Poisson systems (sigma 1) with grid edge U{16..96}, 70 % FP32
+    PBiCGStab-ILU(0) to 1e-6 and 30 % MPIR to 1e-10 (by seed). Throughput at
+    saturation (all requests submitted at once), then p50 / p99 latency from
+    arrival to result at 50 %, 80 % and 100 % of that throughput. 'resident':
+    requests draw from `pool` distinct matrices that stay resident; 'cold':
+    every request brings a matrix the server has not seen (upload and ILU
+    factorisation in its latency)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    ilu = {"type": "PBiCGStab", "maxIterations": 1000, "relResidual": 1e-6, "preconditioner": {"type": "ILU"}}
+    mpir = {"type": "IterativeRefinement", "relResidual": 1e-10, "maxIterations": 30,
+            "extendedPrecisionType": "float64",
+            "innerSolver": {"type": "PBiCGStab", "maxIterations": 500, "relResidual": 1e-4,
+                            "preconditioner": {"type": "ILU"}}}
+
+    def make(k):
+        L = int(rng.integers(16, 97))
+        tiles = max(1, (L ** 3 + 3455) // 3456)
+        h = gb.generateMatrix(gb.GEN_VAR_POISSON, L, L, L, (1.0,), 1000 + k, tiles)
+        return h, gb.randomVector(2000 + k, h.numRows).astype(np.float32)
+
+    def run(srv, items, rate):
+        ids, t0 = [], time.perf_counter()
+        gaps = rng.exponential(1.0 / rate, len(items)) if rate else np.zeros(len(items))
+        due = 0.0
+        for (h, b, cfg), g in zip(items, gaps):
+            due += g
+            d = due - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            ids.append(srv.submit(h, cfg, b))
+        res = [srv.wait(i) for i in ids]
+        lat = np.array([tm["finished_ms"] - tm["arrival_ms"] for _, _, tm in res])
+        span = max(tm["finished_ms"] for _, _, tm in res) - min(tm["arrival_ms"] for _, _, tm in res)
+        ok = all(st.converged for _, st, _ in res)
+        hits = sum(tm["cache_hit"] for _, _, tm in res)
+        return {"offered_per_s": rate, "throughput_per_s": len(res) / (span * 1e-3),
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "all_converged": ok, "resident_hits": int(hits)}
+
+    out = {"requests": requests, "slots": slots}
+    mats = [make(k) for k in range(pool)]
+    cfgs = [mpir if u < 0.3 else ilu for u in rng.random(requests)]
+    items = [(mats[k][0], mats[k][1], c) for k, c in zip(rng.integers(0, pool, requests), cfgs)]
+    srv = gb.Server(slots=slots)
+    run(srv, items[: min(len(items), 2 * pool)], None)  # fills the resident set
+    sat = run(srv, items, None)
+    res = {"saturation": sat}
+    for f in (0.5, 0.8, 1.0):
+        res[f"load_{f}"] = run(srv, items, f * sat["throughput_per_s"])
+    srv.close()
+    out["resident"] = res
+    cold_n = min(requests, 48)
+    cold = [make(pool + k) for k in range(cold_n)]
+    srv = gb.Server(slots=slots)
+    out["cold"] = {"requests": cold_n,
+                   "saturation": run(srv, [(h, b, c) for (h, b), c in zip(cold, cfgs)], None)}
+    srv.close()
+    return out
+
+
 def event_ms(fn):
     import torch
     e0 = torch.cuda.Event(enable_timing=True)
@@ -319,6 +461,8 @@ def main():
             ms, (sv, _, sx) = event_ms(lambda: solve(A, c, b))
             extra[name] = {"ms": ms, "outer": sx.iterations, "inner": sx.innerIterations,
                            "converged": sx.converged, "rel_residual_fp64": rel64(A, sv.phi(gb.FLOAT64), b)}
+        extra["configs"] = other_configs(gb, peak)
+        extra["serving"] = serving(gb)
 
     # Kernel timings: SpMV and the ILU(0) application (HBM rooflines).
     y = torch.empty_like(x_true)

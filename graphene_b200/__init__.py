@@ -35,6 +35,7 @@ __all__ = [
     "PART_AUTO", "PART_CONTIGUOUS", "PART_RCB", "PART_BFS", "PART_EXPLICIT",
     "GrapheneError", "HostMatrix", "Matrix", "Configuration", "Solver", "SolverStats",
     "generate3DPoissonMatrix", "loadMatrixFromFile", "parseType", "launch_count",
+    "generateMatrix", "generateLduMesh", "randomVector", "Server",
 ]
 
 _NP = {FLOAT32: np.float32, FLOAT64: np.float64}
@@ -144,6 +145,44 @@ class HostMatrix:
                                                   C.byref(h)))
         return HostMatrix(h)
 
+    @staticmethod
+    def from_ldu(numCells: int, owner, neighbour, diag, lower, upper=None, numTiles: int = 1,
+                 partitioner: int = PART_AUTO, rowToTile=None, coords=None,
+                 valueType: int = FLOAT32) -> "HostMatrix":
+        """LDU matrix (matrix/details/ldu/LDUMatrix.hpp): faces owner <
+        neighbour sorted by owner, coefficients in face order (upper None:
+        symmetric)."""
+        o = np.ascontiguousarray(owner, dtype=np.int64)
+        nb = np.ascontiguousarray(neighbour, dtype=np.int64)
+        d = np.ascontiguousarray(diag, dtype=np.float64)
+        lo = np.ascontiguousarray(lower, dtype=np.float64)
+        up = None if upper is None else np.ascontiguousarray(upper, dtype=np.float64)
+        rt = None if rowToTile is None else np.ascontiguousarray(rowToTile, dtype=np.int32)
+        cd = None if coords is None else np.ascontiguousarray(coords, dtype=np.float64)
+        if rt is not None:
+            partitioner = PART_EXPLICIT
+        h = C.c_void_p()
+        check(_lib.lib().gr_host_matrix_from_ldu(numCells, len(o), _ptr(o), _ptr(nb), _ptr(d), _ptr(lo),
+                                                  _ptr(up), numTiles, partitioner, _ptr(rt), _ptr(cd),
+                                                  valueType, C.byref(h)))
+        return HostMatrix(h)
+
+    @property
+    def isLdu(self) -> bool:
+        return self.info.format == FORMAT_LDU
+
+    def ldu(self):
+        """(owner, neighbour, lower, upper, diag) of an LDU matrix, natural
+        numbering, values rounded to the stored type."""
+        nf = C.c_int64()
+        check(_lib.lib().gr_host_matrix_get_ldu(self._h, C.byref(nf), None, None, None, None, None))
+        F, n = nf.value, self.numRows
+        o, nb = np.empty(F, np.int64), np.empty(F, np.int64)
+        lo, up, dg = np.empty(F), np.empty(F), np.empty(n)
+        check(_lib.lib().gr_host_matrix_get_ldu(self._h, C.byref(nf), _ptr(o), _ptr(nb), _ptr(lo),
+                                                _ptr(up), _ptr(dg)))
+        return o, nb, lo, up, dg
+
     # -- layout queries ----------------------------------------------------
     @property
     def numRows(self) -> int:
@@ -218,6 +257,18 @@ def generate3DPoissonMatrix(valueType: int, nx: int, ny: int, nz: int, numTiles:
 
 
 GEN_POISSON, GEN_VAR_POISSON, GEN_CONVDIFF = 0, 1, 2
+FORMAT_CRS, FORMAT_LDU = 0, 1
+
+
+def generateLduMesh(nx: int, ny: int, nz: int, jitterSeed: int = 4, permSeed: int = 5,
+                    coefSeed: int = 6, numTiles: int = 1, partitioner: int = PART_AUTO,
+                    valueType: int = FLOAT32) -> HostMatrix:
+    """Jittered, cell-permuted hexahedral mesh in LDU form with log-uniform
+    face coefficients (gr_host_matrix_ldu_mesh)."""
+    h = C.c_void_p()
+    check(_lib.lib().gr_host_matrix_ldu_mesh(nx, ny, nz, jitterSeed, permSeed, coefSeed, numTiles,
+                                             partitioner, parseType(valueType), C.byref(h)))
+    return HostMatrix(h)
 
 
 def generateMatrix(kind: int, nx: int, ny: int, nz: int, params=(), seed: int = 0,
@@ -423,3 +474,55 @@ class Matrix:
     def solve(self, x, b, config) -> SolverStats:
         """Matrix::solve(x, b, config) (matrix/Matrix.cpp:26-30)."""
         return Solver(self, config).solve(x, b)
+
+
+class Server:
+    """Continuous-batching solve server (gr_server_*): requests are admitted
+    in arrival order as worker slots and device memory free up, run
+    concurrently on separate CUDA streams, and (matrix, configuration) pairs
+    stay resident for later requests."""
+
+    def __init__(self, slots: int = 4, budgetBytes: int = 0, device: int = -1):
+        cfg = _lib.ServerConfig(slots, device, budgetBytes)
+        h = C.c_void_p()
+        check(_lib.lib().gr_server_create(C.byref(cfg), C.byref(h)))
+        self._s = h
+        self._hosts = {}
+
+    def submit(self, h: HostMatrix, config, b: np.ndarray) -> int:
+        """Queues h x = b (natural order, float32 or float64), x0 = 0."""
+        js = config if isinstance(config, str) else _json.dumps(config)
+        bb = np.ascontiguousarray(b)
+        t = FLOAT32 if bb.dtype == np.float32 else FLOAT64
+        rid = C.c_uint64()
+        check(_lib.lib().gr_server_submit(self._s, h._h, js.encode(), _ptr(bb), t, C.byref(rid)))
+        self._hosts[rid.value] = (h, bb.dtype)
+        return rid.value
+
+    def wait(self, rid: int, timeoutMs: float = -1.0):
+        """(x, SolverStats, times dict) of a finished request."""
+        h, dt = self._hosts[rid]
+        x = np.empty(h.numRows, dtype=dt)
+        st = _lib.Stats()
+        tm = _lib.RequestTimes()
+        check(_lib.lib().gr_server_wait(self._s, rid, timeoutMs, _ptr(x), C.byref(st), C.byref(tm)))
+        del self._hosts[rid]
+        times = {k: getattr(tm, k) for k, _ in _lib.RequestTimes._fields_}
+        return x, SolverStats._from(st), times
+
+    def counters(self) -> dict:
+        v = [C.c_int64() for _ in range(5)]
+        check(_lib.lib().gr_server_counters(self._s, *[C.byref(a) for a in v]))
+        return dict(zip(["queued", "running", "completed", "bytes_in_use", "resident"], [a.value for a in v]))
+
+    def close(self):
+        s = getattr(self, "_s", None)
+        if s and _lib is not None:
+            try:
+                _lib.lib().gr_server_destroy(s)
+            except Exception:
+                pass
+            self._s = None
+
+    def __del__(self):
+        self.close()

@@ -58,6 +58,21 @@ class MatrixInfo(C.Structure):
     ]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("slots", C.c_int32), ("device", C.c_int32), ("hbm_budget_bytes", C.c_int64)]
+
+
+class RequestTimes(C.Structure):
+    _fields_ = [
+        ("arrival_ms", C.c_double),
+        ("admitted_ms", C.c_double),
+        ("finished_ms", C.c_double),
+        ("footprint_bytes", C.c_int64),
+        ("cache_hit", C.c_int32),
+        ("slot", C.c_int32),
+    ]
+
+
 vp = C.c_void_p
 i64 = C.c_int64
 i32 = C.c_int32
@@ -70,6 +85,10 @@ SIGNATURES = {
     "gr_launch_count": (i64, []),
     "gr_host_matrix_from_coo": (C.c_int, [i64, i64, vp, vp, vp, i64, C.c_int, vp, vp, C.c_int, P(vp)]),
     "gr_host_matrix_poisson": (C.c_int, [i64, i64, i64, i64, C.c_int, C.c_int, P(vp)]),
+    "gr_host_matrix_from_ldu": (C.c_int, [i64, i64, vp, vp, vp, vp, vp, i64, C.c_int, vp, vp, C.c_int, P(vp)]),
+    "gr_host_matrix_ldu_mesh": (C.c_int, [i64, i64, i64, C.c_uint64, C.c_uint64, C.c_uint64, i64, C.c_int,
+                                          C.c_int, P(vp)]),
+    "gr_host_matrix_get_ldu": (C.c_int, [vp, P(i64), vp, vp, vp, vp, vp]),
     "gr_host_matrix_load_mm": (C.c_int, [C.c_char_p, i64, C.c_int, C.c_int, P(vp)]),
     "gr_host_matrix_generate": (C.c_int, [C.c_int, i64, i64, i64, vp, C.c_uint64, i64, C.c_int,
                                           C.c_int, P(vp)]),
@@ -94,6 +113,11 @@ SIGNATURES = {
     "gr_residual": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, vp, C.c_int, C.c_int]),
     "gr_vector_norm": (C.c_int, [vp, C.c_int, vp, C.c_int, P(C.c_double)]),
     "gr_vector_norms_noalloc": (C.c_int, [vp, i64, i64, i64, C.c_int, C.c_int, vp, vp]),
+    "gr_server_create": (C.c_int, [P(ServerConfig), P(vp)]),
+    "gr_server_submit": (C.c_int, [vp, vp, C.c_char_p, vp, C.c_int, P(C.c_uint64)]),
+    "gr_server_wait": (C.c_int, [vp, C.c_uint64, C.c_double, vp, P(Stats), P(RequestTimes)]),
+    "gr_server_counters": (C.c_int, [vp, P(i64), P(i64), P(i64), P(i64), P(i64)]),
+    "gr_server_destroy": (None, [vp]),
     "gr_decompose_vector": (C.c_int, [vp, vp, vp, C.c_int]),
     "gr_compose_vector": (C.c_int, [vp, vp, vp, C.c_int]),
     "gr_solver_create": (C.c_int, [vp, C.c_char_p, P(vp)]),

@@ -1,4 +1,5 @@
 // extern "C" boundary of graphene_b200 (include/graphene_gpu.h).
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
@@ -7,6 +8,7 @@
 #include "host_matrix.hpp"
 #include "config.hpp"
 #include "solvers.hpp"
+#include "server.hpp"
 
 struct gr_host_matrix {
   std::shared_ptr<gr::HostMatrix> m;
@@ -18,6 +20,10 @@ struct gr_matrix {
 
 struct gr_solver {
   std::unique_ptr<gr::SolverTree> s;
+};
+
+struct gr_server {
+  std::unique_ptr<gr::Server> s;
 };
 
 namespace {
@@ -119,6 +125,48 @@ int gr_host_matrix_generate(gr_generator kind, int64_t nx, int64_t ny, int64_t n
   });
 }
 
+int gr_host_matrix_from_ldu(int64_t num_cells, int64_t num_faces, const int64_t* owner, const int64_t* neighbour,
+                            const double* diag, const double* lower, const double* upper, int64_t num_tiles,
+                            gr_partitioner partitioner, const int32_t* row_to_tile, const double* coords,
+                            gr_dtype value_type, gr_host_matrix** out) {
+  return guarded([&] {
+    need(out, "out");
+    auto h = gr::HostMatrix::fromLdu(num_cells, num_faces, owner, neighbour, diag, lower, upper, num_tiles,
+                                     partitioner, row_to_tile, coords, gr::toDType(value_type));
+    *out = new gr_host_matrix{std::move(h)};
+  });
+}
+
+int gr_host_matrix_ldu_mesh(int64_t nx, int64_t ny, int64_t nz, uint64_t jitter_seed, uint64_t perm_seed,
+                            uint64_t coef_seed, int64_t num_tiles, gr_partitioner partitioner, gr_dtype value_type,
+                            gr_host_matrix** out) {
+  return guarded([&] {
+    need(out, "out");
+    gr::LduMesh M = gr::generateLduMesh(nx, ny, nz, jitter_seed, perm_seed, coef_seed);
+    auto h = gr::HostMatrix::fromLdu(M.n, static_cast<int64_t>(M.owner.size()), M.owner.data(),
+                                     M.neighbour.data(), M.diag.data(), M.lower.data(), M.upper.data(), num_tiles,
+                                     partitioner, nullptr, M.coords.data(), gr::toDType(value_type));
+    *out = new gr_host_matrix{std::move(h)};
+  });
+}
+
+int gr_host_matrix_get_ldu(const gr_host_matrix* h, int64_t* num_faces, int64_t* owner, int64_t* neighbour,
+                           double* lower, double* upper, double* diag) {
+  return guarded([&] {
+    need(h, "host matrix");
+    need(num_faces, "num_faces");
+    const gr::HostMatrix& H = *h->m;
+    if (H.format != GR_FORMAT_LDU) gr::fail(GR_EINVAL, "not an LDU matrix");
+    const size_t F = H.lduOwner.size();
+    *num_faces = static_cast<int64_t>(F);
+    if (owner) std::copy(H.lduOwner.begin(), H.lduOwner.end(), owner);
+    if (neighbour) std::copy(H.lduNeighbour.begin(), H.lduNeighbour.end(), neighbour);
+    if (lower) std::copy(H.lduLower.begin(), H.lduLower.end(), lower);
+    if (upper) std::copy(H.lduUpper.begin(), H.lduUpper.end(), upper);
+    if (diag) std::copy(H.lduDiag.begin(), H.lduDiag.end(), diag);
+  });
+}
+
 int gr_random_vector(uint64_t seed, int64_t n, int dist, double lo, double hi, double* out) {
   return guarded([&] {
     need(out, "out");
@@ -168,6 +216,7 @@ int gr_host_matrix_astype(const gr_host_matrix* h, gr_dtype value_type, gr_host_
         for (double& x : v) x = static_cast<double>(static_cast<float>(x));
       };
       r(c->gVal); r(c->gDiag); r(c->offDiag); r(c->diag);
+      r(c->lduLower); r(c->lduUpper); r(c->lduDiag);
     }
     *out = new gr_host_matrix{std::move(c)};
   });
@@ -446,5 +495,53 @@ int gr_config_parse(const char* json, char* name, size_t name_len, char* unknown
     copy(unk, unknown_keys, unknown_len);
   });
 }
+
+
+int gr_server_create(const gr_server_config* cfg, gr_server** out) {
+  return guarded([&] {
+    need(out, "out");
+    gr_server_config c{0, -1, 0};
+    if (cfg) c = *cfg;
+    auto srv = std::make_unique<gr::Server>(c.slots, c.device, c.hbm_budget_bytes);
+    *out = new gr_server{std::move(srv)};
+  });
+}
+
+int gr_server_submit(gr_server* s, gr_host_matrix* h, const char* json, const void* b, gr_dtype t, uint64_t* id) {
+  return guarded([&] {
+    need(s, "server");
+    need(h, "host matrix");
+    need(json, "json");
+    need(id, "id");
+    *id = s->s->submit(h->m, json, b, gr::toDType(t));
+  });
+}
+
+int gr_server_wait(gr_server* s, uint64_t id, double timeout_ms, void* x_out, gr_stats* stats,
+                   gr_request_times* times) {
+  int status = GR_OK, rc = GR_OK;
+  std::string err;
+  const int g = guarded([&] {
+    need(s, "server");
+    rc = s->s->wait(id, timeout_ms, x_out, stats, times, &status, &err);
+  });
+  if (g != GR_OK) return g;
+  if (rc != GR_OK) {
+    g_lastError = "request has not finished";
+    return rc;
+  }
+  g_lastError = err;
+  return status;
+}
+
+int gr_server_counters(gr_server* s, int64_t* queued, int64_t* running, int64_t* completed, int64_t* bytes_in_use,
+                       int64_t* resident) {
+  return guarded([&] {
+    need(s, "server");
+    s->s->counters(queued, running, completed, bytes_in_use, resident);
+  });
+}
+
+void gr_server_destroy(gr_server* s) { delete s; }
 
 }  // extern "C"

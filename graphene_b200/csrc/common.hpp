@@ -15,6 +15,7 @@ namespace gr {
 
 using i32 = int32_t;
 using i64 = int64_t;
+using u64 = uint64_t;
 
 // Error carried to the C ABI: code is one of the GR_E* values.
 struct Error : std::runtime_error {

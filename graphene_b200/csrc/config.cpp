@@ -245,8 +245,11 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
     if (const Json* v = j.find("preconditioner")) c->preconditioner = fromJson(*v);
   } else if (ty == "ILU") {
     mark("solveMulticolor"); mark("factorizeMulticolor"); mark("diagonalBased"); mark("kernel");
-    mark("ringLog2");
+    mark("ringLog2"); mark("prefetch"); mark("unroll");
     readInt(j, "ringLog2", c->ringLog2);
+    readInt(j, "prefetch", c->prefetchChunks);
+    if (c->prefetchChunks < -1 || c->prefetchChunks > 64) fail(GR_EINVAL, "prefetch must be -1 (default) or 0..64");
+    readBool(j, "unroll", c->unrollRows);
     if (c->ringLog2 != 0 && (c->ringLog2 < 13 || c->ringLog2 > 17))
       fail(GR_EINVAL, "ringLog2 must be 0 (automatic) or between 13 and 17");
     readMultiColor(j, "solveMulticolor", c->solveMulticolor);

@@ -47,6 +47,11 @@ struct SolverConfig {
   // Extension: log2 of the streamed kernel's ring size in bytes (0: the
   // smallest ring that holds the largest level).
   int ringLog2 = 0;
+  // Extensions: ring chunks the streamed kernel keeps prefetched into L2
+  // beyond its ring (-1: default), and whether it loads all terms of short
+  // rows at once.
+  int prefetchChunks = -1;
+  bool unrollRows = false;
   // GaussSeidel (gauss-seidel/Configuration.hpp:19-21)
   int numSweeps = 1, numFixedIterations = 0;
   // Extension: "seed": "b" (default, the codelet specification

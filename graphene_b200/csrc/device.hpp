@@ -197,6 +197,12 @@ struct DeviceMatrix {
   int spmvBlocks() const;
 };
 
+// Raises the dynamic shared-memory limit of kernel `fn` on the current device
+// to at least `bytes`. The limit is shared by every thread of the process,
+// so it is only ever raised (a lower request never undoes a higher one that
+// another thread's launch relies on).
+void ensureDynamicSmem(const void* fn, size_t bytes);
+
 // ---- launchers -------------------------------------------------------
 
 // y = A x (reference CRSMatrix::spmv). xt == yt.

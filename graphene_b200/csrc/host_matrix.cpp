@@ -419,7 +419,7 @@ gr_matrix_info HostMatrix::info() const {
   i.num_lower_levels_total = nl;
   i.num_upper_levels_total = nu;
   i.value_type = static_cast<int32_t>(valueType);
-  i.format = GR_FORMAT_CRS;
+  i.format = format;
   i.multicolor_recommended = multicolorRecommended ? 1 : 0;
   return i;
 }

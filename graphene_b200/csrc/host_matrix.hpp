@@ -78,6 +78,17 @@ struct HostMatrix {
   i64 numHaloTotal = 0;
   i64 maxTileRows = 0;
 
+  // LDU format (matrix/details/ldu/LDUMatrix.cpp:42-168,
+  // LDUAddressing.hpp:42-91). The faces in natural numbering, owner <
+  // neighbour, sorted by owner; coefficients in face order, rounded to the
+  // value type. sumRank gives, for every tile-local CRS entry, its position
+  // in its row's LDU summation order (owned faces in face order, then the
+  // faces the row neighbours in losort order). All empty for CRS matrices.
+  int format = GR_FORMAT_CRS;
+  std::vector<i64> lduOwner, lduNeighbour;
+  std::vector<double> lduLower, lduUpper, lduDiag;
+  std::vector<i32> sumRank;
+
   // Builds everything from triplets. rowToTileIn is used for
   // GR_PART_EXPLICIT; coords (3 per row) for GR_PART_RCB.
   static std::shared_ptr<HostMatrix> fromCoo(Coo coo, i64 numTiles, gr_partitioner part,
@@ -90,6 +101,13 @@ struct HostMatrix {
                                                    i64 numTiles, gr_partitioner part,
                                                    const i32* rowToTileIn,
                                                    std::vector<double> coords, DType valueType);
+
+  // From LDU arrays: num_faces faces (owner, neighbour, lower, upper) and
+  // the diagonal, natural numbering. upper == nullptr means upper = lower.
+  static std::shared_ptr<HostMatrix> fromLdu(i64 n, i64 numFaces, const i64* owner, const i64* neighbour,
+                                             const double* diag, const double* lower, const double* upper,
+                                             i64 numTiles, gr_partitioner part, const i32* rowToTileIn,
+                                             const double* coords, DType valueType);
 
   gr_matrix_info info() const;
 
@@ -129,6 +147,19 @@ GeneratedCsr generatePoisson(i64 nx, i64 ny, i64 nz);
 GeneratedCsr generateVarPoisson(i64 nx, i64 ny, i64 nz, double sigma, uint64_t seed);
 GeneratedCsr generateConvDiff(i64 nx, i64 ny, i64 nz, double vx, double vy, double vz);
 void generateUniform(uint64_t seed, i64 n, double lo, double hi, double* out);
+
+// Unstructured-mesh stand-in in LDU form: an nx x ny x nz hexahedral mesh
+// with node positions jittered by U(-0.2, 0.2) spacings (jitterSeed; only the
+// cell centroids in `coords` depend on it), cell ids permuted (permSeed),
+// face owner = smaller cell id, neighbour = larger, faces sorted by (owner,
+// neighbour), face coefficient c = 10^U(-2, 2) (coefSeed), off-diagonals -c
+// and diagonal = sum of the cell's face coefficients + 1e-3.
+struct LduMesh {
+  i64 n = 0;
+  std::vector<i64> owner, neighbour;
+  std::vector<double> lower, upper, diag, coords;
+};
+LduMesh generateLduMesh(i64 nx, i64 ny, i64 nz, uint64_t jitterSeed, uint64_t permSeed, uint64_t coefSeed);
 void generateNormal(uint64_t seed, i64 n, double* out);
 
 // MatrixMarket reader (public format spec; replaces fast_matrix_market).

@@ -9,6 +9,8 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "device.hpp"
 #include "devmath.cuh"
@@ -38,21 +40,59 @@ void cudaCheck(cudaError_t e, const char* what) {
   }
 }
 
+// Device memory comes from the device's stream-ordered pool. cudaFree may
+// wait for all work on the device, which would serialise solves running
+// concurrently on other streams; cudaFreeAsync does not. Freed blocks stay
+// in the process's pool (release threshold raised once per device) and are
+// reused by later allocations.
+namespace {
+std::once_flag g_poolOnce[64];
+
+void keepPoolMemory() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::call_once(g_poolOnce[dev], [dev] {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  });
+}
+}  // namespace
+
+void ensureDynamicSmem(const void* fn, size_t bytes) {
+  if (bytes <= 48 * 1024) return;  // within the default limit
+  int dev = 0;
+  GR_CUDA(cudaGetDevice(&dev));
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> raised;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& cur = raised[{dev, fn}];
+  if (bytes <= cur) return;
+  GR_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+  cur = bytes;
+}
+
 void DBuf::alloc(size_t bytes) {
   release();
   if (bytes == 0) bytes = 1;
-  cudaError_t e = cudaMalloc(&p_, bytes);
+  keepPoolMemory();
+  cudaError_t e = cudaMallocAsync(&p_, bytes, cudaStreamPerThread);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread);
   if (e != cudaSuccess) {
     p_ = nullptr;
     (void)cudaGetLastError();
-    fail(GR_ENOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " +
+    fail(GR_ENOMEM, "allocation of " + std::to_string(bytes) + " device bytes failed: " +
                         cudaGetErrorString(e));
   }
   bytes_ = bytes;
 }
 
+// The owner guarantees that no work using the buffer is still pending (it
+// synchronises the stream the buffer was used on before releasing it).
 void DBuf::release() {
-  if (p_) cudaFree(p_);
+  if (p_) cudaFreeAsync(p_, cudaStreamPerThread);
   p_ = nullptr;
   bytes_ = 0;
 }
@@ -112,10 +152,14 @@ DeviceMatrix::DeviceMatrix(std::shared_ptr<HostMatrix> h) : host(std::move(h)) {
   parallelChunks(n, [&](i64 b, i64 e) {
     for (i64 r = b; r < e; ++r) {
       i64 c = r / 32, lane = r % 32;
+      // Slot k holds the row's k-th term of its summation order: local
+      // column order for CRS, the LDU order (sumRank) for LDU matrices.
       for (i64 k = 0; k < H.rowPtr[r + 1] - H.rowPtr[r]; ++k) {
-        i64 s = base[c] + 32 * k + lane;
-        col[s] = H.colPerm[H.rowPtr[r] + k];
-        val[s] = H.offDiag[H.rowPtr[r] + k];
+        const i64 p = H.rowPtr[r] + k;
+        const i64 slot = H.sumRank.empty() ? k : H.sumRank[p];
+        i64 s = base[c] + 32 * slot + lane;
+        col[s] = H.colPerm[p];
+        val[s] = H.offDiag[p];
       }
     }
   });
@@ -143,11 +187,12 @@ DeviceMatrix::DeviceMatrix(std::shared_ptr<HostMatrix> h) : host(std::move(h)) {
   redBlocks = numSMs * 8;
   partials.alloc(sizeof(double) * redBlocks * 8);
   counter.alloc(sizeof(unsigned) * 16);
-  GR_CUDA(cudaMemset(counter.get(), 0, sizeof(unsigned) * 16));
+  GR_CUDA(cudaMemsetAsync(counter.get(), 0, sizeof(unsigned) * 16, ownStream));
   scalarOut.alloc(sizeof(double) * 8);
   errFlag.alloc(sizeof(int));
-  GR_CUDA(cudaMemset(errFlag.get(), 0, sizeof(int)));
-  GR_CUDA(cudaDeviceSynchronize());
+  GR_CUDA(cudaMemsetAsync(errFlag.get(), 0, sizeof(int), ownStream));
+  // Only this matrix's stream: other solves may be running on the device.
+  GR_CUDA(cudaStreamSynchronize(ownStream));
 }
 
 DeviceMatrix::~DeviceMatrix() {

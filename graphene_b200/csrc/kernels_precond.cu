@@ -268,14 +268,14 @@ __global__ void prologueKernel(Pro<W> pro, W* copyTo, int n) {
 
 // ---------------------------------------------------------------------------
 int maxDynamicSmem(const DeviceMatrix& A) {
-  static thread_local int cached[64] = {0};
+  static std::atomic<int> cached[64] = {};
   const int d = A.device & 63;
-  if (cached[d] == 0) {
-    int v = 0;
+  int v = cached[d].load();
+  if (v == 0) {
     GR_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, A.device));
-    cached[d] = v;
+    cached[d].store(v);
   }
-  return cached[d];
+  return v;
 }
 
 namespace {
@@ -290,7 +290,7 @@ dev::Pro<W> makePro(const PrologueArgs& p) {
 
 template <class K>
 void setSmem(K kernel, size_t bytes) {
-  GR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+  ensureDynamicSmem(reinterpret_cast<const void*>(kernel), bytes);
 }
 
 int elemBlocks(const DeviceMatrix& A, i64 n) {

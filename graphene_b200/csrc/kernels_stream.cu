@@ -56,6 +56,44 @@ __device__ __forceinline__ bool mbarTryWait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 __device__ __forceinline__ void fenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// Hint: bring [src, src + bytes) into L2 (no completion, no shared memory).
+__device__ __forceinline__ void prefetchL2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
+// Default number of chunks beyond the ring that the producer keeps
+// prefetched into L2, so that a refill reads L2 instead of HBM.
+constexpr int kPrefetchChunks = 2 * kRingChunks;
+
+// temp -= sum_e val_e * xs[col_e] over a row's E entries (entry-major, column
+// -1 = padding, which only trails a row's entries and carries value 0).
+// Rows of up to four entries load all columns and values at once.
+template <class MV, bool UNROLL, class W, class RI, class RV>
+__device__ __forceinline__ W rowDot(W temp, int E, uint32_t co, uint32_t vo, uint32_t colStride,
+                                    uint32_t valStride, const W* xs, RI rdInt, RV rdVal) {
+  if (UNROLL && E <= 4) {
+    int c[4];
+    MV v[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      c[e] = e < E ? rdInt(co + e * colStride) : -1;
+      v[e] = e < E ? rdVal(vo + e * valStride) : MV(0);
+    }
+    W xv[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) xv[e] = c[e] >= 0 ? xs[c[e]] : W(0);
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      if (c[e] >= 0) temp = sub(temp, mul(cvt<W>(v[e]), xv[e]));
+    return temp;
+  }
+  for (int e = 0; e < E; ++e, co += colStride, vo += valStride) {
+    const int c = rdInt(co);
+    if (c < 0) break;
+    temp = sub(temp, mul(cvt<W>(rdVal(vo)), xs[c]));
+  }
+  return temp;
+}
 
 __device__ __forceinline__ long long pad16(long long b) { return (b + 15) & ~15ll; }
 
@@ -95,12 +133,12 @@ __device__ __forceinline__ uint32_t pad16u(uint32_t b) { return (b + 15u) & ~15u
 // until the next level's bytes have landed; one barrier ends the level. The
 // ring therefore has to hold two consecutive levels (the host sizes it from
 // the largest two-level span, see ringLog2ForLevel).
-template <class MV, class W>
+template <class MV, class W, bool UNROLL>
 __global__ void __launch_bounds__(kStreamThreads) iluStreamKernel(const unsigned char* __restrict__ stream,
                                                                    const long long* __restrict__ tileOffset,
                                                                    const int* __restrict__ tileStart, int ringLog2,
-                                                                   bool dilu, SPro<W> pro, W* __restrict__ y,
-                                                                   int* errFlag) {
+                                                                   int prefetchChunks, bool dilu, SPro<W> pro,
+                                                                   W* __restrict__ y, int* errFlag) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int abortFlag;
   if (pro.st && pro.st->done) return;
@@ -134,8 +172,16 @@ __global__ void __launch_bounds__(kStreamThreads) iluStreamKernel(const unsigned
     fenceBarrierInit();
   }
   __syncthreads();
-  if (producer)
+  int pf = 0;  // next chunk to prefetch into L2 (producer lane)
+  auto prefetchTo = [&](int limit) {
+    for (; pf < total && pf < limit; ++pf)
+      prefetchL2(g + static_cast<size_t>(pf) * C, min(C, len - static_cast<uint32_t>(pf) * C));
+  };
+  if (producer) {
     for (; next < total && next < kRingChunks; ++next) issue(next);
+    pf = next;
+    prefetchTo(next + prefetchChunks);
+  }
 
   // Prologue into the tile's slice of x (overlaps the first copies).
   {
@@ -212,6 +258,7 @@ __global__ void __launch_bounds__(kStreamThreads) iluStreamKernel(const unsigned
         const int limit = static_cast<int>(off / C) + kRingChunks;
         if (next < total && next < limit) fenceProxyAsync();
         for (; next < total && next < limit; ++next) issue(next);
+        prefetchTo(next + prefetchChunks);
       }
       if (lv + 1 < nL + nU) {
         waitTo(end + 16);
@@ -222,26 +269,16 @@ __global__ void __launch_bounds__(kStreamThreads) iluStreamKernel(const unsigned
       // Forward substitution (ilu/Solver.cpp:380-411).
       for (int q = threadIdx.x; q < k; q += kComputeThreads) {
         const int il = rdInt(rowsOff + 4u * q);
-        W temp = xs[il];
-        uint32_t co = colsOff + 4u * q, vo = valsOff + static_cast<uint32_t>(sizeof(MV)) * q;
-        for (int e = 0; e < E; ++e, co += colStride, vo += valStride) {
-          const int c = rdInt(co);
-          if (c < 0) break;
-          temp = sub(temp, mul(cvt<W>(rdVal(vo)), xs[c]));
-        }
+        const W temp = rowDot<MV, UNROLL>(xs[il], E, colsOff + 4u * q, valsOff + static_cast<uint32_t>(sizeof(MV)) * q,
+                                  colStride, valStride, xs, rdInt, rdVal);
         xs[il] = dilu ? mul(temp, cvt<W>(rdVal(invOff + static_cast<uint32_t>(sizeof(MV)) * q))) : temp;
       }
     } else {
       // Backward substitution (ilu/Solver.cpp:413-442).
       for (int q = threadIdx.x; q < k; q += kComputeThreads) {
         const int il = rdInt(rowsOff + 4u * q);
-        W temp = W(0);
-        uint32_t co = colsOff + 4u * q, vo = valsOff + static_cast<uint32_t>(sizeof(MV)) * q;
-        for (int e = 0; e < E; ++e, co += colStride, vo += valStride) {
-          const int c = rdInt(co);
-          if (c < 0) break;
-          temp = sub(temp, mul(cvt<W>(rdVal(vo)), xs[c]));
-        }
+        const W temp = rowDot<MV, UNROLL>(W(0), E, colsOff + 4u * q, valsOff + static_cast<uint32_t>(sizeof(MV)) * q,
+                                  colStride, valStride, xs, rdInt, rdVal);
         const W iv = cvt<W>(rdVal(invOff + static_cast<uint32_t>(sizeof(MV)) * q));
         xs[il] = dilu ? add(xs[il], mul(temp, iv)) : mul(add(xs[il], temp), iv);
       }
@@ -315,31 +352,27 @@ void launchStreamPack(DeviceMatrix& A, const SweepStream& S, void* stream, const
 namespace {
 template <class MV, class W>
 void streamApplyT(DeviceMatrix& A, const SweepStream& S, const void* stream, bool dilu, const PrologueArgs& p,
-                  void* y, int ringLog2, cudaStream_t s) {
-  const int lg = iluStreamRingLog2(S, ringLog2);
-  const size_t smem = iluStreamSmem(A, S, dtypeOf<W>(), ringLog2);
-  auto kernel = dev::iluStreamKernel<MV, W>;
-  static thread_local size_t configured[4] = {0, 0, 0, 0};
-  const int slot = (sizeof(MV) == 8) * 2 + (sizeof(W) == 8);
-  if (smem > configured[slot]) {
-    GR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    configured[slot] = smem;
-  }
+                  void* y, const StreamTuning& tune, cudaStream_t s) {
+  const int lg = iluStreamRingLog2(S, tune.ringLog2);
+  const size_t smem = iluStreamSmem(A, S, dtypeOf<W>(), tune.ringLog2);
+  auto kernel = tune.unroll ? dev::iluStreamKernel<MV, W, true> : dev::iluStreamKernel<MV, W, false>;
+  ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
+  const int pf = tune.prefetchChunks < 0 ? dev::kPrefetchChunks : tune.prefetchChunks;
   dev::SPro<W> pro{static_cast<int>(p.kind), static_cast<const W*>(p.b), static_cast<const W*>(p.r),
                    static_cast<W*>(p.pOrS), static_cast<const W*>(p.v), p.st};
   kernel<<<A.P, dev::kStreamThreads, smem, s>>>(static_cast<const unsigned char*>(stream), S.tileOffset.as<long long>(),
-                                A.tileStart.as<int>(), lg, dilu, pro, static_cast<W*>(y), A.errFlag.as<int>());
+                                A.tileStart.as<int>(), lg, pf, dilu, pro, static_cast<W*>(y), A.errFlag.as<int>());
   checkLaunch("ilu_stream");
 }
 }  // namespace
 
 void launchIluStream(DeviceMatrix& A, const SweepStream& S, const void* stream, bool dilu,
-                     const PrologueArgs& pro, void* y, DType W, int ringLog2, cudaStream_t s) {
-  if (A.vt == DType::F32 && W == DType::F32) streamApplyT<float, float>(A, S, stream, dilu, pro, y, ringLog2, s);
+                     const PrologueArgs& pro, void* y, DType W, const StreamTuning& tune, cudaStream_t s) {
+  if (A.vt == DType::F32 && W == DType::F32) streamApplyT<float, float>(A, S, stream, dilu, pro, y, tune, s);
   else if (A.vt == DType::F32 && W == DType::F64)
-    streamApplyT<float, double>(A, S, stream, dilu, pro, y, ringLog2, s);
+    streamApplyT<float, double>(A, S, stream, dilu, pro, y, tune, s);
   else if (A.vt == DType::F64 && W == DType::F64)
-    streamApplyT<double, double>(A, S, stream, dilu, pro, y, ringLog2, s);
+    streamApplyT<double, double>(A, S, stream, dilu, pro, y, tune, s);
   else fail(GR_EUNSUPPORTED, "ILU with float64 coefficients needs float64 vectors");
 }
 

@@ -198,8 +198,7 @@ void warpApplyT(DeviceMatrix& A, const SweepStream& S, const void* stream, bool 
                 cudaStream_t s) {
   const size_t smem = 16 * static_cast<size_t>(S.maxTileLevels) + A.host->maxTileRows * sizeof(W);
   auto kernel = dev::iluWarpKernel<MV, W, J, 4>;
-  if (smem > 48 * 1024)
-    GR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
   dev::WPro<W> pro{static_cast<int>(p.kind), static_cast<const W*>(p.b), static_cast<const W*>(p.r),
                    static_cast<W*>(p.pOrS), static_cast<const W*>(p.v), p.st};
   kernel<<<A.P, 32, smem, s>>>(static_cast<const unsigned char*>(stream), S.tileOffset.as<long long>(),

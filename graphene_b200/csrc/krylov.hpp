@@ -61,8 +61,17 @@ int iluStreamRingLog2(const SweepStream& S, int requested);
 // stream = template with the factor values F and inverse diagonal inv packed in.
 void launchStreamPack(DeviceMatrix& A, const SweepStream& S, void* stream, const void* F, const void* inv,
                       cudaStream_t s);
+// Tuning of the streamed kernel: ring size (log2 bytes, 0 = the smallest
+// that fits), ring chunks kept prefetched into L2 beyond the ring (-1 = the
+// default), and whether rows of up to four entries load all their terms at
+// once.
+struct StreamTuning {
+  int ringLog2 = 0;
+  int prefetchChunks = -1;
+  bool unroll = false;
+};
 void launchIluStream(DeviceMatrix& A, const SweepStream& S, const void* stream, bool dilu,
-                     const PrologueArgs& pro, void* y, DType W, int ringLog2, cudaStream_t s);
+                     const PrologueArgs& pro, void* y, DType W, const StreamTuning& tune, cudaStream_t s);
 int maxDynamicSmem(const DeviceMatrix& A);
 // Warp-per-tile substitution (kernels_warp.cu): shared memory per block and
 // the number of rows per lane to prefetch.

@@ -120,7 +120,8 @@ class IluNode : public Node {
     if (kernel_ == 3)
       launchIluWarp(A_, *sweep_, stream_.get(), dilu_, pro, y, W, rowsPerLane_, s());
     else if (kernel_ == 1)
-      launchIluStream(A_, *sweep_, stream_.get(), dilu_, pro, y, W, cfg_.ringLog2, s());
+      launchIluStream(A_, *sweep_, stream_.get(), dilu_, pro, y, W,
+                      StreamTuning{cfg_.ringLog2, cfg_.prefetchChunks, cfg_.unrollRows}, s());
     else
       launchIluApply(A_, Lval_.get(), Uval_.get(), inv_.get(), dilu_, pro, y, W, s());
   }
@@ -522,6 +523,9 @@ class Tree : public SolverTree {
     GR_CUDA(cudaEventCreate(&e1_));
   }
   ~Tree() override {
+    // The nodes' buffers are released after this body: no work using them
+    // may still be pending on the matrix's stream.
+    cudaStreamSynchronize(A_.stream);
     cudaEventDestroy(e0_);
     cudaEventDestroy(e1_);
   }
@@ -537,9 +541,10 @@ class Tree : public SolverTree {
     st.solve_ms = ms;
     // A bounded device-side wait that ran out marks the solve as failed.
     int err = 0;
-    GR_CUDA(cudaMemcpy(&err, A_.errFlag.get(), sizeof(int), cudaMemcpyDeviceToHost));
+    GR_CUDA(cudaMemcpyAsync(&err, A_.errFlag.get(), sizeof(int), cudaMemcpyDeviceToHost, A_.stream));
+    GR_CUDA(cudaStreamSynchronize(A_.stream));
     if (err != 0) {
-      GR_CUDA(cudaMemset(A_.errFlag.get(), 0, sizeof(int)));
+      GR_CUDA(cudaMemsetAsync(A_.errFlag.get(), 0, sizeof(int), A_.stream));
       st.status = err;
       st.converged = 0;
     }

@@ -166,6 +166,40 @@ int gr_host_matrix_global_crs(const gr_host_matrix* h, int64_t* row_ptr, int64_t
 int gr_host_matrix_load_mm(const char* path, int64_t num_tiles, gr_partitioner partitioner,
                            gr_dtype value_type, gr_host_matrix** out);
 
+/* LDU matrix (matrix/details/ldu/LDUMatrix.hpp:49, LDUAddressing.hpp:42-91):
+ * num_cells cells and num_faces faces in natural numbering; owner[f]
+ * (lowerAddr) < neighbour[f] (upperAddr), faces sorted by owner; lower[f]
+ * and upper[f] are the face's coefficients in face order (upper NULL: upper
+ * = lower, a symmetric matrix), diag[num_cells]. SpMV and residual sum each
+ * row as the reference's LDUMatrix does: diag * x, then the owned faces in
+ * face order, then the neighbouring faces in losort order. The reference has
+ * no host-side LDU builder; its ILU and Gauss-Seidel solvers reject LDU
+ * matrices (ilu/Solver.cpp:554-568, gauss-seidel/Solver.cpp:88-95), here they
+ * run on the same coefficients in tile-local column order. Partitioning,
+ * value_type and the other arguments as for gr_host_matrix_from_coo. */
+int gr_host_matrix_from_ldu(int64_t num_cells, int64_t num_faces, const int64_t* owner,
+                            const int64_t* neighbour, const double* diag, const double* lower,
+                            const double* upper, int64_t num_tiles, gr_partitioner partitioner,
+                            const int32_t* row_to_tile, const double* coords, gr_dtype value_type,
+                            gr_host_matrix** out);
+
+/* Synthetic unstructured-mesh stand-in in LDU form: an nx x ny x nz
+ * hexahedral mesh, node positions jittered by U(-0.2, 0.2) spacings
+ * (jitter_seed; cell centroids drive GR_PART_RCB / AUTO), cell ids permuted
+ * (perm_seed), owner = smaller cell id, faces sorted by (owner, neighbour),
+ * face coefficient c = 10^U(-2, 2) (coef_seed), off-diagonals -c, diagonal
+ * = sum of the cell's face coefficients + 1e-3. */
+int gr_host_matrix_ldu_mesh(int64_t nx, int64_t ny, int64_t nz, uint64_t jitter_seed,
+                            uint64_t perm_seed, uint64_t coef_seed, int64_t num_tiles,
+                            gr_partitioner partitioner, gr_dtype value_type, gr_host_matrix** out);
+
+/* The LDU arrays of an LDU host matrix (values rounded to its value type):
+ * writes *num_faces, and, where the pointer is not NULL, owner, neighbour,
+ * lower, upper (num_faces each) and diag (num_cells). GR_EINVAL for a CRS
+ * matrix. */
+int gr_host_matrix_get_ldu(const gr_host_matrix* h, int64_t* num_faces, int64_t* owner,
+                           int64_t* neighbour, double* lower, double* upper, double* diag);
+
 void gr_host_matrix_destroy(gr_host_matrix* h);
 
 /* A copy of h with the same partition and layout and its coefficients
@@ -300,6 +334,56 @@ int gr_solver_name(const gr_solver* s, char* buf, size_t len);
  * are listed in unknown_keys (comma separated, may be NULL). */
 int gr_config_parse(const char* json, char* name, size_t name_len, char* unknown_keys,
                     size_t unknown_len);
+
+/* ---- solve server ------------------------------------------------------
+ * No counterpart in the reference (its Runtime runs one graph at a time).
+ * Continuous batching of independent solves on one GPU: requests are
+ * queued on arrival and admitted in arrival order as soon as a worker slot
+ * is free and their estimated device footprint fits the budget; each slot
+ * drives its own non-blocking CUDA stream, so admitted solves overlap on the
+ * device. A (host matrix, configuration) pair stays resident after its
+ * request (coefficients, layout, factors, solver buffers), so a later
+ * request for the same pair skips upload and factorisation; idle pairs are
+ * evicted oldest first when memory is needed. Results do not depend on what
+ * else is running (the kernels are deterministic). */
+typedef struct gr_server gr_server;
+
+typedef struct {
+  int32_t slots;            /* concurrent solves (worker threads / streams); 0: 4 */
+  int32_t device;           /* CUDA device; -1: the current device */
+  int64_t hbm_budget_bytes; /* admission limit on resident footprints; 0: 80% of free memory */
+} gr_server_config;
+
+typedef struct {
+  double arrival_ms;   /* submit time, ms since the server was created */
+  double admitted_ms;  /* a slot and memory were granted */
+  double finished_ms;  /* result copied back */
+  int64_t footprint_bytes; /* estimated device bytes of the request's resident pair */
+  int32_t cache_hit;   /* 1: the pair was already resident */
+  int32_t slot;
+} gr_request_times;
+
+int gr_server_create(const gr_server_config* cfg, gr_server** out);
+/* Queues the solve h x = b with the solver configuration json (the same
+ * schema as gr_solver_create), x0 = 0. b is a host vector in natural order of
+ * type t (FLOAT32 or FLOAT64), copied by the call; the server keeps h alive
+ * while the request or its resident pair needs it. */
+int gr_server_submit(gr_server* s, gr_host_matrix* h, const char* json, const void* b, gr_dtype t,
+                     uint64_t* id);
+/* Waits up to timeout_ms (< 0: no limit) for request id. On completion
+ * copies x (natural order, the request's type) to x_out (may be NULL),
+ * fills stats / times (may be NULL), forgets the request and returns the
+ * request's own status (GR_OK, or the error of its solve, message in
+ * gr_last_error). GR_ETIMEOUT if it has not finished in time (the request
+ * stays queued); GR_EINVAL for an unknown id. */
+int gr_server_wait(gr_server* s, uint64_t id, double timeout_ms, void* x_out, gr_stats* stats,
+                   gr_request_times* times);
+/* Current counts: queued, running, completed; device bytes held by resident
+ * pairs; number of resident pairs. Any pointer may be NULL. */
+int gr_server_counters(gr_server* s, int64_t* queued, int64_t* running, int64_t* completed,
+                       int64_t* bytes_in_use, int64_t* resident);
+/* Finishes the running solves, drops the queued ones, releases everything. */
+void gr_server_destroy(gr_server* s);
 
 #ifdef __cplusplus
 }

@@ -317,6 +317,18 @@ struct Local {
   size_t nColors = 0;
 };
 
+// A tile's LDU addressing in the reference's terms (LDUAddressing.hpp:42-91),
+// over tile-local cell ids (halo cells included): local row c owns the faces
+// [ownerStart[c], ownerStart[c+1]) (upper coefficient, x at upperAddr) and
+// neighbours the faces neighbourColInd[s] for s in
+// [neighbourStart[c], neighbourStart[c+1]) (lower coefficient lowerLosort[s],
+// x at lowerAddr[face]). Faces owned by a halo cell are appended after the
+// owned ones so that lowerAddr covers every face a row needs.
+struct LocalLdu {
+  std::vector<size_t> ownerStart, upperAddr, neighbourStart, neighbourColInd, lowerAddr;
+  std::vector<double> upper, lowerLosort;
+};
+
 }  // namespace
 
 struct or_matrix {
@@ -331,6 +343,8 @@ struct or_matrix {
   std::vector<size_t> haloStart;  // layout with halo
   size_t nWithHalo = 0;
   bool multicolor = false;
+  bool ldu = false;
+  std::vector<LocalLdu> lloc;
 };
 
 namespace {
@@ -542,26 +556,52 @@ I rowSum(const Local& L, const std::vector<V>& off, const std::vector<V>& dg, co
   return sum;
 }
 
-// Coefficients of each tile in the stored type.
+// Coefficients of each tile in the stored type (and, for LDU matrices, the
+// upper and losort-ordered lower coefficients).
 template <class V>
 struct TileValues {
-  std::vector<std::vector<V>> off, diag;
-  explicit TileValues(const or_matrix& A) : off(A.P), diag(A.P) {
+  std::vector<std::vector<V>> off, diag, up, lo;
+  explicit TileValues(const or_matrix& A) : off(A.P), diag(A.P), up(A.P), lo(A.P) {
     for (size_t t = 0; t < A.P; ++t) {
       off[t].assign(A.loc[t].off.begin(), A.loc[t].off.end());
       diag[t].assign(A.loc[t].diag.begin(), A.loc[t].diag.end());
+      if (A.ldu) {
+        up[t].assign(A.lloc[t].upper.begin(), A.lloc[t].upper.end());
+        lo[t].assign(A.lloc[t].lowerLosort.begin(), A.lloc[t].lowerLosort.end());
+      }
     }
   }
 };
+
+// LDUMatrix::spmv / residual row loop (LDUMatrix.cpp:64-86, 128-152):
+// sum = diag * x[c], then the owned faces in face order, then the
+// neighbouring faces in losort order, in type I.
+template <class V, class X, class I>
+I rowSumLdu(const LocalLdu& L, const std::vector<V>& up, const std::vector<V>& lo, const std::vector<V>& dg,
+            const std::vector<X>& x, size_t hb, size_t c) {
+  I sum = static_cast<I>(dg[c]) * static_cast<I>(x[hb + c]);
+  for (size_t f = L.ownerStart[c]; f < L.ownerStart[c + 1]; ++f)
+    sum += static_cast<I>(up[f]) * static_cast<I>(x[hb + L.upperAddr[f]]);
+  for (size_t s = L.neighbourStart[c]; s < L.neighbourStart[c + 1]; ++s) {
+    const size_t face = L.neighbourColInd[s];
+    sum += static_cast<I>(lo[s]) * static_cast<I>(x[hb + L.lowerAddr[face]]);
+  }
+  return sum;
+}
+
+template <class V, class X, class I>
+I rowTotal(const or_matrix& A, const TileValues<V>& tv, size_t t, const std::vector<X>& x, size_t hb, size_t i) {
+  if (A.ldu) return rowSumLdu<V, X, I>(A.lloc[t], tv.up[t], tv.lo[t], tv.diag[t], x, hb, i);
+  return rowSum<V, X, I>(A.loc[t], tv.off[t], tv.diag[t], x, hb, i);
+}
 
 template <class V, class T>
 void spmvT(const or_matrix& A, const TileValues<V>& tv, std::vector<T>& x, std::vector<T>& y) {
   exchange(A, x);
   forTiles(A.P, [&](size_t t) {
-    const Local& L = A.loc[t];
     size_t nr = A.tileStart[t + 1] - A.tileStart[t];
     for (size_t i = 0; i < nr; ++i)
-      y[A.haloStart[t] + i] = rowSum<V, T, T>(L, tv.off[t], tv.diag[t], x, A.haloStart[t], i);
+      y[A.haloStart[t] + i] = rowTotal<V, T, T>(A, tv, t, x, A.haloStart[t], i);
   });
 }
 
@@ -570,11 +610,10 @@ void residualT(const or_matrix& A, const TileValues<V>& tv, std::vector<X>& x, c
                std::vector<R>& r) {
   exchange(A, x);
   forTiles(A.P, [&](size_t t) {
-    const Local& L = A.loc[t];
     size_t nr = A.tileStart[t + 1] - A.tileStart[t];
     size_t hb = A.haloStart[t];
     for (size_t i = 0; i < nr; ++i) {
-      I sum = rowSum<V, X, I>(L, tv.off[t], tv.diag[t], x, hb, i);
+      I sum = rowTotal<V, X, I>(A, tv, t, x, hb, i);
       r[hb + i] = static_cast<R>(static_cast<I>(b[hb + i]) - sum);
     }
   });
@@ -595,8 +634,16 @@ void residualDw(const or_matrix& A, const TileValues<float>& tv, std::vector<X>&
     size_t hb = A.haloStart[t];
     for (size_t i = 0; i < nr; ++i) {
       DW sum = dwTimesFp(asDw(x[hb + i]), tv.diag[t][i]);
-      for (size_t j = L.rowPtr[i]; j < L.rowPtr[i + 1]; ++j)
-        sum = dwPlusDw(sum, dwTimesFp(asDw(x[hb + L.colInd[j]]), tv.off[t][j]));
+      if (A.ldu) {
+        const LocalLdu& D = A.lloc[t];
+        for (size_t f = D.ownerStart[i]; f < D.ownerStart[i + 1]; ++f)
+          sum = dwPlusDw(sum, dwTimesFp(asDw(x[hb + D.upperAddr[f]]), tv.up[t][f]));
+        for (size_t s = D.neighbourStart[i]; s < D.neighbourStart[i + 1]; ++s)
+          sum = dwPlusDw(sum, dwTimesFp(asDw(x[hb + D.lowerAddr[D.neighbourColInd[s]]]), tv.lo[t][s]));
+      } else {
+        for (size_t j = L.rowPtr[i]; j < L.rowPtr[i + 1]; ++j)
+          sum = dwPlusDw(sum, dwTimesFp(asDw(x[hb + L.colInd[j]]), tv.off[t][j]));
+      }
       DW res = dwPlusDw(DW{b[hb + i], 0.0f}, DW{-sum.h, -sum.l});
       r[hb + i] = res.h + res.l;
     }
@@ -1067,6 +1114,82 @@ or_matrix* or_build(int64_t n, int64_t nnz, const int64_t* rows, const int64_t* 
           ent[i] = {static_cast<size_t>(rows[i]), static_cast<size_t>(cols[i]), roundVT(value_type, vals[i])};
         }
         buildMatrix(*A, std::move(ent), n, num_tiles, row_to_tile);
+      })) {
+    delete A;
+    return nullptr;
+  }
+  return A;
+}
+
+or_matrix* or_build_ldu(int64_t n, int64_t num_faces, const int64_t* owner, const int64_t* neighbour,
+                        const double* diag, const double* lower, const double* upper, int64_t num_tiles,
+                        const int32_t* row_to_tile, int value_type) {
+  or_matrix* A = new or_matrix();
+  if (guard([&] {
+        A->vt = value_type;
+        const double* up = upper ? upper : lower;
+        std::vector<std::tuple<size_t, size_t, double>> ent;
+        ent.reserve(n + 2 * num_faces);
+        for (int64_t c = 0; c < n; ++c) ent.emplace_back(c, c, roundVT(value_type, diag[c]));
+        for (int64_t f = 0; f < num_faces; ++f) {
+          if (owner[f] < 0 || owner[f] >= neighbour[f] || neighbour[f] >= n) throw OErr("bad face");
+          ent.emplace_back(owner[f], neighbour[f], roundVT(value_type, up[f]));
+          ent.emplace_back(neighbour[f], owner[f], roundVT(value_type, lower[f]));
+        }
+        buildMatrix(*A, std::move(ent), n, num_tiles, row_to_tile);
+        // Global addressing: owned faces per cell (faces are sorted by
+        // owner) and losort (faces by neighbour, then face index).
+        std::vector<size_t> ownerStart(n + 1, 0), losortStart(n + 1, 0), losort(num_faces);
+        for (int64_t f = 0; f < num_faces; ++f) {
+          ownerStart[owner[f] + 1]++;
+          losortStart[neighbour[f] + 1]++;
+        }
+        for (int64_t c = 0; c < n; ++c) {
+          ownerStart[c + 1] += ownerStart[c];
+          losortStart[c + 1] += losortStart[c];
+        }
+        std::vector<size_t> fill(losortStart.begin(), losortStart.end() - 1);
+        for (int64_t f = 0; f < num_faces; ++f) losort[fill[neighbour[f]]++] = f;
+        A->ldu = true;
+        A->lloc.resize(A->P);
+        for (size_t t = 0; t < A->P; ++t) {
+          const Tile& T = A->tiles[t];
+          LocalLdu& L = A->lloc[t];
+          const size_t nr = A->tileStart[t + 1] - A->tileStart[t];
+          std::unordered_map<size_t, size_t> localFace;
+          std::vector<size_t> faceOwner;
+          L.ownerStart.push_back(0);
+          for (size_t c = 0; c < nr; ++c) {
+            const size_t gc = T.l2g[c];
+            for (size_t f = ownerStart[gc]; f < ownerStart[gc + 1]; ++f) {
+              localFace[f] = L.upperAddr.size();
+              L.upperAddr.push_back(T.g2l.at(neighbour[f]));
+              L.upper.push_back(roundVT(value_type, up[f]));
+              faceOwner.push_back(c);
+            }
+            L.ownerStart.push_back(L.upperAddr.size());
+          }
+          L.neighbourStart.push_back(0);
+          for (size_t c = 0; c < nr; ++c) {
+            const size_t gc = T.l2g[c];
+            for (size_t s = losortStart[gc]; s < losortStart[gc + 1]; ++s) {
+              const size_t f = losort[s];
+              auto it = localFace.find(f);
+              size_t lf;
+              if (it != localFace.end()) {
+                lf = it->second;
+              } else {  // owned by a halo cell
+                lf = faceOwner.size();
+                localFace[f] = lf;
+                faceOwner.push_back(T.g2l.at(owner[f]));
+              }
+              L.neighbourColInd.push_back(lf);
+              L.lowerLosort.push_back(roundVT(value_type, lower[f]));
+            }
+            L.neighbourStart.push_back(L.neighbourColInd.size());
+          }
+          L.lowerAddr = faceOwner;
+        }
       })) {
     delete A;
     return nullptr;

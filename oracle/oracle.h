@@ -36,6 +36,14 @@ typedef struct or_matrix or_matrix;
 or_matrix* or_build(int64_t n, int64_t nnz, const int64_t* rows, const int64_t* cols,
                     const double* vals, int64_t num_tiles, const int32_t* row_to_tile,
                     int value_type);
+/* An LDU matrix (LDUMatrix.hpp, LDUAddressing.hpp:42-91): faces with owner <
+ * neighbour sorted by owner, lower / upper coefficients in face order (upper
+ * NULL: upper = lower), diag. Built like or_build from the equivalent
+ * triplets; SpMV and residual then run the reference's LDU row loops
+ * (LDUMatrix.cpp:42-168) over per-tile LDU addressing. */
+or_matrix* or_build_ldu(int64_t n, int64_t num_faces, const int64_t* owner, const int64_t* neighbour,
+                        const double* diag, const double* lower, const double* upper, int64_t num_tiles,
+                        const int32_t* row_to_tile, int value_type);
 /* generate3DPoissonTripletMatrix (Poisson.cpp:26-69) then or_build. */
 or_matrix* or_poisson(int64_t nx, int64_t ny, int64_t nz, int64_t num_tiles,
                       const int32_t* row_to_tile, int value_type);

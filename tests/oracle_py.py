@@ -39,6 +39,7 @@ class Oracle:
         L = C.CDLL(str(LIB))
         sig = {
             "or_build": (vp, [i64, i64, vp, vp, vp, i64, vp, C.c_int]),
+            "or_build_ldu": (vp, [i64, i64, vp, vp, vp, vp, vp, i64, vp, C.c_int]),
             "or_poisson": (vp, [i64, i64, i64, i64, vp, C.c_int]),
             "or_free": (None, [vp]),
             "or_last_error": (C.c_char_p, []),
@@ -83,6 +84,18 @@ class Oracle:
         v = np.ascontiguousarray(vals, np.float64)
         rt = None if row_to_tile is None else np.ascontiguousarray(row_to_tile, np.int32)
         h = self.L.or_build(n, len(v), _p(r), _p(c), _p(v), num_tiles, _p(rt), value_type)
+        if not h:
+            raise RuntimeError(self.err())
+        return OMatrix(self, h, value_type)
+
+    def ldu(self, n, owner, neighbour, diag, lower, upper, num_tiles, row_to_tile,
+            value_type=0) -> "OMatrix":
+        a = [np.ascontiguousarray(v, t) for v, t in ((owner, np.int64), (neighbour, np.int64),
+                                                     (diag, np.float64), (lower, np.float64))]
+        up = None if upper is None else np.ascontiguousarray(upper, np.float64)
+        rt = None if row_to_tile is None else np.ascontiguousarray(row_to_tile, np.int32)
+        h = self.L.or_build_ldu(n, len(a[0]), _p(a[0]), _p(a[1]), _p(a[2]), _p(a[3]), _p(up),
+                                num_tiles, _p(rt), value_type)
         if not h:
             raise RuntimeError(self.err())
         return OMatrix(self, h, value_type)
