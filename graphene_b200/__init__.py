@@ -434,9 +434,12 @@ class Matrix:
         torch = _torch()
         return torch.empty(self.numRows, dtype=_torch_dtype(parseType(t)), device=self.device)
 
-    def vector(self, natural, t: int = FLOAT32):
-        """Device vector in tile order from a natural-order host array."""
+    def vector(self, natural, t: int = None):
+        """Device vector in tile order from a natural-order host array (type t,
+        default: float64 for a float64 array, else float32)."""
         torch = _torch()
+        if t is None:
+            t = FLOAT64 if np.asarray(natural).dtype == np.float64 else FLOAT32
         return torch.from_numpy(self.host.decomposeVector(natural, t)).to(self.device)
 
     def toNatural(self, x) -> np.ndarray:

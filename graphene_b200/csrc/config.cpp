@@ -245,11 +245,23 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
     if (const Json* v = j.find("preconditioner")) c->preconditioner = fromJson(*v);
   } else if (ty == "ILU") {
     mark("solveMulticolor"); mark("factorizeMulticolor"); mark("diagonalBased"); mark("kernel");
-    mark("ringLog2"); mark("prefetch"); mark("unroll");
+    mark("ringLog2"); mark("prefetch"); mark("unroll"); mark("ringBytes"); mark("l2Ahead"); mark("tilesPerBlock");
+    readInt(j, "tilesPerBlock", c->tilesPerBlock);
+    if (c->tilesPerBlock < 0 || c->tilesPerBlock > 64) fail(GR_EINVAL, "tilesPerBlock must be 0 (default) or 1..64");
+    readInt(j, "l2Ahead", c->l2Ahead);
+    if (c->l2Ahead < -1 || c->l2Ahead > (1 << 24)) fail(GR_EINVAL, "l2Ahead must be -1 (default) or 0..16 MiB");
+    if (const Json* v = j.find("ringBytes")) {
+      c->ringBytes = std::stoll(v->text);
+      if (c->ringBytes < 0 || c->ringBytes > 200 * 1024) fail(GR_EINVAL, "ringBytes must be 0 (default) or up to 204800");
+    }
     readInt(j, "ringLog2", c->ringLog2);
     readInt(j, "prefetch", c->prefetchChunks);
     if (c->prefetchChunks < -1 || c->prefetchChunks > 64) fail(GR_EINVAL, "prefetch must be -1 (default) or 0..64");
-    readBool(j, "unroll", c->unrollRows);
+    if (j.find("unroll")) {
+      bool u = false;
+      readBool(j, "unroll", u);
+      c->unrollRows = u ? 1 : 0;
+    }
     if (c->ringLog2 != 0 && (c->ringLog2 < 13 || c->ringLog2 > 17))
       fail(GR_EINVAL, "ringLog2 must be 0 (automatic) or between 13 and 17");
     readMultiColor(j, "solveMulticolor", c->solveMulticolor);
@@ -260,7 +272,8 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
       else if (v->text == "tma") c->iluKernel = 1;
       else if (v->text == "levels") c->iluKernel = 2;
       else if (v->text == "warp") c->iluKernel = 3;
-      else fail(GR_EPARSE, "ILU kernel must be \"auto\", \"warp\", \"tma\" or \"levels\"");
+      else if (v->text == "ring") c->iluKernel = 4;
+      else fail(GR_EPARSE, "ILU kernel must be \"auto\", \"ring\", \"warp\", \"tma\" or \"levels\"");
     }
   } else if (ty == "GaussSeidel") {
     mark("numSweeps"); mark("numFixedIterations"); mark("solveMulticolor"); mark("workingType");

@@ -40,10 +40,19 @@ struct SolverConfig {
   MultiColorMode solveMulticolor = MultiColorMode::Auto;
   MultiColorMode factorizeMulticolor = MultiColorMode::Auto;
   bool diagonalBased = false;
-  // Extension: substitution kernel, "auto" (the bulk-copy ring kernel when
-  // the tile fits shared memory, else the level-schedule kernel), "tma",
-  // "warp" (warp per tile) or "levels".
-  int iluKernel = 0;  // 0 auto, 1 tma, 2 levels, 3 warp
+  // Extension: substitution kernel, "auto" (the host-scheduled ring kernel
+  // when a tile fits shared memory, else the level-schedule kernel), "ring",
+  // "tma" (chunked byte ring with a producer warp), "warp" (warp per tile)
+  // or "levels".
+  int iluKernel = 0;  // 0 auto, 1 tma, 2 levels, 3 warp, 4 ring
+  // Extension: shared-memory ring bytes of the "ring" kernel (0: default).
+  long long ringBytes = 0;
+  // Extension: bytes the "ring" kernel keeps prefetched into L2 beyond its
+  // issued copies (-1: default).
+  int l2Ahead = -1;
+  // Extension: tiles one thread block of the "ring" kernel runs in lockstep
+  // (0: default).
+  int tilesPerBlock = 0;
   // Extension: log2 of the streamed kernel's ring size in bytes (0: the
   // smallest ring that holds the largest level).
   int ringLog2 = 0;
@@ -51,7 +60,7 @@ struct SolverConfig {
   // beyond its ring (-1: default), and whether it loads all terms of short
   // rows at once.
   int prefetchChunks = -1;
-  bool unrollRows = false;
+  int unrollRows = -1;  // -1: the kernel's default, 0 off, 1 on
   // GaussSeidel (gauss-seidel/Configuration.hpp:19-21)
   int numSweeps = 1, numFixedIterations = 0;
   // Extension: "seed": "b" (default, the codelet specification

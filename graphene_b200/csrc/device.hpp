@@ -4,8 +4,10 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
 #include <memory>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "common.hpp"
@@ -143,6 +145,47 @@ int ringLog2ForLevel(i64 maxSpanBytes);
 // out-of-range index, ordering or ring-capacity violation.
 void checkIluStream(const HostMatrix& H, const HostStream& S, bool dilu, DType vt, int ringLog2);
 
+// Level blocks for the host-scheduled ring kernel (kernels_ring.cu). Per
+// tile, the levels in execution order (lower ascending, then upper
+// descending); a level block is
+//   rows  k x i32 tile-local row ids                            (16-byte padded)
+//   inv   k x value type inverse diagonal (upper levels, DILU)  (padded)
+//   ents  E*k entries, entry-major, {i32 column, value}: 8 bytes for float,
+//         16 for double ({column, 0, value})                    (padded)
+// Padding entries use column nRows (a zero slot of the kernel's x slice) and
+// value 0. Two int4 per level: {k, E, block bytes, ring offset} and
+// {inv offset, entries offset, issueAfter, upper}. The kernel copies a
+// level's block into its shared-memory ring at `ring offset` once the tile's
+// level `issueAfter` has been consumed (-1: at the start); the host chose the
+// offsets so that a copy never overwrites a level still to be consumed, and
+// so that every level is copied at least one level before it is needed.
+constexpr int kRingBarriers = 16;
+struct HostRing {
+  std::vector<uint8_t> bytes;
+  std::vector<i64> tileOffset;  // P + 1
+  std::vector<int4> meta;       // 2 per level
+  std::vector<i32> tileLevel;   // P + 1
+  std::vector<i32> valPos, valSrc, invPos, invSrc;  // element positions (value type units)
+  i64 ringBytes = 0, maxLevelBytes = 0, maxGroupRows = 0;
+  i32 maxTileLevels = 0;
+  i32 group = 1;                // tiles per thread block
+  std::vector<i32> groupStart;  // first tile-order row of every block, and n
+};
+// One thread block runs `group` consecutive tiles in lockstep (tileOffset,
+// tileLevel and meta are then per block). ringBytes 0: the default,
+// max(16 KB, 2.5 x the largest level block).
+HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes, i32 group);
+// Replays the kernel's copies and reads on the host; throws GR_EINVAL on an
+// out-of-range index, a dependency-order violation, a copy that would
+// overwrite a level not yet consumed, or a copy issued too late.
+void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt);
+struct LevelRing {
+  bool dilu = false;
+  i64 bytes = 0, ringBytes = 0, nVal = 0, nInv = 0, maxGroupRows = 0;
+  i32 maxTileLevels = 0, group = 1, numGroups = 0;
+  DBuf tileOffset, templ, meta, tileLevel, groupStart, valPos, valSrc, invPos, invSrc;
+};
+
 // Kinds of entries a schedule keeps per row.
 enum class SweepEntries {
   Lower,        // tile-local columns below the row, ascending (ILU forward)
@@ -175,6 +218,8 @@ struct DeviceMatrix {
   std::unique_ptr<LevelSchedule> lowerSched, upperSched, gsSched;
   std::unique_ptr<SweepStream> iluStream[2];  // [dilu]
   SweepStream& iluSweepStream(bool dilu);
+  std::map<std::tuple<bool, i64, i32>, std::unique_ptr<LevelRing>> levelRings;  // [(dilu, ring bytes, group)]
+  LevelRing& levelRing(bool dilu, i64 ringBytes, i32 group);
 
   // Device error word written by kernels whose bounded waits ran out
   // (GR_ETIMEOUT); 0 when clean.

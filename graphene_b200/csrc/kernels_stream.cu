@@ -16,6 +16,7 @@
 // its outstanding copies before the block exits.
 #include <algorithm>
 
+#include "bulk.cuh"
 #include "devmath.cuh"
 #include "krylov.hpp"
 #include "sell.cuh"
@@ -24,42 +25,6 @@ namespace gr {
 namespace dev {
 
 constexpr int kRingChunks = 8;
-constexpr long long kWaitLimit = 1ll << 22;
-
-__device__ __forceinline__ uint32_t smemAddr(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbarInit(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void fenceBarrierInit() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbarExpectTx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulkLoad(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-      "l"(src), "r"(bytes), "r"(bar)
-      : "memory");
-}
-__device__ __forceinline__ bool mbarTryWait(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ void fenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-// Hint: bring [src, src + bytes) into L2 (no completion, no shared memory).
-__device__ __forceinline__ void prefetchL2(const void* src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
-}
 
 // Default number of chunks beyond the ring that the producer keeps
 // prefetched into L2, so that a refill reads L2 instead of HBM.
@@ -96,29 +61,6 @@ __device__ __forceinline__ W rowDot(W temp, int E, uint32_t co, uint32_t vo, uin
 }
 
 __device__ __forceinline__ long long pad16(long long b) { return (b + 15) & ~15ll; }
-
-// Pro<W> (the fused prologue) is defined in kernels_precond.cu; a local copy
-// of the same functor keeps this translation unit self-contained.
-template <class W>
-struct SPro {
-  int kind;
-  const W* __restrict__ b;
-  const W* __restrict__ r;
-  W* pOrS;
-  const W* __restrict__ v;
-  const KState* st;
-  __device__ __forceinline__ W operator()(int i, W beta, W omega, W alpha, bool first) const {
-    if (kind == static_cast<int>(Prologue::Plain)) return b[i];
-    if (kind == static_cast<int>(Prologue::PUpdate)) {
-      W p = first ? r[i] : add(r[i], mul(beta, sub(pOrS[i], mul(omega, v[i]))));
-      pOrS[i] = p;
-      return p;
-    }
-    W s = sub(r[i], mul(alpha, v[i]));
-    pOrS[i] = s;
-    return s;
-  }
-};
 
 // Four compute warps and one producer warp per tile.
 constexpr int kComputeThreads = 128;
@@ -333,20 +275,26 @@ size_t iluStreamSmem(const DeviceMatrix& A, const SweepStream& S, DType W, int r
   return 128 + (size_t(1) << lg) + static_cast<size_t>(A.host->maxTileRows) * dtypeSize(W);
 }
 
-void launchStreamPack(DeviceMatrix& A, const SweepStream& S, void* stream, const void* F, const void* inv,
-                      cudaStream_t s) {
-  GR_CUDA(cudaMemcpyAsync(stream, S.templ.get(), S.bytes, cudaMemcpyDeviceToDevice, s));
-  const int blocks = static_cast<int>(std::max<i64>(1, std::min<i64>(A.redBlocks, (S.nVal + 255) / 256)));
+void launchPackBytes(DeviceMatrix& A, const void* templ, i64 bytes, const int* valPos, const int* valSrc, i64 nVal,
+                     const int* invPos, const int* invSrc, i64 nInv, void* stream, const void* F, const void* inv,
+                     cudaStream_t s) {
+  GR_CUDA(cudaMemcpyAsync(stream, templ, bytes, cudaMemcpyDeviceToDevice, s));
+  const int blocks = static_cast<int>(std::max<i64>(1, std::min<i64>(A.redBlocks, (std::max(nVal, nInv) + 255) / 256)));
   if (A.vt == DType::F32)
-    dev::streamPackKernel<float><<<blocks, 256, 0, s>>>(static_cast<float*>(stream), S.valPos.as<int>(),
-                                                        S.valSrc.as<int>(), S.nVal, static_cast<const float*>(F),
-                                                        S.invPos.as<int>(), S.invSrc.as<int>(), S.nInv,
+    dev::streamPackKernel<float><<<blocks, 256, 0, s>>>(static_cast<float*>(stream), valPos, valSrc, nVal,
+                                                        static_cast<const float*>(F), invPos, invSrc, nInv,
                                                         static_cast<const float*>(inv));
   else
-    dev::streamPackKernel<double><<<blocks, 256, 0, s>>>(
-        static_cast<double*>(stream), S.valPos.as<int>(), S.valSrc.as<int>(), S.nVal, static_cast<const double*>(F),
-        S.invPos.as<int>(), S.invSrc.as<int>(), S.nInv, static_cast<const double*>(inv));
+    dev::streamPackKernel<double><<<blocks, 256, 0, s>>>(static_cast<double*>(stream), valPos, valSrc, nVal,
+                                                         static_cast<const double*>(F), invPos, invSrc, nInv,
+                                                         static_cast<const double*>(inv));
   checkLaunch("stream_pack");
+}
+
+void launchStreamPack(DeviceMatrix& A, const SweepStream& S, void* stream, const void* F, const void* inv,
+                      cudaStream_t s) {
+  launchPackBytes(A, S.templ.get(), S.bytes, S.valPos.as<int>(), S.valSrc.as<int>(), S.nVal, S.invPos.as<int>(),
+                  S.invSrc.as<int>(), S.nInv, stream, F, inv, s);
 }
 
 namespace {

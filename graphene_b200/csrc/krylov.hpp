@@ -73,6 +73,20 @@ struct StreamTuning {
 void launchIluStream(DeviceMatrix& A, const SweepStream& S, const void* stream, bool dilu,
                      const PrologueArgs& pro, void* y, DType W, const StreamTuning& tune, cudaStream_t s);
 int maxDynamicSmem(const DeviceMatrix& A);
+// Copies a stream template and packs factor values F and the inverse
+// diagonal inv into it (element positions in units of the value type).
+void launchPackBytes(DeviceMatrix& A, const void* templ, i64 bytes, const int* valPos, const int* valSrc, i64 nVal,
+                     const int* invPos, const int* invSrc, i64 nInv, void* stream, const void* F, const void* inv,
+                     cudaStream_t s);
+// Host-scheduled ring substitution (kernels_ring.cu): dynamic shared memory
+// per block, packing of a solver's copy of the level blocks, and the launch.
+size_t iluRingSmem(const DeviceMatrix& A, const LevelRing& R, DType W);
+void launchRingPack(DeviceMatrix& A, const LevelRing& R, void* stream, const void* F, const void* inv,
+                    cudaStream_t s);
+// l2Ahead: bytes kept prefetched into L2 beyond the issued copies (-1:
+// default); unroll: rows of up to four entries load all their terms at once.
+void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,
+                   void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s);
 // Warp-per-tile substitution (kernels_warp.cu): shared memory per block and
 // the number of rows per lane to prefetch.
 size_t iluWarpSmem(const DeviceMatrix& A, const SweepStream& S, DType W);

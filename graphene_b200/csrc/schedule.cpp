@@ -375,3 +375,271 @@ SweepStream& DeviceMatrix::iluSweepStream(bool dilu) {
 }
 
 }  // namespace gr
+
+// ---------------------------------------------------------------------------
+// Host-scheduled level ring (kernels_ring.cu).
+namespace gr {
+
+namespace {
+struct TileRing {
+  std::vector<uint8_t> bytes;
+  std::vector<int4> meta;
+  std::vector<std::pair<i64, i32>> vals;  // (byte offset of the value, CRS source)
+  std::vector<std::pair<i64, i32>> invs;  // (byte offset, tile-order row)
+  std::vector<i64> size;
+  i64 maxLevel = 0;
+};
+
+inline bool overlaps(i64 a, i64 sa, i64 b, i64 sb) { return a < b + sb && b < a + sa; }
+}  // namespace
+
+HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes, i32 group) {
+  const i64 vs = static_cast<i64>(dtypeSize(vt));
+  const i64 entSize = vs == 4 ? 8 : 16;
+  if (group < 1) fail(GR_EINVAL, "tiles per block must be at least 1");
+  // A block runs `group` consecutive tiles in lockstep: level l of the block
+  // is level l of each of its tiles (the tiles are independent, so their
+  // rows never reference one another), rows numbered from the block's first
+  // row.
+  const i32 NG = (H.P + group - 1) / group;
+  std::vector<TileRing> tr(NG);
+  parallelFor(NG, [&](i64 G) {
+    TileRing& t = tr[G];
+    const i32 T0 = static_cast<i32>(G) * group, T1 = std::min<i32>(H.P, T0 + group);
+    const i64 gBase = H.tileStart[T0];
+    const i64 gRows = H.tileStart[T1] - gBase;
+    std::vector<i64> ent;
+    for (int sweep = 0; sweep < 2; ++sweep) {
+      const bool upper = sweep == 1;
+      const SweepEntries kind = upper ? SweepEntries::UpperDesc : SweepEntries::Lower;
+      const std::vector<i32>& lev = upper ? H.upperLevel : H.lowerLevel;
+      i32 nLv = 0;
+      for (i32 T = T0; T < T1; ++T) nLv = std::max(nLv, upper ? H.nUpperLevels[T] : H.nLowerLevels[T]);
+      // (block-local row, tile) per level
+      std::vector<std::vector<std::pair<i64, i32>>> byLevel(nLv);
+      for (i32 T = T0; T < T1; ++T)
+        for (i64 p = H.tileStart[T]; p < H.tileStart[T + 1]; ++p) byLevel[lev[p]].emplace_back(p - gBase, T);
+      const bool hasInv = upper || dilu;
+      for (i32 l = 0; l < nLv; ++l) {
+        const auto& rows = byLevel[l];
+        const i64 k = static_cast<i64>(rows.size());
+        i64 E = 0;
+        for (const auto& [gl, T] : rows) {
+          const i64 tb = H.tileStart[T] - gBase;
+          rowEntries(H, kind, gBase + gl, gl - tb, H.tileStart[T + 1] - H.tileStart[T], ent);
+          E = std::max<i64>(E, static_cast<i64>(ent.size()));
+        }
+        const i64 rowsB = pad16(4 * k), invB = hasInv ? pad16(vs * k) : 0, entB = pad16(entSize * E * k);
+        const i64 S = rowsB + invB + entB;
+        const i64 start = static_cast<i64>(t.bytes.size());
+        t.bytes.resize(start + S, 0);
+        for (i64 q = 0; q < k; ++q) {
+          const auto [gl, T] = rows[q];
+          const i64 tb = H.tileStart[T] - gBase;
+          const i32 r32 = static_cast<i32>(gl);
+          std::memcpy(t.bytes.data() + start + 4 * q, &r32, 4);
+          if (hasInv) t.invs.emplace_back(start + rowsB + vs * q, static_cast<i32>(gBase + gl));
+          rowEntries(H, kind, gBase + gl, gl - tb, H.tileStart[T + 1] - H.tileStart[T], ent);
+          for (i64 e = 0; e < E; ++e) {
+            const i64 pos = start + rowsB + invB + entSize * (e * k + q);
+            const bool real = e < static_cast<i64>(ent.size());
+            const i32 col = real ? static_cast<i32>(H.colLocal[ent[e]] + tb) : static_cast<i32>(gRows);
+            std::memcpy(t.bytes.data() + pos, &col, 4);
+            if (real) t.vals.emplace_back(pos + (vs == 4 ? 4 : 8), static_cast<i32>(ent[e]));
+          }
+        }
+        t.meta.push_back(make_int4(static_cast<int>(k), static_cast<int>(E), static_cast<int>(S), 0));
+        t.meta.push_back(make_int4(static_cast<int>(rowsB), static_cast<int>(rowsB + invB), -1, upper ? 1 : 0));
+        t.size.push_back(S);
+        t.maxLevel = std::max(t.maxLevel, S);
+      }
+    }
+  });
+  HostRing R;
+  for (const TileRing& t : tr) R.maxLevelBytes = std::max(R.maxLevelBytes, t.maxLevel);
+  // Ring placement: levels one after another, wrapping to the start when a
+  // level does not fit before the end; a level's copy waits for the most
+  // recent earlier level whose block it overlaps, and for the level that
+  // last used its completion barrier. Placement fails when some level would
+  // have to wait for the level right before it.
+  auto place = [&](i64 ring) {
+    std::atomic<bool> ok{true};
+    parallelFor(NG, [&](i64 T) {
+      TileRing& t = tr[T];
+      const i64 L = static_cast<i64>(t.size.size());
+      std::vector<i64> off(L);
+      i64 pos = 0, prevIa = -1;
+      for (i64 l = 0; l < L && ok; ++l) {
+        const i64 S = t.size[l];
+        if (S > ring) { ok = false; return; }
+        if (pos + S > ring) pos = 0;
+        off[l] = pos;
+        pos += S;
+        i64 ia = -1;
+        for (i64 j = l - 1; j >= 0; --j)
+          if (overlaps(off[j], t.size[j], off[l], S)) { ia = j; break; }
+        ia = std::max({ia, l - kRingBarriers, prevIa});
+        if (l >= 1 && ia > l - 2) { ok = false; return; }
+        t.meta[2 * l].w = static_cast<int>(off[l]);
+        t.meta[2 * l + 1].z = static_cast<int>(ia);
+        prevIa = ia;
+      }
+    });
+    return ok.load();
+  };
+  if (ringBytes > 0) {
+    R.ringBytes = pad16(ringBytes);
+    if (!place(R.ringBytes))
+      fail(GR_EINVAL, "ILU level ring of " + std::to_string(R.ringBytes) + " bytes is too small for this matrix's levels");
+  } else {
+    // Default: the smallest ring from max(16 KB, 2.5 x the largest level) up,
+    // in steps of half a level, that the placement accepts (3 x always does).
+    const i64 step = std::max<i64>(16, pad16(R.maxLevelBytes / 2));
+    R.ringBytes = std::max<i64>(16384, pad16(2 * R.maxLevelBytes + R.maxLevelBytes / 2));
+    while (!place(R.ringBytes)) R.ringBytes += step;
+  }
+  if (R.ringBytes >= (i64(1) << 30)) fail(GR_EUNSUPPORTED, "ILU level ring too large");
+  R.group = group;
+  R.tileOffset.assign(NG + 1, 0);
+  R.tileLevel.assign(NG + 1, 0);
+  R.groupStart.assign(NG + 1, 0);
+  for (i32 G = 0; G <= NG; ++G) R.groupStart[G] = static_cast<i32>(H.tileStart[std::min<i32>(H.P, G * group)]);
+  for (i32 G = 0; G < NG; ++G) R.maxGroupRows = std::max<i64>(R.maxGroupRows, R.groupStart[G + 1] - R.groupStart[G]);
+  i64 nVal = 0, nInv = 0;
+  for (i32 T = 0; T < NG; ++T) {
+    R.tileOffset[T + 1] = R.tileOffset[T] + static_cast<i64>(tr[T].bytes.size());
+    R.tileLevel[T + 1] = R.tileLevel[T] + static_cast<i32>(tr[T].size.size());
+    R.maxTileLevels = std::max<i32>(R.maxTileLevels, static_cast<i32>(tr[T].size.size()));
+    nVal += static_cast<i64>(tr[T].vals.size());
+    nInv += static_cast<i64>(tr[T].invs.size());
+  }
+  const i64 total = R.tileOffset[NG];
+  if (total / vs >= (i64(1) << 31)) fail(GR_EUNSUPPORTED, "ILU level ring stream exceeds 2^31 elements");
+  R.bytes.resize(total);
+  R.meta.resize(2 * static_cast<size_t>(R.tileLevel[NG]));
+  R.valPos.resize(nVal);
+  R.valSrc.resize(nVal);
+  R.invPos.resize(nInv);
+  R.invSrc.resize(nInv);
+  std::vector<i64> vOff(NG + 1, 0), iOff(NG + 1, 0);
+  for (i32 T = 0; T < NG; ++T) {
+    vOff[T + 1] = vOff[T] + static_cast<i64>(tr[T].vals.size());
+    iOff[T + 1] = iOff[T] + static_cast<i64>(tr[T].invs.size());
+  }
+  parallelFor(NG, [&](i64 T) {
+    const i64 off = R.tileOffset[T];
+    std::memcpy(R.bytes.data() + off, tr[T].bytes.data(), tr[T].bytes.size());
+    std::copy(tr[T].meta.begin(), tr[T].meta.end(), R.meta.begin() + 2 * static_cast<size_t>(R.tileLevel[T]));
+    for (size_t i = 0; i < tr[T].vals.size(); ++i) {
+      R.valPos[vOff[T] + i] = static_cast<i32>((off + tr[T].vals[i].first) / vs);
+      R.valSrc[vOff[T] + i] = tr[T].vals[i].second;
+    }
+    for (size_t i = 0; i < tr[T].invs.size(); ++i) {
+      R.invPos[iOff[T] + i] = static_cast<i32>((off + tr[T].invs[i].first) / vs);
+      R.invSrc[iOff[T] + i] = tr[T].invs[i].second;
+    }
+  });
+  return R;
+}
+
+void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt) {
+  const i64 vs = static_cast<i64>(dtypeSize(vt));
+  const i64 entSize = vs == 4 ? 8 : 16;
+  auto bad = [](i32 G, i64 l, const std::string& what) {
+    fail(GR_EINVAL, "level ring check: block " + std::to_string(G) + " level " + std::to_string(l) + ": " + what);
+  };
+  const i32 group = R.group;
+  const i32 NG = group > 0 ? (H.P + group - 1) / group : -1;
+  if (NG < 1 || static_cast<i32>(R.tileOffset.size()) != NG + 1 || static_cast<i32>(R.tileLevel.size()) != NG + 1 ||
+      static_cast<i32>(R.groupStart.size()) != NG + 1)
+    fail(GR_EINVAL, "level ring check: table sizes");
+  for (i32 G = 0; G < NG; ++G) {
+    const i32 T0 = G * group, T1 = std::min<i32>(H.P, T0 + group);
+    const i64 gBase = H.tileStart[T0], gRows = H.tileStart[T1] - gBase;
+    if (R.groupStart[G] != gBase || R.groupStart[G + 1] != H.tileStart[T1]) bad(G, -1, "block rows");
+    std::vector<i32> tileOf(gRows);
+    i32 nLower = 0, nUpper = 0;
+    for (i32 T = T0; T < T1; ++T) {
+      for (i64 p = H.tileStart[T]; p < H.tileStart[T + 1]; ++p) tileOf[p - gBase] = T;
+      nLower = std::max(nLower, H.nLowerLevels[T]);
+      nUpper = std::max(nUpper, H.nUpperLevels[T]);
+    }
+    const i64 L = R.tileLevel[G + 1] - R.tileLevel[G];
+    if (L != nLower + nUpper) bad(G, -1, "level count");
+    std::vector<char> doneL(gRows, 0), doneU(gRows, 0);
+    std::vector<i64> ringOff(L), size(L);
+    i64 src = R.tileOffset[G], prevIa = -1;
+    for (i64 l = 0; l < L; ++l) {
+      const int4 a = R.meta[2 * (R.tileLevel[G] + l)], b = R.meta[2 * (R.tileLevel[G] + l) + 1];
+      const i64 k = a.x, E = a.y, S = a.z, off = a.w, ia = b.z;
+      const bool upper = b.w != 0;
+      if (upper != (l >= nLower)) bad(G, l, "sweep flag");
+      const bool hasInv = upper || dilu;
+      const i64 rowsB = pad16(4 * k), invB = hasInv ? pad16(vs * k) : 0;
+      if (k < 1 || E < 0 || b.x != rowsB || b.y != rowsB + invB || S != rowsB + invB + pad16(entSize * E * k))
+        bad(G, l, "block layout");
+      if (off < 0 || off % 16 != 0 || off + S > R.ringBytes) bad(G, l, "ring offset");
+      if (ia < -1 || ia < prevIa || ia < l - kRingBarriers || (l >= 1 && ia > l - 2) || (l == 0 && ia != -1))
+        bad(G, l, "copy order");
+      ringOff[l] = off;
+      size[l] = S;
+      // Levels issued before this one and not yet consumed when it is copied.
+      for (i64 j = ia + 1; j < l; ++j)
+        if (overlaps(ringOff[j], size[j], off, S)) bad(G, l, "copy overwrites level " + std::to_string(j));
+      if (src + S > static_cast<i64>(R.bytes.size())) bad(G, l, "source range");
+      const uint8_t* blk = R.bytes.data() + src;
+      std::vector<char>& done = upper ? doneU : doneL;
+      std::vector<i64> rows(k);
+      for (i64 q = 0; q < k; ++q) {
+        i32 il;
+        std::memcpy(&il, blk + 4 * q, 4);
+        if (il < 0 || il >= gRows || done[il]) bad(G, l, "row id");
+        rows[q] = il;
+        for (i64 e = 0; e < E; ++e) {
+          i32 c;
+          std::memcpy(&c, blk + b.y + entSize * (e * k + q), 4);
+          if (c < 0 || c > gRows) bad(G, l, "column index");
+          if (c < gRows && (tileOf[c] != tileOf[il] || !done[c] || (upper ? c <= il : c >= il)))
+            bad(G, l, "dependency order");
+        }
+      }
+      for (i64 il : rows) done[il] = 1;
+      src += S;
+      prevIa = ia;
+    }
+    if (src != R.tileOffset[G + 1]) bad(G, L, "stream length");
+    for (i64 i = 0; i < gRows; ++i)
+      if (!doneL[i] || !doneU[i]) bad(G, L, "row not covered");
+  }
+}
+
+LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group) {
+  auto key = std::make_tuple(dilu, ringBytes, group);
+  auto it = levelRings.find(key);
+  if (it != levelRings.end()) return *it->second;
+  HostRing H = buildLevelRing(*host, dilu, vt, ringBytes, group);
+  auto R = std::make_unique<LevelRing>();
+  R->dilu = dilu;
+  R->bytes = static_cast<i64>(H.bytes.size());
+  R->ringBytes = H.ringBytes;
+  R->maxTileLevels = H.maxTileLevels;
+  R->nVal = static_cast<i64>(H.valPos.size());
+  R->nInv = static_cast<i64>(H.invPos.size());
+  R->tileOffset.upload(H.tileOffset);
+  R->templ.upload(H.bytes);
+  R->meta.upload(H.meta);
+  R->tileLevel.upload(H.tileLevel);
+  R->groupStart.upload(H.groupStart);
+  R->group = H.group;
+  R->numGroups = static_cast<i32>(H.groupStart.size()) - 1;
+  R->maxGroupRows = H.maxGroupRows;
+  R->valPos.upload(H.valPos);
+  R->valSrc.upload(H.valSrc);
+  R->invPos.upload(H.invPos);
+  R->invSrc.upload(H.invSrc);
+  LevelRing& ref = *R;
+  levelRings[key] = std::move(R);
+  return ref;
+}
+
+}  // namespace gr

@@ -80,9 +80,23 @@ class IluNode : public Node {
     // the level-schedule kernel ("levels", and auto when a tile does not fit
     // shared memory).
     kernel_ = 2;
-    if (c.iluKernel != 2) {
+    const size_t smemMax = static_cast<size_t>(maxDynamicSmem(A));
+    if (c.iluKernel == 0 || c.iluKernel == 4) {
+      LevelRing* R = nullptr;
+      try {
+        R = &A.levelRing(dilu_, c.ringBytes, c.tilesPerBlock > 0 ? c.tilesPerBlock : 1);
+      } catch (const Error&) {
+        if (c.iluKernel == 4) throw;  // the requested ring cannot hold the levels
+      }
+      if (R && iluRingSmem(A, *R, DType::F64) <= smemMax) {
+        kernel_ = 4;
+        ring_ = R;
+      } else if (c.iluKernel == 4) {
+        fail(GR_EUNSUPPORTED, "the ring ILU kernel does not fit this matrix's tiles in shared memory");
+      }
+    }
+    if (kernel_ == 2 && c.iluKernel != 2 && c.iluKernel != 4) {
       SweepStream& S = A.iluSweepStream(dilu_);
-      const size_t smemMax = static_cast<size_t>(maxDynamicSmem(A));
       const bool warpFits = iluWarpSmem(A, S, DType::F64) <= smemMax;
       const size_t tmaNeed = iluStreamSmem(A, S, DType::F64, c.ringLog2);
       const bool tmaFits = tmaNeed > 0 && tmaNeed <= smemMax;
@@ -91,7 +105,10 @@ class IluNode : public Node {
       else if (c.iluKernel == 1 && tmaFits) kernel_ = 1;
       else fail(GR_EUNSUPPORTED, "the requested ILU kernel does not fit this matrix's tiles in shared memory");
     }
-    if (kernel_ != 2) {
+    if (kernel_ == 4) {
+      stream_.alloc(std::max<i64>(16, ring_->bytes));
+      launchRingPack(A, *ring_, stream_.get(), vals, inv_.get(), s());
+    } else if (kernel_ != 2) {
       SweepStream& S = A.iluSweepStream(dilu_);
       sweep_ = &S;
       rowsPerLane_ = iluWarpRowsPerLane(A, S);
@@ -117,11 +134,13 @@ class IluNode : public Node {
     return st;
   }
   void apply(const PrologueArgs& pro, void* y, DType W) {
-    if (kernel_ == 3)
+    if (kernel_ == 4)
+      launchIluRing(A_, *ring_, stream_.get(), dilu_, pro, y, W, cfg_.l2Ahead, cfg_.unrollRows != 0, s());
+    else if (kernel_ == 3)
       launchIluWarp(A_, *sweep_, stream_.get(), dilu_, pro, y, W, rowsPerLane_, s());
     else if (kernel_ == 1)
       launchIluStream(A_, *sweep_, stream_.get(), dilu_, pro, y, W,
-                      StreamTuning{cfg_.ringLog2, cfg_.prefetchChunks, cfg_.unrollRows}, s());
+                      StreamTuning{cfg_.ringLog2, cfg_.prefetchChunks, cfg_.unrollRows == 1}, s());
     else
       launchIluApply(A_, Lval_.get(), Uval_.get(), inv_.get(), dilu_, pro, y, W, s());
   }
@@ -129,10 +148,11 @@ class IluNode : public Node {
 
  private:
   bool dilu_;
-  int kernel_ = 2;  // 1 tma ring, 2 level schedule, 3 warp per tile
+  int kernel_ = 2;  // 1 tma ring, 2 level schedule, 3 warp per tile, 4 host-scheduled ring
   int rowsPerLane_ = 2;
   DBuf inv_, Lval_, Uval_, stream_;
   const SweepStream* sweep_ = nullptr;
+  const LevelRing* ring_ = nullptr;
 };
 
 // ---------------------------------------------------------------------------

@@ -54,7 +54,7 @@ NAMES = ["poisson16", "poisson_odd_bfs", "poisson_1tile", "random", "many_tiles"
 
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("dilu", [False, True])
-@pytest.mark.parametrize("kernel", ["warp", "tma", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "warp", "tma", "levels"])
 def test_ilu_bit_exact(oracle, name, dilu, kernel):
     h, om = case(name, oracle)
     A = h.copyToTile()
@@ -66,13 +66,50 @@ def test_ilu_bit_exact(oracle, name, dilu, kernel):
 
 
 @pytest.mark.parametrize("name", ["poisson16", "random"])
-@pytest.mark.parametrize("kernel", ["warp", "tma", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "warp", "tma", "levels"])
 def test_ilu_bit_exact_float64(oracle, name, kernel):
     h, om = case(name, oracle, gb.FLOAT64)
     A = h.copyToTile()
     b = np.random.default_rng(4).standard_normal(h.numRows)
     x = A.createUninitializedVector(gb.FLOAT64)
     gb.Solver(A, {"type": "ILU", "kernel": kernel}).solve(x, dev(b))
+    off, inv = om.ilu_factorize(False)
+    np.testing.assert_array_equal(host(x), om.ilu_solve(off, inv, b, False))
+
+
+@pytest.mark.parametrize("name", ["poisson16", "many_tiles", "random", "poisson_odd_bfs"])
+@pytest.mark.parametrize("group", [2, 3, 8])
+@pytest.mark.parametrize("dilu", [False, True])
+def test_ilu_ring_tile_groups_bit_exact(oracle, name, group, dilu):
+    """Several tiles per thread block, run level by level in lockstep: same bits."""
+    h, om = case(name, oracle)
+    A = h.copyToTile()
+    b = np.random.default_rng(7).uniform(-1, 1, h.numRows).astype(np.float32)
+    x = A.createUninitializedVector(gb.FLOAT32)
+    gb.Solver(A, {"type": "ILU", "kernel": "ring", "tilesPerBlock": group, "diagonalBased": dilu}).solve(x, dev(b))
+    off, inv = om.ilu_factorize(dilu)
+    np.testing.assert_array_equal(host(x), om.ilu_solve(off, inv, b, dilu))
+
+
+@pytest.mark.parametrize("name", ["poisson16", "many_tiles", "random"])
+@pytest.mark.parametrize("frac", [0.0, 0.35, 0.6])
+def test_ilu_ring_small_rings_bit_exact(oracle, name, frac):
+    """Rings from a few level blocks up: wrap-around placement and barrier
+    reuse in the host-scheduled ring kernel give the same bits."""
+    import ctypes as C
+    h, om = case(name, oracle)
+    used = C.c_int64()
+    gb._lib.check(gb._lib.lib().gr_host_matrix_check_ilu_ring(h._h, 0, gb.FLOAT32, 0, 1, C.byref(used), None, None))
+    rb = 0 if frac == 0.0 else max(16, int(used.value * frac) // 16 * 16)
+    A = h.copyToTile()
+    b = np.random.default_rng(6).uniform(-1, 1, h.numRows).astype(np.float32)
+    x = A.createUninitializedVector(gb.FLOAT32)
+    try:
+        s = gb.Solver(A, {"type": "ILU", "kernel": "ring", "ringBytes": rb})
+    except gb.GrapheneError as e:
+        assert "too small" in str(e)
+        return
+    s.solve(x, dev(b))
     off, inv = om.ilu_factorize(False)
     np.testing.assert_array_equal(host(x), om.ilu_solve(off, inv, b, False))
 
@@ -112,6 +149,7 @@ PCFG = {
     "ilu": {"type": "ILU"},
     "ilu_levels": {"type": "ILU", "kernel": "levels"},
     "ilu_tma": {"type": "ILU", "kernel": "tma"},
+    "ilu_ring": {"type": "ILU", "kernel": "ring"},
     "dilu": {"type": "ILU", "diagonalBased": True},
     "gs2": {"type": "GaussSeidel", "numFixedIterations": 2},
     "none": None,

@@ -49,3 +49,62 @@ def test_stream_replay_bench_problem():
     h = gb.generateMatrix(gb.GEN_VAR_POISSON, 192, 192, 192, (1.5,), 2, 1024)
     lg, nbytes = check(h, False)
     assert lg <= 16
+
+
+# ---- host-scheduled level ring (kernels_ring.cu) ----------------------------------------
+
+def check_ring(h, dilu, vt=gb.FLOAT32, ring_bytes=0, group=1):
+    used, nbytes, lv = C.c_int64(), C.c_int64(), C.c_int32()
+    gb._lib.check(gb._lib.lib().gr_host_matrix_check_ilu_ring(h._h, int(dilu), vt, ring_bytes, group,
+                                                               C.byref(used), C.byref(nbytes), C.byref(lv)))
+    return used.value, nbytes.value, lv.value
+
+
+@pytest.mark.parametrize("dims,tiles,part", [
+    ((16, 16, 16), 8, gb.PART_RCB),
+    ((13, 11, 7), 6, gb.PART_BFS),
+    ((12, 10, 8), 1, gb.PART_AUTO),
+    ((20, 20, 20), 200, gb.PART_RCB),
+    ((5, 4, 3), 60, gb.PART_RCB),
+    ((33, 17, 9), 5, gb.PART_CONTIGUOUS),
+])
+@pytest.mark.parametrize("dilu", [False, True])
+@pytest.mark.parametrize("vt", [gb.FLOAT32, gb.FLOAT64])
+@pytest.mark.parametrize("group", [1, 3])
+def test_ring_replay(dims, tiles, part, dilu, vt, group):
+    h = gb.generate3DPoissonMatrix(vt, *dims, tiles, part)
+    used, nbytes, lv = check_ring(h, dilu, vt, 0, group)
+    assert used >= 16384 and used % 16 == 0 and nbytes % 16 == 0 and lv >= 2
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_ring_replay_random_and_ldu(seed):
+    n, r, c, v = random_coo(400, 0.03, seed)
+    check_ring(gb.HostMatrix.from_coo(n, r, c, v, 7, partitioner=gb.PART_BFS), seed == 1, group=seed + 1)
+    check_ring(gb.generateLduMesh(9, 8, 7, numTiles=5, partitioner=gb.PART_RCB), seed == 2)
+
+
+def test_ring_small_rings_wrap_and_reuse_barriers():
+    """Rings of a few level blocks force wrap-around placement and more than
+    16 levels in flight per barrier cycle; the replay must still pass, and a
+    ring smaller than two consecutive levels must be rejected."""
+    h = gb.generate3DPoissonMatrix(gb.FLOAT32, 24, 24, 24, 4, gb.PART_RCB)
+    used, _, lv = check_ring(h, False)
+    assert lv > 2 * 16
+    passed = 0
+    for rb in range(used // 4, 2 * used + 1, 1024):
+        try:
+            check_ring(h, False, gb.FLOAT32, rb)
+            passed += 1
+        except gb.GrapheneError as e:
+            assert "too small" in str(e) and rb < used
+    assert passed > (2 * used - used) // 1024
+    with pytest.raises(gb.GrapheneError):
+        check_ring(h, False, gb.FLOAT32, 256)
+
+
+def test_ring_replay_192_workload():
+    h = gb.generateMatrix(gb.GEN_VAR_POISSON, 192, 192, 192, (1.5,), 2, 2048)
+    for group in (1, 2, 4):
+        used, nbytes, lv = check_ring(h, False, gb.FLOAT32, 0, group)
+        assert used >= 16384 and lv < 128
