@@ -395,6 +395,13 @@ class Solver:
         check(_lib.lib().gr_solve_host(self._s, _ptr(x), t, _ptr(b), t, C.byref(st)))
         return SolverStats._from(st)
 
+    def timeRepeated(self, x, b, reps: int = 20) -> float:
+        """Mean device ms per run of reps back-to-back runs (ILU, fixed GS)."""
+        ms = C.c_float()
+        check(_lib.lib().gr_solver_time_repeated(self._s, _ptr(x), _dtype_of(x), _ptr(b), _dtype_of(b), reps,
+                                                 C.byref(ms)))
+        return ms.value
+
     def phi(self, t: int = FLOAT64):
         """Extended-precision solution of the last IterativeRefinement solve."""
         torch = _torch()
@@ -468,6 +475,13 @@ class Matrix:
         check(_lib.lib().gr_residual(self._m, _ptr(x), xt, _ptr(b), _dtype_of(b), _ptr(r),
                                      destType, intermediateType))
         return r
+
+    def tuneSpmv(self, t: int = FLOAT32, reps: int = 5) -> dict:
+        """Runs the SpMV autotuner (gr_matrix_tune_spmv) for vectors of type t."""
+        v = [C.c_int32() for _ in range(3)]
+        ms = C.c_float()
+        check(_lib.lib().gr_matrix_tune_spmv(self._m, t, reps, *[C.byref(a) for a in v], C.byref(ms)))
+        return {"block": v[0].value, "chunks_per_warp": v[1].value, "batch": v[2].value, "ms": ms.value}
 
     def vectorNorm(self, norm: int, x) -> float:
         out = C.c_double()

@@ -394,6 +394,18 @@ int gr_residual(gr_matrix* A, const void* x, gr_dtype x_t, const void* b, gr_dty
   });
 }
 
+int gr_matrix_tune_spmv(gr_matrix* A, gr_dtype t, int32_t reps, int32_t* block, int32_t* chunks_per_warp,
+                        int32_t* batch, float* ms) {
+  return guarded([&] {
+    need(A, "matrix");
+    const gr::SpmvTuning g = gr::tuneSpmv(*A->d, gr::toDType(t), reps);
+    if (block) *block = g.block;
+    if (chunks_per_warp) *chunks_per_warp = g.chunksPerWarp;
+    if (batch) *batch = g.batch;
+    if (ms) *ms = g.ms;
+  });
+}
+
 int gr_vector_norm(gr_matrix* A, gr_norm norm, const void* x, gr_dtype t, double* out) {
   return guarded([&] {
     need(A, "matrix");
@@ -466,6 +478,17 @@ int gr_solve_host(gr_solver* s, void* x, gr_dtype x_t, const void* b, gr_dtype b
     need(b, "b");
     gr_stats st = s->s->solveHost(x, gr::toDType(x_t), b, gr::toDType(b_t));
     if (stats) *stats = st;
+  });
+}
+
+int gr_solver_time_repeated(gr_solver* s, void* x, gr_dtype x_t, const void* b, gr_dtype b_t, int32_t reps,
+                            float* ms_per_run) {
+  return guarded([&] {
+    need(s, "solver");
+    need(x, "x");
+    need(b, "b");
+    need(ms_per_run, "ms_per_run");
+    *ms_per_run = s->s->timeRepeated(x, gr::toDType(x_t), b, gr::toDType(b_t), reps);
   });
 }
 

@@ -193,6 +193,15 @@ enum class SweepEntries {
   All           // every off-diagonal entry in tile-local order (Gauss-Seidel)
 };
 
+// Launch geometry of the SpMV kernel: threads per block, SELL chunks per
+// warp (grid size; 0 = the untuned grid), and entries whose loads are issued
+// together (batch).
+struct SpmvTuning {
+  int block = 256, chunksPerWarp = 0, batch = 8;
+  bool tuned = false;
+  float ms = 0;  // mean time of the chosen geometry when tuned
+};
+
 struct DeviceMatrix {
   std::shared_ptr<HostMatrix> host;
   int device = 0;
@@ -240,6 +249,7 @@ struct DeviceMatrix {
   LevelSchedule& schedule(SweepEntries kind);
   // Rounded-up kernel grid for a row loop of n rows.
   int spmvBlocks() const;
+  SpmvTuning spmvTuning[2];  // [float32 vectors, float64 vectors]
 };
 
 // Raises the dynamic shared-memory limit of kernel `fn` on the current device
@@ -252,6 +262,11 @@ void ensureDynamicSmem(const void* fn, size_t bytes);
 
 // y = A x (reference CRSMatrix::spmv). xt == yt.
 void launchSpmv(DeviceMatrix& A, const void* x, void* y, DType t, cudaStream_t s);
+
+// SpMV autotuner: times every candidate launch geometry `reps` times on the
+// matrix's stream and keeps the fastest for vectors of type t. The results
+// of gr_spmv do not depend on the geometry.
+SpmvTuning tuneSpmv(DeviceMatrix& A, DType t, int reps);
 
 // r = b - A x in inter (reference CRSMatrix::residual); optionally
 // accumulates a norm of r into normOut (device double) when normKind >= 0.

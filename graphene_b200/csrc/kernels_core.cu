@@ -220,9 +220,11 @@ void DeviceMatrix::ensureLocalCrs() {
 // ---------------------------------------------------------------------------
 namespace dev {
 
-// y = A x.
-template <class MV, class VT>
-__global__ void __launch_bounds__(256) spmvKernel(SellView<MV> A, const VT* __restrict__ x,
+// y = A x. Every launch geometry (block size, grid, batch depth B) computes
+// each row with the same sequential sum, so the autotuner's choice never
+// changes y.
+template <class MV, class VT, int B>
+__global__ void __launch_bounds__(512) spmvKernel(SellView<MV> A, const VT* __restrict__ x,
                                                    VT* __restrict__ y) {
   const int lane = threadIdx.x & 31;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
@@ -230,7 +232,7 @@ __global__ void __launch_bounds__(256) spmvKernel(SellView<MV> A, const VT* __re
     const int row = c * 32 + lane;
     const int s0 = __ldg(A.base + c);
     const int K = (__ldg(A.base + c + 1) - s0) >> 5;
-    if (row < A.n) y[row] = sellRowSum<VT>(A, x, row, s0, K, lane);
+    if (row < A.n) y[row] = sellRowSum<VT, MV, VT, B>(A, x, row, s0, K, lane);
   }
 }
 
@@ -344,22 +346,89 @@ namespace {
 
 }  // namespace
 
+namespace {
+template <class MV, class VT>
+void spmvT(DeviceMatrix& A, const void* x, void* y, const SpmvTuning& g, cudaStream_t s) {
+  // chunksPerWarp 0: the untuned geometry (A.spmvBlocks(), at most 8 blocks
+  // per SM, warps striding over the chunks).
+  const int warps = g.block / 32;
+  const int blocks = g.chunksPerWarp == 0
+                         ? A.spmvBlocks()
+                         : std::max(1, std::min((A.sell.nChunks + warps * g.chunksPerWarp - 1) /
+                                                    (warps * g.chunksPerWarp),
+                                                A.numSMs * 64));
+  const auto* xv = static_cast<const VT*>(x);
+  auto* yv = static_cast<VT*>(y);
+  switch (g.batch) {
+    case 4: dev::spmvKernel<MV, VT, 4><<<blocks, g.block, 0, s>>>(sellView<MV>(A), xv, yv); break;
+    case 16: dev::spmvKernel<MV, VT, 16><<<blocks, g.block, 0, s>>>(sellView<MV>(A), xv, yv); break;
+    default: dev::spmvKernel<MV, VT, 8><<<blocks, g.block, 0, s>>>(sellView<MV>(A), xv, yv); break;
+  }
+}
+
+SpmvTuning& tuningFor(DeviceMatrix& A, DType t) { return A.spmvTuning[t == DType::F64 ? 1 : 0]; }
+}  // namespace
+
 void launchSpmv(DeviceMatrix& A, const void* x, void* y, DType t, cudaStream_t s) {
-  const int blocks = A.spmvBlocks();
+  const SpmvTuning& g = tuningFor(A, t);
   if (A.vt == DType::F32 && t == DType::F32) {
-    dev::spmvKernel<float, float><<<blocks, 256, 0, s>>>(sellView<float>(A), static_cast<const float*>(x),
-                                                         static_cast<float*>(y));
+    spmvT<float, float>(A, x, y, g, s);
   } else if (A.vt == DType::F32 && t == DType::F64) {
-    dev::spmvKernel<float, double><<<blocks, 256, 0, s>>>(sellView<float>(A), static_cast<const double*>(x),
-                                                          static_cast<double*>(y));
+    spmvT<float, double>(A, x, y, g, s);
   } else if (A.vt == DType::F64 && t == DType::F64) {
-    dev::spmvKernel<double, double><<<blocks, 256, 0, s>>>(sellView<double>(A), static_cast<const double*>(x),
-                                                           static_cast<double*>(y));
+    spmvT<double, double>(A, x, y, g, s);
   } else {
     fail(GR_EUNSUPPORTED, std::string("spmv with ") + dtypeName(A.vt) + " coefficients and " +
                               dtypeName(t) + " vectors");
   }
   checkLaunch("spmv");
+}
+
+SpmvTuning tuneSpmv(DeviceMatrix& A, DType t, int reps) {
+  if (t != DType::F32 && t != DType::F64) fail(GR_EINVAL, "spmv tuning needs float32 or float64 vectors");
+  if (A.vt == DType::F64 && t == DType::F32) fail(GR_EUNSUPPORTED, "spmv with float64 coefficients and float32 vectors");
+  if (reps < 1 || reps > 1000) fail(GR_EINVAL, "reps must be 1..1000");
+  const size_t bytes = static_cast<size_t>(A.n) * dtypeSize(t);
+  DBuf x(bytes), y(bytes);
+  GR_CUDA(cudaMemsetAsync(x.get(), 0, bytes, A.stream));
+  cudaEvent_t e0, e1;
+  GR_CUDA(cudaEventCreate(&e0));
+  GR_CUDA(cudaEventCreate(&e1));
+  SpmvTuning& slot = tuningFor(A, t);
+  const SpmvTuning keep = slot;
+  SpmvTuning best = keep;
+  float bestMs = 1e30f;
+  try {
+    for (int block : {128, 256, 512})
+      for (int cpw : {0, 1, 2, 4, 8})
+        for (int batch : {4, 8, 16}) {
+          if (cpw == 0 && block != 256) continue;  // the untuned geometry
+          slot = SpmvTuning{block, cpw, batch, false, 0.0f};
+          launchSpmv(A, x.get(), y.get(), t, A.stream);  // warm-up
+          GR_CUDA(cudaEventRecord(e0, A.stream));
+          for (int r = 0; r < reps; ++r) launchSpmv(A, x.get(), y.get(), t, A.stream);
+          GR_CUDA(cudaEventRecord(e1, A.stream));
+          GR_CUDA(cudaEventSynchronize(e1));
+          float ms = 0;
+          GR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          if (ms < bestMs) {
+            bestMs = ms;
+            best = slot;
+          }
+        }
+  } catch (...) {
+    slot = keep;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  best.tuned = true;
+  best.ms = bestMs / static_cast<float>(reps);
+  slot = best;
+  GR_CUDA(cudaStreamSynchronize(A.stream));
+  return best;
 }
 
 void launchResidual(DeviceMatrix& A, const void* x, DType xt, const void* b, DType bt, void* r,

@@ -11,13 +11,13 @@
 // the level after which its copy is issued, so the kernel does no ring
 // arithmetic: a level's rows, inverse diagonal and (column, value) entries
 // sit at fixed offsets. Per level: four compute warps compute the level's
-// rows from shared memory while the producer warp issues the copies that the
-// previous level released and waits until the next level has landed; one
-// barrier ends the level.
+// rows from shared memory, one producer warp issues the copies that the
+// previous level released and another waits until the next level has
+// landed; one barrier ends the level.
 //
 // Every wait is bounded; when one runs out the block records GR_ETIMEOUT in
-// the matrix's error word, stops at the next barrier, and thread 0 waits
-// (bounded) for the copies still in flight before the block exits.
+// the matrix's error word, stops at the next barrier, and the issuing lane
+// waits (bounded) for the copies still in flight before the block exits.
 #include <algorithm>
 
 #include "bulk.cuh"
@@ -29,9 +29,9 @@
 namespace gr {
 namespace dev {
 
-// Four compute warps and one producer warp per block.
+// Four compute warps, an issuing warp and a waiting warp per block.
 constexpr int kRingCompute = 128;
-constexpr int kRingThreads = kRingCompute + 32;
+constexpr int kRingThreads = kRingCompute + 64;
 constexpr int kPrefetchAhead = 0;  // default bytes kept prefetched into L2 beyond the issued copies
 
 // Entry of a level block: column and value (the value at byte 4 for float,
@@ -117,8 +117,9 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
   unsigned char* ring = smem + 256 + 32 * metaLevels;
   W* xs = reinterpret_cast<W*>(ring + ringBytes);
   const unsigned char* g = stream + tileOffset[T];
-  const bool producer = threadIdx.x >= kRingCompute;  // the producer warp
-  const bool lead = threadIdx.x == kRingCompute;      // its lane 0 issues copies and waits
+  const bool producer = threadIdx.x >= kRingCompute;     // the two producer warps
+  const bool lead = threadIdx.x == kRingCompute;         // issues the copies
+  const bool waiter = threadIdx.x == kRingCompute + 32;  // waits for the next level
 
   if (lead) {
     abortFlag = 0;
@@ -142,19 +143,23 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
     for (int i = threadIdx.x; i < nRows; i += blockDim.x) xs[i] = pro(base + i, beta, omega, alpha, first);
     if (lead) xs[nRows] = W(0);
   }
-  // Thread 0 issues copies in level order; `next` is the next level to copy,
-  // `src` its byte offset in the tile stream, `pf` the prefetch frontier.
-  int next = 0;
+  // The issuing lane copies levels in order: `next` is the next level to
+  // copy (its table entries held in na / nia), `src` its byte offset in the
+  // block's stream, `pf` the L2 prefetch frontier.
+  int next = 0, nia = 0;
+  int4 na = make_int4(0, 0, 0, 0);
   uint32_t src = 0, pf = 0;
   const uint32_t tileBytes = static_cast<uint32_t>(tileOffset[T + 1] - tileOffset[T]);
   auto issueUpTo = [&](int consumed) {
-    while (next < L && mt[2 * next + 1].z <= consumed) {
-      const int4 a = mt[2 * next];
+    while (next < L && nia <= consumed) {
       const uint32_t bar = smemAddr(bars + (next % kRingBarriers));
-      mbarExpectTx(bar, static_cast<uint32_t>(a.z));
-      bulkLoad(smemAddr(ring + a.w), g + src, static_cast<uint32_t>(a.z), bar);
-      src += static_cast<uint32_t>(a.z);
-      ++next;
+      mbarExpectTx(bar, static_cast<uint32_t>(na.z));
+      bulkLoad(smemAddr(ring + na.w), g + src, static_cast<uint32_t>(na.z), bar);
+      src += static_cast<uint32_t>(na.z);
+      if (++next < L) {
+        na = mt[2 * next];
+        nia = mt[2 * next + 1].z;
+      }
     }
     if (pf < src) pf = src;
     const uint32_t until = min(tileBytes, src + l2Ahead);
@@ -169,6 +174,8 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
       abortFlag = 1;
     } else {
       tableLanded = true;
+      na = mt[0];
+      nia = mt[1].z;
       issueUpTo(-1);
       if (L > 0 && !waitBar(smemAddr(bars), 0)) abortFlag = 1;
     }
@@ -179,15 +186,15 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
     for (int l = 0; l < L; ++l) {
       if (producer) {
         // Copies released by level l - 1 (finished by every thread before
-        // the previous barrier), then wait until level l + 1 has landed.
-        if (lead) {
-          if (l > 0 && next < L) {
-            fenceProxyAsync();
-            issueUpTo(l - 1);
-          }
-          if (l + 1 < L && !waitBar(smemAddr(bars + ((l + 1) % kRingBarriers)), ((l + 1) / kRingBarriers) & 1))
-            abortFlag = 1;
+        // the previous barrier); meanwhile the waiting warp waits until level
+        // l + 1 has landed.
+        if (lead && l > 0 && next < L) {
+          fenceProxyAsync();
+          issueUpTo(l - 1);
         }
+        if (waiter && l + 1 < L &&
+            !waitBar(smemAddr(bars + ((l + 1) % kRingBarriers)), ((l + 1) / kRingBarriers) & 1))
+          abortFlag = 1;
       } else {
         const int4 a = mt[2 * l], b = mt[2 * l + 1];
         const int k = a.x, E = a.y;

@@ -26,14 +26,13 @@ __device__ __forceinline__ Acc loadX(const XT* __restrict__ x, int i) {
 // Row sum of one row of a SELL-32 chunk, in Acc: diag * x[row] first, then
 // the off-diagonal products added in stored order (padding slots have
 // column -1 and are skipped, so the result is the sequential row sum).
-// The loads of up to 8 entries are issued before the dependent gathers of x
+// The loads of up to B entries are issued before the dependent gathers of x
 // so that a warp keeps many memory requests in flight; the matrix stream is
 // read with evict-first loads so that x stays resident in L2.
-template <class Acc, class MV, class XT>
+template <class Acc, class MV, class XT, int B = 8>
 __device__ __forceinline__ Acc sellRowSum(const SellView<MV>& A, const XT* __restrict__ x, int row,
                                           int s0, int K, int lane) {
   Acc acc = mul(cvt<Acc>(__ldg(A.diag + row)), loadX<Acc>(x, row));
-  constexpr int B = 8;
   for (int k = 0; k < K; k += B) {
     int c[B];
     MV a[B];

@@ -10,6 +10,7 @@
 // and Solver::createSolver's dispatch is makeNode (Solver.cpp:32-56).
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "config.hpp"
 #include "krylov.hpp"
@@ -246,6 +247,34 @@ class GsNode : public Node {
   DBuf Gval_, tmp_;
 };
 
+// Pinned host mirrors of the Krylov state, handed out from slabs that are
+// never returned: cudaFreeHost would wait for all work on the device (every
+// other solve included) and pinning memory per solver is slow.
+namespace {
+constexpr size_t kPinnedSlot = 256;
+constexpr size_t kPinnedSlab = 256;  // slots per cudaMallocHost
+static_assert(sizeof(KState) <= kPinnedSlot, "KState must fit a pinned slot");
+std::mutex g_pinnedMu;
+std::vector<void*> g_pinnedFree;
+
+void* acquirePinnedSlot() {
+  std::lock_guard<std::mutex> lock(g_pinnedMu);
+  if (g_pinnedFree.empty()) {
+    void* slab = nullptr;
+    GR_CUDA(cudaMallocHost(&slab, kPinnedSlot * kPinnedSlab));
+    for (size_t i = 0; i < kPinnedSlab; ++i) g_pinnedFree.push_back(static_cast<char*>(slab) + i * kPinnedSlot);
+  }
+  void* p = g_pinnedFree.back();
+  g_pinnedFree.pop_back();
+  return p;
+}
+
+void releasePinnedSlot(void* p) {
+  std::lock_guard<std::mutex> lock(g_pinnedMu);
+  g_pinnedFree.push_back(p);
+}
+}  // namespace
+
 // ---------------------------------------------------------------------------
 // Right-preconditioned BiCGStab. One iteration is five kernels when the
 // preconditioner is ILU (fused vector updates):
@@ -264,11 +293,11 @@ class PbicgstabNode : public Node {
       gs_ = dynamic_cast<GsNode*>(pre_.get());
     }
     st_.alloc(sizeof(KState));
-    GR_CUDA(cudaMallocHost(&host_, sizeof(KState)));
+    host_ = static_cast<KState*>(acquirePinnedSlot());
   }
   ~PbicgstabNode() override {
     if (exec_) cudaGraphExecDestroy(exec_);
-    if (host_) cudaFreeHost(host_);
+    if (host_) releasePinnedSlot(host_);
   }
 
   gr_stats solve(void* x, const void* b, DType Wx, const KState* gate) override {
@@ -569,6 +598,27 @@ class Tree : public SolverTree {
       st.converged = 0;
     }
     return st;
+  }
+  float timeRepeated(void* x, DType xt, const void* b, DType bt, int reps) override {
+    if (xt != bt) fail(GR_EINVAL, "x and b must have the same type");
+    if (xt == DType::DW) fail(GR_EUNSUPPORTED, "twofloat32 x / b");
+    if (reps < 1 || reps > 100000) fail(GR_EINVAL, "reps must be 1..100000");
+    if (cfg_->type != "ILU" && !(cfg_->type == "GaussSeidel" && cfg_->numFixedIterations > 0))
+      fail(GR_EUNSUPPORTED, "repeated timing is for ILU and fixed-sweep Gauss-Seidel solvers");
+    GR_CUDA(cudaEventRecord(e0_, A_.stream));
+    for (int i = 0; i < reps; ++i) root_->solve(x, b, xt, nullptr);
+    GR_CUDA(cudaEventRecord(e1_, A_.stream));
+    GR_CUDA(cudaEventSynchronize(e1_));
+    float ms = 0;
+    GR_CUDA(cudaEventElapsedTime(&ms, e0_, e1_));
+    int err = 0;
+    GR_CUDA(cudaMemcpyAsync(&err, A_.errFlag.get(), sizeof(int), cudaMemcpyDeviceToHost, A_.stream));
+    GR_CUDA(cudaStreamSynchronize(A_.stream));
+    if (err != 0) {
+      GR_CUDA(cudaMemsetAsync(A_.errFlag.get(), 0, sizeof(int), A_.stream));
+      fail(err, "a device-side wait ran out during the repeated runs");
+    }
+    return ms / static_cast<float>(reps);
   }
   gr_stats solveHost(void* x, DType xt, const void* b, DType bt) override {
     if (xt != bt) fail(GR_EINVAL, "x and b must have the same type");

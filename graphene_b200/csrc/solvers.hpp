@@ -18,6 +18,11 @@ class SolverTree {
   virtual gr_stats solve(void* x, DType xt, const void* b, DType bt) = 0;
   // Host vectors in natural order, copies included.
   virtual gr_stats solveHost(void* x, DType xt, const void* b, DType bt) = 0;
+  // Runs the solve `reps` times back to back on the matrix's stream with no
+  // host synchronisation in between and returns the mean device time per
+  // run (ms) between two events. For timing single-application solvers
+  // (ILU, a fixed number of Gauss-Seidel sweeps).
+  virtual float timeRepeated(void* x, DType xt, const void* b, DType bt, int reps) = 0;
   virtual void copyPhi(void* out, DType t) = 0;
   virtual std::string name() const = 0;
 };

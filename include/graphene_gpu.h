@@ -279,6 +279,16 @@ int gr_matrix_get_info(const gr_matrix* A, gr_matrix_info* out);
  * tile order; xt == yt (FLOAT32 or FLOAT64). */
 int gr_spmv(gr_matrix* A, const void* x, void* y, gr_dtype t);
 
+/* SpMV autotuner (no counterpart in the reference): times the candidate
+ * launch geometries of gr_spmv for vectors of type t (threads per block 128 /
+ * 256 / 512, SELL chunks per warp, entry loads batched 4 / 8 / 16; every
+ * candidate reps times on the matrix's stream) and keeps the fastest for
+ * later gr_spmv calls on this matrix. Every geometry computes each row in the
+ * same order, so results do not change. Writes the choice and its mean time
+ * (ms); chunks_per_warp 0 is the untuned grid. */
+int gr_matrix_tune_spmv(gr_matrix* A, gr_dtype t, int32_t reps, int32_t* block, int32_t* chunks_per_warp,
+                        int32_t* batch, float* ms);
+
 /* Replaces Matrix::residual(x, b, destType, intermediateType)
  * (matrix/Matrix.hpp:86-92, CRSMatrix.cpp:85-128): r = b - A x computed in
  * inter_t and rounded to r_t. x_t may be FLOAT32, FLOAT64 or TWOFLOAT32,
@@ -331,6 +341,13 @@ int gr_solve(gr_solver* s, void* x, gr_dtype x_t, const void* b, gr_dtype b_t, g
  * and x out (the end-to-end path). */
 int gr_solve_host(gr_solver* s, void* x, gr_dtype x_t, const void* b, gr_dtype b_t,
                   gr_stats* stats);
+
+/* Benchmarking: runs an ILU or fixed-sweep Gauss-Seidel solver reps times
+ * back to back on the matrix's stream (device pointers, tile order) without
+ * host synchronisation in between and writes the mean device time per run
+ * in ms. No counterpart in the reference. */
+int gr_solver_time_repeated(gr_solver* s, void* x, gr_dtype x_t, const void* b, gr_dtype b_t, int32_t reps,
+                            float* ms_per_run);
 
 /* After an IterativeRefinement solve: the extended-precision solution phi
  * (iterative-refinement/Solver.cpp:84,103), copied to a device buffer of

@@ -318,3 +318,17 @@ def test_launch_counter_counts_graph_replays():
     used = gb.launch_count() - c0
     assert st.converged
     assert used >= 5 * st.iterations
+
+
+def test_time_repeated_runs_the_same_application(oracle):
+    h, om = case("poisson16", oracle)
+    A = h.copyToTile()
+    b = np.random.default_rng(8).uniform(-1, 1, h.numRows).astype(np.float32)
+    s = gb.Solver(A, {"type": "ILU"})
+    x = A.createUninitializedVector(gb.FLOAT32)
+    ms = s.timeRepeated(x, dev(b), 5)
+    assert ms > 0
+    off, inv = om.ilu_factorize(False)
+    np.testing.assert_array_equal(host(x), om.ilu_solve(off, inv, b, False))
+    with pytest.raises(gb.GrapheneError):
+        gb.Solver(A, pbicgstab("ilu", 5)).timeRepeated(x, dev(b), 2)

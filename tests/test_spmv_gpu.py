@@ -164,3 +164,19 @@ def test_unsupported_combination_raises():
     with pytest.raises(gb.GrapheneError) as e:
         A * x
     assert e.value.code == 8
+
+
+@pytest.mark.parametrize("vt", [gb.FLOAT32, gb.FLOAT64])
+def test_spmv_autotuner_keeps_results(oracle, vt):
+    """The autotuner picks a launch geometry; every geometry computes the
+    same rows in the same order, so y is bit-identical before and after."""
+    h = gb.generateMatrix(gb.GEN_VAR_POISSON, 40, 36, 30, (1.0,), 3, 32)
+    if vt == gb.FLOAT64:
+        h = h.astype(gb.FLOAT64)
+    A = h.copyToTile()
+    t = np.float32 if vt == gb.FLOAT32 else np.float64
+    x = dev(np.random.default_rng(9).standard_normal(h.numRows).astype(t))
+    before = (A * x).cpu().numpy()
+    g = A.tuneSpmv(vt, reps=3)
+    assert g["block"] in (128, 256, 512) and g["batch"] in (4, 8, 16) and g["ms"] > 0
+    np.testing.assert_array_equal((A * x).cpu().numpy(), before)
