@@ -35,7 +35,7 @@ __all__ = [
     "PART_AUTO", "PART_CONTIGUOUS", "PART_RCB", "PART_BFS", "PART_EXPLICIT",
     "GrapheneError", "HostMatrix", "Matrix", "Configuration", "Solver", "SolverStats",
     "generate3DPoissonMatrix", "loadMatrixFromFile", "parseType", "launch_count",
-    "generateMatrix", "generateLduMesh", "randomVector", "Server",
+    "generateMatrix", "generateLduMesh", "randomVector", "Server", "Batch",
 ]
 
 _NP = {FLOAT32: np.float32, FLOAT64: np.float64}
@@ -540,6 +540,46 @@ class Server:
             except Exception:
                 pass
             self._s = None
+
+    def __del__(self):
+        self.close()
+
+
+class Batch:
+    """Many independent systems solved together (gr_batch_*): one PBiCGStab
+    whose kernel launches cover all systems, each with its own device-side
+    convergence test; each system's result equals its result alone."""
+
+    def __init__(self, systems, config):
+        self._hosts = list(systems)
+        js = config if isinstance(config, str) else _json.dumps(config)
+        arr = (C.c_void_p * len(self._hosts))(*[h._h for h in self._hosts])
+        h = C.c_void_p()
+        check(_lib.lib().gr_batch_create(arr, len(self._hosts), js.encode(), C.byref(h)))
+        self._b = h
+
+    def solveHost(self, bs, xs=None):
+        """bs: natural-order host vectors (all float32 or all float64); x0 = 0
+        unless xs is given. Returns (list of x, list of SolverStats)."""
+        bs = [np.ascontiguousarray(b) for b in bs]
+        dt = bs[0].dtype
+        t = FLOAT32 if dt == np.float32 else FLOAT64
+        xs = [np.zeros(h.numRows, dt) for h in self._hosts] if xs is None else \
+            [np.array(x, dtype=dt, copy=True) for x in xs]
+        xa = (C.c_void_p * len(xs))(*[x.ctypes.data for x in xs])
+        ba = (C.c_void_p * len(bs))(*[b.ctypes.data for b in bs])
+        st = (_lib.Stats * len(bs))()
+        check(_lib.lib().gr_batch_solve_host(self._b, xa, ba, t, st))
+        return xs, [SolverStats._from(s) for s in st]
+
+    def close(self):
+        b = getattr(self, "_b", None)
+        if b and _lib is not None:
+            try:
+                _lib.lib().gr_batch_destroy(b)
+            except Exception:
+                pass
+            self._b = None
 
     def __del__(self):
         self.close()

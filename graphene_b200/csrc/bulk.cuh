@@ -60,6 +60,11 @@ struct SPro {
   W* pOrS;
   const W* __restrict__ v;
   const KState* st;
+  // Batches: the state of block b is st[stIndex[b]] (null: st itself).
+  const int* stIndex = nullptr;
+  __device__ __forceinline__ const KState* state() const {
+    return st && stIndex ? st + stIndex[blockIdx.x] : st;
+  }
   __device__ __forceinline__ W operator()(int i, W beta, W omega, W alpha, bool first) const {
     if (kind == static_cast<int>(Prologue::Plain)) return b[i];
     if (kind == static_cast<int>(Prologue::PUpdate)) {

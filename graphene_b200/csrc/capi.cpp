@@ -9,6 +9,7 @@
 #include "config.hpp"
 #include "solvers.hpp"
 #include "server.hpp"
+#include "batch.hpp"
 
 struct gr_host_matrix {
   std::shared_ptr<gr::HostMatrix> m;
@@ -24,6 +25,10 @@ struct gr_solver {
 
 struct gr_server {
   std::unique_ptr<gr::Server> s;
+};
+
+struct gr_batch {
+  std::unique_ptr<gr::BatchSolve> b;
 };
 
 namespace {
@@ -580,5 +585,37 @@ int gr_server_counters(gr_server* s, int64_t* queued, int64_t* running, int64_t*
 }
 
 void gr_server_destroy(gr_server* s) { delete s; }
+
+
+int gr_batch_create(gr_host_matrix* const* systems, int32_t count, const char* json, gr_batch** out) {
+  return guarded([&] {
+    need(systems, "systems");
+    need(json, "json");
+    need(out, "out");
+    if (count < 1 || count > 65536) gr::fail(GR_EINVAL, "count must be 1..65536");
+    std::vector<std::shared_ptr<gr::HostMatrix>> parts;
+    for (int32_t i = 0; i < count; ++i) {
+      need(systems[i], "system");
+      parts.push_back(systems[i]->m);
+    }
+    auto b = std::make_unique<gr::BatchSolve>(std::move(parts), json);
+    *out = new gr_batch{std::move(b)};
+  });
+}
+
+int gr_batch_solve_host(gr_batch* b, void* const* x, const void* const* rhs, gr_dtype t, gr_stats* stats) {
+  return guarded([&] {
+    need(b, "batch");
+    need(x, "x");
+    need(rhs, "b");
+    const int S = b->b->systems();
+    std::vector<void*> xs(x, x + S);
+    std::vector<const void*> bs(rhs, rhs + S);
+    std::vector<gr_stats> st = b->b->solveHost(xs, bs, gr::toDType(t));
+    if (stats) std::copy(st.begin(), st.end(), stats);
+  });
+}
+
+void gr_batch_destroy(gr_batch* b) { delete b; }
 
 }  // extern "C"

@@ -202,6 +202,25 @@ struct SpmvTuning {
   float ms = 0;  // mean time of the chosen geometry when tuned
 };
 
+// A batch of independent systems stored as one block-diagonal device matrix:
+// system s owns tile-order rows [rowBegin[s], rowBegin[s] + rowReal[s]) (its
+// own tile layout, unchanged) followed by padding rows up to the next
+// multiple of 32, so that no SELL chunk mixes systems. Two block tables split
+// the launches of the Krylov kernels per system: `chunk` for the row-chunk
+// kernels (each system gets the block count a solve of it alone would use)
+// and `elem` for the elementwise ones. tileSys maps a tile to its system.
+struct BatchSeg {
+  int systems = 0;
+  std::vector<i64> rowBegin, rowReal;
+  std::vector<i32> tileBegin;                 // first tile of each system, and P
+  DBuf row0, rowEnd;                          // i32[systems]
+  DBuf chunkSys, chunkRank, chunkBlocks, chunkBlock0;
+  DBuf elemSys, elemRank, elemBlocks, elemBlock0;
+  int chunkGrid = 0, elemGrid = 0;
+  DBuf partials, counters;                    // per-block partials, per-system arrival counters
+  DBuf tileSys;                               // i32[P]
+};
+
 struct DeviceMatrix {
   std::shared_ptr<HostMatrix> host;
   int device = 0;
@@ -250,6 +269,11 @@ struct DeviceMatrix {
   // Rounded-up kernel grid for a row loop of n rows.
   int spmvBlocks() const;
   SpmvTuning spmvTuning[2];  // [float32 vectors, float64 vectors]
+  // Set for a batch of systems (makeBatch): the Krylov kernels then keep one
+  // state per system.
+  std::unique_ptr<BatchSeg> batch;
+  void makeBatch(const std::vector<i64>& rowBegin, const std::vector<i64>& rowReal,
+                 const std::vector<i32>& tileBegin);
 };
 
 // Raises the dynamic shared-memory limit of kernel `fn` on the current device
@@ -272,6 +296,9 @@ SpmvTuning tuneSpmv(DeviceMatrix& A, DType t, int reps);
 // accumulates a norm of r into normOut (device double) when normKind >= 0.
 void launchResidual(DeviceMatrix& A, const void* x, DType xt, const void* b, DType bt, void* r,
                     DType rt, DType inter, int normKind, double* normOut, cudaStream_t s);
+
+// Norm of the first n entries of x (same geometry as a matrix of n rows).
+void launchNormN(DeviceMatrix& A, const void* x, i64 n, DType t, int normKind, double* out, cudaStream_t s);
 
 // Norm of a tile-order vector, FP64 accumulation. normKind: gr_norm.
 void launchNorm(DeviceMatrix& A, const void* x, DType t, int normKind, double* out,

@@ -118,20 +118,22 @@ __device__ __forceinline__ void blockReduce(double (&v)[NV], const int (&ops)[NV
   }
 }
 
-// Completes a grid reduction. Every block calls this with its block-reduced
-// values (valid in thread 0). Returns true in exactly one block (the last to
-// arrive); in that block, thread 0's out[] holds the grid totals. The
+// Completes a grid reduction over `nb` blocks, this block being number
+// `rank` of them. Every block calls this with its block-reduced values (valid
+// in thread 0). Returns true in exactly one block (the last to arrive); in
+// that block, thread 0's out[] holds the totals, combined in rank order. The
 // counter is reset for the next launch.
 template <int NV>
-__device__ __forceinline__ bool gridReduce(double (&v)[NV], const int (&ops)[NV], double* partials,
-                                           unsigned* counter, double* smem, double (&out)[NV]) {
+__device__ __forceinline__ bool gridReduceRank(double (&v)[NV], const int (&ops)[NV], double* partials,
+                                               unsigned* counter, double* smem, double (&out)[NV], int rank,
+                                               int nb) {
   __shared__ bool amLast;
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int j = 0; j < NV; ++j) partials[blockIdx.x * NV + j] = v[j];
+    for (int j = 0; j < NV; ++j) partials[rank * NV + j] = v[j];
     __threadfence();
     unsigned ticket = atomicAdd(counter, 1u);
-    amLast = (ticket == gridDim.x - 1);
+    amLast = (ticket == static_cast<unsigned>(nb) - 1);
   }
   __syncthreads();
   if (!amLast) return false;
@@ -139,7 +141,7 @@ __device__ __forceinline__ bool gridReduce(double (&v)[NV], const int (&ops)[NV]
   double acc[NV];
 #pragma unroll
   for (int j = 0; j < NV; ++j) acc[j] = redIdentity(ops[j]);
-  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
 #pragma unroll
     for (int j = 0; j < NV; ++j) acc[j] = redCombine(acc[j], __ldcg(partials + b * NV + j), ops[j]);
   }
@@ -151,6 +153,14 @@ __device__ __forceinline__ bool gridReduce(double (&v)[NV], const int (&ops)[NV]
     __threadfence();
   }
   return true;
+}
+
+// Grid reduction over the whole launch (block rank = blockIdx.x).
+template <int NV>
+__device__ __forceinline__ bool gridReduce(double (&v)[NV], const int (&ops)[NV], double* partials,
+                                           unsigned* counter, double* smem, double (&out)[NV]) {
+  return gridReduceRank<NV>(v, ops, partials, counter, smem, out, static_cast<int>(blockIdx.x),
+                            static_cast<int>(gridDim.x));
 }
 
 }  // namespace dev

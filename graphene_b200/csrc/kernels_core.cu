@@ -202,6 +202,62 @@ DeviceMatrix::~DeviceMatrix() {
   }
 }
 
+void DeviceMatrix::makeBatch(const std::vector<i64>& rowBegin, const std::vector<i64>& rowReal,
+                             const std::vector<i32>& tileBegin) {
+  const int S = static_cast<int>(rowBegin.size());
+  if (S < 1 || static_cast<int>(rowReal.size()) != S || static_cast<int>(tileBegin.size()) != S + 1)
+    fail(GR_EINVAL, "batch tables");
+  auto B = std::make_unique<BatchSeg>();
+  B->systems = S;
+  B->rowBegin = rowBegin;
+  B->rowReal = rowReal;
+  B->tileBegin = tileBegin;
+  std::vector<i32> r0(S), r1(S);
+  // Per system, the block counts a solve of that system alone would use
+  // (spmvBlocks and the elementwise grid), so that the reductions combine the
+  // same partials in the same order.
+  std::vector<i32> cSys, cRank, cBlocks(S), cBlock0(S), eSys, eRank, eBlocks(S), eBlock0(S);
+  for (int s = 0; s < S; ++s) {
+    if (rowBegin[s] % 32 != 0) fail(GR_EINVAL, "batch systems must start at a multiple of 32 rows");
+    r0[s] = static_cast<i32>(rowBegin[s]);
+    r1[s] = static_cast<i32>(rowBegin[s] + rowReal[s]);
+    const i64 chunks = (rowReal[s] + 31) / 32;
+    cBlocks[s] = static_cast<i32>(std::max<i64>(1, std::min<i64>((chunks + 7) / 8, redBlocks)));
+    eBlocks[s] = static_cast<i32>(std::max<i64>(1, std::min<i64>(redBlocks, (rowReal[s] + 255) / 256)));
+    cBlock0[s] = static_cast<i32>(cSys.size());
+    eBlock0[s] = static_cast<i32>(eSys.size());
+    for (int j = 0; j < cBlocks[s]; ++j) {
+      cSys.push_back(s);
+      cRank.push_back(j);
+    }
+    for (int j = 0; j < eBlocks[s]; ++j) {
+      eSys.push_back(s);
+      eRank.push_back(j);
+    }
+  }
+  B->chunkGrid = static_cast<int>(cSys.size());
+  B->elemGrid = static_cast<int>(eSys.size());
+  B->row0.upload(r0);
+  B->rowEnd.upload(r1);
+  B->chunkSys.upload(cSys);
+  B->chunkRank.upload(cRank);
+  B->chunkBlocks.upload(cBlocks);
+  B->chunkBlock0.upload(cBlock0);
+  B->elemSys.upload(eSys);
+  B->elemRank.upload(eRank);
+  B->elemBlocks.upload(eBlocks);
+  B->elemBlock0.upload(eBlock0);
+  B->partials.alloc(sizeof(double) * 2 * std::max(B->chunkGrid, B->elemGrid));
+  B->counters.alloc(sizeof(unsigned) * S);
+  GR_CUDA(cudaMemsetAsync(B->counters.get(), 0, sizeof(unsigned) * S, ownStream));
+  std::vector<i32> tileSys(P);
+  for (int s = 0; s < S; ++s)
+    for (i32 T = tileBegin[s]; T < tileBegin[s + 1]; ++T) tileSys[T] = s;
+  B->tileSys.upload(tileSys);
+  GR_CUDA(cudaStreamSynchronize(ownStream));
+  batch = std::move(B);
+}
+
 int DeviceMatrix::spmvBlocks() const {
   int need = (sell.nChunks + 7) / 8;
   return std::max(1, std::min(need, redBlocks));
@@ -485,17 +541,21 @@ void launchResidual(DeviceMatrix& A, const void* x, DType xt, const void* b, DTy
   checkLaunch("residual");
 }
 
-void launchNorm(DeviceMatrix& A, const void* x, DType t, int normKind, double* out, cudaStream_t s) {
-  const int blocks = std::max(1, std::min(A.redBlocks, (A.n + 255) / 256));
+void launchNormN(DeviceMatrix& A, const void* x, i64 n, DType t, int normKind, double* out, cudaStream_t s) {
+  const int blocks = static_cast<int>(std::max<i64>(1, std::min<i64>(A.redBlocks, (n + 255) / 256)));
   if (t == DType::F32)
-    dev::normKernel<float><<<blocks, 256, 0, s>>>(static_cast<const float*>(x), A.n, normKind, out,
+    dev::normKernel<float><<<blocks, 256, 0, s>>>(static_cast<const float*>(x), static_cast<int>(n), normKind, out,
                                                   A.partials.as<double>(), A.counter.as<unsigned>());
   else if (t == DType::F64)
-    dev::normKernel<double><<<blocks, 256, 0, s>>>(static_cast<const double*>(x), A.n, normKind, out,
-                                                   A.partials.as<double>(), A.counter.as<unsigned>());
+    dev::normKernel<double><<<blocks, 256, 0, s>>>(static_cast<const double*>(x), static_cast<int>(n), normKind,
+                                                   out, A.partials.as<double>(), A.counter.as<unsigned>());
   else
     fail(GR_EUNSUPPORTED, "norm of a twofloat32 vector");
   checkLaunch("norm");
+}
+
+void launchNorm(DeviceMatrix& A, const void* x, DType t, int normKind, double* out, cudaStream_t s) {
+  launchNormN(A, x, A.n, t, normKind, out, s);
 }
 
 void launchPermute(DeviceMatrix& A, const void* src, void* dst, DType t, bool toTile, cudaStream_t s) {

@@ -32,18 +32,21 @@ template <class MV, class W>
 __global__ void __launch_bounds__(256) bicgInitKernel(SellView<MV> A, const W* __restrict__ x,
                                                        const W* __restrict__ b, W* __restrict__ r,
                                                        W* __restrict__ r0, KState* st, double* partials,
-                                                       unsigned* counter) {
+                                                       unsigned* counter, SegView seg) {
   __shared__ double smem[64];
+  const SegPos sp = segPos(seg, A.n);
+  st += sp.sys;
   const int lane = threadIdx.x & 31;
-  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  const int nWarps = (sp.nb * blockDim.x) >> 5;
+  const int cEnd = (sp.r1 + 31) >> 5;
   const int nk = st->normKind;
   double v[2] = {redIdentity(normOp(nk)), 0.0};
   const int ops[2] = {normOp(nk), RED_SUM};
-  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < A.nChunks; c += nWarps) {
+  for (int c = (sp.r0 >> 5) + ((sp.rank * blockDim.x + threadIdx.x) >> 5); c < cEnd; c += nWarps) {
     const int row = c * 32 + lane;
     const int s0 = __ldg(A.base + c);
     const int K = (__ldg(A.base + c + 1) - s0) >> 5;
-    if (row < A.n) {
+    if (row < sp.r1) {
       W res = sub(__ldg(b + row), sellRowSum<W>(A, x, row, s0, K, lane));
       r[row] = res;
       r0[row] = res;
@@ -53,7 +56,8 @@ __global__ void __launch_bounds__(256) bicgInitKernel(SellView<MV> A, const W* _
   }
   double out[2];
   blockReduce<2>(v, ops, smem);
-  if (gridReduce<2>(v, ops, partials, counter, smem, out) && threadIdx.x == 0) {
+  if (gridReduceRank<2>(v, ops, partials + 2 * sp.b0, counter + sp.sys, smem, out, sp.rank, sp.nb) &&
+      threadIdx.x == 0) {
     const double nrm = normFinish(out[0], nk);
     st->normInit = nrm;
     st->normFinal = nrm;
@@ -73,18 +77,22 @@ __global__ void __launch_bounds__(256) bicgInitKernel(SellView<MV> A, const W* _
 template <class MV, class W, int MODE>
 __global__ void __launch_bounds__(256) spmvDotKernel(SellView<MV> A, const W* __restrict__ x,
                                                       W* __restrict__ y, const W* __restrict__ d1,
-                                                      KState* st, double* partials, unsigned* counter) {
+                                                      KState* st, double* partials, unsigned* counter,
+                                                      SegView seg) {
   __shared__ double smem[64];
+  const SegPos sp = segPos(seg, A.n);
+  st += sp.sys;
   if (st->done) return;
   const int lane = threadIdx.x & 31;
-  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  const int nWarps = (sp.nb * blockDim.x) >> 5;
+  const int cEnd = (sp.r1 + 31) >> 5;
   double v[2] = {0.0, 0.0};
   const int ops[2] = {RED_SUM, RED_SUM};
-  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < A.nChunks; c += nWarps) {
+  for (int c = (sp.r0 >> 5) + ((sp.rank * blockDim.x + threadIdx.x) >> 5); c < cEnd; c += nWarps) {
     const int row = c * 32 + lane;
     const int s0 = __ldg(A.base + c);
     const int K = (__ldg(A.base + c + 1) - s0) >> 5;
-    if (row < A.n) {
+    if (row < sp.r1) {
       const W yv = sellRowSum<W>(A, x, row, s0, K, lane);
       y[row] = yv;
       const double yd = toDouble(yv);
@@ -94,7 +102,8 @@ __global__ void __launch_bounds__(256) spmvDotKernel(SellView<MV> A, const W* __
   }
   double out[2];
   blockReduce<2>(v, ops, smem);
-  if (gridReduce<2>(v, ops, partials, counter, smem, out) && threadIdx.x == 0) {
+  if (gridReduceRank<2>(v, ops, partials + 2 * sp.b0, counter + sp.sys, smem, out, sp.rank, sp.nb) &&
+      threadIdx.x == 0) {
     if (MODE == 0) {
       st->dot0 = out[0];
       st->alpha = st->rho / out[0];
@@ -117,14 +126,16 @@ __global__ void __launch_bounds__(256) bicgUpdateKernel(W* __restrict__ x, const
                                                          const W* __restrict__ z, W* __restrict__ r,
                                                          const W* __restrict__ s, const W* __restrict__ t,
                                                          const W* __restrict__ r0, int n, KState* st,
-                                                         double* partials, unsigned* counter) {
+                                                         double* partials, unsigned* counter, SegView seg) {
   __shared__ double smem[64];
+  const SegPos sp = segPos(seg, n);
+  st += sp.sys;
   if (st->done) return;
   const W al = cvt<W>(st->alpha), om = cvt<W>(st->omega);
   const int nk = st->normKind;
   double v[2] = {redIdentity(normOp(nk)), 0.0};
   const int ops[2] = {normOp(nk), RED_SUM};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (int i = sp.r0 + sp.rank * blockDim.x + threadIdx.x; i < sp.r1; i += sp.nb * blockDim.x) {
     x[i] = add(add(x[i], mul(al, y[i])), mul(om, z[i]));
     const W rv = sub(s[i], mul(om, t[i]));
     r[i] = rv;
@@ -133,7 +144,8 @@ __global__ void __launch_bounds__(256) bicgUpdateKernel(W* __restrict__ x, const
   }
   double out[2];
   blockReduce<2>(v, ops, smem);
-  if (gridReduce<2>(v, ops, partials, counter, smem, out) && threadIdx.x == 0) {
+  if (gridReduceRank<2>(v, ops, partials + 2 * sp.b0, counter + sp.sys, smem, out, sp.rank, sp.nb) &&
+      threadIdx.x == 0) {
     st->normFinal = normFinish(out[0], nk);
     st->converged = converged(st);
     st->rhoOld = st->rho;
@@ -154,7 +166,9 @@ __global__ void __launch_bounds__(256) bicgUpdateKernel(W* __restrict__ x, const
   }
 }
 
-__global__ void stateResetKernel(KState* st, KState init) { *st = init; }
+__global__ void stateResetKernel(KState* st, KState init, int count) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) st[i] = init;
+}
 
 // ---- mixed precision ---------------------------------------------------
 __global__ void castUpKernel(const float* __restrict__ x, void* phi, int E, int n) {
@@ -216,23 +230,56 @@ int elemBlocksN(i64 n) { return static_cast<int>(std::max<i64>(1, std::min<i64>(
 
 }  // namespace
 
+namespace {
+// Launch geometry and reduction scratch of a Krylov kernel: the whole matrix
+// as one system, or the batch's per-system split (`chunk`: row-chunk kernels,
+// else elementwise kernels).
+struct Launch {
+  int blocks;
+  dev::SegView seg;
+  double* partials;
+  unsigned* counter;
+};
+
+Launch krylovLaunch(DeviceMatrix& A, bool chunk) {
+  if (!A.batch) {
+    return Launch{chunk ? A.spmvBlocks() : elemBlocks(A, A.n), dev::SegView{}, A.partials.as<double>(),
+                  A.counter.as<unsigned>()};
+  }
+  const BatchSeg& B = *A.batch;
+  dev::SegView g;
+  if (chunk) {
+    g.blockSys = B.chunkSys.as<int>();
+    g.blockRank = B.chunkRank.as<int>();
+    g.sysBlocks = B.chunkBlocks.as<int>();
+    g.sysBlock0 = B.chunkBlock0.as<int>();
+  } else {
+    g.blockSys = B.elemSys.as<int>();
+    g.blockRank = B.elemRank.as<int>();
+    g.sysBlocks = B.elemBlocks.as<int>();
+    g.sysBlock0 = B.elemBlock0.as<int>();
+  }
+  g.sysRow0 = B.row0.as<int>();
+  g.sysRowEnd = B.rowEnd.as<int>();
+  return Launch{chunk ? B.chunkGrid : B.elemGrid, g, B.partials.as<double>(), B.counters.as<unsigned>()};
+}
+}  // namespace
+
 void launchBicgInit(DeviceMatrix& A, const void* x, const void* b, void* r, void* r0, KState* st, DType W,
                     cudaStream_t s) {
-  const int blocks = A.spmvBlocks();
-  double* part = A.partials.as<double>();
-  unsigned* cnt = A.counter.as<unsigned>();
+  const Launch L = krylovLaunch(A, true);
   if (A.vt == DType::F32 && W == DType::F32)
-    dev::bicgInitKernel<float, float><<<blocks, 256, 0, s>>>(sellView<float>(A), static_cast<const float*>(x),
-                                                             static_cast<const float*>(b), static_cast<float*>(r),
-                                                             static_cast<float*>(r0), st, part, cnt);
+    dev::bicgInitKernel<float, float><<<L.blocks, 256, 0, s>>>(
+        sellView<float>(A), static_cast<const float*>(x), static_cast<const float*>(b), static_cast<float*>(r),
+        static_cast<float*>(r0), st, L.partials, L.counter, L.seg);
   else if (A.vt == DType::F32 && W == DType::F64)
-    dev::bicgInitKernel<float, double><<<blocks, 256, 0, s>>>(
+    dev::bicgInitKernel<float, double><<<L.blocks, 256, 0, s>>>(
         sellView<float>(A), static_cast<const double*>(x), static_cast<const double*>(b), static_cast<double*>(r),
-        static_cast<double*>(r0), st, part, cnt);
+        static_cast<double*>(r0), st, L.partials, L.counter, L.seg);
   else if (A.vt == DType::F64 && W == DType::F64)
-    dev::bicgInitKernel<double, double><<<blocks, 256, 0, s>>>(
+    dev::bicgInitKernel<double, double><<<L.blocks, 256, 0, s>>>(
         sellView<double>(A), static_cast<const double*>(x), static_cast<const double*>(b), static_cast<double*>(r),
-        static_cast<double*>(r0), st, part, cnt);
+        static_cast<double*>(r0), st, L.partials, L.counter, L.seg);
   else
     fail(GR_EUNSUPPORTED, "PBiCGStab with float64 coefficients needs float64 vectors");
   checkLaunch("bicg_init");
@@ -241,17 +288,15 @@ void launchBicgInit(DeviceMatrix& A, const void* x, const void* b, void* r, void
 namespace {
 template <class MV, class W>
 void spmvDotT(DeviceMatrix& A, const void* x, void* y, const void* d1, int mode, KState* st, cudaStream_t s) {
-  const int blocks = A.spmvBlocks();
-  double* part = A.partials.as<double>();
-  unsigned* cnt = A.counter.as<unsigned>();
+  const Launch L = krylovLaunch(A, true);
   if (mode == 0)
-    dev::spmvDotKernel<MV, W, 0><<<blocks, 256, 0, s>>>(sellView<MV>(A), static_cast<const W*>(x),
-                                                        static_cast<W*>(y), static_cast<const W*>(d1), st, part,
-                                                        cnt);
+    dev::spmvDotKernel<MV, W, 0><<<L.blocks, 256, 0, s>>>(sellView<MV>(A), static_cast<const W*>(x),
+                                                          static_cast<W*>(y), static_cast<const W*>(d1), st,
+                                                          L.partials, L.counter, L.seg);
   else
-    dev::spmvDotKernel<MV, W, 1><<<blocks, 256, 0, s>>>(sellView<MV>(A), static_cast<const W*>(x),
-                                                        static_cast<W*>(y), static_cast<const W*>(d1), st, part,
-                                                        cnt);
+    dev::spmvDotKernel<MV, W, 1><<<L.blocks, 256, 0, s>>>(sellView<MV>(A), static_cast<const W*>(x),
+                                                          static_cast<W*>(y), static_cast<const W*>(d1), st,
+                                                          L.partials, L.counter, L.seg);
 }
 }  // namespace
 
@@ -266,24 +311,22 @@ void launchSpmvDot(DeviceMatrix& A, const void* x, void* y, const void* d1, int 
 
 void launchBicgUpdate(DeviceMatrix& A, void* x, const void* y, const void* z, void* r, const void* sv,
                       const void* t, const void* r0, KState* st, DType W, cudaStream_t s) {
-  const int blocks = elemBlocks(A, A.n);
-  double* part = A.partials.as<double>();
-  unsigned* cnt = A.counter.as<unsigned>();
+  const Launch L = krylovLaunch(A, false);
   if (W == DType::F32)
-    dev::bicgUpdateKernel<float><<<blocks, 256, 0, s>>>(
+    dev::bicgUpdateKernel<float><<<L.blocks, 256, 0, s>>>(
         static_cast<float*>(x), static_cast<const float*>(y), static_cast<const float*>(z), static_cast<float*>(r),
-        static_cast<const float*>(sv), static_cast<const float*>(t), static_cast<const float*>(r0), A.n, st, part,
-        cnt);
+        static_cast<const float*>(sv), static_cast<const float*>(t), static_cast<const float*>(r0), A.n, st,
+        L.partials, L.counter, L.seg);
   else
-    dev::bicgUpdateKernel<double><<<blocks, 256, 0, s>>>(
+    dev::bicgUpdateKernel<double><<<L.blocks, 256, 0, s>>>(
         static_cast<double*>(x), static_cast<const double*>(y), static_cast<const double*>(z),
         static_cast<double*>(r), static_cast<const double*>(sv), static_cast<const double*>(t),
-        static_cast<const double*>(r0), A.n, st, part, cnt);
+        static_cast<const double*>(r0), A.n, st, L.partials, L.counter, L.seg);
   checkLaunch("bicg_update");
 }
 
-void launchStateReset(KState* st, const KState& init, cudaStream_t s) {
-  dev::stateResetKernel<<<1, 1, 0, s>>>(st, init);
+void launchStateReset(KState* st, const KState& init, cudaStream_t s, int count) {
+  dev::stateResetKernel<<<(count + 255) / 256, 256, 0, s>>>(st, init, count);
   checkLaunch("state_reset");
 }
 

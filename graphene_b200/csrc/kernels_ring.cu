@@ -105,7 +105,8 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
                                                                SPro<W> pro, W* __restrict__ y, int* errFlag) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int abortFlag;
-  if (pro.st && pro.st->done) return;
+  const KState* st = pro.state();
+  if (st && st->done) return;
   constexpr uint32_t kEnt = sizeof(MV) == 4 ? 8 : 16;
   const int T = blockIdx.x;
   const int base = blockStart[T];
@@ -134,11 +135,11 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
   {
     W beta = W(0), omega = W(0), alpha = W(0);
     bool first = true;
-    if (pro.st) {
-      beta = cvt<W>(pro.st->beta);
-      omega = cvt<W>(pro.st->omega);
-      alpha = cvt<W>(pro.st->alpha);
-      first = pro.st->iter == 0;
+    if (st) {
+      beta = cvt<W>(st->beta);
+      omega = cvt<W>(st->omega);
+      alpha = cvt<W>(st->alpha);
+      first = st->iter == 0;
     }
     for (int i = threadIdx.x; i < nRows; i += blockDim.x) xs[i] = pro(base + i, beta, omega, alpha, first);
     if (lead) xs[nRows] = W(0);
@@ -260,8 +261,9 @@ void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool di
   const size_t smem = iluRingSmem(A, R, dtypeOf<W>());
   auto kernel = unroll ? dev::iluRingKernel<MV, W, true> : dev::iluRingKernel<MV, W, false>;
   ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
+  if (p.stIndex && R.group != 1) fail(GR_EUNSUPPORTED, "batched solves run one tile per block");
   dev::SPro<W> pro{static_cast<int>(p.kind), static_cast<const W*>(p.b), static_cast<const W*>(p.r),
-                   static_cast<W*>(p.pOrS), static_cast<const W*>(p.v), p.st};
+                   static_cast<W*>(p.pOrS), static_cast<const W*>(p.v), p.st, p.stIndex};
   kernel<<<R.numGroups, dev::kRingThreads, smem, s>>>(static_cast<const unsigned char*>(stream),
                                              R.tileOffset.as<long long>(), R.meta.as<int4>(), R.tileLevel.as<int>(),
                                              R.groupStart.as<int>(),

@@ -37,6 +37,7 @@ struct PrologueArgs {
   void* pOrS = nullptr;     // p (read and written) or s (written)
   const void* v = nullptr;
   const KState* st = nullptr;  // scalars; also the early-exit flag (may be null)
+  const int* stIndex = nullptr;  // batches: state index per tile (ring kernel only)
 };
 
 // ---- ILU(0) / DILU ----------------------------------------------------
@@ -116,7 +117,7 @@ void launchBicgUpdate(DeviceMatrix& A, void* x, const void* y, const void* z, vo
 // the result into copyTo when non-null.
 void launchPrologue(DeviceMatrix& A, const PrologueArgs& pro, void* copyTo, DType W, cudaStream_t s);
 // Writes the initial state (single thread).
-void launchStateReset(KState* st, const KState& init, cudaStream_t s);
+void launchStateReset(KState* st, const KState& init, cudaStream_t s, int count = 1);
 // Norm of a vector into st->bNorm.
 void launchNormInto(DeviceMatrix& A, const void* x, DType t, int normKind, double* out, cudaStream_t s);
 

@@ -17,6 +17,31 @@ struct SellView {
   const MV* __restrict__ diag;
 };
 
+// Splits one launch into independent systems (a batch of block-diagonal
+// systems solved together). Block b belongs to system sys[b] and is number
+// rank[b] of that system's blocks; system s owns blocks [block0[s],
+// block0[s] + blocks[s]) and rows [row0[s], rowEnd[s]), row0 a multiple of
+// 32. Without tables (blockSys null) the whole launch is one system, and the
+// kernels behave exactly as before.
+struct SegView {
+  const int* blockSys = nullptr;
+  const int* blockRank = nullptr;
+  const int* sysBlocks = nullptr;
+  const int* sysBlock0 = nullptr;
+  const int* sysRow0 = nullptr;
+  const int* sysRowEnd = nullptr;
+};
+
+struct SegPos {
+  int sys, rank, nb, b0, r0, r1;
+};
+
+__device__ __forceinline__ SegPos segPos(const SegView& g, int n) {
+  if (!g.blockSys) return {0, static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x), 0, 0, n};
+  const int s = g.blockSys[blockIdx.x];
+  return {s, g.blockRank[blockIdx.x], g.sysBlocks[s], g.sysBlock0[s], g.sysRow0[s], g.sysRowEnd[s]};
+}
+
 // Loads x[i] converted to the accumulation type.
 template <class Acc, class XT>
 __device__ __forceinline__ Acc loadX(const XT* __restrict__ x, int i) {

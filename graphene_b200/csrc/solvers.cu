@@ -36,6 +36,10 @@ class Node {
   virtual void copyPhi(void*, DType) { fail(GR_EUNSUPPORTED, "only IterativeRefinement keeps phi"); }
   // Allocates the scratch a solve of type W needs (before graph capture).
   virtual void prepare(DType) {}
+  // Per-system statistics of the last solve of a batch.
+  virtual std::vector<gr_stats> batchStats() const {
+    fail(GR_EUNSUPPORTED, "only PBiCGStab solves batches");
+  }
 
  protected:
   DeviceMatrix& A_;
@@ -124,6 +128,7 @@ class IluNode : public Node {
     GR_CUDA(cudaStreamSynchronize(s()));
   }
   bool streamed() const { return sweep_ != nullptr; }
+  bool ringKernel() const { return kernel_ == 4; }
   gr_stats solve(void* x, const void* b, DType W, const KState* gate) override {
     PrologueArgs pro;
     pro.kind = Prologue::Plain;
@@ -292,12 +297,23 @@ class PbicgstabNode : public Node {
       ilu_ = dynamic_cast<IluNode*>(pre_.get());
       gs_ = dynamic_cast<GsNode*>(pre_.get());
     }
-    st_.alloc(sizeof(KState));
-    host_ = static_cast<KState*>(acquirePinnedSlot());
+    if (A.batch) {
+      // A batch keeps one state per system; its preconditioner must look
+      // up a block's system, which the ring substitution kernel does.
+      if (!ilu_ || !ilu_->ringKernel())
+        fail(GR_EUNSUPPORTED, "batched PBiCGStab needs the ILU preconditioner with the ring kernel");
+      systems_ = A.batch->systems;
+      GR_CUDA(cudaMallocHost(&host_, sizeof(KState) * systems_));
+      batchHost_ = true;
+    } else {
+      host_ = static_cast<KState*>(acquirePinnedSlot());
+    }
+    st_.alloc(sizeof(KState) * systems_);
   }
   ~PbicgstabNode() override {
     if (exec_) cudaGraphExecDestroy(exec_);
-    if (host_) releasePinnedSlot(host_);
+    if (host_ && batchHost_) cudaFreeHost(host_);
+    else if (host_) releasePinnedSlot(host_);
   }
 
   gr_stats solve(void* x, const void* b, DType Wx, const KState* gate) override {
@@ -314,10 +330,18 @@ class PbicgstabNode : public Node {
     init.minIter = cfg_.minIterations;
     init.normKind = cfg_.norm;
     KState* st = st_.as<KState>();
-    launchStateReset(st, init, s());
+    launchStateReset(st, init, s(), systems_);
     // The reference takes ||x|| here (pbicgstab/Solver.cpp:69-70); the norm
     // of b is what relTolerance is documented to use (SolverStats.hpp:52-60).
-    if (cfg_.relTolerance > 0) launchNorm(A_, b, W, cfg_.norm, &st->bNorm, s());
+    if (cfg_.relTolerance > 0) {
+      if (!A_.batch) {
+        launchNorm(A_, b, W, cfg_.norm, &st->bNorm, s());
+      } else {
+        for (int k = 0; k < systems_; ++k)
+          launchNormN(A_, static_cast<const char*>(b) + A_.batch->rowBegin[k] * dtypeSize(W), A_.batch->rowReal[k], W,
+                      cfg_.norm, &st[k].bNorm, s());
+      }
+    }
     GR_CUDA(cudaMemcpyAsync(xw(), x, vb, cudaMemcpyDeviceToDevice, s()));
     launchBicgInit(A_, xw(), b, buf(R), buf(R0), st, W, s());
     const bool graphable = ilu_ || !pre_ || (gs_ && cfg_.preconditioner->numFixedIterations > 0);
@@ -331,10 +355,12 @@ class PbicgstabNode : public Node {
         iteration(W);
         issued += 1;
       }
-      GR_CUDA(cudaMemcpyAsync(host_, st, sizeof(KState), cudaMemcpyDeviceToHost, s()));
+      GR_CUDA(cudaMemcpyAsync(host_, st, sizeof(KState) * systems_, cudaMemcpyDeviceToHost, s()));
       GR_CUDA(cudaStreamSynchronize(s()));
       if (perIter) printStats(cfg_, A_, stats());
-      if (host_->done) break;
+      bool all = true;
+      for (int k = 0; k < systems_; ++k) all = all && host_[k].done;
+      if (all) break;
       if (issued > cfg_.maxIterations && issued > (1 << 30)) break;
     }
     GR_CUDA(cudaMemcpyAsync(x, xw(), vb, cudaMemcpyDeviceToDevice, s()));
@@ -344,9 +370,16 @@ class PbicgstabNode : public Node {
     return out;
   }
   bool usesInitialGuess() const override { return true; }
+  std::vector<gr_stats> batchStats() const override {
+    std::vector<gr_stats> out(systems_);
+    for (int k = 0; k < systems_; ++k) out[k] = statsOf(host_[k]);
+    return out;
+  }
 
  private:
   enum { X = 0, R, R0, P, V, Y, S, Z, T, NBUF };
+  int systems_ = 1;
+  bool batchHost_ = false;
   std::unique_ptr<Node> pre_;
   IluNode* ilu_ = nullptr;
   GsNode* gs_ = nullptr;
@@ -373,15 +406,27 @@ class PbicgstabNode : public Node {
     }
   }
 
-  gr_stats stats() const {
+  static gr_stats statsOf(const KState& h) {
     gr_stats o{};
-    o.initial_residual = host_->normInit;
-    o.final_residual = host_->normFinal;
-    o.b_norm = host_->bNorm;
-    o.iterations = host_->iter;
-    o.converged = host_->converged;
-    o.singular = host_->singular;
-    o.status = host_->status;
+    o.initial_residual = h.normInit;
+    o.final_residual = h.normFinal;
+    o.b_norm = h.bNorm;
+    o.iterations = h.iter;
+    o.converged = h.converged;
+    o.singular = h.singular;
+    o.status = h.status;
+    return o;
+  }
+  // One system: its statistics. A batch: the slowest system's iterations,
+  // converged / singular / status over all systems, system 0's norms.
+  gr_stats stats() const {
+    gr_stats o = statsOf(host_[0]);
+    for (int k = 1; k < systems_; ++k) {
+      o.iterations = std::max(o.iterations, host_[k].iter);
+      o.converged = o.converged && host_[k].converged;
+      o.singular = o.singular || host_[k].singular;
+      if (o.status == GR_OK) o.status = host_[k].status;
+    }
     return o;
   }
 
@@ -415,6 +460,7 @@ class PbicgstabNode : public Node {
     p.pOrS = buf(P);
     p.v = buf(V);
     p.st = st;
+    p.stIndex = A_.batch ? A_.batch->tileSys.as<int>() : nullptr;
     precondition(p, buf(Y), W);
     launchSpmvDot(A_, buf(Y), buf(V), buf(R0), 0, st, W, s());
     PrologueArgs q;
@@ -423,6 +469,7 @@ class PbicgstabNode : public Node {
     q.pOrS = buf(S);
     q.v = buf(V);
     q.st = st;
+    q.stIndex = p.stIndex;
     precondition(q, buf(Z), W);
     launchSpmvDot(A_, buf(Z), buf(T), buf(S), 1, st, W, s());
     launchBicgUpdate(A_, xw(), buf(Y), buf(Z), buf(R), buf(S), buf(T), buf(R0), st, W, s());
@@ -636,6 +683,7 @@ class Tree : public SolverTree {
     return st;
   }
   void copyPhi(void* out, DType t) override { root_->copyPhi(out, t); }
+  std::vector<gr_stats> batchStats() const override { return root_->batchStats(); }
   std::string name() const override { return cfg_->solverName(); }
 
  private:

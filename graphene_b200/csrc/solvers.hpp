@@ -4,6 +4,7 @@
 
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "device.hpp"
 
@@ -24,6 +25,8 @@ class SolverTree {
   // (ILU, a fixed number of Gauss-Seidel sweeps).
   virtual float timeRepeated(void* x, DType xt, const void* b, DType bt, int reps) = 0;
   virtual void copyPhi(void* out, DType t) = 0;
+  // Per-system statistics of the last solve on a batch matrix.
+  virtual std::vector<gr_stats> batchStats() const = 0;
   virtual std::string name() const = 0;
 };
 

@@ -414,6 +414,23 @@ int gr_server_counters(gr_server* s, int64_t* queued, int64_t* running, int64_t*
 /* Finishes the running solves, drops the queued ones, releases everything. */
 void gr_server_destroy(gr_server* s);
 
+/* ---- batched solves --------------------------------------------------
+ * No counterpart in the reference. Solves count independent systems of any
+ * sizes with one PBiCGStab whose every kernel launch covers all of them:
+ * the systems are stored as one block-diagonal device matrix, each keeps its
+ * own Krylov state and convergence test on the device, and a system that
+ * has converged drops out of the work while the others continue. Each
+ * system's result equals the result of solving it alone with the same
+ * configuration. json: a PBiCGStab configuration with the ILU
+ * preconditioner (the ring substitution kernel, one tile per block); the
+ * systems share one coefficient type. */
+typedef struct gr_batch gr_batch;
+int gr_batch_create(gr_host_matrix* const* systems, int32_t count, const char* json, gr_batch** out);
+/* x[i] (in: initial guess, out: solution) and b[i]: host vectors of system i
+ * in natural order, type t; stats: count entries (may be NULL). */
+int gr_batch_solve_host(gr_batch* b, void* const* x, const void* const* rhs, gr_dtype t, gr_stats* stats);
+void gr_batch_destroy(gr_batch* b);
+
 #ifdef __cplusplus
 }
 #endif
