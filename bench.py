@@ -382,6 +382,59 @@ def serving(gb, requests=300, slots=4, pool=32, seed=7):
     return out
 
 
+def batching(gb, systems=64, seed=11, reps=3):
+    """Many uneven systems: 7-point variable-coefficient Poisson (sigma 1),
+    grid edge U{16..48}, FP32 PBiCGStab + ILU(0) (ring kernel) to 1e-6,
+    host vectors in and out. One batch (gr_batch_solve_host: every launch
+    covers all systems) against the same systems solved one after another
+    by resident solvers (gr_solve_host); best of `reps` wall-clock passes,
+    setup (upload, factorisation) excluded from both. The batch's solutions
+    are compared bit for bit with the one-by-one ones."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    cfg = {"type": "PBiCGStab", "maxIterations": 1000, "relResidual": 1e-6,
+           "preconditioner": {"type": "ILU", "kernel": "ring"}}
+    hs, bs = [], []
+    for k in range(systems):
+        L = int(rng.integers(16, 49))
+        hs.append(gb.generateMatrix(gb.GEN_VAR_POISSON, L, L, L, (1.0,), 3000 + k, max(1, L ** 3 // 3456)))
+        bs.append(gb.randomVector(4000 + k, hs[-1].numRows).astype(np.float32))
+    rows = sum(h.numRows for h in hs)
+    solvers = [gb.Solver(h.copyToTile(), cfg) for h in hs]
+    B = gb.Batch(hs, cfg)
+
+    def one_by_one():
+        xs, sts = [], []
+        for s, h, b in zip(solvers, hs, bs):
+            x = np.zeros(h.numRows, np.float32)
+            sts.append(s.solveHost(x, b))
+            xs.append(x)
+        return xs, sts
+
+    def best(fn):
+        fn()
+        t, out = None, None
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            out = fn()
+            dt = (time.perf_counter() - t0) * 1e3
+            t = dt if t is None else min(t, dt)
+        return t, out
+    t_seq, (xs_seq, st_seq) = best(one_by_one)
+    t_bat, (xs_bat, st_bat) = best(lambda: B.solveHost(bs))
+    same = all(np.array_equal(a, b) for a, b in zip(xs_seq, xs_bat)) and \
+        all(a.iterations == b.iterations for a, b in zip(st_seq, st_bat))
+    its = [s.iterations for s in st_bat]
+    B.close()
+    return {"systems": systems, "rows_total": rows, "grid_edges": "U{16..48}",
+            "iterations_min_max": [min(its), max(its)],
+            "batch_ms": t_bat, "one_by_one_ms": t_seq,
+            "batch_systems_per_s": systems / (t_bat * 1e-3),
+            "one_by_one_systems_per_s": systems / (t_seq * 1e-3),
+            "speedup": t_seq / t_bat, "identical_to_one_by_one": same,
+            "all_converged": all(s.converged for s in st_bat)}
+
+
 def event_ms(fn):
     import torch
     e0 = torch.cuda.Event(enable_timing=True)
@@ -482,6 +535,7 @@ def main():
                            "converged": sx.converged, "rel_residual_fp64": rel64(A, sv.phi(gb.FLOAT64), b)}
         extra["configs"] = other_configs(gb, peak)
         extra["serving"] = serving(gb)
+        extra["batching"] = batching(gb)
 
     # Kernel timings: SpMV and the ILU(0) application (HBM rooflines).
     y = torch.empty_like(x_true)
