@@ -514,25 +514,38 @@ def main():
         r = Amat.residual(xv, rhs, destType=gb.FLOAT64, intermediateType=gb.FLOAT64)
         return float(torch.linalg.vector_norm(r)) / bnorm
 
+    def best_of(fn, reps=2):
+        """Fastest of `reps` runs (solver creation + solve, CUDA events) after
+        one untimed run; the previous run's solver is released and collected
+        before each timed run, so no teardown falls inside the timed region."""
+        import gc
+        out = fn()
+        best = None
+        for _ in range(reps):
+            out = None
+            gc.collect()
+            torch.cuda.synchronize()
+            ms, out = event_ms(fn)
+            best = ms if best is None else min(best, ms)
+        return best, out
+
     extra = {}
     if not a.no_extras:
         h64 = h.astype(gb.FLOAT64)
         A64 = h64.copyToTile()
         b64 = b.double()
-        solve(A64, FP64_CONFIG, b64)
-        torch.cuda.synchronize()
-        fp64_ms, (_, x64, st64) = event_ms(lambda: solve(A64, FP64_CONFIG, b64))
+        fp64_ms, (s64, x64, st64) = best_of(lambda: solve(A64, FP64_CONFIG, b64))
         extra["fp64_pbicgstab_ilu0"] = {"ms": fp64_ms, "iterations": st64.iterations,
                                         "converged": st64.converged,
                                         "rel_residual_fp64": rel64(A64, x64, b64)}
         extra["speedup_mpir_vs_fp64"] = fp64_ms / ms_per_step
-        del A64, h64
+        del s64, x64, A64, h64, b64
         for name, c in [("mpir_twofloat32", mpir_config(a, "twofloat32")),
                         ("mpir_float64_inner_tol_1e-3", mpir_config(a, "float64", 1e-3))]:
-            solve(A, c, b)
-            ms, (sv, _, sx) = event_ms(lambda: solve(A, c, b))
+            ms, (sv, xv, sx) = best_of(lambda: solve(A, c, b))
             extra[name] = {"ms": ms, "outer": sx.iterations, "inner": sx.innerIterations,
                            "converged": sx.converged, "rel_residual_fp64": rel64(A, sv.phi(gb.FLOAT64), b)}
+            del sv, xv
         extra["configs"] = other_configs(gb, peak)
         extra["serving"] = serving(gb)
         extra["batching"] = batching(gb)
@@ -580,8 +593,8 @@ def main():
     tf = ROOT / "profiles" / "ilu_ring_var_poisson_160.md"
     if dom[0] == "ilu0_apply" and a.grid == 192 and tf.exists():
         import re
-        m = re.search(r"traffic_bytes_192: (\d+)", tf.read_text())
-        traffic = int(m.group(1)) if m else None
+        hit = re.search(r"traffic_bytes_192: (\d+)", tf.read_text())
+        traffic = int(hit.group(1)) if hit else None
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

@@ -44,7 +44,59 @@ __device__ __forceinline__ bool mbarTryWait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// try_wait that lets the thread sleep until the phase completes or about
+// `hintNs` nanoseconds pass, instead of returning at once: a waiting warp
+// then takes no issue slots from the warps that do work.
+__device__ __forceinline__ bool mbarTryWaitSleep(uint32_t bar, uint32_t parity, uint32_t hintNs) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(hintNs)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t globalTimerNs() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Longest wait for one mbarrier phase before a kernel reports GR_ETIMEOUT.
+constexpr uint64_t kWaitNs = 1000000000ull;  // 1 s
+// Bounded sleeping wait for the phase of `bar` with the given parity: true
+// once it has completed; false after kWaitNs, after kWaitLimit sleeps, or
+// (when `abort` is given) once *abort is set by another warp of the block.
+__device__ __forceinline__ bool mbarWaitBounded(uint32_t bar, uint32_t parity, const volatile int* abort = nullptr) {
+  if (mbarTryWait(bar, parity)) return true;
+  const uint64_t t0 = globalTimerNs();
+  for (long long it = 0; it < kWaitLimit; ++it) {
+    if (mbarTryWaitSleep(bar, parity, 20000)) return true;
+    if (abort && *abort) return false;
+    if (globalTimerNs() - t0 > kWaitNs) return false;
+  }
+  return false;
+}
 __device__ __forceinline__ void fenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// Arrival (release semantics, CTA scope) on an mbarrier.
+__device__ __forceinline__ void mbarArrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+// Barrier `id` (1..15) among `count` threads (a multiple of 32) that also
+// returns, to every one of them, the OR of their `v`.
+__device__ __forceinline__ bool namedBarOr(int id, int count, bool v) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 q, %3, 0;\n\t"
+      "bar.red.or.pred p, %1, %2, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(out)
+      : "r"(id), "r"(count), "r"(static_cast<uint32_t>(v))
+      : "memory");
+  return out != 0;
+}
 // Hint: bring [src, src + bytes) into L2 (no completion, no shared memory).
 __device__ __forceinline__ void prefetchL2(const void* src, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");

@@ -153,17 +153,43 @@ void checkIluStream(const HostMatrix& H, const HostStream& S, bool dilu, DType v
 //   ents  E*k entries, entry-major, {i32 column, value}: 8 bytes for float,
 //         16 for double ({column, 0, value})                    (padded)
 // Padding entries use column nRows (a zero slot of the kernel's x slice) and
-// value 0. Two int4 per level: {k, E, block bytes, ring offset} and
-// {inv offset, entries offset, issueAfter, upper}. The kernel copies a
-// level's block into its shared-memory ring at `ring offset` once the tile's
-// level `issueAfter` has been consumed (-1: at the start); the host chose the
-// offsets so that a copy never overwrites a level still to be consumed, and
-// so that every level is copied at least one level before it is needed.
+// value 0. One int4 per level: {k, E | upper << 30, ring offset,
+// issueAfter}; the block's segment offsets and size follow from k, E, upper
+// and DILU (ringLevelLayout). The kernel copies a level's block into its
+// shared-memory ring at `ring offset` once the tile's level `issueAfter` has
+// been consumed (-1: at the start); the host chose the offsets so that a
+// copy never overwrites a level still to be consumed, and so that every
+// level is copied at least one level before it is needed.
 constexpr int kRingBarriers = 16;
+constexpr int kRingUpperBit = 1 << 30;
+
+// Byte offsets of a level block's inverse diagonal and entries, and its size.
+struct RingLevelLayout {
+  uint32_t inv, ents, bytes;
+};
+__host__ __device__ inline RingLevelLayout ringLevelLayout(uint32_t k, uint32_t E, bool hasInv, uint32_t valueBytes) {
+  const uint32_t entBytes = valueBytes == 4 ? 8u : 16u;
+  const uint32_t rowsB = (4u * k + 15u) & ~15u;
+  const uint32_t invB = hasInv ? ((valueBytes * k + 15u) & ~15u) : 0u;
+  const uint32_t entB = (entBytes * E * k + 15u) & ~15u;
+  return RingLevelLayout{rowsB, rowsB + invB, rowsB + invB + entB};
+}
+
+// What the default ring size is chosen for: the SM count, shared memory per
+// SM, the shared memory the runtime reserves per block, and the blocks per SM
+// that threads and registers allow. The default ring is the size (between the
+// smallest that places and max(16 KB, 4 x the largest level)) that needs the
+// fewest waves of blocks, the largest such.
+struct RingBudget {
+  i32 numSMs = 148;
+  i64 smemPerSM = 233472;
+  i64 reservedPerBlock = 1024;
+  i32 maxBlocksPerSM = 10;
+};
 struct HostRing {
   std::vector<uint8_t> bytes;
   std::vector<i64> tileOffset;  // P + 1
-  std::vector<int4> meta;       // 2 per level
+  std::vector<int4> meta;       // 1 per level
   std::vector<i32> tileLevel;   // P + 1
   std::vector<i32> valPos, valSrc, invPos, invSrc;  // element positions (value type units)
   i64 ringBytes = 0, maxLevelBytes = 0, maxGroupRows = 0;
@@ -171,10 +197,18 @@ struct HostRing {
   i32 group = 1;                // tiles per thread block
   std::vector<i32> groupStart;  // first tile-order row of every block, and n
 };
+// Shared memory of one ring-kernel block besides the ring: barriers, the
+// level table and the block's slice of x (plus its zero slot).
+// Header: kRingBarriers full and kRingBarriers empty mbarriers, one for the
+// level table, padded to 16 bytes.
+constexpr i64 kRingHeader = (8 * (2 * kRingBarriers + 1) + 15) / 16 * 16;
+inline i64 ringFixedSmem(i32 maxTileLevels, i64 maxGroupRows, i64 vectorBytes) {
+  return kRingHeader + 16 * static_cast<i64>(maxTileLevels) + (maxGroupRows + 1) * vectorBytes;
+}
 // One thread block runs `group` consecutive tiles in lockstep (tileOffset,
-// tileLevel and meta are then per block). ringBytes 0: the default,
-// max(16 KB, 2.5 x the largest level block).
-HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes, i32 group);
+// tileLevel and meta are then per block). ringBytes 0: the default (RingBudget).
+HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes, i32 group,
+                        const RingBudget& budget = RingBudget{});
 // Replays the kernel's copies and reads on the host; throws GR_EINVAL on an
 // out-of-range index, a dependency-order violation, a copy that would
 // overwrite a level not yet consumed, or a copy issued too late.
@@ -281,6 +315,9 @@ struct DeviceMatrix {
 // so it is only ever raised (a lower request never undoes a higher one that
 // another thread's launch relies on).
 void ensureDynamicSmem(const void* fn, size_t bytes);
+// Asks for the largest shared-memory carveout for `fn` (once per device), so
+// that as many of its blocks as shared memory allows are resident per SM.
+void preferSharedCarveout(const void* fn);
 
 // ---- launchers -------------------------------------------------------
 

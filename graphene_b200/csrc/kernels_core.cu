@@ -10,6 +10,7 @@
 #include <atomic>
 #include <cstring>
 #include <map>
+#include <set>
 #include <mutex>
 
 #include "device.hpp"
@@ -72,6 +73,16 @@ void ensureDynamicSmem(const void* fn, size_t bytes) {
   if (bytes <= cur) return;
   GR_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
   cur = bytes;
+}
+
+void preferSharedCarveout(const void* fn) {
+  int dev = 0;
+  GR_CUDA(cudaGetDevice(&dev));
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!done.insert({dev, fn}).second) return;
+  GR_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
 }
 
 void DBuf::alloc(size_t bytes) {

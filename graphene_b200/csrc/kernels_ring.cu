@@ -10,13 +10,17 @@
 // bytes from this GPU's memory). The host fixed each level's ring offset and
 // the level after which its copy is issued, so the kernel does no ring
 // arithmetic: a level's rows, inverse diagonal and (column, value) entries
-// sit at fixed offsets. Per level: four compute warps compute the level's
-// rows from shared memory, one producer warp issues the copies that the
-// previous level released and another waits until the next level has
-// landed; one barrier ends the level.
+// sit at fixed offsets. Producer and consumers form a pipeline over
+// kRingBarriers pairs of mbarriers: the producer warp issues level j's copy
+// (completing on full[j % 16]) once level issueAfter(j) has been released
+// (empty[...]). The four compute warps compute level l's rows from shared
+// memory while a waiting warp waits for full[(l + 1) % 16]; the five meet
+// at a barrier of their own that ends level l, after which the waiting warp
+// releases level l. Neither the producer's copies nor the mbarrier waits
+// and arrivals sit on the compute warps' per-level chain.
 //
 // Every wait is bounded; when one runs out the block records GR_ETIMEOUT in
-// the matrix's error word, stops at the next barrier, and the issuing lane
+// the matrix's error word, the other waits give up, and the issuing lane
 // waits (bounded) for the copies still in flight before the block exits.
 #include <algorithm>
 
@@ -29,9 +33,10 @@
 namespace gr {
 namespace dev {
 
-// Four compute warps, an issuing warp and a waiting warp per block.
+// Four compute warps, a waiting warp and a producer warp per block.
 constexpr int kRingCompute = 128;
-constexpr int kRingThreads = kRingCompute + 64;
+constexpr int kRingLevelSync = kRingCompute + 32;  // compute warps + waiting warp
+constexpr int kRingThreads = kRingLevelSync + 32;
 constexpr int kPrefetchAhead = 0;  // default bytes kept prefetched into L2 beyond the issued copies
 
 // Entry of a level block: column and value (the value at byte 4 for float,
@@ -49,12 +54,6 @@ __device__ __forceinline__ void loadEntry<double>(const unsigned char* p, int& c
   const int4 e = *reinterpret_cast<const int4*>(p);
   c = e.x;
   v = __hiloint2double(e.w, e.z);
-}
-
-__device__ __forceinline__ bool waitBar(uint32_t bar, uint32_t parity) {
-  for (long long it = 0; it < kWaitLimit; ++it)
-    if (mbarTryWait(bar, parity)) return true;
-  return false;
 }
 
 // temp -= sum_e value_e * xs[column_e] over a row's E entries in order.
@@ -95,6 +94,28 @@ __device__ __forceinline__ W ringRowDot(W temp, const unsigned char* p, uint32_t
   return temp;
 }
 
+// A level of the ring as the compute warps see it.
+template <class MV>
+struct RingLevel {
+  int k, E;
+  bool upper;
+  const unsigned char* blk;  // the level block in the ring
+  uint32_t inv, ents;        // offsets of its inverse diagonal and entries
+};
+template <class MV>
+__device__ __forceinline__ RingLevel<MV> ringLevelAt(const int4 m, const unsigned char* ring, bool dilu) {
+  RingLevel<MV> lv;
+  lv.k = m.x;
+  lv.E = m.y & (kRingUpperBit - 1);
+  lv.upper = (m.y & kRingUpperBit) != 0;
+  const RingLevelLayout lay =
+      ringLevelLayout(static_cast<uint32_t>(lv.k), static_cast<uint32_t>(lv.E), lv.upper || dilu, sizeof(MV));
+  lv.blk = ring + m.z;
+  lv.inv = lay.inv;
+  lv.ents = lay.ents;
+  return lv;
+}
+
 template <class MV, class W, bool UNROLL>
 __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned char* __restrict__ stream,
                                                                const long long* __restrict__ tileOffset,
@@ -104,7 +125,7 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
                                                                int metaLevels, uint32_t l2Ahead, bool dilu,
                                                                SPro<W> pro, W* __restrict__ y, int* errFlag) {
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ int abortFlag;
+  __shared__ int abortFlag, consumedLevels;
   const KState* st = pro.state();
   if (st && st->done) return;
   constexpr uint32_t kEnt = sizeof(MV) == 4 ? 8 : 16;
@@ -113,24 +134,30 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
   const int nRows = blockStart[T + 1] - base;
   const int lv0 = tileLevel[T];
   const int L = tileLevel[T + 1] - lv0;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);  // kRingBarriers level barriers + 1 for the table
-  int4* mt = reinterpret_cast<int4*>(smem + 256);
-  unsigned char* ring = smem + 256 + 32 * metaLevels;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);  // level landed, one per barrier slot
+  uint64_t* empty = full + kRingBarriers;              // level consumed by the compute warps
+  uint64_t* tableBar = empty + kRingBarriers;
+  int4* mt = reinterpret_cast<int4*>(smem + kRingHeader);
+  unsigned char* ring = smem + kRingHeader + 16 * metaLevels;
   W* xs = reinterpret_cast<W*>(ring + ringBytes);
   const unsigned char* g = stream + tileOffset[T];
-  const bool producer = threadIdx.x >= kRingCompute;     // the two producer warps
-  const bool lead = threadIdx.x == kRingCompute;         // issues the copies
-  const bool waiter = threadIdx.x == kRingCompute + 32;  // waits for the next level
+  const bool lead = threadIdx.x == kRingLevelSync;  // the producer warp's issuing lane
+  const volatile int* abortV = &abortFlag;
 
   if (lead) {
     abortFlag = 0;
-    for (int i = 0; i <= kRingBarriers; ++i) mbarInit(smemAddr(bars + i), 1);
+    consumedLevels = L;
+    for (int i = 0; i < kRingBarriers; ++i) {
+      mbarInit(smemAddr(full + i), 1);
+      mbarInit(smemAddr(empty + i), 1);
+    }
+    mbarInit(smemAddr(tableBar), 1);
     fenceBarrierInit();
-    const uint32_t tb = static_cast<uint32_t>(L) * 32u;
-    mbarExpectTx(smemAddr(bars + kRingBarriers), tb);
-    bulkLoad(smemAddr(mt), meta + 2 * static_cast<size_t>(lv0), tb, smemAddr(bars + kRingBarriers));
+    const uint32_t tb = static_cast<uint32_t>(L) * 16u;
+    mbarExpectTx(smemAddr(tableBar), tb);
+    bulkLoad(smemAddr(mt), meta + static_cast<size_t>(lv0), tb, smemAddr(tableBar));
   }
-  // Prologue into the tile's slice of x while the level table lands; the
+  // Prologue into the block's slice of x while the level table lands; the
   // slot after the slice is the zero that padding entries read.
   {
     W beta = W(0), omega = W(0), alpha = W(0);
@@ -144,95 +171,106 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
     for (int i = threadIdx.x; i < nRows; i += blockDim.x) xs[i] = pro(base + i, beta, omega, alpha, first);
     if (lead) xs[nRows] = W(0);
   }
-  // The issuing lane copies levels in order: `next` is the next level to
-  // copy (its table entries held in na / nia), `src` its byte offset in the
-  // block's stream, `pf` the L2 prefetch frontier.
-  int next = 0, nia = 0;
-  int4 na = make_int4(0, 0, 0, 0);
-  uint32_t src = 0, pf = 0;
-  const uint32_t tileBytes = static_cast<uint32_t>(tileOffset[T + 1] - tileOffset[T]);
-  auto issueUpTo = [&](int consumed) {
-    while (next < L && nia <= consumed) {
-      const uint32_t bar = smemAddr(bars + (next % kRingBarriers));
-      mbarExpectTx(bar, static_cast<uint32_t>(na.z));
-      bulkLoad(smemAddr(ring + na.w), g + src, static_cast<uint32_t>(na.z), bar);
-      src += static_cast<uint32_t>(na.z);
-      if (++next < L) {
-        na = mt[2 * next];
-        nia = mt[2 * next + 1].z;
+  __syncthreads();  // barriers initialised, x slice written
+
+  int issued = 0;  // producer: levels whose copies were issued
+  if (threadIdx.x >= kRingLevelSync) {
+    // Producer: copies the levels in order, level j once level
+    // issueAfter(j) has been released on its empty barrier (after the
+    // barrier that ended it, so every read of it is done). It runs ahead of
+    // the compute warps by as much as the ring allows and takes no part in
+    // their per-level barrier.
+    if (lead) {
+      if (!mbarWaitBounded(smemAddr(tableBar), 0, abortV)) {
+        abortFlag = 1;
+      } else {
+        uint32_t src = 0, pf = 0;
+        const uint32_t tileBytes = static_cast<uint32_t>(tileOffset[T + 1] - tileOffset[T]);
+        for (; issued < L && !*abortV; ++issued) {
+          const int4 m = mt[issued];
+          const int ia = m.w;
+          if (ia >= 0 && !mbarWaitBounded(smemAddr(empty + ia % kRingBarriers), (ia / kRingBarriers) & 1, abortV)) {
+            abortFlag = 1;
+            break;
+          }
+          const bool up = (m.y & kRingUpperBit) != 0;
+          const uint32_t bytes =
+              ringLevelLayout(static_cast<uint32_t>(m.x), static_cast<uint32_t>(m.y & (kRingUpperBit - 1)), up || dilu,
+                              sizeof(MV))
+                  .bytes;
+          const uint32_t bar = smemAddr(full + issued % kRingBarriers);
+          mbarExpectTx(bar, bytes);
+          bulkLoad(smemAddr(ring + m.z), g + src, bytes, bar);
+          src += bytes;
+          if (pf < src) pf = src;
+          const uint32_t until = min(tileBytes, src + l2Ahead);
+          if (pf < until) {
+            prefetchL2(g + pf, until - pf);
+            pf = until;
+          }
+        }
       }
     }
-    if (pf < src) pf = src;
-    const uint32_t until = min(tileBytes, src + l2Ahead);
-    if (pf < until) {
-      prefetchL2(g + pf, until - pf);
-      pf = until;
+  } else if (threadIdx.x >= kRingCompute) {
+    // Waiting warp: before the barrier that ends level l it waits until
+    // level l + 1 has landed (so the barrier also publishes the copy to the
+    // compute warps); after it, it releases level l.
+    bool ok = mbarWaitBounded(smemAddr(tableBar), 0, abortV) &&
+              (L == 0 || mbarWaitBounded(smemAddr(full), 0, abortV));
+    if (!ok) abortFlag = 1;
+    bool stop = namedBarOr(1, kRingLevelSync, !ok);
+    if (stop && threadIdx.x == kRingCompute) consumedLevels = 0;
+    for (int l = 0; !stop && l < L; ++l) {
+      bool bad = false;
+      if (l + 1 < L && !mbarWaitBounded(smemAddr(full + (l + 1) % kRingBarriers), ((l + 1) / kRingBarriers) & 1, abortV)) {
+        abortFlag = 1;
+        bad = true;
+      }
+      stop = namedBarOr(1, kRingLevelSync, bad || *abortV != 0);
+      if (threadIdx.x == kRingCompute) {
+        mbarArrive(smemAddr(empty + l % kRingBarriers));
+        if (stop) consumedLevels = l + 1;
+      }
     }
-  };
-  bool tableLanded = false;
-  if (lead) {
-    if (!waitBar(smemAddr(bars + kRingBarriers), 0)) {
-      abortFlag = 1;
-    } else {
-      tableLanded = true;
-      na = mt[0];
-      nia = mt[1].z;
-      issueUpTo(-1);
-      if (L > 0 && !waitBar(smemAddr(bars), 0)) abortFlag = 1;
+  } else {
+    // Compute warps: level l, whose block the waiting warp saw land before
+    // the previous barrier.
+    bool stop = namedBarOr(1, kRingLevelSync, false);
+    for (int l = 0; !stop && l < L; ++l) {
+      const RingLevel<MV> cur = ringLevelAt<MV>(mt[l], ring, dilu);
+      const unsigned char* ents = cur.blk + cur.ents;
+      const uint32_t stride = kEnt * static_cast<uint32_t>(cur.k);
+      const MV* inv = reinterpret_cast<const MV*>(cur.blk + cur.inv);
+      const int* rows = reinterpret_cast<const int*>(cur.blk);
+      if (!cur.upper) {
+        // Forward substitution (ilu/Solver.cpp:380-411).
+        for (int q = threadIdx.x; q < cur.k; q += kRingCompute) {
+          const int il = rows[q];
+          const W temp = ringRowDot<MV, UNROLL>(xs[il], ents + kEnt * q, stride, cur.E, nRows, xs);
+          xs[il] = dilu ? mul(temp, cvt<W>(inv[q])) : temp;
+        }
+      } else {
+        // Backward substitution (ilu/Solver.cpp:413-442).
+        for (int q = threadIdx.x; q < cur.k; q += kRingCompute) {
+          const int il = rows[q];
+          const W temp = ringRowDot<MV, UNROLL>(W(0), ents + kEnt * q, stride, cur.E, nRows, xs);
+          const W iv = cvt<W>(inv[q]);
+          xs[il] = dilu ? add(xs[il], mul(temp, iv)) : mul(add(xs[il], temp), iv);
+        }
+      }
+      stop = namedBarOr(1, kRingLevelSync, *abortV != 0);
     }
   }
   __syncthreads();
-  int consumed = -1;  // last level every thread finished
-  if (!abortFlag) {
-    for (int l = 0; l < L; ++l) {
-      if (producer) {
-        // Copies released by level l - 1 (finished by every thread before
-        // the previous barrier); meanwhile the waiting warp waits until level
-        // l + 1 has landed.
-        if (lead && l > 0 && next < L) {
-          fenceProxyAsync();
-          issueUpTo(l - 1);
-        }
-        if (waiter && l + 1 < L &&
-            !waitBar(smemAddr(bars + ((l + 1) % kRingBarriers)), ((l + 1) / kRingBarriers) & 1))
-          abortFlag = 1;
-      } else {
-        const int4 a = mt[2 * l], b = mt[2 * l + 1];
-        const int k = a.x, E = a.y;
-        const unsigned char* blk = ring + a.w;
-        const int* rows = reinterpret_cast<const int*>(blk);
-        const MV* inv = reinterpret_cast<const MV*>(blk + b.x);
-        const unsigned char* ents = blk + b.y;
-        const uint32_t stride = kEnt * static_cast<uint32_t>(k);
-        if (!b.w) {
-          // Forward substitution (ilu/Solver.cpp:380-411).
-          for (int q = threadIdx.x; q < k; q += kRingCompute) {
-            const int il = rows[q];
-            const W temp = ringRowDot<MV, UNROLL>(xs[il], ents + kEnt * q, stride, E, nRows, xs);
-            xs[il] = dilu ? mul(temp, cvt<W>(inv[q])) : temp;
-          }
-        } else {
-          // Backward substitution (ilu/Solver.cpp:413-442).
-          for (int q = threadIdx.x; q < k; q += kRingCompute) {
-            const int il = rows[q];
-            const W temp = ringRowDot<MV, UNROLL>(W(0), ents + kEnt * q, stride, E, nRows, xs);
-            const W iv = cvt<W>(inv[q]);
-            xs[il] = dilu ? add(xs[il], mul(temp, iv)) : mul(add(xs[il], temp), iv);
-          }
-        }
-      }
-      __syncthreads();
-      consumed = l;
-      if (abortFlag) break;
-    }
-  }
   if (abortFlag) {
     if (lead) {
       atomicExch(errFlag, GR_ETIMEOUT);
       // Let the copies already issued land before the block's shared memory
-      // is released (bounded).
-      if (!tableLanded) waitBar(smemAddr(bars + kRingBarriers), 0);
-      for (int j = consumed + 1; j < next; ++j) waitBar(smemAddr(bars + (j % kRingBarriers)), (j / kRingBarriers) & 1);
+      // is released (bounded). Each barrier has at most one such copy: level
+      // j + kRingBarriers is issued only after level j was consumed.
+      mbarWaitBounded(smemAddr(tableBar), 0);
+      for (int j = consumedLevels; j < issued; ++j)
+        mbarWaitBounded(smemAddr(full + j % kRingBarriers), (j / kRingBarriers) & 1);
     }
     return;
   }
@@ -244,8 +282,8 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
 // ---------------------------------------------------------------------------
 size_t iluRingSmem(const DeviceMatrix& A, const LevelRing& R, DType W) {
   (void)A;
-  return 256 + 32 * static_cast<size_t>(R.maxTileLevels) + static_cast<size_t>(R.ringBytes) +
-         static_cast<size_t>(R.maxGroupRows + 1) * dtypeSize(W);
+  return static_cast<size_t>(ringFixedSmem(R.maxTileLevels, R.maxGroupRows, static_cast<i64>(dtypeSize(W))) +
+                             R.ringBytes);
 }
 
 void launchRingPack(DeviceMatrix& A, const LevelRing& R, void* stream, const void* F, const void* inv,
@@ -261,6 +299,7 @@ void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool di
   const size_t smem = iluRingSmem(A, R, dtypeOf<W>());
   auto kernel = unroll ? dev::iluRingKernel<MV, W, true> : dev::iluRingKernel<MV, W, false>;
   ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
+  preferSharedCarveout(reinterpret_cast<const void*>(kernel));
   if (p.stIndex && R.group != 1) fail(GR_EUNSUPPORTED, "batched solves run one tile per block");
   dev::SPro<W> pro{static_cast<int>(p.kind), static_cast<const W*>(p.b), static_cast<const W*>(p.r),
                    static_cast<W*>(p.pOrS), static_cast<const W*>(p.v), p.st, p.stIndex};

@@ -393,7 +393,8 @@ struct TileRing {
 inline bool overlaps(i64 a, i64 sa, i64 b, i64 sb) { return a < b + sb && b < a + sa; }
 }  // namespace
 
-HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes, i32 group) {
+HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes, i32 group,
+                        const RingBudget& budget) {
   const i64 vs = static_cast<i64>(dtypeSize(vt));
   const i64 entSize = vs == 4 ? 8 : 16;
   if (group < 1) fail(GR_EINVAL, "tiles per block must be at least 1");
@@ -448,8 +449,8 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
             if (real) t.vals.emplace_back(pos + (vs == 4 ? 4 : 8), static_cast<i32>(ent[e]));
           }
         }
-        t.meta.push_back(make_int4(static_cast<int>(k), static_cast<int>(E), static_cast<int>(S), 0));
-        t.meta.push_back(make_int4(static_cast<int>(rowsB), static_cast<int>(rowsB + invB), -1, upper ? 1 : 0));
+        if (E >= kRingUpperBit || k >= (i64(1) << 31)) fail(GR_EUNSUPPORTED, "ILU level too large for the ring kernel");
+        t.meta.push_back(make_int4(static_cast<int>(k), static_cast<int>(E) | (upper ? kRingUpperBit : 0), 0, -1));
         t.size.push_back(S);
         t.maxLevel = std::max(t.maxLevel, S);
       }
@@ -457,46 +458,98 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
   });
   HostRing R;
   for (const TileRing& t : tr) R.maxLevelBytes = std::max(R.maxLevelBytes, t.maxLevel);
-  // Ring placement: levels one after another, wrapping to the start when a
-  // level does not fit before the end; a level's copy waits for the most
-  // recent earlier level whose block it overlaps, and for the level that
-  // last used its completion barrier. Placement fails when some level would
-  // have to wait for the level right before it.
+  // Ring placement. Level l goes to the offset, among the ring's two ends and
+  // the ends and starts of the levels of the last kRingBarriers, whose copy
+  // can be issued earliest: after the most recent earlier level whose block
+  // it overlaps, the level that last used its completion barrier, and the
+  // previous level's copy. Offsets that leave level l + 1 a place beside it
+  // (at either end of the ring or right after it) come first, so that any
+  // ring of at least two of the largest levels places. Ties go to the offset
+  // right after level l - 1, then to the one found first. Placement fails
+  // when some level would have to wait for the level right before it.
   auto place = [&](i64 ring) {
     std::atomic<bool> ok{true};
     parallelFor(NG, [&](i64 T) {
       TileRing& t = tr[T];
       const i64 L = static_cast<i64>(t.size.size());
       std::vector<i64> off(L);
-      i64 pos = 0, prevIa = -1;
+      i64 prevIa = -1;
       for (i64 l = 0; l < L && ok; ++l) {
         const i64 S = t.size[l];
         if (S > ring) { ok = false; return; }
-        if (pos + S > ring) pos = 0;
-        off[l] = pos;
-        pos += S;
-        i64 ia = -1;
-        for (i64 j = l - 1; j >= 0; --j)
-          if (overlaps(off[j], t.size[j], off[l], S)) { ia = j; break; }
-        ia = std::max({ia, l - kRingBarriers, prevIa});
-        if (l >= 1 && ia > l - 2) { ok = false; return; }
-        t.meta[2 * l].w = static_cast<int>(off[l]);
-        t.meta[2 * l + 1].z = static_cast<int>(ia);
-        prevIa = ia;
+        const i64 floorIa = std::max<i64>(prevIa, l - kRingBarriers);
+        // issueAfter for offset c: the most recent overlapping level above
+        // floorIa, else floorIa.
+        auto issueAfter = [&](i64 c) {
+          for (i64 j = l - 1; j > floorIa; --j)
+            if (overlaps(off[j], t.size[j], c, S)) return j;
+          return floorIa;
+        };
+        const i64 Sn = l + 1 < L ? t.size[l + 1] : 0;
+        i64 best = -1, bestIa = 0;
+        bool bestRoom = false;
+        auto consider = [&](i64 c) {
+          if (c < 0 || c + S > ring || c % 16 != 0) return;
+          const i64 ia = issueAfter(c);
+          const bool room = Sn == 0 || c >= Sn || c + S + Sn <= ring;
+          if (best < 0 || (room && !bestRoom) || (room == bestRoom && ia < bestIa)) {
+            best = c;
+            bestIa = ia;
+            bestRoom = room;
+          }
+        };
+        if (l > 0) consider(off[l - 1] + t.size[l - 1]);
+        consider(0);
+        consider((ring - S) / 16 * 16);
+        for (i64 j = l - 1; j >= 0 && j >= l - kRingBarriers; --j) {
+          consider(off[j] + t.size[j]);
+          consider(off[j] - S);
+        }
+        if (best < 0 || (l >= 1 && bestIa > l - 2)) { ok = false; return; }
+        off[l] = best;
+        t.meta[l].z = static_cast<int>(best);
+        t.meta[l].w = static_cast<int>(bestIa);
+        prevIa = bestIa;
       }
     });
     return ok.load();
   };
+  i64 maxGroupRows = 0;
+  for (i32 G = 0; G < NG; ++G)
+    maxGroupRows = std::max<i64>(maxGroupRows, H.tileStart[std::min<i32>(H.P, (G + 1) * group)] - H.tileStart[G * group]);
+  i32 maxLevels = 0;
+  for (const TileRing& t : tr) maxLevels = std::max<i32>(maxLevels, static_cast<i32>(t.size.size()));
   if (ringBytes > 0) {
     R.ringBytes = pad16(ringBytes);
     if (!place(R.ringBytes))
       fail(GR_EINVAL, "ILU level ring of " + std::to_string(R.ringBytes) + " bytes is too small for this matrix's levels");
   } else {
-    // Default: the smallest ring from max(16 KB, 2.5 x the largest level) up,
-    // in steps of half a level, that the placement accepts (3 x always does).
-    const i64 step = std::max<i64>(16, pad16(R.maxLevelBytes / 2));
-    R.ringBytes = std::max<i64>(16384, pad16(2 * R.maxLevelBytes + R.maxLevelBytes / 2));
-    while (!place(R.ringBytes)) R.ringBytes += step;
+    // Default: among the ring sizes from twice the largest level up to
+    // max(16 KB, 4 x the largest level), in steps of 256 bytes (or 1/16 of
+    // the largest level), one that places and runs all blocks in the fewest
+    // waves (blocks resident per SM from the budget); the largest such, as a
+    // larger ring lets copies run further ahead.
+    const i64 fixed = ringFixedSmem(maxLevels, maxGroupRows, vs) + budget.reservedPerBlock;
+    const i64 lo = std::max<i64>(256, pad16(2 * R.maxLevelBytes));
+    const i64 hi = std::max<i64>(std::max<i64>(16384, pad16(4 * R.maxLevelBytes)), lo);
+    const i64 step = std::max<i64>(256, pad16(R.maxLevelBytes / 16));
+    i64 bestRing = -1, bestWaves = 0;
+    auto consider = [&](i64 r) {
+      if (!place(r)) return;
+      const i64 perSM = std::min<i64>(budget.maxBlocksPerSM, budget.smemPerSM / (fixed + r));
+      const i64 slots = std::max<i64>(1, perSM) * std::max<i32>(1, budget.numSMs);
+      const i64 waves = perSM > 0 ? (NG + slots - 1) / slots : (i64(1) << 40);
+      if (bestRing < 0 || waves <= bestWaves) {
+        bestRing = r;
+        bestWaves = waves;
+      }
+    };
+    for (i64 r = lo; r < hi; r += step) consider(r);
+    consider(hi);
+    for (i64 r = hi + step; bestRing < 0 && r < (i64(1) << 30); r += step) consider(r);
+    if (bestRing < 0) fail(GR_EUNSUPPORTED, "ILU level ring too large");
+    R.ringBytes = bestRing;
+    if (!place(R.ringBytes)) fail(GR_EINVAL, "ILU level ring placement");
   }
   if (R.ringBytes >= (i64(1) << 30)) fail(GR_EUNSUPPORTED, "ILU level ring too large");
   R.group = group;
@@ -516,7 +569,7 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
   const i64 total = R.tileOffset[NG];
   if (total / vs >= (i64(1) << 31)) fail(GR_EUNSUPPORTED, "ILU level ring stream exceeds 2^31 elements");
   R.bytes.resize(total);
-  R.meta.resize(2 * static_cast<size_t>(R.tileLevel[NG]));
+  R.meta.resize(static_cast<size_t>(R.tileLevel[NG]));
   R.valPos.resize(nVal);
   R.valSrc.resize(nVal);
   R.invPos.resize(nInv);
@@ -529,7 +582,7 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
   parallelFor(NG, [&](i64 T) {
     const i64 off = R.tileOffset[T];
     std::memcpy(R.bytes.data() + off, tr[T].bytes.data(), tr[T].bytes.size());
-    std::copy(tr[T].meta.begin(), tr[T].meta.end(), R.meta.begin() + 2 * static_cast<size_t>(R.tileLevel[T]));
+    std::copy(tr[T].meta.begin(), tr[T].meta.end(), R.meta.begin() + static_cast<size_t>(R.tileLevel[T]));
     for (size_t i = 0; i < tr[T].vals.size(); ++i) {
       R.valPos[vOff[T] + i] = static_cast<i32>((off + tr[T].vals[i].first) / vs);
       R.valSrc[vOff[T] + i] = tr[T].vals[i].second;
@@ -570,14 +623,18 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
     std::vector<i64> ringOff(L), size(L);
     i64 src = R.tileOffset[G], prevIa = -1;
     for (i64 l = 0; l < L; ++l) {
-      const int4 a = R.meta[2 * (R.tileLevel[G] + l)], b = R.meta[2 * (R.tileLevel[G] + l) + 1];
-      const i64 k = a.x, E = a.y, S = a.z, off = a.w, ia = b.z;
-      const bool upper = b.w != 0;
+      const int4 a = R.meta[R.tileLevel[G] + l];
+      const i64 k = a.x, E = a.y & (kRingUpperBit - 1), off = a.z, ia = a.w;
+      const bool upper = (a.y & kRingUpperBit) != 0;
       if (upper != (l >= nLower)) bad(G, l, "sweep flag");
       const bool hasInv = upper || dilu;
       const i64 rowsB = pad16(4 * k), invB = hasInv ? pad16(vs * k) : 0;
-      if (k < 1 || E < 0 || b.x != rowsB || b.y != rowsB + invB || S != rowsB + invB + pad16(entSize * E * k))
-        bad(G, l, "block layout");
+      const i64 S = rowsB + invB + pad16(entSize * E * k);
+      if (k < 1 || E < 0 || S > R.ringBytes) bad(G, l, "block layout");
+      const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(k), static_cast<uint32_t>(E), hasInv,
+                                                  static_cast<uint32_t>(vs));
+      if (lay.inv != rowsB || lay.ents != rowsB + invB || lay.bytes != S) bad(G, l, "block layout");
+      const i64 entOff = rowsB + invB;
       if (off < 0 || off % 16 != 0 || off + S > R.ringBytes) bad(G, l, "ring offset");
       if (ia < -1 || ia < prevIa || ia < l - kRingBarriers || (l >= 1 && ia > l - 2) || (l == 0 && ia != -1))
         bad(G, l, "copy order");
@@ -597,7 +654,7 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
         rows[q] = il;
         for (i64 e = 0; e < E; ++e) {
           i32 c;
-          std::memcpy(&c, blk + b.y + entSize * (e * k + q), 4);
+          std::memcpy(&c, blk + entOff + entSize * (e * k + q), 4);
           if (c < 0 || c > gRows) bad(G, l, "column index");
           if (c < gRows && (tileOf[c] != tileOf[il] || !done[c] || (upper ? c <= il : c >= il)))
             bad(G, l, "dependency order");
@@ -617,7 +674,15 @@ LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group) {
   auto key = std::make_tuple(dilu, ringBytes, group);
   auto it = levelRings.find(key);
   if (it != levelRings.end()) return *it->second;
-  HostRing H = buildLevelRing(*host, dilu, vt, ringBytes, group);
+  RingBudget budget;
+  budget.numSMs = numSMs;
+  int dev = 0, v = 0;
+  GR_CUDA(cudaGetDevice(&dev));
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess && v > 0)
+    budget.smemPerSM = v;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess)
+    budget.reservedPerBlock = v;
+  HostRing H = buildLevelRing(*host, dilu, vt, ringBytes, group, budget);
   auto R = std::make_unique<LevelRing>();
   R->dilu = dilu;
   R->bytes = static_cast<i64>(H.bytes.size());

@@ -74,7 +74,7 @@ def check_ring(h, dilu, vt=gb.FLOAT32, ring_bytes=0, group=1):
 def test_ring_replay(dims, tiles, part, dilu, vt, group):
     h = gb.generate3DPoissonMatrix(vt, *dims, tiles, part)
     used, nbytes, lv = check_ring(h, dilu, vt, 0, group)
-    assert used >= 16384 and used % 16 == 0 and nbytes % 16 == 0 and lv >= 2
+    assert used > 0 and used % 16 == 0 and nbytes % 16 == 0 and lv >= 2
 
 
 @pytest.mark.parametrize("seed", [0, 1, 2])
