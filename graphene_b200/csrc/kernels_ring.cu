@@ -168,7 +168,14 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
       alpha = cvt<W>(st->alpha);
       first = st->iter == 0;
     }
-    for (int i = threadIdx.x; i < nRows; i += blockDim.x) xs[i] = pro(base + i, beta, omega, alpha, first);
+    const int bd = static_cast<int>(blockDim.x);
+    for (int i0 = threadIdx.x; i0 < nRows; i0 += 4 * bd) {
+      W v4[4];
+      pro.four(base + i0, bd, base + nRows, beta, omega, alpha, first, v4);
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (i0 + j * bd < nRows) xs[i0 + j * bd] = v4[j];
+    }
     if (lead) xs[nRows] = W(0);
   }
   __syncthreads();  // barriers initialised, x slice written
@@ -312,6 +319,17 @@ void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool di
   checkLaunch("ilu_ring");
 }
 }  // namespace
+
+int ringBlocksPerSMWithoutSmem(DType vt) {
+  int n = 0;
+  const void* fn = vt == DType::F64 ? reinterpret_cast<const void*>(dev::iluRingKernel<double, double, true>)
+                                    : reinterpret_cast<const void*>(dev::iluRingKernel<float, float, true>);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, dev::kRingThreads, 0) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
 
 void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,
                    void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s) {

@@ -81,6 +81,9 @@ void launchPackBytes(DeviceMatrix& A, const void* templ, i64 bytes, const int* v
                      cudaStream_t s);
 // Host-scheduled ring substitution (kernels_ring.cu): dynamic shared memory
 // per block, packing of a solver's copy of the level blocks, and the launch.
+// Blocks of the ring kernel (value type vt) an SM holds when shared memory
+// is not the limit (0 if unknown).
+int ringBlocksPerSMWithoutSmem(DType vt);
 size_t iluRingSmem(const DeviceMatrix& A, const LevelRing& R, DType W);
 void launchRingPack(DeviceMatrix& A, const LevelRing& R, void* stream, const void* F, const void* inv,
                     cudaStream_t s);

@@ -11,6 +11,7 @@
 #include <cstring>
 
 #include "device.hpp"
+#include "krylov.hpp"
 
 namespace gr {
 
@@ -682,6 +683,7 @@ LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group) {
     budget.smemPerSM = v;
   if (cudaDeviceGetAttribute(&v, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess)
     budget.reservedPerBlock = v;
+  if (const int b = ringBlocksPerSMWithoutSmem(vt); b > 0) budget.maxBlocksPerSM = b;
   HostRing H = buildLevelRing(*host, dilu, vt, ringBytes, group, budget);
   auto R = std::make_unique<LevelRing>();
   R->dilu = dilu;
