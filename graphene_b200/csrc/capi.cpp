@@ -309,12 +309,13 @@ int gr_host_matrix_check_ilu_stream(const gr_host_matrix* h, int dilu, gr_dtype 
 }
 
 int gr_host_matrix_check_ilu_ring(const gr_host_matrix* h, int dilu, gr_dtype value_type, int64_t ring_bytes,
-                                  int32_t tiles_per_block, int64_t* ring_bytes_used, int64_t* stream_bytes,
-                                  int32_t* max_tile_levels) {
+                                  int32_t tiles_per_block, int32_t allow_compact, int64_t* ring_bytes_used,
+                                  int64_t* stream_bytes, int32_t* max_tile_levels) {
   return guarded([&] {
     need(h, "matrix");
     const gr::DType vt = gr::toDType(value_type);
-    gr::HostRing R = gr::buildLevelRing(*h->m, dilu != 0, vt, ring_bytes, tiles_per_block);
+    gr::HostRing R =
+        gr::buildLevelRing(*h->m, dilu != 0, vt, ring_bytes, tiles_per_block, gr::RingBudget{}, allow_compact != 0);
     gr::checkLevelRing(*h->m, R, dilu != 0, vt);
     if (ring_bytes_used) *ring_bytes_used = R.ringBytes;
     if (stream_bytes) *stream_bytes = static_cast<int64_t>(R.bytes.size());

@@ -36,9 +36,9 @@ class DBuf {
   ~DBuf() { release(); }
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
-  DBuf(DBuf&& o) noexcept : p_(o.p_), bytes_(o.bytes_) { o.p_ = nullptr; o.bytes_ = 0; }
+  DBuf(DBuf&& o) noexcept : p_(o.p_), bytes_(o.bytes_), dev_(o.dev_) { o.p_ = nullptr; o.bytes_ = 0; }
   DBuf& operator=(DBuf&& o) noexcept {
-    if (this != &o) { release(); p_ = o.p_; bytes_ = o.bytes_; o.p_ = nullptr; o.bytes_ = 0; }
+    if (this != &o) { release(); p_ = o.p_; bytes_ = o.bytes_; dev_ = o.dev_; o.p_ = nullptr; o.bytes_ = 0; }
     return *this;
   }
   void alloc(size_t bytes);
@@ -55,6 +55,7 @@ class DBuf {
  private:
   void* p_ = nullptr;
   size_t bytes_ = 0;
+  int dev_ = 0;
 };
 
 // Values converted to the stored coefficient type (float or double).
@@ -147,32 +148,47 @@ void checkIluStream(const HostMatrix& H, const HostStream& S, bool dilu, DType v
 
 // Level blocks for the host-scheduled ring kernel (kernels_ring.cu). Per
 // tile, the levels in execution order (lower ascending, then upper
-// descending); a level block is
-//   rows  k x i32 tile-local row ids                            (16-byte padded)
-//   inv   k x value type inverse diagonal (upper levels, DILU)  (padded)
+// descending). A level block (every segment 16-byte padded) is, in the
+// compact layout (blocks of at most 65535 rows):
+//   rows  k x u16 block-local row ids
+//   inv   k x value type inverse diagonal (upper levels, DILU)
+//   cols  E*k x u16 columns, entry-major
+//   vals  E*k x value type, entry-major
+// and otherwise (the wide layout):
+//   rows  k x i32
+//   inv   k x value type (upper levels, DILU)
 //   ents  E*k entries, entry-major, {i32 column, value}: 8 bytes for float,
-//         16 for double ({column, 0, value})                    (padded)
+//         16 for double ({column, 0, value})
 // Padding entries use column nRows (a zero slot of the kernel's x slice) and
 // value 0. One int4 per level: {k, E | upper << 30, ring offset,
-// issueAfter}; the block's segment offsets and size follow from k, E, upper
-// and DILU (ringLevelLayout). The kernel copies a level's block into its
-// shared-memory ring at `ring offset` once the tile's level `issueAfter` has
-// been consumed (-1: at the start); the host chose the offsets so that a
-// copy never overwrites a level still to be consumed, and so that every
-// level is copied at least one level before it is needed.
+// issueAfter}; the block's segment offsets and size follow from k, E, upper,
+// DILU and the layout (ringLevelLayout). The kernel copies a level's block
+// into its shared-memory ring at `ring offset` once the tile's level
+// `issueAfter` has been consumed (-1: at the start); the host chose the
+// offsets so that a copy never overwrites a level still to be consumed, and
+// so that every level is copied at least one level before it is needed.
 constexpr int kRingBarriers = 16;
 constexpr int kRingUpperBit = 1 << 30;
+constexpr long long kRingCompactRows = 65535;  // largest block (rows + zero slot) of the compact layout
 
-// Byte offsets of a level block's inverse diagonal and entries, and its size.
+// Byte offsets of a level block's inverse diagonal, entries (columns, or
+// column/value pairs) and values, and its size.
 struct RingLevelLayout {
-  uint32_t inv, ents, bytes;
+  uint32_t inv, ents, vals, bytes;
 };
-__host__ __device__ inline RingLevelLayout ringLevelLayout(uint32_t k, uint32_t E, bool hasInv, uint32_t valueBytes) {
-  const uint32_t entBytes = valueBytes == 4 ? 8u : 16u;
-  const uint32_t rowsB = (4u * k + 15u) & ~15u;
+__host__ __device__ inline RingLevelLayout ringLevelLayout(uint32_t k, uint32_t E, bool hasInv, uint32_t valueBytes,
+                                                           bool compact) {
+  const uint32_t idB = compact ? 2u : 4u;
+  const uint32_t rowsB = (idB * k + 15u) & ~15u;
   const uint32_t invB = hasInv ? ((valueBytes * k + 15u) & ~15u) : 0u;
+  if (compact) {
+    const uint32_t colsB = (2u * E * k + 15u) & ~15u;
+    const uint32_t valsB = (valueBytes * E * k + 15u) & ~15u;
+    return RingLevelLayout{rowsB, rowsB + invB, rowsB + invB + colsB, rowsB + invB + colsB + valsB};
+  }
+  const uint32_t entBytes = valueBytes == 4 ? 8u : 16u;
   const uint32_t entB = (entBytes * E * k + 15u) & ~15u;
-  return RingLevelLayout{rowsB, rowsB + invB, rowsB + invB + entB};
+  return RingLevelLayout{rowsB, rowsB + invB, rowsB + invB, rowsB + invB + entB};
 }
 
 // What the default ring size is chosen for: the SM count, shared memory per
@@ -195,6 +211,7 @@ struct HostRing {
   i64 ringBytes = 0, maxLevelBytes = 0, maxGroupRows = 0;
   i32 maxTileLevels = 0;
   i32 group = 1;                // tiles per thread block
+  bool compact = false;         // 16-bit row and column ids
   std::vector<i32> groupStart;  // first tile-order row of every block, and n
 };
 // Shared memory of one ring-kernel block besides the ring: barriers, the
@@ -207,8 +224,10 @@ inline i64 ringFixedSmem(i32 maxTileLevels, i64 maxGroupRows, i64 vectorBytes) {
 }
 // One thread block runs `group` consecutive tiles in lockstep (tileOffset,
 // tileLevel and meta are then per block). ringBytes 0: the default (RingBudget).
+// The compact layout is used when every block has at most kRingCompactRows
+// rows and `allowCompact`.
 HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes, i32 group,
-                        const RingBudget& budget = RingBudget{});
+                        const RingBudget& budget = RingBudget{}, bool allowCompact = false);
 // Replays the kernel's copies and reads on the host; throws GR_EINVAL on an
 // out-of-range index, a dependency-order violation, a copy that would
 // overwrite a level not yet consumed, or a copy issued too late.
@@ -217,6 +236,7 @@ struct LevelRing {
   bool dilu = false;
   i64 bytes = 0, ringBytes = 0, nVal = 0, nInv = 0, maxGroupRows = 0;
   i32 maxTileLevels = 0, group = 1, numGroups = 0;
+  bool compact = false;
   DBuf tileOffset, templ, meta, tileLevel, groupStart, valPos, valSrc, invPos, invSrc;
 };
 
@@ -280,8 +300,8 @@ struct DeviceMatrix {
   std::unique_ptr<LevelSchedule> lowerSched, upperSched, gsSched;
   std::unique_ptr<SweepStream> iluStream[2];  // [dilu]
   SweepStream& iluSweepStream(bool dilu);
-  std::map<std::tuple<bool, i64, i32>, std::unique_ptr<LevelRing>> levelRings;  // [(dilu, ring bytes, group)]
-  LevelRing& levelRing(bool dilu, i64 ringBytes, i32 group);
+  std::map<std::tuple<bool, i64, i32, bool>, std::unique_ptr<LevelRing>> levelRings;  // [(dilu, ring bytes, group, compact allowed)]
+  LevelRing& levelRing(bool dilu, i64 ringBytes, i32 group, bool allowCompact = false);
 
   // Device error word written by kernels whose bounded waits ran out
   // (GR_ETIMEOUT); 0 when clean.

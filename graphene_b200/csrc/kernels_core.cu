@@ -85,12 +85,70 @@ void preferSharedCarveout(const void* fn) {
   GR_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
 }
 
+namespace {
+// Device blocks released by DBufs, kept for reuse (by device and size, up to
+// kBlockCacheBytes in all). A solver's setup then takes its buffers from here
+// rather than from the stream-ordered allocator, whose requests for memory it
+// had to grow for took up to a quarter of a second on B200. Every owner
+// synchronises the buffer's stream before releasing it, so a cached block has
+// no work pending.
+struct BlockCache {
+  std::mutex mu;
+  std::multimap<std::pair<int, size_t>, void*> blocks;
+  size_t bytes = 0;
+};
+BlockCache& blockCache() {
+  static BlockCache* c = new BlockCache();  // outlives every DBuf
+  return *c;
+}
+constexpr size_t kBlockCacheBytes = size_t(8) << 30;
+
+// Returns every cached block of `dev` to the allocator.
+void trimBlockCache(int dev) {
+  BlockCache& c = blockCache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  for (auto it = c.blocks.begin(); it != c.blocks.end();) {
+    if (it->first.first == dev) {
+      cudaFreeAsync(it->second, cudaStreamPerThread);
+      c.bytes -= it->first.second;
+      it = c.blocks.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  cudaStreamSynchronize(cudaStreamPerThread);
+}
+}  // namespace
+
 void DBuf::alloc(size_t bytes) {
   release();
   if (bytes == 0) bytes = 1;
+  int dev = 0;
+  GR_CUDA(cudaGetDevice(&dev));
+  {
+    // A cached block of this device at most 1/8 larger than asked for.
+    BlockCache& c = blockCache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    auto it = c.blocks.lower_bound({dev, bytes});
+    if (it != c.blocks.end() && it->first.first == dev && it->first.second <= bytes + bytes / 8) {
+      p_ = it->second;
+      bytes_ = it->first.second;
+      dev_ = dev;
+      c.bytes -= bytes_;
+      c.blocks.erase(it);
+      return;
+    }
+  }
   keepPoolMemory();
   cudaError_t e = cudaMallocAsync(&p_, bytes, cudaStreamPerThread);
   if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread);
+  if (e == cudaErrorMemoryAllocation) {
+    // Out of memory: give the cached blocks back and try once more.
+    (void)cudaGetLastError();
+    trimBlockCache(dev);
+    e = cudaMallocAsync(&p_, bytes, cudaStreamPerThread);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread);
+  }
   if (e != cudaSuccess) {
     p_ = nullptr;
     (void)cudaGetLastError();
@@ -98,12 +156,25 @@ void DBuf::alloc(size_t bytes) {
                         cudaGetErrorString(e));
   }
   bytes_ = bytes;
+  dev_ = dev;
 }
 
 // The owner guarantees that no work using the buffer is still pending (it
 // synchronises the stream the buffer was used on before releasing it).
 void DBuf::release() {
-  if (p_) cudaFreeAsync(p_, cudaStreamPerThread);
+  if (!p_) return;
+  {
+    BlockCache& c = blockCache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    if (c.bytes + bytes_ <= kBlockCacheBytes) {
+      c.blocks.insert({{dev_, bytes_}, p_});
+      c.bytes += bytes_;
+      p_ = nullptr;
+      bytes_ = 0;
+      return;
+    }
+  }
+  cudaFreeAsync(p_, cudaStreamPerThread);
   p_ = nullptr;
   bytes_ = 0;
 }

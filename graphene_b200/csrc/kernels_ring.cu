@@ -56,22 +56,57 @@ __device__ __forceinline__ void loadEntry<double>(const unsigned char* p, int& c
   v = __hiloint2double(e.w, e.z);
 }
 
-// temp -= sum_e value_e * xs[column_e] over a row's E entries in order.
+// A level of the ring as the compute warps see it.
+template <class MV, bool COMPACT>
+struct RingLevel {
+  int k, E;
+  bool upper;
+  const unsigned char* blk;  // the level block in the ring
+  uint32_t inv, ents, vals;  // offsets of its inverse diagonal, entries (columns) and values
+  __device__ __forceinline__ int row(int q) const {
+    return COMPACT ? static_cast<int>(reinterpret_cast<const uint16_t*>(blk)[q]) : reinterpret_cast<const int*>(blk)[q];
+  }
+  __device__ __forceinline__ MV invDiag(int q) const { return reinterpret_cast<const MV*>(blk + inv)[q]; }
+  // Entry e of row q.
+  __device__ __forceinline__ void entry(int e, int q, int& c, MV& v) const {
+    const int idx = e * k + q;
+    if (COMPACT) {
+      c = reinterpret_cast<const uint16_t*>(blk + ents)[idx];
+      v = reinterpret_cast<const MV*>(blk + vals)[idx];
+    } else {
+      loadEntry<MV>(blk + ents + (sizeof(MV) == 4 ? 8 : 16) * idx, c, v);
+    }
+  }
+};
+template <class MV, bool COMPACT>
+__device__ __forceinline__ RingLevel<MV, COMPACT> ringLevelAt(const int4 m, const unsigned char* ring, bool dilu) {
+  RingLevel<MV, COMPACT> lv;
+  lv.k = m.x;
+  lv.E = m.y & (kRingUpperBit - 1);
+  lv.upper = (m.y & kRingUpperBit) != 0;
+  const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(lv.k), static_cast<uint32_t>(lv.E),
+                                              lv.upper || dilu, sizeof(MV), COMPACT);
+  lv.blk = ring + m.z;
+  lv.inv = lay.inv;
+  lv.ents = lay.ents;
+  lv.vals = lay.vals;
+  return lv;
+}
+
+// temp -= sum_e value_e * xs[column_e] over row q's E entries in order.
 // Padding entries (column = the zero slot, value 0) leave temp unchanged.
 // Rows of up to four entries load all their entries, then all x values,
 // before the arithmetic.
-template <class MV, bool UNROLL, class W>
-__device__ __forceinline__ W ringRowDot(W temp, const unsigned char* p, uint32_t stride, int E, int zeroSlot,
+template <bool UNROLL, class MV, bool COMPACT, class W>
+__device__ __forceinline__ W ringRowDot(W temp, const RingLevel<MV, COMPACT>& lv, int q, int zeroSlot,
                                         const W* xs) {
-  constexpr uint32_t kEnt = sizeof(MV) == 4 ? 8 : 16;
-  (void)kEnt;
-  if (UNROLL && E <= 4) {
+  if (UNROLL && lv.E <= 4) {
     int c[4];
     MV v[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
-      if (e < E) {
-        loadEntry<MV>(p + e * stride, c[e], v[e]);
+      if (e < lv.E) {
+        lv.entry(e, q, c[e], v[e]);
       } else {
         c[e] = zeroSlot;
         v[e] = MV(0);
@@ -82,41 +117,19 @@ __device__ __forceinline__ W ringRowDot(W temp, const unsigned char* p, uint32_t
     for (int e = 0; e < 4; ++e) xv[e] = xs[c[e]];
 #pragma unroll
     for (int e = 0; e < 4; ++e)
-      if (e < E) temp = sub(temp, mul(cvt<W>(v[e]), xv[e]));
+      if (e < lv.E) temp = sub(temp, mul(cvt<W>(v[e]), xv[e]));
     return temp;
   }
-  for (int e = 0; e < E; ++e, p += stride) {
+  for (int e = 0; e < lv.E; ++e) {
     int c;
     MV v;
-    loadEntry<MV>(p, c, v);
+    lv.entry(e, q, c, v);
     temp = sub(temp, mul(cvt<W>(v), xs[c]));
   }
   return temp;
 }
 
-// A level of the ring as the compute warps see it.
-template <class MV>
-struct RingLevel {
-  int k, E;
-  bool upper;
-  const unsigned char* blk;  // the level block in the ring
-  uint32_t inv, ents;        // offsets of its inverse diagonal and entries
-};
-template <class MV>
-__device__ __forceinline__ RingLevel<MV> ringLevelAt(const int4 m, const unsigned char* ring, bool dilu) {
-  RingLevel<MV> lv;
-  lv.k = m.x;
-  lv.E = m.y & (kRingUpperBit - 1);
-  lv.upper = (m.y & kRingUpperBit) != 0;
-  const RingLevelLayout lay =
-      ringLevelLayout(static_cast<uint32_t>(lv.k), static_cast<uint32_t>(lv.E), lv.upper || dilu, sizeof(MV));
-  lv.blk = ring + m.z;
-  lv.inv = lay.inv;
-  lv.ents = lay.ents;
-  return lv;
-}
-
-template <class MV, class W, bool UNROLL>
+template <class MV, class W, bool UNROLL, bool COMPACT>
 __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned char* __restrict__ stream,
                                                                const long long* __restrict__ tileOffset,
                                                                const int4* __restrict__ meta,
@@ -128,7 +141,6 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
   __shared__ int abortFlag, consumedLevels;
   const KState* st = pro.state();
   if (st && st->done) return;
-  constexpr uint32_t kEnt = sizeof(MV) == 4 ? 8 : 16;
   const int T = blockIdx.x;
   const int base = blockStart[T];
   const int nRows = blockStart[T + 1] - base;
@@ -203,7 +215,7 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
           const bool up = (m.y & kRingUpperBit) != 0;
           const uint32_t bytes =
               ringLevelLayout(static_cast<uint32_t>(m.x), static_cast<uint32_t>(m.y & (kRingUpperBit - 1)), up || dilu,
-                              sizeof(MV))
+                              sizeof(MV), COMPACT)
                   .bytes;
           const uint32_t bar = smemAddr(full + issued % kRingBarriers);
           mbarExpectTx(bar, bytes);
@@ -244,24 +256,20 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
     // the previous barrier.
     bool stop = namedBarOr(1, kRingLevelSync, false);
     for (int l = 0; !stop && l < L; ++l) {
-      const RingLevel<MV> cur = ringLevelAt<MV>(mt[l], ring, dilu);
-      const unsigned char* ents = cur.blk + cur.ents;
-      const uint32_t stride = kEnt * static_cast<uint32_t>(cur.k);
-      const MV* inv = reinterpret_cast<const MV*>(cur.blk + cur.inv);
-      const int* rows = reinterpret_cast<const int*>(cur.blk);
+      const RingLevel<MV, COMPACT> cur = ringLevelAt<MV, COMPACT>(mt[l], ring, dilu);
       if (!cur.upper) {
         // Forward substitution (ilu/Solver.cpp:380-411).
         for (int q = threadIdx.x; q < cur.k; q += kRingCompute) {
-          const int il = rows[q];
-          const W temp = ringRowDot<MV, UNROLL>(xs[il], ents + kEnt * q, stride, cur.E, nRows, xs);
-          xs[il] = dilu ? mul(temp, cvt<W>(inv[q])) : temp;
+          const int il = cur.row(q);
+          const W temp = ringRowDot<UNROLL>(xs[il], cur, q, nRows, xs);
+          xs[il] = dilu ? mul(temp, cvt<W>(cur.invDiag(q))) : temp;
         }
       } else {
         // Backward substitution (ilu/Solver.cpp:413-442).
         for (int q = threadIdx.x; q < cur.k; q += kRingCompute) {
-          const int il = rows[q];
-          const W temp = ringRowDot<MV, UNROLL>(W(0), ents + kEnt * q, stride, cur.E, nRows, xs);
-          const W iv = cvt<W>(inv[q]);
+          const int il = cur.row(q);
+          const W temp = ringRowDot<UNROLL>(W(0), cur, q, nRows, xs);
+          const W iv = cvt<W>(cur.invDiag(q));
           xs[il] = dilu ? add(xs[il], mul(temp, iv)) : mul(add(xs[il], temp), iv);
         }
       }
@@ -304,7 +312,8 @@ template <class MV, class W>
 void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& p, void* y,
                 int l2Ahead, bool unroll, cudaStream_t s) {
   const size_t smem = iluRingSmem(A, R, dtypeOf<W>());
-  auto kernel = unroll ? dev::iluRingKernel<MV, W, true> : dev::iluRingKernel<MV, W, false>;
+  auto kernel = R.compact ? (unroll ? dev::iluRingKernel<MV, W, true, true> : dev::iluRingKernel<MV, W, false, true>)
+                         : (unroll ? dev::iluRingKernel<MV, W, true, false> : dev::iluRingKernel<MV, W, false, false>);
   ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
   preferSharedCarveout(reinterpret_cast<const void*>(kernel));
   if (p.stIndex && R.group != 1) fail(GR_EUNSUPPORTED, "batched solves run one tile per block");
@@ -322,8 +331,8 @@ void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool di
 
 int ringBlocksPerSMWithoutSmem(DType vt) {
   int n = 0;
-  const void* fn = vt == DType::F64 ? reinterpret_cast<const void*>(dev::iluRingKernel<double, double, true>)
-                                    : reinterpret_cast<const void*>(dev::iluRingKernel<float, float, true>);
+  const void* fn = vt == DType::F64 ? reinterpret_cast<const void*>(dev::iluRingKernel<double, double, true, false>)
+                                    : reinterpret_cast<const void*>(dev::iluRingKernel<float, float, true, false>);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, dev::kRingThreads, 0) != cudaSuccess) {
     (void)cudaGetLastError();
     return 0;

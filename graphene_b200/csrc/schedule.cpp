@@ -395,7 +395,7 @@ inline bool overlaps(i64 a, i64 sa, i64 b, i64 sb) { return a < b + sb && b < a 
 }  // namespace
 
 HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes, i32 group,
-                        const RingBudget& budget) {
+                        const RingBudget& budget, bool allowCompact) {
   const i64 vs = static_cast<i64>(dtypeSize(vt));
   const i64 entSize = vs == 4 ? 8 : 16;
   if (group < 1) fail(GR_EINVAL, "tiles per block must be at least 1");
@@ -404,6 +404,10 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
   // rows never reference one another), rows numbered from the block's first
   // row.
   const i32 NG = (H.P + group - 1) / group;
+  i64 maxGroupRows = 0;
+  for (i32 G = 0; G < NG; ++G)
+    maxGroupRows = std::max<i64>(maxGroupRows, H.tileStart[std::min<i32>(H.P, (G + 1) * group)] - H.tileStart[G * group]);
+  const bool compact = allowCompact && maxGroupRows + 1 <= kRingCompactRows;
   std::vector<TileRing> tr(NG);
   parallelFor(NG, [&](i64 G) {
     TileRing& t = tr[G];
@@ -431,26 +435,39 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
           rowEntries(H, kind, gBase + gl, gl - tb, H.tileStart[T + 1] - H.tileStart[T], ent);
           E = std::max<i64>(E, static_cast<i64>(ent.size()));
         }
-        const i64 rowsB = pad16(4 * k), invB = hasInv ? pad16(vs * k) : 0, entB = pad16(entSize * E * k);
-        const i64 S = rowsB + invB + entB;
+        if (E >= kRingUpperBit || k >= (i64(1) << 31) || entSize * E * k >= (i64(1) << 31))
+          fail(GR_EUNSUPPORTED, "ILU level too large for the ring kernel");
+        const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(k), static_cast<uint32_t>(E), hasInv,
+                                                    static_cast<uint32_t>(vs), compact);
+        const i64 S = lay.bytes;
         const i64 start = static_cast<i64>(t.bytes.size());
         t.bytes.resize(start + S, 0);
         for (i64 q = 0; q < k; ++q) {
           const auto [gl, T] = rows[q];
           const i64 tb = H.tileStart[T] - gBase;
-          const i32 r32 = static_cast<i32>(gl);
-          std::memcpy(t.bytes.data() + start + 4 * q, &r32, 4);
-          if (hasInv) t.invs.emplace_back(start + rowsB + vs * q, static_cast<i32>(gBase + gl));
+          if (compact) {
+            const uint16_t r16 = static_cast<uint16_t>(gl);
+            std::memcpy(t.bytes.data() + start + 2 * q, &r16, 2);
+          } else {
+            const i32 r32 = static_cast<i32>(gl);
+            std::memcpy(t.bytes.data() + start + 4 * q, &r32, 4);
+          }
+          if (hasInv) t.invs.emplace_back(start + lay.inv + vs * q, static_cast<i32>(gBase + gl));
           rowEntries(H, kind, gBase + gl, gl - tb, H.tileStart[T + 1] - H.tileStart[T], ent);
           for (i64 e = 0; e < E; ++e) {
-            const i64 pos = start + rowsB + invB + entSize * (e * k + q);
             const bool real = e < static_cast<i64>(ent.size());
             const i32 col = real ? static_cast<i32>(H.colLocal[ent[e]] + tb) : static_cast<i32>(gRows);
-            std::memcpy(t.bytes.data() + pos, &col, 4);
-            if (real) t.vals.emplace_back(pos + (vs == 4 ? 4 : 8), static_cast<i32>(ent[e]));
+            if (compact) {
+              const uint16_t c16 = static_cast<uint16_t>(col);
+              std::memcpy(t.bytes.data() + start + lay.ents + 2 * (e * k + q), &c16, 2);
+              if (real) t.vals.emplace_back(start + lay.vals + vs * (e * k + q), static_cast<i32>(ent[e]));
+            } else {
+              const i64 pos = start + lay.ents + entSize * (e * k + q);
+              std::memcpy(t.bytes.data() + pos, &col, 4);
+              if (real) t.vals.emplace_back(pos + (vs == 4 ? 4 : 8), static_cast<i32>(ent[e]));
+            }
           }
         }
-        if (E >= kRingUpperBit || k >= (i64(1) << 31)) fail(GR_EUNSUPPORTED, "ILU level too large for the ring kernel");
         t.meta.push_back(make_int4(static_cast<int>(k), static_cast<int>(E) | (upper ? kRingUpperBit : 0), 0, -1));
         t.size.push_back(S);
         t.maxLevel = std::max(t.maxLevel, S);
@@ -515,9 +532,6 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
     });
     return ok.load();
   };
-  i64 maxGroupRows = 0;
-  for (i32 G = 0; G < NG; ++G)
-    maxGroupRows = std::max<i64>(maxGroupRows, H.tileStart[std::min<i32>(H.P, (G + 1) * group)] - H.tileStart[G * group]);
   i32 maxLevels = 0;
   for (const TileRing& t : tr) maxLevels = std::max<i32>(maxLevels, static_cast<i32>(t.size.size()));
   if (ringBytes > 0) {
@@ -554,6 +568,7 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
   }
   if (R.ringBytes >= (i64(1) << 30)) fail(GR_EUNSUPPORTED, "ILU level ring too large");
   R.group = group;
+  R.compact = compact;
   R.tileOffset.assign(NG + 1, 0);
   R.tileLevel.assign(NG + 1, 0);
   R.groupStart.assign(NG + 1, 0);
@@ -629,12 +644,17 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
       const bool upper = (a.y & kRingUpperBit) != 0;
       if (upper != (l >= nLower)) bad(G, l, "sweep flag");
       const bool hasInv = upper || dilu;
-      const i64 rowsB = pad16(4 * k), invB = hasInv ? pad16(vs * k) : 0;
-      const i64 S = rowsB + invB + pad16(entSize * E * k);
+      const i64 idB = R.compact ? 2 : 4;
+      const i64 rowsB = pad16(idB * k), invB = hasInv ? pad16(vs * k) : 0;
+      const i64 colsB = R.compact ? pad16(2 * E * k) : pad16(entSize * E * k);
+      const i64 valsB = R.compact ? pad16(vs * E * k) : 0;
+      const i64 S = rowsB + invB + colsB + valsB;
       if (k < 1 || E < 0 || S > R.ringBytes) bad(G, l, "block layout");
       const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(k), static_cast<uint32_t>(E), hasInv,
-                                                  static_cast<uint32_t>(vs));
-      if (lay.inv != rowsB || lay.ents != rowsB + invB || lay.bytes != S) bad(G, l, "block layout");
+                                                  static_cast<uint32_t>(vs), R.compact);
+      if (lay.inv != rowsB || lay.ents != rowsB + invB || lay.bytes != S ||
+          lay.vals != (R.compact ? rowsB + invB + colsB : rowsB + invB))
+        bad(G, l, "block layout");
       const i64 entOff = rowsB + invB;
       if (off < 0 || off % 16 != 0 || off + S > R.ringBytes) bad(G, l, "ring offset");
       if (ia < -1 || ia < prevIa || ia < l - kRingBarriers || (l >= 1 && ia > l - 2) || (l == 0 && ia != -1))
@@ -650,12 +670,24 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
       std::vector<i64> rows(k);
       for (i64 q = 0; q < k; ++q) {
         i32 il;
-        std::memcpy(&il, blk + 4 * q, 4);
+        if (R.compact) {
+          uint16_t r16;
+          std::memcpy(&r16, blk + 2 * q, 2);
+          il = r16;
+        } else {
+          std::memcpy(&il, blk + 4 * q, 4);
+        }
         if (il < 0 || il >= gRows || done[il]) bad(G, l, "row id");
         rows[q] = il;
         for (i64 e = 0; e < E; ++e) {
           i32 c;
-          std::memcpy(&c, blk + entOff + entSize * (e * k + q), 4);
+          if (R.compact) {
+            uint16_t c16;
+            std::memcpy(&c16, blk + entOff + 2 * (e * k + q), 2);
+            c = c16;
+          } else {
+            std::memcpy(&c, blk + entOff + entSize * (e * k + q), 4);
+          }
           if (c < 0 || c > gRows) bad(G, l, "column index");
           if (c < gRows && (tileOf[c] != tileOf[il] || !done[c] || (upper ? c <= il : c >= il)))
             bad(G, l, "dependency order");
@@ -671,8 +703,8 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
   }
 }
 
-LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group) {
-  auto key = std::make_tuple(dilu, ringBytes, group);
+LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group, bool allowCompact) {
+  auto key = std::make_tuple(dilu, ringBytes, group, allowCompact);
   auto it = levelRings.find(key);
   if (it != levelRings.end()) return *it->second;
   RingBudget budget;
@@ -684,7 +716,7 @@ LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group) {
   if (cudaDeviceGetAttribute(&v, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess)
     budget.reservedPerBlock = v;
   if (const int b = ringBlocksPerSMWithoutSmem(vt); b > 0) budget.maxBlocksPerSM = b;
-  HostRing H = buildLevelRing(*host, dilu, vt, ringBytes, group, budget);
+  HostRing H = buildLevelRing(*host, dilu, vt, ringBytes, group, budget, allowCompact);
   auto R = std::make_unique<LevelRing>();
   R->dilu = dilu;
   R->bytes = static_cast<i64>(H.bytes.size());
@@ -698,6 +730,7 @@ LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group) {
   R->tileLevel.upload(H.tileLevel);
   R->groupStart.upload(H.groupStart);
   R->group = H.group;
+  R->compact = H.compact;
   R->numGroups = static_cast<i32>(H.groupStart.size()) - 1;
   R->maxGroupRows = H.maxGroupRows;
   R->valPos.upload(H.valPos);

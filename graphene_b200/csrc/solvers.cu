@@ -89,7 +89,7 @@ class IluNode : public Node {
     if (c.iluKernel == 0 || c.iluKernel == 4) {
       LevelRing* R = nullptr;
       try {
-        R = &A.levelRing(dilu_, c.ringBytes, c.tilesPerBlock > 0 ? c.tilesPerBlock : 1);
+        R = &A.levelRing(dilu_, c.ringBytes, c.tilesPerBlock > 0 ? c.tilesPerBlock : 1, c.compactRing);
       } catch (const Error&) {
         if (c.iluKernel == 4) throw;  // the requested ring cannot hold the levels
       }

@@ -245,15 +245,16 @@ int gr_host_matrix_check_ilu_stream(const gr_host_matrix* h, int dilu, gr_dtype 
 
 /* Builds the level blocks and copy schedule of the host-scheduled ring
  * substitution kernel for a ring of ring_bytes (0: the default) with
- * tiles_per_block consecutive tiles per thread block, and replays
+ * tiles_per_block consecutive tiles per thread block (allow_compact: 16-bit
+ * row and column ids where the blocks are small enough), and replays
  * the kernel's copies and reads on the host, checking every index, the
  * dependency order of the levels, that no copy overwrites a level still to
  * be consumed and that every copy is issued before its level is needed.
  * Host only. Writes the ring size used, the stream length and the largest
  * number of levels of a tile. No counterpart in the reference. */
 int gr_host_matrix_check_ilu_ring(const gr_host_matrix* h, int dilu, gr_dtype value_type, int64_t ring_bytes,
-                                  int32_t tiles_per_block, int64_t* ring_bytes_used, int64_t* stream_bytes,
-                                  int32_t* max_tile_levels);
+                                  int32_t tiles_per_block, int32_t allow_compact, int64_t* ring_bytes_used,
+                                  int64_t* stream_bytes, int32_t* max_tile_levels);
 
 /* Natural order <-> tile order (DistributedTileLayout::decomposeVector,
  * DistributedTileLayout.cpp:156-183, without halo). Host buffers. */

@@ -52,27 +52,36 @@ def case(name, oracle, vt=gb.FLOAT32):
 NAMES = ["poisson16", "poisson_odd_bfs", "poisson_1tile", "random", "many_tiles"]
 
 
+def ilu_config(kernel, **kw):
+    """'ring_compact': the ring kernel with 16-bit row and column ids."""
+    c = {"type": "ILU", "kernel": "ring" if kernel == "ring_compact" else kernel}
+    if kernel == "ring_compact":
+        c["compactRing"] = True
+    c.update(kw)
+    return c
+
+
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("dilu", [False, True])
-@pytest.mark.parametrize("kernel", ["ring", "warp", "tma", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "ring_compact", "warp", "tma", "levels"])
 def test_ilu_bit_exact(oracle, name, dilu, kernel):
     h, om = case(name, oracle)
     A = h.copyToTile()
     b = np.random.default_rng(3).uniform(-1, 1, h.numRows).astype(np.float32)
     x = A.createUninitializedVector(gb.FLOAT32)
-    gb.Solver(A, {"type": "ILU", "diagonalBased": dilu, "kernel": kernel}).solve(x, dev(b))
+    gb.Solver(A, ilu_config(kernel, diagonalBased=dilu)).solve(x, dev(b))
     off, inv = om.ilu_factorize(dilu)
     np.testing.assert_array_equal(host(x), om.ilu_solve(off, inv, b, dilu))
 
 
 @pytest.mark.parametrize("name", ["poisson16", "random"])
-@pytest.mark.parametrize("kernel", ["ring", "warp", "tma", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "ring_compact", "warp", "tma", "levels"])
 def test_ilu_bit_exact_float64(oracle, name, kernel):
     h, om = case(name, oracle, gb.FLOAT64)
     A = h.copyToTile()
     b = np.random.default_rng(4).standard_normal(h.numRows)
     x = A.createUninitializedVector(gb.FLOAT64)
-    gb.Solver(A, {"type": "ILU", "kernel": kernel}).solve(x, dev(b))
+    gb.Solver(A, ilu_config(kernel)).solve(x, dev(b))
     off, inv = om.ilu_factorize(False)
     np.testing.assert_array_equal(host(x), om.ilu_solve(off, inv, b, False))
 
@@ -99,7 +108,7 @@ def test_ilu_ring_small_rings_bit_exact(oracle, name, frac):
     import ctypes as C
     h, om = case(name, oracle)
     used = C.c_int64()
-    gb._lib.check(gb._lib.lib().gr_host_matrix_check_ilu_ring(h._h, 0, gb.FLOAT32, 0, 1, C.byref(used), None, None))
+    gb._lib.check(gb._lib.lib().gr_host_matrix_check_ilu_ring(h._h, 0, gb.FLOAT32, 0, 1, 1, C.byref(used), None, None))
     rb = 0 if frac == 0.0 else max(16, int(used.value * frac) // 16 * 16)
     A = h.copyToTile()
     b = np.random.default_rng(6).uniform(-1, 1, h.numRows).astype(np.float32)

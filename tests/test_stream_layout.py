@@ -53,9 +53,9 @@ def test_stream_replay_bench_problem():
 
 # ---- host-scheduled level ring (kernels_ring.cu) ----------------------------------------
 
-def check_ring(h, dilu, vt=gb.FLOAT32, ring_bytes=0, group=1):
+def check_ring(h, dilu, vt=gb.FLOAT32, ring_bytes=0, group=1, compact=True):
     used, nbytes, lv = C.c_int64(), C.c_int64(), C.c_int32()
-    gb._lib.check(gb._lib.lib().gr_host_matrix_check_ilu_ring(h._h, int(dilu), vt, ring_bytes, group,
+    gb._lib.check(gb._lib.lib().gr_host_matrix_check_ilu_ring(h._h, int(dilu), vt, ring_bytes, group, int(compact),
                                                                C.byref(used), C.byref(nbytes), C.byref(lv)))
     return used.value, nbytes.value, lv.value
 
@@ -71,10 +71,20 @@ def check_ring(h, dilu, vt=gb.FLOAT32, ring_bytes=0, group=1):
 @pytest.mark.parametrize("dilu", [False, True])
 @pytest.mark.parametrize("vt", [gb.FLOAT32, gb.FLOAT64])
 @pytest.mark.parametrize("group", [1, 3])
-def test_ring_replay(dims, tiles, part, dilu, vt, group):
+@pytest.mark.parametrize("compact", [True, False])
+def test_ring_replay(dims, tiles, part, dilu, vt, group, compact):
     h = gb.generate3DPoissonMatrix(vt, *dims, tiles, part)
-    used, nbytes, lv = check_ring(h, dilu, vt, 0, group)
+    used, nbytes, lv = check_ring(h, dilu, vt, 0, group, compact)
     assert used > 0 and used % 16 == 0 and nbytes % 16 == 0 and lv >= 2
+
+
+def test_ring_compact_layout_is_smaller():
+    """16-bit row and column ids: a 7-point lower-sweep row takes 2 + 3 x 6
+    bytes instead of 4 + 3 x 8."""
+    h = gb.generate3DPoissonMatrix(gb.FLOAT32, 24, 24, 24, 8, gb.PART_RCB)
+    _, wide, _ = check_ring(h, False, gb.FLOAT32, 0, 1, False)
+    _, compact, _ = check_ring(h, False, gb.FLOAT32, 0, 1, True)
+    assert compact < 0.8 * wide
 
 
 @pytest.mark.parametrize("seed", [0, 1, 2])
