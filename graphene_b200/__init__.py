@@ -236,6 +236,14 @@ class HostMatrix:
         check(_lib.lib().gr_host_matrix_decompose_vector(self._h, _ptr(a), _ptr(out), t))
         return out
 
+    def loadVectorFromFile(self, t: int, path: str) -> np.ndarray:
+        """DistributedTileLayout::loadVectorFromFile (DistributedTileLayout.cpp:185-206)
+        without halo cells: a MatrixMarket vector, in tile order."""
+        t = parseType(t)
+        out = np.empty(self.numRows, dtype=_NP[t])
+        check(_lib.lib().gr_host_matrix_load_vector_mm(self._h, str(path).encode(), t, _ptr(out)))
+        return out
+
     def composeVector(self, vec, t: int = FLOAT32) -> np.ndarray:
         a = np.ascontiguousarray(vec, dtype=_NP[t])
         out = np.empty_like(a)

@@ -103,6 +103,7 @@ SIGNATURES = {
     "gr_host_matrix_local_crs": (C.c_int, [vp, vp, vp, vp, vp]),
     "gr_host_matrix_levels": (C.c_int, [vp, vp, vp]),
     "gr_host_matrix_check_ilu_stream": (C.c_int, [vp, C.c_int, C.c_int, P(i32), P(i64)]),
+    "gr_host_matrix_load_vector_mm": (C.c_int, [vp, C.c_char_p, C.c_int, vp]),
     "gr_host_matrix_check_ilu_ring": (C.c_int, [vp, C.c_int, C.c_int, i64, i32, i32, P(i64), P(i64), P(i32)]),
     "gr_host_matrix_decompose_vector": (C.c_int, [vp, vp, vp, C.c_int]),
     "gr_host_matrix_compose_vector": (C.c_int, [vp, vp, vp, C.c_int]),

@@ -337,6 +337,26 @@ int gr_host_matrix_decompose_vector(const gr_host_matrix* h, const void* natural
   });
 }
 
+int gr_host_matrix_load_vector_mm(const gr_host_matrix* h, const char* path, gr_dtype t, void* tile_ordered) {
+  return guarded([&] {
+    need(h, "matrix");
+    need(path, "path");
+    need(tile_ordered, "tile_ordered");
+    const gr::DType dt = gr::toDType(t);
+    if (dt != gr::DType::F32 && dt != gr::DType::F64) gr::fail(GR_EUNSUPPORTED, "vectors are float32 or float64");
+    const std::vector<double> v = gr::readMatrixMarketVector(path, dt);
+    if (static_cast<gr::i64>(v.size()) != h->m->n)
+      gr::fail(GR_EINVAL, "vector file has " + std::to_string(v.size()) + " rows, the matrix " +
+                              std::to_string(h->m->n));
+    if (dt == gr::DType::F32) {
+      std::vector<float> f(v.begin(), v.end());
+      h->m->decompose(f.data(), static_cast<float*>(tile_ordered));
+    } else {
+      h->m->decompose(v.data(), static_cast<double*>(tile_ordered));
+    }
+  });
+}
+
 int gr_host_matrix_compose_vector(const gr_host_matrix* h, const void* tile_ordered, void* natural,
                                   gr_dtype t) {
   return guarded([&] {

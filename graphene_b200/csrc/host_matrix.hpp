@@ -166,5 +166,11 @@ void generateNormal(uint64_t seed, i64 n, double* out);
 // Values are parsed directly into valueType (strtof for float32) so that
 // they are rounded once, as a reader templated on the value type does.
 Coo readMatrixMarket(const std::string& path, DType valueType);
+// A vector from a MatrixMarket file (matrix/host/details/MatrixMarket.cpp:66-102):
+// a "vector" object (coordinate: index value pairs; array: one value a line)
+// or the first column of a "matrix" object (coordinate or array). Entries
+// the file does not list are 0; a later entry for an index replaces an
+// earlier one. Returns the rows, values rounded once to valueType.
+std::vector<double> readMatrixMarketVector(const std::string& path, DType valueType);
 
 }  // namespace gr

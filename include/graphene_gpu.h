@@ -256,6 +256,13 @@ int gr_host_matrix_check_ilu_ring(const gr_host_matrix* h, int dilu, gr_dtype va
                                   int32_t tiles_per_block, int32_t allow_compact, int64_t* ring_bytes_used,
                                   int64_t* stream_bytes, int32_t* max_tile_levels);
 
+/* DistributedTileLayout::loadVectorFromFile (DistributedTileLayout.cpp:185-206,
+ * without halo): reads a MatrixMarket vector (a "vector" object, coordinate
+ * or array, or the first column of a "matrix" object; unlisted entries are
+ * 0), which must have as many rows as h, and writes it in tile order, type t
+ * (float32 or float64). Host only. */
+int gr_host_matrix_load_vector_mm(const gr_host_matrix* h, const char* path, gr_dtype t, void* tile_ordered);
+
 /* Natural order <-> tile order (DistributedTileLayout::decomposeVector,
  * DistributedTileLayout.cpp:156-183, without halo). Host buffers. */
 int gr_host_matrix_decompose_vector(const gr_host_matrix* h, const void* natural,
