@@ -160,15 +160,31 @@ void checkIluStream(const HostMatrix& H, const HostStream& S, bool dilu, DType v
 //   ents  E*k entries, entry-major, {i32 column, value}: 8 bytes for float,
 //         16 for double ({column, 0, value})
 // Padding entries use column nRows (a zero slot of the kernel's x slice) and
-// value 0. One int4 per level: {k, E | upper << 30, ring offset,
-// issueAfter}; the block's segment offsets and size follow from k, E, upper,
-// DILU and the layout (ringLevelLayout). The kernel copies a level's block
-// into its shared-memory ring at `ring offset` once the tile's level
-// `issueAfter` has been consumed (-1: at the start); the host chose the
-// offsets so that a copy never overwrites a level still to be consumed, and
-// so that every level is copied at least one level before it is needed.
+// value 0. One int4 per level (RingLevelCode): k; E, the entries' offset
+// and the sweep; the ring offset and the block's size; issueAfter. The
+// kernel copies a level's block into its shared-memory ring at `ring offset`
+// once the tile's level `issueAfter` has been consumed (-1: at the start);
+// the host chose the offsets so that a copy never overwrites a level still
+// to be consumed, and so that every level is copied at least one level
+// before it is needed.
 constexpr int kRingBarriers = 16;
 constexpr int kRingUpperBit = 1 << 30;
+// Field packing of a level's int4: y = E | (entries offset / 16) << 14 |
+// upper << 30, z = ring offset | (block bytes / 16) << 18.
+constexpr int kRingEBits = 14, kRingOffBits = 18;
+struct RingLevelCode {
+  __host__ __device__ static int k(const int4 m) { return m.x; }
+  __host__ __device__ static int E(const int4 m) { return m.y & ((1 << kRingEBits) - 1); }
+  __host__ __device__ static uint32_t ents(const int4 m) {
+    return ((static_cast<uint32_t>(m.y) >> kRingEBits) & 0xFFFFu) << 4;
+  }
+  __host__ __device__ static bool upper(const int4 m) { return (m.y & kRingUpperBit) != 0; }
+  __host__ __device__ static uint32_t ringOffset(const int4 m) {
+    return static_cast<uint32_t>(m.z) & ((1u << kRingOffBits) - 1);
+  }
+  __host__ __device__ static uint32_t bytes(const int4 m) { return (static_cast<uint32_t>(m.z) >> kRingOffBits) << 4; }
+  __host__ __device__ static int issueAfter(const int4 m) { return m.w; }
+};
 constexpr long long kRingCompactRows = 65535;  // largest block (rows + zero slot) of the compact layout
 
 // Byte offsets of a level block's inverse diagonal, entries (columns, or

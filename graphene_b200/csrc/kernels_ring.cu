@@ -78,18 +78,19 @@ struct RingLevel {
     }
   }
 };
+// The level's view from its table entry (RingLevelCode): the inverse
+// diagonal follows the row ids, the values (compact layout) the columns.
 template <class MV, bool COMPACT>
-__device__ __forceinline__ RingLevel<MV, COMPACT> ringLevelAt(const int4 m, const unsigned char* ring, bool dilu) {
+__device__ __forceinline__ RingLevel<MV, COMPACT> ringLevelAt(const int4 m, const unsigned char* ring) {
   RingLevel<MV, COMPACT> lv;
-  lv.k = m.x;
-  lv.E = m.y & (kRingUpperBit - 1);
-  lv.upper = (m.y & kRingUpperBit) != 0;
-  const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(lv.k), static_cast<uint32_t>(lv.E),
-                                              lv.upper || dilu, sizeof(MV), COMPACT);
-  lv.blk = ring + m.z;
-  lv.inv = lay.inv;
-  lv.ents = lay.ents;
-  lv.vals = lay.vals;
+  lv.k = RingLevelCode::k(m);
+  lv.E = RingLevelCode::E(m);
+  lv.upper = RingLevelCode::upper(m);
+  lv.blk = ring + RingLevelCode::ringOffset(m);
+  lv.inv = ((COMPACT ? 2u : 4u) * static_cast<uint32_t>(lv.k) + 15u) & ~15u;
+  lv.ents = RingLevelCode::ents(m);
+  lv.vals = COMPACT ? lv.ents + ((2u * static_cast<uint32_t>(lv.E) * static_cast<uint32_t>(lv.k) + 15u) & ~15u)
+                    : lv.ents;
   return lv;
 }
 
@@ -207,19 +208,15 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
         const uint32_t tileBytes = static_cast<uint32_t>(tileOffset[T + 1] - tileOffset[T]);
         for (; issued < L && !*abortV; ++issued) {
           const int4 m = mt[issued];
-          const int ia = m.w;
+          const int ia = RingLevelCode::issueAfter(m);
           if (ia >= 0 && !mbarWaitBounded(smemAddr(empty + ia % kRingBarriers), (ia / kRingBarriers) & 1, abortV)) {
             abortFlag = 1;
             break;
           }
-          const bool up = (m.y & kRingUpperBit) != 0;
-          const uint32_t bytes =
-              ringLevelLayout(static_cast<uint32_t>(m.x), static_cast<uint32_t>(m.y & (kRingUpperBit - 1)), up || dilu,
-                              sizeof(MV), COMPACT)
-                  .bytes;
+          const uint32_t bytes = RingLevelCode::bytes(m);
           const uint32_t bar = smemAddr(full + issued % kRingBarriers);
           mbarExpectTx(bar, bytes);
-          bulkLoad(smemAddr(ring + m.z), g + src, bytes, bar);
+          bulkLoad(smemAddr(ring + RingLevelCode::ringOffset(m)), g + src, bytes, bar);
           src += bytes;
           if (pf < src) pf = src;
           const uint32_t until = min(tileBytes, src + l2Ahead);
@@ -256,7 +253,8 @@ __global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned cha
     // the previous barrier.
     bool stop = namedBarOr(1, kRingLevelSync, false);
     for (int l = 0; !stop && l < L; ++l) {
-      const RingLevel<MV, COMPACT> cur = ringLevelAt<MV, COMPACT>(mt[l], ring, dilu);
+      const int4 m = mt[l];
+      const RingLevel<MV, COMPACT> cur = ringLevelAt<MV, COMPACT>(m, ring);
       if (!cur.upper) {
         // Forward substitution (ilu/Solver.cpp:380-411).
         for (int q = threadIdx.x; q < cur.k; q += kRingCompute) {

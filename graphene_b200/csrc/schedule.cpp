@@ -435,7 +435,7 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
           rowEntries(H, kind, gBase + gl, gl - tb, H.tileStart[T + 1] - H.tileStart[T], ent);
           E = std::max<i64>(E, static_cast<i64>(ent.size()));
         }
-        if (E >= kRingUpperBit || k >= (i64(1) << 31) || entSize * E * k >= (i64(1) << 31))
+        if (E >= (i64(1) << kRingEBits) || k >= (i64(1) << 31) || entSize * E * k >= (i64(1) << 31))
           fail(GR_EUNSUPPORTED, "ILU level too large for the ring kernel");
         const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(k), static_cast<uint32_t>(E), hasInv,
                                                     static_cast<uint32_t>(vs), compact);
@@ -494,7 +494,7 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
       i64 prevIa = -1;
       for (i64 l = 0; l < L && ok; ++l) {
         const i64 S = t.size[l];
-        if (S > ring) { ok = false; return; }
+        if (S > ring || S >= (i64(1) << (32 - kRingOffBits + 4))) { ok = false; return; }
         const i64 floorIa = std::max<i64>(prevIa, l - kRingBarriers);
         // issueAfter for offset c: the most recent overlapping level above
         // floorIa, else floorIa.
@@ -566,7 +566,7 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
     R.ringBytes = bestRing;
     if (!place(R.ringBytes)) fail(GR_EINVAL, "ILU level ring placement");
   }
-  if (R.ringBytes >= (i64(1) << 30)) fail(GR_EUNSUPPORTED, "ILU level ring too large");
+  if (R.ringBytes > (i64(1) << kRingOffBits)) fail(GR_EUNSUPPORTED, "ILU level ring too large");
   R.group = group;
   R.compact = compact;
   R.tileOffset.assign(NG + 1, 0);
@@ -598,7 +598,18 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
   parallelFor(NG, [&](i64 T) {
     const i64 off = R.tileOffset[T];
     std::memcpy(R.bytes.data() + off, tr[T].bytes.data(), tr[T].bytes.size());
-    std::copy(tr[T].meta.begin(), tr[T].meta.end(), R.meta.begin() + static_cast<size_t>(R.tileLevel[T]));
+    // Pack the placed levels (RingLevelCode): E, entries offset and sweep in
+    // y; ring offset and block size in z.
+    for (size_t l = 0; l < tr[T].meta.size(); ++l) {
+      int4 m = tr[T].meta[l];
+      const bool upper = (m.y & kRingUpperBit) != 0;
+      const uint32_t E = static_cast<uint32_t>(m.y & (kRingUpperBit - 1));
+      const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(m.x), E, upper || dilu,
+                                                  static_cast<uint32_t>(vs), compact);
+      m.y = static_cast<int>(E | ((lay.ents >> 4) << kRingEBits) | (upper ? static_cast<uint32_t>(kRingUpperBit) : 0u));
+      m.z = static_cast<int>(static_cast<uint32_t>(m.z) | ((lay.bytes >> 4) << kRingOffBits));
+      R.meta[static_cast<size_t>(R.tileLevel[T]) + l] = m;
+    }
     for (size_t i = 0; i < tr[T].vals.size(); ++i) {
       R.valPos[vOff[T] + i] = static_cast<i32>((off + tr[T].vals[i].first) / vs);
       R.valSrc[vOff[T] + i] = tr[T].vals[i].second;
@@ -640,8 +651,9 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
     i64 src = R.tileOffset[G], prevIa = -1;
     for (i64 l = 0; l < L; ++l) {
       const int4 a = R.meta[R.tileLevel[G] + l];
-      const i64 k = a.x, E = a.y & (kRingUpperBit - 1), off = a.z, ia = a.w;
-      const bool upper = (a.y & kRingUpperBit) != 0;
+      const i64 k = RingLevelCode::k(a), E = RingLevelCode::E(a), off = RingLevelCode::ringOffset(a);
+      const i64 ia = RingLevelCode::issueAfter(a);
+      const bool upper = RingLevelCode::upper(a);
       if (upper != (l >= nLower)) bad(G, l, "sweep flag");
       const bool hasInv = upper || dilu;
       const i64 idB = R.compact ? 2 : 4;
@@ -653,7 +665,8 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
       const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(k), static_cast<uint32_t>(E), hasInv,
                                                   static_cast<uint32_t>(vs), R.compact);
       if (lay.inv != rowsB || lay.ents != rowsB + invB || lay.bytes != S ||
-          lay.vals != (R.compact ? rowsB + invB + colsB : rowsB + invB))
+          lay.vals != (R.compact ? rowsB + invB + colsB : rowsB + invB) || RingLevelCode::ents(a) != lay.ents ||
+          RingLevelCode::bytes(a) != lay.bytes)
         bad(G, l, "block layout");
       const i64 entOff = rowsB + invB;
       if (off < 0 || off % 16 != 0 || off + S > R.ringBytes) bad(G, l, "ring offset");
