@@ -216,7 +216,7 @@ struct RingBudget {
   i32 numSMs = 148;
   i64 smemPerSM = 233472;
   i64 reservedPerBlock = 1024;
-  i32 maxBlocksPerSM = 7;  // the ring kernel's register limit on B200
+  i32 maxBlocksPerSM = 16;  // the ring kernel's thread and register limit on B200
 };
 struct HostRing {
   std::vector<uint8_t> bytes;

@@ -13,10 +13,10 @@
 // sit at fixed offsets. Producer and consumers form a pipeline over
 // kRingBarriers pairs of mbarriers: the producer warp issues level j's copy
 // (completing on full[j % 16]) once level issueAfter(j) has been released
-// (empty[...]). The four compute warps compute level l's rows from shared
-// memory while a waiting warp waits for full[(l + 1) % 16]; the five meet
-// at a barrier of their own that ends level l, after which the waiting warp
-// releases level l. Neither the producer's copies nor the mbarrier waits
+// (empty[...]). The compute warps compute level l's rows from shared memory
+// while a waiting warp waits for full[(l + 1) % 16]; they meet at a barrier
+// of their own that ends level l, after which the waiting warp releases
+// level l. Neither the producer's copies nor the mbarrier waits
 // and arrivals sit on the compute warps' per-level chain.
 //
 // Every wait is bounded; when one runs out the block records GR_ETIMEOUT in
@@ -33,10 +33,18 @@
 namespace gr {
 namespace dev {
 
-// Four compute warps, a waiting warp and a producer warp per block.
-constexpr int kRingCompute = 128;
-constexpr int kRingLevelSync = kRingCompute + 32;  // compute warps + waiting warp
-constexpr int kRingThreads = kRingLevelSync + 32;
+// Compute warps, a waiting warp and a producer warp per block. Fewer
+// compute warps mean fewer instructions and barrier arrivals per level; with
+// float vectors (seven blocks an SM at 192^3, 2048 tiles) two were fastest on
+// B200 (116.8 us against 123.0 for one, 117.0 for three, 121 for four, 125.5
+// for six); double vectors take twice the shared memory, so fewer blocks
+// share an SM, and four were faster for them.
+template <class W>
+struct RingShape {
+  static constexpr int compute = sizeof(W) == 4 ? 64 : 128;
+  static constexpr int levelSync = compute + 32;  // compute warps + waiting warp
+  static constexpr int threads = levelSync + 32;
+};
 constexpr int kPrefetchAhead = 0;  // default bytes kept prefetched into L2 beyond the issued copies
 
 // Entry of a level block: column and value (the value at byte 4 for float,
@@ -131,13 +139,15 @@ __device__ __forceinline__ W ringRowDot(W temp, const RingLevel<MV, COMPACT>& lv
 }
 
 template <class MV, class W, bool UNROLL, bool COMPACT>
-__global__ void __launch_bounds__(kRingThreads) iluRingKernel(const unsigned char* __restrict__ stream,
+__global__ void __launch_bounds__(RingShape<W>::threads) iluRingKernel(const unsigned char* __restrict__ stream,
                                                                const long long* __restrict__ tileOffset,
                                                                const int4* __restrict__ meta,
                                                                const int* __restrict__ tileLevel,
                                                                const int* __restrict__ blockStart, int ringBytes,
                                                                int metaLevels, uint32_t l2Ahead, bool dilu,
                                                                SPro<W> pro, W* __restrict__ y, int* errFlag) {
+  constexpr int kRingCompute = RingShape<W>::compute;
+  constexpr int kRingLevelSync = RingShape<W>::levelSync;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int abortFlag, consumedLevels;
   const KState* st = pro.state();
@@ -317,7 +327,7 @@ void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool di
   if (p.stIndex && R.group != 1) fail(GR_EUNSUPPORTED, "batched solves run one tile per block");
   dev::SPro<W> pro{static_cast<int>(p.kind), static_cast<const W*>(p.b), static_cast<const W*>(p.r),
                    static_cast<W*>(p.pOrS), static_cast<const W*>(p.v), p.st, p.stIndex};
-  kernel<<<R.numGroups, dev::kRingThreads, smem, s>>>(static_cast<const unsigned char*>(stream),
+  kernel<<<R.numGroups, dev::RingShape<W>::threads, smem, s>>>(static_cast<const unsigned char*>(stream),
                                              R.tileOffset.as<long long>(), R.meta.as<int4>(), R.tileLevel.as<int>(),
                                              R.groupStart.as<int>(),
                                              static_cast<int>(R.ringBytes), R.maxTileLevels,
@@ -331,7 +341,8 @@ int ringBlocksPerSMWithoutSmem(DType vt) {
   int n = 0;
   const void* fn = vt == DType::F64 ? reinterpret_cast<const void*>(dev::iluRingKernel<double, double, true, false>)
                                     : reinterpret_cast<const void*>(dev::iluRingKernel<float, float, true, false>);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, dev::kRingThreads, 0) != cudaSuccess) {
+  const int threads = vt == DType::F64 ? dev::RingShape<double>::threads : dev::RingShape<float>::threads;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, 0) != cudaSuccess) {
     (void)cudaGetLastError();
     return 0;
   }
