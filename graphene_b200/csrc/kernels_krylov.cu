@@ -121,7 +121,26 @@ __global__ void __launch_bounds__(256) spmvDotKernel(SellView<MV> A, const W* __
 
 // x = x + alpha y + omega z, r = s - omega t (pbicgstab/Solver.cpp:164-168),
 // then norm, convergence, iteration count and the next rho / beta.
-template <class W>
+// Four consecutive elements from index i (a multiple of 4 of a buffer
+// aligned to 16 bytes): one 16-byte access for float, two for double.
+__device__ __forceinline__ void load4(const float* p, int i, float (&o)[4]) {
+  const float4 v = __ldg(reinterpret_cast<const float4*>(p + i));
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+__device__ __forceinline__ void load4(const double* p, int i, double (&o)[4]) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p + i));
+  const double2 b = __ldg(reinterpret_cast<const double2*>(p + i + 2));
+  o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+__device__ __forceinline__ void store4(float* p, int i, const float (&o)[4]) {
+  *reinterpret_cast<float4*>(p + i) = make_float4(o[0], o[1], o[2], o[3]);
+}
+__device__ __forceinline__ void store4(double* p, int i, const double (&o)[4]) {
+  *reinterpret_cast<double2*>(p + i) = make_double2(o[0], o[1]);
+  *reinterpret_cast<double2*>(p + i + 2) = make_double2(o[2], o[3]);
+}
+
+template <class W, bool VEC>
 __global__ void __launch_bounds__(256) bicgUpdateKernel(W* __restrict__ x, const W* __restrict__ y,
                                                          const W* __restrict__ z, W* __restrict__ r,
                                                          const W* __restrict__ s, const W* __restrict__ t,
@@ -135,12 +154,40 @@ __global__ void __launch_bounds__(256) bicgUpdateKernel(W* __restrict__ x, const
   const int nk = st->normKind;
   double v[2] = {redIdentity(normOp(nk)), 0.0};
   const int ops[2] = {normOp(nk), RED_SUM};
-  for (int i = sp.r0 + sp.rank * blockDim.x + threadIdx.x; i < sp.r1; i += sp.nb * blockDim.x) {
+  // Four consecutive elements a thread, all loads issued before the
+  // arithmetic, so that a warp keeps four times the bytes in flight; each
+  // thread adds its elements to the reductions in index order.
+  auto one = [&](int i) {
     x[i] = add(add(x[i], mul(al, y[i])), mul(om, z[i]));
     const W rv = sub(s[i], mul(om, t[i]));
     r[i] = rv;
     v[0] = normStep(v[0], toDouble(rv), nk);
     v[1] = __dadd_rn(v[1], __dmul_rn(toDouble(__ldg(r0 + i)), toDouble(rv)));
+  };
+  const int stride = 4 * sp.nb * static_cast<int>(blockDim.x);
+  for (int i0 = sp.r0 + 4 * (sp.rank * static_cast<int>(blockDim.x) + static_cast<int>(threadIdx.x)); i0 < sp.r1;
+       i0 += stride) {
+    if (VEC && i0 + 3 < sp.r1) {
+      W xa[4], ya[4], za[4], sa[4], ta[4], ra[4];
+      load4(x, i0, xa);
+      load4(y, i0, ya);
+      load4(z, i0, za);
+      load4(s, i0, sa);
+      load4(t, i0, ta);
+      load4(r0, i0, ra);
+      W xo[4], ro[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        xo[j] = add(add(xa[j], mul(al, ya[j])), mul(om, za[j]));
+        ro[j] = sub(sa[j], mul(om, ta[j]));
+        v[0] = normStep(v[0], toDouble(ro[j]), nk);
+        v[1] = __dadd_rn(v[1], __dmul_rn(toDouble(ra[j]), toDouble(ro[j])));
+      }
+      store4(x, i0, xo);
+      store4(r, i0, ro);
+    } else {
+      for (int i = i0; i < min(i0 + 4, sp.r1); ++i) one(i);
+    }
   }
   double out[2];
   blockReduce<2>(v, ops, smem);
@@ -312,13 +359,19 @@ void launchSpmvDot(DeviceMatrix& A, const void* x, void* y, const void* d1, int 
 void launchBicgUpdate(DeviceMatrix& A, void* x, const void* y, const void* z, void* r, const void* sv,
                       const void* t, const void* r0, KState* st, DType W, cudaStream_t s) {
   const Launch L = krylovLaunch(A, false);
+  // 16-byte accesses need every vector 16-byte aligned (segments start at
+  // multiples of 32 rows); otherwise the same order element by element.
+  const bool vec = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(z) |
+                     reinterpret_cast<uintptr_t>(r) | reinterpret_cast<uintptr_t>(sv) | reinterpret_cast<uintptr_t>(t) |
+                     reinterpret_cast<uintptr_t>(r0)) &
+                    15u) == 0;
   if (W == DType::F32)
-    dev::bicgUpdateKernel<float><<<L.blocks, 256, 0, s>>>(
+    (vec ? dev::bicgUpdateKernel<float, true> : dev::bicgUpdateKernel<float, false>)<<<L.blocks, 256, 0, s>>>(
         static_cast<float*>(x), static_cast<const float*>(y), static_cast<const float*>(z), static_cast<float*>(r),
         static_cast<const float*>(sv), static_cast<const float*>(t), static_cast<const float*>(r0), A.n, st,
         L.partials, L.counter, L.seg);
   else
-    dev::bicgUpdateKernel<double><<<L.blocks, 256, 0, s>>>(
+    (vec ? dev::bicgUpdateKernel<double, true> : dev::bicgUpdateKernel<double, false>)<<<L.blocks, 256, 0, s>>>(
         static_cast<double*>(x), static_cast<const double*>(y), static_cast<const double*>(z),
         static_cast<double*>(r), static_cast<const double*>(sv), static_cast<const double*>(t),
         static_cast<const double*>(r0), A.n, st, L.partials, L.counter, L.seg);
