@@ -243,7 +243,7 @@ inline i64 ringFixedSmem(i32 maxTileLevels, i64 maxGroupRows, i64 vectorBytes) {
 // The compact layout is used when every block has at most kRingCompactRows
 // rows and `allowCompact`.
 HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes, i32 group,
-                        const RingBudget& budget = RingBudget{}, bool allowCompact = false);
+                        const RingBudget& budget = RingBudget{}, bool allowCompact = true);
 // Replays the kernel's copies and reads on the host; throws GR_EINVAL on an
 // out-of-range index, a dependency-order violation, a copy that would
 // overwrite a level not yet consumed, or a copy issued too late.
@@ -317,7 +317,7 @@ struct DeviceMatrix {
   std::unique_ptr<SweepStream> iluStream[2];  // [dilu]
   SweepStream& iluSweepStream(bool dilu);
   std::map<std::tuple<bool, i64, i32, bool>, std::unique_ptr<LevelRing>> levelRings;  // [(dilu, ring bytes, group, compact allowed)]
-  LevelRing& levelRing(bool dilu, i64 ringBytes, i32 group, bool allowCompact = false);
+  LevelRing& levelRing(bool dilu, i64 ringBytes, i32 group, bool allowCompact = true);
 
   // Device error word written by kernels whose bounded waits ran out
   // (GR_ETIMEOUT); 0 when clean.

@@ -339,8 +339,8 @@ void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool di
 
 int ringBlocksPerSMWithoutSmem(DType vt) {
   int n = 0;
-  const void* fn = vt == DType::F64 ? reinterpret_cast<const void*>(dev::iluRingKernel<double, double, true, false>)
-                                    : reinterpret_cast<const void*>(dev::iluRingKernel<float, float, true, false>);
+  const void* fn = vt == DType::F64 ? reinterpret_cast<const void*>(dev::iluRingKernel<double, double, true, true>)
+                                    : reinterpret_cast<const void*>(dev::iluRingKernel<float, float, true, true>);
   const int threads = vt == DType::F64 ? dev::RingShape<double>::threads : dev::RingShape<float>::threads;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, 0) != cudaSuccess) {
     (void)cudaGetLastError();

@@ -53,17 +53,17 @@ NAMES = ["poisson16", "poisson_odd_bfs", "poisson_1tile", "random", "many_tiles"
 
 
 def ilu_config(kernel, **kw):
-    """'ring_compact': the ring kernel with 16-bit row and column ids."""
-    c = {"type": "ILU", "kernel": "ring" if kernel == "ring_compact" else kernel}
-    if kernel == "ring_compact":
-        c["compactRing"] = True
+    """'ring_wide': the ring kernel with 32-bit row and column ids."""
+    c = {"type": "ILU", "kernel": "ring" if kernel == "ring_wide" else kernel}
+    if kernel == "ring_wide":
+        c["compactRing"] = False
     c.update(kw)
     return c
 
 
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("dilu", [False, True])
-@pytest.mark.parametrize("kernel", ["ring", "ring_compact", "warp", "tma", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "ring_wide", "warp", "tma", "levels"])
 def test_ilu_bit_exact(oracle, name, dilu, kernel):
     h, om = case(name, oracle)
     A = h.copyToTile()
@@ -75,7 +75,7 @@ def test_ilu_bit_exact(oracle, name, dilu, kernel):
 
 
 @pytest.mark.parametrize("name", ["poisson16", "random"])
-@pytest.mark.parametrize("kernel", ["ring", "ring_compact", "warp", "tma", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "ring_wide", "warp", "tma", "levels"])
 def test_ilu_bit_exact_float64(oracle, name, kernel):
     h, om = case(name, oracle, gb.FLOAT64)
     A = h.copyToTile()
