@@ -548,23 +548,29 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
     const i64 lo = std::max<i64>(256, pad16(2 * R.maxLevelBytes));
     const i64 hi = std::max<i64>(std::max<i64>(16384, pad16(4 * R.maxLevelBytes)), lo);
     const i64 step = std::max<i64>(256, pad16(R.maxLevelBytes / 16));
-    i64 bestRing = -1, bestWaves = 0;
-    auto consider = [&](i64 r) {
-      if (!place(r)) return;
+    // Waves depend only on the size, so the sizes are tried best first
+    // (fewest waves, then largest); the first that places is taken, which
+    // usually costs one or two placement passes.
+    auto wavesOf = [&](i64 r) {
       const i64 perSM = std::min<i64>(budget.maxBlocksPerSM, budget.smemPerSM / (fixed + r));
       const i64 slots = std::max<i64>(1, perSM) * std::max<i32>(1, budget.numSMs);
-      const i64 waves = perSM > 0 ? (NG + slots - 1) / slots : (i64(1) << 40);
-      if (bestRing < 0 || waves <= bestWaves) {
-        bestRing = r;
-        bestWaves = waves;
-      }
+      return perSM > 0 ? (NG + slots - 1) / slots : (i64(1) << 40);
     };
-    for (i64 r = lo; r < hi; r += step) consider(r);
-    consider(hi);
-    for (i64 r = hi + step; bestRing < 0 && r < (i64(1) << 30); r += step) consider(r);
+    std::vector<std::pair<i64, i64>> order;  // (waves, -size)
+    for (i64 r = lo; r < hi; r += step) order.emplace_back(wavesOf(r), -r);
+    order.emplace_back(wavesOf(hi), -hi);
+    std::sort(order.begin(), order.end());
+    i64 bestRing = -1;
+    for (const auto& [w, negR] : order) {
+      if (place(-negR)) {
+        bestRing = -negR;
+        break;
+      }
+    }
+    for (i64 r = hi + step; bestRing < 0 && r < (i64(1) << kRingOffBits); r += step)
+      if (place(r)) bestRing = r;
     if (bestRing < 0) fail(GR_EUNSUPPORTED, "ILU level ring too large");
-    R.ringBytes = bestRing;
-    if (!place(R.ringBytes)) fail(GR_EINVAL, "ILU level ring placement");
+    R.ringBytes = bestRing;  // the last placement pass was this size's
   }
   if (R.ringBytes > (i64(1) << kRingOffBits)) fail(GR_EUNSUPPORTED, "ILU level ring too large");
   R.group = group;
