@@ -125,6 +125,7 @@ SIGNATURES = {
     "gr_batch_create": (C.c_int, [P(vp), i32, C.c_char_p, P(vp)]),
     "gr_batch_solve_host": (C.c_int, [vp, P(vp), P(vp), C.c_int, P(Stats)]),
     "gr_batch_destroy": (None, [vp]),
+    "gr_selftest_wait_timeout": (C.c_int, [P(i32), P(i64)]),
     "gr_decompose_vector": (C.c_int, [vp, vp, vp, C.c_int]),
     "gr_compose_vector": (C.c_int, [vp, vp, vp, C.c_int]),
     "gr_solver_create": (C.c_int, [vp, C.c_char_p, P(vp)]),

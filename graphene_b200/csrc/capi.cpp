@@ -106,7 +106,10 @@ int gr_host_matrix_generate(gr_generator kind, int64_t nx, int64_t ny, int64_t n
                             gr_host_matrix** out) {
   return guarded([&] {
     need(out, "out");
+    GR_TRACE_SCOPE("gr_host_matrix_generate");
     gr::GeneratedCsr g;
+    {
+    GR_TRACE_SCOPE("generate CRS");
     switch (kind) {
       case GR_GEN_POISSON:
         g = gr::generatePoisson(nx, ny, nz);
@@ -122,6 +125,7 @@ int gr_host_matrix_generate(gr_generator kind, int64_t nx, int64_t ny, int64_t n
         break;
       default:
         gr::fail(GR_EINVAL, "unknown generator");
+    }
     }
     auto h = gr::HostMatrix::fromSortedCsr(g.n, std::move(g.rowPtr), std::move(g.col), std::move(g.val),
                                            num_tiles, partitioner, nullptr, std::move(g.coords),
@@ -638,5 +642,13 @@ int gr_batch_solve_host(gr_batch* b, void* const* x, const void* const* rhs, gr_
 }
 
 void gr_batch_destroy(gr_batch* b) { delete b; }
+
+int gr_selftest_wait_timeout(int32_t* status, int64_t* elapsed_ns) {
+  return guarded([&] {
+    need(status, "status");
+    need(elapsed_ns, "elapsed_ns");
+    gr::selftestWaitTimeout(status, elapsed_ns);
+  });
+}
 
 }  // extern "C"

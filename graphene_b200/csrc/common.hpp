@@ -54,6 +54,25 @@ inline DType toDType(int t) {
   return static_cast<DType>(t);
 }
 
+// Host tracing (the reference's GRAPHENE_TRACEPOINT, util/Tracepoint.hpp):
+// with GR_TRACE=1 in the environment, every traced scope prints its name and
+// wall time to stderr when it ends. Off, a scope costs one cached flag read.
+bool traceEnabled();
+class TraceScope {
+ public:
+  explicit TraceScope(const char* name);
+  ~TraceScope();
+  TraceScope(const TraceScope&) = delete;
+  TraceScope& operator=(const TraceScope&) = delete;
+
+ private:
+  const char* name_;
+  int64_t t0_ = -1;  // steady-clock ns at entry, -1 when tracing is off
+};
+#define GR_TRACE_CAT2(a, b) a##b
+#define GR_TRACE_CAT(a, b) GR_TRACE_CAT2(a, b)
+#define GR_TRACE_SCOPE(name) ::gr::TraceScope GR_TRACE_CAT(grTraceScope_, __LINE__)(name)
+
 // Number of host worker threads used by the host pipeline.
 inline int hostThreads() {
   unsigned h = std::thread::hardware_concurrency();

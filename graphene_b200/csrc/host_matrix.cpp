@@ -2,12 +2,36 @@
 #include "host_matrix.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <numeric>
 
 namespace gr {
+
+bool traceEnabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("GR_TRACE");
+    return v && *v && std::string(v) != "0";
+  }();
+  return on;
+}
+
+TraceScope::TraceScope(const char* name) : name_(name) {
+  if (traceEnabled())
+    t0_ = std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now().time_since_epoch())
+              .count();
+}
+
+TraceScope::~TraceScope() {
+  if (t0_ < 0) return;
+  const int64_t t1 =
+      std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  std::fprintf(stderr, "[graphene_b200] %s: %.3f ms\n", name_, static_cast<double>(t1 - t0_) * 1e-6);
+}
 
 namespace {
 
@@ -98,6 +122,8 @@ std::shared_ptr<HostMatrix> HostMatrix::fromSortedCsr(i64 n, std::vector<i64> ro
   A->valueType = valueType;
   A->n = n;
   A->coords = std::move(coords);
+  {
+  GR_TRACE_SCOPE("split diagonal");
   // Split off the diagonal (CRSHostMatrix.cpp:96-132). A missing diagonal
   // stays 0.
   std::vector<i64> offCount(n, 0);
@@ -136,6 +162,7 @@ std::shared_ptr<HostMatrix> HostMatrix::fromSortedCsr(i64 n, std::vector<i64> ro
   rowPtr.clear(); rowPtr.shrink_to_fit();
   col.clear(); col.shrink_to_fit();
   val.clear(); val.shrink_to_fit();
+  }
   A->buildFromGlobalCrs(numTiles, part, rowToTileIn);
   return A;
 }
@@ -143,9 +170,12 @@ std::shared_ptr<HostMatrix> HostMatrix::fromSortedCsr(i64 n, std::vector<i64> ro
 // ---------------------------------------------------------------------------
 // Partitioning and empty-part removal (CRSHostMatrix.cpp:139-271).
 void HostMatrix::buildFromGlobalCrs(i64 numTiles, gr_partitioner part, const i32* rowToTileIn) {
+  GR_TRACE_SCOPE("host layout (partition, tiles, local CRS, levels)");
   if (numTiles <= 0) fail(GR_EINVAL, "numTiles must be positive");
   if (numTiles > (i64(1) << 30)) fail(GR_EINVAL, "numTiles too large");
   std::vector<i32> raw;
+  {
+  GR_TRACE_SCOPE("partition");
   if (numTiles == 1 && part != GR_PART_EXPLICIT) {
     // Single tile: no partitioning (CRSHostMatrix.cpp:151-158).
     raw.assign(n, 0);
@@ -176,6 +206,7 @@ void HostMatrix::buildFromGlobalCrs(i64 numTiles, gr_partitioner part, const i32
         fail(GR_EINVAL, "unknown partitioner");
     }
   }
+  }
   // Remove empty parts, keeping the relative order of the others.
   std::vector<i64> perPart(numTiles, 0);
   for (i64 r = 0; r < n; ++r) perPart[raw[r]]++;
@@ -201,6 +232,7 @@ void HostMatrix::buildFromGlobalCrs(i64 numTiles, gr_partitioner part, const i32
 // loop over tiles runs sequentially (the reference's own order depends on
 // thread timing).
 void HostMatrix::buildTileLayout() {
+  GR_TRACE_SCOPE("tile layout");
   // Rows of each tile in ascending order.
   std::vector<i64> cnt(P, 0);
   for (i64 r = 0; r < n; ++r) cnt[rowToTile[r]]++;
@@ -301,6 +333,7 @@ void HostMatrix::buildTileLayout() {
 // values): each row's columns translated to tile-local ids and sorted by
 // them, so interior columns come first, then separator, then halo columns.
 void HostMatrix::buildLocalCrs() {
+  GR_TRACE_SCOPE("tile-local CRS");
   rowPtr.assign(n + 1, 0);
   for (i64 p = 0; p < n; ++p) {
     i64 g = iperm[p];
@@ -361,6 +394,7 @@ void HostMatrix::buildLocalCrs() {
 // valid schedule for unsymmetric ones. Upper levels are the same for the
 // upper-triangular DAG, used by the backward sweep.
 void HostMatrix::buildLevels() {
+  GR_TRACE_SCOPE("level sets");
   lowerLevel.assign(n, 0);
   upperLevel.assign(n, 0);
   nLowerLevels.assign(P, 0);
@@ -461,6 +495,31 @@ std::vector<i32> partitionContiguous(const HostMatrix& A, i32 numParts) {
 
 namespace {
 
+// Sorts v ascending by `less`: chunks sorted on the host threads, then
+// merged pairwise in parallel rounds. `less` must be a strict total order,
+// so that the result equals a sequential sort's.
+template <class T, class Less>
+void parallelSort(std::vector<T>& v, i64 b, i64 e, Less less) {
+  const i64 n = e - b;
+  int P = 1;
+  while (P * 2 <= hostThreads() && P < 64) P *= 2;
+  if (n < (i64(1) << 17) || P == 1) {
+    std::sort(v.begin() + b, v.begin() + e, less);
+    return;
+  }
+  std::vector<i64> cut(P + 1);
+  for (int t = 0; t <= P; ++t) cut[t] = b + n * t / P;
+  parallelFor(P, [&](i64 t) { std::sort(v.begin() + cut[t], v.begin() + cut[t + 1], less); });
+  std::vector<T> tmp(static_cast<size_t>(n));
+  for (int width = 1; width < P; width *= 2) {
+    parallelFor(P / (2 * width), [&](i64 j) {
+      const i64 lo = cut[2 * width * j], mid = cut[2 * width * j + width], hi = cut[2 * width * (j + 1)];
+      std::merge(v.begin() + lo, v.begin() + mid, v.begin() + mid, v.begin() + hi, tmp.begin() + (lo - b), less);
+    });
+    std::copy(tmp.begin(), tmp.end(), v.begin() + b);
+  }
+}
+
 void rcbRec(const HostMatrix& A, i64* rows, i64 cnt, i32 parts, i32 first, i32* out, int depth) {
   if (parts == 1) {
     for (i64 i = 0; i < cnt; ++i) out[rows[i]] = first;
@@ -478,10 +537,14 @@ void rcbRec(const HostMatrix& A, i64* rows, i64 cnt, i32 parts, i32 first, i32* 
   int axis = 0;
   for (int d = 1; d < 3; ++d)
     if (hi[d] - lo[d] > hi[axis] - lo[axis]) axis = d;
-  std::sort(rows, rows + cnt, [&](i64 a, i64 b) {
-    double ca = c[3 * a + axis], cb = c[3 * b + axis];
-    return ca < cb || (ca == cb && a < b);
-  });
+  // Rows by (coordinate along the axis, row), sorted as contiguous
+  // (key, row) pairs.
+  {
+    std::vector<std::pair<double, i64>> kv(cnt);
+    for (i64 i = 0; i < cnt; ++i) kv[i] = {c[3 * rows[i] + axis], rows[i]};
+    parallelSort(kv, 0, cnt, std::less<std::pair<double, i64>>());
+    for (i64 i = 0; i < cnt; ++i) rows[i] = kv[i].second;
+  }
   i32 p1 = parts / 2;
   auto w = [&](i64 i) { return vertexWeight(A, rows[i]); };
   i64 s = weightedSplit(cnt, p1, parts, w);

@@ -439,6 +439,15 @@ int gr_batch_create(gr_host_matrix* const* systems, int32_t count, const char* j
 int gr_batch_solve_host(gr_batch* b, void* const* x, const void* const* rhs, gr_dtype t, gr_stats* stats);
 void gr_batch_destroy(gr_batch* b);
 
+/* ---- self-test ----------------------------------------------------------
+ * No counterpart in the reference. Every wait of this library's pipelined
+ * kernels on an mbarrier (a copy landing, a level released) is bounded: after
+ * 1 s it gives up, the kernel records GR_ETIMEOUT and exits. This runs that
+ * wait on a barrier nothing arrives on and writes the status the kernel
+ * reported (GR_ETIMEOUT when the bound works) and how long it waited (ns);
+ * the device stays usable. Takes about a second. */
+int gr_selftest_wait_timeout(int32_t* status, int64_t* elapsed_ns);
+
 #ifdef __cplusplus
 }
 #endif
