@@ -150,36 +150,32 @@ void checkIluStream(const HostMatrix& H, const HostStream& S, bool dilu, DType v
 // tile, the levels in execution order (lower ascending, then upper
 // descending). A level block (every segment 16-byte padded) is, in the
 // compact layout (blocks of at most 65535 rows):
-//   cnt   E x u16: cnt[e] = rows with more than e entries
-//   rows  k x u16 block-local row ids, by entry count descending
+//   rows  k x u16 block-local row ids
 //   inv   k x value type inverse diagonal (upper levels, DILU)
-//   cols  sum(cnt) x u16: entry e of row q (q < cnt[e]) at cnt[0] + ... +
-//         cnt[e - 1] + q
-//   vals  sum(cnt) x value type, in the same places
-// so no row is padded; and otherwise (the wide layout):
+//   cols  E*k x u16 columns, entry-major
+//   vals  E*k x value type, entry-major
+// and otherwise (the wide layout):
 //   rows  k x i32
 //   inv   k x value type (upper levels, DILU)
 //   ents  E*k entries, entry-major, {i32 column, value}: 8 bytes for float,
-//         16 for double ({column, 0, value}); rows with fewer than E entries
-//         are padded with column nRows (a zero slot of the kernel's x slice)
-//         and value 0.
-// One int4 per level (RingLevelCode): k; E, the values' offset (wide: the
-// entries') and the sweep; the ring offset and the block's size;
-// issueAfter. The kernel copies a level's block into its shared-memory ring
-// at `ring offset` once the tile's level `issueAfter` has been consumed (-1:
-// at the start); the host chose the offsets so that a copy never overwrites
-// a level still to be consumed, and so that every level is copied at least
-// one level before it is needed.
+//         16 for double ({column, 0, value})
+// Padding entries use column nRows (a zero slot of the kernel's x slice) and
+// value 0. One int4 per level (RingLevelCode): k; E, the entries' offset
+// and the sweep; the ring offset and the block's size; issueAfter. The
+// kernel copies a level's block into its shared-memory ring at `ring offset`
+// once the tile's level `issueAfter` has been consumed (-1: at the start);
+// the host chose the offsets so that a copy never overwrites a level still
+// to be consumed, and so that every level is copied at least one level
+// before it is needed.
 constexpr int kRingBarriers = 16;
 constexpr int kRingUpperBit = 1 << 30;
-constexpr long long kRingCompactRows = 65535;  // largest block (rows + zero slot) of the compact layout
-// Field packing of a level's int4: y = E | (values offset / 16) << 14 |
+// Field packing of a level's int4: y = E | (entries offset / 16) << 14 |
 // upper << 30, z = ring offset | (block bytes / 16) << 18.
 constexpr int kRingEBits = 14, kRingOffBits = 18;
 struct RingLevelCode {
   __host__ __device__ static int k(const int4 m) { return m.x; }
   __host__ __device__ static int E(const int4 m) { return m.y & ((1 << kRingEBits) - 1); }
-  __host__ __device__ static uint32_t values(const int4 m) {
+  __host__ __device__ static uint32_t ents(const int4 m) {
     return ((static_cast<uint32_t>(m.y) >> kRingEBits) & 0xFFFFu) << 4;
   }
   __host__ __device__ static bool upper(const int4 m) { return (m.y & kRingUpperBit) != 0; }
@@ -189,30 +185,26 @@ struct RingLevelCode {
   __host__ __device__ static uint32_t bytes(const int4 m) { return (static_cast<uint32_t>(m.z) >> kRingOffBits) << 4; }
   __host__ __device__ static int issueAfter(const int4 m) { return m.w; }
 };
+constexpr long long kRingCompactRows = 65535;  // largest block (rows + zero slot) of the compact layout
 
-// Byte offsets of a level block's segments and its size. T: the entries
-// stored (compact: the sum of cnt; wide: E * k).
+// Byte offsets of a level block's inverse diagonal, entries (columns, or
+// column/value pairs) and values, and its size.
 struct RingLevelLayout {
-  uint32_t rows, inv, ents, vals, bytes;
+  uint32_t inv, ents, vals, bytes;
 };
-__host__ __device__ inline uint32_t ringPad16(uint32_t b) { return (b + 15u) & ~15u; }
-__host__ __device__ inline RingLevelLayout ringLevelLayout(uint32_t k, uint32_t E, uint32_t T, bool hasInv,
-                                                           uint32_t valueBytes, bool compact) {
-  RingLevelLayout l;
+__host__ __device__ inline RingLevelLayout ringLevelLayout(uint32_t k, uint32_t E, bool hasInv, uint32_t valueBytes,
+                                                           bool compact) {
+  const uint32_t idB = compact ? 2u : 4u;
+  const uint32_t rowsB = (idB * k + 15u) & ~15u;
+  const uint32_t invB = hasInv ? ((valueBytes * k + 15u) & ~15u) : 0u;
   if (compact) {
-    l.rows = ringPad16(2u * E);
-    l.inv = l.rows + ringPad16(2u * k);
-    l.ents = l.inv + (hasInv ? ringPad16(valueBytes * k) : 0u);
-    l.vals = l.ents + ringPad16(2u * T);
-    l.bytes = l.vals + ringPad16(valueBytes * T);
-  } else {
-    l.rows = 0;
-    l.inv = ringPad16(4u * k);
-    l.ents = l.inv + (hasInv ? ringPad16(valueBytes * k) : 0u);
-    l.vals = l.ents;
-    l.bytes = l.ents + ringPad16((valueBytes == 4 ? 8u : 16u) * T);
+    const uint32_t colsB = (2u * E * k + 15u) & ~15u;
+    const uint32_t valsB = (valueBytes * E * k + 15u) & ~15u;
+    return RingLevelLayout{rowsB, rowsB + invB, rowsB + invB + colsB, rowsB + invB + colsB + valsB};
   }
-  return l;
+  const uint32_t entBytes = valueBytes == 4 ? 8u : 16u;
+  const uint32_t entB = (entBytes * E * k + 15u) & ~15u;
+  return RingLevelLayout{rowsB, rowsB + invB, rowsB + invB, rowsB + invB + entB};
 }
 
 // What the default ring size is chosen for: the SM count, shared memory per

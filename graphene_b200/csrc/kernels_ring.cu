@@ -64,77 +64,58 @@ __device__ __forceinline__ void loadEntry<double>(const unsigned char* p, int& c
   v = __hiloint2double(e.w, e.z);
 }
 
-// A level of the ring as the compute warps see it (layouts: device.hpp).
+// A level of the ring as the compute warps see it.
 template <class MV, bool COMPACT>
 struct RingLevel {
   int k, E;
   bool upper;
-  const unsigned char* blk;        // the level block in the ring
-  uint32_t rows, inv, ents, vals;  // segment offsets
+  const unsigned char* blk;  // the level block in the ring
+  uint32_t inv, ents, vals;  // offsets of its inverse diagonal, entries (columns) and values
   __device__ __forceinline__ int row(int q) const {
-    return COMPACT ? static_cast<int>(reinterpret_cast<const uint16_t*>(blk + rows)[q])
-                   : reinterpret_cast<const int*>(blk)[q];
+    return COMPACT ? static_cast<int>(reinterpret_cast<const uint16_t*>(blk)[q]) : reinterpret_cast<const int*>(blk)[q];
   }
   __device__ __forceinline__ MV invDiag(int q) const { return reinterpret_cast<const MV*>(blk + inv)[q]; }
-  // Compact: rows with more than e entries.
-  __device__ __forceinline__ int count(int e) const {
-    return static_cast<int>(reinterpret_cast<const uint16_t*>(blk)[e]);
-  }
-  // The entry stored in `slot`.
-  __device__ __forceinline__ void entryAt(int slot, int& c, MV& v) const {
+  // Entry e of row q.
+  __device__ __forceinline__ void entry(int e, int q, int& c, MV& v) const {
+    const int idx = e * k + q;
     if (COMPACT) {
-      c = reinterpret_cast<const uint16_t*>(blk + ents)[slot];
-      v = reinterpret_cast<const MV*>(blk + vals)[slot];
+      c = reinterpret_cast<const uint16_t*>(blk + ents)[idx];
+      v = reinterpret_cast<const MV*>(blk + vals)[idx];
     } else {
-      loadEntry<MV>(blk + ents + (sizeof(MV) == 4 ? 8 : 16) * slot, c, v);
+      loadEntry<MV>(blk + ents + (sizeof(MV) == 4 ? 8 : 16) * idx, c, v);
     }
   }
 };
-// The level's view from its table entry (RingLevelCode).
+// The level's view from its table entry (RingLevelCode): the inverse
+// diagonal follows the row ids, the values (compact layout) the columns.
 template <class MV, bool COMPACT>
-__device__ __forceinline__ RingLevel<MV, COMPACT> ringLevelAt(const int4 m, const unsigned char* ring, bool dilu) {
+__device__ __forceinline__ RingLevel<MV, COMPACT> ringLevelAt(const int4 m, const unsigned char* ring) {
   RingLevel<MV, COMPACT> lv;
   lv.k = RingLevelCode::k(m);
   lv.E = RingLevelCode::E(m);
   lv.upper = RingLevelCode::upper(m);
   lv.blk = ring + RingLevelCode::ringOffset(m);
-  lv.vals = RingLevelCode::values(m);
-  const uint32_t k = static_cast<uint32_t>(lv.k);
-  lv.rows = COMPACT ? ringPad16(2u * static_cast<uint32_t>(lv.E)) : 0u;
-  lv.inv = lv.rows + ringPad16((COMPACT ? 2u : 4u) * k);
-  lv.ents = COMPACT ? lv.inv + ((lv.upper || dilu) ? ringPad16(static_cast<uint32_t>(sizeof(MV)) * k) : 0u) : lv.vals;
+  lv.inv = ((COMPACT ? 2u : 4u) * static_cast<uint32_t>(lv.k) + 15u) & ~15u;
+  lv.ents = RingLevelCode::ents(m);
+  lv.vals = COMPACT ? lv.ents + ((2u * static_cast<uint32_t>(lv.E) * static_cast<uint32_t>(lv.k) + 15u) & ~15u)
+                    : lv.ents;
   return lv;
 }
 
-// temp -= sum_e value_e * xs[column_e] over row q's entries in order. Rows
-// with fewer entries than the level's E are padded (wide layout: column =
-// the zero slot, value 0) or simply end early (compact layout); either way
-// the missing terms leave temp unchanged. Rows of up to four entries load
-// all their entries, then all x values, before the arithmetic.
+// temp -= sum_e value_e * xs[column_e] over row q's E entries in order.
+// Padding entries (column = the zero slot, value 0) leave temp unchanged.
+// Rows of up to four entries load all their entries, then all x values,
+// before the arithmetic.
 template <bool UNROLL, class MV, bool COMPACT, class W>
 __device__ __forceinline__ W ringRowDot(W temp, const RingLevel<MV, COMPACT>& lv, int q, int zeroSlot,
                                         const W* xs) {
   if (UNROLL && lv.E <= 4) {
     int c[4];
     MV v[4];
-    int off = 0;
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
-      bool has = false;
-      int slot = 0;
       if (e < lv.E) {
-        if (COMPACT) {
-          const int n = lv.count(e);
-          has = q < n;
-          slot = off + q;
-          off += n;
-        } else {
-          has = true;
-          slot = e * lv.k + q;
-        }
-      }
-      if (has) {
-        lv.entryAt(slot, c[e], v[e]);
+        lv.entry(e, q, c[e], v[e]);
       } else {
         c[e] = zeroSlot;
         v[e] = MV(0);
@@ -148,20 +129,10 @@ __device__ __forceinline__ W ringRowDot(W temp, const RingLevel<MV, COMPACT>& lv
       if (e < lv.E) temp = sub(temp, mul(cvt<W>(v[e]), xv[e]));
     return temp;
   }
-  int off = 0;
   for (int e = 0; e < lv.E; ++e) {
-    int slot;
-    if (COMPACT) {
-      const int n = lv.count(e);
-      if (q >= n) break;
-      slot = off + q;
-      off += n;
-    } else {
-      slot = e * lv.k + q;
-    }
     int c;
     MV v;
-    lv.entryAt(slot, c, v);
+    lv.entry(e, q, c, v);
     temp = sub(temp, mul(cvt<W>(v), xs[c]));
   }
   return temp;
@@ -293,7 +264,7 @@ __global__ void __launch_bounds__(RingShape<W>::threads) iluRingKernel(const uns
     bool stop = namedBarOr(1, kRingLevelSync, false);
     for (int l = 0; !stop && l < L; ++l) {
       const int4 m = mt[l];
-      const RingLevel<MV, COMPACT> cur = ringLevelAt<MV, COMPACT>(m, ring, dilu);
+      const RingLevel<MV, COMPACT> cur = ringLevelAt<MV, COMPACT>(m, ring);
       if (!cur.upper) {
         // Forward substitution (ilu/Solver.cpp:380-411).
         for (int q = threadIdx.x; q < cur.k; q += kRingCompute) {

@@ -388,7 +388,6 @@ struct TileRing {
   std::vector<std::pair<i64, i32>> vals;  // (byte offset of the value, CRS source)
   std::vector<std::pair<i64, i32>> invs;  // (byte offset, tile-order row)
   std::vector<i64> size;
-  std::vector<i64> stored;  // entries stored per level (compact: without padding)
   i64 maxLevel = 0;
 };
 
@@ -415,6 +414,7 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
     const i32 T0 = static_cast<i32>(G) * group, T1 = std::min<i32>(H.P, T0 + group);
     const i64 gBase = H.tileStart[T0];
     const i64 gRows = H.tileStart[T1] - gBase;
+    std::vector<i64> ent;
     for (int sweep = 0; sweep < 2; ++sweep) {
       const bool upper = sweep == 1;
       const SweepEntries kind = upper ? SweepEntries::UpperDesc : SweepEntries::Lower;
@@ -426,76 +426,48 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
       for (i32 T = T0; T < T1; ++T)
         for (i64 p = H.tileStart[T]; p < H.tileStart[T + 1]; ++p) byLevel[lev[p]].emplace_back(p - gBase, T);
       const bool hasInv = upper || dilu;
-      std::vector<std::vector<i64>> rowEnt;
-      std::vector<i64> cnt;
       for (i32 l = 0; l < nLv; ++l) {
-        auto rows = byLevel[l];
+        const auto& rows = byLevel[l];
         const i64 k = static_cast<i64>(rows.size());
-        rowEnt.assign(k, {});
         i64 E = 0;
-        for (i64 q = 0; q < k; ++q) {
-          const auto [gl, T] = rows[q];
+        for (const auto& [gl, T] : rows) {
           const i64 tb = H.tileStart[T] - gBase;
-          rowEntries(H, kind, gBase + gl, gl - tb, H.tileStart[T + 1] - H.tileStart[T], rowEnt[q]);
-          E = std::max<i64>(E, static_cast<i64>(rowEnt[q].size()));
+          rowEntries(H, kind, gBase + gl, gl - tb, H.tileStart[T + 1] - H.tileStart[T], ent);
+          E = std::max<i64>(E, static_cast<i64>(ent.size()));
         }
         if (E >= (i64(1) << kRingEBits) || k >= (i64(1) << 31) || entSize * E * k >= (i64(1) << 31))
           fail(GR_EUNSUPPORTED, "ILU level too large for the ring kernel");
-        // Compact layout: rows by entry count, descending (rows of a level
-        // are independent, so their order within it does not matter), and
-        // cnt[e] = rows with more than e entries.
-        std::vector<i64> order(k);
-        for (i64 q = 0; q < k; ++q) order[q] = q;
-        if (compact)
-          std::stable_sort(order.begin(), order.end(),
-                           [&](i64 a, i64 b) { return rowEnt[a].size() > rowEnt[b].size(); });
-        cnt.assign(E, 0);
-        for (i64 q = 0; q < k; ++q)
-          for (i64 e = 0; e < static_cast<i64>(rowEnt[q].size()); ++e) ++cnt[e];
-        i64 stored = 0;
-        for (i64 e = 0; e < E; ++e) stored += compact ? cnt[e] : k;
-        const RingLevelLayout lay =
-            ringLevelLayout(static_cast<uint32_t>(k), static_cast<uint32_t>(E), static_cast<uint32_t>(stored), hasInv,
-                            static_cast<uint32_t>(vs), compact);
+        const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(k), static_cast<uint32_t>(E), hasInv,
+                                                    static_cast<uint32_t>(vs), compact);
         const i64 S = lay.bytes;
         const i64 start = static_cast<i64>(t.bytes.size());
         t.bytes.resize(start + S, 0);
-        if (compact)
-          for (i64 e = 0; e < E; ++e) {
-            const uint16_t c16 = static_cast<uint16_t>(cnt[e]);
-            std::memcpy(t.bytes.data() + start + 2 * e, &c16, 2);
-          }
-        std::vector<i64> eOff(E, 0);  // compact: first stored slot of entry e
-        for (i64 e = 1; e < E; ++e) eOff[e] = eOff[e - 1] + cnt[e - 1];
         for (i64 q = 0; q < k; ++q) {
-          const auto [gl, T] = rows[order[q]];
-          const std::vector<i64>& ent = rowEnt[order[q]];
+          const auto [gl, T] = rows[q];
           const i64 tb = H.tileStart[T] - gBase;
           if (compact) {
             const uint16_t r16 = static_cast<uint16_t>(gl);
-            std::memcpy(t.bytes.data() + start + lay.rows + 2 * q, &r16, 2);
+            std::memcpy(t.bytes.data() + start + 2 * q, &r16, 2);
           } else {
             const i32 r32 = static_cast<i32>(gl);
             std::memcpy(t.bytes.data() + start + 4 * q, &r32, 4);
           }
           if (hasInv) t.invs.emplace_back(start + lay.inv + vs * q, static_cast<i32>(gBase + gl));
+          rowEntries(H, kind, gBase + gl, gl - tb, H.tileStart[T + 1] - H.tileStart[T], ent);
           for (i64 e = 0; e < E; ++e) {
             const bool real = e < static_cast<i64>(ent.size());
+            const i32 col = real ? static_cast<i32>(H.colLocal[ent[e]] + tb) : static_cast<i32>(gRows);
             if (compact) {
-              if (!real) break;  // counts descend: q >= cnt[e] for the rest
-              const uint16_t c16 = static_cast<uint16_t>(H.colLocal[ent[e]] + tb);
-              const i64 slot = eOff[e] + q;
-              std::memcpy(t.bytes.data() + start + lay.ents + 2 * slot, &c16, 2);
-              t.vals.emplace_back(start + lay.vals + vs * slot, static_cast<i32>(ent[e]));
+              const uint16_t c16 = static_cast<uint16_t>(col);
+              std::memcpy(t.bytes.data() + start + lay.ents + 2 * (e * k + q), &c16, 2);
+              if (real) t.vals.emplace_back(start + lay.vals + vs * (e * k + q), static_cast<i32>(ent[e]));
             } else {
-              const i32 col = real ? static_cast<i32>(H.colLocal[ent[e]] + tb) : static_cast<i32>(gRows);
               const i64 pos = start + lay.ents + entSize * (e * k + q);
               std::memcpy(t.bytes.data() + pos, &col, 4);
               if (real) t.vals.emplace_back(pos + (vs == 4 ? 4 : 8), static_cast<i32>(ent[e]));
             }
           }
         }
-        t.stored.push_back(stored);
         t.meta.push_back(make_int4(static_cast<int>(k), static_cast<int>(E) | (upper ? kRingUpperBit : 0), 0, -1));
         t.size.push_back(S);
         t.maxLevel = std::max(t.maxLevel, S);
@@ -638,9 +610,9 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
       int4 m = tr[T].meta[l];
       const bool upper = (m.y & kRingUpperBit) != 0;
       const uint32_t E = static_cast<uint32_t>(m.y & (kRingUpperBit - 1));
-      const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(m.x), E, static_cast<uint32_t>(tr[T].stored[l]),
-                                                  upper || dilu, static_cast<uint32_t>(vs), compact);
-      m.y = static_cast<int>(E | ((lay.vals >> 4) << kRingEBits) | (upper ? static_cast<uint32_t>(kRingUpperBit) : 0u));
+      const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(m.x), E, upper || dilu,
+                                                  static_cast<uint32_t>(vs), compact);
+      m.y = static_cast<int>(E | ((lay.ents >> 4) << kRingEBits) | (upper ? static_cast<uint32_t>(kRingUpperBit) : 0u));
       m.z = static_cast<int>(static_cast<uint32_t>(m.z) | ((lay.bytes >> 4) << kRingOffBits));
       R.meta[static_cast<size_t>(R.tileLevel[T]) + l] = m;
     }
@@ -690,33 +662,19 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
       const bool upper = RingLevelCode::upper(a);
       if (upper != (l >= nLower)) bad(G, l, "sweep flag");
       const bool hasInv = upper || dilu;
-      if (k < 1 || E < 0) bad(G, l, "block layout");
-      if (src + 2 * E > static_cast<i64>(R.bytes.size())) bad(G, l, "source range");
-      // Compact: the per-entry row counts, non-increasing, at most k.
-      std::vector<i64> cnt(E, k), eOff(E, 0);
-      i64 T = E * k;
-      if (R.compact) {
-        T = 0;
-        for (i64 e = 0; e < E; ++e) {
-          uint16_t c16;
-          std::memcpy(&c16, R.bytes.data() + src + 2 * e, 2);
-          cnt[e] = c16;
-          if (cnt[e] > k || (e > 0 && cnt[e] > cnt[e - 1]) || cnt[e] < 1) bad(G, l, "entry counts");
-          eOff[e] = T;
-          T += cnt[e];
-        }
-      }
-      const i64 rowsB = R.compact ? pad16(2 * E) : 0;
-      const i64 invOff = rowsB + pad16((R.compact ? 2 : 4) * k);
-      const i64 entOff = invOff + (hasInv ? pad16(vs * k) : 0);
-      const i64 valOff = R.compact ? entOff + pad16(2 * T) : entOff;
-      const i64 S = R.compact ? valOff + pad16(vs * T) : entOff + pad16(entSize * T);
-      if (S > R.ringBytes) bad(G, l, "block layout");
-      const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(k), static_cast<uint32_t>(E),
-                                                  static_cast<uint32_t>(T), hasInv, static_cast<uint32_t>(vs), R.compact);
-      if (lay.rows != rowsB || lay.inv != invOff || lay.ents != entOff || lay.vals != valOff || lay.bytes != S ||
-          RingLevelCode::values(a) != lay.vals || RingLevelCode::bytes(a) != lay.bytes)
+      const i64 idB = R.compact ? 2 : 4;
+      const i64 rowsB = pad16(idB * k), invB = hasInv ? pad16(vs * k) : 0;
+      const i64 colsB = R.compact ? pad16(2 * E * k) : pad16(entSize * E * k);
+      const i64 valsB = R.compact ? pad16(vs * E * k) : 0;
+      const i64 S = rowsB + invB + colsB + valsB;
+      if (k < 1 || E < 0 || S > R.ringBytes) bad(G, l, "block layout");
+      const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(k), static_cast<uint32_t>(E), hasInv,
+                                                  static_cast<uint32_t>(vs), R.compact);
+      if (lay.inv != rowsB || lay.ents != rowsB + invB || lay.bytes != S ||
+          lay.vals != (R.compact ? rowsB + invB + colsB : rowsB + invB) || RingLevelCode::ents(a) != lay.ents ||
+          RingLevelCode::bytes(a) != lay.bytes)
         bad(G, l, "block layout");
+      const i64 entOff = rowsB + invB;
       if (off < 0 || off % 16 != 0 || off + S > R.ringBytes) bad(G, l, "ring offset");
       if (ia < -1 || ia < prevIa || ia < l - kRingBarriers || (l >= 1 && ia > l - 2) || (l == 0 && ia != -1))
         bad(G, l, "copy order");
@@ -733,7 +691,7 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
         i32 il;
         if (R.compact) {
           uint16_t r16;
-          std::memcpy(&r16, blk + rowsB + 2 * q, 2);
+          std::memcpy(&r16, blk + 2 * q, 2);
           il = r16;
         } else {
           std::memcpy(&il, blk + 4 * q, 4);
@@ -743,9 +701,8 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
         for (i64 e = 0; e < E; ++e) {
           i32 c;
           if (R.compact) {
-            if (q >= cnt[e]) break;  // row q has no entry e or later
             uint16_t c16;
-            std::memcpy(&c16, blk + entOff + 2 * (eOff[e] + q), 2);
+            std::memcpy(&c16, blk + entOff + 2 * (e * k + q), 2);
             c = c16;
           } else {
             std::memcpy(&c, blk + entOff + entSize * (e * k + q), 4);
