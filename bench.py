@@ -48,6 +48,17 @@ FALLBACK_HBM = 6650.0
 SEED_MATRIX, SEED_X = 2, 3
 
 
+def max_over_ranks(value, dist=None, device="cuda"):
+    """The largest `value` over the ranks of the process group, for timing a
+    multi-GPU run as its slowest rank (`value` itself without a group)."""
+    if dist is None or not dist.is_initialized():
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def parse_args():
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument("--gpus", type=int, default=1)
@@ -507,11 +518,7 @@ def main():
     barrier()
     launches = gb.launch_count() - launches0
     clk.mark_end()
-    total = sum(step_ms)
-    if dist:
-        t = torch.tensor([total], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
+    total = max_over_ranks(sum(step_ms), dist)
     ms_per_step = total / a.steps
     st = stats[-1]
     phi = s.phi(gb.FLOAT64)
