@@ -73,6 +73,9 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true")
     p.add_argument("--cpu-threads", type=int, default=0)
+    p.add_argument("--case", choices=sorted(CASES), default=None,
+                   help="run one benchmark configuration alone (timing and profiling): "
+                        "W untimed + K timed solves of it, one JSON line")
     return p.parse_args()
 
 
@@ -98,6 +101,15 @@ FP64_CONFIG = {"type": "PBiCGStab", "maxIterations": 20000, "relResidual": 1e-10
 def workload_name(a, n, m):
     return (f"MPIR(FP64 residual+update) over FP32 PBiCGStab-ILU(0), var-coeff 7-pt Poisson "
             f"{a.grid}^3 (n={n}, offdiag={m}), sigma={a.sigma}, {a.tiles} tiles, to 1e-10")
+
+
+def bench_config(a, world):
+    """The `config` of both arms' JSON lines (identical by construction)."""
+    g = a.grid
+    n, m = g ** 3, 6 * g * g * (g - 1)  # 7-point stencil: 2 x 3 (g - 1) g^2 off-diagonals
+    return {"workload": workload_name(a, n, m), "tiles": a.tiles, "inner_rel_residual": a.inner_tol,
+            "parallelism": "replicas" if world > 1 else "single GPU",
+            "l2": "inputs larger than L2 (no flush)"}
 
 
 class ClockSampler:
@@ -163,13 +175,18 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def oracle_for(h, threads):
+def oracle_system(a, threads):
+    """The headline system built by the oracle alone (its own generator,
+    coordinate bisection and seeded vectors; no part of the product
+    library): (oracle matrix, b in tile order, float32)."""
+    import numpy as np
     from tests.oracle_py import Oracle
 
     o = Oracle()
     o.threads(threads)
-    rows, cols, vals = h.coo()
-    return o.matrix(h.numRows, rows, cols, vals, h.numTiles, h.rowToTile(), 0)
+    om = o.grid_system(1, a.grid, a.grid, a.grid, (a.sigma,), SEED_MATRIX, a.tiles)
+    xt = o.random_vector(SEED_X, om.n).astype(np.float32)
+    return om, om.spmv(om.decompose(xt))
 
 
 def oracle_sample(om, b_tile, k=3):
@@ -191,40 +208,45 @@ def oracle_sample(om, b_tile, k=3):
 
 
 def reference_arm(a):
-    """The CPU oracle on the host cores (rank 0 only)."""
+    """The CPU oracle on the host cores (rank 0 only). Everything it runs is
+    the oracle's: the system (generator, bisection, seeded x_true, b = A x in
+    FP32) and the MPIR solve. One full solve is measured for the iteration
+    counts and as a check; each of the W + K steps is a bounded sample of
+    the same solve (ILU(0) factorisation, 3 PBiCGStab-ILU(0) iterations, one
+    FP64 residual), and `value` scales the timed steps' median sample to the
+    full solve's iteration counts."""
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
     import numpy as np
-    import graphene_b200 as gb
 
     threads = a.cpu_threads or os.cpu_count() or 1
-    h = gb.generateMatrix(gb.GEN_VAR_POISSON, a.grid, a.grid, a.grid, (a.sigma,), SEED_MATRIX, a.tiles)
-    om = oracle_for(h, threads)
-    xt = gb.randomVector(SEED_X, h.numRows).astype(np.float32)
-    b = om.spmv(h.decomposeVector(xt))
-    # One full MPIR solve: the measured CPU time-to-solution and iteration counts.
+    om, b = oracle_system(a, threads)
     t0 = time.perf_counter()
     _, st, _, _ = om.solve(json.dumps(mpir_config(a)), np.zeros_like(b), b)
-    full_s = time.perf_counter() - t0
-    samples = []
+    full_ms = (time.perf_counter() - t0) * 1e3
+    samples, step_ms = [], []
     for step in range(a.warmup + a.steps):
+        t0 = time.perf_counter()
         s = oracle_sample(om, b)
         if step >= a.warmup:
             samples.append(s)
+            step_ms.append((time.perf_counter() - t0) * 1e3)
     t_fact = statistics.median(x[0] for x in samples)
     t_iter = statistics.median(x[1] for x in samples)
     t_res = statistics.median(x[2] for x in samples)
-    projected_ms = (t_fact + st.inner_iterations * t_iter + st.iterations * t_res) * 1e3
-    value = full_s * 1e3
-    sample = (f"one full oracle MPIR solve ({st.iterations} outer / {st.inner_iterations} inner "
-              f"iterations, converged={bool(st.converged)}) measured on {threads} threads; each step: "
-              f"ILU(0) factorisation + 3 PBiCGStab-ILU(0) iterations + one FP64 residual "
-              f"({t_fact:.2f} s, {t_iter:.3f} s/iter, {t_res:.3f} s), projecting {projected_ms:.0f} ms")
+    value = (t_fact + st.inner_iterations * t_iter + st.iterations * t_res) * 1e3
+    sample = (f"each step: ILU(0) factorisation + 3 PBiCGStab-ILU(0) iterations + one FP64 residual of the "
+              f"oracle on the full system, {threads} threads ({t_fact:.2f} s, {t_iter:.3f} s/iteration, "
+              f"{t_res:.3f} s); value = those medians scaled to the full solve's {st.iterations} outer / "
+              f"{st.inner_iterations} inner iterations; one full solve measured {full_ms:.0f} ms "
+              f"(converged={bool(st.converged)})")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "ms",
             "higher_is_better": False, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": statistics.mean(x[0] + 3 * x[1] + x[2] for x in samples) * 1e3,
+            "ms_per_step": statistics.mean(step_ms), "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 inner / f64 outer", "data": "synthetic (seeded generator)",
-            "config": {"workload": workload_name(a, h.numRows, h.numOffDiag), "tiles": h.numTiles},
+            "config": bench_config(a, int(os.environ.get("WORLD_SIZE", "1"))),
+            "full_solve_ms": full_ms, "outer_iterations": st.iterations,
+            "inner_iterations": st.inner_iterations,
             "cpu_baseline": {"value": value, "unit": "ms", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -448,6 +470,105 @@ def batching(gb, systems=64, seed=11, reps=3):
             "all_converged": all(s.converged for s in st_bat)}
 
 
+def _case_c1(gb):
+    import numpy as np
+    h = gb.generate3DPoissonMatrix(gb.FLOAT32, 32, 32, 32, 64)
+    A = h.copyToTile()
+    b = A * A.vector(gb.randomVector(0, h.numRows).astype(np.float32))
+    return A, pbicgstab("ILU", 1e-6), b
+
+
+def _case_c2(pre, vt_name):
+    def build(gb):
+        import numpy as np
+        h = gb.generateMatrix(gb.GEN_CONVDIFF, 128, 128, 128, (0.5, 0.25, 0.125), 0, 1024)
+        vt = gb.FLOAT32 if vt_name == "f32" else gb.FLOAT64
+        hv = h if vt == gb.FLOAT32 else h.astype(gb.FLOAT64)
+        A = hv.copyToTile()
+        xt = gb.randomVector(1, h.numRows, "normal")
+        b = A * A.vector(xt.astype(np.float32 if vt == gb.FLOAT32 else np.float64))
+        return A, pbicgstab(pre, 1e-8, 2000), b
+    return build
+
+
+def _case_c3(kind):
+    def build(gb):
+        import numpy as np
+
+        class _A:  # the bench's own defaults
+            inner_maxit, inner_tol = 500, 1e-4
+        h = gb.generateMatrix(gb.GEN_VAR_POISSON, 192, 192, 192, (1.5,), SEED_MATRIX, 2048)
+        xt = gb.randomVector(SEED_X, h.numRows).astype(np.float32)
+        if kind == "fp64":
+            A = h.astype(gb.FLOAT64).copyToTile()
+            A32 = h.copyToTile()
+            b = (A32 * A32.vector(xt)).double()
+            del A32
+            return A, FP64_CONFIG, b
+        A = h.copyToTile()
+        b = A * A.vector(xt)
+        return A, mpir_config(_A, "twofloat32" if kind == "dw" else "float64"), b
+    return build
+
+
+def _case_c4(gb):
+    import numpy as np
+    h = gb.generateLduMesh(100, 100, 100, 4, 5, 6, numTiles=1024)
+    A = h.copyToTile()
+    b = A * A.vector(gb.randomVector(1, h.numRows, "normal").astype(np.float32))
+    return A, pbicgstab("GS", 1e-8, 260), b
+
+
+# One benchmark configuration each: (builder, description).
+CASES = {
+    "c1": (_case_c1, "32^3 Poisson, 64 tiles, FP32 PBiCGStab-ILU(0) to 1e-6"),
+    "c2-gs-f32": (_case_c2("GS", "f32"), "128^3 convection-diffusion, 1024 tiles, FP32 PBiCGStab-GS(2) to 1e-8"),
+    "c2-gs-f64": (_case_c2("GS", "f64"), "128^3 convection-diffusion, 1024 tiles, FP64 PBiCGStab-GS(2) to 1e-8"),
+    "c2-ilu-f32": (_case_c2("ILU", "f32"), "128^3 convection-diffusion, 1024 tiles, FP32 PBiCGStab-ILU(0) to 1e-8"),
+    "c2-ilu-f64": (_case_c2("ILU", "f64"), "128^3 convection-diffusion, 1024 tiles, FP64 PBiCGStab-ILU(0) to 1e-8"),
+    "c3-mpir": (_case_c3("mpir"), "192^3 var-coeff Poisson, 2048 tiles, MPIR FP64 outer / FP32 ILU inner"),
+    "c3-mpir-dw": (_case_c3("dw"), "192^3 var-coeff Poisson, 2048 tiles, MPIR double-word outer"),
+    "c3-fp64": (_case_c3("fp64"), "192^3 var-coeff Poisson, 2048 tiles, FP64 PBiCGStab-ILU(0) to 1e-10"),
+    "c4-gs-f32": (_case_c4, "100^3 LDU mesh, 1024 tiles, FP32 PBiCGStab-GS(2), 260 iterations at most"),
+}
+
+
+def run_case(a):
+    """W untimed and K timed solves (solver creation + solve, CUDA events) of
+    one configuration; one JSON line with the mean, iterations and the FP64
+    relative residual of the last solution."""
+    import torch
+    import graphene_b200 as gb
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    build, desc = CASES[a.case]
+    A, cfg, b = build(gb)
+    n = A.numRows
+
+    def once():
+        s = gb.Solver(A, cfg)
+        x = torch.zeros(n, dtype=b.dtype, device="cuda")
+        return s, x, s.solve(x, b)
+    for _ in range(a.warmup):
+        once()
+    torch.cuda.synchronize()
+    times, out = [], None
+    l0 = gb.launch_count()
+    for _ in range(a.steps):
+        out = None
+        ms, out = event_ms(once)
+        times.append(ms)
+    launches = gb.launch_count() - l0
+    s, x, st = out
+    xv = s.phi(gb.FLOAT64) if cfg["type"] == "IterativeRefinement" else x
+    r = A.residual(xv, b, destType=gb.FLOAT64, intermediateType=gb.FLOAT64)
+    rel = float(torch.linalg.vector_norm(r) / torch.linalg.vector_norm(b.double()))
+    print(json.dumps({"case": a.case, "workload": desc, "ms": statistics.mean(times) if times else None,
+                      "ms_each": times, "iterations": st.iterations, "inner_iterations": st.innerIterations,
+                      "converged": st.converged, "rel_residual_fp64": rel, "gpu_launches": launches,
+                      "steps": a.steps, "warmup": a.warmup}))
+    return 0
+
+
 def event_ms(fn):
     import torch
     e0 = torch.cuda.Event(enable_timing=True)
@@ -463,6 +584,8 @@ def main():
     a = parse_args()
     if a.impl == "reference":
         return reference_arm(a)
+    if a.case:
+        return run_case(a)
     import numpy as np
     import torch
     import graphene_b200 as gb
@@ -567,6 +690,7 @@ def main():
             extra[name] = {"ms": ms, "outer": sx.iterations, "inner": sx.innerIterations,
                            "converged": sx.converged, "rel_residual_fp64": rel64(A, sv.phi(gb.FLOAT64), b)}
             del sv, xv
+        extra["speedup_mpir_dw_vs_fp64"] = fp64_ms / extra["mpir_twofloat32"]["ms"]
         extra["configs"] = other_configs(gb, peak)
         extra["serving"] = serving(gb)
         extra["batching"] = batching(gb)
@@ -621,8 +745,8 @@ def main():
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             threads = a.cpu_threads or os.cpu_count() or 1
-            om = oracle_for(h, threads)
-            tf_, ti_, tr_ = oracle_sample(om, h.decomposeVector(A.toNatural(b)))
+            om, b_or = oracle_system(a, threads)
+            tf_, ti_, tr_ = oracle_sample(om, b_or)
             proj = (tf_ + inner * ti_ + st.iterations * tr_) * 1e3
             cpu = {"value": proj, "unit": "ms", "cores": threads, "kind": "port",
                    "sample": (f"oracle on the full {a.grid}^3 system ({threads} threads): ILU(0) "
@@ -631,8 +755,8 @@ def main():
                               f"solve's {inner} inner / {st.iterations} outer iterations")}
             if threads > 1:
                 # The same sample on one thread (one PBiCGStab iteration).
-                om1 = oracle_for(h, 1)
-                tf1, ti1, tr1 = oracle_sample(om1, h.decomposeVector(A.toNatural(b)), k=1)
+                om.o.threads(1)
+                tf1, ti1, tr1 = oracle_sample(om, b_or, k=1)
                 cpu["single_thread"] = {"value": (tf1 + inner * ti1 + st.iterations * tr1) * 1e3,
                                         "unit": "ms", "cores": 1,
                                         "sample": (f"factorisation {tf1:.2f} s + 1 iteration {ti1:.3f} s + "
@@ -646,10 +770,13 @@ def main():
         "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 outer",
         "data": "synthetic (seeded generator)",
-        "config": {"workload": workload_name(a, n, m), "tiles": h.numTiles,
-                   "inner_rel_residual": a.inner_tol,
-                   "parallelism": "replicas" if world > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (no flush)"},
+        "config": bench_config(a, world),
+        # The north-star comparison on the same GPU: plain FP64 PBiCGStab-ILU(0)
+        # to 1e-10, and MPIR with a double-word outer residual.
+        "fp64_ms": extra.get("fp64_pbicgstab_ilu0", {}).get("ms"),
+        "speedup_mpir_vs_fp64": extra.get("speedup_mpir_vs_fp64"),
+        "mpir_dw_ms": extra.get("mpir_twofloat32", {}).get("ms"),
+        "speedup_mpir_dw_vs_fp64": extra.get("speedup_mpir_dw_vs_fp64"),
         "solve": {"outer_iterations": st.iterations, "inner_iterations": inner,
                   "converged": st.converged, "rel_residual_fp64_of_phi": rel64(A, phi, b),
                   "p50_ms": statistics.median(step_ms), "p99_ms": max(step_ms),

@@ -102,6 +102,22 @@ typedef struct {
 int or_solve(const or_matrix* A, const char* json, void* x, int xt, const void* b, int bt,
              or_stats* stats, double* phi_out, double* history, int history_len);
 
+/* ---- seeded benchmark inputs (oracle/generators.cpp) ----------------------
+ * The benchmark's synthetic inputs, restated for the oracle so that its
+ * reference arm needs no part of the product library. */
+/* Triplet count of a 7-point matrix on an nx x ny x nz grid. */
+int64_t or_generate_nnz(int64_t nx, int64_t ny, int64_t nz);
+/* Triplets sorted by (row, column) and grid coordinates (3 per row,
+ * nullable) of kind 0 (constant Poisson, Poisson.cpp:26-69), 1
+ * (variable-coefficient Poisson, params[0] = sigma) or 2 (upwind
+ * convection-diffusion, params = velocity). */
+int or_generate(int kind, int64_t nx, int64_t ny, int64_t nz, const double* params, uint64_t seed,
+                int64_t* rows, int64_t* cols, double* vals, double* coords);
+/* Seeded vector: dist 0 uniform [lo, hi), 1 standard normal. */
+int or_random_vector(uint64_t seed, int64_t n, int dist, double lo, double hi, double* out);
+/* Recursive coordinate bisection into `parts` parts (raw part ids). */
+int or_partition_rcb(int64_t n, const double* coords, const int64_t* weights, int32_t parts, int32_t* out);
+
 #ifdef __cplusplus
 }
 #endif

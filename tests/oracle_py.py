@@ -61,6 +61,10 @@ class Oracle:
             "or_gs_sweep": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),
             "or_solve": (C.c_int, [vp, C.c_char_p, vp, C.c_int, vp, C.c_int, C.POINTER(OrStats),
                                    vp, vp, C.c_int]),
+            "or_generate_nnz": (i64, [i64, i64, i64]),
+            "or_generate": (C.c_int, [C.c_int, i64, i64, i64, vp, C.c_uint64, vp, vp, vp, vp]),
+            "or_random_vector": (C.c_int, [C.c_uint64, i64, C.c_int, C.c_double, C.c_double, vp]),
+            "or_partition_rcb": (C.c_int, [i64, vp, vp, i32, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -100,6 +104,45 @@ class Oracle:
             raise RuntimeError(self.err())
         return OMatrix(self, h, value_type)
 
+    # -- seeded benchmark inputs (oracle/generators.cpp) -------------------
+    def generate(self, kind, nx, ny, nz, params=(), seed=0):
+        """(rows, cols, vals, coords[n, 3]) of a 7-point matrix: kind 0
+        constant Poisson, 1 variable-coefficient (params = (sigma,)), 2
+        convection-diffusion (params = velocity)."""
+        nnz = self.L.or_generate_nnz(nx, ny, nz)
+        if nnz < 0:
+            raise ValueError("grid dimensions must be positive")
+        r = np.empty(nnz, np.int64)
+        c = np.empty(nnz, np.int64)
+        v = np.empty(nnz, np.float64)
+        xyz = np.empty((nx * ny * nz, 3), np.float64)
+        p = np.array(list(params) + [0.0] * (3 - len(params)), np.float64)
+        self.check(self.L.or_generate(kind, nx, ny, nz, _p(p), seed, _p(r), _p(c), _p(v), _p(xyz)))
+        return r, c, v, xyz
+
+    def random_vector(self, seed, n, dist="uniform", lo=-1.0, hi=1.0):
+        out = np.empty(n, np.float64)
+        self.check(self.L.or_random_vector(seed, n, 0 if dist == "uniform" else 1, lo, hi, _p(out)))
+        return out
+
+    def partition_rcb(self, coords, weights, parts):
+        coords = np.ascontiguousarray(coords, np.float64)
+        w = np.ascontiguousarray(weights, np.int64)
+        out = np.empty(len(w), np.int32)
+        self.check(self.L.or_partition_rcb(len(w), _p(coords), _p(w), parts, _p(out)))
+        return out
+
+    def grid_system(self, kind, nx, ny, nz, params, seed, num_tiles, value_type=0):
+        """A generated 7-point matrix partitioned by coordinate bisection
+        into num_tiles tiles (vertex weight: row off-diagonals + 1), built as
+        an oracle matrix: the benchmark's systems without the product
+        library."""
+        r, c, v, xyz = self.generate(kind, nx, ny, nz, params, seed)
+        n = nx * ny * nz
+        w = np.bincount(r, minlength=n).astype(np.int64)  # row entries = off-diagonals + 1
+        rt = self.partition_rcb(xyz, w, num_tiles) if num_tiles > 1 else None
+        return self.matrix(n, r, c, v, num_tiles, rt, value_type)
+
     def poisson(self, nx, ny, nz, num_tiles, row_to_tile, value_type=0) -> "OMatrix":
         rt = None if row_to_tile is None else np.ascontiguousarray(row_to_tile, np.int32)
         h = self.L.or_poisson(nx, ny, nz, num_tiles, _p(rt), value_type)
@@ -121,6 +164,20 @@ class OMatrix:
         if getattr(self, "h", None):
             self.o.L.or_free(self.h)
             self.h = None
+
+    def tile_order(self):
+        """Natural row index of every tile-order position."""
+        sizes = self.tile_sizes()
+        l2g = self.local_to_global()
+        out, o = [], 0
+        for ni, ns, nh in sizes:
+            out.append(l2g[o:o + ni + ns])
+            o += ni + ns + nh
+        return np.concatenate(out) if out else np.empty(0, np.int64)
+
+    def decompose(self, natural):
+        """Natural-order vector to tile order."""
+        return np.ascontiguousarray(np.asarray(natural)[self.tile_order()])
 
     def row_to_tile(self):
         out = np.empty(self.n, np.int32)
