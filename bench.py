@@ -309,6 +309,21 @@ def other_configs(gb, peak):
             ms, st, rel = timed_solve(gb, A, pbicgstab(pre, 1e-8, 2000), b)
             out[f"convdiff128_{pre.lower()}_{name}"] = {"ms": ms, "iterations": st.iterations,
                                                        "converged": st.converged, "rel_residual_fp64": rel}
+        if vt == gb.FLOAT32:
+            # One Gauss-Seidel sweep from a nonzero x (every entry read), back
+            # to back on device; 8m + 20n algorithmic bytes (matrix values and
+            # columns, row pointers, diagonal, b, x in, x out). The matrix
+            # (133 MB) is larger than L2.
+            gs1 = gb.Solver(A, {"type": "GaussSeidel", "numFixedIterations": 1})
+            xg = A.vector(gb.randomVector(5, h.numRows).astype(np.float32))
+            gs1.timeRepeated(xg, b, 3)
+            ms = gs1.timeRepeated(xg, b, 20)
+            byts = 8 * h.numOffDiag + 20 * h.numRows
+            out["convdiff128_gs_sweep"] = {"ms": ms, "bytes_per_sweep": byts,
+                                           "GBs": byts / (ms * 1e-3) / 1e9,
+                                           "frac_of_hbm": byts / (ms * 1e-3) / 1e9 / peak,
+                                           "kernel": "gsRingKernel"}
+            del gs1, xg
         del A
     # 100^3 LDU mesh (jittered, permuted), Gauss-Seidel PBiCGStab to 1e-8,
     # and the LDU SpMV (matrix smaller than L2: L2 flushed before each launch).

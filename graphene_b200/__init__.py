@@ -530,10 +530,20 @@ class Server:
         x = np.empty(h.numRows, dtype=dt)
         st = _lib.Stats()
         tm = _lib.RequestTimes()
-        check(_lib.lib().gr_server_wait(self._s, rid, timeoutMs, _ptr(x), C.byref(st), C.byref(tm)))
-        del self._hosts[rid]
+        rc = _lib.lib().gr_server_wait(self._s, rid, timeoutMs, _ptr(x), C.byref(st), C.byref(tm))
+        if rc != _lib.GR_ETIMEOUT:  # finished (or cancelled): the server forgot it
+            self._hosts.pop(rid, None)
+        check(rc)
         times = {k: getattr(tm, k) for k, _ in _lib.RequestTimes._fields_}
         return x, SolverStats._from(st), times
+
+    def cancel(self, rid: int) -> bool:
+        """Cancels a request that has not been admitted yet (True; its wait
+        then raises GrapheneError with code GR_ECANCELED); False when it is
+        already running or finished."""
+        c = C.c_int32()
+        check(_lib.lib().gr_server_cancel(self._s, rid, C.byref(c)))
+        return bool(c.value)
 
     def counters(self) -> dict:
         v = [C.c_int64() for _ in range(5)]

@@ -21,6 +21,7 @@ GR_ECUDA = 7
 GR_EUNSUPPORTED = 8
 GR_EIO = 9
 GR_ENONFINITE = 10
+GR_ECANCELED = 11
 
 FLOAT32, FLOAT64, TWOFLOAT32 = 0, 1, 2
 NORM_L1, NORM_L2, NORM_LINF, NORM_NONE = 0, 1, 2, 3
@@ -105,6 +106,7 @@ SIGNATURES = {
     "gr_host_matrix_check_ilu_stream": (C.c_int, [vp, C.c_int, C.c_int, P(i32), P(i64)]),
     "gr_host_matrix_load_vector_mm": (C.c_int, [vp, C.c_char_p, C.c_int, vp]),
     "gr_host_matrix_check_ilu_ring": (C.c_int, [vp, C.c_int, C.c_int, i64, i32, i32, P(i64), P(i64), P(i32)]),
+    "gr_host_matrix_check_gs_ring": (C.c_int, [vp, C.c_int, C.c_int, i64, i32, P(i64), P(i64), P(i32)]),
     "gr_host_matrix_decompose_vector": (C.c_int, [vp, vp, vp, C.c_int]),
     "gr_host_matrix_compose_vector": (C.c_int, [vp, vp, vp, C.c_int]),
     "gr_matrix_create": (C.c_int, [vp, P(vp)]),
@@ -122,6 +124,8 @@ SIGNATURES = {
     "gr_server_wait": (C.c_int, [vp, C.c_uint64, C.c_double, vp, P(Stats), P(RequestTimes)]),
     "gr_server_counters": (C.c_int, [vp, P(i64), P(i64), P(i64), P(i64), P(i64)]),
     "gr_server_destroy": (None, [vp]),
+    "gr_server_cancel": (C.c_int, [vp, C.c_uint64, P(i32)]),
+    "gr_matrix_inject_status": (C.c_int, [vp, i32]),
     "gr_batch_create": (C.c_int, [P(vp), i32, C.c_char_p, P(vp)]),
     "gr_batch_solve_host": (C.c_int, [vp, P(vp), P(vp), C.c_int, P(Stats)]),
     "gr_batch_destroy": (None, [vp]),

@@ -327,6 +327,21 @@ int gr_host_matrix_check_ilu_ring(const gr_host_matrix* h, int dilu, gr_dtype va
   });
 }
 
+int gr_host_matrix_check_gs_ring(const gr_host_matrix* h, int lower_only, gr_dtype value_type, int64_t ring_bytes,
+                                 int32_t allow_compact, int64_t* ring_bytes_used, int64_t* stream_bytes,
+                                 int32_t* max_tile_levels) {
+  return guarded([&] {
+    need(h, "matrix");
+    const gr::DType vt = gr::toDType(value_type);
+    gr::HostRing R = gr::buildLevelRing(*h->m, false, vt, ring_bytes, 1, gr::RingBudget{}, allow_compact != 0,
+                                        lower_only ? gr::RingKind::GaussSeidelLower : gr::RingKind::GaussSeidel);
+    gr::checkLevelRing(*h->m, R, false, vt);
+    if (ring_bytes_used) *ring_bytes_used = R.ringBytes;
+    if (stream_bytes) *stream_bytes = static_cast<int64_t>(R.bytes.size());
+    if (max_tile_levels) *max_tile_levels = R.maxTileLevels;
+  });
+}
+
 int gr_host_matrix_decompose_vector(const gr_host_matrix* h, const void* natural, void* tile_ordered,
                                     gr_dtype t) {
   return guarded([&] {
@@ -445,6 +460,15 @@ int gr_vector_norm(gr_matrix* A, gr_norm norm, const void* x, gr_dtype t, double
     double* d = A->d->scalarOut.as<double>();
     gr::launchNorm(*A->d, x, gr::toDType(t), norm, d, A->d->stream);
     GR_CUDA(cudaMemcpyAsync(out, d, sizeof(double), cudaMemcpyDeviceToHost, A->d->stream));
+    GR_CUDA(cudaStreamSynchronize(A->d->stream));
+  });
+}
+
+int gr_matrix_inject_status(gr_matrix* A, int32_t status) {
+  return guarded([&] {
+    need(A, "matrix");
+    if (status < 0) gr::fail(GR_EINVAL, "status must not be negative");
+    GR_CUDA(cudaMemcpyAsync(A->d->errFlag.get(), &status, sizeof(int32_t), cudaMemcpyHostToDevice, A->d->stream));
     GR_CUDA(cudaStreamSynchronize(A->d->stream));
   });
 }
@@ -606,6 +630,14 @@ int gr_server_counters(gr_server* s, int64_t* queued, int64_t* running, int64_t*
   return guarded([&] {
     need(s, "server");
     s->s->counters(queued, running, completed, bytes_in_use, resident);
+  });
+}
+
+int gr_server_cancel(gr_server* s, uint64_t id, int32_t* cancelled) {
+  return guarded([&] {
+    need(s, "server");
+    const bool c = s->s->cancel(id);
+    if (cancelled) *cancelled = c ? 1 : 0;
   });
 }
 

@@ -239,7 +239,12 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
     if (const Json* v = j.find("norm")) c->norm = parseNorm(v->text);
   }
   if (ty == "PBiCGStab") {
-    mark("verbose"); mark("workingType"); mark("preconditioner");
+    mark("verbose"); mark("workingType"); mark("preconditioner"); mark("reduce");
+    if (const Json* v = j.find("reduce")) {
+      if (v->text == "float64") c->reduceRef = false;
+      else if (v->text == "f32_ref_order") c->reduceRef = true;
+      else fail(GR_EPARSE, "PBiCGStab reduce must be \"float64\" or \"f32_ref_order\"");
+    }
     readBool(j, "verbose", c->verbose);
     if (const Json* v = j.find("workingType")) c->workingType = parseTypeName(v->text);
     if (const Json* v = j.find("preconditioner")) c->preconditioner = fromJson(*v);
@@ -279,7 +284,13 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
     }
   } else if (ty == "GaussSeidel") {
     mark("numSweeps"); mark("numFixedIterations"); mark("solveMulticolor"); mark("workingType");
-    mark("seed");
+    mark("seed"); mark("kernel");
+    if (const Json* v = j.find("kernel")) {
+      if (v->text == "auto") c->gsKernel = 0;
+      else if (v->text == "ring") c->gsKernel = 1;
+      else if (v->text == "levels") c->gsKernel = 2;
+      else fail(GR_EPARSE, "GaussSeidel kernel must be \"auto\", \"ring\" or \"levels\"");
+    }
     readInt(j, "numSweeps", c->numSweeps);
     readInt(j, "numFixedIterations", c->numFixedIterations);
     readMultiColor(j, "solveMulticolor", c->solveMulticolor);

@@ -73,6 +73,15 @@ struct SolverConfig {
   // codelet/ipu/matrix/solvers/gauss-seidel.cpp:44) or "diag" (the CodeDSL
   // version, gauss-seidel/Solver.cpp:74).
   bool gsSeedB = true;
+  // PBiCGStab "reduce": false (default, "float64"): dot products and norms
+  // accumulate in FP64; true ("f32_ref_order"): in float, in the reference's
+  // own reduction order (dsl/tensor/Expression.cpp:472-481, :597-769), with
+  // alpha, beta, omega and the convergence test in float, as the reference
+  // computes them (float32 vectors only).
+  bool reduceRef = false;
+  // Gauss-Seidel sweep kernel: 0 auto (the level ring when a tile fits
+  // shared memory), 1 the level ring, 2 level schedules in global memory.
+  int gsKernel = 0;
   // IterativeRefinement (iterative-refinement/Configuration.hpp:23-25)
   int extendedPrecisionType = -1;  // -1: the type of x
   // restarter (restarter/Configuration.hpp:14)

@@ -218,7 +218,28 @@ struct RingBudget {
   i64 reservedPerBlock = 1024;
   i32 maxBlocksPerSM = 16;  // the ring kernel's thread and register limit on B200
 };
+// What a level ring holds: the ILU(0) / DILU forward and backward
+// substitution (each row's lower, then upper entries, halo dropped), or one
+// Gauss-Seidel sweep over the lower levels with each row's entries in
+// tile-local order (all of them; or, for a sweep that starts from x = 0,
+// only the lower ones, the others multiplying zero).
+//
+// Gauss-Seidel rings address x through one shared-memory array per tile of
+// 2 nRows + nHalo + 1 slots: [0, nRows) the values of this sweep, [nRows,
+// 2 nRows) the tile's values at the start of the sweep, then the halo
+// values at the start of the sweep (the reference's halo exchange,
+// gauss-seidel/Solver.cpp:61) and a zero slot for padding entries. An entry
+// with tile-local column c of row i reads slot c when c < i and nRows + c
+// otherwise (halo columns are >= nRows). The row's diagonal takes the
+// inverse diagonal's place in the level block, and the right-hand side
+// (nRows more slots) follows the array.
+enum class RingKind { Ilu = 0, GaussSeidel = 1, GaussSeidelLower = 2 };
+
 struct HostRing {
+  RingKind kind = RingKind::Ilu;
+  i64 maxXSlots = 0;               // Gauss-Seidel: shared-memory x slots per tile (with the right-hand side)
+  std::vector<i32> haloStart;      // Gauss-Seidel: P + 1 offsets into haloSrc
+  std::vector<i32> haloSrc;        // Gauss-Seidel: tile-order index of every tile's halo cells
   std::vector<uint8_t> bytes;
   std::vector<i64> tileOffset;  // P + 1
   std::vector<int4> meta;       // 1 per level
@@ -235,25 +256,31 @@ struct HostRing {
 // Header: kRingBarriers full and kRingBarriers empty mbarriers, one for the
 // level table, padded to 16 bytes.
 constexpr i64 kRingHeader = (8 * (2 * kRingBarriers + 1) + 15) / 16 * 16;
+inline i64 ringFixedSmemSlots(i32 maxTileLevels, i64 xSlots, i64 vectorBytes) {
+  return kRingHeader + 16 * static_cast<i64>(maxTileLevels) + xSlots * vectorBytes;
+}
 inline i64 ringFixedSmem(i32 maxTileLevels, i64 maxGroupRows, i64 vectorBytes) {
-  return kRingHeader + 16 * static_cast<i64>(maxTileLevels) + (maxGroupRows + 1) * vectorBytes;
+  return ringFixedSmemSlots(maxTileLevels, maxGroupRows + 1, vectorBytes);
 }
 // One thread block runs `group` consecutive tiles in lockstep (tileOffset,
 // tileLevel and meta are then per block). ringBytes 0: the default (RingBudget).
 // The compact layout is used when every block has at most kRingCompactRows
 // rows and `allowCompact`.
 HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes, i32 group,
-                        const RingBudget& budget = RingBudget{}, bool allowCompact = true);
+                        const RingBudget& budget = RingBudget{}, bool allowCompact = true,
+                        RingKind kind = RingKind::Ilu);
 // Replays the kernel's copies and reads on the host; throws GR_EINVAL on an
 // out-of-range index, a dependency-order violation, a copy that would
 // overwrite a level not yet consumed, or a copy issued too late.
 void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt);
 struct LevelRing {
+  RingKind kind = RingKind::Ilu;
   bool dilu = false;
-  i64 bytes = 0, ringBytes = 0, nVal = 0, nInv = 0, maxGroupRows = 0;
+  i64 bytes = 0, ringBytes = 0, nVal = 0, nInv = 0, maxGroupRows = 0, maxXSlots = 0;
   i32 maxTileLevels = 0, group = 1, numGroups = 0;
   bool compact = false;
   DBuf tileOffset, templ, meta, tileLevel, groupStart, valPos, valSrc, invPos, invSrc;
+  DBuf haloStart, haloSrc;  // Gauss-Seidel rings
 };
 
 // Kinds of entries a schedule keeps per row.
@@ -316,8 +343,10 @@ struct DeviceMatrix {
   std::unique_ptr<LevelSchedule> lowerSched, upperSched, gsSched;
   std::unique_ptr<SweepStream> iluStream[2];  // [dilu]
   SweepStream& iluSweepStream(bool dilu);
-  std::map<std::tuple<bool, i64, i32, bool>, std::unique_ptr<LevelRing>> levelRings;  // [(dilu, ring bytes, group, compact allowed)]
-  LevelRing& levelRing(bool dilu, i64 ringBytes, i32 group, bool allowCompact = true);
+  std::map<std::tuple<bool, i64, i32, bool, int>, std::unique_ptr<LevelRing>>
+      levelRings;  // [(dilu, ring bytes, group, compact allowed, kind)]
+  LevelRing& levelRing(bool dilu, i64 ringBytes, i32 group, bool allowCompact = true,
+                       RingKind kind = RingKind::Ilu);
 
   // Device error word written by kernels whose bounded waits ran out
   // (GR_ETIMEOUT); 0 when clean.

@@ -32,7 +32,7 @@ template <class MV, class W>
 __global__ void __launch_bounds__(256) bicgInitKernel(SellView<MV> A, const W* __restrict__ x,
                                                        const W* __restrict__ b, W* __restrict__ r,
                                                        W* __restrict__ r0, KState* st, double* partials,
-                                                       unsigned* counter, SegView seg) {
+                                                       unsigned* counter, SegView seg, bool stateless) {
   __shared__ double smem[64];
   const SegPos sp = segPos(seg, A.n);
   st += sp.sys;
@@ -54,6 +54,7 @@ __global__ void __launch_bounds__(256) bicgInitKernel(SellView<MV> A, const W* _
       v[1] = __dadd_rn(v[1], __dmul_rn(toDouble(res), toDouble(res)));
     }
   }
+  if (stateless) return;  // the vectors only (reference-order reductions follow)
   double out[2];
   blockReduce<2>(v, ops, smem);
   if (gridReduceRank<2>(v, ops, partials + 2 * sp.b0, counter + sp.sys, smem, out, sp.rank, sp.nb) &&
@@ -78,7 +79,7 @@ template <class MV, class W, int MODE>
 __global__ void __launch_bounds__(256) spmvDotKernel(SellView<MV> A, const W* __restrict__ x,
                                                       W* __restrict__ y, const W* __restrict__ d1,
                                                       KState* st, double* partials, unsigned* counter,
-                                                      SegView seg) {
+                                                      SegView seg, bool stateless) {
   __shared__ double smem[64];
   const SegPos sp = segPos(seg, A.n);
   st += sp.sys;
@@ -100,6 +101,7 @@ __global__ void __launch_bounds__(256) spmvDotKernel(SellView<MV> A, const W* __
       if (MODE == 1) v[1] = __dadd_rn(v[1], __dmul_rn(yd, yd));
     }
   }
+  if (stateless) return;
   double out[2];
   blockReduce<2>(v, ops, smem);
   if (gridReduceRank<2>(v, ops, partials + 2 * sp.b0, counter + sp.sys, smem, out, sp.rank, sp.nb) &&
@@ -145,7 +147,8 @@ __global__ void __launch_bounds__(256) bicgUpdateKernel(W* __restrict__ x, const
                                                          const W* __restrict__ z, W* __restrict__ r,
                                                          const W* __restrict__ s, const W* __restrict__ t,
                                                          const W* __restrict__ r0, int n, KState* st,
-                                                         double* partials, unsigned* counter, SegView seg) {
+                                                         double* partials, unsigned* counter, SegView seg,
+                                                         bool stateless) {
   __shared__ double smem[64];
   const SegPos sp = segPos(seg, n);
   st += sp.sys;
@@ -189,6 +192,7 @@ __global__ void __launch_bounds__(256) bicgUpdateKernel(W* __restrict__ x, const
       for (int i = i0; i < min(i0 + 4, sp.r1); ++i) one(i);
     }
   }
+  if (stateless) return;
   double out[2];
   blockReduce<2>(v, ops, smem);
   if (gridReduceRank<2>(v, ops, partials + 2 * sp.b0, counter + sp.sys, smem, out, sp.rank, sp.nb) &&
@@ -209,6 +213,194 @@ __global__ void __launch_bounds__(256) bicgUpdateKernel(W* __restrict__ x, const
       } else {
         st->beta = (st->rho / st->rhoOld) * (st->alpha / st->omega);
       }
+    }
+  }
+}
+
+// ---- the reference's reduction order --------------------------------------
+// Float reductions in the order of Expression::reduce (Expression.cpp:
+// 472-481, :597-769): per tile, six workers over chunks of floor(n_t/6/4)*4
+// rows (worker 5 takes the rest), each chunk summed in row order from 0,
+// then the six partials in worker order; with 6 rows or fewer in all, the
+// tile's rows in order. Across tiles, runs of 368, 736, 1472 and then all
+// tiles, each run summed in tile order (per worker first when some run has
+// more than 6 values). Explicitly rounded operations only.
+struct RefQ {
+  int kind;  // RefKind
+  const float* a;
+  const float* b;
+};
+
+__device__ __forceinline__ float refVal(const RefQ& q, int i) {
+  const float a = q.a[i];
+  return q.kind == static_cast<int>(RefKind::Dot) ? __fmul_rn(a, q.b[i]) : a;
+}
+__device__ __forceinline__ float refStep(float acc, float v, int kind) {
+  return kind == static_cast<int>(RefKind::SquareSum) ? __fadd_rn(acc, __fmul_rn(v, v)) : __fadd_rn(acc, v);
+}
+
+// One block (two warps) per tile: warp q computes reduction q, lanes 0..5
+// being the reference's six workers.
+__global__ void __launch_bounds__(64) refTileKernel(const int* __restrict__ tileStart, long long total, RefQ q0,
+                                                    RefQ q1, float* __restrict__ out, int P, const KState* st) {
+  __shared__ float part[2][6];
+  if (st->done) return;
+  const int T = blockIdx.x;
+  const int base = tileStart[T];
+  const int nt = tileStart[T + 1] - base;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const RefQ q = w == 0 ? q0 : q1;
+  if (q.kind == static_cast<int>(RefKind::None)) return;  // warp-uniform
+  if (q.kind == static_cast<int>(RefKind::Max)) {
+    float m = -INFINITY;
+    for (int i = lane; i < nt; i += 32) m = fmaxf(m, q.a[base + i]);
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) out[w * P + T] = m;
+    return;
+  }
+  if (total > 6) {
+    const int chunk = (nt / 6 / 4) * 4;
+    if (lane < 6) {
+      const int s0 = chunk * lane, e0 = lane == 5 ? nt : s0 + chunk;
+      float acc = 0.0f;
+      for (int i = s0; i < e0; ++i) acc = refStep(acc, refVal(q, base + i), q.kind);
+      part[w][lane] = acc;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      float acc = 0.0f;
+      for (int k = 0; k < 6; ++k) acc = __fadd_rn(acc, part[w][k]);
+      out[w * P + T] = acc;
+    }
+  } else if (lane == 0) {
+    float acc = 0.0f;
+    for (int i = 0; i < nt; ++i) acc = refStep(acc, refVal(q, base + i), q.kind);
+    out[w * P + T] = acc;
+  }
+}
+
+__device__ float refSeq(const float* v, int s0, int e0) {
+  float acc = 0.0f;
+  for (int i = s0; i < e0; ++i) acc = __fadd_rn(acc, v[i]);
+  return acc;
+}
+__device__ float refWorkers(const float* v, int cnt) {
+  const int chunk = (cnt / 6 / 4) * 4;
+  float part[6];
+  for (int w = 0; w < 6; ++w) part[w] = refSeq(v, chunk * w, w == 5 ? cnt : chunk * w + chunk);
+  return refSeq(part, 0, 6);
+}
+constexpr int kRefMaxRuns = 256;  // values after the first stage: at most 368 * 256 tiles
+// The cross-tile stages over the P per-tile values.
+__device__ float refAcrossTiles(const float* v, int P, bool isMax) {
+  if (isMax) {
+    float m = -INFINITY;
+    for (int t = 0; t < P; ++t) m = fmaxf(m, v[t]);
+    return m;
+  }
+  if (P == 1) return v[0];
+  float cur[kRefMaxRuns];
+  int at[kRefMaxRuns];
+  int n = 0;
+  {
+    const int G = 368;
+    const bool pw = (P < G ? P : G) > 6;  // the first run is the largest
+    for (int g = 0; g * G < P; ++g) {
+      const int cnt = min(G, P - g * G);
+      cur[n] = pw ? refWorkers(v + g * G, cnt) : refSeq(v + g * G, 0, cnt);
+      at[n++] = g * G;
+    }
+  }
+  const int runs[3] = {736, 1472, 0};  // 0: all
+  for (int k = 0; k < 3 && n > 1; ++k) {
+    const int G = runs[k];
+    float nxt[kRefMaxRuns];
+    int nat[kRefMaxRuns], start[kRefMaxRuns + 1];
+    int m = 0;
+    for (int i = 0; i < n; ++i) {
+      const int key = G == 0 ? 0 : at[i] / G * G;
+      if (m == 0 || nat[m - 1] != key) {
+        nat[m] = key;
+        start[m++] = i;
+      }
+    }
+    start[m] = n;
+    bool pw = false;
+    for (int g = 0; g < m; ++g) pw = pw || start[g + 1] - start[g] > 6;
+    for (int g = 0; g < m; ++g) {
+      const int cnt = start[g + 1] - start[g];
+      nxt[g] = pw ? refWorkers(cur + start[g], cnt) : refSeq(cur + start[g], 0, cnt);
+    }
+    for (int g = 0; g < m; ++g) {
+      cur[g] = nxt[g];
+      at[g] = nat[g];
+    }
+    n = m;
+  }
+  return cur[0];
+}
+
+__device__ __forceinline__ float refNormFinish(float v, int normKind) {
+  return normKind == GR_NORM_L2 ? __fsqrt_rn(v) : v;
+}
+
+__global__ void refStateKernel(const float* __restrict__ tiles, int P, int kind0, int kind1, int stage,
+                               KState* st) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const bool pre = stage == static_cast<int>(RefStage::BNorm) || stage == static_cast<int>(RefStage::Init);
+  if (!pre && st->done) return;
+  const float q0 = kind0 ? refAcrossTiles(tiles, P, kind0 == static_cast<int>(RefKind::Max)) : 0.0f;
+  const float q1 = kind1 ? refAcrossTiles(tiles + P, P, kind1 == static_cast<int>(RefKind::Max)) : 0.0f;
+  const float vsmall = 1e-37f;  // Traits<float>::vsmall (common/Traits.hpp:43)
+  const int nk = st->normKind;
+  switch (static_cast<RefStage>(stage)) {
+    case RefStage::BNorm:
+      st->bNorm = refNormFinish(q0, nk);
+      break;
+    case RefStage::Init: {
+      const float nrm = refNormFinish(q1, nk);
+      st->rho = q0;
+      st->normInit = nrm;
+      st->normFinal = nrm;
+      st->iter = 0;
+      st->converged = 0;
+      st->singular = fabsf(q0) < vsmall;
+      st->status = isfinite(nrm) ? GR_OK : GR_ENONFINITE;
+      st->done = st->maxIter <= 0 || st->singular || st->status != GR_OK;
+      break;
+    }
+    case RefStage::Alpha:
+      st->alpha = __fdiv_rn(static_cast<float>(st->rho), q0);
+      break;
+    case RefStage::Omega: {
+      const float om = __fdiv_rn(q1, q0);
+      st->omega = om;
+      st->singular = fabsf(om) < vsmall;
+      st->done = st->singular;
+      break;
+    }
+    case RefStage::Update: {
+      const float fin = refNormFinish(q1, nk);
+      const float init = static_cast<float>(st->normInit);
+      bool c = fin < static_cast<float>(st->absTol) || fin < __fmul_rn(init, static_cast<float>(st->relRes));
+      if (st->relTol > 0) c = c || fin < __fmul_rn(static_cast<float>(st->bNorm), static_cast<float>(st->relTol));
+      st->normFinal = fin;
+      st->converged = c;
+      st->rhoOld = st->rho;
+      st->iter += 1;
+      st->status = isfinite(fin) ? GR_OK : GR_ENONFINITE;
+      st->done = (c && st->iter >= st->minIter) || st->iter >= st->maxIter || st->status != GR_OK;
+      if (!st->done) {
+        st->rho = q0;
+        if (fabsf(q0) < vsmall) {
+          st->singular = 1;
+          st->done = 1;
+        } else {
+          st->beta = __fmul_rn(__fdiv_rn(q0, static_cast<float>(st->rhoOld)),
+                               __fdiv_rn(static_cast<float>(st->alpha), static_cast<float>(st->omega)));
+        }
+      }
+      break;
     }
   }
 }
@@ -313,20 +505,20 @@ Launch krylovLaunch(DeviceMatrix& A, bool chunk) {
 }  // namespace
 
 void launchBicgInit(DeviceMatrix& A, const void* x, const void* b, void* r, void* r0, KState* st, DType W,
-                    cudaStream_t s) {
+                    cudaStream_t s, bool stateless) {
   const Launch L = krylovLaunch(A, true);
   if (A.vt == DType::F32 && W == DType::F32)
     dev::bicgInitKernel<float, float><<<L.blocks, 256, 0, s>>>(
         sellView<float>(A), static_cast<const float*>(x), static_cast<const float*>(b), static_cast<float*>(r),
-        static_cast<float*>(r0), st, L.partials, L.counter, L.seg);
+        static_cast<float*>(r0), st, L.partials, L.counter, L.seg, stateless);
   else if (A.vt == DType::F32 && W == DType::F64)
     dev::bicgInitKernel<float, double><<<L.blocks, 256, 0, s>>>(
         sellView<float>(A), static_cast<const double*>(x), static_cast<const double*>(b), static_cast<double*>(r),
-        static_cast<double*>(r0), st, L.partials, L.counter, L.seg);
+        static_cast<double*>(r0), st, L.partials, L.counter, L.seg, stateless);
   else if (A.vt == DType::F64 && W == DType::F64)
     dev::bicgInitKernel<double, double><<<L.blocks, 256, 0, s>>>(
         sellView<double>(A), static_cast<const double*>(x), static_cast<const double*>(b), static_cast<double*>(r),
-        static_cast<double*>(r0), st, L.partials, L.counter, L.seg);
+        static_cast<double*>(r0), st, L.partials, L.counter, L.seg, stateless);
   else
     fail(GR_EUNSUPPORTED, "PBiCGStab with float64 coefficients needs float64 vectors");
   checkLaunch("bicg_init");
@@ -334,30 +526,31 @@ void launchBicgInit(DeviceMatrix& A, const void* x, const void* b, void* r, void
 
 namespace {
 template <class MV, class W>
-void spmvDotT(DeviceMatrix& A, const void* x, void* y, const void* d1, int mode, KState* st, cudaStream_t s) {
+void spmvDotT(DeviceMatrix& A, const void* x, void* y, const void* d1, int mode, KState* st, cudaStream_t s,
+              bool stateless) {
   const Launch L = krylovLaunch(A, true);
   if (mode == 0)
     dev::spmvDotKernel<MV, W, 0><<<L.blocks, 256, 0, s>>>(sellView<MV>(A), static_cast<const W*>(x),
                                                           static_cast<W*>(y), static_cast<const W*>(d1), st,
-                                                          L.partials, L.counter, L.seg);
+                                                          L.partials, L.counter, L.seg, stateless);
   else
     dev::spmvDotKernel<MV, W, 1><<<L.blocks, 256, 0, s>>>(sellView<MV>(A), static_cast<const W*>(x),
                                                           static_cast<W*>(y), static_cast<const W*>(d1), st,
-                                                          L.partials, L.counter, L.seg);
+                                                          L.partials, L.counter, L.seg, stateless);
 }
 }  // namespace
 
 void launchSpmvDot(DeviceMatrix& A, const void* x, void* y, const void* d1, int mode, KState* st, DType W,
-                   cudaStream_t s) {
-  if (A.vt == DType::F32 && W == DType::F32) spmvDotT<float, float>(A, x, y, d1, mode, st, s);
-  else if (A.vt == DType::F32 && W == DType::F64) spmvDotT<float, double>(A, x, y, d1, mode, st, s);
-  else if (A.vt == DType::F64 && W == DType::F64) spmvDotT<double, double>(A, x, y, d1, mode, st, s);
+                   cudaStream_t s, bool stateless) {
+  if (A.vt == DType::F32 && W == DType::F32) spmvDotT<float, float>(A, x, y, d1, mode, st, s, stateless);
+  else if (A.vt == DType::F32 && W == DType::F64) spmvDotT<float, double>(A, x, y, d1, mode, st, s, stateless);
+  else if (A.vt == DType::F64 && W == DType::F64) spmvDotT<double, double>(A, x, y, d1, mode, st, s, stateless);
   else fail(GR_EUNSUPPORTED, "PBiCGStab with float64 coefficients needs float64 vectors");
   checkLaunch("spmv_dot");
 }
 
 void launchBicgUpdate(DeviceMatrix& A, void* x, const void* y, const void* z, void* r, const void* sv,
-                      const void* t, const void* r0, KState* st, DType W, cudaStream_t s) {
+                      const void* t, const void* r0, KState* st, DType W, cudaStream_t s, bool stateless) {
   const Launch L = krylovLaunch(A, false);
   // 16-byte accesses need every vector 16-byte aligned (segments start at
   // multiples of 32 rows); otherwise the same order element by element.
@@ -369,13 +562,27 @@ void launchBicgUpdate(DeviceMatrix& A, void* x, const void* y, const void* z, vo
     (vec ? dev::bicgUpdateKernel<float, true> : dev::bicgUpdateKernel<float, false>)<<<L.blocks, 256, 0, s>>>(
         static_cast<float*>(x), static_cast<const float*>(y), static_cast<const float*>(z), static_cast<float*>(r),
         static_cast<const float*>(sv), static_cast<const float*>(t), static_cast<const float*>(r0), A.n, st,
-        L.partials, L.counter, L.seg);
+        L.partials, L.counter, L.seg, stateless);
   else
     (vec ? dev::bicgUpdateKernel<double, true> : dev::bicgUpdateKernel<double, false>)<<<L.blocks, 256, 0, s>>>(
         static_cast<double*>(x), static_cast<const double*>(y), static_cast<const double*>(z),
         static_cast<double*>(r), static_cast<const double*>(sv), static_cast<const double*>(t),
-        static_cast<const double*>(r0), A.n, st, L.partials, L.counter, L.seg);
+        static_cast<const double*>(r0), A.n, st, L.partials, L.counter, L.seg, stateless);
   checkLaunch("bicg_update");
+}
+
+void launchRefReduce(DeviceMatrix& A, const RefRed& q0, const RefRed& q1, RefStage stage, KState* st, void* tiles,
+                     cudaStream_t s) {
+  if (A.P > 368 * dev::kRefMaxRuns) fail(GR_EUNSUPPORTED, "reference-order reductions support up to 94208 tiles");
+  auto q = [](const RefRed& r) {
+    return dev::RefQ{static_cast<int>(r.kind), static_cast<const float*>(r.a), static_cast<const float*>(r.b)};
+  };
+  float* t = static_cast<float*>(tiles);
+  dev::refTileKernel<<<A.P, 64, 0, s>>>(A.tileStart.as<int>(), static_cast<long long>(A.n), q(q0), q(q1), t, A.P, st);
+  checkLaunch("ref_tile_reduce");
+  dev::refStateKernel<<<1, 32, 0, s>>>(t, A.P, static_cast<int>(q0.kind), static_cast<int>(q1.kind),
+                                       static_cast<int>(stage), st);
+  checkLaunch("ref_state");
 }
 
 void launchStateReset(KState* st, const KState& init, cudaStream_t s, int count) {

@@ -300,12 +300,183 @@ __global__ void __launch_bounds__(RingShape<W>::threads) iluRingKernel(const uns
   for (int i = threadIdx.x; i < nRows; i += blockDim.x) y[base + i] = xs[i];
 }
 
+// One Gauss-Seidel sweep of every tile (gauss-seidel/Solver.cpp:45-86)
+// through a Gauss-Seidel level ring: rows in ascending tile-local order, as
+// the lower levels, each x_i = (seed_i - sum_j a_ij x_j) / d_i over the row's
+// entries in tile-local order, where x_j is this sweep's value for earlier
+// rows of the tile and the sweep-start value for later rows and for halo
+// cells. The same producer / waiting / compute warp pipeline as
+// iluRingKernel copies the level blocks (rows, diagonal, slots, values); the
+// tile's x lives in shared memory as [this sweep | sweep start | halo |
+// zero], so every entry is one shared-memory read at a slot the host fixed.
+// The prologue fills the sweep-start values and halo cells from xin (zeros
+// when xinZero) and, with seedB, the right-hand side from the fused
+// PBiCGStab prologue (which also writes p or s).
+template <class MV, class W, bool COMPACT>
+__global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
+    const unsigned char* __restrict__ stream, const long long* __restrict__ tileOffset, const int4* __restrict__ meta,
+    const int* __restrict__ tileLevel, const int* __restrict__ tileStart, const int* __restrict__ haloStart,
+    const int* __restrict__ haloSrc, int ringBytes, int metaLevels, bool seedB, SPro<W> pro,
+    const W* __restrict__ xin, bool xinZero, W* __restrict__ xout, int* errFlag) {
+  constexpr int kRingCompute = RingShape<W>::compute;
+  constexpr int kRingLevelSync = RingShape<W>::levelSync;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ int abortFlag, consumedLevels;
+  const KState* st = pro.state();
+  if (st && st->done) return;
+  const int T = blockIdx.x;
+  const int base = tileStart[T];
+  const int nRows = tileStart[T + 1] - base;
+  const int h0 = haloStart[T];
+  const int nHalo = haloStart[T + 1] - h0;
+  const int lv0 = tileLevel[T];
+  const int L = tileLevel[T + 1] - lv0;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* empty = full + kRingBarriers;
+  uint64_t* tableBar = empty + kRingBarriers;
+  int4* mt = reinterpret_cast<int4*>(smem + kRingHeader);
+  unsigned char* ring = smem + kRingHeader + 16 * metaLevels;
+  W* xs = reinterpret_cast<W*>(ring + ringBytes);  // this sweep | sweep start | halo | zero
+  W* rhs = xs + 2 * nRows + nHalo + 1;
+  const unsigned char* g = stream + tileOffset[T];
+  const bool lead = threadIdx.x == kRingLevelSync;
+  const volatile int* abortV = &abortFlag;
+
+  if (lead) {
+    abortFlag = 0;
+    consumedLevels = L;
+    for (int i = 0; i < kRingBarriers; ++i) {
+      mbarInit(smemAddr(full + i), 1);
+      mbarInit(smemAddr(empty + i), 1);
+    }
+    mbarInit(smemAddr(tableBar), 1);
+    fenceBarrierInit();
+    const uint32_t tb = static_cast<uint32_t>(L) * 16u;
+    mbarExpectTx(smemAddr(tableBar), tb);
+    bulkLoad(smemAddr(mt), meta + static_cast<size_t>(lv0), tb, smemAddr(tableBar));
+  }
+  {
+    const int bd = static_cast<int>(blockDim.x);
+    if (seedB || pro.kind != static_cast<int>(Prologue::Plain)) {
+      W beta = W(0), omega = W(0), alpha = W(0);
+      bool first = true;
+      if (st) {
+        beta = cvt<W>(st->beta);
+        omega = cvt<W>(st->omega);
+        alpha = cvt<W>(st->alpha);
+        first = st->iter == 0;
+      }
+      for (int i0 = threadIdx.x; i0 < nRows; i0 += 4 * bd) {
+        W v4[4];
+        pro.four(base + i0, bd, base + nRows, beta, omega, alpha, first, v4);
+        if (seedB) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (i0 + j * bd < nRows) rhs[i0 + j * bd] = v4[j];
+        }
+      }
+    }
+    for (int i = threadIdx.x; i < nRows; i += bd) xs[nRows + i] = xinZero ? W(0) : xin[base + i];
+    for (int h = threadIdx.x; h < nHalo; h += bd) xs[2 * nRows + h] = xinZero ? W(0) : xin[haloSrc[h0 + h]];
+    if (lead) xs[2 * nRows + nHalo] = W(0);
+  }
+  __syncthreads();
+
+  int issued = 0;
+  if (threadIdx.x >= kRingLevelSync) {
+    if (lead) {
+      if (!mbarWaitBounded(smemAddr(tableBar), 0, abortV)) {
+        abortFlag = 1;
+      } else {
+        uint32_t src = 0;
+        for (; issued < L && !*abortV; ++issued) {
+          const int4 m = mt[issued];
+          const int ia = RingLevelCode::issueAfter(m);
+          if (ia >= 0 && !mbarWaitBounded(smemAddr(empty + ia % kRingBarriers), (ia / kRingBarriers) & 1, abortV)) {
+            abortFlag = 1;
+            break;
+          }
+          const uint32_t bytes = RingLevelCode::bytes(m);
+          const uint32_t bar = smemAddr(full + issued % kRingBarriers);
+          mbarExpectTx(bar, bytes);
+          bulkLoad(smemAddr(ring + RingLevelCode::ringOffset(m)), g + src, bytes, bar);
+          src += bytes;
+        }
+      }
+    }
+  } else if (threadIdx.x >= kRingCompute) {
+    bool ok = mbarWaitBounded(smemAddr(tableBar), 0, abortV) && (L == 0 || mbarWaitBounded(smemAddr(full), 0, abortV));
+    if (!ok) abortFlag = 1;
+    bool stop = namedBarOr(1, kRingLevelSync, !ok);
+    if (stop && threadIdx.x == kRingCompute) consumedLevels = 0;
+    for (int l = 0; !stop && l < L; ++l) {
+      bool bad = false;
+      if (l + 1 < L &&
+          !mbarWaitBounded(smemAddr(full + (l + 1) % kRingBarriers), ((l + 1) / kRingBarriers) & 1, abortV)) {
+        abortFlag = 1;
+        bad = true;
+      }
+      stop = namedBarOr(1, kRingLevelSync, bad || *abortV != 0);
+      if (threadIdx.x == kRingCompute) {
+        mbarArrive(smemAddr(empty + l % kRingBarriers));
+        if (stop) consumedLevels = l + 1;
+      }
+    }
+  } else {
+    bool stop = namedBarOr(1, kRingLevelSync, false);
+    for (int l = 0; !stop && l < L; ++l) {
+      const RingLevel<MV, COMPACT> cur = ringLevelAt<MV, COMPACT>(mt[l], ring);
+      for (int q = threadIdx.x; q < cur.k; q += kRingCompute) {
+        const int il = cur.row(q);
+        const W d = cvt<W>(cur.invDiag(q));
+        W sum = seedB ? rhs[il] : d;
+        if (cur.E <= 8) {
+          // Every entry's slot and value first, then the x values, then the
+          // sum in order: the loads overlap.
+          int c[8];
+          MV v[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e)
+            if (e < cur.E) cur.entry(e, q, c[e], v[e]);
+          W xv[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e)
+            if (e < cur.E) xv[e] = xs[c[e]];
+#pragma unroll
+          for (int e = 0; e < 8; ++e)
+            if (e < cur.E) sum = sub(sum, mul(cvt<W>(v[e]), xv[e]));
+        } else {
+          for (int e = 0; e < cur.E; ++e) {
+            int c;
+            MV v;
+            cur.entry(e, q, c, v);
+            sum = sub(sum, mul(cvt<W>(v), xs[c]));
+          }
+        }
+        xs[il] = dvd(sum, d);
+      }
+      stop = namedBarOr(1, kRingLevelSync, *abortV != 0);
+    }
+  }
+  __syncthreads();
+  if (abortFlag) {
+    if (lead) {
+      atomicExch(errFlag, GR_ETIMEOUT);
+      mbarWaitBounded(smemAddr(tableBar), 0);
+      for (int j = consumedLevels; j < issued; ++j)
+        mbarWaitBounded(smemAddr(full + j % kRingBarriers), (j / kRingBarriers) & 1);
+    }
+    return;
+  }
+  for (int i = threadIdx.x; i < nRows; i += blockDim.x) xout[base + i] = xs[i];
+}
+
 }  // namespace dev
 
 // ---------------------------------------------------------------------------
 size_t iluRingSmem(const DeviceMatrix& A, const LevelRing& R, DType W) {
   (void)A;
-  return static_cast<size_t>(ringFixedSmem(R.maxTileLevels, R.maxGroupRows, static_cast<i64>(dtypeSize(W))) +
+  return static_cast<size_t>(ringFixedSmemSlots(R.maxTileLevels, R.maxXSlots, static_cast<i64>(dtypeSize(W))) +
                              R.ringBytes);
 }
 
@@ -337,16 +508,52 @@ void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool di
 }
 }  // namespace
 
-int ringBlocksPerSMWithoutSmem(DType vt) {
+int ringBlocksPerSMWithoutSmem(DType vt, RingKind kind) {
   int n = 0;
-  const void* fn = vt == DType::F64 ? reinterpret_cast<const void*>(dev::iluRingKernel<double, double, true, true>)
-                                    : reinterpret_cast<const void*>(dev::iluRingKernel<float, float, true, true>);
+  const bool gs = kind != RingKind::Ilu;
+  const void* fn = vt == DType::F64
+                       ? (gs ? reinterpret_cast<const void*>(dev::gsRingKernel<double, double, true>)
+                             : reinterpret_cast<const void*>(dev::iluRingKernel<double, double, true, true>))
+                       : (gs ? reinterpret_cast<const void*>(dev::gsRingKernel<float, float, true>)
+                             : reinterpret_cast<const void*>(dev::iluRingKernel<float, float, true, true>));
   const int threads = vt == DType::F64 ? dev::RingShape<double>::threads : dev::RingShape<float>::threads;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, 0) != cudaSuccess) {
     (void)cudaGetLastError();
     return 0;
   }
   return n;
+}
+
+namespace {
+template <class MV, class W>
+void gsRingT(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& p, bool seedB,
+             const void* xin, bool xinZero, void* xout, cudaStream_t s) {
+  if (R.kind == RingKind::Ilu) fail(GR_EINVAL, "not a Gauss-Seidel ring");
+  if (R.kind == RingKind::GaussSeidelLower && !xinZero)
+    fail(GR_EINVAL, "a lower-only Gauss-Seidel ring sweeps from x = 0 only");
+  const size_t smem = iluRingSmem(A, R, dtypeOf<W>());
+  auto kernel = R.compact ? dev::gsRingKernel<MV, W, true> : dev::gsRingKernel<MV, W, false>;
+  ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
+  preferSharedCarveout(reinterpret_cast<const void*>(kernel));
+  dev::SPro<W> pro{static_cast<int>(p.kind), static_cast<const W*>(p.b), static_cast<const W*>(p.r),
+                   static_cast<W*>(p.pOrS), static_cast<const W*>(p.v), p.st, nullptr};
+  kernel<<<R.numGroups, dev::RingShape<W>::threads, smem, s>>>(
+      static_cast<const unsigned char*>(stream), R.tileOffset.as<long long>(), R.meta.as<int4>(),
+      R.tileLevel.as<int>(), R.groupStart.as<int>(), R.haloStart.as<int>(), R.haloSrc.as<int>(),
+      static_cast<int>(R.ringBytes), R.maxTileLevels, seedB, pro, static_cast<const W*>(xin), xinZero,
+      static_cast<W*>(xout), A.errFlag.as<int>());
+  checkLaunch("gs_ring");
+}
+}  // namespace
+
+void launchGsRing(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& pro, bool seedB,
+                  const void* xin, bool xinZero, void* xout, DType W, cudaStream_t s) {
+  if (A.vt == DType::F32 && W == DType::F32) gsRingT<float, float>(A, R, stream, pro, seedB, xin, xinZero, xout, s);
+  else if (A.vt == DType::F32 && W == DType::F64)
+    gsRingT<float, double>(A, R, stream, pro, seedB, xin, xinZero, xout, s);
+  else if (A.vt == DType::F64 && W == DType::F64)
+    gsRingT<double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, s);
+  else fail(GR_EUNSUPPORTED, "Gauss-Seidel with float64 coefficients needs float64 vectors");
 }
 
 void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,

@@ -83,7 +83,7 @@ void launchPackBytes(DeviceMatrix& A, const void* templ, i64 bytes, const int* v
 // per block, packing of a solver's copy of the level blocks, and the launch.
 // Blocks of the ring kernel (value type vt) an SM holds when shared memory
 // is not the limit (0 if unknown).
-int ringBlocksPerSMWithoutSmem(DType vt);
+int ringBlocksPerSMWithoutSmem(DType vt, RingKind kind = RingKind::Ilu);
 size_t iluRingSmem(const DeviceMatrix& A, const LevelRing& R, DType W);
 void launchRingPack(DeviceMatrix& A, const LevelRing& R, void* stream, const void* F, const void* inv,
                     cudaStream_t s);
@@ -91,6 +91,14 @@ void launchRingPack(DeviceMatrix& A, const LevelRing& R, void* stream, const voi
 // default); unroll: rows of up to four entries load all their terms at once.
 void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,
                    void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s);
+// One Gauss-Seidel sweep through a Gauss-Seidel level ring (kernels_ring.cu):
+// xout from xin (xinZero: xin is all zeros and is not read; the ring may
+// then be a lower-only one). The right-hand side is the prologue's vector
+// (seedB), or each row starts from its diagonal (seedB false, the
+// reference's CodeDSL solver, gauss-seidel/Solver.cpp:74). stream: the ring
+// template with the coefficients and the diagonal packed in.
+void launchGsRing(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& pro, bool seedB,
+                  const void* xin, bool xinZero, void* xout, DType W, cudaStream_t s);
 // Warp-per-tile substitution (kernels_warp.cu): shared memory per block and
 // the number of rows per lane to prefetch.
 size_t iluWarpSmem(const DeviceMatrix& A, const SweepStream& S, DType W);
@@ -107,15 +115,42 @@ void launchGsSweep(DeviceMatrix& A, const void* Gval, const void* b, bool seedB,
 
 // ---- Krylov kernels ----------------------------------------------------
 // r = b - A x, r0 = r; state initialised (norm, rho = r0.r, flags).
+// stateless (this and the next two): the vectors only, no reduction and no
+// state update (the reference-order reductions below do those).
 void launchBicgInit(DeviceMatrix& A, const void* x, const void* b, void* r, void* r0, KState* st,
-                    DType W, cudaStream_t s);
+                    DType W, cudaStream_t s, bool stateless = false);
 // y = A x and the dots of the step: mode 0: alpha = rho / (r0 . y);
 // mode 1: omega = (y . s) / (y . y), singularity check.
 void launchSpmvDot(DeviceMatrix& A, const void* x, void* y, const void* d1, int mode, KState* st,
-                   DType W, cudaStream_t s);
+                   DType W, cudaStream_t s, bool stateless = false);
 // x = x + alpha y + omega z; r = s - omega t; convergence; next rho, beta.
 void launchBicgUpdate(DeviceMatrix& A, void* x, const void* y, const void* z, void* r, const void* sv,
-                      const void* t, const void* r0, KState* st, DType W, cudaStream_t s);
+                      const void* t, const void* r0, KState* st, DType W, cudaStream_t s, bool stateless = false);
+
+// ---- the reference's reduction order ("reduce": "f32_ref_order") -------
+// A reduction over the non-halo rows, per tile in the reference's order
+// (six worker chunks, then the partials; dsl/tensor/Expression.cpp:472-481,
+// :597-646) and across tiles in runs of 368, 736, 1472 and all tiles
+// (:680-769), accumulating in float.
+enum class RefKind : int { None = 0, Dot = 1, SquareSum = 2, Sum = 3, Max = 4 };
+struct RefRed {
+  RefKind kind = RefKind::None;
+  const void* a = nullptr;
+  const void* b = nullptr;  // Dot: a . b
+};
+// What the reduced values update in the state (one thread):
+//  BNorm:  bNorm = norm(q0)
+//  Init:   rho = q0 (r0 . r), normInit = normFinal = norm(q1), flags
+//  Alpha:  alpha = rho / q0
+//  Omega:  omega = q1 / q0 (q0 = t . t, q1 = t . s), singularity
+//  Update: normFinal = norm(q1), convergence, iteration count, next rho
+//          = q0 and beta, singularity
+// Norms are rounded to float and compared in float, as the reference's
+// SolverStats tensors are (SolverStats.hpp:33-36).
+enum class RefStage : int { BNorm = 0, Init = 1, Alpha = 2, Omega = 3, Update = 4 };
+// tiles: scratch of 2 P floats.
+void launchRefReduce(DeviceMatrix& A, const RefRed& q0, const RefRed& q1, RefStage stage, KState* st, void* tiles,
+                     cudaStream_t s);
 // Elementwise prologue when no fused preconditioner is used; also copies
 // the result into copyTo when non-null.
 void launchPrologue(DeviceMatrix& A, const PrologueArgs& pro, void* copyTo, DType W, cudaStream_t s);

@@ -395,10 +395,12 @@ inline bool overlaps(i64 a, i64 sa, i64 b, i64 sb) { return a < b + sb && b < a 
 }  // namespace
 
 HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes, i32 group,
-                        const RingBudget& budget, bool allowCompact) {
+                        const RingBudget& budget, bool allowCompact, RingKind kind) {
   const i64 vs = static_cast<i64>(dtypeSize(vt));
   const i64 entSize = vs == 4 ? 8 : 16;
+  const bool gs = kind != RingKind::Ilu;
   if (group < 1) fail(GR_EINVAL, "tiles per block must be at least 1");
+  if (gs && group != 1) fail(GR_EINVAL, "Gauss-Seidel rings run one tile per block");
   // A block runs `group` consecutive tiles in lockstep: level l of the block
   // is level l of each of its tiles (the tiles are independent, so their
   // rows never reference one another), rows numbered from the block's first
@@ -407,7 +409,27 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
   i64 maxGroupRows = 0;
   for (i32 G = 0; G < NG; ++G)
     maxGroupRows = std::max<i64>(maxGroupRows, H.tileStart[std::min<i32>(H.P, (G + 1) * group)] - H.tileStart[G * group]);
-  const bool compact = allowCompact && maxGroupRows + 1 <= kRingCompactRows;
+  // Gauss-Seidel: x slots per tile (this sweep's values, the sweep-start
+  // values, the halo and the zero slot) and the halo cells' tile-order
+  // indices.
+  i64 maxGsSlots = 0;
+  std::vector<i32> haloStart, haloSrc;
+  if (gs) {
+    haloStart.assign(H.P + 1, 0);
+    for (i32 T = 0; T < H.P; ++T) {
+      haloStart[T + 1] = haloStart[T] + static_cast<i32>(H.tiles[T].nHalo);
+      maxGsSlots = std::max<i64>(maxGsSlots, 2 * H.tiles[T].rows() + H.tiles[T].nHalo + 1);
+    }
+    haloSrc.assign(haloStart[H.P], -1);
+    parallelFor(H.P, [&](i64 T) {
+      const i64 base = H.tileStart[T], nRows = H.tileStart[T + 1] - base;
+      for (i64 k = H.rowPtr[base]; k < H.rowPtr[base + nRows]; ++k)
+        if (H.colLocal[k] >= nRows) haloSrc[haloStart[T] + H.colLocal[k] - nRows] = H.colPerm[k];
+    });
+    for (i32 v : haloSrc)
+      if (v < 0) fail(GR_EINVAL, "Gauss-Seidel ring: a halo cell no entry reads");
+  }
+  const bool compact = allowCompact && (gs ? maxGsSlots <= kRingCompactRows : maxGroupRows + 1 <= kRingCompactRows);
   std::vector<TileRing> tr(NG);
   parallelFor(NG, [&](i64 G) {
     TileRing& t = tr[G];
@@ -415,9 +437,11 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
     const i64 gBase = H.tileStart[T0];
     const i64 gRows = H.tileStart[T1] - gBase;
     std::vector<i64> ent;
-    for (int sweep = 0; sweep < 2; ++sweep) {
+    const i64 zeroSlot = gs ? 2 * gRows + H.tiles[T0].nHalo : gRows;
+    for (int sweep = 0; sweep < (gs ? 1 : 2); ++sweep) {
       const bool upper = sweep == 1;
-      const SweepEntries kind = upper ? SweepEntries::UpperDesc : SweepEntries::Lower;
+      const SweepEntries ekind = gs ? (kind == RingKind::GaussSeidelLower ? SweepEntries::Lower : SweepEntries::All)
+                                    : (upper ? SweepEntries::UpperDesc : SweepEntries::Lower);
       const std::vector<i32>& lev = upper ? H.upperLevel : H.lowerLevel;
       i32 nLv = 0;
       for (i32 T = T0; T < T1; ++T) nLv = std::max(nLv, upper ? H.nUpperLevels[T] : H.nLowerLevels[T]);
@@ -425,14 +449,14 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
       std::vector<std::vector<std::pair<i64, i32>>> byLevel(nLv);
       for (i32 T = T0; T < T1; ++T)
         for (i64 p = H.tileStart[T]; p < H.tileStart[T + 1]; ++p) byLevel[lev[p]].emplace_back(p - gBase, T);
-      const bool hasInv = upper || dilu;
+      const bool hasInv = gs || upper || dilu;  // Gauss-Seidel: the diagonal
       for (i32 l = 0; l < nLv; ++l) {
         const auto& rows = byLevel[l];
         const i64 k = static_cast<i64>(rows.size());
         i64 E = 0;
         for (const auto& [gl, T] : rows) {
           const i64 tb = H.tileStart[T] - gBase;
-          rowEntries(H, kind, gBase + gl, gl - tb, H.tileStart[T + 1] - H.tileStart[T], ent);
+          rowEntries(H, ekind, gBase + gl, gl - tb, H.tileStart[T + 1] - H.tileStart[T], ent);
           E = std::max<i64>(E, static_cast<i64>(ent.size()));
         }
         if (E >= (i64(1) << kRingEBits) || k >= (i64(1) << 31) || entSize * E * k >= (i64(1) << 31))
@@ -453,10 +477,14 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
             std::memcpy(t.bytes.data() + start + 4 * q, &r32, 4);
           }
           if (hasInv) t.invs.emplace_back(start + lay.inv + vs * q, static_cast<i32>(gBase + gl));
-          rowEntries(H, kind, gBase + gl, gl - tb, H.tileStart[T + 1] - H.tileStart[T], ent);
+          rowEntries(H, ekind, gBase + gl, gl - tb, H.tileStart[T + 1] - H.tileStart[T], ent);
           for (i64 e = 0; e < E; ++e) {
             const bool real = e < static_cast<i64>(ent.size());
-            const i32 col = real ? static_cast<i32>(H.colLocal[ent[e]] + tb) : static_cast<i32>(gRows);
+            i32 col = static_cast<i32>(zeroSlot);
+            if (real) {
+              const i64 lc = H.colLocal[ent[e]];
+              col = static_cast<i32>(gs ? (lc < gl ? lc : gRows + lc) : lc + tb);
+            }
             if (compact) {
               const uint16_t c16 = static_cast<uint16_t>(col);
               std::memcpy(t.bytes.data() + start + lay.ents + 2 * (e * k + q), &c16, 2);
@@ -544,7 +572,8 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
     // the largest level), one that places and runs all blocks in the fewest
     // waves (blocks resident per SM from the budget); the largest such, as a
     // larger ring lets copies run further ahead.
-    const i64 fixed = ringFixedSmem(maxLevels, maxGroupRows, vs) + budget.reservedPerBlock;
+    const i64 fixed = ringFixedSmemSlots(maxLevels, gs ? maxGsSlots + maxGroupRows : maxGroupRows + 1, vs) +
+                      budget.reservedPerBlock;
     const i64 lo = std::max<i64>(256, pad16(2 * R.maxLevelBytes));
     const i64 hi = std::max<i64>(std::max<i64>(16384, pad16(4 * R.maxLevelBytes)), lo);
     const i64 step = std::max<i64>(256, pad16(R.maxLevelBytes / 16));
@@ -575,6 +604,10 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
   if (R.ringBytes > (i64(1) << kRingOffBits)) fail(GR_EUNSUPPORTED, "ILU level ring too large");
   R.group = group;
   R.compact = compact;
+  R.kind = kind;
+  R.maxXSlots = gs ? maxGsSlots + maxGroupRows : maxGroupRows + 1;
+  R.haloStart = std::move(haloStart);
+  R.haloSrc = std::move(haloSrc);
   R.tileOffset.assign(NG + 1, 0);
   R.tileLevel.assign(NG + 1, 0);
   R.groupStart.assign(NG + 1, 0);
@@ -610,7 +643,7 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
       int4 m = tr[T].meta[l];
       const bool upper = (m.y & kRingUpperBit) != 0;
       const uint32_t E = static_cast<uint32_t>(m.y & (kRingUpperBit - 1));
-      const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(m.x), E, upper || dilu,
+      const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(m.x), E, gs || upper || dilu,
                                                   static_cast<uint32_t>(vs), compact);
       m.y = static_cast<int>(E | ((lay.ents >> 4) << kRingEBits) | (upper ? static_cast<uint32_t>(kRingUpperBit) : 0u));
       m.z = static_cast<int>(static_cast<uint32_t>(m.z) | ((lay.bytes >> 4) << kRingOffBits));
@@ -635,10 +668,14 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
     fail(GR_EINVAL, "level ring check: block " + std::to_string(G) + " level " + std::to_string(l) + ": " + what);
   };
   const i32 group = R.group;
+  const bool gs = R.kind != RingKind::Ilu;
   const i32 NG = group > 0 ? (H.P + group - 1) / group : -1;
   if (NG < 1 || static_cast<i32>(R.tileOffset.size()) != NG + 1 || static_cast<i32>(R.tileLevel.size()) != NG + 1 ||
       static_cast<i32>(R.groupStart.size()) != NG + 1)
     fail(GR_EINVAL, "level ring check: table sizes");
+  if (gs && (group != 1 || static_cast<i32>(R.haloStart.size()) != H.P + 1 ||
+             static_cast<i64>(R.haloSrc.size()) != static_cast<i64>(R.haloStart.back())))
+    fail(GR_EINVAL, "level ring check: Gauss-Seidel tables");
   for (i32 G = 0; G < NG; ++G) {
     const i32 T0 = G * group, T1 = std::min<i32>(H.P, T0 + group);
     const i64 gBase = H.tileStart[T0], gRows = H.tileStart[T1] - gBase;
@@ -651,7 +688,16 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
       nUpper = std::max(nUpper, H.nUpperLevels[T]);
     }
     const i64 L = R.tileLevel[G + 1] - R.tileLevel[G];
-    if (L != nLower + nUpper) bad(G, -1, "level count");
+    if (L != (gs ? nLower : nLower + nUpper)) bad(G, -1, "level count");
+    // Gauss-Seidel slots: this sweep's values, the sweep-start values, the
+    // halo, the zero slot.
+    const i64 nHalo = gs ? H.tiles[T0].nHalo : 0;
+    if (gs) {
+      for (i64 h = 0; h < nHalo; ++h) {
+        const i32 src = R.haloSrc[R.haloStart[T0] + h];
+        if (src < 0 || src >= H.n || (src >= gBase && src < gBase + gRows)) bad(G, -1, "halo source");
+      }
+    }
     std::vector<char> doneL(gRows, 0), doneU(gRows, 0);
     std::vector<i64> ringOff(L), size(L);
     i64 src = R.tileOffset[G], prevIa = -1;
@@ -661,7 +707,7 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
       const i64 ia = RingLevelCode::issueAfter(a);
       const bool upper = RingLevelCode::upper(a);
       if (upper != (l >= nLower)) bad(G, l, "sweep flag");
-      const bool hasInv = upper || dilu;
+      const bool hasInv = gs || upper || dilu;
       const i64 idB = R.compact ? 2 : 4;
       const i64 rowsB = pad16(idB * k), invB = hasInv ? pad16(vs * k) : 0;
       const i64 colsB = R.compact ? pad16(2 * E * k) : pad16(entSize * E * k);
@@ -707,6 +753,16 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
           } else {
             std::memcpy(&c, blk + entOff + entSize * (e * k + q), 4);
           }
+          if (gs) {
+            // New value of an earlier row, start value of a later row or of
+            // a halo cell, or the zero slot (lower-only rings: no start values).
+            const bool lowerOnly = R.kind == RingKind::GaussSeidelLower;
+            if (c < 0 || c > 2 * gRows + nHalo) bad(G, l, "column index");
+            if (c < gRows && (!done[c] || c >= il)) bad(G, l, "dependency order");
+            if (c >= gRows && c < 2 * gRows && (lowerOnly || c - gRows <= il)) bad(G, l, "start value");
+            if (c >= 2 * gRows && c < 2 * gRows + nHalo && lowerOnly) bad(G, l, "halo in a lower-only ring");
+            continue;
+          }
           if (c < 0 || c > gRows) bad(G, l, "column index");
           if (c < gRows && (tileOf[c] != tileOf[il] || !done[c] || (upper ? c <= il : c >= il)))
             bad(G, l, "dependency order");
@@ -718,12 +774,12 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
     }
     if (src != R.tileOffset[G + 1]) bad(G, L, "stream length");
     for (i64 i = 0; i < gRows; ++i)
-      if (!doneL[i] || !doneU[i]) bad(G, L, "row not covered");
+      if (!doneL[i] || (!gs && !doneU[i])) bad(G, L, "row not covered");
   }
 }
 
-LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group, bool allowCompact) {
-  auto key = std::make_tuple(dilu, ringBytes, group, allowCompact);
+LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group, bool allowCompact, RingKind kind) {
+  auto key = std::make_tuple(dilu, ringBytes, group, allowCompact, static_cast<int>(kind));
   auto it = levelRings.find(key);
   if (it != levelRings.end()) return *it->second;
   RingBudget budget;
@@ -734,8 +790,8 @@ LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group, bool all
     budget.smemPerSM = v;
   if (cudaDeviceGetAttribute(&v, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess)
     budget.reservedPerBlock = v;
-  if (const int b = ringBlocksPerSMWithoutSmem(vt); b > 0) budget.maxBlocksPerSM = b;
-  HostRing H = buildLevelRing(*host, dilu, vt, ringBytes, group, budget, allowCompact);
+  if (const int b = ringBlocksPerSMWithoutSmem(vt, kind); b > 0) budget.maxBlocksPerSM = b;
+  HostRing H = buildLevelRing(*host, dilu, vt, ringBytes, group, budget, allowCompact, kind);
   auto R = std::make_unique<LevelRing>();
   R->dilu = dilu;
   R->bytes = static_cast<i64>(H.bytes.size());
@@ -756,6 +812,12 @@ LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group, bool all
   R->valSrc.upload(H.valSrc);
   R->invPos.upload(H.invPos);
   R->invSrc.upload(H.invSrc);
+  R->kind = H.kind;
+  R->maxXSlots = H.maxXSlots;
+  if (H.kind != RingKind::Ilu) {
+    R->haloStart.upload(H.haloStart);
+    if (!H.haloSrc.empty()) R->haloSrc.upload(H.haloSrc);
+  }
   LevelRing& ref = *R;
   levelRings[key] = std::move(R);
   return ref;

@@ -281,6 +281,25 @@ int Server::wait(u64 id, double timeoutMs, void* x, gr_stats* stats, gr_request_
   return GR_OK;
 }
 
+bool Server::cancel(u64 id) {
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = requests_.find(id);
+    if (it == requests_.end()) fail(GR_EINVAL, "unknown request id " + std::to_string(id));
+    std::shared_ptr<Request> r = it->second;
+    auto q = std::find(queue_.begin(), queue_.end(), r);
+    if (q == queue_.end()) return false;  // admitted (running or finished)
+    queue_.erase(q);
+    r->status = GR_ECANCELED;
+    r->err = "request cancelled before it was admitted";
+    r->tFinish = now();
+    r->done = true;
+  }
+  cvDone_.notify_all();
+  cvWork_.notify_all();  // the head may have changed
+  return true;
+}
+
 void Server::counters(i64* queued, i64* running, i64* completed, i64* bytesInUse, i64* resident) {
   std::lock_guard<std::mutex> lk(mu_);
   if (queued) *queued = static_cast<i64>(queue_.size());

@@ -50,6 +50,9 @@ class Server {
   int wait(u64 id, double timeoutMs, void* x, gr_stats* stats, gr_request_times* times, int* status,
            std::string* err);
   void counters(i64* queued, i64* running, i64* completed, i64* bytesInUse, i64* resident);
+  // Removes request id from the queue if it has not been admitted (true);
+  // its wait then reports GR_ECANCELED. False when it is running or done.
+  bool cancel(u64 id);
 
  private:
   struct Entry;

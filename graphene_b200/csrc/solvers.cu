@@ -166,15 +166,58 @@ class GsNode : public Node {
  public:
   GsNode(DeviceMatrix& A, const SolverConfig& c) : Node(A, c) {
     A.ensureLocalCrs();
-    LevelSchedule& G = A.schedule(SweepEntries::All);
-    Gval_.alloc(std::max<i64>(1, G.slots) * dtypeSize(A.vt));
-    launchPack(A, G, A.offDiag.get(), Gval_.get(), s());
+    // The level-ring kernel when the tiles fit shared memory (for either
+    // vector type): one ring with every entry, and one with the lower
+    // entries only for sweeps that start from x = 0.
+    if (c.gsKernel != 2) {
+      try {
+        ring_ = &A.levelRing(false, 0, 1, true, RingKind::GaussSeidel);
+        ringLo_ = &A.levelRing(false, 0, 1, true, RingKind::GaussSeidelLower);
+      } catch (const Error&) {
+        if (c.gsKernel == 1) throw;
+        ring_ = ringLo_ = nullptr;
+      }
+      const size_t smemMax = static_cast<size_t>(maxDynamicSmem(A));
+      if (ring_ && (iluRingSmem(A, *ring_, DType::F64) > smemMax || iluRingSmem(A, *ringLo_, DType::F64) > smemMax)) {
+        if (c.gsKernel == 1)
+          fail(GR_EUNSUPPORTED, "the Gauss-Seidel ring kernel does not fit this matrix's tiles in shared memory");
+        ring_ = ringLo_ = nullptr;
+      }
+    }
+    if (ring_) {
+      stream_.alloc(std::max<i64>(16, ring_->bytes));
+      launchRingPack(A, *ring_, stream_.get(), A.offDiag.get(), A.diag.get(), s());
+      streamLo_.alloc(std::max<i64>(16, ringLo_->bytes));
+      launchRingPack(A, *ringLo_, streamLo_.get(), A.offDiag.get(), A.diag.get(), s());
+    } else {
+      LevelSchedule& G = A.schedule(SweepEntries::All);
+      Gval_.alloc(std::max<i64>(1, G.slots) * dtypeSize(A.vt));
+      launchPack(A, G, A.offDiag.get(), Gval_.get(), s());
+    }
     GR_CUDA(cudaStreamSynchronize(s()));
+  }
+
+  // Whether the first sweep can take PBiCGStab's p / s update as its
+  // right-hand side (the level-ring kernel), and that application:
+  // numFixedIterations sweeps from x = 0.
+  bool fusedPrologue() const { return ring_ != nullptr && cfg_.numFixedIterations > 0; }
+  void applyFused(const PrologueArgs& pro, void* out, DType W) {
+    if (workingType(cfg_, W) != W)
+      fail(GR_EUNSUPPORTED, "GaussSeidel workingType different from the vector type");
+    ringSweeps(pro, out, W, cfg_.numFixedIterations, true);
   }
 
   // Sweeps ping-pong between x and a scratch vector; the result ends in x.
   void sweeps(void* x, const void* b, DType W, int count, bool xZero, const KState* gate) {
     if (count <= 0) return;
+    if (ring_) {
+      PrologueArgs pro;
+      pro.kind = Prologue::Plain;
+      pro.b = b;
+      pro.st = gate;
+      ringSweeps(pro, x, W, count, xZero);
+      return;
+    }
     ensureTmp(W);
     void* cur = x;
     void* other = tmp_.get();
@@ -249,7 +292,29 @@ class GsNode : public Node {
     const size_t bytes = A_.n * dtypeSize(W);
     if (tmp_.bytes() < bytes) tmp_.alloc(bytes);
   }
-  DBuf Gval_, tmp_;
+  // Level-ring sweeps: the first takes its right-hand side from `first`
+  // (b itself, or a fused p / s update, which it also writes); later ones
+  // from b or the written p / s. A sweep from x = 0 uses the lower-only ring.
+  void ringSweeps(const PrologueArgs& first, void* x, DType W, int count, bool xZero) {
+    if (count <= 0) return;
+    ensureTmp(W);
+    PrologueArgs plain;
+    plain.kind = Prologue::Plain;
+    plain.b = first.kind == Prologue::Plain ? first.b : first.pOrS;
+    plain.st = first.st;
+    void* cur = x;
+    void* other = tmp_.get();
+    for (int k = 0; k < count; ++k) {
+      const bool zero = xZero && k == 0;
+      launchGsRing(A_, zero ? *ringLo_ : *ring_, zero ? streamLo_.get() : stream_.get(), k == 0 ? first : plain,
+                   cfg_.gsSeedB, cur, zero, other, W, s());
+      std::swap(cur, other);
+    }
+    if (cur != x) GR_CUDA(cudaMemcpyAsync(x, cur, A_.n * dtypeSize(W), cudaMemcpyDeviceToDevice, s()));
+  }
+  const LevelRing* ring_ = nullptr;
+  const LevelRing* ringLo_ = nullptr;
+  DBuf Gval_, tmp_, stream_, streamLo_;
 };
 
 // Pinned host mirrors of the Krylov state, handed out from slabs that are
@@ -258,7 +323,7 @@ class GsNode : public Node {
 namespace {
 constexpr size_t kPinnedSlot = 256;
 constexpr size_t kPinnedSlab = 256;  // slots per cudaMallocHost
-static_assert(sizeof(KState) <= kPinnedSlot, "KState must fit a pinned slot");
+static_assert(sizeof(KState) + sizeof(int) <= kPinnedSlot, "KState and the error word must fit a pinned slot");
 std::mutex g_pinnedMu;
 std::vector<void*> g_pinnedFree;
 
@@ -303,7 +368,7 @@ class PbicgstabNode : public Node {
       if (!ilu_ || !ilu_->ringKernel())
         fail(GR_EUNSUPPORTED, "batched PBiCGStab needs the ILU preconditioner with the ring kernel");
       systems_ = A.batch->systems;
-      GR_CUDA(cudaMallocHost(&host_, sizeof(KState) * systems_));
+      GR_CUDA(cudaMallocHost(&host_, sizeof(KState) * systems_ + sizeof(int)));
       batchHost_ = true;
     } else {
       host_ = static_cast<KState*>(acquirePinnedSlot());
@@ -320,7 +385,12 @@ class PbicgstabNode : public Node {
     (void)gate;
     const DType W = workingType(cfg_, Wx);
     if (W != Wx) fail(GR_EUNSUPPORTED, "PBiCGStab workingType different from the vector type");
+    const bool ref = cfg_.reduceRef;
+    if (ref && (W != DType::F32 || A_.batch))
+      fail(GR_EUNSUPPORTED, "reduce \"f32_ref_order\" needs float32 vectors and a single system");
     ensureBuffers(W);
+    if (ref && refTiles_.bytes() < 2 * static_cast<size_t>(A_.P) * sizeof(float))
+      refTiles_.alloc(2 * static_cast<size_t>(A_.P) * sizeof(float));
     const size_t vb = A_.n * dtypeSize(W);
     KState init{};
     init.absTol = cfg_.absTolerance;
@@ -334,7 +404,9 @@ class PbicgstabNode : public Node {
     // The reference takes ||x|| here (pbicgstab/Solver.cpp:69-70); the norm
     // of b is what relTolerance is documented to use (SolverStats.hpp:52-60).
     if (cfg_.relTolerance > 0) {
-      if (!A_.batch) {
+      if (ref) {
+        launchRefReduce(A_, RefRed{normRed(), b, nullptr}, RefRed{}, RefStage::BNorm, st, refTiles_.get(), s());
+      } else if (!A_.batch) {
         launchNorm(A_, b, W, cfg_.norm, &st->bNorm, s());
       } else {
         for (int k = 0; k < systems_; ++k)
@@ -343,7 +415,10 @@ class PbicgstabNode : public Node {
       }
     }
     GR_CUDA(cudaMemcpyAsync(xw(), x, vb, cudaMemcpyDeviceToDevice, s()));
-    launchBicgInit(A_, xw(), b, buf(R), buf(R0), st, W, s());
+    launchBicgInit(A_, xw(), b, buf(R), buf(R0), st, W, s(), ref);
+    if (ref)
+      launchRefReduce(A_, RefRed{RefKind::Dot, buf(R0), buf(R)}, RefRed{normRed(), buf(R), nullptr}, RefStage::Init,
+                      st, refTiles_.get(), s());
     const bool graphable = ilu_ || !pre_ || (gs_ && cfg_.preconditioner->numFixedIterations > 0);
     const bool perIter = cfg_.printPerformanceEachIteration;
     int issued = 0;
@@ -356,8 +431,13 @@ class PbicgstabNode : public Node {
         issued += 1;
       }
       GR_CUDA(cudaMemcpyAsync(host_, st, sizeof(KState) * systems_, cudaMemcpyDeviceToHost, s()));
+      // The matrix's error word rides along: a kernel whose bounded wait ran
+      // out (or a status injected from the host) ends the solve here; the
+      // tree reports it.
+      GR_CUDA(cudaMemcpyAsync(errHost(), A_.errFlag.get(), sizeof(int), cudaMemcpyDeviceToHost, s()));
       GR_CUDA(cudaStreamSynchronize(s()));
       if (perIter) printStats(cfg_, A_, stats());
+      if (*errHost() != 0) break;
       bool all = true;
       for (int k = 0; k < systems_; ++k) all = all && host_[k].done;
       if (all) break;
@@ -366,6 +446,10 @@ class PbicgstabNode : public Node {
     GR_CUDA(cudaMemcpyAsync(x, xw(), vb, cudaMemcpyDeviceToDevice, s()));
     GR_CUDA(cudaStreamSynchronize(s()));
     gr_stats out = stats();
+    if (*errHost() != 0) {  // a device-side wait ran out (or an injected status)
+      out.status = *errHost();
+      out.converged = 0;
+    }
     if (cfg_.printPerformanceAfterSolve) printStats(cfg_, A_, out);
     return out;
   }
@@ -393,6 +477,12 @@ class PbicgstabNode : public Node {
   int graphKernels_ = 0;
 
   void* buf(int i) { return static_cast<char*>(vec_.get()) + static_cast<size_t>(i) * A_.n * dtypeSize(bufType_); }
+  DBuf refTiles_;  // per-tile values of the reference-order reductions
+  RefKind normRed() const {
+    return cfg_.norm == GR_NORM_L1 ? RefKind::Sum : (cfg_.norm == GR_NORM_LINF ? RefKind::Max : RefKind::SquareSum);
+  }
+  // Pinned host word for the matrix's error flag, after the states.
+  int* errHost() { return reinterpret_cast<int*>(host_ + systems_); }
   void* xw() { return buf(X); }
 
   void ensureBuffers(DType W) {
@@ -441,6 +531,10 @@ class PbicgstabNode : public Node {
       launchPrologue(A_, pro, out, W, s());
       return;
     }
+    if (gs_ && gs_->fusedPrologue()) {
+      gs_->applyFused(pro, out, W);
+      return;
+    }
     launchPrologue(A_, pro, nullptr, W, s());
     const void* in = pro.pOrS;
     if (gs_) {
@@ -453,6 +547,10 @@ class PbicgstabNode : public Node {
 
   // One PBiCGStab iteration (pbicgstab/Solver.cpp:90-186).
   void iteration(DType W) {
+    if (cfg_.reduceRef) {
+      iterationRef(W);
+      return;
+    }
     KState* st = st_.as<KState>();
     PrologueArgs p;
     p.kind = Prologue::PUpdate;
@@ -473,6 +571,36 @@ class PbicgstabNode : public Node {
     precondition(q, buf(Z), W);
     launchSpmvDot(A_, buf(Z), buf(T), buf(S), 1, st, W, s());
     launchBicgUpdate(A_, xw(), buf(Y), buf(Z), buf(R), buf(S), buf(T), buf(R0), st, W, s());
+  }
+
+  // The same iteration with the reference's float reductions: the fused
+  // kernels compute the vectors only, and each dot product / norm is a
+  // reference-order reduction whose last step derives the scalars in float.
+  void iterationRef(DType W) {
+    KState* st = st_.as<KState>();
+    void* tiles = refTiles_.get();
+    PrologueArgs p;
+    p.kind = Prologue::PUpdate;
+    p.r = buf(R);
+    p.pOrS = buf(P);
+    p.v = buf(V);
+    p.st = st;
+    precondition(p, buf(Y), W);
+    launchSpmvDot(A_, buf(Y), buf(V), buf(R0), 0, st, W, s(), true);
+    launchRefReduce(A_, RefRed{RefKind::Dot, buf(R0), buf(V)}, RefRed{}, RefStage::Alpha, st, tiles, s());
+    PrologueArgs q;
+    q.kind = Prologue::SUpdate;
+    q.r = buf(R);
+    q.pOrS = buf(S);
+    q.v = buf(V);
+    q.st = st;
+    precondition(q, buf(Z), W);
+    launchSpmvDot(A_, buf(Z), buf(T), buf(S), 1, st, W, s(), true);
+    launchRefReduce(A_, RefRed{RefKind::Dot, buf(T), buf(T)}, RefRed{RefKind::Dot, buf(T), buf(S)}, RefStage::Omega,
+                    st, tiles, s());
+    launchBicgUpdate(A_, xw(), buf(Y), buf(Z), buf(R), buf(S), buf(T), buf(R0), st, W, s(), true);
+    launchRefReduce(A_, RefRed{RefKind::Dot, buf(R0), buf(R)}, RefRed{normRed(), buf(R), nullptr}, RefStage::Update,
+                    st, tiles, s());
   }
 
   void launchBatch(DType W) {
@@ -539,6 +667,10 @@ class MpirNode : public Node {
       if (inner_->usesInitialGuess()) GR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(float), s()));
       gr_stats is = inner_->solve(x, r, DType::F32, nullptr);
       innerTotal += is.inner_iterations > 0 ? is.inner_iterations : is.iterations;
+      if (is.status != GR_OK) {  // the inner solve failed on the device: no correction to apply
+        st.status = is.status;
+        break;
+      }
       launchPhiUpdate(phi_.get(), static_cast<const float*>(x), E_, n, s());
       launchResidual(A_, phi_.get(), E_, b, DType::F32, r, DType::F32, E_, cfg_.norm, d, s());
       st.final_residual = readScalar(d);

@@ -50,6 +50,7 @@ extern "C" {
 #define GR_EUNSUPPORTED 8 /* combination not supported (reference: runtime_error) */
 #define GR_EIO 9          /* file could not be opened */
 #define GR_ENONFINITE 10  /* NaN or Inf detected in a residual norm */
+#define GR_ECANCELED 11   /* a queued server request was cancelled before it ran */
 
 /* ---- enumerations ---------------------------------------------------- */
 /* Element types; names follow common/Type.hpp:125-214 (parseType accepts
@@ -256,6 +257,15 @@ int gr_host_matrix_check_ilu_ring(const gr_host_matrix* h, int dilu, gr_dtype va
                                   int32_t tiles_per_block, int32_t allow_compact, int64_t* ring_bytes_used,
                                   int64_t* stream_bytes, int32_t* max_tile_levels);
 
+/* The same for the Gauss-Seidel sweep's level ring (one tile per block):
+ * every entry must read this sweep's value of an earlier row of its tile,
+ * the sweep-start value of a later row or of a halo cell, or the zero slot
+ * (lower_only: the ring of a sweep from x = 0, which keeps only the entries
+ * of earlier rows). Host only. No counterpart in the reference. */
+int gr_host_matrix_check_gs_ring(const gr_host_matrix* h, int lower_only, gr_dtype value_type, int64_t ring_bytes,
+                                 int32_t allow_compact, int64_t* ring_bytes_used, int64_t* stream_bytes,
+                                 int32_t* max_tile_levels);
+
 /* DistributedTileLayout::loadVectorFromFile (DistributedTileLayout.cpp:185-206,
  * without halo): reads a MatrixMarket vector (a "vector" object, coordinate
  * or array, or the first column of a "matrix" object; unlisted entries are
@@ -307,6 +317,14 @@ int gr_residual(gr_matrix* A, const void* x, gr_dtype x_t, const void* b, gr_dty
 /* Replaces Matrix::vectorNorm(norm, x) (matrix/Matrix.hpp:120-122,
  * details/MatrixBase.cpp:149-152). Accumulates in FP64. */
 int gr_vector_norm(gr_matrix* A, gr_norm norm, const void* x, gr_dtype t, double* out);
+
+/* Failure injection from the host (no counterpart in the reference):
+ * stores `status` (GR_ETIMEOUT, ...) in the matrix's device error word, the
+ * word a kernel whose bounded wait ran out writes. The next solve on A then
+ * stops at its first convergence check and reports that status, and the
+ * word is cleared, as after a real device-side timeout. No kernel runs and
+ * nothing faults; tests use it to exercise the failure path. */
+int gr_matrix_inject_status(gr_matrix* A, int32_t status);
 
 /* Norms of `count` device vectors of n elements (vector j starts at element
  * j * ld of x), FP64 accumulation, written to out[0..count) (device
@@ -419,6 +437,12 @@ int gr_server_wait(gr_server* s, uint64_t id, double timeout_ms, void* x_out, gr
  * pairs; number of resident pairs. Any pointer may be NULL. */
 int gr_server_counters(gr_server* s, int64_t* queued, int64_t* running, int64_t* completed,
                        int64_t* bytes_in_use, int64_t* resident);
+/* Cancels request id if it is still queued (not yet admitted): *cancelled
+ * = 1, and gr_server_wait then returns GR_ECANCELED for it. A request that
+ * has been admitted runs to completion: *cancelled = 0. GR_EINVAL for an
+ * unknown id. No counterpart in the reference (one compiled graph runs at a
+ * time there). */
+int gr_server_cancel(gr_server* s, uint64_t id, int32_t* cancelled);
 /* Finishes the running solves, drops the queued ones, releases everything. */
 void gr_server_destroy(gr_server* s);
 

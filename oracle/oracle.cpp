@@ -24,6 +24,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <memory>
 #include <queue>
@@ -209,6 +210,10 @@ struct Conf {
   int extendedType = -1;    // -1: x.type(); 0 f32, 1 f64, 2 dw
   int maxRestarts = 1;
   int gsSeedB = 1;          // extension: 1 seeds Gauss-Seidel rows with b
+  // extension: PBiCGStab dot products and norms in the reference's own
+  // reduction order and operand type ("reduce": "f32_ref_order") instead of
+  // FP64 accumulation ("float64", the default).
+  bool reduceRef = false;
   std::unique_ptr<Conf> pre, inner;
 };
 
@@ -246,6 +251,11 @@ std::unique_ptr<Conf> parseConf(const JVal& j) {
   if (auto v = j.get("workingType")) c->workingType = parseTypeName(v->s);
   if (auto v = j.get("extendedPrecisionType")) c->extendedType = parseTypeName(v->s);
   if (auto v = j.get("seed")) c->gsSeedB = (v->s == "b") ? 1 : 0;
+  if (auto v = j.get("reduce")) {
+    if (v->s == "f32_ref_order") c->reduceRef = true;
+    else if (v->s == "float64") c->reduceRef = false;
+    else throw OErr("reduce must be \"float64\" or \"f32_ref_order\"");
+  }
   if (auto v = j.get("preconditioner")) c->pre = parseConf(*v);
   if (auto v = j.get("innerSolver")) c->inner = parseConf(*v);
   if (c->type == "IterativeRefinement" && !c->inner)
@@ -688,6 +698,95 @@ double dotT(const or_matrix& A, const std::vector<T>& a, const std::vector<T>& b
   return acc;
 }
 
+// Expression::reduce in the reference's own order, accumulating in the
+// operand type R (dsl/tensor/Expression.cpp:472-481, :597-769), for a value
+// per non-halo row (value(i), i an index of the with-halo layout):
+//  stage 1 (more than 6 rows in all, :735-740): each tile's rows split over
+//    6 workers, chunks of floor(n_t / 6 / 4) * 4 rows with the rest on worker
+//    5 (:472-481), each chunk summed in row order from 0 (out = out + v, or
+//    out + v * v for a squared sum, :522-533);
+//  stage 2 (:743, reducePerTile :597-646): the tile's 6 partials summed in
+//    worker order from 0 (with 6 rows or fewer in all: the tile's rows);
+//  stages 2.1-4 (:749-752, reduceGrouped :680-727): the values of each run
+//    of 368, then 736, then 1472 consecutive tiles, then of all, collected
+//    on the run's first tile (common/Shape.hpp:336-351) and summed in tile
+//    order - per worker first, as in stage 1, when some run holds more than
+//    6 values. A run holding one value passes it on unchanged.
+template <class R, class F>
+R refReduce(const or_matrix& A, F value, bool square) {
+  size_t total = 0;
+  for (size_t t = 0; t < A.P; ++t) total += A.tileStart[t + 1] - A.tileStart[t];
+  auto seqSum = [&](auto get, size_t b, size_t e, bool sq) {
+    R acc = R(0);
+    for (size_t i = b; i < e; ++i) {
+      const R v = get(i);
+      acc = sq ? acc + v * v : acc + v;
+    }
+    return acc;
+  };
+  // Per worker (6 chunks), then the 6 partials.
+  auto workers = [&](auto get, size_t cnt, bool sq) {
+    const size_t chunk = (cnt / 6 / 4) * 4;
+    R part[6];
+    for (size_t w = 0; w < 6; ++w) {
+      const size_t s = chunk * w, e = w == 5 ? cnt : s + chunk;
+      part[w] = seqSum(get, s, e, sq);
+    }
+    return seqSum([&](size_t w) { return part[w]; }, 0, 6, false);
+  };
+  std::vector<R> vals(A.P);
+  forTiles(A.P, [&](size_t t) {
+    const size_t nt = A.tileStart[t + 1] - A.tileStart[t], hb = A.haloStart[t];
+    auto get = [&](size_t i) { return static_cast<R>(value(hb + i)); };
+    vals[t] = total > 6 ? workers(get, nt, square) : seqSum(get, 0, nt, square);
+  });
+  std::vector<size_t> at(A.P);  // tile holding each value
+  for (size_t t = 0; t < A.P; ++t) at[t] = t;
+  const size_t groups[4] = {1472 / 4, 1472 / 2, 1472, static_cast<size_t>(-1)};
+  for (size_t G : groups) {
+    if (vals.size() <= 1) break;
+    std::vector<size_t> key, start;
+    for (size_t k = 0; k < vals.size(); ++k) {
+      const size_t g = G == static_cast<size_t>(-1) ? 0 : at[k] / G * G;
+      if (key.empty() || key.back() != g) {
+        key.push_back(g);
+        start.push_back(k);
+      }
+    }
+    start.push_back(vals.size());
+    bool perWorker = false;
+    for (size_t q = 0; q + 1 < start.size(); ++q) perWorker = perWorker || start[q + 1] - start[q] > 6;
+    std::vector<R> next(key.size());
+    for (size_t q = 0; q < key.size(); ++q) {
+      auto get = [&](size_t i) { return vals[start[q] + i]; };
+      const size_t cnt = start[q + 1] - start[q];
+      next[q] = perWorker ? workers(get, cnt, false) : seqSum(get, 0, cnt, false);
+    }
+    vals.swap(next);
+    at.swap(key);
+  }
+  return vals.empty() ? R(0) : vals[0];
+}
+
+// Tensor::norm (dsl/tensor/Tensor.cpp:425-439) of the non-halo cells in the
+// reference's reduction order and the vector's type.
+template <class T>
+T refNorm(const or_matrix& A, const std::vector<T>& v, int norm) {
+  if (norm == 2) {
+    T m = -std::numeric_limits<T>::infinity();
+    for (size_t t = 0; t < A.P; ++t)
+      for (size_t i = 0; i < A.tileStart[t + 1] - A.tileStart[t]; ++i) m = std::max(m, v[A.haloStart[t] + i]);
+    return m;
+  }
+  const T s = refReduce<T>(A, [&](size_t i) { return v[i]; }, norm == 1);
+  return norm == 1 ? std::sqrt(s) : s;
+}
+
+template <class T>
+T refDot(const or_matrix& A, const std::vector<T>& a, const std::vector<T>& b) {
+  return refReduce<T>(A, [&](size_t i) { return static_cast<T>(a[i] * b[i]); }, false);
+}
+
 // ---- ILU(0) / DILU (ilu/Solver.cpp) -----------------------------------------
 template <class V>
 struct IluFactors {
@@ -886,6 +985,7 @@ struct PbicgstabNode : SolverNode<V, T> {
     if (conf.pre) pre = makeNode<V, T>(ctx, *conf.pre);
   }
   Stats solve(std::vector<T>& x, const std::vector<T>& b) override {
+    if (c.reduceRef) return solveRef(x, b);
     const or_matrix& A = C.A;
     const size_t N = A.nWithHalo;
     Stats s;
@@ -942,6 +1042,77 @@ struct PbicgstabNode : SolverNode<V, T> {
       });
       s.fin = normT(A, r, c.norm);
       s.check(c);
+      rhoOld = rho;
+      s.iterations++;
+      if (C.history && C.root == this) C.history->push_back(s.fin);
+    }
+    return s;
+  }
+
+  // The same iteration with every scalar in the vector type T: dot products
+  // and norms in the reference's reduction order (refReduce), alpha, beta,
+  // omega in T, the residual norms stored as float and compared in float
+  // (SolverStats.hpp:33-36, SolverStats.cpp:33-63).
+  Stats solveRef(std::vector<T>& x, const std::vector<T>& b) {
+    const or_matrix& A = C.A;
+    const size_t N = A.nWithHalo;
+    Stats s;
+    std::vector<T> r(N), r0, p, v(N), y(N), z(N), sv(N), tv(N);
+    residualT<V, T, T, T, T>(A, C.tv, x, b, r);
+    float bNorm = 0;
+    if (c.relTolerance > 0) bNorm = static_cast<float>(refNorm(A, b, c.norm));
+    const float init = static_cast<float>(refNorm(A, r, c.norm));
+    float fin = init;
+    s.init = s.fin = init;
+    s.bNorm = bNorm;
+    r0 = r;
+    p = r;
+    T rhoOld = 0, alpha = 0, omega = 0;
+    const float vsmall = 1e-37f;
+    auto rows = [&](auto&& f) {
+      forTiles(A.P, [&](size_t t) {
+        for (size_t i = A.haloStart[t]; i < A.haloStart[t] + A.tileStart[t + 1] - A.tileStart[t]; ++i) f(i);
+      });
+    };
+    while (!((s.converged && s.iterations >= c.minIterations) || s.iterations >= c.maxIterations ||
+             s.singular)) {
+      const T rho = refDot(A, r0, r);
+      s.singular = s.singular || std::fabs(rho) < static_cast<T>(vsmall);
+      if (s.singular) break;
+      if (s.iterations != 0) {
+        const T beta = (rho / rhoOld) * (alpha / omega);
+        rows([&](size_t i) { p[i] = r[i] + beta * (p[i] - omega * v[i]); });
+      }
+      if (pre) {
+        if (pre->usesInitialGuess()) std::fill(y.begin(), y.end(), T(0));
+        pre->solve(y, p);
+      } else {
+        y = p;
+      }
+      spmvT<V, T>(A, C.tv, y, v);
+      alpha = rho / refDot(A, r0, v);
+      rows([&](size_t i) { sv[i] = r[i] - alpha * v[i]; });
+      if (pre) {
+        if (pre->usesInitialGuess()) std::fill(z.begin(), z.end(), T(0));
+        pre->solve(z, sv);
+      } else {
+        z = sv;
+      }
+      spmvT<V, T>(A, C.tv, z, tv);
+      const T tt = refDot(A, tv, tv);
+      omega = refDot(A, tv, sv) / tt;
+      s.singular = s.singular || std::fabs(omega) < static_cast<T>(vsmall);
+      if (s.singular) break;
+      rows([&](size_t i) {
+        x[i] = x[i] + alpha * y[i] + omega * z[i];
+        r[i] = sv[i] - omega * tv[i];
+      });
+      fin = static_cast<float>(refNorm(A, r, c.norm));
+      s.fin = fin;
+      if (c.relTolerance > 0)
+        s.converged = fin < c.absTolerance || fin < init * c.relResidual || fin < bNorm * c.relTolerance;
+      else
+        s.converged = fin < c.absTolerance || fin < init * c.relResidual;
       rhoOld = rho;
       s.iterations++;
       if (C.history && C.root == this) C.history->push_back(s.fin);
@@ -1369,6 +1540,17 @@ double or_reduce_sum(const float* x, int64_t n, int f32) {
     tot += acc;
   }
   return tot;
+}
+
+double or_ref_dot(const or_matrix* A, const void* a, const void* b, int t) {
+  if (t == 0)
+    return refDot(*A, withHalo(*A, static_cast<const float*>(a)), withHalo(*A, static_cast<const float*>(b)));
+  return refDot(*A, withHalo(*A, static_cast<const double*>(a)), withHalo(*A, static_cast<const double*>(b)));
+}
+
+double or_ref_norm(const or_matrix* A, const void* x, int t, int norm) {
+  if (t == 0) return refNorm(*A, withHalo(*A, static_cast<const float*>(x)), norm);
+  return refNorm(*A, withHalo(*A, static_cast<const double*>(x)), norm);
 }
 
 int or_ilu_factorize(const or_matrix* A, int dilu, double* off_out, double* inv_out) {

@@ -77,6 +77,11 @@ double or_norm(const or_matrix* A, const void* x, int t, int norm);
  * f32 != 0, in the reference's per-worker chunk order of
  * Expression.cpp:472-481 for one tile). */
 double or_reduce_sum(const float* x, int64_t n, int f32);
+/* Dot product a . b and norm (0 L1, 1 L2, 2 LINF) of tile-ordered vectors
+ * of type t (0 f32, 1 f64) in the reference's reduction order and operand
+ * type (Expression.cpp:472-481, :597-769; see refReduce). */
+double or_ref_dot(const or_matrix* A, const void* a, const void* b, int t);
+double or_ref_norm(const or_matrix* A, const void* x, int t, int norm);
 
 /* ILU(0) / DILU factorisation (ilu/Solver.cpp:134-292): writes the factored
  * off-diagonal values (tile-local CRS order, m entries) and the inverted

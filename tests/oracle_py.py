@@ -56,6 +56,8 @@ class Oracle:
             "or_residual": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, vp, C.c_int, C.c_int]),
             "or_norm": (C.c_double, [vp, vp, C.c_int, C.c_int]),
             "or_reduce_sum": (C.c_double, [vp, i64, C.c_int]),
+            "or_ref_dot": (C.c_double, [vp, vp, vp, C.c_int]),
+            "or_ref_norm": (C.c_double, [vp, vp, C.c_int, C.c_int]),
             "or_ilu_factorize": (C.c_int, [vp, C.c_int, vp, vp]),
             "or_ilu_solve": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, C.c_int]),
             "or_gs_sweep": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),
@@ -228,6 +230,15 @@ class OMatrix:
     def norm(self, x, norm):
         t = 0 if x.dtype == np.float32 else 1
         return self.o.L.or_norm(self.h, _p(np.ascontiguousarray(x)), t, norm)
+
+    def ref_dot(self, a, b):
+        """a . b in the reference's reduction order and operand type."""
+        t = 0 if a.dtype == np.float32 else 1
+        return self.o.L.or_ref_dot(self.h, _p(np.ascontiguousarray(a)), _p(np.ascontiguousarray(b)), t)
+
+    def ref_norm(self, x, norm=1):
+        t = 0 if x.dtype == np.float32 else 1
+        return self.o.L.or_ref_norm(self.h, _p(np.ascontiguousarray(x)), t, norm)
 
     def ilu_factorize(self, dilu=False):
         off = np.empty(self.m, np.float64)

@@ -278,3 +278,78 @@ def test_oracle_solvers_match_scipy(oracle, cfg, tol):
     sol = np.empty(n)
     sol[l2g] = got
     assert np.max(np.abs(sol - exact)) <= tol * max(1.0, np.max(np.abs(exact)))
+
+
+# ---- the reference's FP32 reduction order (Expression::reduce) ------------------------
+
+def _ref_reduce_py(tiles, square=False):
+    """Expression::reduce restated stage by stage in numpy float32 scalars
+    (dsl/tensor/Expression.cpp:472-481, :597-769; common/Shape.hpp:336-351):
+    per-tile 6-worker chunks of floor(n/6/4)*4 (rest on worker 5), the 6
+    partials, then runs of 368, 736, 1472 and all tiles."""
+    f = np.float32
+
+    def seq(vals, sq):
+        acc = f(0)
+        for v in vals:
+            acc = f(acc + f(v * v)) if sq else f(acc + v)
+        return acc
+
+    def workers(vals, sq):
+        cnt = len(vals)
+        chunk = (cnt // 6 // 4) * 4
+        parts = [seq(vals[chunk * w:(cnt if w == 5 else chunk * w + chunk)], sq) for w in range(6)]
+        return seq(parts, False)
+
+    total = sum(len(t) for t in tiles)
+    vals = [workers(list(t), square) if total > 6 else seq(list(t), square) for t in tiles]
+    at = list(range(len(tiles)))
+    for G in (368, 736, 1472, None):
+        if len(vals) <= 1:
+            break
+        keys, groups = [], []
+        for k, v in enumerate(vals):
+            g = 0 if G is None else at[k] // G * G
+            if not keys or keys[-1] != g:
+                keys.append(g)
+                groups.append([])
+            groups[-1].append(v)
+        per_worker = any(len(g) > 6 for g in groups)
+        vals = [workers(g, False) if per_worker else seq(g, False) for g in groups]
+        at = keys
+    return vals[0]
+
+
+@pytest.mark.parametrize("dims,tiles", [((5, 1, 1), 1), ((6, 5, 4), 1), ((9, 8, 7), 5), ((20, 20, 20), 64),
+                                        ((30, 30, 24), 400), ((40, 40, 30), 800), ((48, 40, 40), 1600)])
+def test_reference_order_reduction(oracle, dims, tiles):
+    """The oracle's reduction in the reference's order equals the stage-by-
+    stage restatement bit for bit, for tile counts that exercise the 368 /
+    736 / 1472 tile runs, for dot products, squared sums and signed sums."""
+    from tests.oracle_py import Oracle
+    import graphene_b200 as gb
+    h = gb.generate3DPoissonMatrix(gb.FLOAT32, *dims, tiles, gb.PART_RCB)
+    om = oracle.poisson(*dims, tiles, h.rowToTile())
+    starts = np.concatenate([[0], np.cumsum(om.tile_sizes().reshape(-1, 3)[:, :2].sum(1))])
+    rng = np.random.default_rng(tiles)
+    a = rng.uniform(-1, 1, om.n).astype(F32)
+    b = rng.uniform(-1, 1, om.n).astype(F32)
+    split = lambda v: [v[starts[t]:starts[t + 1]] for t in range(om.P)]  # noqa: E731
+    want_dot = _ref_reduce_py(split((a * b).astype(F32)))
+    assert om.ref_dot(a, b) == float(want_dot)
+    want_sq = _ref_reduce_py(split(a), square=True)
+    assert om.ref_norm(a, 1) == float(np.sqrt(want_sq))
+    assert om.ref_norm(a, 0) == float(_ref_reduce_py(split(a)))
+    assert om.ref_norm(a, 2) == float(a.max())
+    # FP32 accumulation differs from the FP64 reduction by rounding only.
+    assert abs(om.ref_dot(a, b) - float(np.dot(a.astype(np.float64), b.astype(np.float64)))) < 1e-3 * om.n ** 0.5
+
+
+def test_reference_order_reduction_golden(oracle):
+    """TensorTests.cpp:136-160 through the staged reduction: 0..15 in an 8x2
+    tensor over 4 tiles, column sums 56 and 64 (exact in any order; the
+    per-tile chunks are (2) on worker 5)."""
+    data = np.arange(16, dtype=F32).reshape(8, 2)
+    om = oracle.poisson(8, 1, 1, 4, np.repeat(np.arange(4, dtype=np.int32), 2))
+    assert om.ref_norm(np.ascontiguousarray(data[:, 0]), 0) == 56.0
+    assert om.ref_norm(np.ascontiguousarray(data[:, 1]), 0) == 64.0

@@ -126,17 +126,55 @@ def test_ilu_ring_small_rings_bit_exact(oracle, name, frac):
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("sweeps", [1, 2, 3])
 @pytest.mark.parametrize("seed", ["b", "diag"])
-def test_gauss_seidel_bit_exact(oracle, name, sweeps, seed):
+@pytest.mark.parametrize("kernel", ["ring", "levels"])
+def test_gauss_seidel_bit_exact(oracle, name, sweeps, seed, kernel):
     h, om = case(name, oracle)
     A = h.copyToTile()
     rng = np.random.default_rng(5)
     b = rng.uniform(-1, 1, h.numRows).astype(np.float32)
     x0 = rng.uniform(-1, 1, h.numRows).astype(np.float32)
     x = dev(x0)
-    gb.Solver(A, {"type": "GaussSeidel", "numFixedIterations": sweeps, "seed": seed}).solve(x, dev(b))
+    gb.Solver(A, {"type": "GaussSeidel", "numFixedIterations": sweeps, "seed": seed, "kernel": kernel}).solve(
+        x, dev(b))
     ref = x0
     for _ in range(sweeps):
         ref = om.gs_sweep(ref, b, seed_b=(seed == "b"))
+    np.testing.assert_array_equal(host(x), ref)
+
+
+@pytest.mark.parametrize("name", ["poisson16", "random", "many_tiles"])
+@pytest.mark.parametrize("vt", ["f32", "f64", "f32_matrix_f64_vectors"])
+def test_gauss_seidel_ring_types_bit_exact(oracle, name, vt):
+    """The level-ring sweep with float64 vectors (float32 or float64
+    coefficients): same bits as the oracle."""
+    mt = gb.FLOAT64 if vt == "f64" else gb.FLOAT32
+    h, om = case(name, oracle, mt)
+    A = h.copyToTile()
+    rng = np.random.default_rng(9)
+    dt = np.float32 if vt == "f32" else np.float64
+    b = rng.uniform(-1, 1, h.numRows).astype(dt)
+    x0 = rng.uniform(-1, 1, h.numRows).astype(dt)
+    x = dev(x0)
+    gb.Solver(A, {"type": "GaussSeidel", "numFixedIterations": 2, "kernel": "ring"}).solve(x, dev(b))
+    ref = om.gs_sweep(om.gs_sweep(x0, b), b)
+    np.testing.assert_array_equal(host(x), ref)
+
+
+@pytest.mark.parametrize("name", ["poisson16", "random", "many_tiles", "poisson_odd_bfs"])
+@pytest.mark.parametrize("sweeps", [1, 2, 3])
+def test_gauss_seidel_ring_from_zero_bit_exact(oracle, name, sweeps):
+    """Sweeps from x = 0 (the first one through the lower-only ring), as a
+    PBiCGStab preconditioner applies them: same bits as the oracle's full
+    sweeps from zero."""
+    h, om = case(name, oracle)
+    A = h.copyToTile()
+    b = np.random.default_rng(10).uniform(-1, 1, h.numRows).astype(np.float32)
+    cfg = {"type": "GaussSeidel", "numFixedIterations": sweeps, "kernel": "ring"}
+    x = dev(np.zeros_like(b))
+    gb.Solver(A, cfg).solve(x, dev(b))
+    ref = np.zeros_like(b)
+    for _ in range(sweeps):
+        ref = om.gs_sweep(ref, b)
     np.testing.assert_array_equal(host(x), ref)
 
 
@@ -161,6 +199,8 @@ PCFG = {
     "ilu_ring": {"type": "ILU", "kernel": "ring"},
     "dilu": {"type": "ILU", "diagonalBased": True},
     "gs2": {"type": "GaussSeidel", "numFixedIterations": 2},
+    "gs2_levels": {"type": "GaussSeidel", "numFixedIterations": 2, "kernel": "levels"},
+    "gs3_diag": {"type": "GaussSeidel", "numFixedIterations": 3, "seed": "diag"},
     "none": None,
 }
 
@@ -341,3 +381,46 @@ def test_time_repeated_runs_the_same_application(oracle):
     np.testing.assert_array_equal(host(x), om.ilu_solve(off, inv, b, False))
     with pytest.raises(gb.GrapheneError):
         gb.Solver(A, pbicgstab("ilu", 5)).timeRepeated(x, dev(b), 2)
+
+
+@pytest.mark.parametrize("name", ["poisson16", "poisson_odd_bfs", "random", "many_tiles", "poisson_1tile"])
+@pytest.mark.parametrize("pre", ["ilu", "gs2", "dilu", "none"])
+def test_pbicgstab_reference_order_bit_exact(oracle, name, pre):
+    """"reduce": "f32_ref_order": dot products and norms in the reference's
+    float reduction order (Expression.cpp:472-481, :597-769), alpha, beta,
+    omega and the convergence test in float. Every other step is already
+    bit-exact, so whole solves agree with the oracle bit for bit: same
+    iteration count, same solution, same residual norms."""
+    h, om = case(name, oracle)
+    A = h.copyToTile()
+    xt = np.random.default_rng(11).uniform(-1, 1, h.numRows).astype(np.float32)
+    b = om.spmv(xt)
+    cfg = pbicgstab(pre, 1000, 1e-6, reduce="f32_ref_order")
+    x = dev(np.zeros_like(b))
+    st = gb.Solver(A, cfg).solve(x, dev(b))
+    xo, ost, _, _ = om.solve(json.dumps(cfg), np.zeros_like(b), b)
+    assert st.converged and ost.converged
+    assert st.iterations == ost.iterations
+    np.testing.assert_array_equal(host(x), xo)
+    assert st.finalResidual == ost.final_residual and st.initialResidual == ost.initial_residual
+
+
+@pytest.mark.parametrize("norm", ["L1", "LINF"])
+def test_pbicgstab_reference_order_other_norms(oracle, norm):
+    h, om = case("many_tiles", oracle)
+    A = h.copyToTile()
+    b = om.spmv(np.random.default_rng(12).uniform(-1, 1, h.numRows).astype(np.float32))
+    cfg = pbicgstab("ilu", 1000, 1e-5, reduce="f32_ref_order", norm=norm, relTolerance=1e-6)
+    x = dev(np.zeros_like(b))
+    st = gb.Solver(A, cfg).solve(x, dev(b))
+    xo, ost, _, _ = om.solve(json.dumps(cfg), np.zeros_like(b), b)
+    assert st.iterations == ost.iterations
+    np.testing.assert_array_equal(host(x), xo)
+
+
+def test_reference_order_rejects_float64_vectors(oracle):
+    h, _ = case("poisson16", oracle, gb.FLOAT64)
+    A = h.copyToTile()
+    b = dev(np.ones(h.numRows))
+    with pytest.raises(gb.GrapheneError):
+        gb.Solver(A, pbicgstab("ilu", 10, 1e-6, reduce="f32_ref_order")).solve(dev(np.zeros(h.numRows)), b)

@@ -118,3 +118,60 @@ def test_ring_replay_192_workload():
     for group in (1, 2, 4):
         used, nbytes, lv = check_ring(h, False, gb.FLOAT32, 0, group)
         assert used >= 16384 and lv < 128
+
+
+# ---- Gauss-Seidel level ring -------------------------------------------------------------
+
+def check_gs_ring(h, lower_only, vt=gb.FLOAT32, ring_bytes=0, compact=True):
+    used, nbytes, lv = C.c_int64(), C.c_int64(), C.c_int32()
+    gb._lib.check(gb._lib.lib().gr_host_matrix_check_gs_ring(h._h, int(lower_only), vt, ring_bytes, int(compact),
+                                                              C.byref(used), C.byref(nbytes), C.byref(lv)))
+    return used.value, nbytes.value, lv.value
+
+
+@pytest.mark.parametrize("dims,tiles,part", [
+    ((16, 16, 16), 8, gb.PART_RCB),
+    ((13, 11, 7), 6, gb.PART_BFS),
+    ((12, 10, 8), 1, gb.PART_AUTO),
+    ((20, 20, 20), 200, gb.PART_RCB),
+    ((5, 4, 3), 60, gb.PART_RCB),
+    ((33, 17, 9), 5, gb.PART_CONTIGUOUS),
+])
+@pytest.mark.parametrize("lower_only", [False, True])
+@pytest.mark.parametrize("vt", [gb.FLOAT32, gb.FLOAT64])
+@pytest.mark.parametrize("compact", [True, False])
+def test_gs_ring_replay(dims, tiles, part, lower_only, vt, compact):
+    h = gb.generate3DPoissonMatrix(vt, *dims, tiles, part)
+    used, nbytes, lv = check_gs_ring(h, lower_only, vt, 0, compact)
+    assert used > 0 and used % 16 == 0 and nbytes % 16 == 0 and lv >= 1
+    # One sweep: the tile's lower levels only.
+    _, _, lv_ilu = check_ring(h, False, vt)
+    assert lv <= lv_ilu
+
+
+def test_gs_ring_lower_only_is_smaller():
+    """A sweep from x = 0 reads only the entries of earlier rows: about half
+    the level bytes of a full sweep on a 7-point matrix."""
+    h = gb.generate3DPoissonMatrix(gb.FLOAT32, 24, 24, 24, 8, gb.PART_RCB)
+    _, full, _ = check_gs_ring(h, False)
+    _, lower, _ = check_gs_ring(h, True)
+    assert lower < 0.7 * full
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_gs_ring_replay_random_and_ldu(seed):
+    n, r, c, v = random_coo(400, 0.03, seed)
+    h = gb.HostMatrix.from_coo(n, r, c, v, 7, partitioner=gb.PART_BFS)
+    check_gs_ring(h, False)
+    check_gs_ring(h, True)
+    h1 = gb.HostMatrix.from_coo(*random_coo(300, 0.04, seed, symmetric=False), 1)
+    check_gs_ring(h1, False)
+    check_gs_ring(gb.generateLduMesh(9, 8, 7, numTiles=5, partitioner=gb.PART_RCB), seed == 2)
+
+
+def test_gs_ring_replay_convdiff_workload():
+    """The 128^3 convection-diffusion system at its 1024 tiles."""
+    h = gb.generateMatrix(gb.GEN_CONVDIFF, 128, 128, 128, (0.5, 0.25, 0.125), 0, 1024)
+    for lower_only in (False, True):
+        used, nbytes, lv = check_gs_ring(h, lower_only)
+        assert used >= 4096 and lv < 64
