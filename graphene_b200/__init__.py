@@ -35,7 +35,7 @@ __all__ = [
     "PART_AUTO", "PART_CONTIGUOUS", "PART_RCB", "PART_BFS", "PART_EXPLICIT",
     "GrapheneError", "HostMatrix", "Matrix", "Configuration", "Solver", "SolverStats",
     "generate3DPoissonMatrix", "loadMatrixFromFile", "parseType", "launch_count",
-    "generateMatrix", "generateLduMesh", "randomVector", "Server", "Batch",
+    "generateMatrix", "generateMatrixLike", "generateLduMesh", "randomVector", "Server", "Batch",
 ]
 
 _NP = {FLOAT32: np.float32, FLOAT64: np.float64}
@@ -291,6 +291,26 @@ def generateMatrix(kind: int, nx: int, ny: int, nz: int, params=(), seed: int = 
     return HostMatrix(h)
 
 
+def generateMatrixLike(like: HostMatrix, kind: int, nx: int, ny: int, nz: int, params=(),
+                       seed: int = 0) -> HostMatrix:
+    """generateMatrix with `like`'s structure (gr_host_matrix_generate_like):
+    fresh values from (kind, params, seed), partition / layout / levels copied
+    from `like`, which must come from the same generator and grid."""
+    p = (C.c_double * 3)(*(list(params) + [0.0] * (3 - len(params))))
+    h = C.c_void_p()
+    check(_lib.lib().gr_host_matrix_generate_like(like._h, kind, nx, ny, nz, p, seed, C.byref(h)))
+    return HostMatrix(h)
+
+
+def _structure_key(self: HostMatrix) -> int:
+    k = C.c_uint64()
+    check(_lib.lib().gr_host_matrix_structure_key(self._h, C.byref(k)))
+    return k.value
+
+
+HostMatrix.structureKey = property(_structure_key)
+
+
 def randomVector(seed: int, n: int, dist: str = "uniform", lo: float = -1.0,
                  hi: float = 1.0) -> np.ndarray:
     """Seeded vector from the generators' counter-based stream (float64)."""
@@ -410,6 +430,10 @@ class Solver:
                                                  C.byref(ms)))
         return ms.value
 
+    def refresh(self) -> None:
+        """Recomputes the factors after Matrix.updateValues (gr_solver_refresh)."""
+        check(_lib.lib().gr_solver_refresh(self._s))
+
     def phi(self, t: int = FLOAT64):
         """Extended-precision solution of the last IterativeRefinement solve."""
         torch = _torch()
@@ -490,6 +514,12 @@ class Matrix:
         ms = C.c_float()
         check(_lib.lib().gr_matrix_tune_spmv(self._m, t, reps, *[C.byref(a) for a in v], C.byref(ms)))
         return {"block": v[0].value, "chunks_per_warp": v[1].value, "batch": v[2].value, "ms": ms.value}
+
+    def updateValues(self, h: HostMatrix) -> None:
+        """Takes h's coefficients (h has this matrix's structure); solvers on
+        this matrix then need Solver.refresh() (gr_matrix_update_values)."""
+        check(_lib.lib().gr_matrix_update_values(self._m, h._h))
+        self.host = h
 
     def vectorNorm(self, norm: int, x) -> float:
         out = C.c_double()

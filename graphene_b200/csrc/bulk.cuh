@@ -1,6 +1,6 @@
 // Bulk asynchronous copies into shared memory with mbarrier completion
-// (cp.async.bulk, no multicast: a block copies only from this GPU's global
-// memory into its own shared memory), and the fused PBiCGStab prologue
+// (cp.async.bulk, single-CTA copies: a block copies only from this GPU's
+// global memory into its own shared memory), and the fused PBiCGStab prologue
 // shared by the streamed ILU substitution kernels.
 #pragma once
 

@@ -134,6 +134,41 @@ int gr_host_matrix_generate(gr_generator kind, int64_t nx, int64_t ny, int64_t n
   });
 }
 
+int gr_host_matrix_generate_like(const gr_host_matrix* like, gr_generator kind, int64_t nx, int64_t ny,
+                                 int64_t nz, const double* params, uint64_t seed, gr_host_matrix** out) {
+  return guarded([&] {
+    need(like, "like");
+    need(out, "out");
+    gr::GeneratedCsr g;
+    switch (kind) {
+      case GR_GEN_POISSON:
+        g = gr::generatePoisson(nx, ny, nz);
+        break;
+      case GR_GEN_VAR_POISSON:
+        need(params, "params");
+        g = gr::generateVarPoisson(nx, ny, nz, params[0], seed);
+        break;
+      case GR_GEN_CONVDIFF:
+        need(params, "params");
+        if (params[0] < 0 || params[1] < 0 || params[2] < 0) gr::fail(GR_EINVAL, "velocity must be >= 0");
+        g = gr::generateConvDiff(nx, ny, nz, params[0], params[1], params[2]);
+        break;
+      default:
+        gr::fail(GR_EINVAL, "unknown generator");
+    }
+    if (g.n != like->m->n) gr::fail(GR_EINVAL, "the template matrix has another grid");
+    *out = new gr_host_matrix{gr::HostMatrix::withValues(*like->m, g.rowPtr, g.col, g.val)};
+  });
+}
+
+int gr_host_matrix_structure_key(const gr_host_matrix* h, uint64_t* key) {
+  return guarded([&] {
+    need(h, "matrix");
+    need(key, "key");
+    *key = h->m->structureKey;
+  });
+}
+
 int gr_host_matrix_from_ldu(int64_t num_cells, int64_t num_faces, const int64_t* owner, const int64_t* neighbour,
                             const double* diag, const double* lower, const double* upper, int64_t num_tiles,
                             gr_partitioner partitioner, const int32_t* row_to_tile, const double* coords,
@@ -543,6 +578,21 @@ int gr_solver_time_repeated(gr_solver* s, void* x, gr_dtype x_t, const void* b, 
     need(b, "b");
     need(ms_per_run, "ms_per_run");
     *ms_per_run = s->s->timeRepeated(x, gr::toDType(x_t), b, gr::toDType(b_t), reps);
+  });
+}
+
+int gr_matrix_update_values(gr_matrix* A, gr_host_matrix* h) {
+  return guarded([&] {
+    need(A, "matrix");
+    need(h, "host matrix");
+    A->d->updateValues(h->m);
+  });
+}
+
+int gr_solver_refresh(gr_solver* s) {
+  return guarded([&] {
+    need(s, "solver");
+    s->s->refresh();
   });
 }
 

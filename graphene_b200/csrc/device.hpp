@@ -364,6 +364,13 @@ struct DeviceMatrix {
   ~DeviceMatrix();
 
   void ensureLocalCrs();
+  // Replaces the coefficients by those of h, a matrix with this matrix's
+  // structure (equal HostMatrix::structureKey, CRS): the new tile-local
+  // values and diagonal are uploaded in place and scattered into the SpMV
+  // layout on the device; every layout array, schedule and level-ring
+  // template stays. Solver trees on this matrix then need refresh().
+  void updateValues(std::shared_ptr<HostMatrix> h);
+  DBuf sellSrc;  // tile-local CRS entry of every SELL slot (-1: padding), built on the first update
   LevelSchedule& schedule(SweepEntries kind);
   // Rounded-up kernel grid for a row loop of n rows.
   int spmvBlocks() const;

@@ -220,6 +220,69 @@ void HostMatrix::buildFromGlobalCrs(i64 numTiles, gr_partitioner part, const i32
   buildTileLayout();
   buildLocalCrs();
   buildLevels();
+  computeStructureKey();
+}
+
+// splitmix64-style mixing of the pattern, in parallel chunks combined in
+// order (the key does not depend on the thread count).
+void HostMatrix::computeStructureKey() {
+  auto mix = [](u64 h, u64 v) {
+    h ^= v + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+    h = (h ^ (h >> 30)) * 0xBF58476D1CE4E5B9ull;
+    return h ^ (h >> 27);
+  };
+  const i64 chunk = i64(1) << 16;
+  const i64 nc = (std::max(n, m) + chunk - 1) / chunk;
+  std::vector<u64> part(static_cast<size_t>(nc) + 1, 0);
+  parallelFor(nc, [&](i64 c) {
+    u64 h = static_cast<u64>(c);
+    for (i64 i = c * chunk; i < std::min(m, (c + 1) * chunk); ++i) h = mix(h, static_cast<u64>(gCol[i]));
+    for (i64 i = c * chunk; i < std::min(n, (c + 1) * chunk); ++i)
+      h = mix(mix(h, static_cast<u64>(gRowPtr[i + 1])), static_cast<u64>(rowToTile[i]));
+    part[c] = h;
+  });
+  u64 h = mix(mix(mix(static_cast<u64>(n), static_cast<u64>(m)), static_cast<u64>(P)),
+              static_cast<u64>(valueType) * 16 + static_cast<u64>(format));
+  for (i64 c = 0; c < nc; ++c) h = mix(h, part[c]);
+  structureKey = h == 0 ? 1 : h;
+}
+
+std::shared_ptr<HostMatrix> HostMatrix::withValues(const HostMatrix& like, const std::vector<i64>& rowPtr,
+                                                   const std::vector<i64>& col, const std::vector<double>& val) {
+  if (like.format != GR_FORMAT_CRS || !like.sumRank.empty())
+    fail(GR_EUNSUPPORTED, "values-only updates are for CRS matrices");
+  if (static_cast<i64>(rowPtr.size()) != like.n + 1 || static_cast<i64>(col.size()) != like.n + like.m ||
+      col.size() != val.size() || static_cast<i64>(like.localSrc.size()) != like.m)
+    fail(GR_EINVAL, "the new values do not have the template matrix's pattern");
+  auto A = std::make_shared<HostMatrix>(like);
+  std::atomic<bool> bad{false};
+  parallelChunks(like.n, [&](i64 b, i64 e) {
+    for (i64 r = b; r < e && !bad; ++r) {
+      i64 o = like.gRowPtr[r];
+      bool diagSeen = false;
+      for (i64 k = rowPtr[r]; k < rowPtr[r + 1]; ++k) {
+        if (col[k] == r) {
+          A->gDiag[r] = roundTo(like.valueType, val[k]);
+          diagSeen = true;
+        } else {
+          if (o >= like.gRowPtr[r + 1] || like.gCol[o] != col[k]) {
+            bad = true;
+            break;
+          }
+          A->gVal[o++] = roundTo(like.valueType, val[k]);
+        }
+      }
+      if (o != like.gRowPtr[r + 1] || !diagSeen) bad = true;
+    }
+  });
+  if (bad) fail(GR_EINVAL, "the new values do not have the template matrix's pattern");
+  parallelChunks(like.m, [&](i64 b, i64 e) {
+    for (i64 p = b; p < e; ++p) A->offDiag[p] = A->gVal[like.localSrc[p]];
+  });
+  parallelChunks(like.n, [&](i64 b, i64 e) {
+    for (i64 p = b; p < e; ++p) A->diag[p] = A->gDiag[like.iperm[p]];
+  });
+  return A;
 }
 
 // ---------------------------------------------------------------------------
@@ -342,6 +405,7 @@ void HostMatrix::buildLocalCrs() {
   colPerm.assign(m, 0);
   colLocal.assign(m, 0);
   offDiag.assign(m, 0.0);
+  localSrc.assign(m, 0);
   diag.assign(n, 0.0);
   parallelFor(P, [&](i64 T) {
     const auto& tile = tiles[T];
@@ -380,6 +444,7 @@ void HostMatrix::buildLocalCrs() {
         colLocal[o] = static_cast<i32>(lc);
         colPerm[o] = perm[gCol[k]];
         offDiag[o] = gVal[k];
+        localSrc[o] = static_cast<i32>(k);
         ++o;
       }
     }

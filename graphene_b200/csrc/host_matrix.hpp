@@ -78,6 +78,14 @@ struct HostMatrix {
   i64 numHaloTotal = 0;
   i64 maxTileRows = 0;
 
+  // Structure identity: a hash of the value type, the sparsity pattern and
+  // the tile map. Matrices with equal keys have the same partition, tile
+  // layout, tile-local CRS pattern and level sets, so a device copy of one
+  // can take the other's values without any host-side layout work.
+  u64 structureKey = 0;
+  // Global CRS entry (gVal index) of every tile-local CRS entry.
+  std::vector<i32> localSrc;
+
   // LDU format (matrix/details/ldu/LDUMatrix.cpp:42-168,
   // LDUAddressing.hpp:42-91). The faces in natural numbering, owner <
   // neighbour, sorted by owner; coefficients in face order, rounded to the
@@ -109,6 +117,13 @@ struct HostMatrix {
                                              i64 numTiles, gr_partitioner part, const i32* rowToTileIn,
                                              const double* coords, DType valueType);
 
+  // The structure of `like` (a CRS matrix) with new values: a natural-order
+  // CRS, diagonal included, rows sorted by column, whose pattern must be
+  // like's exactly (GR_EINVAL otherwise). Partition, layout and levels are
+  // copied, not rebuilt.
+  static std::shared_ptr<HostMatrix> withValues(const HostMatrix& like, const std::vector<i64>& rowPtr,
+                                                const std::vector<i64>& col, const std::vector<double>& val);
+
   gr_matrix_info info() const;
 
   template <class T>
@@ -129,6 +144,7 @@ struct HostMatrix {
   void buildTileLayout();
   void buildLocalCrs();
   void buildLevels();
+  void computeStructureKey();
 };
 
 // Row partitioners (raw part ids in [0, numParts), before empty-part removal).

@@ -355,6 +355,78 @@ void DeviceMatrix::ensureLocalCrs() {
   haveLocalCrs = true;
 }
 
+namespace dev {
+// SELL value of every slot from the tile-local CRS values (padding: 0).
+template <class MV>
+__global__ void sellScatterKernel(const int* __restrict__ src, const MV* __restrict__ off, int2* ent, MV* val,
+                                  long long slots) {
+  for (long long s = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; s < slots;
+       s += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int p = src[s];
+    const MV v = p >= 0 ? off[p] : MV(0);
+    if (ent) ent[s].y = __float_as_int(static_cast<float>(v));
+    else val[s] = v;
+  }
+}
+}  // namespace dev
+
+namespace {
+// Values converted to t and copied into an existing device buffer.
+void copyValuesInto(DBuf& dst, const std::vector<double>& v, DType t, cudaStream_t s) {
+  const size_t bytes = v.size() * dtypeSize(t);
+  if (dst.bytes() < bytes) fail(GR_EINVAL, "value buffer too small");
+  if (t == DType::F64) {
+    GR_CUDA(cudaMemcpyAsync(dst.get(), v.data(), bytes, cudaMemcpyHostToDevice, s));
+  } else {
+    std::vector<float> f(v.size());
+    parallelChunks(static_cast<i64>(v.size()), [&](i64 b, i64 e) {
+      for (i64 i = b; i < e; ++i) f[i] = static_cast<float>(v[i]);
+    });
+    GR_CUDA(cudaMemcpyAsync(dst.get(), f.data(), bytes, cudaMemcpyHostToDevice, s));
+    GR_CUDA(cudaStreamSynchronize(s));  // f is released on return
+  }
+}
+}  // namespace
+
+void DeviceMatrix::updateValues(std::shared_ptr<HostMatrix> h) {
+  const HostMatrix& H = *h;
+  if (batch || !host || H.structureKey != host->structureKey || H.n != n || H.m != m || H.P != P ||
+      H.valueType != vt || !H.sumRank.empty() || !host->sumRank.empty())
+    fail(GR_EINVAL, "updateValues needs a CRS matrix with this matrix's structure");
+  ensureLocalCrs();
+  if (!sellSrc.get()) {
+    // The constructor's slot assignment, recording entries instead of values.
+    std::vector<i32> base(sell.nChunks + 1, 0);
+    i64 acc = 0;
+    for (i64 c = 0; c < sell.nChunks; ++c) {
+      base[c] = static_cast<i32>(acc);
+      i64 mx = 0;
+      for (i64 r = c * 32; r < std::min<i64>(n, c * 32 + 32); ++r) mx = std::max(mx, H.rowPtr[r + 1] - H.rowPtr[r]);
+      acc += 32 * mx;
+    }
+    if (acc != sell.slots) fail(GR_EINVAL, "SELL layout mismatch");
+    std::vector<i32> src(sell.slots, -1);
+    parallelChunks(n, [&](i64 b, i64 e) {
+      for (i64 r = b; r < e; ++r)
+        for (i64 k = 0; k < H.rowPtr[r + 1] - H.rowPtr[r]; ++k)
+          src[base[r / 32] + 32 * k + r % 32] = static_cast<i32>(H.rowPtr[r] + k);
+    });
+    sellSrc.upload(src);
+  }
+  copyValuesInto(offDiag, H.offDiag, vt, stream);
+  copyValuesInto(diag, H.diag, vt, stream);
+  const int blocks = static_cast<int>(std::min<i64>(numSMs * 8, (sell.slots + 255) / 256 + 1));
+  if (vt == DType::F32)
+    dev::sellScatterKernel<float><<<blocks, 256, 0, stream>>>(sellSrc.as<int>(), offDiag.as<float>(),
+                                                              sell.ent.as<int2>(), nullptr, sell.slots);
+  else
+    dev::sellScatterKernel<double><<<blocks, 256, 0, stream>>>(sellSrc.as<int>(), offDiag.as<double>(), nullptr,
+                                                               sell.val.as<double>(), sell.slots);
+  checkLaunch("sell_scatter");
+  GR_CUDA(cudaStreamSynchronize(stream));
+  host = std::move(h);
+}
+
 // ---------------------------------------------------------------------------
 namespace dev {
 
@@ -605,6 +677,7 @@ void launchResidual(DeviceMatrix& A, const void* x, DType xt, const void* b, DTy
     switch (key) {
       case 0: GR_RES(float, float, float, float, float); break;
       case 1: GR_RES(float, float, float, float, double); break;
+      case 3: GR_RES(float, float, float, double, double); break;  // a float64 working type over float32 x and b
       case 7: GR_RES(float, float, double, double, double); break;
       case 9: GR_RES(float, double, float, float, double); break;
       case 11: GR_RES(float, double, float, double, double); break;

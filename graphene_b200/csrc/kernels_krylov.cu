@@ -142,13 +142,21 @@ __device__ __forceinline__ void store4(double* p, int i, const double (&o)[4]) {
   *reinterpret_cast<double2*>(p + i + 2) = make_double2(o[2], o[3]);
 }
 
+// x kept in float while the working type is double (workingType float64
+// over float32 vectors, pbicgstab/Solver.cpp:63, :164): the update is
+// evaluated in double and rounded to float.
+__device__ __forceinline__ float roundTo(float v, bool) { return v; }
+__device__ __forceinline__ double roundTo(double v, bool toFloat) {
+  return toFloat ? static_cast<double>(__double2float_rn(v)) : v;
+}
+
 template <class W, bool VEC>
 __global__ void __launch_bounds__(256) bicgUpdateKernel(W* __restrict__ x, const W* __restrict__ y,
                                                          const W* __restrict__ z, W* __restrict__ r,
                                                          const W* __restrict__ s, const W* __restrict__ t,
                                                          const W* __restrict__ r0, int n, KState* st,
                                                          double* partials, unsigned* counter, SegView seg,
-                                                         bool stateless) {
+                                                         bool stateless, bool roundX) {
   __shared__ double smem[64];
   const SegPos sp = segPos(seg, n);
   st += sp.sys;
@@ -161,7 +169,7 @@ __global__ void __launch_bounds__(256) bicgUpdateKernel(W* __restrict__ x, const
   // arithmetic, so that a warp keeps four times the bytes in flight; each
   // thread adds its elements to the reductions in index order.
   auto one = [&](int i) {
-    x[i] = add(add(x[i], mul(al, y[i])), mul(om, z[i]));
+    x[i] = roundTo(add(add(x[i], mul(al, y[i])), mul(om, z[i])), roundX);
     const W rv = sub(s[i], mul(om, t[i]));
     r[i] = rv;
     v[0] = normStep(v[0], toDouble(rv), nk);
@@ -181,7 +189,7 @@ __global__ void __launch_bounds__(256) bicgUpdateKernel(W* __restrict__ x, const
       W xo[4], ro[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        xo[j] = add(add(xa[j], mul(al, ya[j])), mul(om, za[j]));
+        xo[j] = roundTo(add(add(xa[j], mul(al, ya[j])), mul(om, za[j])), roundX);
         ro[j] = sub(sa[j], mul(om, ta[j]));
         v[0] = normStep(v[0], toDouble(ro[j]), nk);
         v[1] = __dadd_rn(v[1], __dmul_rn(toDouble(ra[j]), toDouble(ro[j])));
@@ -550,7 +558,8 @@ void launchSpmvDot(DeviceMatrix& A, const void* x, void* y, const void* d1, int 
 }
 
 void launchBicgUpdate(DeviceMatrix& A, void* x, const void* y, const void* z, void* r, const void* sv,
-                      const void* t, const void* r0, KState* st, DType W, cudaStream_t s, bool stateless) {
+                      const void* t, const void* r0, KState* st, DType W, cudaStream_t s, bool stateless,
+                      bool roundX) {
   const Launch L = krylovLaunch(A, false);
   // 16-byte accesses need every vector 16-byte aligned (segments start at
   // multiples of 32 rows); otherwise the same order element by element.
@@ -562,12 +571,12 @@ void launchBicgUpdate(DeviceMatrix& A, void* x, const void* y, const void* z, vo
     (vec ? dev::bicgUpdateKernel<float, true> : dev::bicgUpdateKernel<float, false>)<<<L.blocks, 256, 0, s>>>(
         static_cast<float*>(x), static_cast<const float*>(y), static_cast<const float*>(z), static_cast<float*>(r),
         static_cast<const float*>(sv), static_cast<const float*>(t), static_cast<const float*>(r0), A.n, st,
-        L.partials, L.counter, L.seg, stateless);
+        L.partials, L.counter, L.seg, stateless, false);
   else
     (vec ? dev::bicgUpdateKernel<double, true> : dev::bicgUpdateKernel<double, false>)<<<L.blocks, 256, 0, s>>>(
         static_cast<double*>(x), static_cast<const double*>(y), static_cast<const double*>(z),
         static_cast<double*>(r), static_cast<const double*>(sv), static_cast<const double*>(t),
-        static_cast<const double*>(r0), A.n, st, L.partials, L.counter, L.seg, stateless);
+        static_cast<const double*>(r0), A.n, st, L.partials, L.counter, L.seg, stateless, roundX);
   checkLaunch("bicg_update");
 }
 

@@ -6,8 +6,8 @@
 // of the block is level l of each of its tiles). The level blocks (LevelRing, device.hpp)
 // are copied from global memory into a shared-memory ring with one bulk
 // asynchronous copy per level (cp.async.bulk, completion on one of
-// kRingBarriers mbarriers; no multicast: a block copies only its own tile's
-// bytes from this GPU's memory). The host fixed each level's ring offset and
+// kRingBarriers mbarriers; a single-CTA bulk copy: a block copies only its
+// own tile's bytes from this GPU's memory). The host fixed each level's ring offset and
 // the level after which its copy is issued, so the kernel does no ring
 // arithmetic: a level's rows, inverse diagonal and (column, value) entries
 // sit at fixed offsets. Producer and consumers form a pipeline over
@@ -312,12 +312,18 @@ __global__ void __launch_bounds__(RingShape<W>::threads) iluRingKernel(const uns
 // The prologue fills the sweep-start values and halo cells from xin (zeros
 // when xinZero) and, with seedB, the right-hand side from the fused
 // PBiCGStab prologue (which also writes p or s).
-template <class MV, class W, bool COMPACT>
+// Vectors are stored in X; rows are computed in W, each new value rounded to
+// X as it is stored (the working type of gauss-seidel/Solver.cpp:65-84).
+template <class X, class W>
+__device__ __forceinline__ W storeRound(W v) {
+  return cvt<W>(cvt<X>(v));
+}
+template <class MV, class X, class W, bool COMPACT>
 __global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
     const unsigned char* __restrict__ stream, const long long* __restrict__ tileOffset, const int4* __restrict__ meta,
     const int* __restrict__ tileLevel, const int* __restrict__ tileStart, const int* __restrict__ haloStart,
-    const int* __restrict__ haloSrc, int ringBytes, int metaLevels, bool seedB, SPro<W> pro,
-    const W* __restrict__ xin, bool xinZero, W* __restrict__ xout, int* errFlag) {
+    const int* __restrict__ haloSrc, int ringBytes, int metaLevels, bool seedB, SPro<X> pro,
+    const X* __restrict__ xin, bool xinZero, X* __restrict__ xout, int* errFlag) {
   constexpr int kRingCompute = RingShape<W>::compute;
   constexpr int kRingLevelSync = RingShape<W>::levelSync;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -358,26 +364,27 @@ __global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
   {
     const int bd = static_cast<int>(blockDim.x);
     if (seedB || pro.kind != static_cast<int>(Prologue::Plain)) {
-      W beta = W(0), omega = W(0), alpha = W(0);
+      X beta = X(0), omega = X(0), alpha = X(0);
       bool first = true;
       if (st) {
-        beta = cvt<W>(st->beta);
-        omega = cvt<W>(st->omega);
-        alpha = cvt<W>(st->alpha);
+        beta = cvt<X>(st->beta);
+        omega = cvt<X>(st->omega);
+        alpha = cvt<X>(st->alpha);
         first = st->iter == 0;
       }
       for (int i0 = threadIdx.x; i0 < nRows; i0 += 4 * bd) {
-        W v4[4];
+        X v4[4];
         pro.four(base + i0, bd, base + nRows, beta, omega, alpha, first, v4);
         if (seedB) {
 #pragma unroll
           for (int j = 0; j < 4; ++j)
-            if (i0 + j * bd < nRows) rhs[i0 + j * bd] = v4[j];
+            if (i0 + j * bd < nRows) rhs[i0 + j * bd] = cvt<W>(v4[j]);
         }
       }
     }
-    for (int i = threadIdx.x; i < nRows; i += bd) xs[nRows + i] = xinZero ? W(0) : xin[base + i];
-    for (int h = threadIdx.x; h < nHalo; h += bd) xs[2 * nRows + h] = xinZero ? W(0) : xin[haloSrc[h0 + h]];
+    for (int i = threadIdx.x; i < nRows; i += bd) xs[nRows + i] = xinZero ? W(0) : cvt<W>(xin[base + i]);
+    for (int h = threadIdx.x; h < nHalo; h += bd)
+      xs[2 * nRows + h] = xinZero ? W(0) : cvt<W>(xin[haloSrc[h0 + h]]);
     if (lead) xs[2 * nRows + nHalo] = W(0);
   }
   __syncthreads();
@@ -453,7 +460,7 @@ __global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
             sum = sub(sum, mul(cvt<W>(v), xs[c]));
           }
         }
-        xs[il] = dvd(sum, d);
+        xs[il] = storeRound<X>(dvd(sum, d));
       }
       stop = namedBarOr(1, kRingLevelSync, *abortV != 0);
     }
@@ -468,7 +475,7 @@ __global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
     }
     return;
   }
-  for (int i = threadIdx.x; i < nRows; i += blockDim.x) xout[base + i] = xs[i];
+  for (int i = threadIdx.x; i < nRows; i += blockDim.x) xout[base + i] = cvt<X>(xs[i]);
 }
 
 }  // namespace dev
@@ -512,9 +519,9 @@ int ringBlocksPerSMWithoutSmem(DType vt, RingKind kind) {
   int n = 0;
   const bool gs = kind != RingKind::Ilu;
   const void* fn = vt == DType::F64
-                       ? (gs ? reinterpret_cast<const void*>(dev::gsRingKernel<double, double, true>)
+                       ? (gs ? reinterpret_cast<const void*>(dev::gsRingKernel<double, double, double, true>)
                              : reinterpret_cast<const void*>(dev::iluRingKernel<double, double, true, true>))
-                       : (gs ? reinterpret_cast<const void*>(dev::gsRingKernel<float, float, true>)
+                       : (gs ? reinterpret_cast<const void*>(dev::gsRingKernel<float, float, float, true>)
                              : reinterpret_cast<const void*>(dev::iluRingKernel<float, float, true, true>));
   const int threads = vt == DType::F64 ? dev::RingShape<double>::threads : dev::RingShape<float>::threads;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, 0) != cudaSuccess) {
@@ -525,35 +532,40 @@ int ringBlocksPerSMWithoutSmem(DType vt, RingKind kind) {
 }
 
 namespace {
-template <class MV, class W>
+template <class MV, class X, class W>
 void gsRingT(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& p, bool seedB,
              const void* xin, bool xinZero, void* xout, cudaStream_t s) {
   if (R.kind == RingKind::Ilu) fail(GR_EINVAL, "not a Gauss-Seidel ring");
   if (R.kind == RingKind::GaussSeidelLower && !xinZero)
     fail(GR_EINVAL, "a lower-only Gauss-Seidel ring sweeps from x = 0 only");
   const size_t smem = iluRingSmem(A, R, dtypeOf<W>());
-  auto kernel = R.compact ? dev::gsRingKernel<MV, W, true> : dev::gsRingKernel<MV, W, false>;
+  auto kernel = R.compact ? dev::gsRingKernel<MV, X, W, true> : dev::gsRingKernel<MV, X, W, false>;
   ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
   preferSharedCarveout(reinterpret_cast<const void*>(kernel));
-  dev::SPro<W> pro{static_cast<int>(p.kind), static_cast<const W*>(p.b), static_cast<const W*>(p.r),
-                   static_cast<W*>(p.pOrS), static_cast<const W*>(p.v), p.st, nullptr};
+  dev::SPro<X> pro{static_cast<int>(p.kind), static_cast<const X*>(p.b), static_cast<const X*>(p.r),
+                   static_cast<X*>(p.pOrS), static_cast<const X*>(p.v), p.st, nullptr};
   kernel<<<R.numGroups, dev::RingShape<W>::threads, smem, s>>>(
       static_cast<const unsigned char*>(stream), R.tileOffset.as<long long>(), R.meta.as<int4>(),
       R.tileLevel.as<int>(), R.groupStart.as<int>(), R.haloStart.as<int>(), R.haloSrc.as<int>(),
-      static_cast<int>(R.ringBytes), R.maxTileLevels, seedB, pro, static_cast<const W*>(xin), xinZero,
-      static_cast<W*>(xout), A.errFlag.as<int>());
+      static_cast<int>(R.ringBytes), R.maxTileLevels, seedB, pro, static_cast<const X*>(xin), xinZero,
+      static_cast<X*>(xout), A.errFlag.as<int>());
   checkLaunch("gs_ring");
 }
 }  // namespace
 
 void launchGsRing(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& pro, bool seedB,
-                  const void* xin, bool xinZero, void* xout, DType W, cudaStream_t s) {
-  if (A.vt == DType::F32 && W == DType::F32) gsRingT<float, float>(A, R, stream, pro, seedB, xin, xinZero, xout, s);
-  else if (A.vt == DType::F32 && W == DType::F64)
-    gsRingT<float, double>(A, R, stream, pro, seedB, xin, xinZero, xout, s);
-  else if (A.vt == DType::F64 && W == DType::F64)
-    gsRingT<double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, s);
-  else fail(GR_EUNSUPPORTED, "Gauss-Seidel with float64 coefficients needs float64 vectors");
+                  const void* xin, bool xinZero, void* xout, DType X, DType W, cudaStream_t s) {
+  if (A.vt == DType::F32 && X == DType::F32 && W == DType::F32)
+    gsRingT<float, float, float>(A, R, stream, pro, seedB, xin, xinZero, xout, s);
+  else if (A.vt == DType::F32 && X == DType::F32 && W == DType::F64)
+    gsRingT<float, float, double>(A, R, stream, pro, seedB, xin, xinZero, xout, s);
+  else if (A.vt == DType::F32 && X == DType::F64 && W == DType::F64)
+    gsRingT<float, double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, s);
+  else if (A.vt == DType::F64 && X == DType::F64 && W == DType::F64)
+    gsRingT<double, double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, s);
+  else
+    fail(GR_EUNSUPPORTED, "Gauss-Seidel: float64 coefficients need float64 vectors, and the working type must be "
+                          "the vectors' type or float64 over float32 vectors");
 }
 
 void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,

@@ -7,8 +7,8 @@
 // (cp.async.bulk, completion tracked by one mbarrier per ring chunk). One
 // elected thread keeps up to kRingChunks chunks in flight ahead of the level
 // being processed, so a level's work reads only shared memory and the
-// per-level cost is a barrier instead of an HBM round trip. No multicast is
-// used: every CTA copies only its own tile's bytes from this GPU's memory.
+// per-level cost is a barrier instead of an HBM round trip. Every copy is a
+// single-CTA bulk copy of the block's own tile bytes from this GPU's memory.
 //
 // Every wait on an mbarrier is bounded; a wait that runs out sets the
 // matrix's error word to GR_ETIMEOUT, all threads leave the level loop

@@ -96,9 +96,10 @@ void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool
 // then be a lower-only one). The right-hand side is the prologue's vector
 // (seedB), or each row starts from its diagonal (seedB false, the
 // reference's CodeDSL solver, gauss-seidel/Solver.cpp:74). stream: the ring
-// template with the coefficients and the diagonal packed in.
+// template with the coefficients and the diagonal packed in. Vectors of
+// type X, rows computed in W (X, or float64 over float32 vectors).
 void launchGsRing(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& pro, bool seedB,
-                  const void* xin, bool xinZero, void* xout, DType W, cudaStream_t s);
+                  const void* xin, bool xinZero, void* xout, DType X, DType W, cudaStream_t s);
 // Warp-per-tile substitution (kernels_warp.cu): shared memory per block and
 // the number of rows per lane to prefetch.
 size_t iluWarpSmem(const DeviceMatrix& A, const SweepStream& S, DType W);
@@ -125,7 +126,8 @@ void launchSpmvDot(DeviceMatrix& A, const void* x, void* y, const void* d1, int 
                    DType W, cudaStream_t s, bool stateless = false);
 // x = x + alpha y + omega z; r = s - omega t; convergence; next rho, beta.
 void launchBicgUpdate(DeviceMatrix& A, void* x, const void* y, const void* z, void* r, const void* sv,
-                      const void* t, const void* r0, KState* st, DType W, cudaStream_t s, bool stateless = false);
+                      const void* t, const void* r0, KState* st, DType W, cudaStream_t s, bool stateless = false,
+                      bool roundX = false);
 
 // ---- the reference's reduction order ("reduce": "f32_ref_order") -------
 // A reduction over the non-halo rows, per tile in the reference's order

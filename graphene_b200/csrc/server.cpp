@@ -31,6 +31,9 @@ i64 estimateFootprint(const HostMatrix& H, const std::string& json, DType t) {
 
 struct Server::Entry {
   std::shared_ptr<HostMatrix> H;
+  const HostMatrix* hid = nullptr;  // the matrix whose values are on the device (changed under mu_)
+  u64 key = 0;                      // structure key (CRS matrices)
+  bool crs = false;
   std::string json;
   i64 footprint = 0;
   bool busy = false, ready = false;
@@ -49,7 +52,7 @@ struct Server::Request {
   double tArrive = 0, tAdmit = 0, tFinish = 0;
   gr_stats st{};
   int status = GR_OK, slot = -1;
-  bool cacheHit = false, done = false;
+  bool cacheHit = false, done = false, valuesUpdated = false;
   std::string err;
   std::shared_ptr<Entry> entry;
 };
@@ -127,9 +130,14 @@ u64 Server::submit(std::shared_ptr<HostMatrix> H, const std::string& json, const
   return r->id;
 }
 
+// The resident pair of a request: the same matrix, or (CRS matrices) the
+// same structure, whose values the worker then replaces.
 std::shared_ptr<Server::Entry> Server::findEntry(const Request& r) {
-  for (auto& e : resident_)
-    if (e->H == r.H && e->json == r.json) return e;
+  const bool crs = r.H->format == GR_FORMAT_CRS && r.H->sumRank.empty();
+  for (auto& e : resident_) {
+    if (e->json != r.json) continue;
+    if (e->hid == r.H.get() || (crs && e->crs && e->key == r.H->structureKey)) return e;
+  }
   return nullptr;
 }
 
@@ -192,6 +200,9 @@ void Server::worker(int slot) {
             }
             auto e = std::make_shared<Entry>();
             e->H = r->H;
+            e->hid = r->H.get();
+            e->key = r->H->structureKey;
+            e->crs = r->H->format == GR_FORMAT_CRS && r->H->sumRank.empty();
             e->json = r->json;
             e->footprint = r->footprint;
             resident_.push_back(e);
@@ -220,6 +231,18 @@ void Server::worker(int slot) {
         e.ready = true;
       }
       e.D->stream = stream;
+      if (e.hid != r->H.get()) {
+        // Same structure, new values: upload them into the resident device
+        // matrix and refactorise in place (no host layout work, no new
+        // buffers, the captured iteration graphs stay valid).
+        e.D->updateValues(r->H);
+        e.tree->refresh();
+        e.H = r->H;
+        std::lock_guard<std::mutex> lk(mu_);
+        e.hid = r->H.get();
+        r->cacheHit = true;
+        r->valuesUpdated = true;
+      }
       r->st = e.tree->solveHost(r->x.data(), r->t, r->b.data(), r->t);
     } catch (const Error& ex) {
       r->status = ex.code;
@@ -273,7 +296,7 @@ int Server::wait(u64 id, double timeoutMs, void* x, gr_stats* stats, gr_request_
     times->admitted_ms = r->tAdmit;
     times->finished_ms = r->tFinish;
     times->footprint_bytes = r->footprint;
-    times->cache_hit = r->cacheHit ? 1 : 0;
+    times->cache_hit = r->valuesUpdated ? 2 : (r->cacheHit ? 1 : 0);
     times->slot = r->slot;
   }
   *status = r->status;

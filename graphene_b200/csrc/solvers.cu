@@ -36,6 +36,8 @@ class Node {
   virtual void copyPhi(void*, DType) { fail(GR_EUNSUPPORTED, "only IterativeRefinement keeps phi"); }
   // Allocates the scratch a solve of type W needs (before graph capture).
   virtual void prepare(DType) {}
+  // Recomputes the parts that depend on the matrix's values, in place.
+  virtual void refresh() {}
   // Per-system statistics of the last solve of a batch.
   virtual std::vector<gr_stats> batchStats() const {
     fail(GR_EUNSUPPORTED, "only PBiCGStab solves batches");
@@ -63,21 +65,7 @@ class IluNode : public Node {
  public:
   IluNode(DeviceMatrix& A, const SolverConfig& c) : Node(A, c), dilu_(c.diagonalBased) {
     A.ensureLocalCrs();
-    LevelSchedule& L = A.schedule(SweepEntries::Lower);
-    LevelSchedule& U = A.schedule(SweepEntries::UpperDesc);
     const size_t vs = dtypeSize(A.vt);
-    DBuf F, D;
-    if (!dilu_) {
-      F.alloc(std::max<i64>(1, A.m) * vs);
-      GR_CUDA(cudaMemcpyAsync(F.get(), A.offDiag.get(), A.m * vs, cudaMemcpyDeviceToDevice, s()));
-    }
-    D.alloc(A.n * vs);
-    GR_CUDA(cudaMemcpyAsync(D.get(), A.diag.get(), A.n * vs, cudaMemcpyDeviceToDevice, s()));
-    // ilu::Solver::factorize at construction (ilu/Solver.cpp:44-51).
-    launchIluFactor(A, dilu_ ? nullptr : F.get(), D.get(), A.offDiag.get(), dilu_, s());
-    inv_.alloc(A.n * vs);
-    launchInvert(A, D.get(), inv_.get(), s());
-    const void* vals = dilu_ ? A.offDiag.get() : F.get();
     // Streamed substitution when the ring and the tile slice fit in shared
     // memory for either vector type; the level-schedule kernel otherwise.
     // Substitution kernel: the bulk-copy ring kernel over the tile byte
@@ -110,22 +98,46 @@ class IluNode : public Node {
       else if (c.iluKernel == 1 && tmaFits) kernel_ = 1;
       else fail(GR_EUNSUPPORTED, "the requested ILU kernel does not fit this matrix's tiles in shared memory");
     }
+    inv_.alloc(A.n * vs);
     if (kernel_ == 4) {
       stream_.alloc(std::max<i64>(16, ring_->bytes));
-      launchRingPack(A, *ring_, stream_.get(), vals, inv_.get(), s());
     } else if (kernel_ != 2) {
       SweepStream& S = A.iluSweepStream(dilu_);
       sweep_ = &S;
       rowsPerLane_ = iluWarpRowsPerLane(A, S);
       stream_.alloc(std::max<i64>(16, S.bytes));
-      launchStreamPack(A, S, stream_.get(), vals, inv_.get(), s());
     } else {
-      Lval_.alloc(std::max<i64>(1, L.slots) * vs);
-      Uval_.alloc(std::max<i64>(1, U.slots) * vs);
-      launchPack(A, L, vals, Lval_.get(), s());
-      launchPack(A, U, vals, Uval_.get(), s());
+      Lval_.alloc(std::max<i64>(1, A.schedule(SweepEntries::Lower).slots) * vs);
+      Uval_.alloc(std::max<i64>(1, A.schedule(SweepEntries::UpperDesc).slots) * vs);
     }
-    GR_CUDA(cudaStreamSynchronize(s()));
+    factorAndPack();
+  }
+  void refresh() override { factorAndPack(); }
+  // ilu::Solver::factorize (ilu/Solver.cpp:44-51, :134-292) of the matrix's
+  // current values, and the packing of the factors into this solver's own
+  // level blocks (the buffers allocated at construction).
+  void factorAndPack() {
+    DeviceMatrix& A = A_;
+    const size_t vs = dtypeSize(A.vt);
+    DBuf F, D;
+    if (!dilu_) {
+      F.alloc(std::max<i64>(1, A.m) * vs);
+      GR_CUDA(cudaMemcpyAsync(F.get(), A.offDiag.get(), A.m * vs, cudaMemcpyDeviceToDevice, s()));
+    }
+    D.alloc(A.n * vs);
+    GR_CUDA(cudaMemcpyAsync(D.get(), A.diag.get(), A.n * vs, cudaMemcpyDeviceToDevice, s()));
+    launchIluFactor(A, dilu_ ? nullptr : F.get(), D.get(), A.offDiag.get(), dilu_, s());
+    launchInvert(A, D.get(), inv_.get(), s());
+    const void* vals = dilu_ ? A.offDiag.get() : F.get();
+    if (kernel_ == 4) {
+      launchRingPack(A, *ring_, stream_.get(), vals, inv_.get(), s());
+    } else if (kernel_ != 2) {
+      launchStreamPack(A, *sweep_, stream_.get(), vals, inv_.get(), s());
+    } else {
+      launchPack(A, A.schedule(SweepEntries::Lower), vals, Lval_.get(), s());
+      launchPack(A, A.schedule(SweepEntries::UpperDesc), vals, Uval_.get(), s());
+    }
+    GR_CUDA(cudaStreamSynchronize(s()));  // F and D are released on return
   }
   bool streamed() const { return sweep_ != nullptr; }
   bool ringKernel() const { return kernel_ == 4; }
@@ -186,13 +198,20 @@ class GsNode : public Node {
     }
     if (ring_) {
       stream_.alloc(std::max<i64>(16, ring_->bytes));
-      launchRingPack(A, *ring_, stream_.get(), A.offDiag.get(), A.diag.get(), s());
       streamLo_.alloc(std::max<i64>(16, ringLo_->bytes));
-      launchRingPack(A, *ringLo_, streamLo_.get(), A.offDiag.get(), A.diag.get(), s());
     } else {
-      LevelSchedule& G = A.schedule(SweepEntries::All);
-      Gval_.alloc(std::max<i64>(1, G.slots) * dtypeSize(A.vt));
-      launchPack(A, G, A.offDiag.get(), Gval_.get(), s());
+      Gval_.alloc(std::max<i64>(1, A.schedule(SweepEntries::All).slots) * dtypeSize(A.vt));
+    }
+    refresh();
+  }
+  // Packs the matrix's current coefficients and diagonal into this
+  // solver's level blocks.
+  void refresh() override {
+    if (ring_) {
+      launchRingPack(A_, *ring_, stream_.get(), A_.offDiag.get(), A_.diag.get(), s());
+      launchRingPack(A_, *ringLo_, streamLo_.get(), A_.offDiag.get(), A_.diag.get(), s());
+    } else {
+      launchPack(A_, A_.schedule(SweepEntries::All), A_.offDiag.get(), Gval_.get(), s());
     }
     GR_CUDA(cudaStreamSynchronize(s()));
   }
@@ -202,8 +221,6 @@ class GsNode : public Node {
   // numFixedIterations sweeps from x = 0.
   bool fusedPrologue() const { return ring_ != nullptr && cfg_.numFixedIterations > 0; }
   void applyFused(const PrologueArgs& pro, void* out, DType W) {
-    if (workingType(cfg_, W) != W)
-      fail(GR_EUNSUPPORTED, "GaussSeidel workingType different from the vector type");
     ringSweeps(pro, out, W, cfg_.numFixedIterations, true);
   }
 
@@ -240,8 +257,9 @@ class GsNode : public Node {
  private:
   gr_stats solveImpl(void* x, const void* b, DType W, const KState* gate, bool xZero) {
     gr_stats st{};
-    if (workingType(cfg_, W) != W)
-      fail(GR_EUNSUPPORTED, "GaussSeidel workingType different from the vector type");
+    // The working type (gauss-seidel/Solver.cpp:65, :114): the sweeps'
+    // arithmetic and the convergence residual; x stays in its own type.
+    const DType Wc = computeType(W);
     if (cfg_.numFixedIterations > 0) {
       // gauss-seidel/Solver.cpp:116-126
       sweeps(x, b, W, cfg_.numFixedIterations, xZero, gate);
@@ -250,7 +268,7 @@ class GsNode : public Node {
     }
     if (gate) fail(GR_EUNSUPPORTED, "a GaussSeidel preconditioner needs numFixedIterations > 0");
     ensureTmp(W);
-    DBuf r(A_.n * dtypeSize(W));
+    DBuf r(A_.n * dtypeSize(Wc));
     double* d = A_.scalarOut.as<double>();
     double h = 0;
     if (cfg_.relTolerance > 0) {
@@ -260,7 +278,7 @@ class GsNode : public Node {
       st.b_norm = h;
     }
     auto residualNorm = [&]() {
-      launchResidual(A_, x, W, b, W, r.get(), W, W, cfg_.norm, d, s());
+      launchResidual(A_, x, W, b, W, r.get(), Wc, Wc, cfg_.norm, d, s());
       double v = 0;
       GR_CUDA(cudaMemcpyAsync(&v, d, sizeof(double), cudaMemcpyDeviceToHost, s()));
       GR_CUDA(cudaStreamSynchronize(s()));
@@ -292,6 +310,16 @@ class GsNode : public Node {
     const size_t bytes = A_.n * dtypeSize(W);
     if (tmp_.bytes() < bytes) tmp_.alloc(bytes);
   }
+  // The sweeps' arithmetic type for vectors of type W: W, or float64 over
+  // float32 vectors (level-ring kernel only).
+  DType computeType(DType W) const {
+    const DType Wc = workingType(cfg_, W);
+    if (Wc == W) return W;
+    if (!(W == DType::F32 && Wc == DType::F64))
+      fail(GR_EUNSUPPORTED, "GaussSeidel workingType must be the vectors' type or float64 over float32 vectors");
+    if (!ring_) fail(GR_EUNSUPPORTED, "a GaussSeidel workingType other than the vectors' needs the ring kernel");
+    return Wc;
+  }
   // Level-ring sweeps: the first takes its right-hand side from `first`
   // (b itself, or a fused p / s update, which it also writes); later ones
   // from b or the written p / s. A sweep from x = 0 uses the lower-only ring.
@@ -307,7 +335,7 @@ class GsNode : public Node {
     for (int k = 0; k < count; ++k) {
       const bool zero = xZero && k == 0;
       launchGsRing(A_, zero ? *ringLo_ : *ring_, zero ? streamLo_.get() : stream_.get(), k == 0 ? first : plain,
-                   cfg_.gsSeedB, cur, zero, other, W, s());
+                   cfg_.gsSeedB, cur, zero, other, W, computeType(W), s());
       std::swap(cur, other);
     }
     if (cur != x) GR_CUDA(cudaMemcpyAsync(x, cur, A_.n * dtypeSize(W), cudaMemcpyDeviceToDevice, s()));
@@ -384,11 +412,21 @@ class PbicgstabNode : public Node {
   gr_stats solve(void* x, const void* b, DType Wx, const KState* gate) override {
     (void)gate;
     const DType W = workingType(cfg_, Wx);
-    if (W != Wx) fail(GR_EUNSUPPORTED, "PBiCGStab workingType different from the vector type");
+    // workingType float64 over float32 x and b (pbicgstab/Solver.cpp:63-79):
+    // every vector but x in double, x rounded to float at each update.
+    mixed_ = W != Wx;
+    if (mixed_ && !(Wx == DType::F32 && W == DType::F64))
+      fail(GR_EUNSUPPORTED, "PBiCGStab workingType must be float64 over float32 vectors, or the vectors' type");
+    if (mixed_ && A_.batch) fail(GR_EUNSUPPORTED, "batched PBiCGStab needs the working type of the vectors");
     const bool ref = cfg_.reduceRef;
     if (ref && (W != DType::F32 || A_.batch))
       fail(GR_EUNSUPPORTED, "reduce \"f32_ref_order\" needs float32 vectors and a single system");
     ensureBuffers(W);
+    if (mixed_) {
+      if (bw_.bytes() < A_.n * sizeof(double)) bw_.alloc(A_.n * sizeof(double));
+      launchConvert(b, Wx, bw_.get(), W, static_cast<int>(A_.n), s());
+    }
+    const void* bW = mixed_ ? bw_.get() : b;
     if (ref && refTiles_.bytes() < 2 * static_cast<size_t>(A_.P) * sizeof(float))
       refTiles_.alloc(2 * static_cast<size_t>(A_.P) * sizeof(float));
     const size_t vb = A_.n * dtypeSize(W);
@@ -407,15 +445,16 @@ class PbicgstabNode : public Node {
       if (ref) {
         launchRefReduce(A_, RefRed{normRed(), b, nullptr}, RefRed{}, RefStage::BNorm, st, refTiles_.get(), s());
       } else if (!A_.batch) {
-        launchNorm(A_, b, W, cfg_.norm, &st->bNorm, s());
+        launchNorm(A_, b, Wx, cfg_.norm, &st->bNorm, s());
       } else {
         for (int k = 0; k < systems_; ++k)
           launchNormN(A_, static_cast<const char*>(b) + A_.batch->rowBegin[k] * dtypeSize(W), A_.batch->rowReal[k], W,
                       cfg_.norm, &st[k].bNorm, s());
       }
     }
-    GR_CUDA(cudaMemcpyAsync(xw(), x, vb, cudaMemcpyDeviceToDevice, s()));
-    launchBicgInit(A_, xw(), b, buf(R), buf(R0), st, W, s(), ref);
+    if (mixed_) launchConvert(x, Wx, xw(), W, static_cast<int>(A_.n), s());
+    else GR_CUDA(cudaMemcpyAsync(xw(), x, vb, cudaMemcpyDeviceToDevice, s()));
+    launchBicgInit(A_, xw(), bW, buf(R), buf(R0), st, W, s(), ref);
     if (ref)
       launchRefReduce(A_, RefRed{RefKind::Dot, buf(R0), buf(R)}, RefRed{normRed(), buf(R), nullptr}, RefStage::Init,
                       st, refTiles_.get(), s());
@@ -443,7 +482,8 @@ class PbicgstabNode : public Node {
       if (all) break;
       if (issued > cfg_.maxIterations && issued > (1 << 30)) break;
     }
-    GR_CUDA(cudaMemcpyAsync(x, xw(), vb, cudaMemcpyDeviceToDevice, s()));
+    if (mixed_) launchConvert(xw(), W, x, Wx, static_cast<int>(A_.n), s());  // exact: x holds float values
+    else GR_CUDA(cudaMemcpyAsync(x, xw(), vb, cudaMemcpyDeviceToDevice, s()));
     GR_CUDA(cudaStreamSynchronize(s()));
     gr_stats out = stats();
     if (*errHost() != 0) {  // a device-side wait ran out (or an injected status)
@@ -454,6 +494,9 @@ class PbicgstabNode : public Node {
     return out;
   }
   bool usesInitialGuess() const override { return true; }
+  void refresh() override {
+    if (pre_) pre_->refresh();
+  }
   std::vector<gr_stats> batchStats() const override {
     std::vector<gr_stats> out(systems_);
     for (int k = 0; k < systems_; ++k) out[k] = statsOf(host_[k]);
@@ -478,6 +521,8 @@ class PbicgstabNode : public Node {
 
   void* buf(int i) { return static_cast<char*>(vec_.get()) + static_cast<size_t>(i) * A_.n * dtypeSize(bufType_); }
   DBuf refTiles_;  // per-tile values of the reference-order reductions
+  DBuf bw_;        // b in the working type (workingType float64 over float32 vectors)
+  bool mixed_ = false, graphMixed_ = false;
   RefKind normRed() const {
     return cfg_.norm == GR_NORM_L1 ? RefKind::Sum : (cfg_.norm == GR_NORM_LINF ? RefKind::Max : RefKind::SquareSum);
   }
@@ -570,7 +615,7 @@ class PbicgstabNode : public Node {
     q.stIndex = p.stIndex;
     precondition(q, buf(Z), W);
     launchSpmvDot(A_, buf(Z), buf(T), buf(S), 1, st, W, s());
-    launchBicgUpdate(A_, xw(), buf(Y), buf(Z), buf(R), buf(S), buf(T), buf(R0), st, W, s());
+    launchBicgUpdate(A_, xw(), buf(Y), buf(Z), buf(R), buf(S), buf(T), buf(R0), st, W, s(), false, mixed_);
   }
 
   // The same iteration with the reference's float reductions: the fused
@@ -604,7 +649,7 @@ class PbicgstabNode : public Node {
   }
 
   void launchBatch(DType W) {
-    if (!exec_ || graphType_ != W) {
+    if (!exec_ || graphType_ != W || graphMixed_ != mixed_) {
       if (exec_) cudaGraphExecDestroy(exec_);
       exec_ = nullptr;
       cudaGraph_t g = nullptr;
@@ -627,6 +672,7 @@ class PbicgstabNode : public Node {
       GR_CUDA(cudaGraphInstantiate(&exec_, g, 0));
       cudaGraphDestroy(g);
       graphType_ = W;
+      graphMixed_ = mixed_;
       graphKernels_ = kernels;
     }
     GR_CUDA(cudaGraphLaunch(exec_, s()));
@@ -693,6 +739,7 @@ class MpirNode : public Node {
     return st;
   }
   bool usesInitialGuess() const override { return true; }
+  void refresh() override { inner_->refresh(); }
   void copyPhi(void* out, DType t) override {
     if (!phi_.get()) fail(GR_EINVAL, "no IterativeRefinement solve has run yet");
     launchConvert(phi_.get(), E_, out, t, A_.n, s());
@@ -729,6 +776,7 @@ class RestarterNode : public Node {
   }
   bool usesInitialGuess() const override { return inner_->usesInitialGuess(); }
   void copyPhi(void* out, DType t) override { inner_->copyPhi(out, t); }
+  void refresh() override { inner_->refresh(); }
 
  private:
   std::unique_ptr<Node> inner_;
@@ -817,6 +865,10 @@ class Tree : public SolverTree {
   void copyPhi(void* out, DType t) override { root_->copyPhi(out, t); }
   std::vector<gr_stats> batchStats() const override { return root_->batchStats(); }
   std::string name() const override { return cfg_->solverName(); }
+  void refresh() override {
+    root_->refresh();
+    GR_CUDA(cudaStreamSynchronize(A_.stream));
+  }
 
  private:
   DeviceMatrix& A_;

@@ -28,6 +28,11 @@ class SolverTree {
   // Per-system statistics of the last solve on a batch matrix.
   virtual std::vector<gr_stats> batchStats() const = 0;
   virtual std::string name() const = 0;
+  // After the matrix's values were replaced (DeviceMatrix::updateValues):
+  // recomputes every value-dependent part (ILU factors, packed level
+  // blocks) in the buffers the tree already owns, so its captured iteration
+  // graphs stay valid.
+  virtual void refresh() = 0;
 };
 
 }  // namespace gr

@@ -153,6 +153,19 @@ int gr_host_matrix_generate(gr_generator kind, int64_t nx, int64_t ny, int64_t n
                             gr_partitioner partitioner, gr_dtype value_type,
                             gr_host_matrix** out);
 
+/* The same generator with `like`'s structure: the new matrix's values come
+ * from (kind, params, seed), its partition, tile layout, tile-local pattern
+ * and level sets are copied from `like` (which must have been generated
+ * with the same kind and grid; GR_EINVAL if the pattern differs). The cheap
+ * way to produce many systems that share a sparsity pattern, e.g. a stream
+ * of solves with fresh coefficients. No counterpart in the reference. */
+int gr_host_matrix_generate_like(const gr_host_matrix* like, gr_generator kind, int64_t nx, int64_t ny,
+                                 int64_t nz, const double* params, uint64_t seed, gr_host_matrix** out);
+/* Structure identity of a host matrix (a hash of its value type, sparsity
+ * pattern and tile map): equal keys mean equal partition, layout and level
+ * sets. No counterpart in the reference. */
+int gr_host_matrix_structure_key(const gr_host_matrix* h, uint64_t* key);
+
 /* Seeded vectors from the generators' counter-based stream: dist 0 =
  * uniform [lo, hi), dist 1 = standard normal. */
 int gr_random_vector(uint64_t seed, int64_t n, int dist, double lo, double hi, double* out);
@@ -380,6 +393,18 @@ int gr_solver_time_repeated(gr_solver* s, void* x, gr_dtype x_t, const void* b, 
  * type t in tile order. The reference returns only (float)phi. */
 int gr_solver_phi(gr_solver* s, void* out, gr_dtype t);
 
+/* Value updates on a resident structure (no counterpart in the reference,
+ * whose graph is compiled for one matrix). gr_matrix_update_values replaces
+ * A's coefficients by h's, where h has A's structure (equal
+ * gr_host_matrix_structure_key, CRS; GR_EINVAL otherwise): the values are
+ * uploaded and scattered into the device layout in place, and no host-side
+ * layout work is redone. gr_solver_refresh then recomputes a solver's
+ * value-dependent parts (ILU factors, packed level blocks) in the buffers
+ * it owns. The pair costs one upload and one factorisation instead of a
+ * new matrix and solver. */
+int gr_matrix_update_values(gr_matrix* A, gr_host_matrix* h);
+int gr_solver_refresh(gr_solver* s);
+
 /* Name of the solver tree, e.g. "IterativeRefinement(PBiCGStab(ILU(0)))". */
 int gr_solver_name(const gr_solver* s, char* buf, size_t len);
 
@@ -414,7 +439,8 @@ typedef struct {
   double admitted_ms;  /* a slot and memory were granted */
   double finished_ms;  /* result copied back */
   int64_t footprint_bytes; /* estimated device bytes of the request's resident pair */
-  int32_t cache_hit;   /* 1: the pair was already resident */
+  int32_t cache_hit;   /* 1: the pair was already resident; 2: a pair with the
+                          same structure was, and took this matrix's values */
   int32_t slot;
 } gr_request_times;
 

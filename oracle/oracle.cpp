@@ -874,8 +874,10 @@ void iluSolve(const or_matrix& A, const std::vector<std::vector<V>>& off,
   });
 }
 
-// gaussseidel::Solver::solveIterationCSR (gauss-seidel/Solver.cpp:45-86).
-template <class V, class T>
+// gaussseidel::Solver::solveIterationCSR (gauss-seidel/Solver.cpp:45-86):
+// each row computed in the working type W (:76-82, every operand cast to
+// it) and stored in x's type T (:83).
+template <class V, class T, class W = T>
 void gsSweep(const or_matrix& A, const TileValues<V>& tv, std::vector<T>& x, const std::vector<T>& b,
              bool seedB) {
   exchange(A, x);
@@ -884,10 +886,10 @@ void gsSweep(const or_matrix& A, const TileValues<V>& tv, std::vector<T>& x, con
     const size_t nRows = L.diag.size();
     const size_t hb = A.haloStart[t];
     for (size_t i = 0; i < nRows; ++i) {
-      T sum = seedB ? b[hb + i] : static_cast<T>(tv.diag[t][i]);
+      W sum = seedB ? static_cast<W>(b[hb + i]) : static_cast<W>(tv.diag[t][i]);
       for (size_t j = L.rowPtr[i]; j < L.rowPtr[i + 1]; ++j)
-        sum -= static_cast<T>(tv.off[t][j]) * x[hb + L.colInd[j]];
-      x[hb + i] = sum / static_cast<T>(tv.diag[t][i]);
+        sum -= static_cast<W>(tv.off[t][j]) * static_cast<W>(x[hb + L.colInd[j]]);
+      x[hb + i] = static_cast<T>(sum / static_cast<W>(tv.diag[t][i]));
     }
   });
 }
@@ -949,22 +951,31 @@ struct GsNode : SolverNode<V, T> {
   const Conf& c;
   GsNode(Ctx<V>& ctx, const Conf& conf) : C(ctx), c(conf) {}
   Stats solve(std::vector<T>& x, const std::vector<T>& b) override {
+    // workingType (gauss-seidel/Solver.cpp:65, :114): the sweeps and the
+    // residual in W, x kept in its own type.
+    const int wt = c.workingType < 0 ? (std::is_same_v<T, float> ? 0 : 1) : c.workingType;
+    if (wt == 1) return solveIn<double>(x, b);
+    if (wt == 0) return solveIn<float>(x, b);
+    throw OErr("GaussSeidel workingType must be float32 or float64");
+  }
+  template <class W>
+  Stats solveIn(std::vector<T>& x, const std::vector<T>& b) {
     Stats s;
     if (c.numFixedIterations > 0) {
-      for (int k = 0; k < c.numFixedIterations; ++k) gsSweep<V, T>(C.A, C.tv, x, b, c.gsSeedB);
+      for (int k = 0; k < c.numFixedIterations; ++k) gsSweep<V, T, W>(C.A, C.tv, x, b, c.gsSeedB);
       s.iterations = c.numFixedIterations;
       return s;
     }
     if (c.relTolerance > 0) s.bNorm = normT(C.A, b, c.norm);
-    std::vector<T> r(C.A.nWithHalo);
-    residualT<V, T, T, T, T>(C.A, C.tv, x, b, r);
+    std::vector<W> r(C.A.nWithHalo);
+    residualT<V, T, T, W, W>(C.A, C.tv, x, b, r);
     s.init = s.fin = normT(C.A, r, c.norm);
     while (!((s.converged && s.iterations >= c.minIterations) || s.iterations >= c.maxIterations)) {
       for (int k = 0; k < c.numSweeps; ++k) {
-        gsSweep<V, T>(C.A, C.tv, x, b, c.gsSeedB);
+        gsSweep<V, T, W>(C.A, C.tv, x, b, c.gsSeedB);
         s.iterations++;
       }
-      residualT<V, T, T, T, T>(C.A, C.tv, x, b, r);
+      residualT<V, T, T, W, W>(C.A, C.tv, x, b, r);
       s.fin = normT(C.A, r, c.norm);
       s.check(c);
     }
@@ -975,22 +986,42 @@ struct GsNode : SolverNode<V, T> {
 
 template <class T> T rnd(double v) { return static_cast<T>(v); }
 
-// pbicgstab::Solver::solve (pbicgstab/Solver.cpp:48-194)
+// pbicgstab::Solver::solve (pbicgstab/Solver.cpp:48-194). With a
+// workingType other than x's type (:63), every vector but x is in the
+// working type W, the residual is computed in W (:66), the preconditioner
+// runs on W vectors, and x = x + alpha y + omega z is evaluated in W and
+// rounded to x's type each iteration (:164).
 template <class V, class T>
 struct PbicgstabNode : SolverNode<V, T> {
+  using O = std::conditional_t<std::is_same_v<T, float>, double, float>;
   Ctx<V>& C;
   const Conf& c;
   std::unique_ptr<SolverNode<V, T>> pre;
+  std::unique_ptr<SolverNode<V, O>> preO;  // the preconditioner on working-type vectors
+  bool other = false;                       // working type differs from x's type
   PbicgstabNode(Ctx<V>& ctx, const Conf& conf) : C(ctx), c(conf) {
-    if (conf.pre) pre = makeNode<V, T>(ctx, *conf.pre);
+    if (conf.workingType == 2) throw OErr("PBiCGStab workingType twofloat32 is not supported");
+    other = conf.workingType >= 0 && conf.workingType != (std::is_same_v<T, float> ? 0 : 1);
+    if (conf.pre) {
+      if (other) preO = makeNode<V, O>(ctx, *conf.pre);
+      else pre = makeNode<V, T>(ctx, *conf.pre);
+    }
   }
   Stats solve(std::vector<T>& x, const std::vector<T>& b) override {
-    if (c.reduceRef) return solveRef(x, b);
+    if (c.reduceRef) {
+      if (other) throw OErr("reduce f32_ref_order needs the working type of x");
+      return solveRef(x, b);
+    }
+    if (other) return core<O>(x, b, preO.get());
+    return core<T>(x, b, pre.get());
+  }
+  template <class W>
+  Stats core(std::vector<T>& x, const std::vector<T>& b, SolverNode<V, W>* pre) {
     const or_matrix& A = C.A;
     const size_t N = A.nWithHalo;
     Stats s;
-    std::vector<T> r(N), r0, p, v(N), y(N), z(N), sv(N), tv(N);
-    residualT<V, T, T, T, T>(A, C.tv, x, b, r);
+    std::vector<W> r(N), r0, p, v(N), y(N), z(N), sv(N), tv(N);
+    residualT<V, T, T, W, W>(A, C.tv, x, b, r);
     if (c.relTolerance > 0) s.bNorm = normT(A, b, c.norm);  // the reference uses x here (:70)
     s.init = s.fin = normT(A, r, c.norm);
     r0 = r;
@@ -1002,41 +1033,41 @@ struct PbicgstabNode : SolverNode<V, T> {
       s.singular = s.singular || std::fabs(rho) < kVsmall;
       if (s.singular) break;
       if (s.iterations != 0) {
-        T beta = rnd<T>((rho / rhoOld) * (alpha / omega));
-        T om = rnd<T>(omega);
+        W beta = rnd<W>((rho / rhoOld) * (alpha / omega));
+        W om = rnd<W>(omega);
         forTiles(A.P, [&](size_t t) {
           for (size_t i = A.haloStart[t]; i < A.haloStart[t] + A.tileStart[t + 1] - A.tileStart[t]; ++i)
             p[i] = r[i] + beta * (p[i] - om * v[i]);
         });
       }
       if (pre) {
-        if (pre->usesInitialGuess()) std::fill(y.begin(), y.end(), T(0));
+        if (pre->usesInitialGuess()) std::fill(y.begin(), y.end(), W(0));
         pre->solve(y, p);
       } else {
         y = p;
       }
-      spmvT<V, T>(A, C.tv, y, v);
+      spmvT<V, W>(A, C.tv, y, v);
       alpha = rho / dotT(A, r0, v);
-      T al = rnd<T>(alpha);
+      W al = rnd<W>(alpha);
       forTiles(A.P, [&](size_t t) {
         for (size_t i = A.haloStart[t]; i < A.haloStart[t] + A.tileStart[t + 1] - A.tileStart[t]; ++i)
           sv[i] = r[i] - al * v[i];
       });
       if (pre) {
-        if (pre->usesInitialGuess()) std::fill(z.begin(), z.end(), T(0));
+        if (pre->usesInitialGuess()) std::fill(z.begin(), z.end(), W(0));
         pre->solve(z, sv);
       } else {
         z = sv;
       }
-      spmvT<V, T>(A, C.tv, z, tv);
+      spmvT<V, W>(A, C.tv, z, tv);
       double tt = dotT(A, tv, tv);
       omega = dotT(A, tv, sv) / tt;
       s.singular = s.singular || std::fabs(omega) < kVsmall;
       if (s.singular) break;
-      T om = rnd<T>(omega);
+      W om = rnd<W>(omega);
       forTiles(A.P, [&](size_t t) {
         for (size_t i = A.haloStart[t]; i < A.haloStart[t] + A.tileStart[t + 1] - A.tileStart[t]; ++i) {
-          x[i] = x[i] + al * y[i] + om * z[i];
+          x[i] = static_cast<T>(static_cast<W>(x[i]) + al * y[i] + om * z[i]);
           r[i] = sv[i] - om * tv[i];
         }
       });

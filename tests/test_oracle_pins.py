@@ -353,3 +353,42 @@ def test_reference_order_reduction_golden(oracle):
     om = oracle.poisson(8, 1, 1, 4, np.repeat(np.arange(4, dtype=np.int32), 2))
     assert om.ref_norm(np.ascontiguousarray(data[:, 0]), 0) == 56.0
     assert om.ref_norm(np.ascontiguousarray(data[:, 1]), 0) == 64.0
+
+
+def py_gs_sweep_working_f64(rp, ci, od, dg, x, b):
+    """A Gauss-Seidel sweep with workingType float64 over float32 x
+    (gauss-seidel/Solver.cpp:65-84): each row in double, stored as float."""
+    x = x.copy()
+    for i in range(len(dg)):
+        s = np.float64(b[i])
+        for p in range(rp[i], rp[i + 1]):
+            s = s - np.float64(F32(od[p])) * np.float64(x[ci[p]])
+        x[i] = F32(s / np.float64(F32(dg[i])))
+    return x
+
+
+def test_oracle_gs_float64_working_type(small_case):
+    n, r, c, v, om = small_case
+    rng = np.random.default_rng(15)
+    x = rng.standard_normal(n).astype(F32)
+    b = rng.standard_normal(n).astype(F32)
+    cfg = json.dumps({"type": "GaussSeidel", "numFixedIterations": 2, "workingType": "float64"})
+    got, _, _, _ = om.solve(cfg, x, b)
+    parts = csr_parts(om)
+    want = py_gs_sweep_working_f64(*parts, py_gs_sweep_working_f64(*parts, x, b), b)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_oracle_reference_order_pbicgstab_converges(oracle):
+    """The oracle's PBiCGStab with the reference's float reductions reaches
+    the tolerance like the FP64-reduction one, with a similar count."""
+    n, r, c, v = poisson_coo(10, 9, 8)
+    tiles = np.arange(n, dtype=np.int32) * 6 // n
+    om = oracle.matrix(n, r, c, v, 6, tiles, 0)
+    b = om.spmv(np.random.default_rng(1).uniform(-1, 1, n).astype(F32))
+    cfg = {"type": "PBiCGStab", "maxIterations": 300, "relResidual": 1e-6, "preconditioner": {"type": "ILU"}}
+    _, st64, _, _ = om.solve(json.dumps(cfg), np.zeros(n, F32), b)
+    _, st32, _, _ = om.solve(json.dumps(dict(cfg, reduce="f32_ref_order")), np.zeros(n, F32), b)
+    assert st64.converged and st32.converged
+    assert abs(st64.iterations - st32.iterations) <= 2
+    assert np.float32(st32.final_residual) == st32.final_residual  # stored as float

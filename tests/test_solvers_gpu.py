@@ -424,3 +424,64 @@ def test_reference_order_rejects_float64_vectors(oracle):
     b = dev(np.ones(h.numRows))
     with pytest.raises(gb.GrapheneError):
         gb.Solver(A, pbicgstab("ilu", 10, 1e-6, reduce="f32_ref_order")).solve(dev(np.zeros(h.numRows)), b)
+
+
+@pytest.mark.parametrize("name", ["poisson16", "random", "many_tiles"])
+@pytest.mark.parametrize("sweeps", [1, 3])
+def test_gauss_seidel_float64_working_type_bit_exact(oracle, name, sweeps):
+    """GaussSeidel "workingType": "float64" over float32 x and b: each row
+    computed in double and stored as float (gauss-seidel/Solver.cpp:65-84)."""
+    h, om = case(name, oracle)
+    A = h.copyToTile()
+    rng = np.random.default_rng(13)
+    b = rng.uniform(-1, 1, h.numRows).astype(np.float32)
+    x0 = rng.uniform(-1, 1, h.numRows).astype(np.float32)
+    cfg = {"type": "GaussSeidel", "numFixedIterations": sweeps, "workingType": "float64"}
+    x = dev(x0)
+    gb.Solver(A, cfg).solve(x, dev(b))
+    xo, _, _, _ = om.solve(json.dumps(cfg), x0.copy(), b)
+    np.testing.assert_array_equal(host(x), xo)
+    # It differs from the float32 sweep (the working type matters).
+    xf, _, _, _ = om.solve(json.dumps({"type": "GaussSeidel", "numFixedIterations": sweeps}), x0.copy(), b)
+    assert not np.array_equal(xo, xf)
+
+
+def test_gauss_seidel_float64_working_type_with_checks(oracle):
+    h, om = case("poisson16", oracle)
+    A = h.copyToTile()
+    b = np.ones(h.numRows, np.float32)
+    cfg = {"type": "GaussSeidel", "numSweeps": 2, "maxIterations": 300, "relResidual": 1e-4,
+           "workingType": "float64"}
+    x = dev(np.zeros(h.numRows, np.float32))
+    st = gb.Solver(A, cfg).solve(x, dev(b))
+    xo, ost, _, _ = om.solve(json.dumps(cfg), np.zeros(h.numRows, np.float32), b)
+    assert st.converged and ost.converged and st.iterations == ost.iterations
+    np.testing.assert_array_equal(host(x), xo)
+
+
+@pytest.mark.parametrize("pre", ["ilu", "gs2", "none"])
+def test_pbicgstab_float64_working_type(oracle, pre):
+    """PBiCGStab "workingType": "float64" over float32 x and b
+    (pbicgstab/Solver.cpp:63-79): the Krylov vectors in double, x rounded to
+    float at every update; iterates as close to the oracle's as the FP64
+    reductions allow, and a solution closer to the FP64 truth than a float32
+    working type can reach."""
+    h, om = case("poisson16", oracle)
+    A = h.copyToTile()
+    xt = np.random.default_rng(14).uniform(-1, 1, h.numRows).astype(np.float32)
+    b = om.spmv(xt)
+    for k in (1, 3):
+        cfg = pbicgstab(pre, k, 0.0, workingType="float64")
+        x = dev(np.zeros_like(b))
+        st = gb.Solver(A, cfg).solve(x, dev(b))
+        xo, ost, _, _ = om.solve(json.dumps(cfg), np.zeros_like(b), b)
+        assert st.iterations == ost.iterations == k
+        assert np.abs(host(x) - xo).max() <= 1e-6 * np.abs(xo).max()
+    cfg = pbicgstab(pre, 1000, 1e-9, workingType="float64")
+    x = dev(np.zeros_like(b))
+    st = gb.Solver(A, cfg).solve(x, dev(b))
+    xo, ost, _, _ = om.solve(json.dumps(cfg), np.zeros_like(b), b)
+    assert st.converged and ost.converged
+    assert abs(st.iterations - ost.iterations) <= 2
+    assert host(x).dtype == np.float32
+    np.testing.assert_allclose(host(x), xo, rtol=0, atol=2e-6 * np.abs(xo).max())
