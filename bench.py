@@ -369,66 +369,124 @@ def other_configs(gb, peak):
     return out
 
 
-def serving(gb, requests=300, slots=4, pool=32, seed=7):
-    """Solve server under a Poisson arrival stream: 7-point variable-coefficient
-    Poisson systems (sigma 1) with grid edge U{16..96}, 70 % FP32
-    PBiCGStab-ILU(0) to 1e-6 and 30 % MPIR to 1e-10 (by seed). Throughput at
-    saturation (all requests submitted at once), then p50 / p99 latency from
-    arrival to result at 50 %, 80 % and 100 % of that throughput. 'resident':
-    requests draw from `pool` distinct matrices that stay resident; 'cold':
-    every request brings a matrix the server has not seen (upload and ILU
-    factorisation in its latency)."""
+def serving(gb, requests=10000, slots=8, seed=7, rate_requests=2000, cold_requests=48, gen_threads=0):
+    """C5: a stream of solves, each a fresh 7-point variable-coefficient
+    Poisson system (sigma 1) with grid edge L ~ U{16..96}, 70 % FP32
+    PBiCGStab-ILU(0) to 1e-6 and 30 % MPIR to 1e-10 (by seed).
+
+    Every request has its own coefficients (seed 100000 + k). Host threads
+    generate the requests just ahead of their arrival: the values alone
+    (gr_host_matrix_generate_values) on the layout of one template matrix
+    per edge, submitted with gr_server_submit_values, so the client never
+    holds more than a bounded number of systems. The server keeps one
+    resident pair per (structure, configuration) and serves a request on a
+    resident structure by uploading its values and refactorising in place.
+
+    Saturation: all `requests` submitted as fast as they are generated;
+    throughput = requests / (last finish - first arrival). Latency: Poisson
+    arrivals at 50 %, 80 % and 100 % of that throughput, `rate_requests`
+    each; p50 / p99 from arrival to result. Cold: `cold_requests` requests
+    whose structures the server has never seen (tile layout, level rings,
+    upload and factorisation all in the latency)."""
+    import concurrent.futures as cf
     import numpy as np
-    rng = np.random.default_rng(seed)
     ilu = {"type": "PBiCGStab", "maxIterations": 1000, "relResidual": 1e-6, "preconditioner": {"type": "ILU"}}
     mpir = {"type": "IterativeRefinement", "relResidual": 1e-10, "maxIterations": 30,
             "extendedPrecisionType": "float64",
             "innerSolver": {"type": "PBiCGStab", "maxIterations": 500, "relResidual": 1e-4,
                             "preconditioner": {"type": "ILU"}}}
+    rng = np.random.default_rng(seed)
+    edges = rng.integers(16, 97, requests)
+    kinds = rng.random(requests) < 0.3
+    tiles = lambda L: max(1, (L ** 3 + 3455) // 3456)  # noqa: E731  (~3456 rows a tile)
+    templates, tlock = {}, threading.Lock()
 
-    def make(k):
-        L = int(rng.integers(16, 97))
-        tiles = max(1, (L ** 3 + 3455) // 3456)
-        h = gb.generateMatrix(gb.GEN_VAR_POISSON, L, L, L, (1.0,), 1000 + k, tiles)
-        return h, gb.randomVector(2000 + k, h.numRows).astype(np.float32)
+    def template(L):
+        with tlock:
+            if L not in templates:
+                templates[L] = (threading.Lock(), None)
+            lk, _ = templates[L]
+        with lk:
+            if templates[L][1] is None:
+                templates[L] = (lk, gb.generateMatrix(gb.GEN_VAR_POISSON, L, L, L, (1.0,), 99, tiles(L)))
+            return templates[L][1]
 
-    def run(srv, items, rate):
-        ids, t0 = [], time.perf_counter()
-        gaps = rng.exponential(1.0 / rate, len(items)) if rate else np.zeros(len(items))
+    def make(k, fresh_structure=False):
+        L = int(edges[k % requests])
+        cfg = mpir if kinds[k % requests] else ilu
+        b = gb.randomVector(200000 + k, L ** 3).astype(np.float32)
+        if fresh_structure:  # a structure nobody has seen: its own tile count
+            return (gb.generateMatrix(gb.GEN_VAR_POISSON, L, L, L, (1.0,), 100000 + k, tiles(L) + 1 + k % 7),
+                    None, b, cfg)
+        tm = template(L)
+        return tm, gb.generateValues(tm, gb.GEN_VAR_POISSON, L, L, L, (1.0,), 100000 + k), b, cfg
+
+    threads = gen_threads or max(2, (os.cpu_count() or 4) - slots // 2)
+    pool = cf.ThreadPoolExecutor(max_workers=threads)
+
+    def run(srv, ks, rate, fresh_structure=False, ahead=256):
+        """Submits requests ks (arrival times from `rate`, None: at once) and
+        collects the results; generation runs `ahead` requests ahead."""
+        gaps = rng.exponential(1.0 / rate, len(ks)) if rate else np.zeros(len(ks))
+        futs, nxt = {}, 0
+
+        def fill(i):
+            nonlocal nxt
+            while nxt < len(ks) and nxt < i + ahead:
+                futs[nxt] = pool.submit(make, ks[nxt], fresh_structure)
+                nxt += 1
+        ids, pending = [], []
+        lat, hits, conv = [], {0: 0, 1: 0, 2: 0}, True
+        first_arrival, last_finish = None, None
+
+        def collect(block):
+            nonlocal conv, last_finish, first_arrival
+            while pending and (block or len(pending) > 2 * slots + 64):
+                rid = pending.pop(0)
+                _, st, tm = srv.wait(rid)
+                lat.append(tm["finished_ms"] - tm["arrival_ms"])
+                hits[tm["cache_hit"]] += 1
+                conv = conv and st.converged
+                first_arrival = tm["arrival_ms"] if first_arrival is None else min(first_arrival, tm["arrival_ms"])
+                last_finish = tm["finished_ms"] if last_finish is None else max(last_finish, tm["finished_ms"])
+        t0 = time.perf_counter()
         due = 0.0
-        for (h, b, cfg), g in zip(items, gaps):
-            due += g
+        for i in range(len(ks)):
+            fill(i)
+            h, vals, b, cfg = futs.pop(i).result()
+            due += gaps[i]
             d = due - (time.perf_counter() - t0)
-            if d > 0:
+            if rate and d > 0:
                 time.sleep(d)
-            ids.append(srv.submit(h, cfg, b))
-        res = [srv.wait(i) for i in ids]
-        lat = np.array([tm["finished_ms"] - tm["arrival_ms"] for _, _, tm in res])
-        span = max(tm["finished_ms"] for _, _, tm in res) - min(tm["arrival_ms"] for _, _, tm in res)
-        ok = all(st.converged for _, st, _ in res)
-        hits = sum(tm["cache_hit"] for _, _, tm in res)
-        return {"offered_per_s": rate, "throughput_per_s": len(res) / (span * 1e-3),
+            pending.append(srv.submit(h, cfg, b) if vals is None else srv.submitValues(h, vals[0], vals[1], cfg, b))
+            del h, vals, b
+            collect(False)
+        collect(True)
+        lat = np.array(lat)
+        span = (last_finish - first_arrival) * 1e-3
+        return {"offered_per_s": rate, "requests": len(ks), "throughput_per_s": len(ks) / span,
                 "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                "all_converged": ok, "resident_hits": int(hits)}
+                "all_converged": conv, "fresh_values_on_resident_structure": hits[2],
+                "resident_same_matrix": hits[1], "new_pairs": hits[0]}
 
-    out = {"requests": requests, "slots": slots}
-    mats = [make(k) for k in range(pool)]
-    cfgs = [mpir if u < 0.3 else ilu for u in rng.random(requests)]
-    items = [(mats[k][0], mats[k][1], c) for k, c in zip(rng.integers(0, pool, requests), cfgs)]
+    out = {"requests": requests, "slots": slots, "generator_threads": threads,
+           "edges": "U{16..96}", "mix": "70 % FP32 PBiCGStab-ILU(0) 1e-6, 30 % MPIR 1e-10",
+           "systems": "every request fresh coefficients (seed 100000 + k)"}
     srv = gb.Server(slots=slots)
-    run(srv, items[: min(len(items), 2 * pool)], None)  # fills the resident set
-    sat = run(srv, items, None)
+    t0 = time.perf_counter()
+    sat = run(srv, list(range(requests)), None)
+    sat["wall_s"] = time.perf_counter() - t0
     res = {"saturation": sat}
     for f in (0.5, 0.8, 1.0):
-        res[f"load_{f}"] = run(srv, items, f * sat["throughput_per_s"])
+        ks = list(range(requests, requests + rate_requests))
+        res[f"load_{f}"] = run(srv, ks, f * sat["throughput_per_s"])
     srv.close()
-    out["resident"] = res
-    cold_n = min(requests, 48)
-    cold = [make(pool + k) for k in range(cold_n)]
+    out["stream"] = res
     srv = gb.Server(slots=slots)
-    out["cold"] = {"requests": cold_n,
-                   "saturation": run(srv, [(h, b, c) for (h, b), c in zip(cold, cfgs)], None)}
+    out["cold"] = run(srv, list(range(requests + rate_requests, requests + rate_requests + cold_requests)), None,
+                      fresh_structure=True)
     srv.close()
+    pool.shutdown()
     return out
 
 
@@ -545,6 +603,7 @@ CASES = {
     "c3-mpir-dw": (_case_c3("dw"), "192^3 var-coeff Poisson, 2048 tiles, MPIR double-word outer"),
     "c3-fp64": (_case_c3("fp64"), "192^3 var-coeff Poisson, 2048 tiles, FP64 PBiCGStab-ILU(0) to 1e-10"),
     "c4-gs-f32": (_case_c4, "100^3 LDU mesh, 1024 tiles, FP32 PBiCGStab-GS(2), 260 iterations at most"),
+    "c5": (None, "serving: 10,000 fresh variable-coefficient Poisson systems, edge U{16..96}, 70/30 ILU/MPIR"),
 }
 
 
@@ -556,6 +615,11 @@ def run_case(a):
     import graphene_b200 as gb
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     build, desc = CASES[a.case]
+    if build is None:  # serving
+        t0 = time.perf_counter()
+        res = serving(gb)
+        print(json.dumps({"case": a.case, "workload": desc, "serving": res, "wall_s": time.perf_counter() - t0}))
+        return 0
     A, cfg, b = build(gb)
     n = A.numRows
 

@@ -35,7 +35,7 @@ __all__ = [
     "PART_AUTO", "PART_CONTIGUOUS", "PART_RCB", "PART_BFS", "PART_EXPLICIT",
     "GrapheneError", "HostMatrix", "Matrix", "Configuration", "Solver", "SolverStats",
     "generate3DPoissonMatrix", "loadMatrixFromFile", "parseType", "launch_count",
-    "generateMatrix", "generateMatrixLike", "generateLduMesh", "randomVector", "Server", "Batch",
+    "generateMatrix", "generateMatrixLike", "generateValues", "generateLduMesh", "randomVector", "Server", "Batch",
 ]
 
 _NP = {FLOAT32: np.float32, FLOAT64: np.float64}
@@ -302,6 +302,16 @@ def generateMatrixLike(like: HostMatrix, kind: int, nx: int, ny: int, nz: int, p
     return HostMatrix(h)
 
 
+def generateValues(like: HostMatrix, kind: int, nx: int, ny: int, nz: int, params=(), seed: int = 0):
+    """(gVal, gDiag): the generator's values in like's global CRS order
+    (gr_host_matrix_generate_values), FP64."""
+    p = (C.c_double * 3)(*(list(params) + [0.0] * (3 - len(params))))
+    gv = np.empty(like.numOffDiag, np.float64)
+    gd = np.empty(like.numRows, np.float64)
+    check(_lib.lib().gr_host_matrix_generate_values(like._h, kind, nx, ny, nz, p, seed, _ptr(gv), _ptr(gd)))
+    return gv, gd
+
+
 def _structure_key(self: HostMatrix) -> int:
     k = C.c_uint64()
     check(_lib.lib().gr_host_matrix_structure_key(self._h, C.byref(k)))
@@ -566,6 +576,22 @@ class Server:
         check(rc)
         times = {k: getattr(tm, k) for k, _ in _lib.RequestTimes._fields_}
         return x, SolverStats._from(st), times
+
+    def submitValues(self, like: HostMatrix, gVal: np.ndarray, gDiag: np.ndarray, config, b: np.ndarray) -> int:
+        """Queues a solve of the matrix with like's structure and the global
+        CRS values gVal / gDiag (gr_server_submit_values), x0 = 0."""
+        js = config if isinstance(config, str) else _json.dumps(config)
+        bb = np.ascontiguousarray(b)
+        gv = np.ascontiguousarray(gVal, dtype=np.float64)
+        gd = np.ascontiguousarray(gDiag, dtype=np.float64)
+        if len(gv) != like.numOffDiag or len(gd) != like.numRows or len(bb) != like.numRows:
+            raise ValueError("values, diagonal or b do not fit the template matrix")
+        t = FLOAT32 if bb.dtype == np.float32 else FLOAT64
+        rid = C.c_uint64()
+        check(_lib.lib().gr_server_submit_values(self._s, like._h, _ptr(gv), _ptr(gd), js.encode(), _ptr(bb), t,
+                                                 C.byref(rid)))
+        self._hosts[rid.value] = (like, bb.dtype)
+        return rid.value
 
     def cancel(self, rid: int) -> bool:
         """Cancels a request that has not been admitted yet (True; its wait

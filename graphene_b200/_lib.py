@@ -130,6 +130,8 @@ SIGNATURES = {
     "gr_host_matrix_structure_key": (C.c_int, [vp, P(C.c_uint64)]),
     "gr_matrix_update_values": (C.c_int, [vp, vp]),
     "gr_solver_refresh": (C.c_int, [vp]),
+    "gr_host_matrix_generate_values": (C.c_int, [vp, C.c_int, i64, i64, i64, P(C.c_double), C.c_uint64, vp, vp]),
+    "gr_server_submit_values": (C.c_int, [vp, vp, vp, vp, C.c_char_p, vp, C.c_int, P(C.c_uint64)]),
     "gr_batch_create": (C.c_int, [P(vp), i32, C.c_char_p, P(vp)]),
     "gr_batch_solve_host": (C.c_int, [vp, P(vp), P(vp), C.c_int, P(Stats)]),
     "gr_batch_destroy": (None, [vp]),

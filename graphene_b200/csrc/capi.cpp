@@ -139,6 +139,7 @@ int gr_host_matrix_generate_like(const gr_host_matrix* like, gr_generator kind, 
   return guarded([&] {
     need(like, "like");
     need(out, "out");
+    GR_TRACE_SCOPE("gr_host_matrix_generate_like");
     gr::GeneratedCsr g;
     switch (kind) {
       case GR_GEN_POISSON:
@@ -158,6 +159,22 @@ int gr_host_matrix_generate_like(const gr_host_matrix* like, gr_generator kind, 
     }
     if (g.n != like->m->n) gr::fail(GR_EINVAL, "the template matrix has another grid");
     *out = new gr_host_matrix{gr::HostMatrix::withValues(*like->m, g.rowPtr, g.col, g.val)};
+  });
+}
+
+int gr_host_matrix_generate_values(const gr_host_matrix* like, gr_generator kind, int64_t nx, int64_t ny,
+                                   int64_t nz, const double* params, uint64_t seed, double* g_val, double* g_diag) {
+  return guarded([&] {
+    need(like, "like");
+    need(g_val, "g_val");
+    need(g_diag, "g_diag");
+    const double zero[3] = {0, 0, 0};
+    if (kind != GR_GEN_POISSON) need(params, "params");
+    if (nx * ny * nz != like->m->n || like->m->format != GR_FORMAT_CRS)
+      gr::fail(GR_EINVAL, "the template matrix has another grid");
+    if (!gr::generateValues(static_cast<int>(kind), nx, ny, nz, params ? params : zero, seed, like->m->gRowPtr,
+                            g_val, g_diag))
+      gr::fail(GR_EINVAL, "the template matrix does not have this generator's pattern");
   });
 }
 
@@ -680,6 +697,19 @@ int gr_server_counters(gr_server* s, int64_t* queued, int64_t* running, int64_t*
   return guarded([&] {
     need(s, "server");
     s->s->counters(queued, running, completed, bytes_in_use, resident);
+  });
+}
+
+int gr_server_submit_values(gr_server* s, gr_host_matrix* like, const double* g_val, const double* g_diag,
+                            const char* json, const void* b, gr_dtype t, uint64_t* id) {
+  return guarded([&] {
+    need(s, "server");
+    need(like, "like");
+    need(g_val, "g_val");
+    need(g_diag, "g_diag");
+    need(json, "json");
+    need(id, "id");
+    *id = s->s->submitValues(like->m, g_val, g_diag, json, b, gr::toDType(t));
   });
 }
 

@@ -370,6 +370,10 @@ struct DeviceMatrix {
   // layout on the device; every layout array, schedule and level-ring
   // template stays. Solver trees on this matrix then need refresh().
   void updateValues(std::shared_ptr<HostMatrix> h);
+  // The same from values already in this matrix's layout: tile-local CRS
+  // off-diagonals (m) and the tile-ordered diagonal (n), in FP64 (rounded
+  // to the coefficient type here). The host matrix's own values go stale.
+  void updateValues(const std::vector<double>& localOff, const std::vector<double>& tileDiag);
   DBuf sellSrc;  // tile-local CRS entry of every SELL slot (-1: padding), built on the first update
   LevelSchedule& schedule(SweepEntries kind);
   // Rounded-up kernel grid for a row loop of n rows.

@@ -3,6 +3,8 @@
 // natural row order row = k*nx*ny + j*nx + i and drop neighbours outside the
 // grid; rows are emitted sorted by column. Random numbers come from a
 // counter-based splitmix64 stream, so a matrix depends only on its seed.
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 
 #include "host_matrix.hpp"
@@ -69,43 +71,107 @@ GeneratedCsr sevenPoint(i64 nx, i64 ny, i64 nz, Coef coef, Diag diag) {
   return g;
 }
 
-}  // namespace
-
-// Variable-coefficient Poisson: cell conductivity k = exp(sigma * N(0,1));
-// face coefficient = harmonic mean 2 k_a k_b / (k_a + k_b); off-diagonal =
-// -face coefficient; diagonal = sum of face coefficients plus 2 k for every
-// boundary face (Dirichlet condition at the face). Computed in FP64.
-GeneratedCsr generateVarPoisson(i64 nx, i64 ny, i64 nz, double sigma, uint64_t seed) {
+// The values of a 7-point matrix only, in the order sevenPoint emits them:
+// each row's off-diagonals (-z, -y, -x, +x, +y, +z, present ones) at
+// gVal[gRowPtr[r]..], its diagonal at gDiag[r]. False if gRowPtr is not
+// this grid's pattern.
+template <class Coef, class Diag>
+bool sevenPointValues(i64 nx, i64 ny, i64 nz, Coef coef, Diag diag, const std::vector<i64>& gRowPtr, double* gVal,
+                      double* gDiag) {
   const i64 n = nx * ny * nz;
-  std::vector<double> kc(n);
+  if (static_cast<i64>(gRowPtr.size()) != n + 1) return false;
+  std::atomic<bool> ok{true};
   parallelChunks(n, [&](i64 b, i64 e) {
-    for (i64 r = b; r < e; ++r) kc[r] = std::exp(sigma * normal(seed, static_cast<uint64_t>(r)));
+    for (i64 r = b; r < e; ++r) {
+      const i64 i = r % nx, j = (r / nx) % ny, k = r / (nx * ny);
+      const bool has[6] = {k > 0, j > 0, i > 0, i < nx - 1, j < ny - 1, k < nz - 1};
+      i64 o = gRowPtr[r];
+      for (int d = 0; d < 6; ++d)
+        if (has[d]) {
+          if (o >= gRowPtr[r + 1]) {
+            ok = false;
+            return;
+          }
+          gVal[o++] = coef(r, d);
+        }
+      if (o != gRowPtr[r + 1]) ok = false;
+      gDiag[r] = diag(r);
+    }
   });
-  const i64 off[6] = {-nx * ny, -nx, -1, 1, nx, nx * ny};
-  auto face = [&](i64 r, int d) {
+  return ok;
+}
+
+// Variable-coefficient Poisson stencil: cell conductivity k = exp(sigma *
+// N(0,1)); face coefficient = harmonic mean 2 k_a k_b / (k_a + k_b);
+// off-diagonal = -face coefficient; diagonal = sum of face coefficients
+// plus 2 k for every boundary face (Dirichlet condition at the face).
+// Computed in FP64.
+struct VarPoissonStencil {
+  i64 nx, ny, nz;
+  std::vector<double> kc;
+  i64 off[6];
+  VarPoissonStencil(i64 x, i64 y, i64 z, double sigma, uint64_t seed) : nx(x), ny(y), nz(z), kc(x * y * z) {
+    const i64 n = nx * ny * nz;
+    parallelChunks(n, [&](i64 b, i64 e) {
+      for (i64 r = b; r < e; ++r) kc[r] = std::exp(sigma * normal(seed, static_cast<uint64_t>(r)));
+    });
+    const i64 o[6] = {-nx * ny, -nx, -1, 1, nx, nx * ny};
+    std::copy(o, o + 6, off);
+  }
+  double face(i64 r, int d) const {
     const double a = kc[r], bb = kc[r + off[d]];
     return 2.0 * a * bb / (a + bb);
-  };
-  auto coef = [&](i64 r, int d) { return -face(r, d); };
-  auto diag = [&](i64 r) {
+  }
+  double coef(i64 r, int d) const { return -face(r, d); }
+  double diag(i64 r) const {
     i64 i = r % nx, j = (r / nx) % ny, k = r / (nx * ny);
     const bool has[6] = {k > 0, j > 0, i > 0, i < nx - 1, j < ny - 1, k < nz - 1};
     double s = 0;
     for (int d = 0; d < 6; ++d) s += has[d] ? face(r, d) : 2.0 * kc[r];
     return s;
-  };
-  return sevenPoint(nx, ny, nz, coef, diag);
-}
+  }
+};
 
 // Upwind convection-diffusion with unit diffusion and grid spacing and
 // velocity (vx, vy, vz) >= 0: neighbour coefficients -(1 + v_d) upstream,
 // -1 downstream; diagonal 6 + vx + vy + vz, kept at the boundary.
+struct ConvDiffStencil {
+  double up[6], dg;
+  ConvDiffStencil(double vx, double vy, double vz)
+      : up{-(1.0 + vz), -(1.0 + vy), -(1.0 + vx), -1.0, -1.0, -1.0}, dg(6.0 + vx + vy + vz) {}
+  double coef(i64, int d) const { return up[d]; }
+  double diag(i64) const { return dg; }
+};
+
+}  // namespace
+
+GeneratedCsr generateVarPoisson(i64 nx, i64 ny, i64 nz, double sigma, uint64_t seed) {
+  const VarPoissonStencil S(nx, ny, nz, sigma, seed);
+  return sevenPoint(nx, ny, nz, [&](i64 r, int d) { return S.coef(r, d); }, [&](i64 r) { return S.diag(r); });
+}
+
 GeneratedCsr generateConvDiff(i64 nx, i64 ny, i64 nz, double vx, double vy, double vz) {
-  const double up[6] = {-(1.0 + vz), -(1.0 + vy), -(1.0 + vx), -1.0, -1.0, -1.0};
-  auto coef = [&](i64, int d) { return up[d]; };
-  const double dg = 6.0 + vx + vy + vz;
-  auto diag = [&](i64) { return dg; };
-  return sevenPoint(nx, ny, nz, coef, diag);
+  const ConvDiffStencil S(vx, vy, vz);
+  return sevenPoint(nx, ny, nz, [&](i64 r, int d) { return S.coef(r, d); }, [&](i64 r) { return S.diag(r); });
+}
+
+bool generateValues(int kind, i64 nx, i64 ny, i64 nz, const double* params, uint64_t seed,
+                    const std::vector<i64>& gRowPtr, double* gVal, double* gDiag) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) fail(GR_EINVAL, "grid dimensions must be positive");
+  if (kind == 0)
+    return sevenPointValues(nx, ny, nz, [](i64, int) { return -1.0; }, [](i64) { return 6.0; }, gRowPtr, gVal, gDiag);
+  if (kind == 1) {
+    const VarPoissonStencil S(nx, ny, nz, params[0], seed);
+    return sevenPointValues(nx, ny, nz, [&](i64 r, int d) { return S.coef(r, d); },
+                            [&](i64 r) { return S.diag(r); }, gRowPtr, gVal, gDiag);
+  }
+  if (kind == 2) {
+    if (params[0] < 0 || params[1] < 0 || params[2] < 0) fail(GR_EINVAL, "velocity must be >= 0");
+    const ConvDiffStencil S(params[0], params[1], params[2]);
+    return sevenPointValues(nx, ny, nz, [&](i64 r, int d) { return S.coef(r, d); },
+                            [&](i64 r) { return S.diag(r); }, gRowPtr, gVal, gDiag);
+  }
+  fail(GR_EINVAL, "unknown generator");
 }
 
 // Uniform [lo, hi) values of stream `seed` (used for seeded right-hand sides).

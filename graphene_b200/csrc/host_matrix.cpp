@@ -247,6 +247,34 @@ void HostMatrix::computeStructureKey() {
   structureKey = h == 0 ? 1 : h;
 }
 
+void HostMatrix::localValues(const double* gv, const double* gd, std::vector<double>& off,
+                             std::vector<double>& dg) const {
+  if (static_cast<i64>(localSrc.size()) != m) fail(GR_EUNSUPPORTED, "no tile-local entry map");
+  off.resize(m);
+  dg.resize(n);
+  parallelChunks(m, [&](i64 b, i64 e) {
+    for (i64 p = b; p < e; ++p) off[p] = roundTo(valueType, gv[localSrc[p]]);
+  });
+  parallelChunks(n, [&](i64 b, i64 e) {
+    for (i64 p = b; p < e; ++p) dg[p] = roundTo(valueType, gd[iperm[p]]);
+  });
+}
+
+std::shared_ptr<HostMatrix> HostMatrix::withGlobalValues(const HostMatrix& like, const double* gv,
+                                                         const double* gd) {
+  if (like.format != GR_FORMAT_CRS || !like.sumRank.empty())
+    fail(GR_EUNSUPPORTED, "values-only updates are for CRS matrices");
+  auto A = std::make_shared<HostMatrix>(like);
+  parallelChunks(like.m, [&](i64 b, i64 e) {
+    for (i64 k = b; k < e; ++k) A->gVal[k] = roundTo(like.valueType, gv[k]);
+  });
+  parallelChunks(like.n, [&](i64 b, i64 e) {
+    for (i64 k = b; k < e; ++k) A->gDiag[k] = roundTo(like.valueType, gd[k]);
+  });
+  like.localValues(gv, gd, A->offDiag, A->diag);
+  return A;
+}
+
 std::shared_ptr<HostMatrix> HostMatrix::withValues(const HostMatrix& like, const std::vector<i64>& rowPtr,
                                                    const std::vector<i64>& col, const std::vector<double>& val) {
   if (like.format != GR_FORMAT_CRS || !like.sumRank.empty())
@@ -254,6 +282,7 @@ std::shared_ptr<HostMatrix> HostMatrix::withValues(const HostMatrix& like, const
   if (static_cast<i64>(rowPtr.size()) != like.n + 1 || static_cast<i64>(col.size()) != like.n + like.m ||
       col.size() != val.size() || static_cast<i64>(like.localSrc.size()) != like.m)
     fail(GR_EINVAL, "the new values do not have the template matrix's pattern");
+  GR_TRACE_SCOPE("values on a template's structure");
   auto A = std::make_shared<HostMatrix>(like);
   std::atomic<bool> bad{false};
   parallelChunks(like.n, [&](i64 b, i64 e) {

@@ -124,6 +124,15 @@ struct HostMatrix {
   static std::shared_ptr<HostMatrix> withValues(const HostMatrix& like, const std::vector<i64>& rowPtr,
                                                 const std::vector<i64>& col, const std::vector<double>& val);
 
+  // Global CRS values of this structure (gVal order, rounded to the value
+  // type) converted to the tile-local CRS order and the tile-ordered
+  // diagonal, the layout a device matrix takes them in.
+  void localValues(const double* gVal, const double* gDiag, std::vector<double>& off,
+                   std::vector<double>& dg) const;
+  // `like`'s structure with global CRS values (gVal order) and a diagonal.
+  static std::shared_ptr<HostMatrix> withGlobalValues(const HostMatrix& like, const double* gVal,
+                                                      const double* gDiag);
+
   gr_matrix_info info() const;
 
   template <class T>
@@ -163,6 +172,12 @@ GeneratedCsr generatePoisson(i64 nx, i64 ny, i64 nz);
 GeneratedCsr generateVarPoisson(i64 nx, i64 ny, i64 nz, double sigma, uint64_t seed);
 GeneratedCsr generateConvDiff(i64 nx, i64 ny, i64 nz, double vx, double vy, double vz);
 void generateUniform(uint64_t seed, i64 n, double lo, double hi, double* out);
+// The values of generator `kind` (0 Poisson, 1 variable-coefficient, 2
+// convection-diffusion) in a generated matrix's global CRS order: the
+// off-diagonals at gVal (gRowPtr offsets), the diagonal at gDiag. The same
+// numbers as the full generator; false when gRowPtr is not the grid's.
+bool generateValues(int kind, i64 nx, i64 ny, i64 nz, const double* params, uint64_t seed,
+                    const std::vector<i64>& gRowPtr, double* gVal, double* gDiag);
 
 // Unstructured-mesh stand-in in LDU form: an nx x ny x nz hexahedral mesh
 // with node positions jittered by U(-0.2, 0.2) spacings (jitterSeed; only the

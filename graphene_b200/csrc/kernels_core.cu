@@ -393,6 +393,15 @@ void DeviceMatrix::updateValues(std::shared_ptr<HostMatrix> h) {
   if (batch || !host || H.structureKey != host->structureKey || H.n != n || H.m != m || H.P != P ||
       H.valueType != vt || !H.sumRank.empty() || !host->sumRank.empty())
     fail(GR_EINVAL, "updateValues needs a CRS matrix with this matrix's structure");
+  updateValues(H.offDiag, H.diag);
+  host = std::move(h);
+}
+
+void DeviceMatrix::updateValues(const std::vector<double>& localOff, const std::vector<double>& tileDiag) {
+  if (batch || !host || !host->sumRank.empty() || static_cast<i64>(localOff.size()) != m ||
+      static_cast<i64>(tileDiag.size()) != n)
+    fail(GR_EINVAL, "updateValues needs a CRS matrix's tile-local values and diagonal");
+  const HostMatrix& H = *host;
   ensureLocalCrs();
   if (!sellSrc.get()) {
     // The constructor's slot assignment, recording entries instead of values.
@@ -413,8 +422,8 @@ void DeviceMatrix::updateValues(std::shared_ptr<HostMatrix> h) {
     });
     sellSrc.upload(src);
   }
-  copyValuesInto(offDiag, H.offDiag, vt, stream);
-  copyValuesInto(diag, H.diag, vt, stream);
+  copyValuesInto(offDiag, localOff, vt, stream);
+  copyValuesInto(diag, tileDiag, vt, stream);
   const int blocks = static_cast<int>(std::min<i64>(numSMs * 8, (sell.slots + 255) / 256 + 1));
   if (vt == DType::F32)
     dev::sellScatterKernel<float><<<blocks, 256, 0, stream>>>(sellSrc.as<int>(), offDiag.as<float>(),
@@ -424,7 +433,6 @@ void DeviceMatrix::updateValues(std::shared_ptr<HostMatrix> h) {
                                                                sell.val.as<double>(), sell.slots);
   checkLaunch("sell_scatter");
   GR_CUDA(cudaStreamSynchronize(stream));
-  host = std::move(h);
 }
 
 // ---------------------------------------------------------------------------

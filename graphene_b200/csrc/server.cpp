@@ -53,6 +53,9 @@ struct Server::Request {
   gr_stats st{};
   int status = GR_OK, slot = -1;
   bool cacheHit = false, done = false, valuesUpdated = false;
+  // Values-only requests: H is the structure's template, these its values.
+  bool valuesOnly = false;
+  std::vector<double> gVal, gDiag;
   std::string err;
   std::shared_ptr<Entry> entry;
 };
@@ -104,7 +107,20 @@ double Server::now() const {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0_).count();
 }
 
+u64 Server::submitValues(std::shared_ptr<HostMatrix> like, const double* gVal, const double* gDiag,
+                         const std::string& json, const void* b, DType t) {
+  if (!like) fail(GR_EINVAL, "host matrix must not be NULL");
+  if (like->format != GR_FORMAT_CRS || !like->sumRank.empty())
+    fail(GR_EUNSUPPORTED, "values-only requests are for CRS matrices");
+  return enqueue(std::move(like), json, b, t, gVal, gDiag);
+}
+
 u64 Server::submit(std::shared_ptr<HostMatrix> H, const std::string& json, const void* b, DType t) {
+  return enqueue(std::move(H), json, b, t, nullptr, nullptr);
+}
+
+u64 Server::enqueue(std::shared_ptr<HostMatrix> H, const std::string& json, const void* b, DType t,
+                    const double* gVal, const double* gDiag) {
   if (!H) fail(GR_EINVAL, "host matrix must not be NULL");
   if (!b) fail(GR_EINVAL, "b must not be NULL");
   if (t != DType::F32 && t != DType::F64) fail(GR_EINVAL, "b must be float32 or float64");
@@ -117,6 +133,11 @@ u64 Server::submit(std::shared_ptr<HostMatrix> H, const std::string& json, const
   r->b.resize(bytes);
   std::memcpy(r->b.data(), b, bytes);
   r->x.assign(bytes, 0);
+  if (gVal) {
+    r->valuesOnly = true;
+    r->gVal.assign(gVal, gVal + r->H->m);
+    r->gDiag.assign(gDiag, gDiag + r->H->n);
+  }
   r->footprint = estimateFootprint(*r->H, json, t);
   {
     std::lock_guard<std::mutex> lk(mu_);
@@ -136,7 +157,7 @@ std::shared_ptr<Server::Entry> Server::findEntry(const Request& r) {
   const bool crs = r.H->format == GR_FORMAT_CRS && r.H->sumRank.empty();
   for (auto& e : resident_) {
     if (e->json != r.json) continue;
-    if (e->hid == r.H.get() || (crs && e->crs && e->key == r.H->structureKey)) return e;
+    if ((e->hid == r.H.get() && !r.valuesOnly) || (crs && e->crs && e->key == r.H->structureKey)) return e;
   }
   return nullptr;
 }
@@ -224,6 +245,14 @@ void Server::worker(int slot) {
     evicted.clear();  // outside the lock: synchronises and frees their memory
     Entry& e = *r->entry;
     try {
+      if (!e.ready && r->valuesOnly) {
+        // A new pair for a values-only request: the template's layout with
+        // the request's values.
+        auto M = HostMatrix::withGlobalValues(*r->H, r->gVal.data(), r->gDiag.data());
+        e.H = M;
+        std::lock_guard<std::mutex> lk(mu_);
+        e.hid = M.get();
+      }
       if (!e.ready) {
         e.D = std::make_unique<DeviceMatrix>(e.H);
         e.D->stream = stream;
@@ -231,7 +260,16 @@ void Server::worker(int slot) {
         e.ready = true;
       }
       e.D->stream = stream;
-      if (e.hid != r->H.get()) {
+      if (r->valuesOnly && r->cacheHit) {
+        // Values-only request on a resident structure.
+        std::vector<double> off, dg;
+        r->H->localValues(r->gVal.data(), r->gDiag.data(), off, dg);
+        e.D->updateValues(off, dg);
+        e.tree->refresh();
+        std::lock_guard<std::mutex> lk(mu_);
+        e.hid = nullptr;  // no host matrix holds these values
+        r->valuesUpdated = true;
+      } else if (e.hid != r->H.get()) {
         // Same structure, new values: upload them into the resident device
         // matrix and refactorise in place (no host layout work, no new
         // buffers, the captured iteration graphs stay valid).

@@ -45,6 +45,10 @@ class Server {
   Server& operator=(const Server&) = delete;
 
   u64 submit(std::shared_ptr<HostMatrix> H, const std::string& json, const void* b, DType t);
+  // A request for the matrix with `like`'s structure and new values (global
+  // CRS order: off-diagonals gVal, diagonal gDiag), copied.
+  u64 submitValues(std::shared_ptr<HostMatrix> like, const double* gVal, const double* gDiag, const std::string& json,
+                   const void* b, DType t);
   // GR_OK when the request finished (its own status in *status); GR_ETIMEOUT
   // when it did not finish within timeoutMs (< 0: wait forever).
   int wait(u64 id, double timeoutMs, void* x, gr_stats* stats, gr_request_times* times, int* status,
@@ -58,6 +62,8 @@ class Server {
   struct Entry;
   struct Request;
   void worker(int slot);
+  u64 enqueue(std::shared_ptr<HostMatrix> H, const std::string& json, const void* b, DType t, const double* gVal,
+              const double* gDiag);
   double now() const;
   bool admissible(const Request& r, bool* needEvict);
   std::shared_ptr<Entry> findEntry(const Request& r);

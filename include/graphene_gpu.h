@@ -165,6 +165,13 @@ int gr_host_matrix_generate_like(const gr_host_matrix* like, gr_generator kind, 
  * pattern and tile map): equal keys mean equal partition, layout and level
  * sets. No counterpart in the reference. */
 int gr_host_matrix_structure_key(const gr_host_matrix* h, uint64_t* key);
+/* The values alone: generator (kind, params, seed) on `like`'s grid, written
+ * in like's global CRS order - off-diagonals (like's num_off_diag, row by
+ * row, columns ascending) to g_val, the diagonal (num_rows) to g_diag,
+ * natural row order, FP64 before rounding. The input of
+ * gr_server_submit_values. No counterpart in the reference. */
+int gr_host_matrix_generate_values(const gr_host_matrix* like, gr_generator kind, int64_t nx, int64_t ny,
+                                   int64_t nz, const double* params, uint64_t seed, double* g_val, double* g_diag);
 
 /* Seeded vectors from the generators' counter-based stream: dist 0 =
  * uniform [lo, hi), dist 1 = standard normal. */
@@ -469,6 +476,15 @@ int gr_server_counters(gr_server* s, int64_t* queued, int64_t* running, int64_t*
  * unknown id. No counterpart in the reference (one compiled graph runs at a
  * time there). */
 int gr_server_cancel(gr_server* s, uint64_t id, int32_t* cancelled);
+/* Queues a solve of the matrix with `like`'s structure and the values g_val
+ * (like's global CRS order, off-diagonals) and g_diag (natural order),
+ * copied by the call, with the same meaning as gr_server_submit otherwise.
+ * On a resident pair of that structure the values are uploaded and the
+ * solver refactorised in place (cache_hit 2); otherwise a matrix is built
+ * from like's layout and the values. The request never needs a host matrix
+ * of its own - the form for streams of systems that share a pattern. */
+int gr_server_submit_values(gr_server* s, gr_host_matrix* like, const double* g_val, const double* g_diag,
+                            const char* json, const void* b, gr_dtype t, uint64_t* id);
 /* Finishes the running solves, drops the queued ones, releases everything. */
 void gr_server_destroy(gr_server* s);
 

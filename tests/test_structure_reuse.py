@@ -44,3 +44,25 @@ def test_generate_like_rejects_other_grids():
     ldu = gb.generateLduMesh(5, 5, 5, numTiles=2)
     with pytest.raises(gb.GrapheneError):
         gb.generateMatrixLike(ldu, gb.GEN_VAR_POISSON, 5, 5, 5, (1.0,), 2)
+
+
+@pytest.mark.parametrize("kind,params", [(gb.GEN_VAR_POISSON, (1.3,)), (gb.GEN_CONVDIFF, (0.5, 0.25, 0.125)),
+                                         (gb.GEN_POISSON, ())])
+def test_generate_values_equals_generator(kind, params):
+    """The values alone, in the template's global CRS order, are the full
+    generator's values bit for bit (FP64 template: no rounding)."""
+    dims, tiles = (13, 12, 11), 9
+    tmpl = gb.generateMatrix(gb.GEN_VAR_POISSON, *dims, (1.0,), 3, tiles, valueType=gb.FLOAT64)
+    gv, gd = gb.generateValues(tmpl, kind, *dims, params, 42)
+    full = gb.generateMatrix(kind, *dims, params, 42, tiles, valueType=gb.FLOAT64)
+    rp, col, off, dg = full.globalCrs()
+    assert np.array_equal(gv.view(np.int64), off.view(np.int64))
+    assert np.array_equal(gd.view(np.int64), dg.view(np.int64))
+
+
+def test_generate_values_checks_the_grid():
+    tmpl = gb.generateMatrix(gb.GEN_VAR_POISSON, 10, 10, 10, (1.0,), 3, 4)
+    with pytest.raises(gb.GrapheneError):
+        gb.generateValues(tmpl, gb.GEN_VAR_POISSON, 10, 10, 11, (1.0,), 1)
+    with pytest.raises(gb.GrapheneError):
+        gb.generateValues(tmpl, gb.GEN_VAR_POISSON, 20, 10, 5, (1.0,), 1)

@@ -96,3 +96,29 @@ def test_server_reuses_structure():
         st = gb.Solver(fresh.copyToTile(), cfg).solveHost(x, b)
         np.testing.assert_array_equal(res[k][0], x)
         assert res[k][1].iterations == st.iterations
+
+
+@pytest.mark.parametrize("cfg", ["ilu", "mpir"])
+def test_server_values_only_requests(cfg):
+    """gr_server_submit_values: a request carrying only new values for a
+    template's structure gives the result of the full matrix, bit for bit,
+    whether its pair is new (the first request) or resident (cache_hit 2)."""
+    c = CFGS[cfg]
+    dims, tiles = (22, 21, 20), 12
+    tmpl = gb.generateMatrix(gb.GEN_VAR_POISSON, *dims, (1.0,), 30, tiles)
+    srv = gb.Server(slots=2)
+    ids, bs = [], []
+    for k in range(5):
+        gv, gd = gb.generateValues(tmpl, gb.GEN_VAR_POISSON, *dims, (1.0,), 31 + k)
+        b = gb.randomVector(40 + k, tmpl.numRows).astype(np.float32)
+        bs.append(b)
+        ids.append(srv.submitValues(tmpl, gv, gd, c, b))
+    res = [srv.wait(i) for i in ids]
+    srv.close()
+    assert res[0][2]["cache_hit"] == 0 and all(r[2]["cache_hit"] == 2 for r in res[2:])
+    for k, b in enumerate(bs):
+        fresh = gb.generateMatrix(gb.GEN_VAR_POISSON, *dims, (1.0,), 31 + k, tiles)
+        x = np.zeros_like(b)
+        st = gb.Solver(fresh.copyToTile(), c).solveHost(x, b)
+        np.testing.assert_array_equal(res[k][0], x)
+        assert res[k][1].converged and st.converged
