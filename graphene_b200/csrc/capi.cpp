@@ -370,8 +370,8 @@ int gr_host_matrix_check_ilu_ring(const gr_host_matrix* h, int dilu, gr_dtype va
   return guarded([&] {
     need(h, "matrix");
     const gr::DType vt = gr::toDType(value_type);
-    gr::HostRing R =
-        gr::buildLevelRing(*h->m, dilu != 0, vt, ring_bytes, tiles_per_block, gr::RingBudget{}, allow_compact != 0);
+    gr::HostRing R = gr::buildLevelRing(*h->m, dilu != 0, vt, ring_bytes, tiles_per_block, gr::RingBudget{},
+                                        allow_compact != 0, gr::RingKind::Ilu, allow_compact == 2);
     gr::checkLevelRing(*h->m, R, dilu != 0, vt);
     if (ring_bytes_used) *ring_bytes_used = R.ringBytes;
     if (stream_bytes) *stream_bytes = static_cast<int64_t>(R.bytes.size());
@@ -386,7 +386,8 @@ int gr_host_matrix_check_gs_ring(const gr_host_matrix* h, int lower_only, gr_dty
     need(h, "matrix");
     const gr::DType vt = gr::toDType(value_type);
     gr::HostRing R = gr::buildLevelRing(*h->m, false, vt, ring_bytes, 1, gr::RingBudget{}, allow_compact != 0,
-                                        lower_only ? gr::RingKind::GaussSeidelLower : gr::RingKind::GaussSeidel);
+                                        lower_only ? gr::RingKind::GaussSeidelLower : gr::RingKind::GaussSeidel,
+                                        allow_compact == 2);
     gr::checkLevelRing(*h->m, R, false, vt);
     if (ring_bytes_used) *ring_bytes_used = R.ringBytes;
     if (stream_bytes) *stream_bytes = static_cast<int64_t>(R.bytes.size());

@@ -251,8 +251,9 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
   } else if (ty == "ILU") {
     mark("solveMulticolor"); mark("factorizeMulticolor"); mark("diagonalBased"); mark("kernel");
     mark("ringLog2"); mark("prefetch"); mark("unroll"); mark("ringBytes"); mark("l2Ahead"); mark("tilesPerBlock");
-    mark("compactRing");
+    mark("compactRing"); mark("recordLevels");
     readBool(j, "compactRing", c->compactRing);
+    readBool(j, "recordLevels", c->ringRecords);
     readInt(j, "tilesPerBlock", c->tilesPerBlock);
     if (c->tilesPerBlock < 0 || c->tilesPerBlock > 64) fail(GR_EINVAL, "tilesPerBlock must be 0 (default) or 1..64");
     readInt(j, "l2Ahead", c->l2Ahead);
@@ -284,7 +285,8 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
     }
   } else if (ty == "GaussSeidel") {
     mark("numSweeps"); mark("numFixedIterations"); mark("solveMulticolor"); mark("workingType");
-    mark("seed"); mark("kernel");
+    mark("seed"); mark("kernel"); mark("recordLevels");
+    readBool(j, "recordLevels", c->ringRecords);
     if (const Json* v = j.find("kernel")) {
       if (v->text == "auto") c->gsKernel = 0;
       else if (v->text == "ring") c->gsKernel = 1;

@@ -59,6 +59,9 @@ struct SolverConfig {
   // B200 at 192^3 with 2048 tiles it ran in 111.0 us against 116.8 for the
   // 32-bit layout.
   bool compactRing = true;
+  // Level rings: 16-byte row records for the levels of 3 entries a row
+  // (ILU and Gauss-Seidel "recordLevels").
+  bool ringRecords = false;
   // Extension: log2 of the streamed kernel's ring size in bytes (0: the
   // smallest ring that holds the largest level).
   int ringLog2 = 0;

@@ -170,8 +170,9 @@ void checkIluStream(const HostMatrix& H, const HostStream& S, bool dilu, DType v
 constexpr int kRingBarriers = 16;
 constexpr int kRingUpperBit = 1 << 30;
 // Field packing of a level's int4: y = E | (entries offset / 16) << 14 |
-// upper << 30, z = ring offset | (block bytes / 16) << 18.
+// upper << 30 | record << 31, z = ring offset | (block bytes / 16) << 18.
 constexpr int kRingEBits = 14, kRingOffBits = 18;
+constexpr uint32_t kRingRecordBit = 1u << 31;
 struct RingLevelCode {
   __host__ __device__ static int k(const int4 m) { return m.x; }
   __host__ __device__ static int E(const int4 m) { return m.y & ((1 << kRingEBits) - 1); }
@@ -179,6 +180,7 @@ struct RingLevelCode {
     return ((static_cast<uint32_t>(m.y) >> kRingEBits) & 0xFFFFu) << 4;
   }
   __host__ __device__ static bool upper(const int4 m) { return (m.y & kRingUpperBit) != 0; }
+  __host__ __device__ static bool record(const int4 m) { return (static_cast<uint32_t>(m.y) & kRingRecordBit) != 0; }
   __host__ __device__ static uint32_t ringOffset(const int4 m) {
     return static_cast<uint32_t>(m.z) & ((1u << kRingOffBits) - 1);
   }
@@ -189,11 +191,25 @@ constexpr long long kRingCompactRows = 65535;  // largest block (rows + zero slo
 
 // Byte offsets of a level block's inverse diagonal, entries (columns, or
 // column/value pairs) and values, and its size.
+//
+// Record levels (compact layout, float values, exactly 3 entries a row, as
+// a 7-point stencil's lower or upper part has): a row is one 16-byte record
+// {v0, v1, v2, c0 | c1 << 16} at 16 q, then, after all of them, a 4-byte
+// word {c2 | row << 16} at ents + 4 q, or with an inverse diagonal an 8-byte
+// pair {c2 | row << 16, inv} at ents + 8 q. Two shared-memory loads a row
+// instead of seven, at the bytes of the column-major compact layout.
+__host__ __device__ inline bool ringRecordLevel(uint32_t E, uint32_t valueBytes, bool compact) {
+  return compact && valueBytes == 4 && E == 3;
+}
 struct RingLevelLayout {
   uint32_t inv, ents, vals, bytes;
 };
 __host__ __device__ inline RingLevelLayout ringLevelLayout(uint32_t k, uint32_t E, bool hasInv, uint32_t valueBytes,
-                                                           bool compact) {
+                                                           bool compact, bool record = false) {
+  if (record) {
+    const uint32_t recB = ((hasInv ? 8u : 4u) * k + 15u) & ~15u;
+    return RingLevelLayout{16u * k, 16u * k, 0u, 16u * k + recB};
+  }
   const uint32_t idB = compact ? 2u : 4u;
   const uint32_t rowsB = (idB * k + 15u) & ~15u;
   const uint32_t invB = hasInv ? ((valueBytes * k + 15u) & ~15u) : 0u;
@@ -266,9 +282,10 @@ inline i64 ringFixedSmem(i32 maxTileLevels, i64 maxGroupRows, i64 vectorBytes) {
 // tileLevel and meta are then per block). ringBytes 0: the default (RingBudget).
 // The compact layout is used when every block has at most kRingCompactRows
 // rows and `allowCompact`.
+// records: use record levels where they apply (ringRecordLevel).
 HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes, i32 group,
                         const RingBudget& budget = RingBudget{}, bool allowCompact = true,
-                        RingKind kind = RingKind::Ilu);
+                        RingKind kind = RingKind::Ilu, bool records = false);
 // Replays the kernel's copies and reads on the host; throws GR_EINVAL on an
 // out-of-range index, a dependency-order violation, a copy that would
 // overwrite a level not yet consumed, or a copy issued too late.
@@ -343,10 +360,10 @@ struct DeviceMatrix {
   std::unique_ptr<LevelSchedule> lowerSched, upperSched, gsSched;
   std::unique_ptr<SweepStream> iluStream[2];  // [dilu]
   SweepStream& iluSweepStream(bool dilu);
-  std::map<std::tuple<bool, i64, i32, bool, int>, std::unique_ptr<LevelRing>>
-      levelRings;  // [(dilu, ring bytes, group, compact allowed, kind)]
+  std::map<std::tuple<bool, i64, i32, bool, int, bool>, std::unique_ptr<LevelRing>>
+      levelRings;  // [(dilu, ring bytes, group, compact allowed, kind, record levels)]
   LevelRing& levelRing(bool dilu, i64 ringBytes, i32 group, bool allowCompact = true,
-                       RingKind kind = RingKind::Ilu);
+                       RingKind kind = RingKind::Ilu, bool records = false);
 
   // Device error word written by kernels whose bounded waits ran out
   // (GR_ETIMEOUT); 0 when clean.

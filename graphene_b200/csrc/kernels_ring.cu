@@ -68,7 +68,7 @@ __device__ __forceinline__ void loadEntry<double>(const unsigned char* p, int& c
 template <class MV, bool COMPACT>
 struct RingLevel {
   int k, E;
-  bool upper;
+  bool upper, rec;
   const unsigned char* blk;  // the level block in the ring
   uint32_t inv, ents, vals;  // offsets of its inverse diagonal, entries (columns) and values
   __device__ __forceinline__ int row(int q) const {
@@ -94,12 +94,52 @@ __device__ __forceinline__ RingLevel<MV, COMPACT> ringLevelAt(const int4 m, cons
   lv.k = RingLevelCode::k(m);
   lv.E = RingLevelCode::E(m);
   lv.upper = RingLevelCode::upper(m);
+  lv.rec = COMPACT && sizeof(MV) == 4 && RingLevelCode::record(m);
   lv.blk = ring + RingLevelCode::ringOffset(m);
   lv.inv = ((COMPACT ? 2u : 4u) * static_cast<uint32_t>(lv.k) + 15u) & ~15u;
   lv.ents = RingLevelCode::ents(m);
   lv.vals = COMPACT ? lv.ents + ((2u * static_cast<uint32_t>(lv.E) * static_cast<uint32_t>(lv.k) + 15u) & ~15u)
                     : lv.ents;
   return lv;
+}
+
+// Row q of a record level (float values, 3 entries): one 16-byte load
+// {v0, v1, v2, c0 | c1 << 16} and one 4- or 8-byte load {c2 | row << 16,
+// inverse diagonal}.
+struct RowRecord {
+  int row, c[3];
+  float v[3], inv;
+};
+template <class MV, bool COMPACT>
+__device__ __forceinline__ RowRecord ringRecord(const RingLevel<MV, COMPACT>& lv, int q, bool hasInv) {
+  RowRecord r;
+  const float4 a = reinterpret_cast<const float4*>(lv.blk)[q];
+  uint32_t w2;
+  if (hasInv) {
+    const uint2 b = reinterpret_cast<const uint2*>(lv.blk + lv.ents)[q];
+    w2 = b.x;
+    r.inv = __uint_as_float(b.y);
+  } else {
+    w2 = reinterpret_cast<const uint32_t*>(lv.blk + lv.ents)[q];
+    r.inv = 0.0f;
+  }
+  const uint32_t w01 = __float_as_uint(a.w);
+  r.c[0] = static_cast<int>(w01 & 0xFFFFu);
+  r.c[1] = static_cast<int>(w01 >> 16);
+  r.c[2] = static_cast<int>(w2 & 0xFFFFu);
+  r.row = static_cast<int>(w2 >> 16);
+  r.v[0] = a.x;
+  r.v[1] = a.y;
+  r.v[2] = a.z;
+  return r;
+}
+// temp -= v0 x[c0], v1 x[c1], v2 x[c2], in order (x loads first).
+template <class W>
+__device__ __forceinline__ W recordDot(W temp, const RowRecord& r, const W* xs) {
+  const W x0 = xs[r.c[0]], x1 = xs[r.c[1]], x2 = xs[r.c[2]];
+  temp = sub(temp, mul(cvt<W>(r.v[0]), x0));
+  temp = sub(temp, mul(cvt<W>(r.v[1]), x1));
+  return sub(temp, mul(cvt<W>(r.v[2]), x2));
 }
 
 // temp -= sum_e value_e * xs[column_e] over row q's E entries in order.
@@ -265,7 +305,22 @@ __global__ void __launch_bounds__(RingShape<W>::threads) iluRingKernel(const uns
     for (int l = 0; !stop && l < L; ++l) {
       const int4 m = mt[l];
       const RingLevel<MV, COMPACT> cur = ringLevelAt<MV, COMPACT>(m, ring);
-      if (!cur.upper) {
+      if (cur.rec) {
+        // Record level (7-point lower or upper part): the same operations
+        // as below, from two loads a row.
+        const bool hasInv = cur.upper || dilu;
+        for (int q = threadIdx.x; q < cur.k; q += kRingCompute) {
+          const RowRecord r = ringRecord(cur, q, hasInv);
+          if (!cur.upper) {
+            const W temp = recordDot(xs[r.row], r, xs);
+            xs[r.row] = dilu ? mul(temp, cvt<W>(r.inv)) : temp;
+          } else {
+            const W temp = recordDot(W(0), r, xs);
+            const W iv = cvt<W>(r.inv);
+            xs[r.row] = dilu ? add(xs[r.row], mul(temp, iv)) : mul(add(xs[r.row], temp), iv);
+          }
+        }
+      } else if (!cur.upper) {
         // Forward substitution (ilu/Solver.cpp:380-411).
         for (int q = threadIdx.x; q < cur.k; q += kRingCompute) {
           const int il = cur.row(q);
@@ -433,6 +488,16 @@ __global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
     bool stop = namedBarOr(1, kRingLevelSync, false);
     for (int l = 0; !stop && l < L; ++l) {
       const RingLevel<MV, COMPACT> cur = ringLevelAt<MV, COMPACT>(mt[l], ring);
+      if (cur.rec) {
+        for (int q = threadIdx.x; q < cur.k; q += kRingCompute) {
+          const RowRecord r = ringRecord(cur, q, true);
+          const W d = cvt<W>(r.inv);
+          const W sum = recordDot(seedB ? rhs[r.row] : d, r, xs);
+          xs[r.row] = storeRound<X>(dvd(sum, d));
+        }
+        stop = namedBarOr(1, kRingLevelSync, *abortV != 0);
+        continue;
+      }
       for (int q = threadIdx.x; q < cur.k; q += kRingCompute) {
         const int il = cur.row(q);
         const W d = cvt<W>(cur.invDiag(q));

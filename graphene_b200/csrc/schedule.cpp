@@ -395,7 +395,7 @@ inline bool overlaps(i64 a, i64 sa, i64 b, i64 sb) { return a < b + sb && b < a 
 }  // namespace
 
 HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes, i32 group,
-                        const RingBudget& budget, bool allowCompact, RingKind kind) {
+                        const RingBudget& budget, bool allowCompact, RingKind kind, bool records) {
   const i64 vs = static_cast<i64>(dtypeSize(vt));
   const i64 entSize = vs == 4 ? 8 : 16;
   const bool gs = kind != RingKind::Ilu;
@@ -461,11 +461,44 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
         }
         if (E >= (i64(1) << kRingEBits) || k >= (i64(1) << 31) || entSize * E * k >= (i64(1) << 31))
           fail(GR_EUNSUPPORTED, "ILU level too large for the ring kernel");
+        const bool rec = records && ringRecordLevel(static_cast<uint32_t>(E), static_cast<uint32_t>(vs), compact);
         const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(k), static_cast<uint32_t>(E), hasInv,
-                                                    static_cast<uint32_t>(vs), compact);
+                                                    static_cast<uint32_t>(vs), compact, rec);
         const i64 S = lay.bytes;
         const i64 start = static_cast<i64>(t.bytes.size());
         t.bytes.resize(start + S, 0);
+        if (rec) {
+          // Record level: {v0, v1, v2, c0 | c1 << 16} per row, then
+          // {c2 | row << 16} (and the inverse diagonal) per row.
+          const i64 recB = hasInv ? 8 : 4;
+          for (i64 q = 0; q < k; ++q) {
+            const auto [gl, T] = rows[q];
+            const i64 tb = H.tileStart[T] - gBase;
+            rowEntries(H, ekind, gBase + gl, gl - tb, H.tileStart[T + 1] - H.tileStart[T], ent);
+            uint32_t c[3];
+            for (int e = 0; e < 3; ++e) {
+              const bool real = e < static_cast<int>(ent.size());
+              i64 col = zeroSlot;
+              if (real) {
+                const i64 lc = H.colLocal[ent[e]];
+                col = gs ? (lc < gl ? lc : gRows + lc) : lc + tb;
+                t.vals.emplace_back(start + 16 * q + 4 * e, static_cast<i32>(ent[e]));
+              }
+              c[e] = static_cast<uint32_t>(col);
+            }
+            const uint32_t w01 = c[0] | (c[1] << 16), w2 = c[2] | (static_cast<uint32_t>(gl) << 16);
+            std::memcpy(t.bytes.data() + start + 16 * q + 12, &w01, 4);
+            std::memcpy(t.bytes.data() + start + lay.ents + recB * q, &w2, 4);
+            if (hasInv) t.invs.emplace_back(start + lay.ents + recB * q + 4, static_cast<i32>(gBase + gl));
+          }
+          t.meta.push_back(make_int4(static_cast<int>(k), static_cast<int>(static_cast<uint32_t>(E) |
+                                                                              (upper ? kRingUpperBit : 0u) |
+                                                                              kRingRecordBit),
+                                     0, -1));
+          t.size.push_back(S);
+          t.maxLevel = std::max(t.maxLevel, S);
+          continue;
+        }
         for (i64 q = 0; q < k; ++q) {
           const auto [gl, T] = rows[q];
           const i64 tb = H.tileStart[T] - gBase;
@@ -642,10 +675,12 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
     for (size_t l = 0; l < tr[T].meta.size(); ++l) {
       int4 m = tr[T].meta[l];
       const bool upper = (m.y & kRingUpperBit) != 0;
-      const uint32_t E = static_cast<uint32_t>(m.y & (kRingUpperBit - 1));
+      const bool rec = (static_cast<uint32_t>(m.y) & kRingRecordBit) != 0;
+      const uint32_t E = static_cast<uint32_t>(m.y) & ((1u << kRingEBits) - 1);
       const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(m.x), E, gs || upper || dilu,
-                                                  static_cast<uint32_t>(vs), compact);
-      m.y = static_cast<int>(E | ((lay.ents >> 4) << kRingEBits) | (upper ? static_cast<uint32_t>(kRingUpperBit) : 0u));
+                                                  static_cast<uint32_t>(vs), compact, rec);
+      m.y = static_cast<int>(E | ((lay.ents >> 4) << kRingEBits) | (upper ? static_cast<uint32_t>(kRingUpperBit) : 0u) |
+                             (rec ? kRingRecordBit : 0u));
       m.z = static_cast<int>(static_cast<uint32_t>(m.z) | ((lay.bytes >> 4) << kRingOffBits));
       R.meta[static_cast<size_t>(R.tileLevel[T]) + l] = m;
     }
@@ -708,18 +743,23 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
       const bool upper = RingLevelCode::upper(a);
       if (upper != (l >= nLower)) bad(G, l, "sweep flag");
       const bool hasInv = gs || upper || dilu;
+      const bool rec = RingLevelCode::record(a);
+      if (rec && !ringRecordLevel(static_cast<uint32_t>(E), static_cast<uint32_t>(vs), R.compact))
+        bad(G, l, "record level");
       const i64 idB = R.compact ? 2 : 4;
       const i64 rowsB = pad16(idB * k), invB = hasInv ? pad16(vs * k) : 0;
       const i64 colsB = R.compact ? pad16(2 * E * k) : pad16(entSize * E * k);
       const i64 valsB = R.compact ? pad16(vs * E * k) : 0;
-      const i64 S = rowsB + invB + colsB + valsB;
+      const i64 recWord = hasInv ? 8 : 4;
+      const i64 S = rec ? 16 * k + pad16(recWord * k) : rowsB + invB + colsB + valsB;
       if (k < 1 || E < 0 || S > R.ringBytes) bad(G, l, "block layout");
       const RingLevelLayout lay = ringLevelLayout(static_cast<uint32_t>(k), static_cast<uint32_t>(E), hasInv,
-                                                  static_cast<uint32_t>(vs), R.compact);
-      if (lay.inv != rowsB || lay.ents != rowsB + invB || lay.bytes != S ||
-          lay.vals != (R.compact ? rowsB + invB + colsB : rowsB + invB) || RingLevelCode::ents(a) != lay.ents ||
-          RingLevelCode::bytes(a) != lay.bytes)
+                                                  static_cast<uint32_t>(vs), R.compact, rec);
+      if (rec ? (lay.ents != 16 * k || lay.bytes != S)
+              : (lay.inv != rowsB || lay.ents != rowsB + invB || lay.bytes != S ||
+                 lay.vals != (R.compact ? rowsB + invB + colsB : rowsB + invB)))
         bad(G, l, "block layout");
+      if (RingLevelCode::ents(a) != lay.ents || RingLevelCode::bytes(a) != lay.bytes) bad(G, l, "block layout");
       const i64 entOff = rowsB + invB;
       if (off < 0 || off % 16 != 0 || off + S > R.ringBytes) bad(G, l, "ring offset");
       if (ia < -1 || ia < prevIa || ia < l - kRingBarriers || (l >= 1 && ia > l - 2) || (l == 0 && ia != -1))
@@ -735,7 +775,12 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
       std::vector<i64> rows(k);
       for (i64 q = 0; q < k; ++q) {
         i32 il;
-        if (R.compact) {
+        uint32_t recW01 = 0, recW2 = 0;
+        if (rec) {
+          std::memcpy(&recW01, blk + 16 * q + 12, 4);
+          std::memcpy(&recW2, blk + lay.ents + recWord * q, 4);
+          il = static_cast<i32>(recW2 >> 16);
+        } else if (R.compact) {
           uint16_t r16;
           std::memcpy(&r16, blk + 2 * q, 2);
           il = r16;
@@ -746,7 +791,9 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
         rows[q] = il;
         for (i64 e = 0; e < E; ++e) {
           i32 c;
-          if (R.compact) {
+          if (rec) {
+            c = static_cast<i32>(e == 0 ? (recW01 & 0xFFFFu) : e == 1 ? (recW01 >> 16) : (recW2 & 0xFFFFu));
+          } else if (R.compact) {
             uint16_t c16;
             std::memcpy(&c16, blk + entOff + 2 * (e * k + q), 2);
             c = c16;
@@ -778,8 +825,9 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
   }
 }
 
-LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group, bool allowCompact, RingKind kind) {
-  auto key = std::make_tuple(dilu, ringBytes, group, allowCompact, static_cast<int>(kind));
+LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group, bool allowCompact, RingKind kind,
+                                   bool records) {
+  auto key = std::make_tuple(dilu, ringBytes, group, allowCompact, static_cast<int>(kind), records);
   auto it = levelRings.find(key);
   if (it != levelRings.end()) return *it->second;
   RingBudget budget;
@@ -791,7 +839,7 @@ LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group, bool all
   if (cudaDeviceGetAttribute(&v, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess)
     budget.reservedPerBlock = v;
   if (const int b = ringBlocksPerSMWithoutSmem(vt, kind); b > 0) budget.maxBlocksPerSM = b;
-  HostRing H = buildLevelRing(*host, dilu, vt, ringBytes, group, budget, allowCompact, kind);
+  HostRing H = buildLevelRing(*host, dilu, vt, ringBytes, group, budget, allowCompact, kind, records);
   auto R = std::make_unique<LevelRing>();
   R->dilu = dilu;
   R->bytes = static_cast<i64>(H.bytes.size());

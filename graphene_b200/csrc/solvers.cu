@@ -77,7 +77,8 @@ class IluNode : public Node {
     if (c.iluKernel == 0 || c.iluKernel == 4) {
       LevelRing* R = nullptr;
       try {
-        R = &A.levelRing(dilu_, c.ringBytes, c.tilesPerBlock > 0 ? c.tilesPerBlock : 1, c.compactRing);
+        R = &A.levelRing(dilu_, c.ringBytes, c.tilesPerBlock > 0 ? c.tilesPerBlock : 1, c.compactRing,
+                         RingKind::Ilu, c.ringRecords);
       } catch (const Error&) {
         if (c.iluKernel == 4) throw;  // the requested ring cannot hold the levels
       }
@@ -183,8 +184,8 @@ class GsNode : public Node {
     // entries only for sweeps that start from x = 0.
     if (c.gsKernel != 2) {
       try {
-        ring_ = &A.levelRing(false, 0, 1, true, RingKind::GaussSeidel);
-        ringLo_ = &A.levelRing(false, 0, 1, true, RingKind::GaussSeidelLower);
+        ring_ = &A.levelRing(false, 0, 1, true, RingKind::GaussSeidel, c.ringRecords);
+        ringLo_ = &A.levelRing(false, 0, 1, true, RingKind::GaussSeidelLower, c.ringRecords);
       } catch (const Error&) {
         if (c.gsKernel == 1) throw;
         ring_ = ringLo_ = nullptr;

@@ -266,8 +266,9 @@ int gr_host_matrix_check_ilu_stream(const gr_host_matrix* h, int dilu, gr_dtype 
 
 /* Builds the level blocks and copy schedule of the host-scheduled ring
  * substitution kernel for a ring of ring_bytes (0: the default) with
- * tiles_per_block consecutive tiles per thread block (allow_compact: 16-bit
- * row and column ids where the blocks are small enough), and replays
+ * tiles_per_block consecutive tiles per thread block (allow_compact: 1,
+ * 16-bit row and column ids where the blocks are small enough; 2, the same
+ * with 16-byte row records for levels of 3 entries a row), and replays
  * the kernel's copies and reads on the host, checking every index, the
  * dependency order of the levels, that no copy overwrites a level still to
  * be consumed and that every copy is issued before its level is needed.

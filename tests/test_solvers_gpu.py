@@ -53,17 +53,20 @@ NAMES = ["poisson16", "poisson_odd_bfs", "poisson_1tile", "random", "many_tiles"
 
 
 def ilu_config(kernel, **kw):
-    """'ring_wide': the ring kernel with 32-bit row and column ids."""
-    c = {"type": "ILU", "kernel": "ring" if kernel == "ring_wide" else kernel}
+    """'ring_wide': the ring kernel with 32-bit row and column ids;
+    'ring_rec': with 16-byte row records for levels of 3 entries a row."""
+    c = {"type": "ILU", "kernel": "ring" if kernel in ("ring_wide", "ring_rec") else kernel}
     if kernel == "ring_wide":
         c["compactRing"] = False
+    if kernel == "ring_rec":
+        c["recordLevels"] = True
     c.update(kw)
     return c
 
 
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("dilu", [False, True])
-@pytest.mark.parametrize("kernel", ["ring", "ring_wide", "warp", "tma", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "ring_wide", "warp", "tma", "levels"])
 def test_ilu_bit_exact(oracle, name, dilu, kernel):
     h, om = case(name, oracle)
     A = h.copyToTile()
@@ -75,7 +78,7 @@ def test_ilu_bit_exact(oracle, name, dilu, kernel):
 
 
 @pytest.mark.parametrize("name", ["poisson16", "random"])
-@pytest.mark.parametrize("kernel", ["ring", "ring_wide", "warp", "tma", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "ring_wide", "warp", "tma", "levels"])
 def test_ilu_bit_exact_float64(oracle, name, kernel):
     h, om = case(name, oracle, gb.FLOAT64)
     A = h.copyToTile()
@@ -126,7 +129,7 @@ def test_ilu_ring_small_rings_bit_exact(oracle, name, frac):
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("sweeps", [1, 2, 3])
 @pytest.mark.parametrize("seed", ["b", "diag"])
-@pytest.mark.parametrize("kernel", ["ring", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "levels"])
 def test_gauss_seidel_bit_exact(oracle, name, sweeps, seed, kernel):
     h, om = case(name, oracle)
     A = h.copyToTile()
@@ -134,8 +137,9 @@ def test_gauss_seidel_bit_exact(oracle, name, sweeps, seed, kernel):
     b = rng.uniform(-1, 1, h.numRows).astype(np.float32)
     x0 = rng.uniform(-1, 1, h.numRows).astype(np.float32)
     x = dev(x0)
-    gb.Solver(A, {"type": "GaussSeidel", "numFixedIterations": sweeps, "seed": seed, "kernel": kernel}).solve(
-        x, dev(b))
+    cfg = {"type": "GaussSeidel", "numFixedIterations": sweeps, "seed": seed,
+           "kernel": "ring" if kernel == "ring_rec" else kernel, "recordLevels": kernel == "ring_rec"}
+    gb.Solver(A, cfg).solve(x, dev(b))
     ref = x0
     for _ in range(sweeps):
         ref = om.gs_sweep(ref, b, seed_b=(seed == "b"))
@@ -162,14 +166,15 @@ def test_gauss_seidel_ring_types_bit_exact(oracle, name, vt):
 
 @pytest.mark.parametrize("name", ["poisson16", "random", "many_tiles", "poisson_odd_bfs"])
 @pytest.mark.parametrize("sweeps", [1, 2, 3])
-def test_gauss_seidel_ring_from_zero_bit_exact(oracle, name, sweeps):
+@pytest.mark.parametrize("records", [False, True])
+def test_gauss_seidel_ring_from_zero_bit_exact(oracle, name, sweeps, records):
     """Sweeps from x = 0 (the first one through the lower-only ring), as a
     PBiCGStab preconditioner applies them: same bits as the oracle's full
     sweeps from zero."""
     h, om = case(name, oracle)
     A = h.copyToTile()
     b = np.random.default_rng(10).uniform(-1, 1, h.numRows).astype(np.float32)
-    cfg = {"type": "GaussSeidel", "numFixedIterations": sweeps, "kernel": "ring"}
+    cfg = {"type": "GaussSeidel", "numFixedIterations": sweeps, "kernel": "ring", "recordLevels": records}
     x = dev(np.zeros_like(b))
     gb.Solver(A, cfg).solve(x, dev(b))
     ref = np.zeros_like(b)

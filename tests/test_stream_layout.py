@@ -71,7 +71,7 @@ def check_ring(h, dilu, vt=gb.FLOAT32, ring_bytes=0, group=1, compact=True):
 @pytest.mark.parametrize("dilu", [False, True])
 @pytest.mark.parametrize("vt", [gb.FLOAT32, gb.FLOAT64])
 @pytest.mark.parametrize("group", [1, 3])
-@pytest.mark.parametrize("compact", [True, False])
+@pytest.mark.parametrize("compact", [True, False, 2])
 def test_ring_replay(dims, tiles, part, dilu, vt, group, compact):
     h = gb.generate3DPoissonMatrix(vt, *dims, tiles, part)
     used, nbytes, lv = check_ring(h, dilu, vt, 0, group, compact)
@@ -139,7 +139,7 @@ def check_gs_ring(h, lower_only, vt=gb.FLOAT32, ring_bytes=0, compact=True):
 ])
 @pytest.mark.parametrize("lower_only", [False, True])
 @pytest.mark.parametrize("vt", [gb.FLOAT32, gb.FLOAT64])
-@pytest.mark.parametrize("compact", [True, False])
+@pytest.mark.parametrize("compact", [True, False, 2])
 def test_gs_ring_replay(dims, tiles, part, lower_only, vt, compact):
     h = gb.generate3DPoissonMatrix(vt, *dims, tiles, part)
     used, nbytes, lv = check_gs_ring(h, lower_only, vt, 0, compact)
@@ -175,3 +175,13 @@ def test_gs_ring_replay_convdiff_workload():
     for lower_only in (False, True):
         used, nbytes, lv = check_gs_ring(h, lower_only)
         assert used >= 4096 and lv < 64
+
+
+def test_ring_record_levels_same_bytes():
+    """Row records (levels of 3 entries a row): 16 + 4 bytes a row without an
+    inverse diagonal, 16 + 8 with one - the column-major compact layout's
+    bytes (2 + 3 x 2 + 3 x 4, plus 4), up to 16-byte padding."""
+    h = gb.generate3DPoissonMatrix(gb.FLOAT32, 24, 24, 24, 8, gb.PART_RCB)
+    _, compact, _ = check_ring(h, False, gb.FLOAT32, 0, 1, True)
+    _, record, _ = check_ring(h, False, gb.FLOAT32, 0, 1, 2)
+    assert abs(record - compact) <= 0.02 * compact
