@@ -22,7 +22,13 @@
 // another call still running on the GPU) share the scratch and race; the
 // caller serialises them. The first call on each device performs the set-up
 // (symbol lookup, which may load the module, and the counter clear); make it
-// before any stream capture.
+// before any stream capture. Every call looks the symbol up again and
+// repeats the set-up if its address changed (the device was reset and the
+// module reloaded), so a reset needs no restart of the process.
+//
+// Every vector read (x .. x + ((count - 1) * ld + n) elements) and the count
+// results written must lie inside one device allocation each, as the driver
+// reports it; otherwise the call returns GR_EINVAL before anything runs.
 #include <algorithm>
 #include <climits>
 #include <mutex>
@@ -46,8 +52,9 @@ struct NoAllocScratch {
 static __device__ __align__(256) NoAllocScratch g_naScratch;
 
 // Block y reduces vector y (x + y * ld) exactly as normKernel reduces one
-// vector: grid-stride partials, block reduction, last-block combination of
-// the block partials in block order.
+// vector: grid-stride partials, block reduction, and the last block's
+// combination of the block partials in the same deterministic order as
+// normKernel's gridReduce.
 template <class T>
 __global__ void __launch_bounds__(256) normsNoAllocKernel(const T* __restrict__ x, int n, long long ld,
                                                            int kind, double* __restrict__ out,
@@ -74,7 +81,7 @@ namespace {
 constexpr int kNaMaxDevices = 64;
 
 struct NaDevice {
-  dev::NoAllocScratch* scratch = nullptr;
+  dev::NoAllocScratch* scratch = nullptr;  // the address the set-up was done for
   int blocks = 0;  // reduction blocks: min(8 per SM, kNaBlocks)
 };
 
@@ -90,10 +97,10 @@ const NaDevice& naDevice() {
   if (d < 0 || d >= kNaMaxDevices) fail(GR_EUNSUPPORTED, "device index beyond the no-allocation table");
   std::lock_guard<std::mutex> lock(g_naMutex);
   NaDevice& nd = g_naDevices[d];
-  if (nd.scratch) return nd;
   void* p = nullptr;
   e = cudaGetSymbolAddress(&p, dev::g_naScratch);
   if (e != cudaSuccess) fail(GR_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  if (nd.scratch == p) return nd;
   int sms = 0;
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d);
   if (e != cudaSuccess) fail(GR_ECUDA, std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e));
@@ -121,6 +128,37 @@ void needDevicePointer(const void* p, size_t align, const char* what) {
   if (reinterpret_cast<uintptr_t>(p) % align != 0) fail(GR_EINVAL, std::string(what) + " is misaligned");
 }
 
+// The driver's allocation range query, found through the runtime (no link
+// against the driver library): CUresult cuMemGetAddressRange(CUdeviceptr*
+// base, size_t* size, CUdeviceptr ptr).
+using MemRangeFn = int (*)(unsigned long long*, size_t*, unsigned long long);
+MemRangeFn memRangeFn() {
+  static MemRangeFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return static_cast<MemRangeFn>(nullptr);
+    }
+    return reinterpret_cast<MemRangeFn>(f);
+  }();
+  return fn;
+}
+
+// [p, p + bytes) must lie inside the device allocation that holds p.
+void needRange(const void* p, size_t bytes, const char* what) {
+  MemRangeFn fn = memRangeFn();
+  if (!fn) fail(GR_EUNSUPPORTED, "the driver's allocation range query is unavailable");
+  unsigned long long base = 0;
+  size_t size = 0;
+  const unsigned long long a = reinterpret_cast<unsigned long long>(p);
+  if (fn(&base, &size, a) != 0)
+    fail(GR_EINVAL, std::string(what) + " is not inside a device allocation the driver reports");
+  if (a < base || bytes > size || a - base > size - bytes)
+    fail(GR_EINVAL, std::string(what) + " extends past the end of its device allocation");
+}
+
 }  // namespace
 
 void launchNormsNoAlloc(const void* x, i64 n, i64 count, i64 ld, DType t, int normKind, double* out,
@@ -133,6 +171,8 @@ void launchNormsNoAlloc(const void* x, i64 n, i64 count, i64 ld, DType t, int no
   if (t == DType::DW) fail(GR_EUNSUPPORTED, "norm of a twofloat32 vector");
   needDevicePointer(x, dtypeSize(t), "x");
   needDevicePointer(out, sizeof(double), "out");
+  needRange(x, static_cast<size_t>((count - 1) * ld + n) * dtypeSize(t), "x (count vectors of n at stride ld)");
+  needRange(out, static_cast<size_t>(count) * sizeof(double), "out (count results)");
   const NaDevice& nd = naDevice();
   const int blocks = std::max(1, std::min(nd.blocks, static_cast<int>((n + 255) / 256)));
   const dim3 grid(blocks, static_cast<unsigned>(count));
