@@ -321,8 +321,9 @@ int gr_spmv(gr_matrix* A, const void* x, void* y, gr_dtype t);
 /* SpMV autotuner (no counterpart in the reference): times the candidate
  * launch geometries of gr_spmv for vectors of type t (threads per block 128 /
  * 256 / 512, SELL chunks per warp, entry loads batched 4 / 8 / 16; every
- * candidate reps times on the matrix's stream) and keeps the fastest for
- * later gr_spmv calls on this matrix. Every geometry computes each row in the
+ * candidate reps times on the matrix's stream, each launch timed alone with
+ * L2 flushed first, as a solve meets a matrix larger than L2) and keeps the
+ * fastest for later gr_spmv calls on this matrix. Every geometry computes each row in the
  * same order, so results do not change. Writes the choice and its mean time
  * (ms); chunks_per_warp 0 is the untuned grid. */
 int gr_matrix_tune_spmv(gr_matrix* A, gr_dtype t, int32_t reps, int32_t* block, int32_t* chunks_per_warp,
