@@ -251,8 +251,9 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
   } else if (ty == "ILU") {
     mark("solveMulticolor"); mark("factorizeMulticolor"); mark("diagonalBased"); mark("kernel");
     mark("ringLog2"); mark("prefetch"); mark("unroll"); mark("ringBytes"); mark("l2Ahead"); mark("tilesPerBlock");
-    mark("compactRing"); mark("recordLevels");
+    mark("compactRing"); mark("recordLevels"); mark("pairRows");
     readBool(j, "compactRing", c->compactRing);
+    readBool(j, "pairRows", c->pairRows);
     readBool(j, "recordLevels", c->ringRecords);
     readInt(j, "tilesPerBlock", c->tilesPerBlock);
     if (c->tilesPerBlock < 0 || c->tilesPerBlock > 64) fail(GR_EINVAL, "tilesPerBlock must be 0 (default) or 1..64");

@@ -62,6 +62,8 @@ struct SolverConfig {
   // Level rings: 16-byte row records for the levels of 3 entries a row
   // (ILU and Gauss-Seidel "recordLevels").
   bool ringRecords = false;
+  // ILU "pairRows": in record levels each thread computes two rows at once.
+  bool pairRows = false;
   // Extension: log2 of the streamed kernel's ring size in bytes (0: the
   // smallest ring that holds the largest level).
   int ringLog2 = 0;

@@ -185,7 +185,8 @@ __global__ void __launch_bounds__(RingShape<W>::threads) iluRingKernel(const uns
                                                                const int* __restrict__ tileLevel,
                                                                const int* __restrict__ blockStart, int ringBytes,
                                                                int metaLevels, uint32_t l2Ahead, bool dilu,
-                                                               SPro<W> pro, W* __restrict__ y, int* errFlag) {
+                                                               SPro<W> pro, W* __restrict__ y, int* errFlag,
+                                                               bool pairRows) {
   constexpr int kRingCompute = RingShape<W>::compute;
   constexpr int kRingLevelSync = RingShape<W>::levelSync;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -309,7 +310,28 @@ __global__ void __launch_bounds__(RingShape<W>::threads) iluRingKernel(const uns
         // Record level (7-point lower or upper part): the same operations
         // as below, from two loads a row.
         const bool hasInv = cur.upper || dilu;
-        for (int q = threadIdx.x; q < cur.k; q += kRingCompute) {
+        int q0 = threadIdx.x;
+        if (pairRows) {
+          // Two rows of the level a thread at once (rows of one level never
+          // read each other): both rows' loads before either store.
+          for (; q0 + kRingCompute < cur.k; q0 += 2 * kRingCompute) {
+            const RowRecord ra = ringRecord(cur, q0, hasInv);
+            const RowRecord rb = ringRecord(cur, q0 + kRingCompute, hasInv);
+            if (!cur.upper) {
+              const W ta = recordDot(xs[ra.row], ra, xs);
+              const W tb = recordDot(xs[rb.row], rb, xs);
+              xs[ra.row] = dilu ? mul(ta, cvt<W>(ra.inv)) : ta;
+              xs[rb.row] = dilu ? mul(tb, cvt<W>(rb.inv)) : tb;
+            } else {
+              const W ta = recordDot(W(0), ra, xs), tb = recordDot(W(0), rb, xs);
+              const W xa = xs[ra.row], xb = xs[rb.row];
+              const W ia = cvt<W>(ra.inv), ib = cvt<W>(rb.inv);
+              xs[ra.row] = dilu ? add(xa, mul(ta, ia)) : mul(add(xa, ta), ia);
+              xs[rb.row] = dilu ? add(xb, mul(tb, ib)) : mul(add(xb, tb), ib);
+            }
+          }
+        }
+        for (int q = q0; q < cur.k; q += kRingCompute) {
           const RowRecord r = ringRecord(cur, q, hasInv);
           if (!cur.upper) {
             const W temp = recordDot(xs[r.row], r, xs);
@@ -561,7 +583,7 @@ void launchRingPack(DeviceMatrix& A, const LevelRing& R, void* stream, const voi
 namespace {
 template <class MV, class W>
 void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& p, void* y,
-                int l2Ahead, bool unroll, cudaStream_t s) {
+                int l2Ahead, bool unroll, bool pairRows, cudaStream_t s) {
   const size_t smem = iluRingSmem(A, R, dtypeOf<W>());
   auto kernel = R.compact ? (unroll ? dev::iluRingKernel<MV, W, true, true> : dev::iluRingKernel<MV, W, false, true>)
                          : (unroll ? dev::iluRingKernel<MV, W, true, false> : dev::iluRingKernel<MV, W, false, false>);
@@ -575,7 +597,7 @@ void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool di
                                              R.groupStart.as<int>(),
                                              static_cast<int>(R.ringBytes), R.maxTileLevels,
                                              static_cast<uint32_t>(l2Ahead < 0 ? dev::kPrefetchAhead : l2Ahead) & ~15u, dilu, pro,
-                                             static_cast<W*>(y), A.errFlag.as<int>());
+                                             static_cast<W*>(y), A.errFlag.as<int>(), pairRows);
   checkLaunch("ilu_ring");
 }
 }  // namespace
@@ -634,12 +656,13 @@ void launchGsRing(DeviceMatrix& A, const LevelRing& R, const void* stream, const
 }
 
 void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,
-                   void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s) {
-  if (A.vt == DType::F32 && W == DType::F32) ringApplyT<float, float>(A, R, stream, dilu, pro, y, l2Ahead, unroll, s);
+                   void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s, bool pairRows) {
+  if (A.vt == DType::F32 && W == DType::F32)
+    ringApplyT<float, float>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s);
   else if (A.vt == DType::F32 && W == DType::F64)
-    ringApplyT<float, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, s);
+    ringApplyT<float, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s);
   else if (A.vt == DType::F64 && W == DType::F64)
-    ringApplyT<double, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, s);
+    ringApplyT<double, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s);
   else fail(GR_EUNSUPPORTED, "ILU apply with float64 coefficients and float32 vectors");
 }
 

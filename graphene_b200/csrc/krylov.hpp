@@ -89,8 +89,9 @@ void launchRingPack(DeviceMatrix& A, const LevelRing& R, void* stream, const voi
                     cudaStream_t s);
 // l2Ahead: bytes kept prefetched into L2 beyond the issued copies (-1:
 // default); unroll: rows of up to four entries load all their terms at once.
+// pairRows: record levels process two rows a thread at once.
 void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,
-                   void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s);
+                   void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s, bool pairRows = false);
 // One Gauss-Seidel sweep through a Gauss-Seidel level ring (kernels_ring.cu):
 // xout from xin (xinZero: xin is all zeros and is not read; the ring may
 // then be a lower-only one). The right-hand side is the prologue's vector

@@ -154,7 +154,8 @@ class IluNode : public Node {
   }
   void apply(const PrologueArgs& pro, void* y, DType W) {
     if (kernel_ == 4)
-      launchIluRing(A_, *ring_, stream_.get(), dilu_, pro, y, W, cfg_.l2Ahead, cfg_.unrollRows != 0, s());
+      launchIluRing(A_, *ring_, stream_.get(), dilu_, pro, y, W, cfg_.l2Ahead, cfg_.unrollRows != 0, s(),
+                    cfg_.pairRows);
     else if (kernel_ == 3)
       launchIluWarp(A_, *sweep_, stream_.get(), dilu_, pro, y, W, rowsPerLane_, s());
     else if (kernel_ == 1)

@@ -55,18 +55,20 @@ NAMES = ["poisson16", "poisson_odd_bfs", "poisson_1tile", "random", "many_tiles"
 def ilu_config(kernel, **kw):
     """'ring_wide': the ring kernel with 32-bit row and column ids;
     'ring_rec': with 16-byte row records for levels of 3 entries a row."""
-    c = {"type": "ILU", "kernel": "ring" if kernel in ("ring_wide", "ring_rec") else kernel}
+    c = {"type": "ILU", "kernel": "ring" if kernel in ("ring_wide", "ring_rec", "ring_pair") else kernel}
     if kernel == "ring_wide":
         c["compactRing"] = False
-    if kernel == "ring_rec":
+    if kernel in ("ring_rec", "ring_pair"):
         c["recordLevels"] = True
+    if kernel == "ring_pair":
+        c["pairRows"] = True
     c.update(kw)
     return c
 
 
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("dilu", [False, True])
-@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "ring_wide", "warp", "tma", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "ring_pair", "ring_wide", "warp", "tma", "levels"])
 def test_ilu_bit_exact(oracle, name, dilu, kernel):
     h, om = case(name, oracle)
     A = h.copyToTile()
@@ -78,7 +80,7 @@ def test_ilu_bit_exact(oracle, name, dilu, kernel):
 
 
 @pytest.mark.parametrize("name", ["poisson16", "random"])
-@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "ring_wide", "warp", "tma", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "ring_pair", "ring_wide", "warp", "tma", "levels"])
 def test_ilu_bit_exact_float64(oracle, name, kernel):
     h, om = case(name, oracle, gb.FLOAT64)
     A = h.copyToTile()
