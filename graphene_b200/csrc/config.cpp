@@ -251,7 +251,9 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
   } else if (ty == "ILU") {
     mark("solveMulticolor"); mark("factorizeMulticolor"); mark("diagonalBased"); mark("kernel");
     mark("ringLog2"); mark("prefetch"); mark("unroll"); mark("ringBytes"); mark("l2Ahead"); mark("tilesPerBlock");
-    mark("compactRing"); mark("recordLevels"); mark("pairRows");
+    mark("compactRing"); mark("recordLevels"); mark("pairRows"); mark("warpsPerBlock");
+    readInt(j, "warpsPerBlock", c->warpsPerBlock);
+    if (c->warpsPerBlock < 1 || c->warpsPerBlock > 8) fail(GR_EINVAL, "warpsPerBlock must be 1..8");
     readBool(j, "compactRing", c->compactRing);
     readBool(j, "pairRows", c->pairRows);
     readBool(j, "recordLevels", c->ringRecords);
@@ -282,7 +284,8 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
       else if (v->text == "levels") c->iluKernel = 2;
       else if (v->text == "warp") c->iluKernel = 3;
       else if (v->text == "ring") c->iluKernel = 4;
-      else fail(GR_EPARSE, "ILU kernel must be \"auto\", \"ring\", \"warp\", \"tma\" or \"levels\"");
+      else if (v->text == "wring") c->iluKernel = 5;
+      else fail(GR_EPARSE, "ILU kernel must be \"auto\", \"ring\", \"wring\", \"warp\", \"tma\" or \"levels\"");
     }
   } else if (ty == "GaussSeidel") {
     mark("numSweeps"); mark("numFixedIterations"); mark("solveMulticolor"); mark("workingType");

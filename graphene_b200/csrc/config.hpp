@@ -44,7 +44,8 @@ struct SolverConfig {
   // when a tile fits shared memory, else the level-schedule kernel), "ring",
   // "tma" (chunked byte ring with a producer warp), "warp" (warp per tile)
   // or "levels".
-  int iluKernel = 0;  // 0 auto, 1 tma, 2 levels, 3 warp, 4 ring
+  int iluKernel = 0;  // 0 auto, 1 tma, 2 levels, 3 warp, 4 ring, 5 warp-per-tile ring
+  int warpsPerBlock = 1;  // tiles (warps) per block of the warp-per-tile ring kernel
   // Extension: shared-memory ring bytes of the "ring" kernel (0: default).
   long long ringBytes = 0;
   // Extension: bytes the "ring" kernel keeps prefetched into L2 beyond its

@@ -565,6 +565,158 @@ __global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
   for (int i = threadIdx.x; i < nRows; i += blockDim.x) xout[base + i] = cvt<X>(xs[i]);
 }
 
+// Level l's rows for thread t of `stride` threads: the substitution of
+// iluRingKernel's compute warps (same operations, same order).
+template <int STRIDE, class MV, class W, bool COMPACT>
+__device__ __forceinline__ void iluLevelRows(const RingLevel<MV, COMPACT>& cur, int t, int nRows, bool dilu,
+                                             bool pairRows, W* xs) {
+  if (cur.rec) {
+    const bool hasInv = cur.upper || dilu;
+    int q0 = t;
+    if (pairRows) {
+      for (; q0 + STRIDE < cur.k; q0 += 2 * STRIDE) {
+        const RowRecord ra = ringRecord(cur, q0, hasInv);
+        const RowRecord rb = ringRecord(cur, q0 + STRIDE, hasInv);
+        if (!cur.upper) {
+          const W ta = recordDot(xs[ra.row], ra, xs);
+          const W tb = recordDot(xs[rb.row], rb, xs);
+          xs[ra.row] = dilu ? mul(ta, cvt<W>(ra.inv)) : ta;
+          xs[rb.row] = dilu ? mul(tb, cvt<W>(rb.inv)) : tb;
+        } else {
+          const W ta = recordDot(W(0), ra, xs), tb = recordDot(W(0), rb, xs);
+          const W xa = xs[ra.row], xb = xs[rb.row];
+          const W ia = cvt<W>(ra.inv), ib = cvt<W>(rb.inv);
+          xs[ra.row] = dilu ? add(xa, mul(ta, ia)) : mul(add(xa, ta), ia);
+          xs[rb.row] = dilu ? add(xb, mul(tb, ib)) : mul(add(xb, tb), ib);
+        }
+      }
+    }
+    for (int q = q0; q < cur.k; q += STRIDE) {
+      const RowRecord r = ringRecord(cur, q, hasInv);
+      if (!cur.upper) {
+        const W temp = recordDot(xs[r.row], r, xs);
+        xs[r.row] = dilu ? mul(temp, cvt<W>(r.inv)) : temp;
+      } else {
+        const W temp = recordDot(W(0), r, xs);
+        const W iv = cvt<W>(r.inv);
+        xs[r.row] = dilu ? add(xs[r.row], mul(temp, iv)) : mul(add(xs[r.row], temp), iv);
+      }
+    }
+  } else if (!cur.upper) {
+    for (int q = t; q < cur.k; q += STRIDE) {
+      const int il = cur.row(q);
+      const W temp = ringRowDot<true>(xs[il], cur, q, nRows, xs);
+      xs[il] = dilu ? mul(temp, cvt<W>(cur.invDiag(q))) : temp;
+    }
+  } else {
+    for (int q = t; q < cur.k; q += STRIDE) {
+      const int il = cur.row(q);
+      const W temp = ringRowDot<true>(W(0), cur, q, nRows, xs);
+      const W iv = cvt<W>(cur.invDiag(q));
+      xs[il] = dilu ? add(xs[il], mul(temp, iv)) : mul(add(xs[il], temp), iv);
+    }
+  }
+}
+
+// ILU(0) / DILU substitution with one warp per tile (same arithmetic and
+// order as iluRingKernel). Each warp owns a slice of shared memory: its
+// tile's kRingBarriers completion mbarriers, level table, level ring and x
+// slice. The warp waits for level l's block on its own barrier, computes
+// the level's rows, meets its lanes with __syncwarp (no block-wide barrier,
+// no waiting or producer warp), and then lane 0 issues the bulk copies of
+// every later level whose ring space was held by level l or earlier (the
+// host schedule's issueAfter). The prologue keeps 16 (float) or 8 (double)
+// rows a lane in flight. Waits are bounded as in iluRingKernel.
+template <class MV, class W, bool COMPACT>
+__global__ void __launch_bounds__(256) iluWarpRingKernel(const unsigned char* __restrict__ stream,
+                                                          const long long* __restrict__ tileOffset,
+                                                          const int4* __restrict__ meta,
+                                                          const int* __restrict__ tileLevel,
+                                                          const int* __restrict__ tileStart, int P, int ringBytes,
+                                                          int metaLevels, uint32_t sliceBytes, bool dilu,
+                                                          SPro<W> pro, W* __restrict__ y, int* errFlag,
+                                                          bool pairRows) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int w = static_cast<int>(threadIdx.x >> 5), lane = static_cast<int>(threadIdx.x & 31);
+  const int T = static_cast<int>(blockIdx.x) * static_cast<int>(blockDim.x >> 5) + w;
+  if (T >= P) return;  // the whole warp
+  const KState* st = pro.st;
+  if (st && st->done) return;
+  unsigned char* my = smem + static_cast<size_t>(w) * sliceBytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(my);
+  int4* mt = reinterpret_cast<int4*>(my + 8 * kRingBarriers);
+  unsigned char* ring = my + 8 * kRingBarriers + 16 * metaLevels;
+  W* xs = reinterpret_cast<W*>(ring + ringBytes);
+  const int base = tileStart[T];
+  const int nRows = tileStart[T + 1] - base;
+  const int lv0 = tileLevel[T];
+  const int L = tileLevel[T + 1] - lv0;
+  const unsigned char* g = stream + tileOffset[T];
+  for (int i = lane; i < L; i += 32) mt[i] = __ldg(meta + lv0 + i);
+  if (lane == 0) {
+    for (int i = 0; i < kRingBarriers; ++i) mbarInit(smemAddr(full + i), 1);
+    fenceBarrierInit();
+  }
+  __syncwarp();
+  // Lane 0: the copies of every level j with issueAfter(j) <= done (in
+  // order; issueAfter never decreases along the levels).
+  int issued = 0;
+  uint32_t src = 0;
+  auto issueUpTo = [&](int done) {
+    while (issued < L) {
+      const int4 m = mt[issued];
+      if (RingLevelCode::issueAfter(m) > done) break;
+      const uint32_t bytes = RingLevelCode::bytes(m);
+      const uint32_t bar = smemAddr(full + issued % kRingBarriers);
+      mbarExpectTx(bar, bytes);
+      bulkLoad(smemAddr(ring + RingLevelCode::ringOffset(m)), g + src, bytes, bar);
+      src += bytes;
+      ++issued;
+    }
+  };
+  if (lane == 0) issueUpTo(-1);
+  {
+    W beta = W(0), omega = W(0), alpha = W(0);
+    bool first = true;
+    if (st) {
+      beta = cvt<W>(st->beta);
+      omega = cvt<W>(st->omega);
+      alpha = cvt<W>(st->alpha);
+      first = st->iter == 0;
+    }
+    constexpr int kRows = sizeof(W) == 4 ? 16 : 8;
+    for (int i0 = lane; i0 < nRows; i0 += 32 * kRows) {
+      W v[kRows];
+      pro.template rows<kRows>(base + i0, 32, base + nRows, beta, omega, alpha, first, v);
+#pragma unroll
+      for (int j = 0; j < kRows; ++j)
+        if (i0 + j * 32 < nRows) xs[i0 + j * 32] = v[j];
+    }
+    if (lane == 0) xs[nRows] = W(0);
+  }
+  __syncwarp();
+  int l = 0;
+  bool bad = false;
+  for (; l < L; ++l) {
+    bad = !mbarWaitBounded(smemAddr(full + l % kRingBarriers), (l / kRingBarriers) & 1);
+    if (__any_sync(0xFFFFFFFFu, bad)) break;
+    const RingLevel<MV, COMPACT> cur = ringLevelAt<MV, COMPACT>(mt[l], ring);
+    iluLevelRows<32>(cur, lane, nRows, dilu, pairRows, xs);
+    __syncwarp();
+    if (lane == 0) issueUpTo(l);
+  }
+  if (l < L) {
+    if (lane == 0) {
+      atomicExch(errFlag, GR_ETIMEOUT);
+      // Let the copies still in flight land before the slice is released
+      // (bounded): levels l .. issued - 1.
+      for (int j = l; j < issued; ++j) mbarWaitBounded(smemAddr(full + j % kRingBarriers), (j / kRingBarriers) & 1);
+    }
+    return;
+  }
+  for (int i = lane; i < nRows; i += 32) y[base + i] = xs[i];
+}
+
 }  // namespace dev
 
 // ---------------------------------------------------------------------------
@@ -653,6 +805,49 @@ void launchGsRing(DeviceMatrix& A, const LevelRing& R, const void* stream, const
   else
     fail(GR_EUNSUPPORTED, "Gauss-Seidel: float64 coefficients need float64 vectors, and the working type must be "
                           "the vectors' type or float64 over float32 vectors");
+}
+
+namespace {
+inline size_t warpRingSlice(const LevelRing& R, DType W) {
+  const size_t b = 8 * kRingBarriers + 16 * static_cast<size_t>(R.maxTileLevels) + static_cast<size_t>(R.ringBytes) +
+                   static_cast<size_t>(R.maxGroupRows + 1) * dtypeSize(W);
+  return (b + 127) / 128 * 128;
+}
+template <class MV, class W>
+void warpRingT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& p, void* y,
+               int warpsPerBlock, bool pairRows, cudaStream_t s) {
+  if (R.kind != RingKind::Ilu || R.group != 1) fail(GR_EINVAL, "the warp ring kernel runs one tile per warp");
+  if (p.stIndex) fail(GR_EUNSUPPORTED, "batched solves use the block ring kernel");
+  const size_t slice = warpRingSlice(R, dtypeOf<W>());
+  const size_t smem = slice * static_cast<size_t>(warpsPerBlock);
+  auto kernel = R.compact ? dev::iluWarpRingKernel<MV, W, true> : dev::iluWarpRingKernel<MV, W, false>;
+  ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
+  preferSharedCarveout(reinterpret_cast<const void*>(kernel));
+  dev::SPro<W> pro{static_cast<int>(p.kind), static_cast<const W*>(p.b), static_cast<const W*>(p.r),
+                   static_cast<W*>(p.pOrS), static_cast<const W*>(p.v), p.st, nullptr};
+  const int blocks = (R.numGroups + warpsPerBlock - 1) / warpsPerBlock;
+  kernel<<<blocks, 32 * warpsPerBlock, smem, s>>>(
+      static_cast<const unsigned char*>(stream), R.tileOffset.as<long long>(), R.meta.as<int4>(), R.tileLevel.as<int>(),
+      R.groupStart.as<int>(), R.numGroups, static_cast<int>(R.ringBytes), R.maxTileLevels,
+      static_cast<uint32_t>(slice), dilu, pro, static_cast<W*>(y), A.errFlag.as<int>(), pairRows);
+  checkLaunch("ilu_warp_ring");
+}
+}  // namespace
+
+size_t iluWarpRingSmem(const LevelRing& R, DType W, int warpsPerBlock) {
+  return warpRingSlice(R, W) * static_cast<size_t>(warpsPerBlock);
+}
+
+void launchIluWarpRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,
+                       void* y, DType W, int warpsPerBlock, bool pairRows, cudaStream_t s) {
+  if (warpsPerBlock < 1 || warpsPerBlock > 8) fail(GR_EINVAL, "warpsPerBlock must be 1..8");
+  if (A.vt == DType::F32 && W == DType::F32)
+    warpRingT<float, float>(A, R, stream, dilu, pro, y, warpsPerBlock, pairRows, s);
+  else if (A.vt == DType::F32 && W == DType::F64)
+    warpRingT<float, double>(A, R, stream, dilu, pro, y, warpsPerBlock, pairRows, s);
+  else if (A.vt == DType::F64 && W == DType::F64)
+    warpRingT<double, double>(A, R, stream, dilu, pro, y, warpsPerBlock, pairRows, s);
+  else fail(GR_EUNSUPPORTED, "ILU apply with float64 coefficients and float32 vectors");
 }
 
 void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,

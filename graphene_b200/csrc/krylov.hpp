@@ -89,6 +89,11 @@ void launchRingPack(DeviceMatrix& A, const LevelRing& R, void* stream, const voi
                     cudaStream_t s);
 // l2Ahead: bytes kept prefetched into L2 beyond the issued copies (-1:
 // default); unroll: rows of up to four entries load all their terms at once.
+// The same substitution with one warp per tile (iluWarpRingKernel):
+// dynamic shared memory of a block of warpsPerBlock tiles, and the launch.
+size_t iluWarpRingSmem(const LevelRing& R, DType W, int warpsPerBlock);
+void launchIluWarpRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,
+                       void* y, DType W, int warpsPerBlock, bool pairRows, cudaStream_t s);
 // pairRows: record levels process two rows a thread at once.
 void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,
                    void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s, bool pairRows = false);

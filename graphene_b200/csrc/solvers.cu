@@ -74,6 +74,13 @@ class IluNode : public Node {
     // shared memory).
     kernel_ = 2;
     const size_t smemMax = static_cast<size_t>(maxDynamicSmem(A));
+    if (c.iluKernel == 5) {
+      // Warp per tile over the same host-scheduled level ring.
+      ring_ = &A.levelRing(dilu_, c.ringBytes, 1, c.compactRing, RingKind::Ilu, c.ringRecords);
+      if (iluWarpRingSmem(*ring_, DType::F64, c.warpsPerBlock) > smemMax)
+        fail(GR_EUNSUPPORTED, "the warp ring ILU kernel does not fit this matrix's tiles in shared memory");
+      kernel_ = 5;
+    }
     if (c.iluKernel == 0 || c.iluKernel == 4) {
       LevelRing* R = nullptr;
       try {
@@ -100,7 +107,7 @@ class IluNode : public Node {
       else fail(GR_EUNSUPPORTED, "the requested ILU kernel does not fit this matrix's tiles in shared memory");
     }
     inv_.alloc(A.n * vs);
-    if (kernel_ == 4) {
+    if (kernel_ == 4 || kernel_ == 5) {
       stream_.alloc(std::max<i64>(16, ring_->bytes));
     } else if (kernel_ != 2) {
       SweepStream& S = A.iluSweepStream(dilu_);
@@ -130,7 +137,7 @@ class IluNode : public Node {
     launchIluFactor(A, dilu_ ? nullptr : F.get(), D.get(), A.offDiag.get(), dilu_, s());
     launchInvert(A, D.get(), inv_.get(), s());
     const void* vals = dilu_ ? A.offDiag.get() : F.get();
-    if (kernel_ == 4) {
+    if (kernel_ == 4 || kernel_ == 5) {
       launchRingPack(A, *ring_, stream_.get(), vals, inv_.get(), s());
     } else if (kernel_ != 2) {
       launchStreamPack(A, *sweep_, stream_.get(), vals, inv_.get(), s());
@@ -153,7 +160,9 @@ class IluNode : public Node {
     return st;
   }
   void apply(const PrologueArgs& pro, void* y, DType W) {
-    if (kernel_ == 4)
+    if (kernel_ == 5)
+      launchIluWarpRing(A_, *ring_, stream_.get(), dilu_, pro, y, W, cfg_.warpsPerBlock, cfg_.pairRows, s());
+    else if (kernel_ == 4)
       launchIluRing(A_, *ring_, stream_.get(), dilu_, pro, y, W, cfg_.l2Ahead, cfg_.unrollRows != 0, s(),
                     cfg_.pairRows);
     else if (kernel_ == 3)
@@ -168,7 +177,7 @@ class IluNode : public Node {
 
  private:
   bool dilu_;
-  int kernel_ = 2;  // 1 tma ring, 2 level schedule, 3 warp per tile, 4 host-scheduled ring
+  int kernel_ = 2;  // 1 tma ring, 2 level schedule, 3 warp per tile, 4 host-scheduled ring, 5 its warp-per-tile form
   int rowsPerLane_ = 2;
   DBuf inv_, Lval_, Uval_, stream_;
   const SweepStream* sweep_ = nullptr;

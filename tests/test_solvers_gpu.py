@@ -56,19 +56,24 @@ def ilu_config(kernel, **kw):
     """'ring_wide': the ring kernel with 32-bit row and column ids;
     'ring_rec': with 16-byte row records for levels of 3 entries a row."""
     c = {"type": "ILU", "kernel": "ring" if kernel in ("ring_wide", "ring_rec", "ring_pair") else kernel}
+    if kernel.startswith("wring"):
+        c["kernel"] = "wring"
     if kernel == "ring_wide":
         c["compactRing"] = False
-    if kernel in ("ring_rec", "ring_pair"):
+    if kernel in ("ring_rec", "ring_pair", "wring_rec", "wring_pair", "wring_w4"):
         c["recordLevels"] = True
-    if kernel == "ring_pair":
+    if kernel in ("ring_pair", "wring_pair"):
         c["pairRows"] = True
+    if kernel == "wring_w4":
+        c["warpsPerBlock"] = 4
     c.update(kw)
     return c
 
 
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("dilu", [False, True])
-@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "ring_pair", "ring_wide", "warp", "tma", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "ring_pair", "ring_wide", "wring", "wring_rec", "wring_pair",
+                                    "wring_w4", "warp", "tma", "levels"])
 def test_ilu_bit_exact(oracle, name, dilu, kernel):
     h, om = case(name, oracle)
     A = h.copyToTile()
@@ -80,7 +85,8 @@ def test_ilu_bit_exact(oracle, name, dilu, kernel):
 
 
 @pytest.mark.parametrize("name", ["poisson16", "random"])
-@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "ring_pair", "ring_wide", "warp", "tma", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "ring_pair", "ring_wide", "wring", "wring_pair", "warp", "tma",
+                                    "levels"])
 def test_ilu_bit_exact_float64(oracle, name, kernel):
     h, om = case(name, oracle, gb.FLOAT64)
     A = h.copyToTile()
