@@ -289,13 +289,16 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
     }
   } else if (ty == "GaussSeidel") {
     mark("numSweeps"); mark("numFixedIterations"); mark("solveMulticolor"); mark("workingType");
-    mark("seed"); mark("kernel"); mark("recordLevels");
+    mark("seed"); mark("kernel"); mark("recordLevels"); mark("warpsPerBlock");
     readBool(j, "recordLevels", c->ringRecords);
+    readInt(j, "warpsPerBlock", c->warpsPerBlock);
+    if (c->warpsPerBlock < 1 || c->warpsPerBlock > 8) fail(GR_EINVAL, "warpsPerBlock must be 1..8");
     if (const Json* v = j.find("kernel")) {
       if (v->text == "auto") c->gsKernel = 0;
       else if (v->text == "ring") c->gsKernel = 1;
       else if (v->text == "levels") c->gsKernel = 2;
-      else fail(GR_EPARSE, "GaussSeidel kernel must be \"auto\", \"ring\" or \"levels\"");
+      else if (v->text == "wring") c->gsKernel = 3;
+      else fail(GR_EPARSE, "GaussSeidel kernel must be \"auto\", \"ring\", \"wring\" or \"levels\"");
     }
     readInt(j, "numSweeps", c->numSweeps);
     readInt(j, "numFixedIterations", c->numFixedIterations);

@@ -717,6 +717,149 @@ __global__ void __launch_bounds__(256) iluWarpRingKernel(const unsigned char* __
   for (int i = lane; i < nRows; i += 32) y[base + i] = xs[i];
 }
 
+// Level l's rows of a Gauss-Seidel sweep for thread t of `stride` threads
+// (gsRingKernel's compute warps' operations, in the same order).
+template <int STRIDE, class MV, class X, class W, bool COMPACT>
+__device__ __forceinline__ void gsLevelRows(const RingLevel<MV, COMPACT>& cur, int t, bool seedB, const W* rhs,
+                                            W* xs) {
+  if (cur.rec) {
+    for (int q = t; q < cur.k; q += STRIDE) {
+      const RowRecord r = ringRecord(cur, q, true);
+      const W d = cvt<W>(r.inv);
+      const W sum = recordDot(seedB ? rhs[r.row] : d, r, xs);
+      xs[r.row] = storeRound<X>(dvd(sum, d));
+    }
+    return;
+  }
+  for (int q = t; q < cur.k; q += STRIDE) {
+    const int il = cur.row(q);
+    const W d = cvt<W>(cur.invDiag(q));
+    W sum = seedB ? rhs[il] : d;
+    if (cur.E <= 8) {
+      int c[8];
+      MV v[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+        if (e < cur.E) cur.entry(e, q, c[e], v[e]);
+      W xv[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+        if (e < cur.E) xv[e] = xs[c[e]];
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+        if (e < cur.E) sum = sub(sum, mul(cvt<W>(v[e]), xv[e]));
+    } else {
+      for (int e = 0; e < cur.E; ++e) {
+        int c;
+        MV v;
+        cur.entry(e, q, c, v);
+        sum = sub(sum, mul(cvt<W>(v), xs[c]));
+      }
+    }
+    xs[il] = storeRound<X>(dvd(sum, d));
+  }
+}
+
+// One Gauss-Seidel sweep with one warp per tile: gsRingKernel's sweep in
+// iluWarpRingKernel's organisation (a shared-memory slice per warp, the
+// warp's own barriers, __syncwarp between levels, lane 0 issuing its
+// tile's copies).
+template <class MV, class X, class W, bool COMPACT>
+__global__ void __launch_bounds__(256) gsWarpRingKernel(
+    const unsigned char* __restrict__ stream, const long long* __restrict__ tileOffset, const int4* __restrict__ meta,
+    const int* __restrict__ tileLevel, const int* __restrict__ tileStart, const int* __restrict__ haloStart,
+    const int* __restrict__ haloSrc, int P, int ringBytes, int metaLevels, uint32_t sliceBytes, bool seedB,
+    SPro<X> pro, const X* __restrict__ xin, bool xinZero, X* __restrict__ xout, int* errFlag) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int w = static_cast<int>(threadIdx.x >> 5), lane = static_cast<int>(threadIdx.x & 31);
+  const int T = static_cast<int>(blockIdx.x) * static_cast<int>(blockDim.x >> 5) + w;
+  if (T >= P) return;
+  const KState* st = pro.st;
+  if (st && st->done) return;
+  unsigned char* my = smem + static_cast<size_t>(w) * sliceBytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(my);
+  int4* mt = reinterpret_cast<int4*>(my + 8 * kRingBarriers);
+  unsigned char* ring = my + 8 * kRingBarriers + 16 * metaLevels;
+  W* xs = reinterpret_cast<W*>(ring + ringBytes);
+  const int base = tileStart[T];
+  const int nRows = tileStart[T + 1] - base;
+  const int h0 = haloStart[T];
+  const int nHalo = haloStart[T + 1] - h0;
+  W* rhs = xs + 2 * nRows + nHalo + 1;
+  const int lv0 = tileLevel[T];
+  const int L = tileLevel[T + 1] - lv0;
+  const unsigned char* g = stream + tileOffset[T];
+  for (int i = lane; i < L; i += 32) mt[i] = __ldg(meta + lv0 + i);
+  if (lane == 0) {
+    for (int i = 0; i < kRingBarriers; ++i) mbarInit(smemAddr(full + i), 1);
+    fenceBarrierInit();
+  }
+  __syncwarp();
+  int issued = 0;
+  uint32_t src = 0;
+  auto issueUpTo = [&](int done) {
+    while (issued < L) {
+      const int4 m = mt[issued];
+      if (RingLevelCode::issueAfter(m) > done) break;
+      const uint32_t bytes = RingLevelCode::bytes(m);
+      const uint32_t bar = smemAddr(full + issued % kRingBarriers);
+      mbarExpectTx(bar, bytes);
+      bulkLoad(smemAddr(ring + RingLevelCode::ringOffset(m)), g + src, bytes, bar);
+      src += bytes;
+      ++issued;
+    }
+  };
+  if (lane == 0) issueUpTo(-1);
+  constexpr int kRows = sizeof(W) == 4 ? 16 : 8;
+  if (seedB || pro.kind != static_cast<int>(Prologue::Plain)) {
+    X beta = X(0), omega = X(0), alpha = X(0);
+    bool first = true;
+    if (st) {
+      beta = cvt<X>(st->beta);
+      omega = cvt<X>(st->omega);
+      alpha = cvt<X>(st->alpha);
+      first = st->iter == 0;
+    }
+    for (int i0 = lane; i0 < nRows; i0 += 32 * kRows) {
+      X v[kRows];
+      pro.template rows<kRows>(base + i0, 32, base + nRows, beta, omega, alpha, first, v);
+      if (seedB) {
+#pragma unroll
+        for (int j = 0; j < kRows; ++j)
+          if (i0 + j * 32 < nRows) rhs[i0 + j * 32] = cvt<W>(v[j]);
+      }
+    }
+  }
+  for (int i0 = lane; i0 < nRows; i0 += 32 * kRows) {
+    W v[kRows];
+#pragma unroll
+    for (int j = 0; j < kRows; ++j) v[j] = !xinZero && i0 + j * 32 < nRows ? cvt<W>(xin[base + i0 + j * 32]) : W(0);
+#pragma unroll
+    for (int j = 0; j < kRows; ++j)
+      if (i0 + j * 32 < nRows) xs[nRows + i0 + j * 32] = v[j];
+  }
+  for (int h = lane; h < nHalo; h += 32) xs[2 * nRows + h] = xinZero ? W(0) : cvt<W>(xin[haloSrc[h0 + h]]);
+  if (lane == 0) xs[2 * nRows + nHalo] = W(0);
+  __syncwarp();
+  int l = 0;
+  bool bad = false;
+  for (; l < L; ++l) {
+    bad = !mbarWaitBounded(smemAddr(full + l % kRingBarriers), (l / kRingBarriers) & 1);
+    if (__any_sync(0xFFFFFFFFu, bad)) break;
+    gsLevelRows<32, MV, X, W, COMPACT>(ringLevelAt<MV, COMPACT>(mt[l], ring), lane, seedB, rhs, xs);
+    __syncwarp();
+    if (lane == 0) issueUpTo(l);
+  }
+  if (l < L) {
+    if (lane == 0) {
+      atomicExch(errFlag, GR_ETIMEOUT);
+      for (int j = l; j < issued; ++j) mbarWaitBounded(smemAddr(full + j % kRingBarriers), (j / kRingBarriers) & 1);
+    }
+    return;
+  }
+  for (int i = lane; i < nRows; i += 32) xout[base + i] = cvt<X>(xs[i]);
+}
+
 }  // namespace dev
 
 // ---------------------------------------------------------------------------
@@ -771,12 +914,34 @@ int ringBlocksPerSMWithoutSmem(DType vt, RingKind kind) {
 }
 
 namespace {
+inline size_t gsWarpRingSlice(const LevelRing& R, DType W) {
+  const size_t b = 8 * kRingBarriers + 16 * static_cast<size_t>(R.maxTileLevels) + static_cast<size_t>(R.ringBytes) +
+                   static_cast<size_t>(R.maxXSlots) * dtypeSize(W);
+  return (b + 127) / 128 * 128;
+}
 template <class MV, class X, class W>
 void gsRingT(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& p, bool seedB,
-             const void* xin, bool xinZero, void* xout, cudaStream_t s) {
+             const void* xin, bool xinZero, void* xout, int warps, cudaStream_t s) {
   if (R.kind == RingKind::Ilu) fail(GR_EINVAL, "not a Gauss-Seidel ring");
   if (R.kind == RingKind::GaussSeidelLower && !xinZero)
     fail(GR_EINVAL, "a lower-only Gauss-Seidel ring sweeps from x = 0 only");
+  if (warps > 0) {
+    if (warps > 8) fail(GR_EINVAL, "warpsPerBlock must be 1..8");
+    const size_t slice = gsWarpRingSlice(R, dtypeOf<W>());
+    const size_t smem = slice * static_cast<size_t>(warps);
+    auto kernel = R.compact ? dev::gsWarpRingKernel<MV, X, W, true> : dev::gsWarpRingKernel<MV, X, W, false>;
+    ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
+    preferSharedCarveout(reinterpret_cast<const void*>(kernel));
+    dev::SPro<X> pro{static_cast<int>(p.kind), static_cast<const X*>(p.b), static_cast<const X*>(p.r),
+                     static_cast<X*>(p.pOrS), static_cast<const X*>(p.v), p.st, nullptr};
+    kernel<<<(R.numGroups + warps - 1) / warps, 32 * warps, smem, s>>>(
+        static_cast<const unsigned char*>(stream), R.tileOffset.as<long long>(), R.meta.as<int4>(),
+        R.tileLevel.as<int>(), R.groupStart.as<int>(), R.haloStart.as<int>(), R.haloSrc.as<int>(), R.numGroups,
+        static_cast<int>(R.ringBytes), R.maxTileLevels, static_cast<uint32_t>(slice), seedB, pro,
+        static_cast<const X*>(xin), xinZero, static_cast<X*>(xout), A.errFlag.as<int>());
+    checkLaunch("gs_warp_ring");
+    return;
+  }
   const size_t smem = iluRingSmem(A, R, dtypeOf<W>());
   auto kernel = R.compact ? dev::gsRingKernel<MV, X, W, true> : dev::gsRingKernel<MV, X, W, false>;
   ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
@@ -792,16 +957,20 @@ void gsRingT(DeviceMatrix& A, const LevelRing& R, const void* stream, const Prol
 }
 }  // namespace
 
+size_t gsWarpRingSmem(const LevelRing& R, DType W, int warpsPerBlock) {
+  return gsWarpRingSlice(R, W) * static_cast<size_t>(warpsPerBlock);
+}
+
 void launchGsRing(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& pro, bool seedB,
-                  const void* xin, bool xinZero, void* xout, DType X, DType W, cudaStream_t s) {
+                  const void* xin, bool xinZero, void* xout, DType X, DType W, cudaStream_t s, int warps) {
   if (A.vt == DType::F32 && X == DType::F32 && W == DType::F32)
-    gsRingT<float, float, float>(A, R, stream, pro, seedB, xin, xinZero, xout, s);
+    gsRingT<float, float, float>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s);
   else if (A.vt == DType::F32 && X == DType::F32 && W == DType::F64)
-    gsRingT<float, float, double>(A, R, stream, pro, seedB, xin, xinZero, xout, s);
+    gsRingT<float, float, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s);
   else if (A.vt == DType::F32 && X == DType::F64 && W == DType::F64)
-    gsRingT<float, double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, s);
+    gsRingT<float, double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s);
   else if (A.vt == DType::F64 && X == DType::F64 && W == DType::F64)
-    gsRingT<double, double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, s);
+    gsRingT<double, double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s);
   else
     fail(GR_EUNSUPPORTED, "Gauss-Seidel: float64 coefficients need float64 vectors, and the working type must be "
                           "the vectors' type or float64 over float32 vectors");

@@ -104,8 +104,11 @@ void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool
 // reference's CodeDSL solver, gauss-seidel/Solver.cpp:74). stream: the ring
 // template with the coefficients and the diagonal packed in. Vectors of
 // type X, rows computed in W (X, or float64 over float32 vectors).
+// warps > 0: the warp-per-tile form (gsWarpRingKernel) with `warps` tiles a
+// block; gsWarpRingSmem gives its dynamic shared memory.
 void launchGsRing(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& pro, bool seedB,
-                  const void* xin, bool xinZero, void* xout, DType X, DType W, cudaStream_t s);
+                  const void* xin, bool xinZero, void* xout, DType X, DType W, cudaStream_t s, int warps = 0);
+size_t gsWarpRingSmem(const LevelRing& R, DType W, int warpsPerBlock);
 // Warp-per-tile substitution (kernels_warp.cu): shared memory per block and
 // the number of rows per lane to prefetch.
 size_t iluWarpSmem(const DeviceMatrix& A, const SweepStream& S, DType W);

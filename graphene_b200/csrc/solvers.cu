@@ -197,12 +197,15 @@ class GsNode : public Node {
         ring_ = &A.levelRing(false, 0, 1, true, RingKind::GaussSeidel, c.ringRecords);
         ringLo_ = &A.levelRing(false, 0, 1, true, RingKind::GaussSeidelLower, c.ringRecords);
       } catch (const Error&) {
-        if (c.gsKernel == 1) throw;
+        if (c.gsKernel == 1 || c.gsKernel == 3) throw;
         ring_ = ringLo_ = nullptr;
       }
       const size_t smemMax = static_cast<size_t>(maxDynamicSmem(A));
-      if (ring_ && (iluRingSmem(A, *ring_, DType::F64) > smemMax || iluRingSmem(A, *ringLo_, DType::F64) > smemMax)) {
-        if (c.gsKernel == 1)
+      auto need = [&](const LevelRing& R) {
+        return c.gsKernel == 3 ? gsWarpRingSmem(R, DType::F64, c.warpsPerBlock) : iluRingSmem(A, R, DType::F64);
+      };
+      if (ring_ && (need(*ring_) > smemMax || need(*ringLo_) > smemMax)) {
+        if (c.gsKernel == 1 || c.gsKernel == 3)
           fail(GR_EUNSUPPORTED, "the Gauss-Seidel ring kernel does not fit this matrix's tiles in shared memory");
         ring_ = ringLo_ = nullptr;
       }
@@ -346,7 +349,7 @@ class GsNode : public Node {
     for (int k = 0; k < count; ++k) {
       const bool zero = xZero && k == 0;
       launchGsRing(A_, zero ? *ringLo_ : *ring_, zero ? streamLo_.get() : stream_.get(), k == 0 ? first : plain,
-                   cfg_.gsSeedB, cur, zero, other, W, computeType(W), s());
+                   cfg_.gsSeedB, cur, zero, other, W, computeType(W), s(), cfg_.gsKernel == 3 ? cfg_.warpsPerBlock : 0);
       std::swap(cur, other);
     }
     if (cur != x) GR_CUDA(cudaMemcpyAsync(x, cur, A_.n * dtypeSize(W), cudaMemcpyDeviceToDevice, s()));

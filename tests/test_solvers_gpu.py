@@ -137,7 +137,7 @@ def test_ilu_ring_small_rings_bit_exact(oracle, name, frac):
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("sweeps", [1, 2, 3])
 @pytest.mark.parametrize("seed", ["b", "diag"])
-@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "wring", "wring_rec", "levels"])
 def test_gauss_seidel_bit_exact(oracle, name, sweeps, seed, kernel):
     h, om = case(name, oracle)
     A = h.copyToTile()
@@ -146,7 +146,7 @@ def test_gauss_seidel_bit_exact(oracle, name, sweeps, seed, kernel):
     x0 = rng.uniform(-1, 1, h.numRows).astype(np.float32)
     x = dev(x0)
     cfg = {"type": "GaussSeidel", "numFixedIterations": sweeps, "seed": seed,
-           "kernel": "ring" if kernel == "ring_rec" else kernel, "recordLevels": kernel == "ring_rec"}
+           "kernel": kernel.replace("_rec", ""), "recordLevels": kernel.endswith("_rec")}
     gb.Solver(A, cfg).solve(x, dev(b))
     ref = x0
     for _ in range(sweeps):
@@ -156,7 +156,8 @@ def test_gauss_seidel_bit_exact(oracle, name, sweeps, seed, kernel):
 
 @pytest.mark.parametrize("name", ["poisson16", "random", "many_tiles"])
 @pytest.mark.parametrize("vt", ["f32", "f64", "f32_matrix_f64_vectors"])
-def test_gauss_seidel_ring_types_bit_exact(oracle, name, vt):
+@pytest.mark.parametrize("kernel", ["ring", "wring"])
+def test_gauss_seidel_ring_types_bit_exact(oracle, name, vt, kernel):
     """The level-ring sweep with float64 vectors (float32 or float64
     coefficients): same bits as the oracle."""
     mt = gb.FLOAT64 if vt == "f64" else gb.FLOAT32
@@ -167,7 +168,7 @@ def test_gauss_seidel_ring_types_bit_exact(oracle, name, vt):
     b = rng.uniform(-1, 1, h.numRows).astype(dt)
     x0 = rng.uniform(-1, 1, h.numRows).astype(dt)
     x = dev(x0)
-    gb.Solver(A, {"type": "GaussSeidel", "numFixedIterations": 2, "kernel": "ring"}).solve(x, dev(b))
+    gb.Solver(A, {"type": "GaussSeidel", "numFixedIterations": 2, "kernel": kernel}).solve(x, dev(b))
     ref = om.gs_sweep(om.gs_sweep(x0, b), b)
     np.testing.assert_array_equal(host(x), ref)
 
@@ -175,14 +176,15 @@ def test_gauss_seidel_ring_types_bit_exact(oracle, name, vt):
 @pytest.mark.parametrize("name", ["poisson16", "random", "many_tiles", "poisson_odd_bfs"])
 @pytest.mark.parametrize("sweeps", [1, 2, 3])
 @pytest.mark.parametrize("records", [False, True])
-def test_gauss_seidel_ring_from_zero_bit_exact(oracle, name, sweeps, records):
+@pytest.mark.parametrize("kernel", ["ring", "wring"])
+def test_gauss_seidel_ring_from_zero_bit_exact(oracle, name, sweeps, records, kernel):
     """Sweeps from x = 0 (the first one through the lower-only ring), as a
     PBiCGStab preconditioner applies them: same bits as the oracle's full
     sweeps from zero."""
     h, om = case(name, oracle)
     A = h.copyToTile()
     b = np.random.default_rng(10).uniform(-1, 1, h.numRows).astype(np.float32)
-    cfg = {"type": "GaussSeidel", "numFixedIterations": sweeps, "kernel": "ring", "recordLevels": records}
+    cfg = {"type": "GaussSeidel", "numFixedIterations": sweeps, "kernel": kernel, "recordLevels": records}
     x = dev(np.zeros_like(b))
     gb.Solver(A, cfg).solve(x, dev(b))
     ref = np.zeros_like(b)
