@@ -369,7 +369,8 @@ def other_configs(gb, peak):
     return out
 
 
-def serving(gb, requests=10000, slots=8, seed=7, rate_requests=2000, cold_requests=48, gen_threads=0):
+def serving(gb, requests=10000, slots=8, seed=7, rate_requests=2000, cold_requests=48, gen_threads=0,
+            max_wall_s=300.0):
     """C5: a stream of solves, each a fresh 7-point variable-coefficient
     Poisson system (sigma 1) with grid edge L ~ U{16..96}, 70 % FP32
     PBiCGStab-ILU(0) to 1e-6 and 30 % MPIR to 1e-10 (by seed).
@@ -387,7 +388,9 @@ def serving(gb, requests=10000, slots=8, seed=7, rate_requests=2000, cold_reques
     arrivals at 50 %, 80 % and 100 % of that throughput, `rate_requests`
     each; p50 / p99 from arrival to result. Cold: `cold_requests` requests
     whose structures the server has never seen (tile layout, level rings,
-    upload and factorisation all in the latency)."""
+    upload and factorisation all in the latency). A run that exceeds
+    `max_wall_s` stops submitting and reports the requests it served
+    ("truncated")."""
     import concurrent.futures as cf
     import numpy as np
     ilu = {"type": "PBiCGStab", "maxIterations": 1000, "relResidual": 1e-6, "preconditioner": {"type": "ILU"}}
@@ -451,7 +454,11 @@ def serving(gb, requests=10000, slots=8, seed=7, rate_requests=2000, cold_reques
                 last_finish = tm["finished_ms"] if last_finish is None else max(last_finish, tm["finished_ms"])
         t0 = time.perf_counter()
         due = 0.0
+        truncated = False
         for i in range(len(ks)):
+            if time.perf_counter() - t0 > max_wall_s:
+                truncated = True
+                break
             fill(i)
             h, vals, b, cfg = futs.pop(i).result()
             due += gaps[i]
@@ -462,9 +469,12 @@ def serving(gb, requests=10000, slots=8, seed=7, rate_requests=2000, cold_reques
             del h, vals, b
             collect(False)
         collect(True)
+        for f in futs.values():
+            f.cancel()
         lat = np.array(lat)
         span = (last_finish - first_arrival) * 1e-3
-        return {"offered_per_s": rate, "requests": len(ks), "throughput_per_s": len(ks) / span,
+        return {"offered_per_s": rate, "requests": len(lat), "truncated": truncated,
+                "throughput_per_s": len(lat) / span,
                 "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                 "all_converged": conv, "fresh_values_on_resident_structure": hits[2],
                 "resident_same_matrix": hits[1], "new_pairs": hits[0]}
