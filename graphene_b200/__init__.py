@@ -250,6 +250,18 @@ class HostMatrix:
         check(_lib.lib().gr_host_matrix_compose_vector(self._h, _ptr(a), _ptr(out), t))
         return out
 
+    def setSpmvLayout(self, layout: int) -> None:
+        """SpMV column encoding of later device copies: -1 automatic, 0 32-bit
+        columns, 1 16-bit row offsets (gr_host_matrix_set_spmv_layout)."""
+        check(_lib.lib().gr_host_matrix_set_spmv_layout(self._h, layout))
+
+    def checkSpmvLayout(self, layout: int = -1) -> dict:
+        """Builds and decodes the SpMV layout on the host
+        (gr_host_matrix_check_spmv_layout); raises on a mismatch."""
+        c, sl, far = C.c_int32(), C.c_int64(), C.c_int64()
+        check(_lib.lib().gr_host_matrix_check_spmv_layout(self._h, layout, C.byref(c), C.byref(sl), C.byref(far)))
+        return {"compact": bool(c.value), "slots": sl.value, "far": far.value}
+
     def copyToTile(self) -> "Matrix":
         """HostMatrix::copyToTile: upload to the current CUDA device."""
         return Matrix(self)
@@ -517,6 +529,12 @@ class Matrix:
         check(_lib.lib().gr_residual(self._m, _ptr(x), xt, _ptr(b), _dtype_of(b), _ptr(r),
                                      destType, intermediateType))
         return r
+
+    def spmvLayout(self) -> dict:
+        """The device SpMV layout (gr_matrix_spmv_layout)."""
+        c, sl, far = C.c_int32(), C.c_int64(), C.c_int64()
+        check(_lib.lib().gr_matrix_spmv_layout(self._m, C.byref(c), C.byref(sl), C.byref(far)))
+        return {"compact": bool(c.value), "slots": sl.value, "far": far.value}
 
     def tuneSpmv(self, t: int = FLOAT32, reps: int = 5) -> dict:
         """Runs the SpMV autotuner (gr_matrix_tune_spmv) for vectors of type t."""

@@ -27,6 +27,7 @@ std::shared_ptr<HostMatrix> concatForBatch(const std::vector<std::shared_ptr<Hos
   const DType vt = parts[0]->valueType;
   auto U = std::make_shared<HostMatrix>();
   U->valueType = vt;
+  U->spmvLayout = parts[0]->spmvLayout;
   bool anyRank = false;
   for (const auto& h : parts) {
     if (!h) fail(GR_EINVAL, "batch system is NULL");

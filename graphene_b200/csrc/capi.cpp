@@ -395,6 +395,26 @@ int gr_host_matrix_check_gs_ring(const gr_host_matrix* h, int lower_only, gr_dty
   });
 }
 
+int gr_host_matrix_set_spmv_layout(gr_host_matrix* h, int32_t layout) {
+  return guarded([&] {
+    need(h, "matrix");
+    if (layout < -1 || layout > 1) gr::fail(GR_EINVAL, "spmv layout must be -1, 0 or 1");
+    h->m->spmvLayout = layout;
+  });
+}
+
+int gr_host_matrix_check_spmv_layout(const gr_host_matrix* h, int32_t layout, int32_t* compact, int64_t* slots,
+                                     int64_t* far_entries) {
+  return guarded([&] {
+    need(h, "matrix");
+    gr::SellHost S = gr::buildSell(*h->m, layout);
+    gr::checkSellDecode(S, h->m->n);
+    if (compact) *compact = S.compact ? 1 : 0;
+    if (slots) *slots = S.slots;
+    if (far_entries) *far_entries = static_cast<int64_t>(S.farCol.size());
+  });
+}
+
 int gr_host_matrix_decompose_vector(const gr_host_matrix* h, const void* natural, void* tile_ordered,
                                     gr_dtype t) {
   return guarded([&] {
@@ -466,6 +486,15 @@ int gr_matrix_get_info(const gr_matrix* A, gr_matrix_info* out) {
     need(A, "matrix");
     need(out, "out");
     *out = A->d->host->info();
+  });
+}
+
+int gr_matrix_spmv_layout(const gr_matrix* A, int32_t* compact, int64_t* slots, int64_t* far_entries) {
+  return guarded([&] {
+    need(A, "matrix");
+    if (compact) *compact = A->d->sell.compact ? 1 : 0;
+    if (slots) *slots = A->d->sell.slots;
+    if (far_entries) *far_entries = A->d->sell.far;
   });
 }
 

@@ -65,14 +65,43 @@ void uploadValues(DBuf& dst, const std::vector<double>& v, DType t);
 // order. Row r of chunk c keeps its entries in the reference's tile-local
 // column order at slots base[c] + 32*k + (r % 32); padding slots hold
 // column -1 and value 0. Used by SpMV and residual kernels.
+//
+// Two column encodings. The 32-bit layout stores each slot's tile-order
+// column. The 16-bit layout stores column - row as a 16-bit integer (0:
+// padding) and moves the columns too far from their row (|column - row| >
+// 32767, code -32768) to a side list in slot order, with the count of such
+// entries before each chunk: for a float matrix 6 bytes a slot instead of
+// 8. Both give every row the same terms in the same order.
 struct SellMatrix {
   i32 n = 0, nChunks = 0;
   i64 slots = 0;
-  DBuf base;  // i32[nChunks + 1]
-  DBuf ent;   // float coefficients: int2 {tile-order column, value bits} [slots]
-  DBuf col;   // double coefficients: i32 tile-order column [slots]
-  DBuf val;   // double coefficients: values [slots]
+  bool compact = false;  // the 16-bit layout
+  i64 far = 0;           // entries in the far list
+  DBuf base;     // i32[nChunks + 1]
+  DBuf ent;      // 32-bit layout, float coefficients: int2 {tile-order column, value bits} [slots]
+  DBuf col;      // 32-bit layout, double coefficients: i32 tile-order column [slots]
+  DBuf val;      // values [slots]: double coefficients, or the 16-bit layout
+  DBuf d16;      // 16-bit layout: i16 column - row [slots]
+  DBuf farCol;   // 16-bit layout: i32 far columns [far]
+  DBuf farBase;  // 16-bit layout: i32[nChunks + 1], far entries before each chunk
 };
+
+// Host image of the SELL layout of H (both encodings' arrays; the 16-bit
+// ones filled when `compact`). layout: 0 the 32-bit layout, 1 the 16-bit
+// layout, -1 the 16-bit layout when at most one entry in eight is far.
+struct SellHost {
+  i64 slots = 0;
+  bool compact = false;
+  std::vector<i32> base, col;  // col: tile-order column of every slot (-1 padding)
+  std::vector<double> val;
+  std::vector<int16_t> d16;
+  std::vector<i32> farCol, farBase;
+};
+SellHost buildSell(const HostMatrix& H, int layout);
+// Decodes the 16-bit arrays of S chunk by chunk, in the order the device's
+// warps walk them, and checks every slot against the 32-bit columns;
+// throws on the first mismatch.
+void checkSellDecode(const SellHost& S, i64 n);
 
 // Level schedule of one sweep over all tiles: for each tile its levels, for
 // each level its rows, and for each row its entries stored level-major

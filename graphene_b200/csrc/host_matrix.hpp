@@ -83,6 +83,9 @@ struct HostMatrix {
   // layout, tile-local CRS pattern and level sets, so a device copy of one
   // can take the other's values without any host-side layout work.
   u64 structureKey = 0;
+  // SpMV column encoding of device copies (SellMatrix): -1 automatic, 0 the
+  // 32-bit layout, 1 the 16-bit layout.
+  int spmvLayout = -1;
   // Global CRS entry (gVal index) of every tile-local CRS entry.
   std::vector<i32> localSrc;
 

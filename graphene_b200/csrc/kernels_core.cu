@@ -194,6 +194,123 @@ void uploadValues(DBuf& dst, const std::vector<double>& v, DType t) {
 }
 
 // ---------------------------------------------------------------------------
+// SELL layout on the host.
+SellHost buildSell(const HostMatrix& H, int layout) {
+  if (layout < -1 || layout > 1) fail(GR_EINVAL, "spmv layout must be -1, 0 or 1");
+  SellHost S;
+  const i64 n = H.n;
+  const i64 nChunks = (n + 31) / 32;
+  std::vector<i64> chunkLen(nChunks, 0);
+  parallelChunks(nChunks, [&](i64 b, i64 e) {
+    for (i64 c = b; c < e; ++c) {
+      i64 mx = 0;
+      for (i64 r = c * 32; r < std::min<i64>(n, c * 32 + 32); ++r) mx = std::max(mx, H.rowPtr[r + 1] - H.rowPtr[r]);
+      chunkLen[c] = mx;
+    }
+  });
+  S.base.assign(nChunks + 1, 0);
+  i64 acc = 0;
+  for (i64 c = 0; c < nChunks; ++c) {
+    S.base[c] = static_cast<i32>(acc);
+    acc += 32 * chunkLen[c];
+    if (acc >= (i64(1) << 31)) fail(GR_EUNSUPPORTED, "SELL storage exceeds 2^31 slots");
+  }
+  S.base[nChunks] = static_cast<i32>(acc);
+  S.slots = acc;
+  S.col.assign(acc, -1);
+  S.val.assign(acc, 0.0);
+  parallelChunks(n, [&](i64 b, i64 e) {
+    for (i64 r = b; r < e; ++r) {
+      i64 c = r / 32, lane = r % 32;
+      // Slot k holds the row's k-th term of its summation order: local
+      // column order for CRS, the LDU order (sumRank) for LDU matrices.
+      for (i64 k = 0; k < H.rowPtr[r + 1] - H.rowPtr[r]; ++k) {
+        const i64 p = H.rowPtr[r] + k;
+        const i64 slot = H.sumRank.empty() ? k : H.sumRank[p];
+        i64 s = S.base[c] + 32 * slot + lane;
+        S.col[s] = H.colPerm[p];
+        S.val[s] = H.offDiag[p];
+      }
+    }
+  });
+  if (layout == 0) return S;
+  // 16-bit offsets; far entries counted per chunk in slot order.
+  std::vector<int16_t> d16(acc, static_cast<int16_t>(dev::kSellPad));
+  std::vector<i32> farCount(nChunks + 1, 0);
+  parallelChunks(nChunks, [&](i64 b, i64 e) {
+    for (i64 c = b; c < e; ++c) {
+      i32 f = 0;
+      for (i64 s = S.base[c]; s < S.base[c + 1]; ++s) {
+        if (S.col[s] < 0) continue;
+        const i64 row = c * 32 + (s - S.base[c]) % 32;
+        const i64 d = static_cast<i64>(S.col[s]) - row;
+        if (d == 0 || d < -32767 || d > 32767) {
+          d16[s] = static_cast<int16_t>(dev::kSellFar);
+          ++f;
+        } else {
+          d16[s] = static_cast<int16_t>(d);
+        }
+      }
+      farCount[c] = f;
+    }
+  });
+  i64 far = 0;
+  for (i64 c = 0; c < nChunks; ++c) far += farCount[c];
+  if (layout == -1 && far * 8 > acc) return S;
+  S.compact = true;
+  S.d16 = std::move(d16);
+  S.farBase.assign(nChunks + 1, 0);
+  i64 run = 0;
+  for (i64 c = 0; c < nChunks; ++c) {
+    S.farBase[c] = static_cast<i32>(run);
+    run += farCount[c];
+  }
+  S.farBase[nChunks] = static_cast<i32>(run);
+  S.farCol.resize(run);
+  parallelChunks(nChunks, [&](i64 b, i64 e) {
+    for (i64 c = b; c < e; ++c) {
+      i32 f = S.farBase[c];
+      for (i64 s = S.base[c]; s < S.base[c + 1]; ++s)
+        if (S.d16[s] == dev::kSellFar) S.farCol[f++] = S.col[s];
+    }
+  });
+  return S;
+}
+
+void checkSellDecode(const SellHost& S, i64 n) {
+  if (!S.compact) return;
+  const i64 nChunks = (n + 31) / 32;
+  for (i64 c = 0; c < nChunks; ++c) {
+    const i64 s0 = S.base[c];
+    const i64 K = (S.base[c + 1] - s0) / 32;
+    i64 run = 0;  // the warp's running count of far slots, votes in k order
+    for (i64 k = 0; k < K; ++k) {
+      i64 below = 0;  // far slots of lower lanes at this k
+      for (i64 lane = 0; lane < 32; ++lane) {
+        const i64 s = s0 + 32 * k + lane;
+        const int d = S.d16[s];
+        i64 colv;
+        if (d == dev::kSellPad) {
+          colv = -1;
+        } else if (d == dev::kSellFar) {
+          const i64 idx = S.farBase[c] + run + below;
+          if (idx >= S.farBase[c + 1]) fail(GR_EINVAL, "SELL far list overrun in chunk " + std::to_string(c));
+          colv = S.farCol[idx];
+          ++below;
+        } else {
+          colv = c * 32 + lane + d;
+        }
+        if (colv != S.col[s])
+          fail(GR_EINVAL, "SELL 16-bit layout decodes slot " + std::to_string(s) + " to column " +
+                              std::to_string(colv) + ", expected " + std::to_string(S.col[s]));
+      }
+      run += below;
+    }
+    if (S.farBase[c] + run != S.farBase[c + 1]) fail(GR_EINVAL, "SELL far count mismatch in chunk " + std::to_string(c));
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Device matrix (HostMatrix::copyToTile, CRSHostMatrix.cpp:356-378).
 DeviceMatrix::DeviceMatrix(std::shared_ptr<HostMatrix> h) : host(std::move(h)) {
   const HostMatrix& H = *host;
@@ -209,57 +326,34 @@ DeviceMatrix::DeviceMatrix(std::shared_ptr<HostMatrix> h) : host(std::move(h)) {
   vt = H.valueType;
 
   // Sliced ELLPACK, chunk height 32, rows in tile order.
+  SellHost S = buildSell(H, H.spmvLayout);
   sell.n = n;
   sell.nChunks = (n + 31) / 32;
-  std::vector<i64> chunkLen(sell.nChunks, 0);
-  parallelChunks(sell.nChunks, [&](i64 b, i64 e) {
-    for (i64 c = b; c < e; ++c) {
-      i64 mx = 0;
-      for (i64 r = c * 32; r < std::min<i64>(n, c * 32 + 32); ++r)
-        mx = std::max(mx, H.rowPtr[r + 1] - H.rowPtr[r]);
-      chunkLen[c] = mx;
-    }
-  });
-  std::vector<i32> base(sell.nChunks + 1, 0);
-  i64 acc = 0;
-  for (i64 c = 0; c < sell.nChunks; ++c) {
-    base[c] = static_cast<i32>(acc);
-    acc += 32 * chunkLen[c];
-    if (acc >= (i64(1) << 31)) fail(GR_EUNSUPPORTED, "SELL storage exceeds 2^31 slots");
-  }
-  base[sell.nChunks] = static_cast<i32>(acc);
-  sell.slots = acc;
-  std::vector<i32> col(acc, -1);
-  std::vector<double> val(acc, 0.0);
-  parallelChunks(n, [&](i64 b, i64 e) {
-    for (i64 r = b; r < e; ++r) {
-      i64 c = r / 32, lane = r % 32;
-      // Slot k holds the row's k-th term of its summation order: local
-      // column order for CRS, the LDU order (sumRank) for LDU matrices.
-      for (i64 k = 0; k < H.rowPtr[r + 1] - H.rowPtr[r]; ++k) {
-        const i64 p = H.rowPtr[r] + k;
-        const i64 slot = H.sumRank.empty() ? k : H.sumRank[p];
-        i64 s = base[c] + 32 * slot + lane;
-        col[s] = H.colPerm[p];
-        val[s] = H.offDiag[p];
-      }
-    }
-  });
-  sell.base.upload(base);
-  if (vt == DType::F32) {
-    std::vector<int2> ent(acc);
-    parallelChunks(acc, [&](i64 b, i64 e) {
+  sell.slots = S.slots;
+  sell.compact = S.compact;
+  sell.far = static_cast<i64>(S.farCol.size());
+  sell.base.upload(S.base);
+  if (S.compact) {
+    sell.d16.upload(S.d16);
+    std::vector<i32> fc = S.farCol;
+    if (fc.empty()) fc.push_back(0);  // a valid pointer for the kernels
+    sell.farCol.upload(fc);
+    sell.farBase.upload(S.farBase);
+    uploadValues(sell.val, S.val, vt);
+  } else if (vt == DType::F32) {
+    std::vector<int2> ent(S.slots);
+    parallelChunks(S.slots, [&](i64 b, i64 e) {
       for (i64 s = b; s < e; ++s) {
-        float f = static_cast<float>(val[s]);
+        float f = static_cast<float>(S.val[s]);
         int bits;
         std::memcpy(&bits, &f, sizeof(bits));
-        ent[s] = make_int2(col[s], bits);
+        ent[s] = make_int2(S.col[s], bits);
       }
     });
     sell.ent.upload(ent);
   } else {
-    sell.col.upload(col);
-    uploadValues(sell.val, val, vt);
+    sell.col.upload(S.col);
+    uploadValues(sell.val, S.val, vt);
   }
   uploadValues(diag, H.diag, vt);
   std::vector<i32> ts(H.tileStart.begin(), H.tileStart.end());
@@ -426,8 +520,9 @@ void DeviceMatrix::updateValues(const std::vector<double>& localOff, const std::
   copyValuesInto(diag, tileDiag, vt, stream);
   const int blocks = static_cast<int>(std::min<i64>(numSMs * 8, (sell.slots + 255) / 256 + 1));
   if (vt == DType::F32)
-    dev::sellScatterKernel<float><<<blocks, 256, 0, stream>>>(sellSrc.as<int>(), offDiag.as<float>(),
-                                                              sell.ent.as<int2>(), nullptr, sell.slots);
+    dev::sellScatterKernel<float><<<blocks, 256, 0, stream>>>(
+        sellSrc.as<int>(), offDiag.as<float>(), sell.compact ? nullptr : sell.ent.as<int2>(),
+        sell.compact ? sell.val.as<float>() : nullptr, sell.slots);
   else
     dev::sellScatterKernel<double><<<blocks, 256, 0, stream>>>(sellSrc.as<int>(), offDiag.as<double>(), nullptr,
                                                                sell.val.as<double>(), sell.slots);
@@ -448,9 +543,8 @@ __global__ void __launch_bounds__(512) spmvKernel(SellView<MV> A, const VT* __re
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
   for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < A.nChunks; c += nWarps) {
     const int row = c * 32 + lane;
-    const int s0 = __ldg(A.base + c);
-    const int K = (__ldg(A.base + c + 1) - s0) >> 5;
-    if (row < A.n) y[row] = sellRowSum<VT, MV, VT, B>(A, x, row, s0, K, lane);
+    const VT v = sellRowSum<VT, MV, VT, B>(A, x, c, lane, row < A.n);
+    if (row < A.n) y[row] = v;
   }
 }
 
@@ -468,10 +562,8 @@ __global__ void __launch_bounds__(256) residualKernel(SellView<MV> A, const XT* 
   double part = redIdentity(normOp(normKind));
   for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < A.nChunks; c += nWarps) {
     const int row = c * 32 + lane;
-    const int s0 = __ldg(A.base + c);
-    const int K = (__ldg(A.base + c + 1) - s0) >> 5;
+    const I sum = sellRowSum<I>(A, x, c, lane, row < A.n);
     if (row < A.n) {
-      I sum = sellRowSum<I>(A, x, row, s0, K, lane);
       RT res = cvt<RT>(sub(cvt<I>(__ldg(b + row)), sum));
       r[row] = res;
       if (normKind >= 0) part = normStep(part, toDouble(res), normKind);
@@ -507,15 +599,18 @@ __global__ void __launch_bounds__(256) residualDwKernel(SellView<float> A, const
   };
   for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < A.nChunks; c += nWarps) {
     const int row = c * 32 + lane;
-    const int s0 = __ldg(A.base + c);
-    const int K = (__ldg(A.base + c + 1) - s0) >> 5;
-    if (row < A.n) {
-      dw sum = dwTimesFp(ld(row), __ldg(A.diag + row));
-      const int2* ep = A.ent + s0 + lane;
-      for (int k = 0; k < K; ++k) {
-        int2 e = __ldcs(ep + 32 * k);
-        if (e.x >= 0) sum = dwPlusDw(sum, dwTimesFp(ld(e.x), __int_as_float(e.y)));
-      }
+    const bool live = row < A.n;
+    dw sum = live ? dwTimesFp(ld(row), __ldg(A.diag + row)) : dw{0.0f, 0.0f};
+    ChunkWalk<float> w(A, c, lane);
+    for (int k = 0; k < w.K; k += 4) {
+      int cl[4];
+      float a[4];
+      w.template load<4>(A, k, cl, a);
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (cl[j] >= 0) sum = dwPlusDw(sum, dwTimesFp(ld(cl[j]), a[j]));
+    }
+    if (live) {
       dw res = dwPlusDw(dw{__ldg(b + row), 0.0f}, dwNeg(sum));
       float rv = dwToFloat(res);
       r[row] = rv;

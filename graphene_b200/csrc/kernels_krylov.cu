@@ -44,10 +44,9 @@ __global__ void __launch_bounds__(256) bicgInitKernel(SellView<MV> A, const W* _
   const int ops[2] = {normOp(nk), RED_SUM};
   for (int c = (sp.r0 >> 5) + ((sp.rank * blockDim.x + threadIdx.x) >> 5); c < cEnd; c += nWarps) {
     const int row = c * 32 + lane;
-    const int s0 = __ldg(A.base + c);
-    const int K = (__ldg(A.base + c + 1) - s0) >> 5;
+    const W sum = sellRowSum<W>(A, x, c, lane, row < sp.r1);
     if (row < sp.r1) {
-      W res = sub(__ldg(b + row), sellRowSum<W>(A, x, row, s0, K, lane));
+      W res = sub(__ldg(b + row), sum);
       r[row] = res;
       r0[row] = res;
       v[0] = normStep(v[0], toDouble(res), nk);
@@ -91,10 +90,8 @@ __global__ void __launch_bounds__(256) spmvDotKernel(SellView<MV> A, const W* __
   const int ops[2] = {RED_SUM, RED_SUM};
   for (int c = (sp.r0 >> 5) + ((sp.rank * blockDim.x + threadIdx.x) >> 5); c < cEnd; c += nWarps) {
     const int row = c * 32 + lane;
-    const int s0 = __ldg(A.base + c);
-    const int K = (__ldg(A.base + c + 1) - s0) >> 5;
+    const W yv = sellRowSum<W>(A, x, c, lane, row < sp.r1);
     if (row < sp.r1) {
-      const W yv = sellRowSum<W>(A, x, row, s0, K, lane);
       y[row] = yv;
       const double yd = toDouble(yv);
       v[0] = __dadd_rn(v[0], __dmul_rn(toDouble(__ldg(d1 + row)), yd));

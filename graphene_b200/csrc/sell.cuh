@@ -7,14 +7,24 @@
 namespace gr {
 namespace dev {
 
+// 16-bit SELL layout codes (column - row is never 0 for an off-diagonal).
+constexpr int kSellPad = 0;
+constexpr int kSellFar = -32768;
+
 template <class MV>
 struct SellView {
   int n, nChunks;
   const int* __restrict__ base;
-  const int2* __restrict__ ent;  // float coefficients: {column, value bits}
-  const int* __restrict__ col;   // double coefficients: columns ...
-  const MV* __restrict__ val;    // ... and values
+  const int2* __restrict__ ent;  // 32-bit layout, float coefficients: {column, value bits}
+  const int* __restrict__ col;   // 32-bit layout, double coefficients: columns ...
+  const MV* __restrict__ val;    // ... and values; the 16-bit layout's values (both types)
   const MV* __restrict__ diag;
+  // 16-bit layout (d16 non-null): column - row per slot (kSellPad: padding,
+  // kSellFar: the column is the chunk's next far column), far columns in
+  // slot order and the number of far entries before each chunk.
+  const short* __restrict__ d16;
+  const int* __restrict__ farCol;
+  const int* __restrict__ farBase;
 };
 
 // Splits one launch into independent systems (a batch of block-diagonal
@@ -48,20 +58,56 @@ __device__ __forceinline__ Acc loadX(const XT* __restrict__ x, int i) {
   return cvt<Acc>(__ldg(x + i));
 }
 
-// Row sum of one row of a SELL-32 chunk, in Acc: diag * x[row] first, then
-// the off-diagonal products added in stored order (padding slots have
-// column -1 and are skipped, so the result is the sequential row sum).
-// The loads of up to B entries are issued before the dependent gathers of x
-// so that a warp keeps many memory requests in flight; the matrix stream is
-// read with evict-first loads so that x stays resident in L2.
-template <class Acc, class MV, class XT, int B = 8>
-__device__ __forceinline__ Acc sellRowSum(const SellView<MV>& A, const XT* __restrict__ x, int row,
-                                          int s0, int K, int lane) {
-  Acc acc = mul(cvt<Acc>(__ldg(A.diag + row)), loadX<Acc>(x, row));
-  for (int k = 0; k < K; k += B) {
-    int c[B];
-    MV a[B];
-    if constexpr (sizeof(MV) == 4) {
+// The slots of SELL chunk c as one warp walks them, k = 0, 1, ... (all 32
+// lanes together: the 16-bit layout resolves far columns with warp votes).
+// Lane l reads the slots of row 32c + l.
+template <class MV>
+struct ChunkWalk {
+  int s0, K, lane, row;
+  int farBase = 0, nFar = 0, farRun = 0, farReg = 0;
+
+  __device__ __forceinline__ ChunkWalk(const SellView<MV>& A, int c, int lane_) : lane(lane_) {
+    row = c * 32 + lane;
+    s0 = __ldg(A.base + c);
+    K = (__ldg(A.base + c + 1) - s0) >> 5;
+    if (A.d16) {
+      farBase = __ldg(A.farBase + c);
+      nFar = __ldg(A.farBase + c + 1) - farBase;
+      // Up to 32 far columns of the chunk live in the lanes' registers and
+      // are handed out by shuffles; longer lists are read from memory.
+      if (nFar <= 32 && lane < nFar) farReg = __ldg(A.farCol + farBase + lane);
+    }
+  }
+
+  // Columns (-1: padding) and coefficients of slots k .. k+B-1 of this lane's
+  // row. The loads of all B slots are issued before any is used.
+  template <int B>
+  __device__ __forceinline__ void load(const SellView<MV>& A, int k, int (&c)[B], MV (&a)[B]) {
+    if (A.d16) {
+      const short* dp = A.d16 + s0 + lane + 32 * k;
+      const MV* vp = A.val + s0 + lane + 32 * k;
+      short d[B];
+#pragma unroll
+      for (int j = 0; j < B; ++j) {
+        const bool in = k + j < K;
+        d[j] = in ? __ldcs(dp + 32 * j) : static_cast<short>(kSellPad);
+        a[j] = in ? __ldcs(vp + 32 * j) : MV(0);
+      }
+      const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+      for (int j = 0; j < B; ++j) {
+        const bool far = d[j] == kSellFar;
+        const unsigned vote = __ballot_sync(0xffffffffu, far);
+        int fc = 0;
+        if (vote) {  // warp-uniform
+          const int idx = farRun + __popc(vote & below);
+          if (nFar <= 32) fc = __shfl_sync(0xffffffffu, farReg, idx & 31);
+          else if (far) fc = __ldg(A.farCol + farBase + idx);
+          farRun += __popc(vote);
+        }
+        c[j] = d[j] == kSellPad ? -1 : (far ? fc : row + d[j]);
+      }
+    } else if constexpr (sizeof(MV) == 4) {
       const int2* p = A.ent + s0 + lane + 32 * k;
 #pragma unroll
       for (int j = 0; j < B; ++j) {
@@ -79,12 +125,33 @@ __device__ __forceinline__ Acc sellRowSum(const SellView<MV>& A, const XT* __res
         a[j] = in ? __ldcs(vp + 32 * j) : MV(0);
       }
     }
+  }
+};
+
+// Row sum of row 32c + lane of SELL chunk c, in Acc: diag * x[row] first,
+// then the off-diagonal products added in stored order (padding slots are
+// skipped, so the result is the sequential row sum). All 32 lanes of the
+// warp call it together; a lane whose row is not `live` (past the matrix or
+// the system) returns 0 and touches neither the diagonal nor x. The loads
+// of up to B entries are issued before the dependent gathers of x so that a
+// warp keeps many memory requests in flight; the matrix stream is read with
+// evict-first loads so that x stays resident in L2.
+template <class Acc, class MV, class XT, int B = 8>
+__device__ __forceinline__ Acc sellRowSum(const SellView<MV>& A, const XT* __restrict__ x, int c, int lane,
+                                          bool live) {
+  ChunkWalk<MV> w(A, c, lane);
+  const int row = w.row;
+  Acc acc = live ? mul(cvt<Acc>(__ldg(A.diag + row)), loadX<Acc>(x, row)) : Acc(0);
+  for (int k = 0; k < w.K; k += B) {
+    int cl[B];
+    MV a[B];
+    w.template load<B>(A, k, cl, a);
     Acc xv[B];
 #pragma unroll
-    for (int j = 0; j < B; ++j) xv[j] = c[j] >= 0 ? loadX<Acc>(x, c[j]) : Acc(0);
+    for (int j = 0; j < B; ++j) xv[j] = cl[j] >= 0 ? loadX<Acc>(x, cl[j]) : Acc(0);
 #pragma unroll
     for (int j = 0; j < B; ++j)
-      if (c[j] >= 0) acc = add(acc, mul(cvt<Acc>(a[j]), xv[j]));
+      if (cl[j] >= 0) acc = add(acc, mul(cvt<Acc>(a[j]), xv[j]));
   }
   return acc;
 }
@@ -108,8 +175,16 @@ __device__ __forceinline__ double normFinish(double total, int kind) {
 
 template <class MV>
 inline dev::SellView<MV> sellView(const DeviceMatrix& A) {
-  return dev::SellView<MV>{A.n, A.sell.nChunks, A.sell.base.as<int>(), A.sell.ent.as<int2>(), A.sell.col.as<int>(),
-                           A.sell.val.as<MV>(), A.diag.as<MV>()};
+  return dev::SellView<MV>{A.n,
+                           A.sell.nChunks,
+                           A.sell.base.as<int>(),
+                           A.sell.compact ? nullptr : A.sell.ent.as<int2>(),
+                           A.sell.compact ? nullptr : A.sell.col.as<int>(),
+                           A.sell.val.as<MV>(),
+                           A.diag.as<MV>(),
+                           A.sell.compact ? A.sell.d16.as<short>() : nullptr,
+                           A.sell.farCol.as<int>(),
+                           A.sell.farBase.as<int>()};
 }
 
 inline void checkLaunch(const char* name) {

@@ -292,6 +292,23 @@ int gr_host_matrix_check_gs_ring(const gr_host_matrix* h, int lower_only, gr_dty
  * or array, or the first column of a "matrix" object; unlisted entries are
  * 0), which must have as many rows as h, and writes it in tile order, type t
  * (float32 or float64). Host only. */
+/* SpMV column encoding of this matrix's later device copies
+ * (gr_matrix_create): -1 automatic (the default), 0 32-bit tile-order
+ * columns, 1 16-bit column - row offsets with a side list for the columns
+ * more than 32767 rows away (6 bytes a float slot instead of 8). Both
+ * layouts give every row the same terms in the same order, so SpMV,
+ * residual and solver results are identical. Automatic picks the 16-bit
+ * layout when at most one entry in eight is far. No counterpart in the
+ * reference (its CRS SpMV reads 32-bit local column indices,
+ * matrix/details/crs/CRSMatrix.cpp:42-128). */
+int gr_host_matrix_set_spmv_layout(gr_host_matrix* h, int32_t layout);
+/* Builds the SpMV layout `layout` selects on the host and decodes every
+ * slot of the 16-bit encoding, in the order the device's warps walk them,
+ * against the 32-bit columns (GR_EINVAL on a mismatch). Reports whether
+ * the 16-bit encoding was chosen, the slot count and the far entries. No
+ * device needed; no counterpart in the reference. */
+int gr_host_matrix_check_spmv_layout(const gr_host_matrix* h, int32_t layout, int32_t* compact, int64_t* slots,
+                                     int64_t* far_entries);
 int gr_host_matrix_load_vector_mm(const gr_host_matrix* h, const char* path, gr_dtype t, void* tile_ordered);
 
 /* Natural order <-> tile order (DistributedTileLayout::decomposeVector,
@@ -316,6 +333,10 @@ int gr_matrix_get_info(const gr_matrix* A, gr_matrix_info* out);
 /* Replaces Matrix::operator*(Tensor& x) (matrix/Matrix.hpp:95-97,
  * details/crs/CRSMatrix.cpp:42-83): y = A x. x and y are device pointers in
  * tile order; xt == yt (FLOAT32 or FLOAT64). */
+/* The SpMV layout of a device matrix (see gr_host_matrix_set_spmv_layout):
+ * 16-bit encoding or not, slots, far entries. No counterpart in the
+ * reference. */
+int gr_matrix_spmv_layout(const gr_matrix* A, int32_t* compact, int64_t* slots, int64_t* far_entries);
 int gr_spmv(gr_matrix* A, const void* x, void* y, gr_dtype t);
 
 /* SpMV autotuner (no counterpart in the reference): times the candidate
