@@ -797,8 +797,16 @@ def main():
     ilu_ms = ilu.timeRepeated(z, b, 20)  # device time, launches back to back
     ilu_bytes = 8 * m + 12 * n
     gbs = lambda byts, ms: byts / (ms * 1e-3) / 1e9  # noqa: E731
+    # Bytes the device layout itself moves: the 16-bit layout's 6-byte slots
+    # and far columns (or 8-byte slots), chunk tables, diagonal, x and y.
+    lay = A.spmvLayout()
+    chunks = (n + 31) // 32
+    lay_bytes = (lay["slots"] * (6 if lay["compact"] else 8) + 4 * lay["far"]
+                 + 4 * (chunks + 1) * (2 if lay["compact"] else 1) + 12 * n)
     extra["spmv"] = {"ms": spmv_ms, "GBs": gbs(spmv_bytes, spmv_ms),
                      "frac_of_hbm": gbs(spmv_bytes, spmv_ms) / peak, "bytes_per_launch": spmv_bytes,
+                     "layout": lay, "layout_bytes_per_launch": lay_bytes,
+                     "layout_GBs": gbs(lay_bytes, spmv_ms), "layout_frac_of_hbm": gbs(lay_bytes, spmv_ms) / peak,
                      "autotuned_geometry": tuned}
     extra["ilu0_apply"] = {"ms": ilu_ms, "GBs": gbs(ilu_bytes, ilu_ms),
                            "frac_of_hbm": gbs(ilu_bytes, ilu_ms) / peak, "bytes_per_launch": ilu_bytes}
