@@ -28,11 +28,11 @@ import numpy as np
 
 from . import _lib
 from ._lib import (FLOAT32, FLOAT64, NORM_L1, NORM_L2, NORM_LINF, NORM_NONE, PART_AUTO, PART_BFS,
-                   PART_CONTIGUOUS, PART_EXPLICIT, PART_RCB, TWOFLOAT32, GrapheneError, check)
+                   PART_CONTIGUOUS, PART_EXPLICIT, PART_MULTILEVEL, PART_RCB, TWOFLOAT32, GrapheneError, check)
 
 __all__ = [
     "FLOAT32", "FLOAT64", "TWOFLOAT32", "NORM_L1", "NORM_L2", "NORM_LINF",
-    "PART_AUTO", "PART_CONTIGUOUS", "PART_RCB", "PART_BFS", "PART_EXPLICIT",
+    "PART_AUTO", "PART_CONTIGUOUS", "PART_RCB", "PART_BFS", "PART_EXPLICIT", "PART_MULTILEVEL",
     "GrapheneError", "HostMatrix", "Matrix", "Configuration", "Solver", "SolverStats",
     "generate3DPoissonMatrix", "loadMatrixFromFile", "parseType", "launch_count",
     "generateMatrix", "generateMatrixLike", "generateValues", "generateLduMesh", "randomVector", "Server", "Batch",
@@ -250,6 +250,13 @@ class HostMatrix:
         check(_lib.lib().gr_host_matrix_compose_vector(self._h, _ptr(a), _ptr(out), t))
         return out
 
+    def edgeCut(self) -> int:
+        """Off-diagonal entries whose column lies in another tile
+        (gr_host_matrix_edge_cut; a symmetric pattern's cut edges count twice)."""
+        c = C.c_int64()
+        check(_lib.lib().gr_host_matrix_edge_cut(self._h, C.byref(c)))
+        return c.value
+
     def setSpmvLayout(self, layout: int) -> None:
         """SpMV column encoding of later device copies: -1 automatic, 0 32-bit
         columns, 1 16-bit row offsets (gr_host_matrix_set_spmv_layout)."""
@@ -258,9 +265,10 @@ class HostMatrix:
     def checkSpmvLayout(self, layout: int = -1) -> dict:
         """Builds and decodes the SpMV layout on the host
         (gr_host_matrix_check_spmv_layout); raises on a mismatch."""
-        c, sl, far = C.c_int32(), C.c_int64(), C.c_int64()
-        check(_lib.lib().gr_host_matrix_check_spmv_layout(self._h, layout, C.byref(c), C.byref(sl), C.byref(far)))
-        return {"compact": bool(c.value), "slots": sl.value, "far": far.value}
+        c, sl, far, mx = C.c_int32(), C.c_int64(), C.c_int64(), C.c_int64()
+        check(_lib.lib().gr_host_matrix_check_spmv_layout(self._h, layout, C.byref(c), C.byref(sl), C.byref(far),
+                                                           C.byref(mx)))
+        return {"compact": bool(c.value), "slots": sl.value, "far": far.value, "max_chunk_far": mx.value}
 
     def copyToTile(self) -> "Matrix":
         """HostMatrix::copyToTile: upload to the current CUDA device."""

@@ -25,7 +25,7 @@ GR_ECANCELED = 11
 
 FLOAT32, FLOAT64, TWOFLOAT32 = 0, 1, 2
 NORM_L1, NORM_L2, NORM_LINF, NORM_NONE = 0, 1, 2, 3
-PART_AUTO, PART_CONTIGUOUS, PART_RCB, PART_BFS, PART_EXPLICIT = 0, 1, 2, 3, 4
+PART_AUTO, PART_CONTIGUOUS, PART_RCB, PART_BFS, PART_EXPLICIT, PART_MULTILEVEL = 0, 1, 2, 3, 4, 5
 
 
 class Stats(C.Structure):
@@ -99,6 +99,7 @@ SIGNATURES = {
     "gr_host_matrix_astype": (C.c_int, [vp, C.c_int, P(vp)]),
     "gr_host_matrix_get_info": (C.c_int, [vp, P(MatrixInfo)]),
     "gr_host_matrix_row_to_tile": (C.c_int, [vp, vp]),
+    "gr_host_matrix_edge_cut": (C.c_int, [vp, P(i64)]),
     "gr_host_matrix_tile_sizes": (C.c_int, [vp, vp]),
     "gr_host_matrix_local_to_global": (C.c_int, [vp, vp]),
     "gr_host_matrix_local_crs": (C.c_int, [vp, vp, vp, vp, vp]),
@@ -108,7 +109,7 @@ SIGNATURES = {
     "gr_host_matrix_check_ilu_ring": (C.c_int, [vp, C.c_int, C.c_int, i64, i32, i32, P(i64), P(i64), P(i32)]),
     "gr_host_matrix_check_gs_ring": (C.c_int, [vp, C.c_int, C.c_int, i64, i32, P(i64), P(i64), P(i32)]),
     "gr_host_matrix_set_spmv_layout": (C.c_int, [vp, i32]),
-    "gr_host_matrix_check_spmv_layout": (C.c_int, [vp, i32, P(i32), P(i64), P(i64)]),
+    "gr_host_matrix_check_spmv_layout": (C.c_int, [vp, i32, P(i32), P(i64), P(i64), P(i64)]),
     "gr_matrix_spmv_layout": (C.c_int, [vp, P(i32), P(i64), P(i64)]),
     "gr_host_matrix_decompose_vector": (C.c_int, [vp, vp, vp, C.c_int]),
     "gr_host_matrix_compose_vector": (C.c_int, [vp, vp, vp, C.c_int]),

@@ -299,6 +299,14 @@ int gr_host_matrix_row_to_tile(const gr_host_matrix* h, int32_t* row_to_tile) {
   });
 }
 
+int gr_host_matrix_edge_cut(const gr_host_matrix* h, int64_t* cut) {
+  return guarded([&] {
+    need(h, "matrix");
+    need(cut, "cut");
+    *cut = gr::edgeCut(*h->m, h->m->rowToTile);
+  });
+}
+
 int gr_host_matrix_tile_sizes(const gr_host_matrix* h, int64_t* out) {
   return guarded([&] {
     need(h, "matrix");
@@ -404,7 +412,7 @@ int gr_host_matrix_set_spmv_layout(gr_host_matrix* h, int32_t layout) {
 }
 
 int gr_host_matrix_check_spmv_layout(const gr_host_matrix* h, int32_t layout, int32_t* compact, int64_t* slots,
-                                     int64_t* far_entries) {
+                                     int64_t* far_entries, int64_t* max_chunk_far) {
   return guarded([&] {
     need(h, "matrix");
     gr::SellHost S = gr::buildSell(*h->m, layout);
@@ -412,6 +420,7 @@ int gr_host_matrix_check_spmv_layout(const gr_host_matrix* h, int32_t layout, in
     if (compact) *compact = S.compact ? 1 : 0;
     if (slots) *slots = S.slots;
     if (far_entries) *far_entries = static_cast<int64_t>(S.farCol.size());
+    if (max_chunk_far) *max_chunk_far = S.maxChunkFar;
   });
 }
 

@@ -88,7 +88,9 @@ struct SellMatrix {
 
 // Host image of the SELL layout of H (both encodings' arrays; the 16-bit
 // ones filled when `compact`). layout: 0 the 32-bit layout, 1 the 16-bit
-// layout, -1 the 16-bit layout when at most one entry in eight is far.
+// layout (GR_EUNSUPPORTED when a chunk has more than 64 far entries), -1
+// the 16-bit layout when it is allowed and at most one entry in eight is
+// far.
 struct SellHost {
   i64 slots = 0;
   bool compact = false;
@@ -96,6 +98,7 @@ struct SellHost {
   std::vector<double> val;
   std::vector<int16_t> d16;
   std::vector<i32> farCol, farBase;
+  i64 maxChunkFar = 0;  // most far entries in one chunk (the 16-bit layout allows 64)
 };
 SellHost buildSell(const HostMatrix& H, int layout);
 // Decodes the 16-bit arrays of S chunk by chunk, in the order the device's
@@ -422,8 +425,11 @@ struct DeviceMatrix {
   void updateValues(const std::vector<double>& localOff, const std::vector<double>& tileDiag);
   DBuf sellSrc;  // tile-local CRS entry of every SELL slot (-1: padding), built on the first update
   LevelSchedule& schedule(SweepEntries kind);
-  // Rounded-up kernel grid for a row loop of n rows.
+  // Grid of the row-chunk kernels (SpMV-dot, residual, PBiCGStab init): a
+  // block per 8 chunks, at most one wave of resident blocks (sellGridCap).
   int spmvBlocks() const;
+  int sellGridCap() const;
+  mutable int sellCap = 0;
   SpmvTuning spmvTuning[2];  // [float32 vectors, float64 vectors]
   // Set for a batch of systems (makeBatch): the Krylov kernels then keep one
   // state per system.
@@ -448,6 +454,11 @@ void preferSharedCarveout(const void* fn);
 
 // y = A x (reference CRSMatrix::spmv). xt == yt.
 void launchSpmv(DeviceMatrix& A, const void* x, void* y, DType t, cudaStream_t s);
+
+// Blocks of 256 threads per SM that every row-chunk Krylov kernel
+// (PBiCGStab init, both SpMV-dot kernels; float and double vectors) of
+// coefficient type vt and SELL layout c16 keeps resident.
+int sellKernelOccupancy(DType vt, bool c16);
 
 // SpMV autotuner: times every candidate launch geometry `reps` times on the
 // matrix's stream and keeps the fastest for vectors of type t. The results

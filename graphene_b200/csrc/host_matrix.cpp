@@ -198,8 +198,11 @@ void HostMatrix::buildFromGlobalCrs(i64 numTiles, gr_partitioner part, const i32
       case GR_PART_BFS:
         raw = partitionBfs(*this, static_cast<i32>(numTiles));
         break;
+      case GR_PART_MULTILEVEL:
+        raw = partitionMultilevel(*this, static_cast<i32>(numTiles));
+        break;
       case GR_PART_AUTO:
-        raw = coords.empty() ? partitionBfs(*this, static_cast<i32>(numTiles))
+        raw = coords.empty() ? partitionMultilevel(*this, static_cast<i32>(numTiles))
                              : partitionRcb(*this, static_cast<i32>(numTiles));
         break;
       default:

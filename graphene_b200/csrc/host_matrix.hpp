@@ -163,6 +163,11 @@ struct HostMatrix {
 std::vector<i32> partitionContiguous(const HostMatrix& A, i32 numParts);
 std::vector<i32> partitionRcb(const HostMatrix& A, i32 numParts);
 std::vector<i32> partitionBfs(const HostMatrix& A, i32 numParts);
+// Multilevel recursive bisection (partition.cpp): heavy-edge coarsening,
+// greedy growing, Fiduccia-Mattheyses refinement; weight = row entries + 1.
+std::vector<i32> partitionMultilevel(const HostMatrix& A, i32 numParts);
+// Off-diagonal entries whose column lies in another part than their row.
+i64 edgeCut(const HostMatrix& A, const std::vector<i32>& rowToTile);
 
 // Generators (rows sorted by column).
 struct GeneratedCsr {

@@ -254,8 +254,20 @@ SellHost buildSell(const HostMatrix& H, int layout) {
       farCount[c] = f;
     }
   });
-  i64 far = 0;
-  for (i64 c = 0; c < nChunks; ++c) far += farCount[c];
+  i64 far = 0, maxFar = 0;
+  for (i64 c = 0; c < nChunks; ++c) {
+    far += farCount[c];
+    maxFar = std::max<i64>(maxFar, farCount[c]);
+  }
+  S.maxChunkFar = maxFar;
+  // The device hands a chunk's far columns out of two registers of the
+  // warp's 32 lanes.
+  if (maxFar > dev::kSellMaxFar) {
+    if (layout == 1)
+      fail(GR_EUNSUPPORTED, "the 16-bit SpMV layout needs at most " + std::to_string(dev::kSellMaxFar) +
+                                " far columns per chunk of 32 rows (this matrix has " + std::to_string(maxFar) + ")");
+    return S;
+  }
   if (layout == -1 && far * 8 > acc) return S;
   S.compact = true;
   S.d16 = std::move(d16);
@@ -361,6 +373,7 @@ DeviceMatrix::DeviceMatrix(std::shared_ptr<HostMatrix> h) : host(std::move(h)) {
   iperm.upload(H.iperm);
 
   redBlocks = numSMs * 8;
+  sellGridCap();  // the occupancy query outside any stream capture
   partials.alloc(sizeof(double) * redBlocks * 8);
   counter.alloc(sizeof(unsigned) * 16);
   GR_CUDA(cudaMemsetAsync(counter.get(), 0, sizeof(unsigned) * 16, ownStream));
@@ -398,7 +411,7 @@ void DeviceMatrix::makeBatch(const std::vector<i64>& rowBegin, const std::vector
     r0[s] = static_cast<i32>(rowBegin[s]);
     r1[s] = static_cast<i32>(rowBegin[s] + rowReal[s]);
     const i64 chunks = (rowReal[s] + 31) / 32;
-    cBlocks[s] = static_cast<i32>(std::max<i64>(1, std::min<i64>((chunks + 7) / 8, redBlocks)));
+    cBlocks[s] = static_cast<i32>(std::max<i64>(1, std::min<i64>((chunks + 7) / 8, sellGridCap())));
     eBlocks[s] = static_cast<i32>(std::max<i64>(1, std::min<i64>(redBlocks, (rowReal[s] + 255) / 256)));
     cBlock0[s] = static_cast<i32>(cSys.size());
     eBlock0[s] = static_cast<i32>(eSys.size());
@@ -434,9 +447,19 @@ void DeviceMatrix::makeBatch(const std::vector<i64>& rowBegin, const std::vector
   batch = std::move(B);
 }
 
+int DeviceMatrix::sellGridCap() const {
+  if (sellCap == 0) {
+    // One wave: as many 256-thread blocks as the row-chunk Krylov kernels of
+    // this value type and SELL layout keep resident on every SM.
+    const int occ = sellKernelOccupancy(vt, sell.compact);
+    sellCap = std::max(1, std::min(redBlocks, numSMs * std::max(1, occ)));
+  }
+  return sellCap;
+}
+
 int DeviceMatrix::spmvBlocks() const {
   int need = (sell.nChunks + 7) / 8;
-  return std::max(1, std::min(need, redBlocks));
+  return std::max(1, std::min(need, sellGridCap()));
 }
 
 void DeviceMatrix::ensureLocalCrs() {
@@ -536,21 +559,21 @@ namespace dev {
 // y = A x. Every launch geometry (block size, grid, batch depth B) computes
 // each row with the same sequential sum, so the autotuner's choice never
 // changes y.
-template <class MV, class VT, int B>
+template <class MV, class VT, int B, bool C16>
 __global__ void __launch_bounds__(512) spmvKernel(SellView<MV> A, const VT* __restrict__ x,
                                                    VT* __restrict__ y) {
   const int lane = threadIdx.x & 31;
   const int nWarps = (gridDim.x * blockDim.x) >> 5;
   for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < A.nChunks; c += nWarps) {
     const int row = c * 32 + lane;
-    const VT v = sellRowSum<VT, MV, VT, B>(A, x, c, lane, row < A.n);
+    const VT v = sellRowSum<VT, MV, VT, C16, B>(A, x, c, lane, row < A.n);
     if (row < A.n) y[row] = v;
   }
 }
 
 // Residual with an IEEE intermediate type I (float or double):
 // r = (b - (d x + sum a x)) computed in I, stored as RT.
-template <class MV, class XT, class BT, class RT, class I>
+template <class MV, class XT, class BT, class RT, class I, bool C16>
 __global__ void __launch_bounds__(256) residualKernel(SellView<MV> A, const XT* __restrict__ x,
                                                        const BT* __restrict__ b,
                                                        RT* __restrict__ r, int normKind,
@@ -562,7 +585,7 @@ __global__ void __launch_bounds__(256) residualKernel(SellView<MV> A, const XT* 
   double part = redIdentity(normOp(normKind));
   for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < A.nChunks; c += nWarps) {
     const int row = c * 32 + lane;
-    const I sum = sellRowSum<I>(A, x, c, lane, row < A.n);
+    const I sum = sellRowSum<I, MV, XT, C16>(A, x, c, lane, row < A.n);
     if (row < A.n) {
       RT res = cvt<RT>(sub(cvt<I>(__ldg(b + row)), sum));
       r[row] = res;
@@ -580,7 +603,7 @@ __global__ void __launch_bounds__(256) residualKernel(SellView<MV> A, const XT* 
 
 // Residual with a double-word intermediate: x is double-word (two floats
 // per entry) or float, the matrix float, b and r float.
-template <bool XDW>
+template <bool XDW, bool C16>
 __global__ void __launch_bounds__(256) residualDwKernel(SellView<float> A, const float* __restrict__ x,
                                                          const float* __restrict__ b,
                                                          float* __restrict__ r, int normKind,
@@ -601,7 +624,7 @@ __global__ void __launch_bounds__(256) residualDwKernel(SellView<float> A, const
     const int row = c * 32 + lane;
     const bool live = row < A.n;
     dw sum = live ? dwTimesFp(ld(row), __ldg(A.diag + row)) : dw{0.0f, 0.0f};
-    ChunkWalk<float> w(A, c, lane);
+    ChunkWalk<float, C16> w(A, c, lane);
     for (int k = 0; k < w.K; k += 4) {
       int cl[4];
       float a[4];
@@ -672,11 +695,11 @@ void spmvT(DeviceMatrix& A, const void* x, void* y, const SpmvTuning& g, cudaStr
                                                 A.numSMs * 64));
   const auto* xv = static_cast<const VT*>(x);
   auto* yv = static_cast<VT*>(y);
-  switch (g.batch) {
-    case 4: dev::spmvKernel<MV, VT, 4><<<blocks, g.block, 0, s>>>(sellView<MV>(A), xv, yv); break;
-    case 16: dev::spmvKernel<MV, VT, 16><<<blocks, g.block, 0, s>>>(sellView<MV>(A), xv, yv); break;
-    default: dev::spmvKernel<MV, VT, 8><<<blocks, g.block, 0, s>>>(sellView<MV>(A), xv, yv); break;
-  }
+  const bool c16 = A.sell.compact;
+  auto kernel = g.batch == 4    ? (c16 ? dev::spmvKernel<MV, VT, 4, true> : dev::spmvKernel<MV, VT, 4, false>)
+                : g.batch == 16 ? (c16 ? dev::spmvKernel<MV, VT, 16, true> : dev::spmvKernel<MV, VT, 16, false>)
+                                : (c16 ? dev::spmvKernel<MV, VT, 8, true> : dev::spmvKernel<MV, VT, 8, false>);
+  kernel<<<blocks, g.block, 0, s>>>(sellView<MV>(A), xv, yv);
 }
 
 SpmvTuning& tuningFor(DeviceMatrix& A, DType t) { return A.spmvTuning[t == DType::F64 ? 1 : 0]; }
@@ -766,23 +789,20 @@ void launchResidual(DeviceMatrix& A, const void* x, DType xt, const void* b, DTy
   };
   if (inter == DType::DW) {
     if (A.vt != DType::F32 || bt != DType::F32 || rt != DType::F32) bad();
-    if (xt == DType::DW)
-      dev::residualDwKernel<true><<<blocks, 256, 0, s>>>(sellView<float>(A), static_cast<const float*>(x),
-                                                         static_cast<const float*>(b), static_cast<float*>(r),
-                                                         normKind, normOut, part, cnt);
-    else if (xt == DType::F32)
-      dev::residualDwKernel<false><<<blocks, 256, 0, s>>>(sellView<float>(A), static_cast<const float*>(x),
-                                                          static_cast<const float*>(b), static_cast<float*>(r),
-                                                          normKind, normOut, part, cnt);
-    else bad();
+    if (xt != DType::DW && xt != DType::F32) bad();
+    const bool c16 = A.sell.compact;
+    auto kernel = xt == DType::DW ? (c16 ? dev::residualDwKernel<true, true> : dev::residualDwKernel<true, false>)
+                                  : (c16 ? dev::residualDwKernel<false, true> : dev::residualDwKernel<false, false>);
+    kernel<<<blocks, 256, 0, s>>>(sellView<float>(A), static_cast<const float*>(x), static_cast<const float*>(b),
+                                  static_cast<float*>(r), normKind, normOut, part, cnt);
     checkLaunch("residual_dw");
     return;
   }
   if (xt == DType::DW) bad();
-#define GR_RES(MV, XT, BT, RT, IT)                                                                 \
-  dev::residualKernel<MV, XT, BT, RT, IT><<<blocks, 256, 0, s>>>(                                 \
-      sellView<MV>(A), static_cast<const XT*>(x), static_cast<const BT*>(b), static_cast<RT*>(r), \
-      normKind, normOut, part, cnt)
+#define GR_RES(MV, XT, BT, RT, IT)                                                                        \
+  (A.sell.compact ? dev::residualKernel<MV, XT, BT, RT, IT, true> : dev::residualKernel<MV, XT, BT, RT, IT, false>) \
+      <<<blocks, 256, 0, s>>>(sellView<MV>(A), static_cast<const XT*>(x), static_cast<const BT*>(b),        \
+                              static_cast<RT*>(r), normKind, normOut, part, cnt)
   const bool mf = A.vt == DType::F32;
   const int key = (xt == DType::F64) * 8 + (bt == DType::F64) * 4 + (rt == DType::F64) * 2 +
                   (inter == DType::F64);

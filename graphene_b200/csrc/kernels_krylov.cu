@@ -7,6 +7,7 @@
 // writes them into the device-resident KState, so an iteration runs without
 // host round trips. Every kernel returns immediately once KState::done is
 // set, which lets the host enqueue iterations ahead of the convergence test.
+#include <algorithm>
 #include <cmath>
 
 #include "devmath.cuh"
@@ -28,7 +29,7 @@ __device__ __forceinline__ bool converged(const KState* st) {
 }
 
 // r = b - A x and r0 = r, with the norm of r and r0 . r.
-template <class MV, class W>
+template <class MV, class W, bool C16>
 __global__ void __launch_bounds__(256) bicgInitKernel(SellView<MV> A, const W* __restrict__ x,
                                                        const W* __restrict__ b, W* __restrict__ r,
                                                        W* __restrict__ r0, KState* st, double* partials,
@@ -44,7 +45,7 @@ __global__ void __launch_bounds__(256) bicgInitKernel(SellView<MV> A, const W* _
   const int ops[2] = {normOp(nk), RED_SUM};
   for (int c = (sp.r0 >> 5) + ((sp.rank * blockDim.x + threadIdx.x) >> 5); c < cEnd; c += nWarps) {
     const int row = c * 32 + lane;
-    const W sum = sellRowSum<W>(A, x, c, lane, row < sp.r1);
+    const W sum = sellRowSum<W, MV, W, C16>(A, x, c, lane, row < sp.r1);
     if (row < sp.r1) {
       W res = sub(__ldg(b + row), sum);
       r[row] = res;
@@ -74,7 +75,7 @@ __global__ void __launch_bounds__(256) bicgInitKernel(SellView<MV> A, const W* _
 // mode 0: dot0 = r0 . y, alpha = rho / dot0 (pbicgstab/Solver.cpp:119-123)
 // mode 1: dot0 = y . s, dot1 = y . y, omega = dot0 / dot1, singularity
 //         check (pbicgstab/Solver.cpp:149-159)
-template <class MV, class W, int MODE>
+template <class MV, class W, int MODE, bool C16>
 __global__ void __launch_bounds__(256) spmvDotKernel(SellView<MV> A, const W* __restrict__ x,
                                                       W* __restrict__ y, const W* __restrict__ d1,
                                                       KState* st, double* partials, unsigned* counter,
@@ -90,7 +91,7 @@ __global__ void __launch_bounds__(256) spmvDotKernel(SellView<MV> A, const W* __
   const int ops[2] = {RED_SUM, RED_SUM};
   for (int c = (sp.r0 >> 5) + ((sp.rank * blockDim.x + threadIdx.x) >> 5); c < cEnd; c += nWarps) {
     const int row = c * 32 + lane;
-    const W yv = sellRowSum<W>(A, x, c, lane, row < sp.r1);
+    const W yv = sellRowSum<W, MV, W, C16>(A, x, c, lane, row < sp.r1);
     if (row < sp.r1) {
       y[row] = yv;
       const double yd = toDouble(yv);
@@ -509,23 +510,24 @@ Launch krylovLaunch(DeviceMatrix& A, bool chunk) {
 }
 }  // namespace
 
+namespace {
+template <class MV, class W>
+void bicgInitT(DeviceMatrix& A, const void* x, const void* b, void* r, void* r0, KState* st, cudaStream_t s,
+               bool stateless) {
+  const Launch L = krylovLaunch(A, true);
+  auto kernel = A.sell.compact ? dev::bicgInitKernel<MV, W, true> : dev::bicgInitKernel<MV, W, false>;
+  kernel<<<L.blocks, 256, 0, s>>>(sellView<MV>(A), static_cast<const W*>(x), static_cast<const W*>(b),
+                                  static_cast<W*>(r), static_cast<W*>(r0), st, L.partials, L.counter, L.seg,
+                                  stateless);
+}
+}  // namespace
+
 void launchBicgInit(DeviceMatrix& A, const void* x, const void* b, void* r, void* r0, KState* st, DType W,
                     cudaStream_t s, bool stateless) {
-  const Launch L = krylovLaunch(A, true);
-  if (A.vt == DType::F32 && W == DType::F32)
-    dev::bicgInitKernel<float, float><<<L.blocks, 256, 0, s>>>(
-        sellView<float>(A), static_cast<const float*>(x), static_cast<const float*>(b), static_cast<float*>(r),
-        static_cast<float*>(r0), st, L.partials, L.counter, L.seg, stateless);
-  else if (A.vt == DType::F32 && W == DType::F64)
-    dev::bicgInitKernel<float, double><<<L.blocks, 256, 0, s>>>(
-        sellView<float>(A), static_cast<const double*>(x), static_cast<const double*>(b), static_cast<double*>(r),
-        static_cast<double*>(r0), st, L.partials, L.counter, L.seg, stateless);
-  else if (A.vt == DType::F64 && W == DType::F64)
-    dev::bicgInitKernel<double, double><<<L.blocks, 256, 0, s>>>(
-        sellView<double>(A), static_cast<const double*>(x), static_cast<const double*>(b), static_cast<double*>(r),
-        static_cast<double*>(r0), st, L.partials, L.counter, L.seg, stateless);
-  else
-    fail(GR_EUNSUPPORTED, "PBiCGStab with float64 coefficients needs float64 vectors");
+  if (A.vt == DType::F32 && W == DType::F32) bicgInitT<float, float>(A, x, b, r, r0, st, s, stateless);
+  else if (A.vt == DType::F32 && W == DType::F64) bicgInitT<float, double>(A, x, b, r, r0, st, s, stateless);
+  else if (A.vt == DType::F64 && W == DType::F64) bicgInitT<double, double>(A, x, b, r, r0, st, s, stateless);
+  else fail(GR_EUNSUPPORTED, "PBiCGStab with float64 coefficients needs float64 vectors");
   checkLaunch("bicg_init");
 }
 
@@ -534,16 +536,36 @@ template <class MV, class W>
 void spmvDotT(DeviceMatrix& A, const void* x, void* y, const void* d1, int mode, KState* st, cudaStream_t s,
               bool stateless) {
   const Launch L = krylovLaunch(A, true);
-  if (mode == 0)
-    dev::spmvDotKernel<MV, W, 0><<<L.blocks, 256, 0, s>>>(sellView<MV>(A), static_cast<const W*>(x),
-                                                          static_cast<W*>(y), static_cast<const W*>(d1), st,
-                                                          L.partials, L.counter, L.seg, stateless);
-  else
-    dev::spmvDotKernel<MV, W, 1><<<L.blocks, 256, 0, s>>>(sellView<MV>(A), static_cast<const W*>(x),
-                                                          static_cast<W*>(y), static_cast<const W*>(d1), st,
-                                                          L.partials, L.counter, L.seg, stateless);
+  const bool c16 = A.sell.compact;
+  auto kernel = mode == 0 ? (c16 ? dev::spmvDotKernel<MV, W, 0, true> : dev::spmvDotKernel<MV, W, 0, false>)
+                          : (c16 ? dev::spmvDotKernel<MV, W, 1, true> : dev::spmvDotKernel<MV, W, 1, false>);
+  kernel<<<L.blocks, 256, 0, s>>>(sellView<MV>(A), static_cast<const W*>(x), static_cast<W*>(y),
+                                  static_cast<const W*>(d1), st, L.partials, L.counter, L.seg, stateless);
 }
 }  // namespace
+
+namespace {
+template <class MV, class W, bool C16>
+int occupancyOf() {
+  const void* fns[3] = {reinterpret_cast<const void*>(dev::bicgInitKernel<MV, W, C16>),
+                        reinterpret_cast<const void*>(dev::spmvDotKernel<MV, W, 0, C16>),
+                        reinterpret_cast<const void*>(dev::spmvDotKernel<MV, W, 1, C16>)};
+  int occ = 1 << 20;
+  for (const void* f : fns) {
+    int n = 0;
+    GR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, 256, 0));
+    occ = std::min(occ, n);
+  }
+  return occ;
+}
+}  // namespace
+
+int sellKernelOccupancy(DType vt, bool c16) {
+  if (vt == DType::F64) return c16 ? occupancyOf<double, double, true>() : occupancyOf<double, double, false>();
+  const int a = c16 ? occupancyOf<float, float, true>() : occupancyOf<float, float, false>();
+  const int b = c16 ? occupancyOf<float, double, true>() : occupancyOf<float, double, false>();
+  return std::min(a, b);
+}
 
 void launchSpmvDot(DeviceMatrix& A, const void* x, void* y, const void* d1, int mode, KState* st, DType W,
                    cudaStream_t s, bool stateless) {

@@ -7,9 +7,11 @@
 namespace gr {
 namespace dev {
 
-// 16-bit SELL layout codes (column - row is never 0 for an off-diagonal).
+// 16-bit SELL layout codes (column - row is never 0 for an off-diagonal),
+// and the most far columns one chunk may have.
 constexpr int kSellPad = 0;
 constexpr int kSellFar = -32768;
+constexpr int kSellMaxFar = 64;
 
 template <class MV>
 struct SellView {
@@ -59,31 +61,53 @@ __device__ __forceinline__ Acc loadX(const XT* __restrict__ x, int i) {
 }
 
 // The slots of SELL chunk c as one warp walks them, k = 0, 1, ... (all 32
-// lanes together: the 16-bit layout resolves far columns with warp votes).
-// Lane l reads the slots of row 32c + l.
-template <class MV>
+// lanes together: the 16-bit layout, C16, resolves far columns with warp
+// votes). Lane l reads the slots of row 32c + l.
+template <class MV, bool C16>
 struct ChunkWalk {
   int s0, K, lane, row;
-  int farBase = 0, nFar = 0, farRun = 0, farReg = 0;
+  int farRun = 0, farReg = 0, farReg2 = 0;
+  bool wide = false;  // more than 32 far columns: the second register too
 
   __device__ __forceinline__ ChunkWalk(const SellView<MV>& A, int c, int lane_) : lane(lane_) {
     row = c * 32 + lane;
     s0 = __ldg(A.base + c);
     K = (__ldg(A.base + c + 1) - s0) >> 5;
-    if (A.d16) {
-      farBase = __ldg(A.farBase + c);
-      nFar = __ldg(A.farBase + c + 1) - farBase;
-      // Up to 32 far columns of the chunk live in the lanes' registers and
-      // are handed out by shuffles; longer lists are read from memory.
-      if (nFar <= 32 && lane < nFar) farReg = __ldg(A.farCol + farBase + lane);
+    if constexpr (C16) {
+      const int farBase = __ldg(A.farBase + c);
+      const int nFar = __ldg(A.farBase + c + 1) - farBase;
+      // The chunk's far columns (at most kSellMaxFar = 64, checked on the
+      // host) live in two registers of the lanes and are handed out by
+      // shuffles.
+      if (lane < nFar) farReg = __ldg(A.farCol + farBase + lane);
+      wide = nFar > 32;
+      if (lane + 32 < nFar) farReg2 = __ldg(A.farCol + farBase + 32 + lane);
     }
+  }
+
+  // 16-bit layout: the column of a slot with code d (-1: padding). All 32
+  // lanes call it together, for their slots of the same k, in k order.
+  __device__ __forceinline__ int column(const SellView<MV>& A, int d) {
+    const bool far = d == kSellFar;
+    const unsigned vote = __ballot_sync(0xffffffffu, far);
+    int fc = 0;
+    if (vote) {  // warp-uniform
+      const int idx = farRun + __popc(vote & ((1u << lane) - 1u));
+      fc = __shfl_sync(0xffffffffu, farReg, idx & 31);
+      if (wide) {  // warp-uniform
+        const int hi = __shfl_sync(0xffffffffu, farReg2, idx & 31);
+        if (idx >= 32) fc = hi;
+      }
+      farRun += __popc(vote);
+    }
+    return d == kSellPad ? -1 : (far ? fc : row + d);
   }
 
   // Columns (-1: padding) and coefficients of slots k .. k+B-1 of this lane's
   // row. The loads of all B slots are issued before any is used.
   template <int B>
   __device__ __forceinline__ void load(const SellView<MV>& A, int k, int (&c)[B], MV (&a)[B]) {
-    if (A.d16) {
+    if constexpr (C16) {
       const short* dp = A.d16 + s0 + lane + 32 * k;
       const MV* vp = A.val + s0 + lane + 32 * k;
       short d[B];
@@ -93,20 +117,8 @@ struct ChunkWalk {
         d[j] = in ? __ldcs(dp + 32 * j) : static_cast<short>(kSellPad);
         a[j] = in ? __ldcs(vp + 32 * j) : MV(0);
       }
-      const unsigned below = (1u << lane) - 1u;
 #pragma unroll
-      for (int j = 0; j < B; ++j) {
-        const bool far = d[j] == kSellFar;
-        const unsigned vote = __ballot_sync(0xffffffffu, far);
-        int fc = 0;
-        if (vote) {  // warp-uniform
-          const int idx = farRun + __popc(vote & below);
-          if (nFar <= 32) fc = __shfl_sync(0xffffffffu, farReg, idx & 31);
-          else if (far) fc = __ldg(A.farCol + farBase + idx);
-          farRun += __popc(vote);
-        }
-        c[j] = d[j] == kSellPad ? -1 : (far ? fc : row + d[j]);
-      }
+      for (int j = 0; j < B; ++j) c[j] = column(A, d[j]);
     } else if constexpr (sizeof(MV) == 4) {
       const int2* p = A.ent + s0 + lane + 32 * k;
 #pragma unroll
@@ -136,15 +148,15 @@ struct ChunkWalk {
 // of up to B entries are issued before the dependent gathers of x so that a
 // warp keeps many memory requests in flight; the matrix stream is read with
 // evict-first loads so that x stays resident in L2.
-template <class Acc, class MV, class XT, int B = 8>
+template <class Acc, class MV, class XT, bool C16, int B = C16 ? 4 : 8>
 __device__ __forceinline__ Acc sellRowSum(const SellView<MV>& A, const XT* __restrict__ x, int c, int lane,
                                           bool live) {
-  ChunkWalk<MV> w(A, c, lane);
+  ChunkWalk<MV, C16> w(A, c, lane);
   const int row = w.row;
   Acc acc = live ? mul(cvt<Acc>(__ldg(A.diag + row)), loadX<Acc>(x, row)) : Acc(0);
   for (int k = 0; k < w.K; k += B) {
-    int cl[B];
     MV a[B];
+    int cl[B];
     w.template load<B>(A, k, cl, a);
     Acc xv[B];
 #pragma unroll

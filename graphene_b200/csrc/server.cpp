@@ -269,7 +269,7 @@ void Server::worker(int slot) {
         std::lock_guard<std::mutex> lk(mu_);
         e.hid = nullptr;  // no host matrix holds these values
         r->valuesUpdated = true;
-      } else if (e.hid != r->H.get()) {
+      } else if (!r->valuesOnly && e.hid != r->H.get()) {
         // Same structure, new values: upload them into the resident device
         // matrix and refactorise in place (no host layout work, no new
         // buffers, the captured iteration graphs stay valid).

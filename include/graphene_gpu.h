@@ -69,11 +69,13 @@ typedef enum { GR_NORM_L1 = 0, GR_NORM_L2 = 1, GR_NORM_LINF = 2, GR_NORM_NONE = 
  * (matrix/host/details/crs/CRSHostMatrix.cpp:139-271), which is not
  * available; these are this library's own deterministic partitioners. */
 typedef enum {
-  GR_PART_AUTO = 0,       /* RCB when grid coordinates exist, else BFS bisection */
+  GR_PART_AUTO = 0,       /* RCB when grid coordinates exist, else multilevel bisection */
   GR_PART_CONTIGUOUS = 1, /* equal-weight blocks in natural row order */
   GR_PART_RCB = 2,        /* recursive coordinate bisection (generated grids) */
   GR_PART_BFS = 3,        /* recursive BFS-level-structure graph bisection */
-  GR_PART_EXPLICIT = 4    /* caller-supplied rowToTile */
+  GR_PART_EXPLICIT = 4,   /* caller-supplied rowToTile */
+  GR_PART_MULTILEVEL = 5  /* multilevel recursive bisection, minimum edge cut, weight = row entries + 1
+                             (the role of METIS_PartGraphRecursive, CRSHostMatrix.cpp:139-271) */
 } gr_partitioner;
 
 typedef struct gr_host_matrix gr_host_matrix;
@@ -233,6 +235,11 @@ int gr_host_matrix_get_info(const gr_host_matrix* h, gr_matrix_info* out);
 /* Partitioning::rowToTile after empty-tile removal (CRSHostMatrix.cpp:235-270). */
 int gr_host_matrix_row_to_tile(const gr_host_matrix* h, int32_t* row_to_tile);
 
+/* Off-diagonal entries whose column lies in another tile than their row
+ * (each cut edge of a symmetric pattern counts twice). The reference logs
+ * METIS's edge cut after partitioning (CRSHostMatrix.cpp:233). */
+int gr_host_matrix_edge_cut(const gr_host_matrix* h, int64_t* cut);
+
 /* Per tile: {numInteriorRows, numSeperatorRows, numHaloRows}
  * (DistributedTileLayout.hpp:309-328). out has 3*num_tiles entries. */
 int gr_host_matrix_tile_sizes(const gr_host_matrix* h, int64_t* out);
@@ -297,18 +304,21 @@ int gr_host_matrix_check_gs_ring(const gr_host_matrix* h, int lower_only, gr_dty
  * columns, 1 16-bit column - row offsets with a side list for the columns
  * more than 32767 rows away (6 bytes a float slot instead of 8). Both
  * layouts give every row the same terms in the same order, so SpMV,
- * residual and solver results are identical. Automatic picks the 16-bit
- * layout when at most one entry in eight is far. No counterpart in the
+ * residual and solver results are identical. The 16-bit layout allows at
+ * most 64 far columns per chunk of 32 rows (GR_EUNSUPPORTED at device copy
+ * otherwise); automatic picks it when that holds and at most one entry in
+ * eight is far. No counterpart in the
  * reference (its CRS SpMV reads 32-bit local column indices,
  * matrix/details/crs/CRSMatrix.cpp:42-128). */
 int gr_host_matrix_set_spmv_layout(gr_host_matrix* h, int32_t layout);
 /* Builds the SpMV layout `layout` selects on the host and decodes every
  * slot of the 16-bit encoding, in the order the device's warps walk them,
  * against the 32-bit columns (GR_EINVAL on a mismatch). Reports whether
- * the 16-bit encoding was chosen, the slot count and the far entries. No
- * device needed; no counterpart in the reference. */
+ * the 16-bit encoding was chosen, the slot count, the far entries and the
+ * most far entries in one chunk. No device needed; no counterpart in the
+ * reference. */
 int gr_host_matrix_check_spmv_layout(const gr_host_matrix* h, int32_t layout, int32_t* compact, int64_t* slots,
-                                     int64_t* far_entries);
+                                     int64_t* far_entries, int64_t* max_chunk_far);
 int gr_host_matrix_load_vector_mm(const gr_host_matrix* h, const char* path, gr_dtype t, void* tile_ordered);
 
 /* Natural order <-> tile order (DistributedTileLayout::decomposeVector,

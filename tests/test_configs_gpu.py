@@ -28,8 +28,10 @@ Stated tolerances:
 * first k iterates (k <= 5): max |x - x_oracle| <= 1e-5 max |x_oracle|;
 * converged solves: iteration counts within max(2, 4 %) of the oracle's,
   both final residuals at the target, and ||x - x_oracle|| / ||x_oracle||
-  no larger than 100 x the solver tolerance (the distance of two solutions
-  that both meet the tolerance, for these matrices' conditioning);
+  at most 1e-4 in FP32 and 1e-5 (1000 x the solver tolerance) in FP64: two
+  solutions that both meet the 1e-8 residual lie up to about cond(A) x 1e-8
+  apart, and C2's FP64 ILU(0) solve stops at 81 iterations against the
+  oracle's 79, 1.7e-6 apart;
 * MPIR (C3): the same outer count, inner counts within 4 %, both FP64
   relative residuals of phi <= 1e-10, ||phi - phi_oracle|| / ||phi_oracle||
   <= 1e-8.
@@ -154,7 +156,7 @@ def test_c2_convection_diffusion(orc, c2, pre, vt):
     if st.converged:
         assert its_close(st.iterations, ost.iterations), (st.iterations, ost.iterations)
         assert st.finalResidual <= 1e-8 * st.initialResidual
-    assert rel(x, xo) <= (100 * 1e-8 if vt == "f64" else 1e-4)
+    assert rel(x, xo) <= (1000 * 1e-8 if vt == "f64" else 1e-4)
     for k in (1, 5):
         x, st, xo, ost, _ = solve_both(A, om, pbicgstab(pre, k, 0.0), b)
         assert st.iterations == ost.iterations == k

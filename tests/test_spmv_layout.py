@@ -37,23 +37,34 @@ def test_permuted_mesh_keeps_32_bit_automatically():
     # Cells in a random order: most couplings are far from their row.
     h = gb.generateLduMesh(48, 48, 48, 4, 5, 6, numTiles=1)
     auto = h.checkSpmvLayout(-1)
-    forced = h.checkSpmvLayout(1)
-    assert not auto["compact"]
-    assert forced["compact"] and far_fraction(forced) > 0.125
+    assert not auto["compact"] and auto["max_chunk_far"] > 64
+    with pytest.raises(gb.GrapheneError):
+        h.checkSpmvLayout(1)
 
 
-def test_many_far_entries_per_chunk():
-    """Chunks with more than 32 far columns (the device reads those from
-    memory instead of lane registers) and far columns on both sides."""
+def test_far_entries_per_chunk_limit():
+    """Two far columns a row give chunks of exactly 64 far columns, the most
+    the device hands out of the warp's lanes (two registers each); more are
+    refused for the 16-bit layout and make the automatic choice keep 32-bit
+    columns."""
     n = 150000
     r = np.arange(n)
-    rows = np.concatenate([r, r, r, r, r])
-    cols = np.concatenate([r, (r + 40000) % n, (r + 90000) % n, (r + 1) % n, (r + 120000) % n])
-    vals = np.concatenate([np.full(n, 8.0), np.full(4 * n, -1.0)])
+    rows = np.concatenate([r, r, r, r[:-1]])
+    cols = np.concatenate([r, (r + 40000) % n, (r + 90000) % n, r[:-1] + 1])
+    vals = np.concatenate([np.full(n, 8.0), np.full(3 * n - 1, -1.0)])
     h = gb.HostMatrix.from_coo(n, rows, cols, vals, 1)
     info = h.checkSpmvLayout(1)
-    assert info["compact"] and info["far"] >= 2 * n
-    assert not h.checkSpmvLayout(-1)["compact"]
+    assert info["compact"] and info["max_chunk_far"] == 64 and info["far"] == 2 * n
+    assert h.checkSpmvLayout(-1)["compact"] is False  # far fraction 2/3 > 1/8
+    rows = np.concatenate([rows, r])
+    cols = np.concatenate([cols, (r + 120000) % n])
+    vals = np.concatenate([vals, np.full(n, -1.0)])
+    h = gb.HostMatrix.from_coo(n, rows, cols, vals, 1)
+    with pytest.raises(gb.GrapheneError):
+        h.checkSpmvLayout(1)
+    info = h.checkSpmvLayout(-1)
+    assert not info["compact"] and info["max_chunk_far"] == 96
+    h.setSpmvLayout(1)  # accepted here; the device copy refuses it
 
 
 def test_ragged_rows_and_empty_rows():
