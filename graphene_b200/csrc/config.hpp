@@ -61,8 +61,10 @@ struct SolverConfig {
   // 32-bit layout.
   bool compactRing = true;
   // Level rings: 16-byte row records for the levels of 3 entries a row
-  // (ILU and Gauss-Seidel "recordLevels").
-  bool ringRecords = false;
+  // (ILU and Gauss-Seidel "recordLevels"). On by default: on B200 at 192^3
+  // with 2048 tiles the ILU(0) substitution ran in 108.6 us against 117.0
+  // without, with identical results.
+  bool ringRecords = true;
   // ILU "pairRows": in record levels each thread computes two rows at once.
   bool pairRows = false;
   // Extension: log2 of the streamed kernel's ring size in bytes (0: the

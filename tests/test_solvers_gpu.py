@@ -60,8 +60,8 @@ def ilu_config(kernel, **kw):
         c["kernel"] = "wring"
     if kernel == "ring_wide":
         c["compactRing"] = False
-    if kernel in ("ring_rec", "ring_pair", "wring_rec", "wring_pair", "wring_w4"):
-        c["recordLevels"] = True
+    # Record levels are the default; the plain names run without them.
+    c["recordLevels"] = kernel in ("ring_rec", "ring_pair", "wring_rec", "wring_pair", "wring_w4")
     if kernel in ("ring_pair", "wring_pair"):
         c["pairRows"] = True
     if kernel == "wring_w4":
