@@ -440,6 +440,7 @@ def serving(gb, requests=10000, slots=8, seed=7, rate_requests=2000, cold_reques
                 nxt += 1
         ids, pending = [], []
         lat, hits, conv = [], {0: 0, 1: 0, 2: 0}, True
+        phases = {"queue": [], "setup": [], "solve": [], "device_solve": []}
         first_arrival, last_finish = None, None
 
         def collect(block):
@@ -448,6 +449,10 @@ def serving(gb, requests=10000, slots=8, seed=7, rate_requests=2000, cold_reques
                 rid = pending.pop(0)
                 _, st, tm = srv.wait(rid)
                 lat.append(tm["finished_ms"] - tm["arrival_ms"])
+                phases["queue"].append(tm["admitted_ms"] - tm["arrival_ms"])
+                phases["setup"].append(tm["solve_start_ms"] - tm["admitted_ms"])
+                phases["solve"].append(tm["finished_ms"] - tm["solve_start_ms"])
+                phases["device_solve"].append(st.solveMs)
                 hits[tm["cache_hit"]] += 1
                 conv = conv and st.converged
                 first_arrival = tm["arrival_ms"] if first_arrival is None else min(first_arrival, tm["arrival_ms"])
@@ -477,7 +482,11 @@ def serving(gb, requests=10000, slots=8, seed=7, rate_requests=2000, cold_reques
                 "throughput_per_s": len(lat) / span,
                 "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                 "all_converged": conv, "fresh_values_on_resident_structure": hits[2],
-                "resident_same_matrix": hits[1], "new_pairs": hits[0]}
+                "resident_same_matrix": hits[1], "new_pairs": hits[0],
+                # Mean ms per request: waiting for a slot, values upload and
+                # refactorisation, the solve with b in and x out, and the
+                # solve's device time alone.
+                "phases_mean_ms": {k: float(np.mean(v)) for k, v in phases.items()}}
 
     out = {"requests": requests, "slots": slots, "generator_threads": threads,
            "edges": "U{16..96}", "mix": "70 % FP32 PBiCGStab-ILU(0) 1e-6, 30 % MPIR 1e-10",

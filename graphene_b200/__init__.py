@@ -557,6 +557,14 @@ class Matrix:
         check(_lib.lib().gr_matrix_update_values(self._m, h._h))
         self.host = h
 
+    def updateGlobalValues(self, gVal, gDiag) -> None:
+        """New coefficients from global CRS values (natural order, FP64),
+        gathered on the device (gr_matrix_update_global_values); solvers on
+        this matrix then need Solver.refresh()."""
+        gv = np.ascontiguousarray(gVal, dtype=np.float64)
+        gd = np.ascontiguousarray(gDiag, dtype=np.float64)
+        check(_lib.lib().gr_matrix_update_global_values(self._m, _ptr(gv), _ptr(gd)))
+
     def vectorNorm(self, norm: int, x) -> float:
         out = C.c_double()
         check(_lib.lib().gr_vector_norm(self._m, norm, _ptr(x), _dtype_of(x), C.byref(out)))

@@ -71,6 +71,7 @@ class RequestTimes(C.Structure):
         ("footprint_bytes", C.c_int64),
         ("cache_hit", C.c_int32),
         ("slot", C.c_int32),
+        ("solve_start_ms", C.c_double),
     ]
 
 
@@ -134,6 +135,7 @@ SIGNATURES = {
     "gr_host_matrix_structure_key": (C.c_int, [vp, P(C.c_uint64)]),
     "gr_matrix_update_values": (C.c_int, [vp, vp]),
     "gr_solver_refresh": (C.c_int, [vp]),
+    "gr_matrix_update_global_values": (C.c_int, [vp, vp, vp]),
     "gr_host_matrix_generate_values": (C.c_int, [vp, C.c_int, i64, i64, i64, P(C.c_double), C.c_uint64, vp, vp]),
     "gr_server_submit_values": (C.c_int, [vp, vp, vp, vp, C.c_char_p, vp, C.c_int, P(C.c_uint64)]),
     "gr_batch_create": (C.c_int, [P(vp), i32, C.c_char_p, P(vp)]),

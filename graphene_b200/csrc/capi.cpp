@@ -645,6 +645,15 @@ int gr_matrix_update_values(gr_matrix* A, gr_host_matrix* h) {
   });
 }
 
+int gr_matrix_update_global_values(gr_matrix* A, const double* g_val, const double* g_diag) {
+  return guarded([&] {
+    need(A, "matrix");
+    need(g_val, "g_val");
+    need(g_diag, "g_diag");
+    A->d->updateGlobalValues(g_val, g_diag);
+  });
+}
+
 int gr_solver_refresh(gr_solver* s) {
   return guarded([&] {
     need(s, "solver");

@@ -487,6 +487,28 @@ __global__ void sellScatterKernel(const int* __restrict__ src, const MV* __restr
 }
 }  // namespace dev
 
+namespace dev {
+// New coefficients from global CRS values (FP64, natural order) gathered on
+// the device: tile-local CRS off-diagonals, SELL slots (padding: 0) and the
+// tile-ordered diagonal, each rounded once to the coefficient type.
+template <class MV>
+__global__ void globalValuesKernel(const double* __restrict__ gVal, const double* __restrict__ gDiag,
+                                   const int* __restrict__ srcOff, const int* __restrict__ srcSell,
+                                   const int* __restrict__ iperm, MV* off, int2* ent, MV* val, MV* diag,
+                                   long long m, long long slots, int n) {
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  const long long i0 = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  for (long long p = i0; p < m; p += stride) off[p] = static_cast<MV>(gVal[srcOff[p]]);
+  for (long long s = i0; s < slots; s += stride) {
+    const int g = srcSell[s];
+    const MV v = g >= 0 ? static_cast<MV>(gVal[g]) : MV(0);
+    if (ent) ent[s].y = __float_as_int(static_cast<float>(v));
+    else val[s] = v;
+  }
+  for (long long p = i0; p < n; p += stride) diag[p] = static_cast<MV>(gDiag[iperm[p]]);
+}
+}  // namespace dev
+
 namespace {
 // Values converted to t and copied into an existing device buffer.
 void copyValuesInto(DBuf& dst, const std::vector<double>& v, DType t, cudaStream_t s) {
@@ -512,6 +534,50 @@ void DeviceMatrix::updateValues(std::shared_ptr<HostMatrix> h) {
     fail(GR_EINVAL, "updateValues needs a CRS matrix with this matrix's structure");
   updateValues(H.offDiag, H.diag);
   host = std::move(h);
+}
+
+void DeviceMatrix::updateGlobalValues(const double* gVal, const double* gDiag) {
+  if (batch || !host || !host->sumRank.empty() || host->format != GR_FORMAT_CRS ||
+      static_cast<i64>(host->localSrc.size()) != m)
+    fail(GR_EINVAL, "global values need a CRS matrix with its tile-local entry map");
+  if (!gVal || !gDiag) fail(GR_EINVAL, "values must not be NULL");
+  const HostMatrix& H = *host;
+  ensureLocalCrs();
+  if (!globalSrcOff.get()) {
+    // Slot and entry maps into the global CRS order, built once.
+    std::vector<i32> slotSrc(sell.slots, -1);
+    const SellHost S = buildSell(H, 0);
+    if (S.slots != sell.slots) fail(GR_EINVAL, "SELL layout mismatch");
+    // The tile-local CRS entry behind every slot: the constructor's slot
+    // assignment replayed.
+    parallelChunks(n, [&](i64 b, i64 e) {
+      for (i64 r = b; r < e; ++r) {
+        const i64 c = r / 32, lane = r % 32;
+        for (i64 k = 0; k < H.rowPtr[r + 1] - H.rowPtr[r]; ++k) {
+          const i64 p = H.rowPtr[r] + k;
+          slotSrc[S.base[c] + 32 * k + lane] = H.localSrc[p];
+        }
+      }
+    });
+    globalSrcOff.upload(H.localSrc);
+    globalSrcSell.upload(slotSrc);
+  }
+  DBuf gv(static_cast<size_t>(m) * sizeof(double)), gd(static_cast<size_t>(n) * sizeof(double));
+  GR_CUDA(cudaMemcpyAsync(gv.get(), gVal, static_cast<size_t>(m) * sizeof(double), cudaMemcpyHostToDevice, stream));
+  GR_CUDA(cudaMemcpyAsync(gd.get(), gDiag, static_cast<size_t>(n) * sizeof(double), cudaMemcpyHostToDevice, stream));
+  const i64 work = std::max<i64>(std::max<i64>(m, sell.slots), n);
+  const int blocks = static_cast<int>(std::max<i64>(1, std::min<i64>(numSMs * 8, (work + 255) / 256)));
+  if (vt == DType::F32)
+    dev::globalValuesKernel<float><<<blocks, 256, 0, stream>>>(
+        gv.as<double>(), gd.as<double>(), globalSrcOff.as<int>(), globalSrcSell.as<int>(), iperm.as<int>(),
+        offDiag.as<float>(), sell.compact ? nullptr : sell.ent.as<int2>(), sell.compact ? sell.val.as<float>() : nullptr,
+        diag.as<float>(), m, sell.slots, n);
+  else
+    dev::globalValuesKernel<double><<<blocks, 256, 0, stream>>>(
+        gv.as<double>(), gd.as<double>(), globalSrcOff.as<int>(), globalSrcSell.as<int>(), iperm.as<int>(),
+        offDiag.as<double>(), nullptr, sell.val.as<double>(), diag.as<double>(), m, sell.slots, n);
+  checkLaunch("global_values");
+  GR_CUDA(cudaStreamSynchronize(stream));  // gv, gd are released on return
 }
 
 void DeviceMatrix::updateValues(const std::vector<double>& localOff, const std::vector<double>& tileDiag) {

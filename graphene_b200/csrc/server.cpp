@@ -49,7 +49,7 @@ struct Server::Request {
   DType t = DType::F32;
   std::vector<unsigned char> b, x;
   i64 footprint = 0;
-  double tArrive = 0, tAdmit = 0, tFinish = 0;
+  double tArrive = 0, tAdmit = 0, tSolve = 0, tFinish = 0;
   gr_stats st{};
   int status = GR_OK, slot = -1;
   bool cacheHit = false, done = false, valuesUpdated = false;
@@ -261,10 +261,9 @@ void Server::worker(int slot) {
       }
       e.D->stream = stream;
       if (r->valuesOnly && r->cacheHit) {
-        // Values-only request on a resident structure.
-        std::vector<double> off, dg;
-        r->H->localValues(r->gVal.data(), r->gDiag.data(), off, dg);
-        e.D->updateValues(off, dg);
+        // Values-only request on a resident structure: the global values
+        // are gathered into place on the device.
+        e.D->updateGlobalValues(r->gVal.data(), r->gDiag.data());
         e.tree->refresh();
         std::lock_guard<std::mutex> lk(mu_);
         e.hid = nullptr;  // no host matrix holds these values
@@ -281,6 +280,7 @@ void Server::worker(int slot) {
         r->cacheHit = true;
         r->valuesUpdated = true;
       }
+      r->tSolve = now();
       r->st = e.tree->solveHost(r->x.data(), r->t, r->b.data(), r->t);
     } catch (const Error& ex) {
       r->status = ex.code;
@@ -336,6 +336,7 @@ int Server::wait(u64 id, double timeoutMs, void* x, gr_stats* stats, gr_request_
     times->footprint_bytes = r->footprint;
     times->cache_hit = r->valuesUpdated ? 2 : (r->cacheHit ? 1 : 0);
     times->slot = r->slot;
+    times->solve_start_ms = r->tSolve;
   }
   *status = r->status;
   *err = r->err;

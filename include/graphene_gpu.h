@@ -444,6 +444,14 @@ int gr_solver_phi(gr_solver* s, void* out, gr_dtype t);
  * new matrix and solver. */
 int gr_matrix_update_values(gr_matrix* A, gr_host_matrix* h);
 int gr_solver_refresh(gr_solver* s);
+/* New coefficients for A from global CRS values in natural order (g_val:
+ * off-diagonals in the order of gr_host_matrix_global_crs, g_diag: the
+ * diagonal; FP64, host memory), gathered into the device layout by a kernel:
+ * no host-side permutation or conversion. A must be a CRS matrix; results
+ * equal those of gr_matrix_update_values with a host matrix holding these
+ * values. Solvers on A then need gr_solver_refresh. No counterpart in the
+ * reference. */
+int gr_matrix_update_global_values(gr_matrix* A, const double* g_val, const double* g_diag);
 
 /* Name of the solver tree, e.g. "IterativeRefinement(PBiCGStab(ILU(0)))". */
 int gr_solver_name(const gr_solver* s, char* buf, size_t len);
@@ -482,6 +490,8 @@ typedef struct {
   int32_t cache_hit;   /* 1: the pair was already resident; 2: a pair with the
                           same structure was, and took this matrix's values */
   int32_t slot;
+  double solve_start_ms; /* values on the device and factorised: the solve (b in,
+                            iterations, x out) starts */
 } gr_request_times;
 
 int gr_server_create(const gr_server_config* cfg, gr_server** out);

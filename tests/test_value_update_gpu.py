@@ -67,6 +67,39 @@ def test_update_values_equals_fresh(name, vt):
         np.testing.assert_array_equal(host(x), host(x1))
 
 
+@pytest.mark.parametrize("name", ["ilu", "gs", "mpir"])
+@pytest.mark.parametrize("vt", [gb.FLOAT32, gb.FLOAT64])
+@pytest.mark.parametrize("layout", [0, 1])
+def test_update_global_values_equals_fresh(name, vt, layout):
+    """Matrix.updateGlobalValues (values gathered on the device from the
+    global CRS order) leaves the state a fresh matrix and solver would have,
+    in both SpMV layouts."""
+    if name == "mpir" and vt == gb.FLOAT64:
+        pytest.skip("IterativeRefinement works on float32 vectors")
+    dims, tiles = (17, 18, 19), 10
+    h0 = gb.generateMatrix(gb.GEN_VAR_POISSON, *dims, (1.0,), 5, tiles, valueType=vt)
+    h0.setSpmvLayout(layout)
+    gv, gd = gb.generateValues(h0, gb.GEN_VAR_POISSON, *dims, (1.0,), 6)
+    h1 = gb.generateMatrixLike(h0, gb.GEN_VAR_POISSON, *dims, (1.0,), 6)
+    h1.setSpmvLayout(layout)
+    dt = np.float32 if vt == gb.FLOAT32 else np.float64
+    b = gb.randomVector(7, h0.numRows).astype(dt)
+    A1 = h1.copyToTile()
+    x1 = dev(np.zeros_like(b))
+    st1 = gb.Solver(A1, CFGS[name]).solve(x1, dev(b))
+    A0 = h0.copyToTile()
+    assert A0.spmvLayout()["compact"] == bool(layout)
+    s0 = gb.Solver(A0, CFGS[name])
+    s0.solve(dev(np.zeros_like(b)), dev(b))
+    A0.updateGlobalValues(gv, gd)
+    s0.refresh()
+    np.testing.assert_array_equal(host(A0 * dev(b)), host(A1 * dev(b)))
+    x = dev(np.zeros_like(b))
+    st = s0.solve(x, dev(b))
+    assert st.iterations == st1.iterations and st.converged == st1.converged
+    np.testing.assert_array_equal(host(x), host(x1))
+
+
 def test_update_values_rejects_other_structures():
     h0 = gb.generateMatrix(gb.GEN_VAR_POISSON, 10, 10, 10, (1.0,), 1, 8)
     other = gb.generateMatrix(gb.GEN_VAR_POISSON, 10, 10, 10, (1.0,), 1, 9)
