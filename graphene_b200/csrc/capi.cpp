@@ -650,7 +650,7 @@ int gr_matrix_update_global_values(gr_matrix* A, const double* g_val, const doub
     need(A, "matrix");
     need(g_val, "g_val");
     need(g_diag, "g_diag");
-    A->d->updateGlobalValues(g_val, g_diag);
+    A->d->updateGlobalValues(g_val, g_diag, gr::DType::F64);
   });
 }
 

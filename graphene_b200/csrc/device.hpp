@@ -424,10 +424,10 @@ struct DeviceMatrix {
   // to the coefficient type here). The host matrix's own values go stale.
   void updateValues(const std::vector<double>& localOff, const std::vector<double>& tileDiag);
   DBuf sellSrc;  // tile-local CRS entry of every SELL slot (-1: padding), built on the first update
-  // The same from global CRS values (natural order, FP64, host pointers to
-  // m and n values), gathered into place on the device: no host-side
-  // permutation or conversion.
-  void updateGlobalValues(const double* gVal, const double* gDiag);
+  // The same from global CRS values (natural order; host pointers to m and
+  // n values of type t, FP64 or the coefficient type), gathered into place
+  // on the device: no host-side permutation.
+  void updateGlobalValues(const void* gVal, const void* gDiag, DType t);
   DBuf globalSrcOff, globalSrcSell;  // global CRS entry of every local entry / SELL slot (-1: padding)
   LevelSchedule& schedule(SweepEntries kind);
   // Grid of the row-chunk kernels (SpMV-dot, residual, PBiCGStab init): a

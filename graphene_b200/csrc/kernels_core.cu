@@ -491,8 +491,8 @@ namespace dev {
 // New coefficients from global CRS values (FP64, natural order) gathered on
 // the device: tile-local CRS off-diagonals, SELL slots (padding: 0) and the
 // tile-ordered diagonal, each rounded once to the coefficient type.
-template <class MV>
-__global__ void globalValuesKernel(const double* __restrict__ gVal, const double* __restrict__ gDiag,
+template <class MV, class SRC>
+__global__ void globalValuesKernel(const SRC* __restrict__ gVal, const SRC* __restrict__ gDiag,
                                    const int* __restrict__ srcOff, const int* __restrict__ srcSell,
                                    const int* __restrict__ iperm, MV* off, int2* ent, MV* val, MV* diag,
                                    long long m, long long slots, int n) {
@@ -536,7 +536,8 @@ void DeviceMatrix::updateValues(std::shared_ptr<HostMatrix> h) {
   host = std::move(h);
 }
 
-void DeviceMatrix::updateGlobalValues(const double* gVal, const double* gDiag) {
+void DeviceMatrix::updateGlobalValues(const void* gVal, const void* gDiag, DType t) {
+  if (t != DType::F64 && t != vt) fail(GR_EINVAL, "global values must be float64 or the coefficient type");
   if (batch || !host || !host->sumRank.empty() || host->format != GR_FORMAT_CRS ||
       static_cast<i64>(host->localSrc.size()) != m)
     fail(GR_EINVAL, "global values need a CRS matrix with its tile-local entry map");
@@ -562,20 +563,27 @@ void DeviceMatrix::updateGlobalValues(const double* gVal, const double* gDiag) {
     globalSrcOff.upload(H.localSrc);
     globalSrcSell.upload(slotSrc);
   }
-  DBuf gv(static_cast<size_t>(m) * sizeof(double)), gd(static_cast<size_t>(n) * sizeof(double));
-  GR_CUDA(cudaMemcpyAsync(gv.get(), gVal, static_cast<size_t>(m) * sizeof(double), cudaMemcpyHostToDevice, stream));
-  GR_CUDA(cudaMemcpyAsync(gd.get(), gDiag, static_cast<size_t>(n) * sizeof(double), cudaMemcpyHostToDevice, stream));
+  const size_t es = dtypeSize(t);
+  DBuf gv(static_cast<size_t>(m) * es), gd(static_cast<size_t>(n) * es);
+  GR_CUDA(cudaMemcpyAsync(gv.get(), gVal, static_cast<size_t>(m) * es, cudaMemcpyHostToDevice, stream));
+  GR_CUDA(cudaMemcpyAsync(gd.get(), gDiag, static_cast<size_t>(n) * es, cudaMemcpyHostToDevice, stream));
   const i64 work = std::max<i64>(std::max<i64>(m, sell.slots), n);
   const int blocks = static_cast<int>(std::max<i64>(1, std::min<i64>(numSMs * 8, (work + 255) / 256)));
-  if (vt == DType::F32)
-    dev::globalValuesKernel<float><<<blocks, 256, 0, stream>>>(
-        gv.as<double>(), gd.as<double>(), globalSrcOff.as<int>(), globalSrcSell.as<int>(), iperm.as<int>(),
-        offDiag.as<float>(), sell.compact ? nullptr : sell.ent.as<int2>(), sell.compact ? sell.val.as<float>() : nullptr,
-        diag.as<float>(), m, sell.slots, n);
+  int2* ent = vt == DType::F32 && !sell.compact ? sell.ent.as<int2>() : nullptr;
+  const int* so = globalSrcOff.as<int>();
+  const int* ss = globalSrcSell.as<int>();
+  if (vt == DType::F32 && t == DType::F32)
+    dev::globalValuesKernel<float, float><<<blocks, 256, 0, stream>>>(
+        gv.as<float>(), gd.as<float>(), so, ss, iperm.as<int>(), offDiag.as<float>(), ent,
+        ent ? nullptr : sell.val.as<float>(), diag.as<float>(), m, sell.slots, n);
+  else if (vt == DType::F32)
+    dev::globalValuesKernel<float, double><<<blocks, 256, 0, stream>>>(
+        gv.as<double>(), gd.as<double>(), so, ss, iperm.as<int>(), offDiag.as<float>(), ent,
+        ent ? nullptr : sell.val.as<float>(), diag.as<float>(), m, sell.slots, n);
   else
-    dev::globalValuesKernel<double><<<blocks, 256, 0, stream>>>(
-        gv.as<double>(), gd.as<double>(), globalSrcOff.as<int>(), globalSrcSell.as<int>(), iperm.as<int>(),
-        offDiag.as<double>(), nullptr, sell.val.as<double>(), diag.as<double>(), m, sell.slots, n);
+    dev::globalValuesKernel<double, double><<<blocks, 256, 0, stream>>>(
+        gv.as<double>(), gd.as<double>(), so, ss, iperm.as<int>(), offDiag.as<double>(), nullptr,
+        sell.val.as<double>(), diag.as<double>(), m, sell.slots, n);
   checkLaunch("global_values");
   GR_CUDA(cudaStreamSynchronize(stream));  // gv, gd are released on return
 }

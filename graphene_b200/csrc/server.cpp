@@ -55,7 +55,9 @@ struct Server::Request {
   bool cacheHit = false, done = false, valuesUpdated = false;
   // Values-only requests: H is the structure's template, these its values.
   bool valuesOnly = false;
-  std::vector<double> gVal, gDiag;
+  // The values rounded to the coefficient type once, at submission (what a
+  // resident pair uploads).
+  std::vector<unsigned char> gValT, gDiagT;
   std::string err;
   std::shared_ptr<Entry> entry;
 };
@@ -135,8 +137,21 @@ u64 Server::enqueue(std::shared_ptr<HostMatrix> H, const std::string& json, cons
   r->x.assign(bytes, 0);
   if (gVal) {
     r->valuesOnly = true;
-    r->gVal.assign(gVal, gVal + r->H->m);
-    r->gDiag.assign(gDiag, gDiag + r->H->n);
+    const i64 m = r->H->m, n = r->H->n;
+    if (r->H->valueType == DType::F32) {
+      // Rounded to float here, in the submitting thread.
+      r->gValT.resize(m * sizeof(float));
+      r->gDiagT.resize(n * sizeof(float));
+      float* fv = reinterpret_cast<float*>(r->gValT.data());
+      float* fd = reinterpret_cast<float*>(r->gDiagT.data());
+      for (i64 k = 0; k < m; ++k) fv[k] = static_cast<float>(gVal[k]);
+      for (i64 k = 0; k < n; ++k) fd[k] = static_cast<float>(gDiag[k]);
+    } else {
+      r->gValT.resize(m * sizeof(double));
+      r->gDiagT.resize(n * sizeof(double));
+      std::memcpy(r->gValT.data(), gVal, m * sizeof(double));
+      std::memcpy(r->gDiagT.data(), gDiag, n * sizeof(double));
+    }
   }
   r->footprint = estimateFootprint(*r->H, json, t);
   {
@@ -248,7 +263,20 @@ void Server::worker(int slot) {
       if (!e.ready && r->valuesOnly) {
         // A new pair for a values-only request: the template's layout with
         // the request's values.
-        auto M = HostMatrix::withGlobalValues(*r->H, r->gVal.data(), r->gDiag.data());
+        // The values as submitted were rounded to the coefficient type;
+        // widened back they round to themselves.
+        const i64 m = r->H->m, n = r->H->n;
+        std::vector<double> gv(m), gd(n);
+        if (r->H->valueType == DType::F32) {
+          const float* fv = reinterpret_cast<const float*>(r->gValT.data());
+          const float* fd = reinterpret_cast<const float*>(r->gDiagT.data());
+          for (i64 k = 0; k < m; ++k) gv[k] = fv[k];
+          for (i64 k = 0; k < n; ++k) gd[k] = fd[k];
+        } else {
+          std::memcpy(gv.data(), r->gValT.data(), m * sizeof(double));
+          std::memcpy(gd.data(), r->gDiagT.data(), n * sizeof(double));
+        }
+        auto M = HostMatrix::withGlobalValues(*r->H, gv.data(), gd.data());
         e.H = M;
         std::lock_guard<std::mutex> lk(mu_);
         e.hid = M.get();
@@ -263,7 +291,7 @@ void Server::worker(int slot) {
       if (r->valuesOnly && r->cacheHit) {
         // Values-only request on a resident structure: the global values
         // are gathered into place on the device.
-        e.D->updateGlobalValues(r->gVal.data(), r->gDiag.data());
+        e.D->updateGlobalValues(r->gValT.data(), r->gDiagT.data(), r->H->valueType);
         e.tree->refresh();
         std::lock_guard<std::mutex> lk(mu_);
         e.hid = nullptr;  // no host matrix holds these values
