@@ -108,7 +108,7 @@ SIGNATURES = {
     "gr_host_matrix_check_ilu_stream": (C.c_int, [vp, C.c_int, C.c_int, P(i32), P(i64)]),
     "gr_host_matrix_load_vector_mm": (C.c_int, [vp, C.c_char_p, C.c_int, vp]),
     "gr_host_matrix_check_ilu_ring": (C.c_int, [vp, C.c_int, C.c_int, i64, i32, i32, P(i64), P(i64), P(i32)]),
-    "gr_host_matrix_check_gs_ring": (C.c_int, [vp, C.c_int, C.c_int, i64, i32, P(i64), P(i64), P(i32)]),
+    "gr_host_matrix_check_gs_ring": (C.c_int, [vp, C.c_int, C.c_int, i64, i32, P(i64), P(i64), P(i32), P(i32)]),
     "gr_host_matrix_set_spmv_layout": (C.c_int, [vp, i32]),
     "gr_host_matrix_check_spmv_layout": (C.c_int, [vp, i32, P(i32), P(i64), P(i64), P(i64)]),
     "gr_matrix_spmv_layout": (C.c_int, [vp, P(i32), P(i64), P(i64)]),

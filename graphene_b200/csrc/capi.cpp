@@ -389,7 +389,7 @@ int gr_host_matrix_check_ilu_ring(const gr_host_matrix* h, int dilu, gr_dtype va
 
 int gr_host_matrix_check_gs_ring(const gr_host_matrix* h, int lower_only, gr_dtype value_type, int64_t ring_bytes,
                                  int32_t allow_compact, int64_t* ring_bytes_used, int64_t* stream_bytes,
-                                 int32_t* max_tile_levels) {
+                                 int32_t* max_tile_levels, int32_t* in_place) {
   return guarded([&] {
     need(h, "matrix");
     const gr::DType vt = gr::toDType(value_type);
@@ -400,6 +400,7 @@ int gr_host_matrix_check_gs_ring(const gr_host_matrix* h, int lower_only, gr_dty
     if (ring_bytes_used) *ring_bytes_used = R.ringBytes;
     if (stream_bytes) *stream_bytes = static_cast<int64_t>(R.bytes.size());
     if (max_tile_levels) *max_tile_levels = R.maxTileLevels;
+    if (in_place) *in_place = R.gsInPlace ? 1 : 0;
   });
 }
 

@@ -280,12 +280,16 @@ struct RingBudget {
 // with tile-local column c of row i reads slot c when c < i and nRows + c
 // otherwise (halo columns are >= nRows). The row's diagonal takes the
 // inverse diagonal's place in the level block, and the right-hand side
-// (nRows more slots) follows the array.
+// (nRows more slots) follows the array. In place (gsInPlace: every upper
+// entry of a tile lies in a later level than its row), the array is nRows +
+// nHalo + 1 slots: the start values are loaded into [0, nRows) and
+// overwritten row by row, and an entry reads slot c whatever its side.
 enum class RingKind { Ilu = 0, GaussSeidel = 1, GaussSeidelLower = 2 };
 
 struct HostRing {
   RingKind kind = RingKind::Ilu;
   i64 maxXSlots = 0;               // Gauss-Seidel: shared-memory x slots per tile (with the right-hand side)
+  bool gsInPlace = false;          // Gauss-Seidel: no sweep-start copy (upper entries read their own slot)
   std::vector<i32> haloStart;      // Gauss-Seidel: P + 1 offsets into haloSrc
   std::vector<i32> haloSrc;        // Gauss-Seidel: tile-order index of every tile's halo cells
   std::vector<uint8_t> bytes;
@@ -328,6 +332,7 @@ struct LevelRing {
   i64 bytes = 0, ringBytes = 0, nVal = 0, nInv = 0, maxGroupRows = 0, maxXSlots = 0;
   i32 maxTileLevels = 0, group = 1, numGroups = 0;
   bool compact = false;
+  bool gsInPlace = false;
   DBuf tileOffset, templ, meta, tileLevel, groupStart, valPos, valSrc, invPos, invSrc;
   DBuf haloStart, haloSrc;  // Gauss-Seidel rings
 };

@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
     const unsigned char* __restrict__ stream, const long long* __restrict__ tileOffset, const int4* __restrict__ meta,
     const int* __restrict__ tileLevel, const int* __restrict__ tileStart, const int* __restrict__ haloStart,
     const int* __restrict__ haloSrc, int ringBytes, int metaLevels, bool seedB, SPro<X> pro,
-    const X* __restrict__ xin, bool xinZero, X* __restrict__ xout, int* errFlag) {
+    const X* __restrict__ xin, bool xinZero, X* __restrict__ xout, int* errFlag, bool inPlace) {
   constexpr int kRingCompute = RingShape<W>::compute;
   constexpr int kRingLevelSync = RingShape<W>::levelSync;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -420,7 +420,9 @@ __global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
   int4* mt = reinterpret_cast<int4*>(smem + kRingHeader);
   unsigned char* ring = smem + kRingHeader + 16 * metaLevels;
   W* xs = reinterpret_cast<W*>(ring + ringBytes);  // this sweep | sweep start | halo | zero
-  W* rhs = xs + 2 * nRows + nHalo + 1;
+  const int s0 = inPlace ? 0 : nRows;               // start values (in place: this sweep's slots)
+  const int hb = s0 + nRows;                        // halo
+  W* rhs = xs + hb + nHalo + 1;
   const unsigned char* g = stream + tileOffset[T];
   const bool lead = threadIdx.x == kRingLevelSync;
   const volatile int* abortV = &abortFlag;
@@ -459,10 +461,10 @@ __global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
         }
       }
     }
-    for (int i = threadIdx.x; i < nRows; i += bd) xs[nRows + i] = xinZero ? W(0) : cvt<W>(xin[base + i]);
+    for (int i = threadIdx.x; i < nRows; i += bd) xs[s0 + i] = xinZero ? W(0) : cvt<W>(xin[base + i]);
     for (int h = threadIdx.x; h < nHalo; h += bd)
-      xs[2 * nRows + h] = xinZero ? W(0) : cvt<W>(xin[haloSrc[h0 + h]]);
-    if (lead) xs[2 * nRows + nHalo] = W(0);
+      xs[hb + h] = xinZero ? W(0) : cvt<W>(xin[haloSrc[h0 + h]]);
+    if (lead) xs[hb + nHalo] = W(0);
   }
   __syncthreads();
 
@@ -769,7 +771,7 @@ __global__ void __launch_bounds__(256) gsWarpRingKernel(
     const unsigned char* __restrict__ stream, const long long* __restrict__ tileOffset, const int4* __restrict__ meta,
     const int* __restrict__ tileLevel, const int* __restrict__ tileStart, const int* __restrict__ haloStart,
     const int* __restrict__ haloSrc, int P, int ringBytes, int metaLevels, uint32_t sliceBytes, bool seedB,
-    SPro<X> pro, const X* __restrict__ xin, bool xinZero, X* __restrict__ xout, int* errFlag) {
+    SPro<X> pro, const X* __restrict__ xin, bool xinZero, X* __restrict__ xout, int* errFlag, bool inPlace) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int w = static_cast<int>(threadIdx.x >> 5), lane = static_cast<int>(threadIdx.x & 31);
   const int T = static_cast<int>(blockIdx.x) * static_cast<int>(blockDim.x >> 5) + w;
@@ -785,7 +787,9 @@ __global__ void __launch_bounds__(256) gsWarpRingKernel(
   const int nRows = tileStart[T + 1] - base;
   const int h0 = haloStart[T];
   const int nHalo = haloStart[T + 1] - h0;
-  W* rhs = xs + 2 * nRows + nHalo + 1;
+  const int s0 = inPlace ? 0 : nRows;  // start values (in place: this sweep's slots)
+  const int hb = s0 + nRows;           // halo
+  W* rhs = xs + hb + nHalo + 1;
   const int lv0 = tileLevel[T];
   const int L = tileLevel[T + 1] - lv0;
   const unsigned char* g = stream + tileOffset[T];
@@ -836,10 +840,10 @@ __global__ void __launch_bounds__(256) gsWarpRingKernel(
     for (int j = 0; j < kRows; ++j) v[j] = !xinZero && i0 + j * 32 < nRows ? cvt<W>(xin[base + i0 + j * 32]) : W(0);
 #pragma unroll
     for (int j = 0; j < kRows; ++j)
-      if (i0 + j * 32 < nRows) xs[nRows + i0 + j * 32] = v[j];
+      if (i0 + j * 32 < nRows) xs[s0 + i0 + j * 32] = v[j];
   }
-  for (int h = lane; h < nHalo; h += 32) xs[2 * nRows + h] = xinZero ? W(0) : cvt<W>(xin[haloSrc[h0 + h]]);
-  if (lane == 0) xs[2 * nRows + nHalo] = W(0);
+  for (int h = lane; h < nHalo; h += 32) xs[hb + h] = xinZero ? W(0) : cvt<W>(xin[haloSrc[h0 + h]]);
+  if (lane == 0) xs[hb + nHalo] = W(0);
   __syncwarp();
   int l = 0;
   bool bad = false;
@@ -938,7 +942,7 @@ void gsRingT(DeviceMatrix& A, const LevelRing& R, const void* stream, const Prol
         static_cast<const unsigned char*>(stream), R.tileOffset.as<long long>(), R.meta.as<int4>(),
         R.tileLevel.as<int>(), R.groupStart.as<int>(), R.haloStart.as<int>(), R.haloSrc.as<int>(), R.numGroups,
         static_cast<int>(R.ringBytes), R.maxTileLevels, static_cast<uint32_t>(slice), seedB, pro,
-        static_cast<const X*>(xin), xinZero, static_cast<X*>(xout), A.errFlag.as<int>());
+        static_cast<const X*>(xin), xinZero, static_cast<X*>(xout), A.errFlag.as<int>(), R.gsInPlace);
     checkLaunch("gs_warp_ring");
     return;
   }
@@ -952,7 +956,7 @@ void gsRingT(DeviceMatrix& A, const LevelRing& R, const void* stream, const Prol
       static_cast<const unsigned char*>(stream), R.tileOffset.as<long long>(), R.meta.as<int4>(),
       R.tileLevel.as<int>(), R.groupStart.as<int>(), R.haloStart.as<int>(), R.haloSrc.as<int>(),
       static_cast<int>(R.ringBytes), R.maxTileLevels, seedB, pro, static_cast<const X*>(xin), xinZero,
-      static_cast<X*>(xout), A.errFlag.as<int>());
+      static_cast<X*>(xout), A.errFlag.as<int>(), R.gsInPlace);
   checkLaunch("gs_ring");
 }
 }  // namespace

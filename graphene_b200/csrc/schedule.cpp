@@ -414,11 +414,31 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
   // indices.
   i64 maxGsSlots = 0;
   std::vector<i32> haloStart, haloSrc;
+  // In place: every in-tile entry above the diagonal lies in a later level
+  // than its row (a lexicographically numbered box of a 7-point grid, for
+  // one), so when a row is updated its upper neighbours still hold their
+  // start values and the sweep needs no copy of them.
+  bool inPlace = gs;
+  if (gs && kind == RingKind::GaussSeidel) {
+    std::atomic<bool> ok{true};
+    parallelFor(H.P, [&](i64 T) {
+      const i64 base = H.tileStart[T], nRows = H.tileStart[T + 1] - base;
+      for (i64 r = 0; r < nRows && ok.load(std::memory_order_relaxed); ++r)
+        for (i64 k = H.rowPtr[base + r]; k < H.rowPtr[base + r + 1]; ++k) {
+          const i64 lc = H.colLocal[k];
+          if (lc > r && lc < nRows && H.lowerLevel[base + lc] <= H.lowerLevel[base + r]) {
+            ok = false;
+            break;
+          }
+        }
+    });
+    inPlace = ok;
+  }
   if (gs) {
     haloStart.assign(H.P + 1, 0);
     for (i32 T = 0; T < H.P; ++T) {
       haloStart[T + 1] = haloStart[T] + static_cast<i32>(H.tiles[T].nHalo);
-      maxGsSlots = std::max<i64>(maxGsSlots, 2 * H.tiles[T].rows() + H.tiles[T].nHalo + 1);
+      maxGsSlots = std::max<i64>(maxGsSlots, (inPlace ? 1 : 2) * H.tiles[T].rows() + H.tiles[T].nHalo + 1);
     }
     haloSrc.assign(haloStart[H.P], -1);
     parallelFor(H.P, [&](i64 T) {
@@ -437,7 +457,8 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
     const i64 gBase = H.tileStart[T0];
     const i64 gRows = H.tileStart[T1] - gBase;
     std::vector<i64> ent;
-    const i64 zeroSlot = gs ? 2 * gRows + H.tiles[T0].nHalo : gRows;
+    const i64 zeroSlot = gs ? (inPlace ? 1 : 2) * gRows + H.tiles[T0].nHalo : gRows;
+    const i64 startBase = inPlace ? 0 : gRows;  // Gauss-Seidel: where start values live
     for (int sweep = 0; sweep < (gs ? 1 : 2); ++sweep) {
       const bool upper = sweep == 1;
       const SweepEntries ekind = gs ? (kind == RingKind::GaussSeidelLower ? SweepEntries::Lower : SweepEntries::All)
@@ -481,7 +502,7 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
               i64 col = zeroSlot;
               if (real) {
                 const i64 lc = H.colLocal[ent[e]];
-                col = gs ? (lc < gl ? lc : gRows + lc) : lc + tb;
+                col = gs ? (lc < gl ? lc : startBase + lc) : lc + tb;
                 t.vals.emplace_back(start + 16 * q + 4 * e, static_cast<i32>(ent[e]));
               }
               c[e] = static_cast<uint32_t>(col);
@@ -516,7 +537,7 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
             i32 col = static_cast<i32>(zeroSlot);
             if (real) {
               const i64 lc = H.colLocal[ent[e]];
-              col = static_cast<i32>(gs ? (lc < gl ? lc : gRows + lc) : lc + tb);
+              col = static_cast<i32>(gs ? (lc < gl ? lc : startBase + lc) : lc + tb);
             }
             if (compact) {
               const uint16_t c16 = static_cast<uint16_t>(col);
@@ -639,6 +660,7 @@ HostRing buildLevelRing(const HostMatrix& H, bool dilu, DType vt, i64 ringBytes,
   R.compact = compact;
   R.kind = kind;
   R.maxXSlots = gs ? maxGsSlots + maxGroupRows : maxGroupRows + 1;
+  R.gsInPlace = gs && inPlace;
   R.haloStart = std::move(haloStart);
   R.haloSrc = std::move(haloSrc);
   R.tileOffset.assign(NG + 1, 0);
@@ -734,6 +756,7 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
       }
     }
     std::vector<char> doneL(gRows, 0), doneU(gRows, 0);
+    std::vector<i64> inLevel(gRows, -1);  // the level a row is in, once seen
     std::vector<i64> ringOff(L), size(L);
     i64 src = R.tileOffset[G], prevIa = -1;
     for (i64 l = 0; l < L; ++l) {
@@ -773,19 +796,31 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
       const uint8_t* blk = R.bytes.data() + src;
       std::vector<char>& done = upper ? doneU : doneL;
       std::vector<i64> rows(k);
-      for (i64 q = 0; q < k; ++q) {
+      auto rowId = [&](i64 q) {
         i32 il;
-        uint32_t recW01 = 0, recW2 = 0;
         if (rec) {
-          std::memcpy(&recW01, blk + 16 * q + 12, 4);
-          std::memcpy(&recW2, blk + lay.ents + recWord * q, 4);
-          il = static_cast<i32>(recW2 >> 16);
+          uint32_t w2;
+          std::memcpy(&w2, blk + lay.ents + recWord * q, 4);
+          il = static_cast<i32>(w2 >> 16);
         } else if (R.compact) {
           uint16_t r16;
           std::memcpy(&r16, blk + 2 * q, 2);
           il = r16;
         } else {
           std::memcpy(&il, blk + 4 * q, 4);
+        }
+        return il;
+      };
+      for (i64 q = 0; q < k; ++q) {  // the level's rows, for the in-place test
+        const i32 il = rowId(q);
+        if (il >= 0 && il < gRows) inLevel[il] = l;
+      }
+      for (i64 q = 0; q < k; ++q) {
+        const i32 il = rowId(q);
+        uint32_t recW01 = 0, recW2 = 0;
+        if (rec) {
+          std::memcpy(&recW01, blk + 16 * q + 12, 4);
+          std::memcpy(&recW2, blk + lay.ents + recWord * q, 4);
         }
         if (il < 0 || il >= gRows || done[il]) bad(G, l, "row id");
         rows[q] = il;
@@ -802,12 +837,19 @@ void checkLevelRing(const HostMatrix& H, const HostRing& R, bool dilu, DType vt)
           }
           if (gs) {
             // New value of an earlier row, start value of a later row or of
-            // a halo cell, or the zero slot (lower-only rings: no start values).
+            // a halo cell, or the zero slot (lower-only rings: no start
+            // values). In place, a later row's start value is its own slot,
+            // which no row of this or an earlier level may have written.
             const bool lowerOnly = R.kind == RingKind::GaussSeidelLower;
-            if (c < 0 || c > 2 * gRows + nHalo) bad(G, l, "column index");
-            if (c < gRows && (!done[c] || c >= il)) bad(G, l, "dependency order");
-            if (c >= gRows && c < 2 * gRows && (lowerOnly || c - gRows <= il)) bad(G, l, "start value");
-            if (c >= 2 * gRows && c < 2 * gRows + nHalo && lowerOnly) bad(G, l, "halo in a lower-only ring");
+            const i64 haloBase = (R.gsInPlace ? 1 : 2) * gRows;
+            if (c < 0 || c > haloBase + nHalo) bad(G, l, "column index");
+            if (c < gRows && c < il && !done[c]) bad(G, l, "dependency order");
+            if (c < gRows && c >= il) {
+              if (!R.gsInPlace || c == il || lowerOnly) bad(G, l, "dependency order");
+              if (done[c] || inLevel[c] == l) bad(G, l, "start value overwritten");
+            }
+            if (!R.gsInPlace && c >= gRows && c < 2 * gRows && (lowerOnly || c - gRows <= il)) bad(G, l, "start value");
+            if (c >= haloBase && c < haloBase + nHalo && lowerOnly) bad(G, l, "halo in a lower-only ring");
             continue;
           }
           if (c < 0 || c > gRows) bad(G, l, "column index");
@@ -862,6 +904,7 @@ LevelRing& DeviceMatrix::levelRing(bool dilu, i64 ringBytes, i32 group, bool all
   R->invSrc.upload(H.invSrc);
   R->kind = H.kind;
   R->maxXSlots = H.maxXSlots;
+  R->gsInPlace = H.gsInPlace;
   if (H.kind != RingKind::Ilu) {
     R->haloStart.upload(H.haloStart);
     if (!H.haloSrc.empty()) R->haloSrc.upload(H.haloSrc);

@@ -289,10 +289,13 @@ int gr_host_matrix_check_ilu_ring(const gr_host_matrix* h, int dilu, gr_dtype va
  * every entry must read this sweep's value of an earlier row of its tile,
  * the sweep-start value of a later row or of a halo cell, or the zero slot
  * (lower_only: the ring of a sweep from x = 0, which keeps only the entries
- * of earlier rows). Host only. No counterpart in the reference. */
+ * of earlier rows). *in_place: the ring keeps no sweep-start copy because
+ * every later row an entry reads lies in a later level (its slot still
+ * holds the start value; checked). Host only. No counterpart in the
+ * reference. */
 int gr_host_matrix_check_gs_ring(const gr_host_matrix* h, int lower_only, gr_dtype value_type, int64_t ring_bytes,
                                  int32_t allow_compact, int64_t* ring_bytes_used, int64_t* stream_bytes,
-                                 int32_t* max_tile_levels);
+                                 int32_t* max_tile_levels, int32_t* in_place);
 
 /* DistributedTileLayout::loadVectorFromFile (DistributedTileLayout.cpp:185-206,
  * without halo): reads a MatrixMarket vector (a "vector" object, coordinate

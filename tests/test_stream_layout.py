@@ -122,10 +122,13 @@ def test_ring_replay_192_workload():
 
 # ---- Gauss-Seidel level ring -------------------------------------------------------------
 
-def check_gs_ring(h, lower_only, vt=gb.FLOAT32, ring_bytes=0, compact=True):
-    used, nbytes, lv = C.c_int64(), C.c_int64(), C.c_int32()
+def check_gs_ring(h, lower_only, vt=gb.FLOAT32, ring_bytes=0, compact=True, want_in_place=False):
+    used, nbytes, lv, ip = C.c_int64(), C.c_int64(), C.c_int32(), C.c_int32()
     gb._lib.check(gb._lib.lib().gr_host_matrix_check_gs_ring(h._h, int(lower_only), vt, ring_bytes, int(compact),
-                                                              C.byref(used), C.byref(nbytes), C.byref(lv)))
+                                                              C.byref(used), C.byref(nbytes), C.byref(lv),
+                                                              C.byref(ip)))
+    if want_in_place:
+        return used.value, nbytes.value, lv.value, bool(ip.value)
     return used.value, nbytes.value, lv.value
 
 
@@ -170,11 +173,29 @@ def test_gs_ring_replay_random_and_ldu(seed):
 
 
 def test_gs_ring_replay_convdiff_workload():
-    """The 128^3 convection-diffusion system at its 1024 tiles."""
+    """The 128^3 convection-diffusion system at its 1024 tiles: boxes of a
+    7-point grid, so the sweep runs in place (no sweep-start copy)."""
     h = gb.generateMatrix(gb.GEN_CONVDIFF, 128, 128, 128, (0.5, 0.25, 0.125), 0, 1024)
     for lower_only in (False, True):
-        used, nbytes, lv = check_gs_ring(h, lower_only)
-        assert used >= 4096 and lv < 64
+        used, nbytes, lv, ip = check_gs_ring(h, lower_only, want_in_place=True)
+        assert used >= 4096 and lv < 64 and ip
+
+
+def test_gs_ring_in_place_only_when_safe():
+    """In place needs every in-tile upper entry in a later level than its
+    row: true whenever the pattern is structurally symmetric (entry (r, c)
+    above the diagonal has (c, r) below it, so c's level exceeds r's), false
+    for a nonsymmetric random pattern whose upper neighbours can sit in
+    earlier levels; the replay checks both."""
+    h = gb.generate3DPoissonMatrix(gb.FLOAT32, 16, 16, 16, 8, gb.PART_RCB)
+    assert check_gs_ring(h, False, want_in_place=True)[3]
+    n, r, c, v = random_coo(400, 0.03, 1)
+    assert check_gs_ring(gb.HostMatrix.from_coo(n, r, c, v, 3, partitioner=gb.PART_BFS), False,
+                         want_in_place=True)[3]
+    n, r, c, v = random_coo(300, 0.04, 1, symmetric=False)
+    hr = gb.HostMatrix.from_coo(n, r, c, v, 1)
+    assert not check_gs_ring(hr, False, want_in_place=True)[3]
+    assert check_gs_ring(hr, True, want_in_place=True)[3]  # lower-only rings have no upper entries
 
 
 def test_ring_record_levels_same_bytes():
