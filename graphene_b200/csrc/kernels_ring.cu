@@ -931,6 +931,7 @@ void gsRingT(DeviceMatrix& A, const LevelRing& R, const void* stream, const Prol
     fail(GR_EINVAL, "a lower-only Gauss-Seidel ring sweeps from x = 0 only");
   if (warps > 0) {
     if (warps > 8) fail(GR_EINVAL, "warpsPerBlock must be 1..8");
+    if (p.stIndex) fail(GR_EUNSUPPORTED, "batched solves use the block ring kernel");
     const size_t slice = gsWarpRingSlice(R, dtypeOf<W>());
     const size_t smem = slice * static_cast<size_t>(warps);
     auto kernel = R.compact ? dev::gsWarpRingKernel<MV, X, W, true> : dev::gsWarpRingKernel<MV, X, W, false>;
@@ -950,8 +951,9 @@ void gsRingT(DeviceMatrix& A, const LevelRing& R, const void* stream, const Prol
   auto kernel = R.compact ? dev::gsRingKernel<MV, X, W, true> : dev::gsRingKernel<MV, X, W, false>;
   ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
   preferSharedCarveout(reinterpret_cast<const void*>(kernel));
+  // Batches: the state of tile T's system is st[stIndex[T]].
   dev::SPro<X> pro{static_cast<int>(p.kind), static_cast<const X*>(p.b), static_cast<const X*>(p.r),
-                   static_cast<X*>(p.pOrS), static_cast<const X*>(p.v), p.st, nullptr};
+                   static_cast<X*>(p.pOrS), static_cast<const X*>(p.v), p.st, p.stIndex};
   kernel<<<R.numGroups, dev::RingShape<W>::threads, smem, s>>>(
       static_cast<const unsigned char*>(stream), R.tileOffset.as<long long>(), R.meta.as<int4>(),
       R.tileLevel.as<int>(), R.groupStart.as<int>(), R.haloStart.as<int>(), R.haloSrc.as<int>(),

@@ -234,6 +234,8 @@ class GsNode : public Node {
   // right-hand side (the level-ring kernel), and that application:
   // numFixedIterations sweeps from x = 0.
   bool fusedPrologue() const { return ring_ != nullptr && cfg_.numFixedIterations > 0; }
+  // The block ring kernel (one block per tile, which batches need).
+  bool blockRing() const { return ring_ != nullptr && cfg_.gsKernel != 3; }
   void applyFused(const PrologueArgs& pro, void* out, DType W) {
     ringSweeps(pro, out, W, cfg_.numFixedIterations, true);
   }
@@ -344,6 +346,7 @@ class GsNode : public Node {
     plain.kind = Prologue::Plain;
     plain.b = first.kind == Prologue::Plain ? first.b : first.pOrS;
     plain.st = first.st;
+    plain.stIndex = first.stIndex;
     void* cur = x;
     void* other = tmp_.get();
     for (int k = 0; k < count; ++k) {
@@ -406,9 +409,13 @@ class PbicgstabNode : public Node {
     }
     if (A.batch) {
       // A batch keeps one state per system; its preconditioner must look
-      // up a block's system, which the ring substitution kernel does.
-      if (!ilu_ || !ilu_->ringKernel())
-        fail(GR_EUNSUPPORTED, "batched PBiCGStab needs the ILU preconditioner with the ring kernel");
+      // up a block's system, which the block ring kernels (ILU substitution,
+      // Gauss-Seidel sweeps) do.
+      const bool iluOk = ilu_ && ilu_->ringKernel();
+      const bool gsOk = gs_ && gs_->fusedPrologue() && gs_->blockRing();
+      if (!iluOk && !gsOk)
+        fail(GR_EUNSUPPORTED, "batched PBiCGStab needs the ILU preconditioner with the ring kernel, or Gauss-Seidel "
+                              "with numFixedIterations > 0 on the block ring kernel");
       systems_ = A.batch->systems;
       GR_CUDA(cudaMallocHost(&host_, sizeof(KState) * systems_ + sizeof(int)));
       batchHost_ = true;

@@ -69,6 +69,23 @@ def test_batch_equals_solo(vt, dt):
     assert all(st.converged for st in sts)
 
 
+@pytest.mark.parametrize("vt,dt", [(gb.FLOAT32, np.float32), (gb.FLOAT64, np.float64)])
+def test_batch_gauss_seidel_equals_solo(vt, dt):
+    """PBiCGStab with Gauss-Seidel (2 sweeps) over a batch: the sweeps'
+    kernel looks up each tile's system like the ILU substitution does."""
+    hs = systems(vt)
+    bs = rhs(hs, dt, seed=21)
+    c = cfg(tol=1e-6 if dt == np.float32 else 1e-10,
+            extra={"preconditioner": {"type": "GaussSeidel", "numFixedIterations": 2, "kernel": "ring"}})
+    xs, sts = gb.Batch(hs, c).solveHost(bs)
+    for h, b, x, st in zip(hs, bs, xs, sts):
+        xr, sr = solo(h, c, b)
+        np.testing.assert_array_equal(x, xr)
+        assert st.iterations == sr.iterations and st.converged == sr.converged
+        assert st.finalResidual == sr.finalResidual
+    assert all(st.converged for st in sts)
+
+
 def test_batch_solutions_accurate():
     import scipy.sparse as sp
     import scipy.sparse.linalg as spl
@@ -128,6 +145,8 @@ def test_batch_many_small_systems():
     cfg(prec="GaussSeidel"),
     {"type": "PBiCGStab", "maxIterations": 10, "relTolerance": 1e-6},
     cfg(extra={"preconditioner": {"type": "ILU", "kernel": "warp"}}),
+    cfg(extra={"preconditioner": {"type": "GaussSeidel", "numFixedIterations": 2, "kernel": "wring"}}),
+    cfg(extra={"preconditioner": {"type": "GaussSeidel", "numFixedIterations": 2, "kernel": "levels"}}),
 ])
 def test_batch_rejects_unsupported_configs(bad):
     hs = systems(gb.FLOAT32, SYSTEMS[:2])
