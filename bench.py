@@ -322,7 +322,7 @@ def other_configs(gb, peak):
             out["convdiff128_gs_sweep"] = {"ms": ms, "bytes_per_sweep": byts,
                                            "GBs": byts / (ms * 1e-3) / 1e9,
                                            "frac_of_hbm": byts / (ms * 1e-3) / 1e9 / peak,
-                                           "kernel": "gsRingKernel"}
+                                           "kernel": "gsWarpRingKernel (one warp per tile)"}
             del gs1, xg
         del A
     # 100^3 LDU mesh (jittered, permuted), Gauss-Seidel PBiCGStab to 1e-8,

@@ -87,9 +87,10 @@ struct SolverConfig {
   // alpha, beta, omega and the convergence test in float, as the reference
   // computes them (float32 vectors only).
   bool reduceRef = false;
-  // Gauss-Seidel sweep kernel: 0 auto (the level ring when a tile fits
-  // shared memory), 1 the level ring, 2 level schedules in global memory,
-  // 3 the level ring with one warp per tile.
+  // Gauss-Seidel sweep kernel: 0 auto (the level ring with one warp per
+  // tile when a tile fits shared memory, a block per tile in batches), 1
+  // the level ring with a block per tile, 2 level schedules in global
+  // memory, 3 the level ring with one warp per tile.
   int gsKernel = 0;
   // IterativeRefinement (iterative-refinement/Configuration.hpp:23-25)
   int extendedPrecisionType = -1;  // -1: the type of x

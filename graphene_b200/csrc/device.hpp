@@ -87,10 +87,9 @@ struct SellMatrix {
 };
 
 // Host image of the SELL layout of H (both encodings' arrays; the 16-bit
-// ones filled when `compact`). layout: 0 the 32-bit layout, 1 the 16-bit
-// layout (GR_EUNSUPPORTED when a chunk has more than 64 far entries), -1
-// the 16-bit layout when it is allowed and at most one entry in eight is
-// far.
+// ones filled when `compact`). layout: 0 or -1 (automatic) the 32-bit
+// layout, 1 the 16-bit layout (GR_EUNSUPPORTED when a chunk has more than
+// 64 far entries).
 struct SellHost {
   i64 slots = 0;
   bool compact = false;

