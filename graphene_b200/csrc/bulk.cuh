@@ -157,34 +157,6 @@ struct SPro {
       if (in[j]) pOrS[i0 + j * stride] = out[j];
     }
   }
-  // The same for rows i0 + j * stride (j < 4, rows below n), all loads
-  // issued before any store, so that the four rows' loads overlap.
-  __device__ __forceinline__ void four(int i0, int stride, int n, W beta, W omega, W alpha, bool first,
-                                       W (&out)[4]) const {
-    bool in[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) in[j] = i0 + j * stride < n;
-    if (kind == static_cast<int>(Prologue::Plain)) {
-#pragma unroll
-      for (int j = 0; j < 4; ++j) out[j] = in[j] ? b[i0 + j * stride] : W(0);
-      return;
-    }
-    W rr[4], pp[4], vv[4];
-    const bool pu = kind == static_cast<int>(Prologue::PUpdate);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int i = i0 + j * stride;
-      rr[j] = in[j] ? r[i] : W(0);
-      pp[j] = in[j] && pu && !first ? pOrS[i] : W(0);
-      vv[j] = in[j] && !(pu && first) ? v[i] : W(0);
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      if (pu) out[j] = first ? rr[j] : add(rr[j], mul(beta, sub(pp[j], mul(omega, vv[j]))));
-      else out[j] = sub(rr[j], mul(alpha, vv[j]));
-      if (in[j]) pOrS[i0 + j * stride] = out[j];
-    }
-  }
 };
 
 

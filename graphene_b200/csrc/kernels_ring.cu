@@ -232,13 +232,16 @@ __global__ void __launch_bounds__(RingShape<W>::threads) iluRingKernel(const uns
       alpha = cvt<W>(st->alpha);
       first = st->iter == 0;
     }
+    // kPro rows a thread at once, all loads before any store: a tile's
+    // prologue is a few round trips to HBM rather than one per 4 rows.
+    constexpr int kPro = sizeof(W) == 4 ? 8 : 4;
     const int bd = static_cast<int>(blockDim.x);
-    for (int i0 = threadIdx.x; i0 < nRows; i0 += 4 * bd) {
-      W v4[4];
-      pro.four(base + i0, bd, base + nRows, beta, omega, alpha, first, v4);
+    for (int i0 = threadIdx.x; i0 < nRows; i0 += kPro * bd) {
+      W v[kPro];
+      pro.template rows<kPro>(base + i0, bd, base + nRows, beta, omega, alpha, first, v);
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (i0 + j * bd < nRows) xs[i0 + j * bd] = v4[j];
+      for (int j = 0; j < kPro; ++j)
+        if (i0 + j * bd < nRows) xs[i0 + j * bd] = v[j];
     }
     if (lead) xs[nRows] = W(0);
   }
@@ -451,13 +454,14 @@ __global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
         alpha = cvt<X>(st->alpha);
         first = st->iter == 0;
       }
-      for (int i0 = threadIdx.x; i0 < nRows; i0 += 4 * bd) {
-        X v4[4];
-        pro.four(base + i0, bd, base + nRows, beta, omega, alpha, first, v4);
+      constexpr int kPro = sizeof(X) == 4 ? 8 : 4;  // rows a thread at once, loads before stores
+      for (int i0 = threadIdx.x; i0 < nRows; i0 += kPro * bd) {
+        X v[kPro];
+        pro.template rows<kPro>(base + i0, bd, base + nRows, beta, omega, alpha, first, v);
         if (seedB) {
 #pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (i0 + j * bd < nRows) rhs[i0 + j * bd] = cvt<W>(v4[j]);
+          for (int j = 0; j < kPro; ++j)
+            if (i0 + j * bd < nRows) rhs[i0 + j * bd] = cvt<W>(v[j]);
         }
       }
     }
