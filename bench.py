@@ -4,7 +4,8 @@
 Workload (one "step"): Matrix::solve(x, b, config) on the 192^3
 variable-coefficient 7-point Poisson system (7,077,888 rows, 42,246,144
 off-diagonals; cell coefficients log-normal sigma = 1.5 from seed 2,
-harmonic-mean faces, Dirichlet boundary), float32 CRS in 2048 tiles,
+harmonic-mean faces, Dirichlet boundary), float32 CRS in 2368 tiles (16 per
+SM of the B200's 148: two full waves of the substitution kernel),
 b = A x_true with x_true ~ U[-1, 1) from seed 3, x0 = 0: mixed-precision
 iterative refinement (FP64 residual and solution update) around an FP32
 PBiCGStab with block-ILU(0), inner relative residual 1e-4, to a 1e-10
@@ -46,6 +47,12 @@ METRIC = "time-to-1e-10 rel. residual (MPIR vs FP64 PBiCGStab), SpMV HBM GB/s, p
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM = 6650.0
 SEED_MATRIX, SEED_X = 2, 3
+# Tiles of the 192^3 system: 16 per SM on 148 SMs. The ILU(0) substitution
+# keeps 8 tiles resident per SM, so 2368 tiles run in two full waves; on
+# B200 MPIR took 126.6 ms at 2368 tiles against 144.5 ms at 2048 and FP64
+# PBiCGStab 167.5 ms against 172.8 ms (block-ILU(0) over these tiles needs
+# 273 inner iterations against 327).
+C3_TILES = 2368
 
 
 def max_over_ranks(value, dist=None, device="cuda"):
@@ -66,7 +73,7 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--grid", type=int, default=192)
-    p.add_argument("--tiles", type=int, default=2048)
+    p.add_argument("--tiles", type=int, default=C3_TILES)
     p.add_argument("--sigma", type=float, default=1.5)
     p.add_argument("--inner-tol", type=float, default=1e-4)
     p.add_argument("--inner-maxit", type=int, default=500)
@@ -589,7 +596,7 @@ def _case_c3(kind):
 
         class _A:  # the bench's own defaults
             inner_maxit, inner_tol = 500, 1e-4
-        h = gb.generateMatrix(gb.GEN_VAR_POISSON, 192, 192, 192, (1.5,), SEED_MATRIX, 2048)
+        h = gb.generateMatrix(gb.GEN_VAR_POISSON, 192, 192, 192, (1.5,), SEED_MATRIX, C3_TILES)
         xt = gb.randomVector(SEED_X, h.numRows).astype(np.float32)
         if kind == "fp64":
             A = h.astype(gb.FLOAT64).copyToTile()
@@ -618,9 +625,9 @@ CASES = {
     "c2-gs-f64": (_case_c2("GS", "f64"), "128^3 convection-diffusion, 1024 tiles, FP64 PBiCGStab-GS(2) to 1e-8"),
     "c2-ilu-f32": (_case_c2("ILU", "f32"), "128^3 convection-diffusion, 1024 tiles, FP32 PBiCGStab-ILU(0) to 1e-8"),
     "c2-ilu-f64": (_case_c2("ILU", "f64"), "128^3 convection-diffusion, 1024 tiles, FP64 PBiCGStab-ILU(0) to 1e-8"),
-    "c3-mpir": (_case_c3("mpir"), "192^3 var-coeff Poisson, 2048 tiles, MPIR FP64 outer / FP32 ILU inner"),
-    "c3-mpir-dw": (_case_c3("dw"), "192^3 var-coeff Poisson, 2048 tiles, MPIR double-word outer"),
-    "c3-fp64": (_case_c3("fp64"), "192^3 var-coeff Poisson, 2048 tiles, FP64 PBiCGStab-ILU(0) to 1e-10"),
+    "c3-mpir": (_case_c3("mpir"), f"192^3 var-coeff Poisson, {C3_TILES} tiles, MPIR FP64 outer / FP32 ILU inner"),
+    "c3-mpir-dw": (_case_c3("dw"), f"192^3 var-coeff Poisson, {C3_TILES} tiles, MPIR double-word outer"),
+    "c3-fp64": (_case_c3("fp64"), f"192^3 var-coeff Poisson, {C3_TILES} tiles, FP64 PBiCGStab-ILU(0) to 1e-10"),
     "c4-gs-f32": (_case_c4, "100^3 LDU mesh, 1024 tiles, FP32 PBiCGStab-GS(2), 260 iterations at most"),
     "c5": (None, "serving: 10,000 fresh variable-coefficient Poisson systems, edge U{16..96}, 70/30 ILU/MPIR"),
 }

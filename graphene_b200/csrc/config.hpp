@@ -88,7 +88,8 @@ struct SolverConfig {
   // computes them (float32 vectors only).
   bool reduceRef = false;
   // Gauss-Seidel sweep kernel: 0 auto (the level ring with one warp per
-  // tile when a tile fits shared memory, a block per tile in batches), 1
+  // tile for float coefficients when a tile fits shared memory, a block per
+  // tile for double coefficients and in batches), 1
   // the level ring with a block per tile, 2 level schedules in global
   // memory, 3 the level ring with one warp per tile.
   int gsKernel = 0;

@@ -207,10 +207,13 @@ class GsNode : public Node {
         };
         return need(*ring_) <= smemMax && need(*ringLo_) <= smemMax;
       };
-      // Automatic: one warp per tile (on B200 a 128^3 convection-diffusion
-      // sweep took 52.7 us against 70.7 us with a block per tile), except in
-      // batches, whose tiles the block kernel maps to their systems.
-      warpRing_ = c.gsKernel == 3 || (c.gsKernel == 0 && !A.batch);
+      // Automatic: for float coefficients one warp per tile (on B200 a
+      // 128^3 convection-diffusion sweep took 52.9 us against 70.7 us with a
+      // block per tile); a block per tile for double coefficients (the
+      // FP64 solve took 28.8 ms against 44.9 ms with a warp per tile, whose
+      // slice holds twice the bytes) and in batches, whose tiles the block
+      // kernel maps to their systems.
+      warpRing_ = c.gsKernel == 3 || (c.gsKernel == 0 && !A.batch && A.vt == DType::F32);
       if (ring_ && warpRing_ && !fits(true)) {
         if (c.gsKernel == 3)
           fail(GR_EUNSUPPORTED, "the Gauss-Seidel ring kernel does not fit this matrix's tiles in shared memory");

@@ -6,7 +6,7 @@ oracle, with the tolerances each comparison is held to.
 * C2: 128^3 upwind convection-diffusion, 1024 tiles, x_true ~ N(0, 1)
   seed 1, PBiCGStab with Gauss-Seidel (2 sweeps) and with ILU(0), FP32 and
   FP64, to 1e-8.
-* C3: 192^3 variable-coefficient Poisson (sigma 1.5, seed 2), 2048 tiles,
+* C3: 192^3 variable-coefficient Poisson (sigma 1.5, seed 2), 2368 tiles,
   x_true seed 3: MPIR (FP64 residual and update, FP32 PBiCGStab-ILU(0)
   inner solves to 1e-4) to 1e-10.
 * C4: the 100^3 jittered, permuted LDU mesh, 1024 tiles: LDU SpMV, a
@@ -165,8 +165,8 @@ def test_c2_convection_diffusion(orc, c2, pre, vt):
 
 # ---- C3 -------------------------------------------------------------------
 def test_c3_mpir_full_size(orc):
-    h = gb.generateMatrix(gb.GEN_VAR_POISSON, 192, 192, 192, (1.5,), 2, 2048)
-    om = orc.grid_system(1, 192, 192, 192, (1.5,), 2, 2048)
+    h = gb.generateMatrix(gb.GEN_VAR_POISSON, 192, 192, 192, (1.5,), 2, 2368)
+    om = orc.grid_system(1, 192, 192, 192, (1.5,), 2, 2368)
     assert np.array_equal(om.row_to_tile(), h.rowToTile())
     A = h.copyToTile()
     n = h.numRows

@@ -1,5 +1,5 @@
 """Parity at the bench's full size: the 192^3 variable-coefficient Poisson
-system with 2048 tiles (7,077,888 rows). SpMV, the FP64-intermediate
+system with 2368 tiles (7,077,888 rows). SpMV, the FP64-intermediate
 residual and the ILU(0) substitution (ring kernel, default layout) are
 compared bit for bit with the oracle on the same tile layout; the oracle
 runs on all host threads, which takes seconds at this size."""
@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def full():
-    h = gb.generateMatrix(gb.GEN_VAR_POISSON, 192, 192, 192, (1.5,), 2, 2048)
+    h = gb.generateMatrix(gb.GEN_VAR_POISSON, 192, 192, 192, (1.5,), 2, 2368)
     o = Oracle()
     o.threads(os.cpu_count() or 1)
     rows, cols, vals = h.coo()
