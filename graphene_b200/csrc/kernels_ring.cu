@@ -232,9 +232,10 @@ __global__ void __launch_bounds__(RingShape<W>::threads) iluRingKernel(const uns
       alpha = cvt<W>(st->alpha);
       first = st->iter == 0;
     }
-    // kPro rows a thread at once, all loads before any store: a tile's
-    // prologue is a few round trips to HBM rather than one per 4 rows.
-    constexpr int kPro = sizeof(W) == 4 ? 8 : 4;
+    // kPro rows a thread at once, all loads before any store. (Eight rows
+    // a thread ran no faster on B200 and took the kernel from 32 to 48
+    // registers, which caps the tiles resident per SM at 10.)
+    constexpr int kPro = 4;
     const int bd = static_cast<int>(blockDim.x);
     for (int i0 = threadIdx.x; i0 < nRows; i0 += kPro * bd) {
       W v[kPro];
@@ -454,7 +455,7 @@ __global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
         alpha = cvt<X>(st->alpha);
         first = st->iter == 0;
       }
-      constexpr int kPro = sizeof(X) == 4 ? 8 : 4;  // rows a thread at once, loads before stores
+      constexpr int kPro = 4;  // rows a thread at once, loads before stores
       for (int i0 = threadIdx.x; i0 < nRows; i0 += kPro * bd) {
         X v[kPro];
         pro.template rows<kPro>(base + i0, bd, base + nRows, beta, omega, alpha, first, v);
