@@ -134,35 +134,27 @@ std::vector<gr_stats> BatchSolve::solveHost(const std::vector<void*>& x, const s
   if (t != DType::F32 && t != DType::F64) fail(GR_EINVAL, "x and b must be float32 or float64");
   const size_t vs = dtypeSize(t);
   const i64 n = union_->n;
-  // Right-hand sides and initial guesses in the union's tile order; padding
-  // rows solve 1 * x = 0.
+  // Right-hand sides and initial guesses in the union's natural order
+  // (system s at rows [rowBegin[s], rowBegin[s] + its rows), padding rows
+  // 0, so that they solve 1 * x = 0), permuted into tile order on the
+  // device.
   std::vector<unsigned char> bh(n * vs, 0), xh(n * vs, 0);
   for (size_t s = 0; s < S; ++s) {
     if (!x[s] || !b[s]) fail(GR_EINVAL, "x and b must not be NULL");
-    unsigned char* bo = bh.data() + rowBegin_[s] * vs;
-    unsigned char* xo = xh.data() + rowBegin_[s] * vs;
-    if (t == DType::F32) {
-      parts_[s]->decompose(static_cast<const float*>(b[s]), reinterpret_cast<float*>(bo));
-      parts_[s]->decompose(static_cast<const float*>(x[s]), reinterpret_cast<float*>(xo));
-    } else {
-      parts_[s]->decompose(static_cast<const double*>(b[s]), reinterpret_cast<double*>(bo));
-      parts_[s]->decompose(static_cast<const double*>(x[s]), reinterpret_cast<double*>(xo));
-    }
+    std::memcpy(bh.data() + rowBegin_[s] * vs, b[s], rowReal_[s] * vs);
+    std::memcpy(xh.data() + rowBegin_[s] * vs, x[s], rowReal_[s] * vs);
   }
-  DBuf xd(n * vs), bd(n * vs);
+  DBuf tmp(n * vs), xd(n * vs), bd(n * vs);
   cudaStream_t st = D_->stream;
-  GR_CUDA(cudaMemcpyAsync(bd.get(), bh.data(), n * vs, cudaMemcpyHostToDevice, st));
-  GR_CUDA(cudaMemcpyAsync(xd.get(), xh.data(), n * vs, cudaMemcpyHostToDevice, st));
+  GR_CUDA(cudaMemcpyAsync(tmp.get(), bh.data(), n * vs, cudaMemcpyHostToDevice, st));
+  launchPermute(*D_, tmp.get(), bd.get(), t, true, st);
+  GR_CUDA(cudaMemcpyAsync(tmp.get(), xh.data(), n * vs, cudaMemcpyHostToDevice, st));
+  launchPermute(*D_, tmp.get(), xd.get(), t, true, st);
   tree_->solve(xd.get(), t, bd.get(), t);
-  GR_CUDA(cudaMemcpyAsync(xh.data(), xd.get(), n * vs, cudaMemcpyDeviceToHost, st));
+  launchPermute(*D_, xd.get(), tmp.get(), t, false, st);
+  GR_CUDA(cudaMemcpyAsync(xh.data(), tmp.get(), n * vs, cudaMemcpyDeviceToHost, st));
   GR_CUDA(cudaStreamSynchronize(st));
-  for (size_t s = 0; s < S; ++s) {
-    const unsigned char* xo = xh.data() + rowBegin_[s] * vs;
-    if (t == DType::F32)
-      parts_[s]->compose(reinterpret_cast<const float*>(xo), static_cast<float*>(x[s]));
-    else
-      parts_[s]->compose(reinterpret_cast<const double*>(xo), static_cast<double*>(x[s]));
-  }
+  for (size_t s = 0; s < S; ++s) std::memcpy(x[s], xh.data() + rowBegin_[s] * vs, rowReal_[s] * vs);
   return tree_->batchStats();
 }
 
