@@ -116,7 +116,9 @@ std::shared_ptr<HostMatrix> concatForBatch(const std::vector<std::shared_ptr<Hos
 BatchSolve::BatchSolve(std::vector<std::shared_ptr<HostMatrix>> parts, const std::string& json)
     : parts_(std::move(parts)) {
   auto cfg = SolverConfig::fromText(json);
-  if (cfg->type != "PBiCGStab") fail(GR_EUNSUPPORTED, "batched solves run PBiCGStab");
+  if (cfg->type != "PBiCGStab" && !(cfg->type == "IterativeRefinement" && cfg->innerSolver &&
+                                    cfg->innerSolver->type == "PBiCGStab"))
+    fail(GR_EUNSUPPORTED, "batched solves run PBiCGStab, or IterativeRefinement over PBiCGStab");
   union_ = concatForBatch(parts_, rowBegin_, rowReal_, tileBegin_);
   D_ = std::make_unique<DeviceMatrix>(union_);
   D_->makeBatch(rowBegin_, rowReal_, tileBegin_);

@@ -476,6 +476,8 @@ SpmvTuning tuneSpmv(DeviceMatrix& A, DType t, int reps);
 
 // r = b - A x in inter (reference CRSMatrix::residual); optionally
 // accumulates a norm of r into normOut (device double) when normKind >= 0.
+// For a batch matrix every system's norm goes to normOut[system], reduced
+// over the blocks and in the order a solve of that system alone uses.
 void launchResidual(DeviceMatrix& A, const void* x, DType xt, const void* b, DType bt, void* r,
                     DType rt, DType inter, int normKind, double* normOut, cudaStream_t s);
 

@@ -647,20 +647,24 @@ __global__ void __launch_bounds__(512) spmvKernel(SellView<MV> A, const VT* __re
 
 // Residual with an IEEE intermediate type I (float or double):
 // r = (b - (d x + sum a x)) computed in I, stored as RT.
+// Batches (seg): each system's rows with the block count a solve of it
+// alone uses, its norm reduced over its own blocks into normOut[system].
 template <class MV, class XT, class BT, class RT, class I, bool C16>
 __global__ void __launch_bounds__(256) residualKernel(SellView<MV> A, const XT* __restrict__ x,
                                                        const BT* __restrict__ b,
                                                        RT* __restrict__ r, int normKind,
                                                        double* __restrict__ normOut,
-                                                       double* partials, unsigned* counter) {
+                                                       double* partials, unsigned* counter, SegView seg) {
   __shared__ double smem[32];
+  const SegPos sp = segPos(seg, A.n);
   const int lane = threadIdx.x & 31;
-  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  const int nWarps = (sp.nb * blockDim.x) >> 5;
+  const int cEnd = (sp.r1 + 31) >> 5;
   double part = redIdentity(normOp(normKind));
-  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < A.nChunks; c += nWarps) {
+  for (int c = (sp.r0 >> 5) + ((sp.rank * blockDim.x + threadIdx.x) >> 5); c < cEnd; c += nWarps) {
     const int row = c * 32 + lane;
-    const I sum = sellRowSum<I, MV, XT, C16>(A, x, c, lane, row < A.n);
-    if (row < A.n) {
+    const I sum = sellRowSum<I, MV, XT, C16>(A, x, c, lane, row < sp.r1);
+    if (row < sp.r1) {
       RT res = cvt<RT>(sub(cvt<I>(__ldg(b + row)), sum));
       r[row] = res;
       if (normKind >= 0) part = normStep(part, toDouble(res), normKind);
@@ -671,8 +675,9 @@ __global__ void __launch_bounds__(256) residualKernel(SellView<MV> A, const XT* 
   const int ops[1] = {normOp(normKind)};
   double out[1];
   blockReduce<1>(v, ops, smem);
-  if (gridReduce<1>(v, ops, partials, counter, smem, out) && threadIdx.x == 0)
-    *normOut = normFinish(out[0], normKind);
+  if (gridReduceRank<1>(v, ops, partials + sp.b0, counter + sp.sys, smem, out, sp.rank, sp.nb) &&
+      threadIdx.x == 0)
+    normOut[sp.sys] = normFinish(out[0], normKind);
 }
 
 // Residual with a double-word intermediate: x is double-word (two floats
@@ -682,10 +687,12 @@ __global__ void __launch_bounds__(256) residualDwKernel(SellView<float> A, const
                                                          const float* __restrict__ b,
                                                          float* __restrict__ r, int normKind,
                                                          double* __restrict__ normOut,
-                                                         double* partials, unsigned* counter) {
+                                                         double* partials, unsigned* counter, SegView seg) {
   __shared__ double smem[32];
+  const SegPos sp = segPos(seg, A.n);
   const int lane = threadIdx.x & 31;
-  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  const int nWarps = (sp.nb * blockDim.x) >> 5;
+  const int cEnd = (sp.r1 + 31) >> 5;
   double part = redIdentity(normOp(normKind));
   auto ld = [&](int i) -> dw {
     if (XDW) {
@@ -694,9 +701,9 @@ __global__ void __launch_bounds__(256) residualDwKernel(SellView<float> A, const
     }
     return {__ldg(x + i), 0.0f};
   };
-  for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < A.nChunks; c += nWarps) {
+  for (int c = (sp.r0 >> 5) + ((sp.rank * blockDim.x + threadIdx.x) >> 5); c < cEnd; c += nWarps) {
     const int row = c * 32 + lane;
-    const bool live = row < A.n;
+    const bool live = row < sp.r1;
     dw sum = live ? dwTimesFp(ld(row), __ldg(A.diag + row)) : dw{0.0f, 0.0f};
     ChunkWalk<float, C16> w(A, c, lane);
     for (int k = 0; k < w.K; k += 4) {
@@ -719,8 +726,9 @@ __global__ void __launch_bounds__(256) residualDwKernel(SellView<float> A, const
   const int ops[1] = {normOp(normKind)};
   double out[1];
   blockReduce<1>(v, ops, smem);
-  if (gridReduce<1>(v, ops, partials, counter, smem, out) && threadIdx.x == 0)
-    *normOut = normFinish(out[0], normKind);
+  if (gridReduceRank<1>(v, ops, partials + sp.b0, counter + sp.sys, smem, out, sp.rank, sp.nb) &&
+      threadIdx.x == 0)
+    normOut[sp.sys] = normFinish(out[0], normKind);
 }
 
 template <class T>
@@ -853,9 +861,24 @@ SpmvTuning tuneSpmv(DeviceMatrix& A, DType t, int reps) {
 
 void launchResidual(DeviceMatrix& A, const void* x, DType xt, const void* b, DType bt, void* r,
                     DType rt, DType inter, int normKind, double* normOut, cudaStream_t s) {
-  const int blocks = A.spmvBlocks();
+  int blocks = A.spmvBlocks();
   double* part = A.partials.as<double>();
   unsigned* cnt = A.counter.as<unsigned>();
+  dev::SegView seg;
+  if (A.batch) {
+    // Every system over its own rows and blocks (the row-chunk tables of
+    // the batch), its norm into normOut[system].
+    const BatchSeg& B = *A.batch;
+    blocks = B.chunkGrid;
+    seg.blockSys = B.chunkSys.as<int>();
+    seg.blockRank = B.chunkRank.as<int>();
+    seg.sysBlocks = B.chunkBlocks.as<int>();
+    seg.sysBlock0 = B.chunkBlock0.as<int>();
+    seg.sysRow0 = B.row0.as<int>();
+    seg.sysRowEnd = B.rowEnd.as<int>();
+    part = B.partials.as<double>();
+    cnt = B.counters.as<unsigned>();
+  }
   auto bad = [&]() {
     fail(GR_EUNSUPPORTED, std::string("residual with x=") + dtypeName(xt) + " b=" + dtypeName(bt) +
                               " r=" + dtypeName(rt) + " intermediate=" + dtypeName(inter) +
@@ -868,7 +891,7 @@ void launchResidual(DeviceMatrix& A, const void* x, DType xt, const void* b, DTy
     auto kernel = xt == DType::DW ? (c16 ? dev::residualDwKernel<true, true> : dev::residualDwKernel<true, false>)
                                   : (c16 ? dev::residualDwKernel<false, true> : dev::residualDwKernel<false, false>);
     kernel<<<blocks, 256, 0, s>>>(sellView<float>(A), static_cast<const float*>(x), static_cast<const float*>(b),
-                                  static_cast<float*>(r), normKind, normOut, part, cnt);
+                                  static_cast<float*>(r), normKind, normOut, part, cnt, seg);
     checkLaunch("residual_dw");
     return;
   }
@@ -876,7 +899,7 @@ void launchResidual(DeviceMatrix& A, const void* x, DType xt, const void* b, DTy
 #define GR_RES(MV, XT, BT, RT, IT)                                                                        \
   (A.sell.compact ? dev::residualKernel<MV, XT, BT, RT, IT, true> : dev::residualKernel<MV, XT, BT, RT, IT, false>) \
       <<<blocks, 256, 0, s>>>(sellView<MV>(A), static_cast<const XT*>(x), static_cast<const BT*>(b),        \
-                              static_cast<RT*>(r), normKind, normOut, part, cnt)
+                              static_cast<RT*>(r), normKind, normOut, part, cnt, seg)
   const bool mf = A.vt == DType::F32;
   const int key = (xt == DType::F64) * 8 + (bt == DType::F64) * 4 + (rt == DType::F64) * 2 +
                   (inter == DType::F64);

@@ -415,6 +415,11 @@ __global__ void stateResetKernel(KState* st, KState init, int count) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) st[i] = init;
 }
 
+__global__ void skipSystemsKernel(KState* st, const int* __restrict__ skip, int count) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    if (skip[i]) st[i].done = 1;
+}
+
 // ---- mixed precision ---------------------------------------------------
 __global__ void castUpKernel(const float* __restrict__ x, void* phi, int E, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -616,6 +621,11 @@ void launchRefReduce(DeviceMatrix& A, const RefRed& q0, const RefRed& q1, RefSta
 void launchStateReset(KState* st, const KState& init, cudaStream_t s, int count) {
   dev::stateResetKernel<<<(count + 255) / 256, 256, 0, s>>>(st, init, count);
   checkLaunch("state_reset");
+}
+
+void launchSkipSystems(KState* st, const int* skip, int count, cudaStream_t s) {
+  dev::skipSystemsKernel<<<(count + 255) / 256, 256, 0, s>>>(st, skip, count);
+  checkLaunch("skip_systems");
 }
 
 void launchNormInto(DeviceMatrix& A, const void* x, DType t, int normKind, double* out, cudaStream_t s) {

@@ -167,6 +167,9 @@ void launchRefReduce(DeviceMatrix& A, const RefRed& q0, const RefRed& q1, RefSta
 void launchPrologue(DeviceMatrix& A, const PrologueArgs& pro, void* copyTo, DType W, cudaStream_t s);
 // Writes the initial state (single thread).
 void launchStateReset(KState* st, const KState& init, cudaStream_t s, int count = 1);
+// Batches: marks the systems whose skip[k] is nonzero done (their kernels
+// then return at once and their x stays as it is).
+void launchSkipSystems(KState* st, const int* skip, int count, cudaStream_t s);
 // Norm of a vector into st->bNorm.
 void launchNormInto(DeviceMatrix& A, const void* x, DType t, int normKind, double* out, cudaStream_t s);
 

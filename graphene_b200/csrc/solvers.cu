@@ -40,7 +40,12 @@ class Node {
   virtual void refresh() {}
   // Per-system statistics of the last solve of a batch.
   virtual std::vector<gr_stats> batchStats() const {
-    fail(GR_EUNSUPPORTED, "only PBiCGStab solves batches");
+    fail(GR_EUNSUPPORTED, "only PBiCGStab and IterativeRefinement solve batches");
+  }
+  // Batches: the systems the next solve leaves alone (nonzero entries; x of
+  // those systems is not touched). Empty: none.
+  virtual void setBatchSkip(const std::vector<int>&) {
+    fail(GR_EUNSUPPORTED, "only PBiCGStab skips systems of a batch");
   }
 
  protected:
@@ -492,6 +497,7 @@ class PbicgstabNode : public Node {
     if (mixed_) launchConvert(x, Wx, xw(), W, static_cast<int>(A_.n), s());
     else GR_CUDA(cudaMemcpyAsync(xw(), x, vb, cudaMemcpyDeviceToDevice, s()));
     launchBicgInit(A_, xw(), bW, buf(R), buf(R0), st, W, s(), ref);
+    if (!skip_.empty()) launchSkipSystems(st, skipDev_.as<int>(), systems_, s());
     if (ref)
       launchRefReduce(A_, RefRed{RefKind::Dot, buf(R0), buf(R)}, RefRed{normRed(), buf(R), nullptr}, RefStage::Init,
                       st, refTiles_.get(), s());
@@ -539,9 +545,21 @@ class PbicgstabNode : public Node {
     for (int k = 0; k < systems_; ++k) out[k] = statsOf(host_[k]);
     return out;
   }
+  void setBatchSkip(const std::vector<int>& skip) override {
+    if (!A_.batch) fail(GR_EINVAL, "skipping systems needs a batch");
+    if (!skip.empty() && static_cast<int>(skip.size()) != systems_) fail(GR_EINVAL, "one skip flag per system");
+    skip_ = skip;
+    if (!skip_.empty()) {
+      if (skipDev_.bytes() < sizeof(int) * systems_) skipDev_.alloc(sizeof(int) * systems_);
+      GR_CUDA(cudaMemcpyAsync(skipDev_.get(), skip_.data(), sizeof(int) * systems_, cudaMemcpyHostToDevice, s()));
+      GR_CUDA(cudaStreamSynchronize(s()));
+    }
+  }
 
  private:
   enum { X = 0, R, R0, P, V, Y, S, Z, T, NBUF };
+  std::vector<int> skip_;
+  DBuf skipDev_;
   int systems_ = 1;
   bool batchHost_ = false;
   std::unique_ptr<Node> pre_;
@@ -729,6 +747,7 @@ class MpirNode : public Node {
     if (W != DType::F32)
       fail(GR_EUNSUPPORTED, "IterativeRefinement expects a float32 working precision (x and b)");
     E_ = cfg_.extendedPrecisionType < 0 ? W : static_cast<DType>(cfg_.extendedPrecisionType);
+    if (A_.batch) return solveBatch(x, b);
     const int n = A_.n;
     gr_stats st{};
     double* d = scal_.as<double>();
@@ -782,11 +801,117 @@ class MpirNode : public Node {
     launchConvert(phi_.get(), E_, out, t, A_.n, s());
     GR_CUDA(cudaStreamSynchronize(s()));
   }
+  std::vector<gr_stats> batchStats() const override {
+    if (batchStats_.empty()) fail(GR_EINVAL, "no batched IterativeRefinement solve has run yet");
+    return batchStats_;
+  }
 
  private:
   std::unique_ptr<Node> inner_;
   DType E_ = DType::F32;
   DBuf phi_, r_, scal_;
+  std::vector<gr_stats> batchStats_;
+
+  // The outer loop of every system of a batch at once
+  // (iterative-refinement/Solver.cpp:48-123 per system): residuals and their
+  // norms for all systems in one launch (each system reduced as it would
+  // be alone), one batched inner solve for the systems still refining (the
+  // others skipped: their correction stays zero and is not applied), phi
+  // updated on the refining systems' rows only. A system's result equals
+  // its solve alone.
+  gr_stats solveBatch(void* x, const void* b) {
+    const BatchSeg& B = *A_.batch;
+    const int S = B.systems;
+    const int n = A_.n;
+    const size_t es = dtypeSize(E_);
+    if (scal_.bytes() < sizeof(double) * (2 * static_cast<size_t>(S) + 4))
+      scal_.alloc(sizeof(double) * (2 * static_cast<size_t>(S) + 4));
+    double* d = scal_.as<double>();  // [0, S): residual norms, [S, 2S): norms of b
+    if (r_.bytes() < n * sizeof(float)) r_.alloc(n * sizeof(float));
+    if (phi_.bytes() < n * es) phi_.alloc(n * es);
+    float* r = r_.as<float>();
+    std::vector<double> res(S), bn(S, 0.0);
+    auto readNorms = [&](const double* src, std::vector<double>& dst) {
+      GR_CUDA(cudaMemcpyAsync(dst.data(), src, sizeof(double) * S, cudaMemcpyDeviceToHost, s()));
+      GR_CUDA(cudaStreamSynchronize(s()));
+    };
+    if (cfg_.relTolerance > 0) {
+      for (int k = 0; k < S; ++k)
+        launchNormN(A_, static_cast<const float*>(b) + B.rowBegin[k], B.rowReal[k], DType::F32, cfg_.norm, d + S + k,
+                    s());
+      readNorms(d + S, bn);
+    }
+    launchResidual(A_, x, DType::F32, b, DType::F32, r, DType::F32, E_, cfg_.norm, d, s());
+    readNorms(d, res);
+    launchCastUp(static_cast<const float*>(x), phi_.get(), E_, n, s());
+    batchStats_.assign(S, gr_stats{});
+    std::vector<int> conv(S, 0), active(S, 1), skip(S, 0);
+    auto finished = [&](int k) {
+      return (conv[k] && batchStats_[k].iterations >= cfg_.minIterations) ||
+             batchStats_[k].iterations >= cfg_.maxIterations;
+    };
+    for (int k = 0; k < S; ++k) {
+      batchStats_[k].initial_residual = batchStats_[k].final_residual = res[k];
+      batchStats_[k].b_norm = bn[k];
+      if (finished(k)) active[k] = 0;
+    }
+    auto anyActive = [&]() { return std::find(active.begin(), active.end(), 1) != active.end(); };
+    while (anyActive()) {
+      for (int k = 0; k < S; ++k) {
+        skip[k] = active[k] ? 0 : 1;
+        if (active[k]) batchStats_[k].iterations += 1;
+      }
+      inner_->setBatchSkip(skip);
+      if (inner_->usesInitialGuess()) GR_CUDA(cudaMemsetAsync(x, 0, n * sizeof(float), s()));
+      inner_->solve(x, r, DType::F32, nullptr);
+      const std::vector<gr_stats> is = inner_->batchStats();
+      for (int k = 0; k < S; ++k) {
+        if (!active[k]) continue;
+        batchStats_[k].inner_iterations += is[k].inner_iterations > 0 ? is[k].inner_iterations : is[k].iterations;
+        if (is[k].status != GR_OK) {  // no correction to apply for this system
+          batchStats_[k].status = is[k].status;
+          active[k] = 0;
+          continue;
+        }
+        launchPhiUpdate(static_cast<char*>(phi_.get()) + B.rowBegin[k] * es,
+                        static_cast<const float*>(x) + B.rowBegin[k], E_, static_cast<int>(B.rowReal[k]), s());
+      }
+      launchResidual(A_, phi_.get(), E_, b, DType::F32, r, DType::F32, E_, cfg_.norm, d, s());
+      readNorms(d, res);
+      for (int k = 0; k < S; ++k) {
+        if (!active[k]) continue;
+        gr_stats& q = batchStats_[k];
+        q.final_residual = res[k];
+        conv[k] = q.final_residual < cfg_.absTolerance || q.final_residual < q.initial_residual * cfg_.relResidual ||
+                  (cfg_.relTolerance > 0 && q.final_residual < q.b_norm * cfg_.relTolerance);
+        if (!std::isfinite(q.final_residual)) {
+          q.status = GR_ENONFINITE;
+          active[k] = 0;
+        } else if (finished(k)) {
+          active[k] = 0;
+        }
+      }
+    }
+    inner_->setBatchSkip({});
+    launchCastDown(phi_.get(), static_cast<float*>(x), E_, n, s());
+    GR_CUDA(cudaStreamSynchronize(s()));
+    gr_stats out = gr_stats{};
+    out.converged = 1;
+    for (int k = 0; k < S; ++k) {
+      gr_stats& q = batchStats_[k];
+      q.converged = conv[k];
+      if (k == 0) {
+        out.initial_residual = q.initial_residual;
+        out.final_residual = q.final_residual;
+        out.b_norm = q.b_norm;
+      }
+      out.iterations = std::max(out.iterations, q.iterations);
+      out.inner_iterations = std::max(out.inner_iterations, q.inner_iterations);
+      out.converged = out.converged && q.converged;
+      if (out.status == GR_OK) out.status = q.status;
+    }
+    return out;
+  }
   double readScalar(const double* d) {
     double v = 0;
     GR_CUDA(cudaMemcpyAsync(&v, d, sizeof(double), cudaMemcpyDeviceToHost, s()));

@@ -86,6 +86,57 @@ def test_batch_gauss_seidel_equals_solo(vt, dt):
     assert all(st.converged for st in sts)
 
 
+def mpir_cfg(ext="float64", pre=None):
+    return {"type": "IterativeRefinement", "relResidual": 1e-10, "maxIterations": 30, "extendedPrecisionType": ext,
+            "innerSolver": {"type": "PBiCGStab", "maxIterations": 300, "relResidual": 1e-4,
+                            "preconditioner": pre or {"type": "ILU", "kernel": "ring"}}}
+
+
+@pytest.mark.parametrize("ext", ["float64", "twofloat32"])
+def test_batch_mpir_equals_solo(ext):
+    """IterativeRefinement over a batch: per-system residual norms (each
+    reduced as alone), one batched inner solve for the systems still
+    refining, phi updated on those systems only. Every system's x, outer and
+    inner iteration counts and norms equal its solo solve's."""
+    hs = systems(gb.FLOAT32, sigma=1.5)
+    bs = rhs(hs, np.float32, seed=31)
+    c = mpir_cfg(ext)
+    xs, sts = gb.Batch(hs, c).solveHost(bs)
+    outer = []
+    for h, b, x, st in zip(hs, bs, xs, sts):
+        xr, sr = solo(h, c, b)
+        np.testing.assert_array_equal(x, xr)
+        assert st.iterations == sr.iterations and st.innerIterations == sr.innerIterations
+        assert st.finalResidual == sr.finalResidual and st.initialResidual == sr.initialResidual
+        assert st.converged == sr.converged
+        outer.append(st.iterations)
+    assert all(st.converged for st in sts)
+
+
+def test_batch_mpir_gauss_seidel_inner():
+    hs = systems(gb.FLOAT32, SYSTEMS[:4])
+    bs = rhs(hs, np.float32, seed=37)
+    c = mpir_cfg(pre={"type": "GaussSeidel", "numFixedIterations": 2, "kernel": "ring"})
+    xs, sts = gb.Batch(hs, c).solveHost(bs)
+    for h, b, x, st in zip(hs, bs, xs, sts):
+        xr, sr = solo(h, c, b)
+        np.testing.assert_array_equal(x, xr)
+        assert st.iterations == sr.iterations and st.innerIterations == sr.innerIterations
+
+
+def test_batch_mpir_outer_cap():
+    """Systems stop at the outer iteration cap independently."""
+    hs = systems(gb.FLOAT32, SYSTEMS[:3])
+    bs = rhs(hs, np.float32, seed=41)
+    c = mpir_cfg()
+    c["maxIterations"] = 1
+    xs, sts = gb.Batch(hs, c).solveHost(bs)
+    for h, b, x, st in zip(hs, bs, xs, sts):
+        xr, sr = solo(h, c, b)
+        np.testing.assert_array_equal(x, xr)
+        assert st.iterations == sr.iterations == 1
+
+
 def test_batch_solutions_accurate():
     import scipy.sparse as sp
     import scipy.sparse.linalg as spl
