@@ -794,7 +794,10 @@ def main():
         return best, out
 
     extra = {}
-    if not a.no_extras:
+    # The extras (FP64 comparison, other configurations, serving, batching)
+    # run in single-GPU runs only: replicas would repeat them on every rank
+    # and contend for the host's cores.
+    if not a.no_extras and world == 1:
         h64 = h.astype(gb.FLOAT64)
         A64 = h64.copyToTile()
         b64 = b.double()
