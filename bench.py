@@ -806,7 +806,24 @@ def main():
                                         "converged": st64.converged,
                                         "rel_residual_fp64": rel64(A64, x64, b64)}
         extra["speedup_mpir_vs_fp64"] = fp64_ms / ms_per_step
-        del s64, x64, A64, h64, b64
+        # The FP64 solve's kernels beside the FP32 ones below: where the
+        # MPIR / FP64 ratio comes from (bytes: 12m + 28n for the SpMV, 12m +
+        # 24n for the substitution's values, columns, inverse diagonal, b
+        # in and x out).
+        y64 = torch.empty_like(b64)
+        A64.tuneSpmv(gb.FLOAT64, reps=5)
+        for _ in range(5):
+            A64.spmv(b64, y64)
+        spmv64_ms = event_ms(lambda: [A64.spmv(b64, y64) for _ in range(50)])[0] / 50
+        ilu64 = gb.Solver(A64, {"type": "ILU"})
+        z64 = torch.empty_like(b64)
+        ilu64.timeRepeated(z64, b64, 3)
+        ilu64_ms = ilu64.timeRepeated(z64, b64, 20)
+        extra["fp64_kernels"] = {"spmv_ms": spmv64_ms, "spmv_GBs": (12 * m + 28 * n) / (spmv64_ms * 1e-3) / 1e9,
+                                 "ilu0_apply_ms": ilu64_ms,
+                                 "ilu0_apply_GBs": (12 * m + 24 * n) / (ilu64_ms * 1e-3) / 1e9,
+                                 "per_iteration_ms": fp64_ms / max(1, st64.iterations)}
+        del s64, x64, A64, h64, b64, y64, ilu64, z64
         for name, c in [("mpir_twofloat32", mpir_config(a, "twofloat32")),
                         ("mpir_float64_inner_tol_1e-3", mpir_config(a, "float64", 1e-3))]:
             ms, (sv, xv, sx) = best_of(lambda: solve(A, c, b))
@@ -844,6 +861,11 @@ def main():
                      "autotuned_geometry": tuned}
     extra["ilu0_apply"] = {"ms": ilu_ms, "GBs": gbs(ilu_bytes, ilu_ms),
                            "frac_of_hbm": gbs(ilu_bytes, ilu_ms) / peak, "bytes_per_launch": ilu_bytes}
+    if "fp64_kernels" in extra:
+        extra["fp64_kernels"]["ilu0_apply_fp32_over_fp64"] = ilu_ms / extra["fp64_kernels"]["ilu0_apply_ms"]
+        extra["fp64_kernels"]["spmv_fp32_over_fp64"] = spmv_ms / extra["fp64_kernels"]["spmv_ms"]
+        st_inner = max(1, st.innerIterations)
+        extra["fp64_kernels"]["mpir_per_inner_iteration_ms"] = ms_per_step / st_inner
 
     # End to end through the C ABI with pinned host buffers (natural order).
     b_host = torch.empty(n, dtype=torch.float32, pin_memory=True)
