@@ -518,15 +518,16 @@ def serving(gb, requests=10000, slots=8, seed=7, rate_requests=2000, cold_reques
     sat = run(srv, list(range(requests)), None)
     sat["wall_s"] = time.perf_counter() - t0
     res = {"saturation": sat}
-    for f in (0.5, 0.8, 1.0):
+    for f in ((0.5, 0.8, 1.0) if rate_requests > 0 else ()):
         ks = list(range(requests, requests + rate_requests))
         res[f"load_{f}"] = run(srv, ks, f * sat["throughput_per_s"])
     srv.close()
     out["stream"] = res
-    srv = gb.Server(slots=slots)
-    out["cold"] = run(srv, list(range(requests + rate_requests, requests + rate_requests + cold_requests)), None,
-                      fresh_structure=True)
-    srv.close()
+    if cold_requests > 0:
+        srv = gb.Server(slots=slots)
+        out["cold"] = run(srv, list(range(requests + rate_requests, requests + rate_requests + cold_requests)),
+                          None, fresh_structure=True)
+        srv.close()
     pool.shutdown()
     return out
 
