@@ -251,8 +251,11 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
   } else if (ty == "ILU") {
     mark("solveMulticolor"); mark("factorizeMulticolor"); mark("diagonalBased"); mark("kernel");
     mark("ringLog2"); mark("prefetch"); mark("unroll"); mark("ringBytes"); mark("l2Ahead"); mark("tilesPerBlock");
-    mark("compactRing"); mark("recordLevels"); mark("pairRows"); mark("warpsPerBlock");
+    mark("compactRing"); mark("recordLevels"); mark("pairRows"); mark("warpsPerBlock"); mark("computeWarps");
     readInt(j, "warpsPerBlock", c->warpsPerBlock);
+    readInt(j, "computeWarps", c->computeWarps);
+    if (c->computeWarps != 0 && c->computeWarps != 2 && c->computeWarps != 4)
+      fail(GR_EINVAL, "computeWarps must be 2 or 4");
     if (c->warpsPerBlock < 1 || c->warpsPerBlock > 8) fail(GR_EINVAL, "warpsPerBlock must be 1..8");
     readBool(j, "compactRing", c->compactRing);
     readBool(j, "pairRows", c->pairRows);

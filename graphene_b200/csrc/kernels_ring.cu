@@ -178,8 +178,11 @@ __device__ __forceinline__ W ringRowDot(W temp, const RingLevel<MV, COMPACT>& lv
   return temp;
 }
 
-template <class MV, class W, bool UNROLL, bool COMPACT>
-__global__ void __launch_bounds__(RingShape<W>::threads) iluRingKernel(const unsigned char* __restrict__ stream,
+// CW compute warps (0: RingShape's default for W); the waiting and
+// producer warps follow them.
+template <class MV, class W, bool UNROLL, bool COMPACT, int CW = 0>
+__global__ void __launch_bounds__(CW > 0 ? 32 * CW + 64 : RingShape<W>::threads) iluRingKernel(
+    const unsigned char* __restrict__ stream,
                                                                const long long* __restrict__ tileOffset,
                                                                const int4* __restrict__ meta,
                                                                const int* __restrict__ tileLevel,
@@ -187,8 +190,8 @@ __global__ void __launch_bounds__(RingShape<W>::threads) iluRingKernel(const uns
                                                                int metaLevels, uint32_t l2Ahead, bool dilu,
                                                                SPro<W> pro, W* __restrict__ y, int* errFlag,
                                                                bool pairRows) {
-  constexpr int kRingCompute = RingShape<W>::compute;
-  constexpr int kRingLevelSync = RingShape<W>::levelSync;
+  constexpr int kRingCompute = CW > 0 ? 32 * CW : RingShape<W>::compute;
+  constexpr int kRingLevelSync = kRingCompute + 32;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int abortFlag, consumedLevels;
   const KState* st = pro.state();
@@ -885,18 +888,28 @@ void launchRingPack(DeviceMatrix& A, const LevelRing& R, void* stream, const voi
 }
 
 namespace {
+template <class MV, class W, int CW>
+auto ringKernelFor(bool compact, bool unroll) {
+  return compact ? (unroll ? dev::iluRingKernel<MV, W, true, true, CW> : dev::iluRingKernel<MV, W, false, true, CW>)
+                 : (unroll ? dev::iluRingKernel<MV, W, true, false, CW> : dev::iluRingKernel<MV, W, false, false, CW>);
+}
+
 template <class MV, class W>
 void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& p, void* y,
-                int l2Ahead, bool unroll, bool pairRows, cudaStream_t s) {
+                int l2Ahead, bool unroll, bool pairRows, cudaStream_t s, int computeWarps) {
   const size_t smem = iluRingSmem(A, R, dtypeOf<W>());
-  auto kernel = R.compact ? (unroll ? dev::iluRingKernel<MV, W, true, true> : dev::iluRingKernel<MV, W, false, true>)
-                         : (unroll ? dev::iluRingKernel<MV, W, true, false> : dev::iluRingKernel<MV, W, false, false>);
+  if (computeWarps != 0 && computeWarps != 2 && computeWarps != 4)
+    fail(GR_EINVAL, "computeWarps must be 2 or 4 (0: the default)");
+  auto kernel = computeWarps == 2   ? ringKernelFor<MV, W, 2>(R.compact, unroll)
+                : computeWarps == 4 ? ringKernelFor<MV, W, 4>(R.compact, unroll)
+                                    : ringKernelFor<MV, W, 0>(R.compact, unroll);
+  const int threads = computeWarps > 0 ? 32 * computeWarps + 64 : dev::RingShape<W>::threads;
   ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
   preferSharedCarveout(reinterpret_cast<const void*>(kernel));
   if (p.stIndex && R.group != 1) fail(GR_EUNSUPPORTED, "batched solves run one tile per block");
   dev::SPro<W> pro{static_cast<int>(p.kind), static_cast<const W*>(p.b), static_cast<const W*>(p.r),
                    static_cast<W*>(p.pOrS), static_cast<const W*>(p.v), p.st, p.stIndex};
-  kernel<<<R.numGroups, dev::RingShape<W>::threads, smem, s>>>(static_cast<const unsigned char*>(stream),
+  kernel<<<R.numGroups, threads, smem, s>>>(static_cast<const unsigned char*>(stream),
                                              R.tileOffset.as<long long>(), R.meta.as<int4>(), R.tileLevel.as<int>(),
                                              R.groupStart.as<int>(),
                                              static_cast<int>(R.ringBytes), R.maxTileLevels,
@@ -1031,13 +1044,13 @@ void launchIluWarpRing(DeviceMatrix& A, const LevelRing& R, const void* stream, 
 }
 
 void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,
-                   void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s, bool pairRows) {
+                   void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s, bool pairRows, int computeWarps) {
   if (A.vt == DType::F32 && W == DType::F32)
-    ringApplyT<float, float>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s);
+    ringApplyT<float, float>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps);
   else if (A.vt == DType::F32 && W == DType::F64)
-    ringApplyT<float, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s);
+    ringApplyT<float, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps);
   else if (A.vt == DType::F64 && W == DType::F64)
-    ringApplyT<double, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s);
+    ringApplyT<double, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps);
   else fail(GR_EUNSUPPORTED, "ILU apply with float64 coefficients and float32 vectors");
 }
 
