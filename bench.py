@@ -391,7 +391,7 @@ def other_configs(gb, peak):
     return out
 
 
-def serving(gb, requests=10000, slots=8, seed=7, rate_requests=2000, cold_requests=48, gen_threads=0,
+def serving(gb, requests=10000, slots=16, seed=7, rate_requests=2000, cold_requests=48, gen_threads=0,
             max_wall_s=300.0):
     """C5: a stream of solves, each a fresh 7-point variable-coefficient
     Poisson system (sigma 1) with grid edge L ~ U{16..96}, 70 % FP32

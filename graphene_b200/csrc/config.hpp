@@ -68,7 +68,7 @@ struct SolverConfig {
   // ILU "pairRows": in record levels each thread computes two rows at once.
   bool pairRows = false;
   // ILU "computeWarps" of the block ring kernel (0: 2 for float, 4 for
-  // double working vectors; or 2, 4).
+  // double working vectors; or 1, 2, 4).
   int computeWarps = 0;
   // Extension: log2 of the streamed kernel's ring size in bytes (0: the
   // smallest ring that holds the largest level).

@@ -898,9 +898,10 @@ template <class MV, class W>
 void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& p, void* y,
                 int l2Ahead, bool unroll, bool pairRows, cudaStream_t s, int computeWarps) {
   const size_t smem = iluRingSmem(A, R, dtypeOf<W>());
-  if (computeWarps != 0 && computeWarps != 2 && computeWarps != 4)
-    fail(GR_EINVAL, "computeWarps must be 2 or 4 (0: the default)");
-  auto kernel = computeWarps == 2   ? ringKernelFor<MV, W, 2>(R.compact, unroll)
+  if (computeWarps != 0 && computeWarps != 1 && computeWarps != 2 && computeWarps != 4)
+    fail(GR_EINVAL, "computeWarps must be 1, 2 or 4 (0: the default)");
+  auto kernel = computeWarps == 1   ? ringKernelFor<MV, W, 1>(R.compact, unroll)
+                : computeWarps == 2 ? ringKernelFor<MV, W, 2>(R.compact, unroll)
                 : computeWarps == 4 ? ringKernelFor<MV, W, 4>(R.compact, unroll)
                                     : ringKernelFor<MV, W, 0>(R.compact, unroll);
   const int threads = computeWarps > 0 ? 32 * computeWarps + 64 : dev::RingShape<W>::threads;
