@@ -254,6 +254,8 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
     mark("compactRing"); mark("recordLevels"); mark("pairRows"); mark("warpsPerBlock"); mark("computeWarps");
     readInt(j, "warpsPerBlock", c->warpsPerBlock);
     readInt(j, "computeWarps", c->computeWarps);
+    mark("waitingWarp");
+    readBool(j, "waitingWarp", c->waitingWarp);
     if (c->computeWarps != 0 && c->computeWarps != 1 && c->computeWarps != 2 && c->computeWarps != 4)
       fail(GR_EINVAL, "computeWarps must be 1, 2 or 4");
     if (c->warpsPerBlock < 1 || c->warpsPerBlock > 8) fail(GR_EINVAL, "warpsPerBlock must be 1..8");

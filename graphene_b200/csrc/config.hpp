@@ -70,6 +70,9 @@ struct SolverConfig {
   // ILU "computeWarps" of the block ring kernel (0: 2 for float, 4 for
   // double working vectors; or 1, 2, 4).
   int computeWarps = 0;
+  // ILU "waitingWarp": false lets the compute warps wait for each level's
+  // copy themselves (no waiting warp; default computeWarps only).
+  bool waitingWarp = true;
   // Extension: log2 of the streamed kernel's ring size in bytes (0: the
   // smallest ring that holds the largest level).
   int ringLog2 = 0;

@@ -178,10 +178,16 @@ __device__ __forceinline__ W ringRowDot(W temp, const RingLevel<MV, COMPACT>& lv
   return temp;
 }
 
-// CW compute warps (0: RingShape's default for W); the waiting and
-// producer warps follow them.
-template <class MV, class W, bool UNROLL, bool COMPACT, int CW = 0>
-__global__ void __launch_bounds__(CW > 0 ? 32 * CW + 64 : RingShape<W>::threads) iluRingKernel(
+// CW compute warps (0: RingShape's default for W); the waiting warp
+// (WAITER) and the producer warp follow them. Without the waiting warp the
+// compute warps wait for each next level themselves and release the level
+// they finished.
+template <int CW, class W>
+constexpr int ringComputeThreads() {
+  return CW > 0 ? 32 * CW : RingShape<W>::compute;
+}
+template <class MV, class W, bool UNROLL, bool COMPACT, int CW = 0, bool WAITER = true>
+__global__ void __launch_bounds__(ringComputeThreads<CW, W>() + (WAITER ? 64 : 32)) iluRingKernel(
     const unsigned char* __restrict__ stream,
                                                                const long long* __restrict__ tileOffset,
                                                                const int4* __restrict__ meta,
@@ -190,8 +196,8 @@ __global__ void __launch_bounds__(CW > 0 ? 32 * CW + 64 : RingShape<W>::threads)
                                                                int metaLevels, uint32_t l2Ahead, bool dilu,
                                                                SPro<W> pro, W* __restrict__ y, int* errFlag,
                                                                bool pairRows) {
-  constexpr int kRingCompute = CW > 0 ? 32 * CW : RingShape<W>::compute;
-  constexpr int kRingLevelSync = kRingCompute + 32;
+  constexpr int kRingCompute = ringComputeThreads<CW, W>();
+  constexpr int kRingLevelSync = kRingCompute + (WAITER ? 32 : 0);
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int abortFlag, consumedLevels;
   const KState* st = pro.state();
@@ -307,9 +313,18 @@ __global__ void __launch_bounds__(CW > 0 ? 32 * CW + 64 : RingShape<W>::threads)
       }
     }
   } else {
-    // Compute warps: level l, whose block the waiting warp saw land before
-    // the previous barrier.
-    bool stop = namedBarOr(1, kRingLevelSync, false);
+    // Compute warps: level l, whose block the waiting warp (or, without
+    // one, each compute thread) saw land before the previous barrier.
+    bool stop;
+    if constexpr (WAITER) {
+      stop = namedBarOr(1, kRingLevelSync, false);
+    } else {
+      const bool ok = mbarWaitBounded(smemAddr(tableBar), 0, abortV) &&
+                      (L == 0 || mbarWaitBounded(smemAddr(full), 0, abortV));
+      if (!ok) abortFlag = 1;
+      stop = namedBarOr(1, kRingCompute, !ok);
+      if (stop && threadIdx.x == 0) consumedLevels = 0;
+    }
     for (int l = 0; !stop && l < L; ++l) {
       const int4 m = mt[l];
       const RingLevel<MV, COMPACT> cur = ringLevelAt<MV, COMPACT>(m, ring);
@@ -365,7 +380,21 @@ __global__ void __launch_bounds__(CW > 0 ? 32 * CW + 64 : RingShape<W>::threads)
           xs[il] = dilu ? add(xs[il], mul(temp, iv)) : mul(add(xs[il], temp), iv);
         }
       }
-      stop = namedBarOr(1, kRingLevelSync, *abortV != 0);
+      if constexpr (WAITER) {
+        stop = namedBarOr(1, kRingLevelSync, *abortV != 0);
+      } else {
+        bool bad = false;
+        if (l + 1 < L &&
+            !mbarWaitBounded(smemAddr(full + (l + 1) % kRingBarriers), ((l + 1) / kRingBarriers) & 1, abortV)) {
+          abortFlag = 1;
+          bad = true;
+        }
+        stop = namedBarOr(1, kRingCompute, bad || *abortV != 0);
+        if (threadIdx.x == 0) {
+          mbarArrive(smemAddr(empty + l % kRingBarriers));
+          if (stop) consumedLevels = l + 1;
+        }
+      }
     }
   }
   __syncthreads();
@@ -888,23 +917,27 @@ void launchRingPack(DeviceMatrix& A, const LevelRing& R, void* stream, const voi
 }
 
 namespace {
-template <class MV, class W, int CW>
+template <class MV, class W, int CW, bool WAITER = true>
 auto ringKernelFor(bool compact, bool unroll) {
-  return compact ? (unroll ? dev::iluRingKernel<MV, W, true, true, CW> : dev::iluRingKernel<MV, W, false, true, CW>)
-                 : (unroll ? dev::iluRingKernel<MV, W, true, false, CW> : dev::iluRingKernel<MV, W, false, false, CW>);
+  return compact ? (unroll ? dev::iluRingKernel<MV, W, true, true, CW, WAITER>
+                           : dev::iluRingKernel<MV, W, false, true, CW, WAITER>)
+                 : (unroll ? dev::iluRingKernel<MV, W, true, false, CW, WAITER>
+                           : dev::iluRingKernel<MV, W, false, false, CW, WAITER>);
 }
 
 template <class MV, class W>
 void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& p, void* y,
-                int l2Ahead, bool unroll, bool pairRows, cudaStream_t s, int computeWarps) {
+                int l2Ahead, bool unroll, bool pairRows, cudaStream_t s, int computeWarps, bool waiter) {
   const size_t smem = iluRingSmem(A, R, dtypeOf<W>());
   if (computeWarps != 0 && computeWarps != 1 && computeWarps != 2 && computeWarps != 4)
     fail(GR_EINVAL, "computeWarps must be 1, 2 or 4 (0: the default)");
-  auto kernel = computeWarps == 1   ? ringKernelFor<MV, W, 1>(R.compact, unroll)
+  if (!waiter && computeWarps != 0) fail(GR_EINVAL, "waitingWarp false needs the default computeWarps");
+  auto kernel = !waiter             ? ringKernelFor<MV, W, 0, false>(R.compact, unroll)
+                : computeWarps == 1 ? ringKernelFor<MV, W, 1>(R.compact, unroll)
                 : computeWarps == 2 ? ringKernelFor<MV, W, 2>(R.compact, unroll)
                 : computeWarps == 4 ? ringKernelFor<MV, W, 4>(R.compact, unroll)
                                     : ringKernelFor<MV, W, 0>(R.compact, unroll);
-  const int threads = computeWarps > 0 ? 32 * computeWarps + 64 : dev::RingShape<W>::threads;
+  const int threads = (computeWarps > 0 ? 32 * computeWarps : dev::RingShape<W>::compute) + (waiter ? 64 : 32);
   ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
   preferSharedCarveout(reinterpret_cast<const void*>(kernel));
   if (p.stIndex && R.group != 1) fail(GR_EUNSUPPORTED, "batched solves run one tile per block");
@@ -1045,13 +1078,14 @@ void launchIluWarpRing(DeviceMatrix& A, const LevelRing& R, const void* stream, 
 }
 
 void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,
-                   void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s, bool pairRows, int computeWarps) {
+                   void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s, bool pairRows, int computeWarps,
+                   bool waiter) {
   if (A.vt == DType::F32 && W == DType::F32)
-    ringApplyT<float, float>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps);
+    ringApplyT<float, float>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps, waiter);
   else if (A.vt == DType::F32 && W == DType::F64)
-    ringApplyT<float, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps);
+    ringApplyT<float, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps, waiter);
   else if (A.vt == DType::F64 && W == DType::F64)
-    ringApplyT<double, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps);
+    ringApplyT<double, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps, waiter);
   else fail(GR_EUNSUPPORTED, "ILU apply with float64 coefficients and float32 vectors");
 }
 

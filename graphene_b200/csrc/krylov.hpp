@@ -96,7 +96,8 @@ void launchIluWarpRing(DeviceMatrix& A, const LevelRing& R, const void* stream, 
                        void* y, DType W, int warpsPerBlock, bool pairRows, cudaStream_t s);
 // pairRows: record levels process two rows a thread at once.
 void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,
-                   void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s, bool pairRows = false, int computeWarps = 0);
+                   void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s, bool pairRows = false, int computeWarps = 0,
+                   bool waiter = true);
 // One Gauss-Seidel sweep through a Gauss-Seidel level ring (kernels_ring.cu):
 // xout from xin (xinZero: xin is all zeros and is not read; the ring may
 // then be a lower-only one). The right-hand side is the prologue's vector

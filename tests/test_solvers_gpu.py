@@ -55,8 +55,10 @@ NAMES = ["poisson16", "poisson_odd_bfs", "poisson_1tile", "random", "many_tiles"
 def ilu_config(kernel, **kw):
     """'ring_wide': the ring kernel with 32-bit row and column ids;
     'ring_rec': with 16-byte row records for levels of 3 entries a row."""
-    c = {"type": "ILU", "kernel": "ring" if kernel in ("ring_wide", "ring_rec", "ring_pair", "ring_cw4", "ring_cw1")
-         else kernel}
+    c = {"type": "ILU", "kernel": "ring" if kernel in ("ring_wide", "ring_rec", "ring_pair", "ring_cw4", "ring_cw1",
+                                                        "ring_nowait") else kernel}
+    if kernel == "ring_nowait":
+        c["waitingWarp"] = False
     if kernel in ("ring_cw4", "ring_cw1"):
         c["computeWarps"] = int(kernel[-1])
     if kernel.startswith("wring"):
@@ -64,8 +66,8 @@ def ilu_config(kernel, **kw):
     if kernel == "ring_wide":
         c["compactRing"] = False
     # Record levels are the default; the plain names run without them.
-    c["recordLevels"] = kernel in ("ring_rec", "ring_pair", "ring_cw4", "ring_cw1", "wring_rec", "wring_pair",
-                                   "wring_w4")
+    c["recordLevels"] = kernel in ("ring_rec", "ring_pair", "ring_cw4", "ring_cw1", "ring_nowait", "wring_rec",
+                                   "wring_pair", "wring_w4")
     if kernel in ("ring_pair", "wring_pair"):
         c["pairRows"] = True
     if kernel == "wring_w4":
@@ -76,7 +78,8 @@ def ilu_config(kernel, **kw):
 
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("dilu", [False, True])
-@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "ring_pair", "ring_wide", "ring_cw4", "ring_cw1", "wring", "wring_rec", "wring_pair",
+@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "ring_pair", "ring_wide", "ring_cw4", "ring_cw1", "ring_nowait",
+                                    "wring", "wring_rec", "wring_pair",
                                     "wring_w4", "warp", "tma", "levels"])
 def test_ilu_bit_exact(oracle, name, dilu, kernel):
     h, om = case(name, oracle)
