@@ -294,8 +294,13 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
     }
   } else if (ty == "GaussSeidel") {
     mark("numSweeps"); mark("numFixedIterations"); mark("solveMulticolor"); mark("workingType");
-    mark("seed"); mark("kernel"); mark("recordLevels"); mark("warpsPerBlock");
+    mark("seed"); mark("kernel"); mark("recordLevels"); mark("warpsPerBlock"); mark("halo");
     readBool(j, "recordLevels", c->ringRecords);
+    if (const Json* v = j.find("halo")) {
+      if (v->text == "stale") c->gsDropHalo = false;
+      else if (v->text == "drop") c->gsDropHalo = true;
+      else fail(GR_EPARSE, "GaussSeidel halo must be \"stale\" or \"drop\"");
+    }
     readInt(j, "warpsPerBlock", c->warpsPerBlock);
     if (c->warpsPerBlock < 1 || c->warpsPerBlock > 8) fail(GR_EINVAL, "warpsPerBlock must be 1..8");
     if (const Json* v = j.find("kernel")) {

@@ -87,6 +87,10 @@ struct SolverConfig {
   // codelet/ipu/matrix/solvers/gauss-seidel.cpp:44) or "diag" (the CodeDSL
   // version, gauss-seidel/Solver.cpp:74).
   bool gsSeedB = true;
+  // Extension: "halo": "stale" (default, the reference: the halo cells keep
+  // the values of the sweep's start, gauss-seidel/Solver.cpp:61) or "drop"
+  // (they read as 0: block Gauss-Seidel without couplings between tiles).
+  bool gsDropHalo = false;
   // PBiCGStab "reduce": false (default, "float64"): dot products and norms
   // accumulate in FP64; true ("f32_ref_order"): in float, in the reference's
   // own reduction order (dsl/tensor/Expression.cpp:472-481, :597-769), with

@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(256) gsSweepKernel(const int* __restrict__ til
                                                       const MV* __restrict__ Gval, const MV* __restrict__ diag,
                                                       const W* __restrict__ b, bool seedB,
                                                       const W* __restrict__ xin, bool xinZero,
-                                                      W* __restrict__ xout, const KState* st) {
+                                                      W* __restrict__ xout, const KState* st, bool dropHalo) {
   extern __shared__ __align__(16) unsigned char smemRaw[];
   if (st && st->done) return;
   const int T = blockIdx.x;
@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(256) gsSweepKernel(const int* __restrict__ til
           if (lc < il) xv = xnew[lc];
           else xv = xinZero ? W(0) : (SMEM ? xold[lc] : xin[c]);
         } else {
-          xv = xinZero ? W(0) : xin[c];
+          xv = xinZero || dropHalo ? W(0) : xin[c];
         }
         sum = sub(sum, mul(cvt<W>(__ldg(Gval + s)), xv));
       }
@@ -359,14 +359,14 @@ void iluApplyT(DeviceMatrix& A, const void* Lval, const void* Uval, const void* 
 
 template <class MV, class W>
 void gsSweepT(DeviceMatrix& A, const void* Gval, const void* b, bool seedB, const void* xin, bool xinZero,
-              void* xout, const KState* st, cudaStream_t s) {
+              void* xout, const KState* st, cudaStream_t s, bool dropHalo) {
   LevelSchedule& G = A.schedule(SweepEntries::All);
   const size_t bytes = 2 * static_cast<size_t>(A.host->maxTileRows) * sizeof(W);
   auto args = [&](auto kernel, size_t smem) {
     kernel<<<A.P, 256, smem, s>>>(A.tileStart.as<int>(), dev::schedView(G), static_cast<const MV*>(Gval),
                                   A.diag.as<MV>(),
                                   static_cast<const W*>(b), seedB, static_cast<const W*>(xin), xinZero,
-                                  static_cast<W*>(xout), st);
+                                  static_cast<W*>(xout), st, dropHalo);
   };
   if (bytes <= static_cast<size_t>(maxSmem(A))) {
     auto k = dev::gsSweepKernel<MV, W, true>;
@@ -389,12 +389,13 @@ void launchIluApply(DeviceMatrix& A, const void* Lval, const void* Uval, const v
 }
 
 void launchGsSweep(DeviceMatrix& A, const void* Gval, const void* b, bool seedB, const void* xin, bool xinZero,
-                   void* xout, DType W, const KState* st, cudaStream_t s) {
-  if (A.vt == DType::F32 && W == DType::F32) gsSweepT<float, float>(A, Gval, b, seedB, xin, xinZero, xout, st, s);
+                   void* xout, DType W, const KState* st, cudaStream_t s, bool dropHalo) {
+  if (A.vt == DType::F32 && W == DType::F32)
+    gsSweepT<float, float>(A, Gval, b, seedB, xin, xinZero, xout, st, s, dropHalo);
   else if (A.vt == DType::F32 && W == DType::F64)
-    gsSweepT<float, double>(A, Gval, b, seedB, xin, xinZero, xout, st, s);
+    gsSweepT<float, double>(A, Gval, b, seedB, xin, xinZero, xout, st, s, dropHalo);
   else if (A.vt == DType::F64 && W == DType::F64)
-    gsSweepT<double, double>(A, Gval, b, seedB, xin, xinZero, xout, st, s);
+    gsSweepT<double, double>(A, Gval, b, seedB, xin, xinZero, xout, st, s, dropHalo);
   else fail(GR_EUNSUPPORTED, "Gauss-Seidel with float64 coefficients needs float64 vectors");
 }
 

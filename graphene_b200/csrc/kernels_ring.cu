@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
     const unsigned char* __restrict__ stream, const long long* __restrict__ tileOffset, const int4* __restrict__ meta,
     const int* __restrict__ tileLevel, const int* __restrict__ tileStart, const int* __restrict__ haloStart,
     const int* __restrict__ haloSrc, int ringBytes, int metaLevels, bool seedB, SPro<X> pro,
-    const X* __restrict__ xin, bool xinZero, X* __restrict__ xout, int* errFlag, bool inPlace) {
+    const X* __restrict__ xin, bool xinZero, X* __restrict__ xout, int* errFlag, bool inPlace, bool dropHalo) {
   constexpr int kRingCompute = RingShape<W>::compute;
   constexpr int kRingLevelSync = RingShape<W>::levelSync;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -500,7 +500,7 @@ __global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
     }
     for (int i = threadIdx.x; i < nRows; i += bd) xs[s0 + i] = xinZero ? W(0) : cvt<W>(xin[base + i]);
     for (int h = threadIdx.x; h < nHalo; h += bd)
-      xs[hb + h] = xinZero ? W(0) : cvt<W>(xin[haloSrc[h0 + h]]);
+      xs[hb + h] = xinZero || dropHalo ? W(0) : cvt<W>(xin[haloSrc[h0 + h]]);
     if (lead) xs[hb + nHalo] = W(0);
   }
   __syncthreads();
@@ -808,7 +808,8 @@ __global__ void __launch_bounds__(256) gsWarpRingKernel(
     const unsigned char* __restrict__ stream, const long long* __restrict__ tileOffset, const int4* __restrict__ meta,
     const int* __restrict__ tileLevel, const int* __restrict__ tileStart, const int* __restrict__ haloStart,
     const int* __restrict__ haloSrc, int P, int ringBytes, int metaLevels, uint32_t sliceBytes, bool seedB,
-    SPro<X> pro, const X* __restrict__ xin, bool xinZero, X* __restrict__ xout, int* errFlag, bool inPlace) {
+    SPro<X> pro, const X* __restrict__ xin, bool xinZero, X* __restrict__ xout, int* errFlag, bool inPlace,
+    bool dropHalo) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int w = static_cast<int>(threadIdx.x >> 5), lane = static_cast<int>(threadIdx.x & 31);
   const int T = static_cast<int>(blockIdx.x) * static_cast<int>(blockDim.x >> 5) + w;
@@ -879,7 +880,7 @@ __global__ void __launch_bounds__(256) gsWarpRingKernel(
     for (int j = 0; j < kRows; ++j)
       if (i0 + j * 32 < nRows) xs[s0 + i0 + j * 32] = v[j];
   }
-  for (int h = lane; h < nHalo; h += 32) xs[hb + h] = xinZero ? W(0) : cvt<W>(xin[haloSrc[h0 + h]]);
+  for (int h = lane; h < nHalo; h += 32) xs[hb + h] = xinZero || dropHalo ? W(0) : cvt<W>(xin[haloSrc[h0 + h]]);
   if (lane == 0) xs[hb + nHalo] = W(0);
   __syncwarp();
   int l = 0;
@@ -977,7 +978,7 @@ inline size_t gsWarpRingSlice(const LevelRing& R, DType W) {
 }
 template <class MV, class X, class W>
 void gsRingT(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& p, bool seedB,
-             const void* xin, bool xinZero, void* xout, int warps, cudaStream_t s) {
+             const void* xin, bool xinZero, void* xout, int warps, cudaStream_t s, bool dropHalo) {
   if (R.kind == RingKind::Ilu) fail(GR_EINVAL, "not a Gauss-Seidel ring");
   if (R.kind == RingKind::GaussSeidelLower && !xinZero)
     fail(GR_EINVAL, "a lower-only Gauss-Seidel ring sweeps from x = 0 only");
@@ -995,7 +996,7 @@ void gsRingT(DeviceMatrix& A, const LevelRing& R, const void* stream, const Prol
         static_cast<const unsigned char*>(stream), R.tileOffset.as<long long>(), R.meta.as<int4>(),
         R.tileLevel.as<int>(), R.groupStart.as<int>(), R.haloStart.as<int>(), R.haloSrc.as<int>(), R.numGroups,
         static_cast<int>(R.ringBytes), R.maxTileLevels, static_cast<uint32_t>(slice), seedB, pro,
-        static_cast<const X*>(xin), xinZero, static_cast<X*>(xout), A.errFlag.as<int>(), R.gsInPlace);
+        static_cast<const X*>(xin), xinZero, static_cast<X*>(xout), A.errFlag.as<int>(), R.gsInPlace, dropHalo);
     checkLaunch("gs_warp_ring");
     return;
   }
@@ -1010,7 +1011,7 @@ void gsRingT(DeviceMatrix& A, const LevelRing& R, const void* stream, const Prol
       static_cast<const unsigned char*>(stream), R.tileOffset.as<long long>(), R.meta.as<int4>(),
       R.tileLevel.as<int>(), R.groupStart.as<int>(), R.haloStart.as<int>(), R.haloSrc.as<int>(),
       static_cast<int>(R.ringBytes), R.maxTileLevels, seedB, pro, static_cast<const X*>(xin), xinZero,
-      static_cast<X*>(xout), A.errFlag.as<int>(), R.gsInPlace);
+      static_cast<X*>(xout), A.errFlag.as<int>(), R.gsInPlace, dropHalo);
   checkLaunch("gs_ring");
 }
 }  // namespace
@@ -1020,15 +1021,15 @@ size_t gsWarpRingSmem(const LevelRing& R, DType W, int warpsPerBlock) {
 }
 
 void launchGsRing(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& pro, bool seedB,
-                  const void* xin, bool xinZero, void* xout, DType X, DType W, cudaStream_t s, int warps) {
+                  const void* xin, bool xinZero, void* xout, DType X, DType W, cudaStream_t s, int warps, bool dropHalo) {
   if (A.vt == DType::F32 && X == DType::F32 && W == DType::F32)
-    gsRingT<float, float, float>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s);
+    gsRingT<float, float, float>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s, dropHalo);
   else if (A.vt == DType::F32 && X == DType::F32 && W == DType::F64)
-    gsRingT<float, float, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s);
+    gsRingT<float, float, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s, dropHalo);
   else if (A.vt == DType::F32 && X == DType::F64 && W == DType::F64)
-    gsRingT<float, double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s);
+    gsRingT<float, double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s, dropHalo);
   else if (A.vt == DType::F64 && X == DType::F64 && W == DType::F64)
-    gsRingT<double, double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s);
+    gsRingT<double, double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s, dropHalo);
   else
     fail(GR_EUNSUPPORTED, "Gauss-Seidel: float64 coefficients need float64 vectors, and the working type must be "
                           "the vectors' type or float64 over float32 vectors");

@@ -108,7 +108,8 @@ void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool
 // warps > 0: the warp-per-tile form (gsWarpRingKernel) with `warps` tiles a
 // block; gsWarpRingSmem gives its dynamic shared memory.
 void launchGsRing(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& pro, bool seedB,
-                  const void* xin, bool xinZero, void* xout, DType X, DType W, cudaStream_t s, int warps = 0);
+                  const void* xin, bool xinZero, void* xout, DType X, DType W, cudaStream_t s, int warps = 0,
+                  bool dropHalo = false);
 size_t gsWarpRingSmem(const LevelRing& R, DType W, int warpsPerBlock);
 // Warp-per-tile substitution (kernels_warp.cu): shared memory per block and
 // the number of rows per lane to prefetch.
@@ -122,7 +123,8 @@ void launchIluWarp(DeviceMatrix& A, const SweepStream& S, const void* stream, bo
 // seedB: start each row from b (true) or from the diagonal (false).
 // Gval: packed values of the All schedule.
 void launchGsSweep(DeviceMatrix& A, const void* Gval, const void* b, bool seedB, const void* xin,
-                   bool xinZero, void* xout, DType W, const KState* st, cudaStream_t s);
+                   bool xinZero, void* xout, DType W, const KState* st, cudaStream_t s,
+                   bool dropHalo = false);
 
 // ---- Krylov kernels ----------------------------------------------------
 // r = b - A x, r0 = r; state initialised (norm, rho = r0.r, flags).

@@ -275,7 +275,7 @@ class GsNode : public Node {
     void* cur = x;
     void* other = tmp_.get();
     for (int k = 0; k < count; ++k) {
-      launchGsSweep(A_, Gval_.get(), b, cfg_.gsSeedB, cur, xZero && k == 0, other, W, gate, s());
+      launchGsSweep(A_, Gval_.get(), b, cfg_.gsSeedB, cur, xZero && k == 0, other, W, gate, s(), cfg_.gsDropHalo);
       std::swap(cur, other);
     }
     if (cur != x) GR_CUDA(cudaMemcpyAsync(x, cur, A_.n * dtypeSize(W), cudaMemcpyDeviceToDevice, s()));
@@ -372,7 +372,8 @@ class GsNode : public Node {
     for (int k = 0; k < count; ++k) {
       const bool zero = xZero && k == 0;
       launchGsRing(A_, zero ? *ringLo_ : *ring_, zero ? streamLo_.get() : stream_.get(), k == 0 ? first : plain,
-                   cfg_.gsSeedB, cur, zero, other, W, computeType(W), s(), warpRing_ ? cfg_.warpsPerBlock : 0);
+                   cfg_.gsSeedB, cur, zero, other, W, computeType(W), s(), warpRing_ ? cfg_.warpsPerBlock : 0,
+                   cfg_.gsDropHalo);
       std::swap(cur, other);
     }
     if (cur != x) GR_CUDA(cudaMemcpyAsync(x, cur, A_.n * dtypeSize(W), cudaMemcpyDeviceToDevice, s()));

@@ -210,6 +210,7 @@ struct Conf {
   int extendedType = -1;    // -1: x.type(); 0 f32, 1 f64, 2 dw
   int maxRestarts = 1;
   int gsSeedB = 1;          // extension: 1 seeds Gauss-Seidel rows with b
+  int gsDropHalo = 0;       // extension: 1 takes halo values as 0 ("halo": "drop")
   // extension: PBiCGStab dot products and norms in the reference's own
   // reduction order and operand type ("reduce": "f32_ref_order") instead of
   // FP64 accumulation ("float64", the default).
@@ -251,6 +252,7 @@ std::unique_ptr<Conf> parseConf(const JVal& j) {
   if (auto v = j.get("workingType")) c->workingType = parseTypeName(v->s);
   if (auto v = j.get("extendedPrecisionType")) c->extendedType = parseTypeName(v->s);
   if (auto v = j.get("seed")) c->gsSeedB = (v->s == "b") ? 1 : 0;
+  if (auto v = j.get("halo")) c->gsDropHalo = (v->s == "drop") ? 1 : 0;
   if (auto v = j.get("reduce")) {
     if (v->s == "f32_ref_order") c->reduceRef = true;
     else if (v->s == "float64") c->reduceRef = false;
@@ -878,13 +880,17 @@ void iluSolve(const or_matrix& A, const std::vector<std::vector<V>>& off,
 // each row computed in the working type W (:76-82, every operand cast to
 // it) and stored in x's type T (:83).
 template <class V, class T, class W = T>
+// dropHalo: the halo cells read as 0 (a block Gauss-Seidel that drops the
+// couplings between tiles) instead of the values the exchange brings.
 void gsSweep(const or_matrix& A, const TileValues<V>& tv, std::vector<T>& x, const std::vector<T>& b,
-             bool seedB) {
+             bool seedB, bool dropHalo = false) {
   exchange(A, x);
   forTiles(A.P, [&](size_t t) {
     const Local& L = A.loc[t];
     const size_t nRows = L.diag.size();
     const size_t hb = A.haloStart[t];
+    if (dropHalo)
+      for (size_t h = hb + nRows; h < A.haloStart[t + 1]; ++h) x[h] = static_cast<T>(0);
     for (size_t i = 0; i < nRows; ++i) {
       W sum = seedB ? static_cast<W>(b[hb + i]) : static_cast<W>(tv.diag[t][i]);
       for (size_t j = L.rowPtr[i]; j < L.rowPtr[i + 1]; ++j)
@@ -962,7 +968,7 @@ struct GsNode : SolverNode<V, T> {
   Stats solveIn(std::vector<T>& x, const std::vector<T>& b) {
     Stats s;
     if (c.numFixedIterations > 0) {
-      for (int k = 0; k < c.numFixedIterations; ++k) gsSweep<V, T, W>(C.A, C.tv, x, b, c.gsSeedB);
+      for (int k = 0; k < c.numFixedIterations; ++k) gsSweep<V, T, W>(C.A, C.tv, x, b, c.gsSeedB, c.gsDropHalo);
       s.iterations = c.numFixedIterations;
       return s;
     }
@@ -972,7 +978,7 @@ struct GsNode : SolverNode<V, T> {
     s.init = s.fin = normT(C.A, r, c.norm);
     while (!((s.converged && s.iterations >= c.minIterations) || s.iterations >= c.maxIterations)) {
       for (int k = 0; k < c.numSweeps; ++k) {
-        gsSweep<V, T, W>(C.A, C.tv, x, b, c.gsSeedB);
+        gsSweep<V, T, W>(C.A, C.tv, x, b, c.gsSeedB, c.gsDropHalo);
         s.iterations++;
       }
       residualT<V, T, T, W, W>(C.A, C.tv, x, b, r);
@@ -1621,14 +1627,14 @@ int or_ilu_solve(const or_matrix* A, int dilu, const double* factor_off, const d
   });
 }
 
-int or_gs_sweep(const or_matrix* A, void* x, const void* b, int t, int seed_b) {
+int or_gs_sweep(const or_matrix* A, void* x, const void* b, int t, int seed_b, int drop_halo) {
   return guard([&] {
     auto run = [&](auto vtag, auto ttag) {
       using V = decltype(vtag);
       using T = decltype(ttag);
       auto xv = withHalo(*A, static_cast<const T*>(x));
       auto bv = withHalo(*A, static_cast<const T*>(b));
-      gsSweep<V, T>(*A, TileValues<V>(*A), xv, bv, seed_b != 0);
+      gsSweep<V, T>(*A, TileValues<V>(*A), xv, bv, seed_b != 0, drop_halo != 0);
       stripHalo(*A, xv, static_cast<T*>(x));
     };
     if (A->vt == 0 && t == 0) run(float(), float());

@@ -94,7 +94,7 @@ int or_ilu_solve(const or_matrix* A, int dilu, const double* factor_off, const d
  * at the start. seed_b: 1 seeds each row with b (the codelet spec,
  * codelet/ipu/matrix/solvers/gauss-seidel.cpp:44), 0 with the diagonal as the
  * reference's CodeDSL version does (gauss-seidel/Solver.cpp:74). */
-int or_gs_sweep(const or_matrix* A, void* x, const void* b, int t, int seed_b);
+int or_gs_sweep(const or_matrix* A, void* x, const void* b, int t, int seed_b, int drop_halo);
 
 typedef struct {
   double initial_residual, final_residual, b_norm;

@@ -60,7 +60,7 @@ class Oracle:
             "or_ref_norm": (C.c_double, [vp, vp, C.c_int, C.c_int]),
             "or_ilu_factorize": (C.c_int, [vp, C.c_int, vp, vp]),
             "or_ilu_solve": (C.c_int, [vp, C.c_int, vp, vp, vp, vp, C.c_int]),
-            "or_gs_sweep": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),
+            "or_gs_sweep": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int]),
             "or_solve": (C.c_int, [vp, C.c_char_p, vp, C.c_int, vp, C.c_int, C.POINTER(OrStats),
                                    vp, vp, C.c_int]),
             "or_generate_nnz": (i64, [i64, i64, i64]),
@@ -253,11 +253,11 @@ class OMatrix:
                                            _p(np.ascontiguousarray(b)), _p(x), t))
         return x
 
-    def gs_sweep(self, x, b, seed_b=True):
+    def gs_sweep(self, x, b, seed_b=True, drop_halo=False):
         t = 0 if x.dtype == np.float32 else 1
         x = np.array(x, copy=True)
         self.o.check(self.o.L.or_gs_sweep(self.h, _p(x), _p(np.ascontiguousarray(b)), t,
-                                          int(seed_b)))
+                                          int(seed_b), int(drop_halo)))
         return x
 
     def solve(self, config: str, x, b, history_len=0, want_phi=False):

@@ -60,6 +60,7 @@ def test_comments_and_unknown_keys():
     ({"type": "PBiCGStab", "workingType": "float16x"}, 3),            # parseType
     ({"type": "ILU", "solveMulticolor": "sometimes"}, 3),             # Configuration.cpp:66-69
     ({"type": "PBiCGStab", "maxIterations": "many"}, 3),
+    ({"type": "GaussSeidel", "halo": "fresh"}, 3),                    # stale | drop
 ])
 def test_invalid_configs(cfg, code):
     with pytest.raises(gb.GrapheneError) as e:
@@ -70,6 +71,14 @@ def test_invalid_configs(cfg, code):
 def test_multicolor_modes_accept_bool_and_strings():
     for v in [True, False, "on", "off", "auto", "true"]:
         gb.Configuration.fromJSON({"type": "ILU", "solveMulticolor": v, "factorizeMulticolor": v})
+
+
+def test_gauss_seidel_halo_modes():
+    """"halo": "stale" (the reference's sweep, halo cells hold the values of the
+    last exchange) and "drop" (halo cells read as 0) are both known keys."""
+    for v in ["stale", "drop"]:
+        c = gb.Configuration.fromJSON({"type": "GaussSeidel", "halo": v})
+        assert "halo" not in c.unknownKeys
 
 
 def test_malformed_json():

@@ -161,6 +161,32 @@ def test_gauss_seidel_bit_exact(oracle, name, sweeps, seed, kernel):
     np.testing.assert_array_equal(host(x), ref)
 
 
+@pytest.mark.parametrize("name", ["poisson16", "poisson_odd_bfs", "many_tiles"])
+@pytest.mark.parametrize("kernel", ["ring", "wring", "levels"])
+@pytest.mark.parametrize("start", ["x0", "zero"])
+def test_gauss_seidel_drop_halo_bit_exact(oracle, name, kernel, start):
+    """"halo": "drop": the halo cells read as 0 in every sweep (block
+    Gauss-Seidel); two sweeps, from a nonzero x and from x = 0, same bits as
+    the oracle's sweep with the halo zeroed."""
+    h, om = case(name, oracle)
+    A = h.copyToTile()
+    rng = np.random.default_rng(13)
+    b = rng.uniform(-1, 1, h.numRows).astype(np.float32)
+    x0 = rng.uniform(-1, 1, h.numRows).astype(np.float32) if start == "x0" else np.zeros(h.numRows, np.float32)
+    x = dev(x0)
+    cfg = {"type": "GaussSeidel", "numFixedIterations": 2, "kernel": kernel, "halo": "drop"}
+    gb.Solver(A, cfg).solve(x, dev(b))
+    ref = x0
+    for _ in range(2):
+        ref = om.gs_sweep(ref, b, drop_halo=True)
+    np.testing.assert_array_equal(host(x), ref)
+    if h.numTiles > 1 and start == "x0":
+        stale = x0
+        for _ in range(2):
+            stale = om.gs_sweep(stale, b)
+        assert not np.array_equal(ref, stale)
+
+
 @pytest.mark.parametrize("name", ["poisson16", "random", "many_tiles"])
 @pytest.mark.parametrize("vt", ["f32", "f64", "f32_matrix_f64_vectors"])
 @pytest.mark.parametrize("kernel", ["ring", "wring"])
