@@ -256,8 +256,9 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
     readInt(j, "computeWarps", c->computeWarps);
     mark("waitingWarp");
     readBool(j, "waitingWarp", c->waitingWarp);
-    if (c->computeWarps != 0 && c->computeWarps != 1 && c->computeWarps != 2 && c->computeWarps != 4)
-      fail(GR_EINVAL, "computeWarps must be 1, 2 or 4");
+    if (c->computeWarps != 0 && c->computeWarps != 1 && c->computeWarps != 2 && c->computeWarps != 4 &&
+        c->computeWarps != 8)
+      fail(GR_EINVAL, "computeWarps must be 1, 2, 4 or 8");
     if (c->warpsPerBlock < 1 || c->warpsPerBlock > 8) fail(GR_EINVAL, "warpsPerBlock must be 1..8");
     readBool(j, "compactRing", c->compactRing);
     readBool(j, "pairRows", c->pairRows);
@@ -294,8 +295,9 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
     }
   } else if (ty == "GaussSeidel") {
     mark("numSweeps"); mark("numFixedIterations"); mark("solveMulticolor"); mark("workingType");
-    mark("seed"); mark("kernel"); mark("recordLevels"); mark("warpsPerBlock"); mark("halo");
+    mark("seed"); mark("kernel"); mark("recordLevels"); mark("warpsPerBlock"); mark("halo"); mark("pairRows");
     readBool(j, "recordLevels", c->ringRecords);
+    readBool(j, "pairRows", c->gsPairRows);
     if (const Json* v = j.find("halo")) {
       if (v->text == "stale") c->gsDropHalo = false;
       else if (v->text == "drop") c->gsDropHalo = true;

@@ -23,6 +23,7 @@
 // the matrix's error word, the other waits give up, and the issuing lane
 // waits (bounded) for the copies still in flight before the block exits.
 #include <algorithm>
+#include <climits>
 
 #include "bulk.cuh"
 #include "device.hpp"
@@ -499,8 +500,23 @@ __global__ void __launch_bounds__(RingShape<W>::threads) gsRingKernel(
       }
     }
     for (int i = threadIdx.x; i < nRows; i += bd) xs[s0 + i] = xinZero ? W(0) : cvt<W>(xin[base + i]);
-    for (int h = threadIdx.x; h < nHalo; h += bd)
-      xs[hb + h] = xinZero || dropHalo ? W(0) : cvt<W>(xin[haloSrc[h0 + h]]);
+    if (xinZero || dropHalo) {
+      for (int h = threadIdx.x; h < nHalo; h += bd) xs[hb + h] = W(0);
+    } else {
+      // Four halo cells a thread: their source indices, then their values.
+      constexpr int kH = 4;
+      for (int h = threadIdx.x; h < nHalo; h += kH * bd) {
+        int src[kH];
+#pragma unroll
+        for (int j = 0; j < kH; ++j) src[j] = h + j * bd < nHalo ? haloSrc[h0 + h + j * bd] : -1;
+        W hv[kH];
+#pragma unroll
+        for (int j = 0; j < kH; ++j) hv[j] = src[j] >= 0 ? cvt<W>(xin[src[j]]) : W(0);
+#pragma unroll
+        for (int j = 0; j < kH; ++j)
+          if (src[j] >= 0) xs[hb + h + j * bd] = hv[j];
+      }
+    }
     if (lead) xs[hb + nHalo] = W(0);
   }
   __syncthreads();
@@ -757,16 +773,71 @@ __global__ void __launch_bounds__(256) iluWarpRingKernel(const unsigned char* __
 }
 
 // Level l's rows of a Gauss-Seidel sweep for thread t of `stride` threads
-// (gsRingKernel's compute warps' operations, in the same order).
-template <int STRIDE, class MV, class X, class W, bool COMPACT>
+// (gsRingKernel's compute warps' operations, in the same order). PAIR: a
+// thread takes rows q and q + STRIDE together, both rows' loads before
+// either's arithmetic and stores (rows of one level never read each other),
+// so a level of up to 2 * STRIDE rows costs one dependent chain, not two.
+template <int STRIDE, bool PAIR, class MV, class X, class W, bool COMPACT>
 __device__ __forceinline__ void gsLevelRows(const RingLevel<MV, COMPACT>& cur, int t, bool seedB, const W* rhs,
                                             W* xs) {
+  constexpr int kStep = PAIR ? 2 * STRIDE : STRIDE;
   if (cur.rec) {
-    for (int q = t; q < cur.k; q += STRIDE) {
+    for (int q = t; q < cur.k; q += kStep) {
       const RowRecord r = ringRecord(cur, q, true);
-      const W d = cvt<W>(r.inv);
-      const W sum = recordDot(seedB ? rhs[r.row] : d, r, xs);
-      xs[r.row] = storeRound<X>(dvd(sum, d));
+      if (PAIR && q + STRIDE < cur.k) {
+        const RowRecord r2 = ringRecord(cur, q + STRIDE, true);
+        const W d = cvt<W>(r.inv), d2 = cvt<W>(r2.inv);
+        const W s1 = recordDot(seedB ? rhs[r.row] : d, r, xs);
+        const W s2 = recordDot(seedB ? rhs[r2.row] : d2, r2, xs);
+        xs[r.row] = storeRound<X>(dvd(s1, d));
+        xs[r2.row] = storeRound<X>(dvd(s2, d2));
+      } else {
+        const W d = cvt<W>(r.inv);
+        const W sum = recordDot(seedB ? rhs[r.row] : d, r, xs);
+        xs[r.row] = storeRound<X>(dvd(sum, d));
+      }
+    }
+    return;
+  }
+  if (cur.E <= 8) {
+    // Every entry's slot and value first, then the x values, then the sums
+    // in order: the loads overlap.
+    for (int q = t; q < cur.k; q += kStep) {
+      constexpr int kR = PAIR ? 2 : 1;
+      int il[kR], c[kR][8];
+      MV v[kR][8];
+      W d[kR], sum[kR], xv[kR][8];
+      bool on[kR];
+#pragma unroll
+      for (int u = 0; u < kR; ++u) {
+        const int qq = q + u * STRIDE;
+        on[u] = u == 0 || qq < cur.k;
+        if (on[u]) {
+          il[u] = cur.row(qq);
+          d[u] = cvt<W>(cur.invDiag(qq));
+#pragma unroll
+          for (int e = 0; e < 8; ++e)
+            if (e < cur.E) cur.entry(e, qq, c[u][e], v[u][e]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kR; ++u)
+        if (on[u]) {
+          sum[u] = seedB ? rhs[il[u]] : d[u];
+#pragma unroll
+          for (int e = 0; e < 8; ++e)
+            if (e < cur.E) xv[u][e] = xs[c[u][e]];
+        }
+#pragma unroll
+      for (int u = 0; u < kR; ++u)
+        if (on[u]) {
+#pragma unroll
+          for (int e = 0; e < 8; ++e)
+            if (e < cur.E) sum[u] = sub(sum[u], mul(cvt<W>(v[u][e]), xv[u][e]));
+        }
+#pragma unroll
+      for (int u = 0; u < kR; ++u)
+        if (on[u]) xs[il[u]] = storeRound<X>(dvd(sum[u], d[u]));
     }
     return;
   }
@@ -774,26 +845,11 @@ __device__ __forceinline__ void gsLevelRows(const RingLevel<MV, COMPACT>& cur, i
     const int il = cur.row(q);
     const W d = cvt<W>(cur.invDiag(q));
     W sum = seedB ? rhs[il] : d;
-    if (cur.E <= 8) {
-      int c[8];
-      MV v[8];
-#pragma unroll
-      for (int e = 0; e < 8; ++e)
-        if (e < cur.E) cur.entry(e, q, c[e], v[e]);
-      W xv[8];
-#pragma unroll
-      for (int e = 0; e < 8; ++e)
-        if (e < cur.E) xv[e] = xs[c[e]];
-#pragma unroll
-      for (int e = 0; e < 8; ++e)
-        if (e < cur.E) sum = sub(sum, mul(cvt<W>(v[e]), xv[e]));
-    } else {
-      for (int e = 0; e < cur.E; ++e) {
-        int c;
-        MV v;
-        cur.entry(e, q, c, v);
-        sum = sub(sum, mul(cvt<W>(v), xs[c]));
-      }
+    for (int e = 0; e < cur.E; ++e) {
+      int c;
+      MV v;
+      cur.entry(e, q, c, v);
+      sum = sub(sum, mul(cvt<W>(v), xs[c]));
     }
     xs[il] = storeRound<X>(dvd(sum, d));
   }
@@ -809,7 +865,7 @@ __global__ void __launch_bounds__(256) gsWarpRingKernel(
     const int* __restrict__ tileLevel, const int* __restrict__ tileStart, const int* __restrict__ haloStart,
     const int* __restrict__ haloSrc, int P, int ringBytes, int metaLevels, uint32_t sliceBytes, bool seedB,
     SPro<X> pro, const X* __restrict__ xin, bool xinZero, X* __restrict__ xout, int* errFlag, bool inPlace,
-    bool dropHalo) {
+    bool dropHalo, bool pairRows) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int w = static_cast<int>(threadIdx.x >> 5), lane = static_cast<int>(threadIdx.x & 31);
   const int T = static_cast<int>(blockIdx.x) * static_cast<int>(blockDim.x >> 5) + w;
@@ -839,56 +895,83 @@ __global__ void __launch_bounds__(256) gsWarpRingKernel(
   __syncwarp();
   int issued = 0;
   uint32_t src = 0;
+  // issueAfter of the next level to copy, kept in a register (levels never
+  // issued: INT_MAX), so a level with nothing to issue costs one compare.
+  int nextAfter = L > 0 ? RingLevelCode::issueAfter(mt[0]) : INT_MAX;
   auto issueUpTo = [&](int done) {
-    while (issued < L) {
+    while (nextAfter <= done) {
       const int4 m = mt[issued];
-      if (RingLevelCode::issueAfter(m) > done) break;
       const uint32_t bytes = RingLevelCode::bytes(m);
       const uint32_t bar = smemAddr(full + issued % kRingBarriers);
       mbarExpectTx(bar, bytes);
       bulkLoad(smemAddr(ring + RingLevelCode::ringOffset(m)), g + src, bytes, bar);
       src += bytes;
       ++issued;
+      nextAfter = issued < L ? RingLevelCode::issueAfter(mt[issued]) : INT_MAX;
     }
   };
   if (lane == 0) issueUpTo(-1);
   constexpr int kRows = sizeof(W) == 4 ? 16 : 8;
-  if (seedB || pro.kind != static_cast<int>(Prologue::Plain)) {
+  {
+    // The right-hand side (seedB, with the fused p / s update) and the start
+    // values of kRows rows a lane at once, all loads before any store.
+    const bool withRhs = seedB || pro.kind != static_cast<int>(Prologue::Plain);
     X beta = X(0), omega = X(0), alpha = X(0);
     bool first = true;
-    if (st) {
+    if (withRhs && st) {
       beta = cvt<X>(st->beta);
       omega = cvt<X>(st->omega);
       alpha = cvt<X>(st->alpha);
       first = st->iter == 0;
     }
     for (int i0 = lane; i0 < nRows; i0 += 32 * kRows) {
-      X v[kRows];
-      pro.template rows<kRows>(base + i0, 32, base + nRows, beta, omega, alpha, first, v);
-      if (seedB) {
+      W xv[kRows];
+#pragma unroll
+      for (int j = 0; j < kRows; ++j)
+        xv[j] = !xinZero && i0 + j * 32 < nRows ? cvt<W>(xin[base + i0 + j * 32]) : W(0);
+      if (withRhs) {
+        X v[kRows];
+        pro.template rows<kRows>(base + i0, 32, base + nRows, beta, omega, alpha, first, v);
+        if (seedB) {
+#pragma unroll
+          for (int j = 0; j < kRows; ++j)
+            if (i0 + j * 32 < nRows) rhs[i0 + j * 32] = cvt<W>(v[j]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kRows; ++j)
+        if (i0 + j * 32 < nRows) xs[s0 + i0 + j * 32] = xv[j];
+    }
+    // Halo cells: kRows source indices a lane, then their values.
+    if (xinZero || dropHalo) {
+      for (int h = lane; h < nHalo; h += 32) xs[hb + h] = W(0);
+    } else {
+      for (int h = lane; h < nHalo; h += 32 * kRows) {
+        int src[kRows];
+#pragma unroll
+        for (int j = 0; j < kRows; ++j) src[j] = h + j * 32 < nHalo ? haloSrc[h0 + h + j * 32] : -1;
+        W hv[kRows];
+#pragma unroll
+        for (int j = 0; j < kRows; ++j) hv[j] = src[j] >= 0 ? cvt<W>(xin[src[j]]) : W(0);
 #pragma unroll
         for (int j = 0; j < kRows; ++j)
-          if (i0 + j * 32 < nRows) rhs[i0 + j * 32] = cvt<W>(v[j]);
+          if (src[j] >= 0) xs[hb + h + j * 32] = hv[j];
       }
     }
   }
-  for (int i0 = lane; i0 < nRows; i0 += 32 * kRows) {
-    W v[kRows];
-#pragma unroll
-    for (int j = 0; j < kRows; ++j) v[j] = !xinZero && i0 + j * 32 < nRows ? cvt<W>(xin[base + i0 + j * 32]) : W(0);
-#pragma unroll
-    for (int j = 0; j < kRows; ++j)
-      if (i0 + j * 32 < nRows) xs[s0 + i0 + j * 32] = v[j];
-  }
-  for (int h = lane; h < nHalo; h += 32) xs[hb + h] = xinZero || dropHalo ? W(0) : cvt<W>(xin[haloSrc[h0 + h]]);
   if (lane == 0) xs[hb + nHalo] = W(0);
   __syncwarp();
   int l = 0;
   bool bad = false;
+  // The next level's table entry is decoded before the wait for its block.
+  RingLevel<MV, COMPACT> nxt = ringLevelAt<MV, COMPACT>(L > 0 ? mt[0] : make_int4(0, 0, 0, 0), ring);
   for (; l < L; ++l) {
+    const RingLevel<MV, COMPACT> cur = nxt;
+    if (l + 1 < L) nxt = ringLevelAt<MV, COMPACT>(mt[l + 1], ring);
     bad = !mbarWaitBounded(smemAddr(full + l % kRingBarriers), (l / kRingBarriers) & 1);
     if (__any_sync(0xFFFFFFFFu, bad)) break;
-    gsLevelRows<32, MV, X, W, COMPACT>(ringLevelAt<MV, COMPACT>(mt[l], ring), lane, seedB, rhs, xs);
+    if (pairRows) gsLevelRows<32, true, MV, X, W, COMPACT>(cur, lane, seedB, rhs, xs);
+    else gsLevelRows<32, false, MV, X, W, COMPACT>(cur, lane, seedB, rhs, xs);
     __syncwarp();
     if (lane == 0) issueUpTo(l);
   }
@@ -930,13 +1013,14 @@ template <class MV, class W>
 void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& p, void* y,
                 int l2Ahead, bool unroll, bool pairRows, cudaStream_t s, int computeWarps, bool waiter) {
   const size_t smem = iluRingSmem(A, R, dtypeOf<W>());
-  if (computeWarps != 0 && computeWarps != 1 && computeWarps != 2 && computeWarps != 4)
-    fail(GR_EINVAL, "computeWarps must be 1, 2 or 4 (0: the default)");
+  if (computeWarps != 0 && computeWarps != 1 && computeWarps != 2 && computeWarps != 4 && computeWarps != 8)
+    fail(GR_EINVAL, "computeWarps must be 1, 2, 4 or 8 (0: the default)");
   if (!waiter && computeWarps != 0) fail(GR_EINVAL, "waitingWarp false needs the default computeWarps");
   auto kernel = !waiter             ? ringKernelFor<MV, W, 0, false>(R.compact, unroll)
                 : computeWarps == 1 ? ringKernelFor<MV, W, 1>(R.compact, unroll)
                 : computeWarps == 2 ? ringKernelFor<MV, W, 2>(R.compact, unroll)
                 : computeWarps == 4 ? ringKernelFor<MV, W, 4>(R.compact, unroll)
+                : computeWarps == 8 ? ringKernelFor<MV, W, 8>(R.compact, unroll)
                                     : ringKernelFor<MV, W, 0>(R.compact, unroll);
   const int threads = (computeWarps > 0 ? 32 * computeWarps : dev::RingShape<W>::compute) + (waiter ? 64 : 32);
   ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
@@ -978,7 +1062,7 @@ inline size_t gsWarpRingSlice(const LevelRing& R, DType W) {
 }
 template <class MV, class X, class W>
 void gsRingT(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& p, bool seedB,
-             const void* xin, bool xinZero, void* xout, int warps, cudaStream_t s, bool dropHalo) {
+             const void* xin, bool xinZero, void* xout, int warps, cudaStream_t s, bool dropHalo, bool pairRows) {
   if (R.kind == RingKind::Ilu) fail(GR_EINVAL, "not a Gauss-Seidel ring");
   if (R.kind == RingKind::GaussSeidelLower && !xinZero)
     fail(GR_EINVAL, "a lower-only Gauss-Seidel ring sweeps from x = 0 only");
@@ -996,7 +1080,8 @@ void gsRingT(DeviceMatrix& A, const LevelRing& R, const void* stream, const Prol
         static_cast<const unsigned char*>(stream), R.tileOffset.as<long long>(), R.meta.as<int4>(),
         R.tileLevel.as<int>(), R.groupStart.as<int>(), R.haloStart.as<int>(), R.haloSrc.as<int>(), R.numGroups,
         static_cast<int>(R.ringBytes), R.maxTileLevels, static_cast<uint32_t>(slice), seedB, pro,
-        static_cast<const X*>(xin), xinZero, static_cast<X*>(xout), A.errFlag.as<int>(), R.gsInPlace, dropHalo);
+        static_cast<const X*>(xin), xinZero, static_cast<X*>(xout), A.errFlag.as<int>(), R.gsInPlace, dropHalo,
+        pairRows);
     checkLaunch("gs_warp_ring");
     return;
   }
@@ -1021,15 +1106,16 @@ size_t gsWarpRingSmem(const LevelRing& R, DType W, int warpsPerBlock) {
 }
 
 void launchGsRing(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& pro, bool seedB,
-                  const void* xin, bool xinZero, void* xout, DType X, DType W, cudaStream_t s, int warps, bool dropHalo) {
+                  const void* xin, bool xinZero, void* xout, DType X, DType W, cudaStream_t s, int warps, bool dropHalo,
+                  bool pairRows) {
   if (A.vt == DType::F32 && X == DType::F32 && W == DType::F32)
-    gsRingT<float, float, float>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s, dropHalo);
+    gsRingT<float, float, float>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s, dropHalo, pairRows);
   else if (A.vt == DType::F32 && X == DType::F32 && W == DType::F64)
-    gsRingT<float, float, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s, dropHalo);
+    gsRingT<float, float, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s, dropHalo, pairRows);
   else if (A.vt == DType::F32 && X == DType::F64 && W == DType::F64)
-    gsRingT<float, double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s, dropHalo);
+    gsRingT<float, double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s, dropHalo, pairRows);
   else if (A.vt == DType::F64 && X == DType::F64 && W == DType::F64)
-    gsRingT<double, double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s, dropHalo);
+    gsRingT<double, double, double>(A, R, stream, pro, seedB, xin, xinZero, xout, warps, s, dropHalo, pairRows);
   else
     fail(GR_EUNSUPPORTED, "Gauss-Seidel: float64 coefficients need float64 vectors, and the working type must be "
                           "the vectors' type or float64 over float32 vectors");

@@ -106,10 +106,11 @@ void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool
 // template with the coefficients and the diagonal packed in. Vectors of
 // type X, rows computed in W (X, or float64 over float32 vectors).
 // warps > 0: the warp-per-tile form (gsWarpRingKernel) with `warps` tiles a
-// block; gsWarpRingSmem gives its dynamic shared memory.
+// block (pairRows: a lane takes two rows of a level at once);
+// gsWarpRingSmem gives its dynamic shared memory.
 void launchGsRing(DeviceMatrix& A, const LevelRing& R, const void* stream, const PrologueArgs& pro, bool seedB,
                   const void* xin, bool xinZero, void* xout, DType X, DType W, cudaStream_t s, int warps = 0,
-                  bool dropHalo = false);
+                  bool dropHalo = false, bool pairRows = false);
 size_t gsWarpRingSmem(const LevelRing& R, DType W, int warpsPerBlock);
 // Warp-per-tile substitution (kernels_warp.cu): shared memory per block and
 // the number of rows per lane to prefetch.

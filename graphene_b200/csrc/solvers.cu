@@ -373,7 +373,7 @@ class GsNode : public Node {
       const bool zero = xZero && k == 0;
       launchGsRing(A_, zero ? *ringLo_ : *ring_, zero ? streamLo_.get() : stream_.get(), k == 0 ? first : plain,
                    cfg_.gsSeedB, cur, zero, other, W, computeType(W), s(), warpRing_ ? cfg_.warpsPerBlock : 0,
-                   cfg_.gsDropHalo);
+                   cfg_.gsDropHalo, cfg_.gsPairRows);
       std::swap(cur, other);
     }
     if (cur != x) GR_CUDA(cudaMemcpyAsync(x, cur, A_.n * dtypeSize(W), cudaMemcpyDeviceToDevice, s()));

@@ -144,8 +144,11 @@ def test_ilu_ring_small_rings_bit_exact(oracle, name, frac):
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("sweeps", [1, 2, 3])
 @pytest.mark.parametrize("seed", ["b", "diag"])
-@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "wring", "wring_rec", "levels"])
+@pytest.mark.parametrize("kernel", ["ring", "ring_rec", "wring", "wring_rec", "wring_pair", "wring_rec_pair",
+                                    "levels"])
 def test_gauss_seidel_bit_exact(oracle, name, sweeps, seed, kernel):
+    """'_rec': record levels; '_pair': the warp ring with two rows a lane at
+    once (pairRows)."""
     h, om = case(name, oracle)
     A = h.copyToTile()
     rng = np.random.default_rng(5)
@@ -153,7 +156,8 @@ def test_gauss_seidel_bit_exact(oracle, name, sweeps, seed, kernel):
     x0 = rng.uniform(-1, 1, h.numRows).astype(np.float32)
     x = dev(x0)
     cfg = {"type": "GaussSeidel", "numFixedIterations": sweeps, "seed": seed,
-           "kernel": kernel.replace("_rec", ""), "recordLevels": kernel.endswith("_rec")}
+           "kernel": kernel.split("_")[0], "recordLevels": "_rec" in kernel,
+           "pairRows": kernel.endswith("_pair")}
     gb.Solver(A, cfg).solve(x, dev(b))
     ref = x0
     for _ in range(sweeps):
@@ -209,7 +213,7 @@ def test_gauss_seidel_ring_types_bit_exact(oracle, name, vt, kernel):
 @pytest.mark.parametrize("name", ["poisson16", "random", "many_tiles", "poisson_odd_bfs"])
 @pytest.mark.parametrize("sweeps", [1, 2, 3])
 @pytest.mark.parametrize("records", [False, True])
-@pytest.mark.parametrize("kernel", ["ring", "wring"])
+@pytest.mark.parametrize("kernel", ["ring", "wring", "wring_pair"])
 def test_gauss_seidel_ring_from_zero_bit_exact(oracle, name, sweeps, records, kernel):
     """Sweeps from x = 0 (the first one through the lower-only ring), as a
     PBiCGStab preconditioner applies them: same bits as the oracle's full
@@ -217,7 +221,8 @@ def test_gauss_seidel_ring_from_zero_bit_exact(oracle, name, sweeps, records, ke
     h, om = case(name, oracle)
     A = h.copyToTile()
     b = np.random.default_rng(10).uniform(-1, 1, h.numRows).astype(np.float32)
-    cfg = {"type": "GaussSeidel", "numFixedIterations": sweeps, "kernel": kernel, "recordLevels": records}
+    cfg = {"type": "GaussSeidel", "numFixedIterations": sweeps, "kernel": kernel.split("_")[0],
+           "recordLevels": records, "pairRows": kernel == "wring_pair"}
     x = dev(np.zeros_like(b))
     gb.Solver(A, cfg).solve(x, dev(b))
     ref = np.zeros_like(b)
