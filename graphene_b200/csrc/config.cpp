@@ -256,6 +256,8 @@ std::unique_ptr<SolverConfig> SolverConfig::fromJson(const Json& j) {
     readInt(j, "computeWarps", c->computeWarps);
     mark("waitingWarp");
     readBool(j, "waitingWarp", c->waitingWarp);
+    mark("producerWarp");
+    readBool(j, "producerWarp", c->producerWarp);
     if (c->computeWarps != 0 && c->computeWarps != 1 && c->computeWarps != 2 && c->computeWarps != 4 &&
         c->computeWarps != 8)
       fail(GR_EINVAL, "computeWarps must be 1, 2, 4 or 8");

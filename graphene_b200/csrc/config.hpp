@@ -73,6 +73,9 @@ struct SolverConfig {
   // ILU "waitingWarp": false lets the compute warps wait for each level's
   // copy themselves (no waiting warp; default computeWarps only).
   bool waitingWarp = true;
+  // ILU "producerWarp": false lets the waiting warp issue the level copies
+  // after each level's barrier (no producer warp).
+  bool producerWarp = true;
   // Extension: log2 of the streamed kernel's ring size in bytes (0: the
   // smallest ring that holds the largest level).
   int ringLog2 = 0;

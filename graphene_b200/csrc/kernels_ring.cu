@@ -187,8 +187,13 @@ template <int CW, class W>
 constexpr int ringComputeThreads() {
   return CW > 0 ? 32 * CW : RingShape<W>::compute;
 }
-template <class MV, class W, bool UNROLL, bool COMPACT, int CW = 0, bool WAITER = true>
-__global__ void __launch_bounds__(ringComputeThreads<CW, W>() + (WAITER ? 64 : 32)) iluRingKernel(
+// PRODUCER false (with WAITER): no producer warp; the waiting warp's first
+// lane issues the copies whose ring space level l freed right after the
+// barrier that ends level l (the host schedule issues every level's copy at
+// least one level before it is needed, so the copy the waiting warp waits
+// for has always been issued), and no empty barriers are used.
+template <class MV, class W, bool UNROLL, bool COMPACT, int CW = 0, bool WAITER = true, bool PRODUCER = true>
+__global__ void __launch_bounds__(ringComputeThreads<CW, W>() + (WAITER ? 32 : 0) + (PRODUCER ? 32 : 0)) iluRingKernel(
     const unsigned char* __restrict__ stream,
                                                                const long long* __restrict__ tileOffset,
                                                                const int4* __restrict__ meta,
@@ -215,7 +220,9 @@ __global__ void __launch_bounds__(ringComputeThreads<CW, W>() + (WAITER ? 64 : 3
   unsigned char* ring = smem + kRingHeader + 16 * metaLevels;
   W* xs = reinterpret_cast<W*>(ring + ringBytes);
   const unsigned char* g = stream + tileOffset[T];
-  const bool lead = threadIdx.x == kRingLevelSync;  // the producer warp's issuing lane
+  static_assert(WAITER || PRODUCER, "a ring kernel without a waiting warp needs the producer warp");
+  // The issuing lane: the producer warp's first lane, or the waiting warp's.
+  const bool lead = threadIdx.x == (PRODUCER ? kRingLevelSync : kRingCompute);
   const volatile int* abortV = &abortFlag;
 
   if (lead) {
@@ -258,8 +265,25 @@ __global__ void __launch_bounds__(ringComputeThreads<CW, W>() + (WAITER ? 64 : 3
   }
   __syncthreads();  // barriers initialised, x slice written
 
-  int issued = 0;  // producer: levels whose copies were issued
-  if (threadIdx.x >= kRingLevelSync) {
+  int issued = 0;  // issuing lane: levels whose copies were issued
+  uint32_t src = 0;
+  // Issuing lane without a producer warp: the copies of every level j with
+  // issueAfter(j) <= done, in order (issueAfter never decreases along the
+  // levels; the next one is kept in a register).
+  int nextAfter = INT_MAX;
+  auto issueUpTo = [&](int done) {
+    while (nextAfter <= done) {
+      const int4 m = mt[issued];
+      const uint32_t bytes = RingLevelCode::bytes(m);
+      const uint32_t bar = smemAddr(full + issued % kRingBarriers);
+      mbarExpectTx(bar, bytes);
+      bulkLoad(smemAddr(ring + RingLevelCode::ringOffset(m)), g + src, bytes, bar);
+      src += bytes;
+      ++issued;
+      nextAfter = issued < L ? RingLevelCode::issueAfter(mt[issued]) : INT_MAX;
+    }
+  };
+  if (PRODUCER && threadIdx.x >= kRingLevelSync) {
     // Producer: copies the levels in order, level j once level
     // issueAfter(j) has been released on its empty barrier (after the
     // barrier that ended it, so every read of it is done). It runs ahead of
@@ -269,7 +293,7 @@ __global__ void __launch_bounds__(ringComputeThreads<CW, W>() + (WAITER ? 64 : 3
       if (!mbarWaitBounded(smemAddr(tableBar), 0, abortV)) {
         abortFlag = 1;
       } else {
-        uint32_t src = 0, pf = 0;
+        uint32_t pf = 0;
         const uint32_t tileBytes = static_cast<uint32_t>(tileOffset[T + 1] - tileOffset[T]);
         for (; issued < L && !*abortV; ++issued) {
           const int4 m = mt[issued];
@@ -292,12 +316,17 @@ __global__ void __launch_bounds__(ringComputeThreads<CW, W>() + (WAITER ? 64 : 3
         }
       }
     }
-  } else if (threadIdx.x >= kRingCompute) {
+  } else if (WAITER && threadIdx.x >= kRingCompute) {
     // Waiting warp: before the barrier that ends level l it waits until
     // level l + 1 has landed (so the barrier also publishes the copy to the
-    // compute warps); after it, it releases level l.
-    bool ok = mbarWaitBounded(smemAddr(tableBar), 0, abortV) &&
-              (L == 0 || mbarWaitBounded(smemAddr(full), 0, abortV));
+    // compute warps); after it, it releases level l (or, without a producer
+    // warp, issues the copies that level l's release allows).
+    bool ok = mbarWaitBounded(smemAddr(tableBar), 0, abortV);
+    if (!PRODUCER && ok && lead) {
+      nextAfter = L > 0 ? RingLevelCode::issueAfter(mt[0]) : INT_MAX;
+      issueUpTo(-1);
+    }
+    ok = ok && (L == 0 || mbarWaitBounded(smemAddr(full), 0, abortV));
     if (!ok) abortFlag = 1;
     bool stop = namedBarOr(1, kRingLevelSync, !ok);
     if (stop && threadIdx.x == kRingCompute) consumedLevels = 0;
@@ -309,7 +338,8 @@ __global__ void __launch_bounds__(ringComputeThreads<CW, W>() + (WAITER ? 64 : 3
       }
       stop = namedBarOr(1, kRingLevelSync, bad || *abortV != 0);
       if (threadIdx.x == kRingCompute) {
-        mbarArrive(smemAddr(empty + l % kRingBarriers));
+        if constexpr (PRODUCER) mbarArrive(smemAddr(empty + l % kRingBarriers));
+        else if (!stop) issueUpTo(l);
         if (stop) consumedLevels = l + 1;
       }
     }
@@ -1001,28 +1031,35 @@ void launchRingPack(DeviceMatrix& A, const LevelRing& R, void* stream, const voi
 }
 
 namespace {
-template <class MV, class W, int CW, bool WAITER = true>
+template <class MV, class W, int CW, bool WAITER = true, bool PRODUCER = true>
 auto ringKernelFor(bool compact, bool unroll) {
-  return compact ? (unroll ? dev::iluRingKernel<MV, W, true, true, CW, WAITER>
-                           : dev::iluRingKernel<MV, W, false, true, CW, WAITER>)
-                 : (unroll ? dev::iluRingKernel<MV, W, true, false, CW, WAITER>
-                           : dev::iluRingKernel<MV, W, false, false, CW, WAITER>);
+  return compact ? (unroll ? dev::iluRingKernel<MV, W, true, true, CW, WAITER, PRODUCER>
+                           : dev::iluRingKernel<MV, W, false, true, CW, WAITER, PRODUCER>)
+                 : (unroll ? dev::iluRingKernel<MV, W, true, false, CW, WAITER, PRODUCER>
+                           : dev::iluRingKernel<MV, W, false, false, CW, WAITER, PRODUCER>);
 }
 
 template <class MV, class W>
 void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& p, void* y,
-                int l2Ahead, bool unroll, bool pairRows, cudaStream_t s, int computeWarps, bool waiter) {
+                int l2Ahead, bool unroll, bool pairRows, cudaStream_t s, int computeWarps, bool waiter,
+                bool producer) {
   const size_t smem = iluRingSmem(A, R, dtypeOf<W>());
   if (computeWarps != 0 && computeWarps != 1 && computeWarps != 2 && computeWarps != 4 && computeWarps != 8)
     fail(GR_EINVAL, "computeWarps must be 1, 2, 4 or 8 (0: the default)");
   if (!waiter && computeWarps != 0) fail(GR_EINVAL, "waitingWarp false needs the default computeWarps");
+  if (!waiter && !producer) fail(GR_EINVAL, "producerWarp false needs the waiting warp");
+  if (!producer && computeWarps != 0 && computeWarps != 4)
+    fail(GR_EINVAL, "producerWarp false runs with the default computeWarps or 4");
   auto kernel = !waiter             ? ringKernelFor<MV, W, 0, false>(R.compact, unroll)
+                : !producer         ? (computeWarps == 4 ? ringKernelFor<MV, W, 4, true, false>(R.compact, unroll)
+                                                         : ringKernelFor<MV, W, 0, true, false>(R.compact, unroll))
                 : computeWarps == 1 ? ringKernelFor<MV, W, 1>(R.compact, unroll)
                 : computeWarps == 2 ? ringKernelFor<MV, W, 2>(R.compact, unroll)
                 : computeWarps == 4 ? ringKernelFor<MV, W, 4>(R.compact, unroll)
                 : computeWarps == 8 ? ringKernelFor<MV, W, 8>(R.compact, unroll)
                                     : ringKernelFor<MV, W, 0>(R.compact, unroll);
-  const int threads = (computeWarps > 0 ? 32 * computeWarps : dev::RingShape<W>::compute) + (waiter ? 64 : 32);
+  const int threads =
+      (computeWarps > 0 ? 32 * computeWarps : dev::RingShape<W>::compute) + (waiter ? 32 : 0) + (producer ? 32 : 0);
   ensureDynamicSmem(reinterpret_cast<const void*>(kernel), smem);
   preferSharedCarveout(reinterpret_cast<const void*>(kernel));
   if (p.stIndex && R.group != 1) fail(GR_EUNSUPPORTED, "batched solves run one tile per block");
@@ -1166,13 +1203,16 @@ void launchIluWarpRing(DeviceMatrix& A, const LevelRing& R, const void* stream, 
 
 void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,
                    void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s, bool pairRows, int computeWarps,
-                   bool waiter) {
+                   bool waiter, bool producer) {
   if (A.vt == DType::F32 && W == DType::F32)
-    ringApplyT<float, float>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps, waiter);
+    ringApplyT<float, float>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps, waiter,
+                             producer);
   else if (A.vt == DType::F32 && W == DType::F64)
-    ringApplyT<float, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps, waiter);
+    ringApplyT<float, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps, waiter,
+                              producer);
   else if (A.vt == DType::F64 && W == DType::F64)
-    ringApplyT<double, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps, waiter);
+    ringApplyT<double, double>(A, R, stream, dilu, pro, y, l2Ahead, unroll, pairRows, s, computeWarps, waiter,
+                               producer);
   else fail(GR_EUNSUPPORTED, "ILU apply with float64 coefficients and float32 vectors");
 }
 

@@ -94,10 +94,11 @@ void launchRingPack(DeviceMatrix& A, const LevelRing& R, void* stream, const voi
 size_t iluWarpRingSmem(const LevelRing& R, DType W, int warpsPerBlock);
 void launchIluWarpRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,
                        void* y, DType W, int warpsPerBlock, bool pairRows, cudaStream_t s);
-// pairRows: record levels process two rows a thread at once.
+// pairRows: record levels process two rows a thread at once; producer
+// false: the waiting warp issues the level copies (no producer warp).
 void launchIluRing(DeviceMatrix& A, const LevelRing& R, const void* stream, bool dilu, const PrologueArgs& pro,
                    void* y, DType W, int l2Ahead, bool unroll, cudaStream_t s, bool pairRows = false, int computeWarps = 0,
-                   bool waiter = true);
+                   bool waiter = true, bool producer = true);
 // One Gauss-Seidel sweep through a Gauss-Seidel level ring (kernels_ring.cu):
 // xout from xin (xinZero: xin is all zeros and is not read; the ring may
 // then be a lower-only one). The right-hand side is the prologue's vector

@@ -169,7 +169,7 @@ class IluNode : public Node {
       launchIluWarpRing(A_, *ring_, stream_.get(), dilu_, pro, y, W, cfg_.warpsPerBlock, cfg_.pairRows, s());
     else if (kernel_ == 4)
       launchIluRing(A_, *ring_, stream_.get(), dilu_, pro, y, W, cfg_.l2Ahead, cfg_.unrollRows != 0, s(),
-                    cfg_.pairRows, cfg_.computeWarps, cfg_.waitingWarp);
+                    cfg_.pairRows, cfg_.computeWarps, cfg_.waitingWarp, cfg_.producerWarp);
     else if (kernel_ == 3)
       launchIluWarp(A_, *sweep_, stream_.get(), dilu_, pro, y, W, rowsPerLane_, s());
     else if (kernel_ == 1)

@@ -54,11 +54,14 @@ NAMES = ["poisson16", "poisson_odd_bfs", "poisson_1tile", "random", "many_tiles"
 
 def ilu_config(kernel, **kw):
     """'ring_wide': the ring kernel with 32-bit row and column ids;
-    'ring_rec': with 16-byte row records for levels of 3 entries a row."""
+    'ring_rec': with 16-byte row records for levels of 3 entries a row;
+    'ring_noprod': records, the waiting warp issuing the copies."""
     c = {"type": "ILU", "kernel": "ring" if kernel in ("ring_wide", "ring_rec", "ring_pair", "ring_cw4", "ring_cw1",
-                                                        "ring_nowait") else kernel}
+                                                        "ring_nowait", "ring_noprod") else kernel}
     if kernel == "ring_nowait":
         c["waitingWarp"] = False
+    if kernel == "ring_noprod":
+        c["producerWarp"] = False
     if kernel in ("ring_cw4", "ring_cw1"):
         c["computeWarps"] = int(kernel[-1])
     if kernel.startswith("wring"):
@@ -66,7 +69,7 @@ def ilu_config(kernel, **kw):
     if kernel == "ring_wide":
         c["compactRing"] = False
     # Record levels are the default; the plain names run without them.
-    c["recordLevels"] = kernel in ("ring_rec", "ring_pair", "ring_cw4", "ring_cw1", "ring_nowait", "wring_rec",
+    c["recordLevels"] = kernel in ("ring_rec", "ring_pair", "ring_cw4", "ring_cw1", "ring_nowait", "ring_noprod", "wring_rec",
                                    "wring_pair", "wring_w4")
     if kernel in ("ring_pair", "wring_pair"):
         c["pairRows"] = True
@@ -79,7 +82,7 @@ def ilu_config(kernel, **kw):
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("dilu", [False, True])
 @pytest.mark.parametrize("kernel", ["ring", "ring_rec", "ring_pair", "ring_wide", "ring_cw4", "ring_cw1", "ring_nowait",
-                                    "wring", "wring_rec", "wring_pair",
+                                    "ring_noprod", "wring", "wring_rec", "wring_pair",
                                     "wring_w4", "warp", "tma", "levels"])
 def test_ilu_bit_exact(oracle, name, dilu, kernel):
     h, om = case(name, oracle)
@@ -107,13 +110,20 @@ def test_ilu_bit_exact_float64(oracle, name, kernel):
 @pytest.mark.parametrize("name", ["poisson16", "many_tiles", "random", "poisson_odd_bfs"])
 @pytest.mark.parametrize("group", [2, 3, 8])
 @pytest.mark.parametrize("dilu", [False, True])
-def test_ilu_ring_tile_groups_bit_exact(oracle, name, group, dilu):
-    """Several tiles per thread block, run level by level in lockstep: same bits."""
+@pytest.mark.parametrize("warps", ["default", "cw4", "cw8", "cw4_noprod"])
+def test_ilu_ring_tile_groups_bit_exact(oracle, name, group, dilu, warps):
+    """Several tiles per thread block, run level by level in lockstep, with
+    2, 4 or 8 compute warps, with or without the producer warp: same bits."""
     h, om = case(name, oracle)
     A = h.copyToTile()
     b = np.random.default_rng(7).uniform(-1, 1, h.numRows).astype(np.float32)
     x = A.createUninitializedVector(gb.FLOAT32)
-    gb.Solver(A, {"type": "ILU", "kernel": "ring", "tilesPerBlock": group, "diagonalBased": dilu}).solve(x, dev(b))
+    cfg = {"type": "ILU", "kernel": "ring", "tilesPerBlock": group, "diagonalBased": dilu}
+    if warps != "default":
+        cfg["computeWarps"] = int(warps[2])
+    if warps.endswith("noprod"):
+        cfg["producerWarp"] = False
+    gb.Solver(A, cfg).solve(x, dev(b))
     off, inv = om.ilu_factorize(dilu)
     np.testing.assert_array_equal(host(x), om.ilu_solve(off, inv, b, dilu))
 
