@@ -373,21 +373,14 @@ def other_configs(gb, peak):
     del A64
     n, F = h.numRows, h.numOffDiag // 2
     y = torch.empty_like(b)
-    flush = torch.ones(64 << 20, dtype=torch.float32, device="cuda")  # 256 MB > L2, read to evict
-    times = []
-    for i in range(23):
-        float(flush.sum())
-        t, _ = event_ms(lambda: A.spmv(b, y))
-        if i >= 3:
-            times.append(t)
-    t = statistics.median(times)
+    t = A.timeSpmv(b, y, reps=20, flushL2=True)  # each launch alone between CUDA events, L2 flushed first
     ldu_bytes = 20 * n + 20 * F       # reference LDU arrays: cells 5 x 4 B, faces 5 x 4 B
     layout_bytes = 16 * F + 16 * n + 4  # this library's layout: 2F (col, value) pairs, diag, x, y, rowPtr
     out["ldu100_spmv"] = {"ms": t, "cells": n, "faces": F,
                           "GBs_ldu_algorithmic": ldu_bytes / (t * 1e-3) / 1e9,
                           "GBs_device_layout": layout_bytes / (t * 1e-3) / 1e9,
                           "frac_of_hbm_device_layout": layout_bytes / (t * 1e-3) / 1e9 / peak,
-                          "l2": "flushed (256 MB read) before each launch"}
+                          "l2": "flushed (256 MB write) before each launch"}
     return out
 
 
@@ -813,9 +806,7 @@ def main():
         # in and x out).
         y64 = torch.empty_like(b64)
         A64.tuneSpmv(gb.FLOAT64, reps=5)
-        for _ in range(5):
-            A64.spmv(b64, y64)
-        spmv64_ms = event_ms(lambda: [A64.spmv(b64, y64) for _ in range(50)])[0] / 50
+        spmv64_ms = A64.timeSpmv(b64, y64, reps=50, flushL2=False)  # each launch alone, matrix > L2
         ilu64 = gb.Solver(A64, {"type": "ILU"})
         z64 = torch.empty_like(b64)
         ilu64.timeRepeated(z64, b64, 3)
@@ -839,9 +830,7 @@ def main():
     # Kernel timings: SpMV and the ILU(0) application (HBM rooflines).
     y = torch.empty_like(x_true)
     tuned = A.tuneSpmv(gb.FLOAT32, reps=5)  # SpMV launch geometry (results unchanged)
-    for _ in range(5):
-        A.spmv(x_true, y)
-    spmv_ms = event_ms(lambda: [A.spmv(x_true, y) for _ in range(50)])[0] / 50
+    spmv_ms = A.timeSpmv(x_true, y, reps=50, flushL2=False)  # each launch alone, matrix > L2
     spmv_bytes = 8 * m + 16 * n + 4
     ilu = gb.Solver(A, {"type": "ILU"})
     z = torch.empty_like(x_true)

@@ -544,6 +544,14 @@ class Matrix:
         check(_lib.lib().gr_matrix_spmv_layout(self._m, C.byref(c), C.byref(sl), C.byref(far)))
         return {"compact": bool(c.value), "slots": sl.value, "far": far.value}
 
+    def timeSpmv(self, x, y, reps: int = 20, flushL2: bool = True) -> float:
+        """Mean device time in ms of y = A x (gr_matrix_time_spmv): each launch
+        timed alone with CUDA events, L2 flushed before it when flushL2."""
+        ms = C.c_float()
+        check(_lib.lib().gr_matrix_time_spmv(self._m, _ptr(x), _ptr(y), _dtype_of(x), int(reps), int(flushL2),
+                                             C.byref(ms)))
+        return float(ms.value)
+
     def tuneSpmv(self, t: int = FLOAT32, reps: int = 5) -> dict:
         """Runs the SpMV autotuner (gr_matrix_tune_spmv) for vectors of type t."""
         v = [C.c_int32() for _ in range(3)]

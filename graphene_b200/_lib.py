@@ -124,6 +124,7 @@ SIGNATURES = {
     "gr_vector_norms_noalloc": (C.c_int, [vp, i64, i64, i64, C.c_int, C.c_int, vp, vp]),
     "gr_solver_time_repeated": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, i32, P(C.c_float)]),
     "gr_matrix_tune_spmv": (C.c_int, [vp, C.c_int, i32, P(i32), P(i32), P(i32), P(C.c_float)]),
+    "gr_matrix_time_spmv": (C.c_int, [vp, vp, vp, C.c_int, i32, i32, P(C.c_float)]),
     "gr_server_create": (C.c_int, [P(ServerConfig), P(vp)]),
     "gr_server_submit": (C.c_int, [vp, vp, C.c_char_p, vp, C.c_int, P(C.c_uint64)]),
     "gr_server_wait": (C.c_int, [vp, C.c_uint64, C.c_double, vp, P(Stats), P(RequestTimes)]),

@@ -543,6 +543,17 @@ int gr_matrix_tune_spmv(gr_matrix* A, gr_dtype t, int32_t reps, int32_t* block, 
   });
 }
 
+int gr_matrix_time_spmv(gr_matrix* A, const void* x, void* y, gr_dtype t, int32_t reps, int32_t flush_l2,
+                        float* ms) {
+  return guarded([&] {
+    need(A, "matrix");
+    need(x, "x");
+    need(y, "y");
+    need(ms, "ms");
+    *ms = gr::timeSpmv(*A->d, x, y, gr::toDType(t), reps, flush_l2 != 0);
+  });
+}
+
 int gr_vector_norm(gr_matrix* A, gr_norm norm, const void* x, gr_dtype t, double* out) {
   return guarded([&] {
     need(A, "matrix");

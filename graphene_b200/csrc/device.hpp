@@ -473,6 +473,10 @@ int sellKernelOccupancy(DType vt, bool c16);
 // matrix's stream and keeps the fastest for vectors of type t. The results
 // of gr_spmv do not depend on the geometry.
 SpmvTuning tuneSpmv(DeviceMatrix& A, DType t, int reps);
+// Mean device time (ms) of y = A x with the current geometry over `reps`
+// launches, each timed alone on the matrix's stream (L2 flushed first when
+// flushL2).
+float timeSpmv(DeviceMatrix& A, const void* x, void* y, DType t, int reps, bool flushL2);
 
 // r = b - A x in inter (reference CRSMatrix::residual); optionally
 // accumulates a norm of r into normOut (device double) when normKind >= 0.

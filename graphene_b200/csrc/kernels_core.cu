@@ -859,6 +859,38 @@ SpmvTuning tuneSpmv(DeviceMatrix& A, DType t, int reps) {
   return best;
 }
 
+float timeSpmv(DeviceMatrix& A, const void* x, void* y, DType t, int reps, bool flushL2) {
+  if (reps < 1 || reps > 10000) fail(GR_EINVAL, "reps must be 1..10000");
+  // Each launch is timed alone between two events on the matrix's stream;
+  // with flushL2, a 256 MB write (twice the B200's 126 MB L2) precedes it.
+  const size_t flushBytes = flushL2 ? size_t(256) << 20 : 0;
+  DBuf flush(flushBytes > 0 ? flushBytes : 16);
+  cudaEvent_t e0, e1;
+  GR_CUDA(cudaEventCreate(&e0));
+  GR_CUDA(cudaEventCreate(&e1));
+  float total = 0;
+  try {
+    launchSpmv(A, x, y, t, A.stream);  // warm-up
+    for (int r = 0; r < reps; ++r) {
+      if (flushL2) GR_CUDA(cudaMemsetAsync(flush.get(), r & 0xFF, flushBytes, A.stream));
+      GR_CUDA(cudaEventRecord(e0, A.stream));
+      launchSpmv(A, x, y, t, A.stream);
+      GR_CUDA(cudaEventRecord(e1, A.stream));
+      GR_CUDA(cudaEventSynchronize(e1));
+      float one = 0;
+      GR_CUDA(cudaEventElapsedTime(&one, e0, e1));
+      total += one;
+    }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return total / static_cast<float>(reps);
+}
+
 void launchResidual(DeviceMatrix& A, const void* x, DType xt, const void* b, DType bt, void* r,
                     DType rt, DType inter, int normKind, double* normOut, cudaStream_t s) {
   int blocks = A.spmvBlocks();

@@ -364,6 +364,13 @@ int gr_spmv(gr_matrix* A, const void* x, void* y, gr_dtype t);
 int gr_matrix_tune_spmv(gr_matrix* A, gr_dtype t, int32_t reps, int32_t* block, int32_t* chunks_per_warp,
                         int32_t* batch, float* ms);
 
+/* Benchmarking (no counterpart in the reference): the mean device time (ms)
+ * of y = A x (gr_spmv's kernel, current geometry) over reps launches, each
+ * timed alone between two CUDA events on the matrix's stream, with L2
+ * flushed before each launch when flush_l2 is nonzero (a 256 MB write). */
+int gr_matrix_time_spmv(gr_matrix* A, const void* x, void* y, gr_dtype t, int32_t reps, int32_t flush_l2,
+                        float* ms);
+
 /* Replaces Matrix::residual(x, b, destType, intermediateType)
  * (matrix/Matrix.hpp:86-92, CRSMatrix.cpp:85-128): r = b - A x computed in
  * inter_t and rounded to r_t. x_t may be FLOAT32, FLOAT64 or TWOFLOAT32,

@@ -180,3 +180,18 @@ def test_spmv_autotuner_keeps_results(oracle, vt):
     g = A.tuneSpmv(vt, reps=3)
     assert g["block"] in (128, 256, 512) and g["batch"] in (4, 8, 16) and g["ms"] > 0
     np.testing.assert_array_equal((A * x).cpu().numpy(), before)
+
+
+@pytest.mark.parametrize("flush", [False, True])
+def test_spmv_device_timing_writes_the_product(flush):
+    """gr_matrix_time_spmv launches the SpMV kernel itself: it reports a
+    positive device time and leaves y = A x, bit-identical to gr_spmv."""
+    h = gb.generateMatrix(gb.GEN_VAR_POISSON, 24, 20, 18, (1.0,), 3, 16)
+    A = h.copyToTile()
+    x = dev(np.random.default_rng(10).standard_normal(h.numRows).astype(np.float32))
+    y = A.createUninitializedVector(gb.FLOAT32)
+    ms = A.timeSpmv(x, y, reps=3, flushL2=flush)
+    assert 0 < ms < 1000
+    np.testing.assert_array_equal(y.cpu().numpy(), (A * x).cpu().numpy())
+    with pytest.raises(gb.GrapheneError):
+        A.timeSpmv(x, y, reps=0)
