@@ -97,6 +97,10 @@ __device__ __forceinline__ bool namedBarOr(int id, int count, bool v) {
       : "memory");
   return out != 0;
 }
+// Named barrier without a reduction (bar.sync id, count).
+__device__ __forceinline__ void namedBarSync(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
 // Hint: bring [src, src + bytes) into L2 (no completion, no shared memory).
 __device__ __forceinline__ void prefetchL2(const void* src, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
