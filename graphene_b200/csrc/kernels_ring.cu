@@ -115,13 +115,17 @@ template <class MV, bool COMPACT>
 __device__ __forceinline__ RowRecord ringRecord(const RingLevel<MV, COMPACT>& lv, int q, bool hasInv) {
   RowRecord r;
   const float4 a = reinterpret_cast<const float4*>(lv.blk)[q];
+  // The {c2 | row, inverse diagonal} words follow the k records (the host
+  // lays record levels out so that ents == 16 k; the ring check verifies
+  // it), so their address comes from k without decoding the table entry.
+  const unsigned char* words = lv.blk + 16 * lv.k;
   uint32_t w2;
   if (hasInv) {
-    const uint2 b = reinterpret_cast<const uint2*>(lv.blk + lv.ents)[q];
+    const uint2 b = reinterpret_cast<const uint2*>(words)[q];
     w2 = b.x;
     r.inv = __uint_as_float(b.y);
   } else {
-    w2 = reinterpret_cast<const uint32_t*>(lv.blk + lv.ents)[q];
+    w2 = reinterpret_cast<const uint32_t*>(words)[q];
     r.inv = 0.0f;
   }
   const uint32_t w01 = __float_as_uint(a.w);
