@@ -61,6 +61,8 @@ def test_comments_and_unknown_keys():
     ({"type": "ILU", "solveMulticolor": "sometimes"}, 3),             # Configuration.cpp:66-69
     ({"type": "PBiCGStab", "maxIterations": "many"}, 3),
     ({"type": "GaussSeidel", "halo": "fresh"}, 3),                    # stale | drop
+    ({"type": "ILU", "computeWarps": 3}, 1),                          # 1, 2, 4 or 8 (GR_EINVAL)
+    ({"type": "ILU", "tilesPerBlock": 65}, 1),
 ])
 def test_invalid_configs(cfg, code):
     with pytest.raises(gb.GrapheneError) as e:
@@ -79,6 +81,16 @@ def test_gauss_seidel_halo_modes():
     for v in ["stale", "drop"]:
         c = gb.Configuration.fromJSON({"type": "GaussSeidel", "halo": v})
         assert "halo" not in c.unknownKeys
+
+
+def test_ring_kernel_options_are_known_keys():
+    """The ILU ring kernel's launch options parse and are not reported as
+    unknown keys."""
+    c = gb.Configuration.fromJSON({"type": "ILU", "kernel": "ring", "computeWarps": 8, "tilesPerBlock": 2,
+                                   "producerWarp": False, "waitingWarp": True, "pairRows": False})
+    assert not set(c.unknownKeys) & {"computeWarps", "tilesPerBlock", "producerWarp", "waitingWarp", "pairRows"}
+    g = gb.Configuration.fromJSON({"type": "GaussSeidel", "kernel": "wring", "pairRows": True})
+    assert "pairRows" not in g.unknownKeys
 
 
 def test_malformed_json():
