@@ -1109,6 +1109,29 @@ void ringApplyT(DeviceMatrix& A, const LevelRing& R, const void* stream, bool di
 }
 }  // namespace
 
+int iluRingBlocksPerSM(const DeviceMatrix& A, const LevelRing& R, DType W, int computeWarps) {
+  const size_t smem = iluRingSmem(A, R, W);
+  const void* fn = nullptr;
+  int threads = 0;
+  if (W == DType::F32) {
+    fn = reinterpret_cast<const void*>(computeWarps == 4 ? ringKernelFor<float, float, 4>(R.compact, true)
+                                                         : ringKernelFor<float, float, 0>(R.compact, true));
+    threads = (computeWarps == 4 ? 128 : dev::RingShape<float>::compute) + 64;
+  } else {
+    fn = reinterpret_cast<const void*>(computeWarps == 4 ? ringKernelFor<double, double, 4>(R.compact, true)
+                                                         : ringKernelFor<double, double, 0>(R.compact, true));
+    threads = (computeWarps == 4 ? 128 : dev::RingShape<double>::compute) + 64;
+  }
+  ensureDynamicSmem(fn, smem);
+  preferSharedCarveout(fn);
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, smem) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
 int ringBlocksPerSMWithoutSmem(DType vt, RingKind kind) {
   int n = 0;
   const bool gs = kind != RingKind::Ilu;

@@ -85,6 +85,9 @@ void launchPackBytes(DeviceMatrix& A, const void* templ, i64 bytes, const int* v
 // is not the limit (0 if unknown).
 int ringBlocksPerSMWithoutSmem(DType vt, RingKind kind = RingKind::Ilu);
 size_t iluRingSmem(const DeviceMatrix& A, const LevelRing& R, DType W);
+// Blocks of the ring substitution kernel resident per SM for vectors of
+// type W with the default compute warps (computeWarps 0) or four.
+int iluRingBlocksPerSM(const DeviceMatrix& A, const LevelRing& R, DType W, int computeWarps);
 void launchRingPack(DeviceMatrix& A, const LevelRing& R, void* stream, const void* F, const void* inv,
                     cudaStream_t s);
 // l2Ahead: bytes kept prefetched into L2 beyond the issued copies (-1:

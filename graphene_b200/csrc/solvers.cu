@@ -97,6 +97,7 @@ class IluNode : public Node {
       if (R && iluRingSmem(A, *R, DType::F64) <= smemMax) {
         kernel_ = 4;
         ring_ = R;
+        autoGroups(A, c, smemMax);
       } else if (c.iluKernel == 4) {
         fail(GR_EUNSUPPORTED, "the ring ILU kernel does not fit this matrix's tiles in shared memory");
       }
@@ -169,7 +170,8 @@ class IluNode : public Node {
       launchIluWarpRing(A_, *ring_, stream_.get(), dilu_, pro, y, W, cfg_.warpsPerBlock, cfg_.pairRows, s());
     else if (kernel_ == 4)
       launchIluRing(A_, *ring_, stream_.get(), dilu_, pro, y, W, cfg_.l2Ahead, cfg_.unrollRows != 0, s(),
-                    cfg_.pairRows, cfg_.computeWarps, cfg_.waitingWarp, cfg_.producerWarp);
+                    cfg_.pairRows, cfg_.computeWarps != 0 ? cfg_.computeWarps : autoWarps_, cfg_.waitingWarp,
+                    cfg_.producerWarp);
     else if (kernel_ == 3)
       launchIluWarp(A_, *sweep_, stream_.get(), dilu_, pro, y, W, rowsPerLane_, s());
     else if (kernel_ == 1)
@@ -182,6 +184,37 @@ class IluNode : public Node {
 
  private:
   bool dilu_;
+  // Tile groups (automatic, ring kernel, FP32 coefficients, default warps):
+  // two consecutive tiles a block with four compute warps when the tiles
+  // fill at least two waves of one-tile blocks and the grouped blocks take
+  // no more waves. The waiting and producer warps' per-level work is then
+  // shared by two tiles; on B200 at 192^3 with 2368 tiles that ran the
+  // substitution in 104.4 us against 111.8 (MPIR 121.7 against 125.0 ms),
+  // while at 2048 tiles, where grouping adds a wave, it ran slower. FP64
+  // coefficients keep one tile a block (their slices halve the blocks per
+  // SM).
+  void autoGroups(DeviceMatrix& A, const SolverConfig& c, size_t smemMax) {
+    if (c.tilesPerBlock != 0 || c.computeWarps != 0 || !c.waitingWarp || !c.producerWarp || A.vt != DType::F32 ||
+        A.batch)  // batched solves run one tile a block
+      return;
+    const long long b1 = iluRingBlocksPerSM(A, *ring_, DType::F32, 0);
+    const long long slots1 = b1 * A.numSMs;
+    if (b1 <= 0 || ring_->numGroups < 2 * slots1) return;
+    const long long waves1 = (ring_->numGroups + slots1 - 1) / slots1;
+    LevelRing* R2 = nullptr;
+    try {
+      R2 = &A.levelRing(dilu_, c.ringBytes, 2, c.compactRing, RingKind::Ilu, c.ringRecords);
+    } catch (const Error&) {
+      return;
+    }
+    if (iluRingSmem(A, *R2, DType::F64) > smemMax) return;
+    const long long b2 = iluRingBlocksPerSM(A, *R2, DType::F32, 4);
+    const long long slots2 = b2 * A.numSMs;
+    if (b2 <= 0 || (R2->numGroups + slots2 - 1) / slots2 > waves1) return;
+    ring_ = R2;
+    autoWarps_ = 4;
+  }
+  int autoWarps_ = 0;  // compute warps chosen with automatic tile groups
   int kernel_ = 2;  // 1 tma ring, 2 level schedule, 3 warp per tile, 4 host-scheduled ring, 5 its warp-per-tile form
   int rowsPerLane_ = 2;
   DBuf inv_, Lval_, Uval_, stream_;
