@@ -79,6 +79,9 @@ def parse_args():
     p.add_argument("--inner-maxit", type=int, default=500)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true")
+    p.add_argument("--tiles-per-block", type=int, default=0,
+                   help="ILU ring: tiles a block (0: automatic; 2 also sets four compute warps), for profiling "
+                        "the grouped kernel on a case where it is not chosen automatically")
     p.add_argument("--cpu-threads", type=int, default=0)
     p.add_argument("--case", choices=sorted(CASES), default=None,
                    help="run one benchmark configuration alone (timing and profiling): "
@@ -94,11 +97,14 @@ def hbm_peak():
 
 
 def mpir_config(a, ext="float64", tol=None):
+    pre = {"type": "ILU"}
+    if a.tiles_per_block > 0:
+        pre.update({"tilesPerBlock": a.tiles_per_block, "computeWarps": 4 if a.tiles_per_block > 1 else 0})
     return {"type": "IterativeRefinement", "relResidual": 1e-10, "maxIterations": 50,
             "extendedPrecisionType": ext,
             "innerSolver": {"type": "PBiCGStab", "maxIterations": a.inner_maxit,
                             "relResidual": a.inner_tol if tol is None else tol,
-                            "preconditioner": {"type": "ILU"}}}
+                            "preconditioner": pre}}
 
 
 FP64_CONFIG = {"type": "PBiCGStab", "maxIterations": 20000, "relResidual": 1e-10,
