@@ -882,9 +882,10 @@ def main():
     else:
         dom = ("spmv", "spmvDotKernel", spmv_bytes, spmv_ms)
     # DRAM bytes per launch of the dominant kernel from the committed ncu
-    # summary (a 160^3 capture scaled by rows to one 192^3 launch).
+    # summary (a 160^3 capture of the two-tiles-a-block kernel the 192^3
+    # solve runs, scaled by rows to one 192^3 launch).
     traffic = None
-    tf = ROOT / "profiles" / "ilu_ring_var_poisson_160.md"
+    tf = ROOT / "profiles" / "ilu_ring_grouped_var_poisson_160.md"
     if dom[0] == "ilu0_apply" and a.grid == 192 and tf.exists():
         import re
         hit = re.search(r"traffic_bytes_192: (\d+)", tf.read_text())
