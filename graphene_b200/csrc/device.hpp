@@ -413,6 +413,16 @@ struct DeviceMatrix {
   // Small device scratch for norms returned to the host.
   DBuf scalarOut;  // double[8]
 
+  // Staging vectors of host-buffer solves (b, x and a permutation buffer),
+  // kept across solvers of this matrix so that a solve from host memory
+  // allocates nothing after the first. Solves of one matrix are ordered on
+  // its stream, so they never use them at the same time.
+  DBuf stage[3];
+  void* staging(int i, size_t bytes) {
+    if (stage[i].bytes() < bytes) stage[i].alloc(bytes);
+    return stage[i].get();
+  }
+
   explicit DeviceMatrix(std::shared_ptr<HostMatrix> h);
   ~DeviceMatrix();
 

@@ -1046,15 +1046,17 @@ class Tree : public SolverTree {
   gr_stats solveHost(void* x, DType xt, const void* b, DType bt) override {
     if (xt != bt) fail(GR_EINVAL, "x and b must have the same type");
     const size_t bytes = A_.n * dtypeSize(xt);
-    DBuf tmp(bytes), xd(bytes), bd(bytes);
+    void* tmp = A_.staging(0, bytes);
+    void* xd = A_.staging(1, bytes);
+    void* bd = A_.staging(2, bytes);
     cudaStream_t s = A_.stream;
-    GR_CUDA(cudaMemcpyAsync(tmp.get(), b, bytes, cudaMemcpyHostToDevice, s));
-    launchPermute(A_, tmp.get(), bd.get(), xt, true, s);
-    GR_CUDA(cudaMemcpyAsync(tmp.get(), x, bytes, cudaMemcpyHostToDevice, s));
-    launchPermute(A_, tmp.get(), xd.get(), xt, true, s);
-    gr_stats st = solve(xd.get(), xt, bd.get(), bt);
-    launchPermute(A_, xd.get(), tmp.get(), xt, false, s);
-    GR_CUDA(cudaMemcpyAsync(x, tmp.get(), bytes, cudaMemcpyDeviceToHost, s));
+    GR_CUDA(cudaMemcpyAsync(tmp, b, bytes, cudaMemcpyHostToDevice, s));
+    launchPermute(A_, tmp, bd, xt, true, s);
+    GR_CUDA(cudaMemcpyAsync(tmp, x, bytes, cudaMemcpyHostToDevice, s));
+    launchPermute(A_, tmp, xd, xt, true, s);
+    gr_stats st = solve(xd, xt, bd, bt);
+    launchPermute(A_, xd, tmp, xt, false, s);
+    GR_CUDA(cudaMemcpyAsync(x, tmp, bytes, cudaMemcpyDeviceToHost, s));
     GR_CUDA(cudaStreamSynchronize(s));
     return st;
   }
