@@ -201,6 +201,11 @@ class IluNode : public Node {
     const long long slots1 = b1 * A.numSMs;
     if (b1 <= 0 || ring_->numGroups < 2 * slots1) return;
     const long long waves1 = (ring_->numGroups + slots1 - 1) / slots1;
+    // A two-tile block holds twice the x slice and about twice the ring, so
+    // at most (b1 + 1) / 2 fit an SM: skip building the grouped ring when
+    // even that many would need more waves.
+    const long long g2 = (ring_->numGroups + 1) / 2, slotsMax = (b1 + 1) / 2 * A.numSMs;
+    if ((g2 + slotsMax - 1) / slotsMax > waves1) return;
     LevelRing* R2 = nullptr;
     try {
       R2 = &A.levelRing(dilu_, c.ringBytes, 2, c.compactRing, RingKind::Ilu, c.ringRecords);
